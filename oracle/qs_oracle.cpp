@@ -1,0 +1,623 @@
+/*
+ * Test infrastructure only — the CPU oracle for the QuickSampling (QS)
+ * per-node hot path.  It restates, in this project's own code, the G2S
+ * reference algorithm for a vector (all variables at once) QS simulation:
+ *
+ *   search template          G2S src/qs.cpp:1010-1137, include/DataImage.hpp:433-490
+ *   path, per-node seeds     G2S src/qs.cpp:975,1159-1201,1250-1258,1604-1641
+ *   neighbour gathering      G2S include/simulation.hpp:447-537
+ *   weights / constant       G2S include/quantileSamplingModule.hpp:368-457
+ *   layers and coefficients  G2S include/DataImage.hpp:538-599,626-710
+ *   mismatch map + border    G2S src/CPUThreadDevice.cpp:349-490 (direct sum here,
+ *                            not FFT: in FP32 with a fixed term order, and in FP64)
+ *   k-best with reservoir    G2S include/fKb.hpp:58-92,121-132,907-954,
+ *                            include/quantileSamplingModule.hpp:45-49,525-557
+ *   draw                     G2S include/quantileSamplingModule.hpp:90-126,
+ *                            src/CPUThreadDevice.cpp:257-268, include/simulation.hpp:556-666
+ *
+ * The FP32 map uses exactly the term order and the fused multiply-adds that
+ * the CUDA kernels use, so the GPU path can be checked bit for bit; the FP64
+ * map gives the exact reference scores used to classify near-ties.  Only the
+ * tests, the smoke check and the CPU-baseline leg of bench.py load this
+ * library; the product never does.
+ */
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <numeric>
+#include <random>
+#include <vector>
+
+namespace {
+
+/* ------------------------------------------------------------------ */
+/* problem description                                                 */
+/* ------------------------------------------------------------------ */
+struct Grid {
+    int nd = 0;
+    unsigned dims[8] = {0};
+    int nvar = 0;
+    size_t cells() const {
+        size_t c = 1;
+        for (int i = 0; i < nd; ++i) c *= dims[i];
+        return c;
+    }
+};
+
+/* x-fastest flat index of a coordinate vector */
+static inline long flat(const Grid &g, const int *c) {
+    long f = 0;
+    for (int d = g.nd - 1; d >= 0; --d) f = f * long(g.dims[d]) + c[d];
+    return f;
+}
+
+static inline void coords(const Grid &g, long f, int *c) {
+    for (int d = 0; d < g.nd; ++d) {
+        c[d] = int(f % long(g.dims[d]));
+        f /= long(g.dims[d]);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* a1: search template                                                 */
+/* ------------------------------------------------------------------ */
+/* Offsets of the kernel box, in the generation order of G2S
+ * src/qs.cpp:1055-1080, kernel-NaN offsets removed (:1107-1128), then sorted
+ * nearest first with the reference's (unstable) std::sort on -|o|^2
+ * (:1085-1089,1130-1135). */
+std::vector<std::vector<int>> make_template(int nd, const unsigned *kdims, const float *kernel, int knvar) {
+    std::vector<std::vector<int>> pos;
+    pos.push_back(std::vector<int>());
+    for (int i = 0; i < nd; ++i) {
+        size_t orig = pos.size();
+        int half = (int(kdims[i]) + 1) / 2;
+        pos.resize(orig * (2 * half - 1));
+        for (size_t k = 0; k < orig; ++k) pos[k].push_back(0);
+        for (int j = 1; j < half; ++j) {
+            std::copy(pos.begin(), pos.begin() + orig, pos.begin() + orig * (2 * j - 1));
+            std::copy(pos.begin(), pos.begin() + orig, pos.begin() + orig * (2 * j));
+            for (size_t k = orig * (2 * j - 1); k < orig * (2 * j); ++k) pos[k][i] = j;
+            for (size_t k = orig * (2 * j); k < orig * (2 * j + 1); ++k) pos[k][i] = -j;
+        }
+    }
+    if (kernel) {
+        Grid kg;
+        kg.nd = nd;
+        for (int d = 0; d < nd; ++d) kg.dims[d] = kdims[d];
+        std::vector<std::vector<int>> kept;
+        for (auto &v : pos) {
+            int c[8];
+            for (int d = 0; d < nd; ++d) c[d] = int((kdims[d] - 1) / 2) + v[d];
+            if (!std::isnan(kernel[size_t(flat(kg, c)) * knvar + 0])) kept.push_back(v);
+        }
+        pos.swap(kept);
+    }
+    std::sort(pos.begin(), pos.end(), [](const std::vector<int> &a, const std::vector<int> &b) {
+        float da = 0.f, db = 0.f;
+        for (size_t i = 0; i < a.size(); ++i) da += float(a[i] * a[i]);
+        for (size_t i = 0; i < b.size(); ++i) db += float(b[i] * b[i]);
+        return -da > -db;
+    });
+    return pos;
+}
+
+/* ------------------------------------------------------------------ */
+/* a2: path and seeds                                                  */
+/* ------------------------------------------------------------------ */
+struct Path {
+    std::vector<unsigned> order;   /* cell index per path position, informed cells first */
+    std::vector<float> seeds;      /* U[0,1) per path position (not offset by begin) */
+    unsigned begin = 0;            /* number of fully informed cells */
+    std::vector<unsigned> posterior; /* per cell: path order, 0 for informed, UINT_MAX never */
+};
+
+Path make_path(const Grid &di, const float *dival, unsigned seed) {
+    Path p;
+    std::mt19937 gen(seed);
+    const size_t n = di.cells();
+    p.order.resize(n);
+    std::iota(p.order.begin(), p.order.end(), 0u);
+    unsigned begin = 0;
+    for (size_t i = 0; i < n; ++i) {
+        bool set = true;
+        for (int v = 0; v < di.nvar; ++v)
+            if (std::isnan(dival[i * di.nvar + v])) set = false;
+        if (set) {
+            std::swap(p.order[begin], p.order[i]);
+            begin++;
+        }
+    }
+    std::shuffle(p.order.begin() + begin, p.order.end(), gen);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    p.seeds.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        p.seeds[i] = u(gen);
+        if (p.seeds[i] == 1.f) p.seeds[i] = u(gen);
+    }
+    p.begin = begin;
+    p.posterior.assign(n, UINT_MAX);
+    for (size_t i = 0; i < n; ++i) {
+        bool withNan = false;
+        for (int v = 0; v < di.nvar; ++v) withNan |= std::isnan(dival[i * di.nvar + v]);
+        if (!withNan) p.posterior[i] = 0;
+    }
+    for (size_t i = 0; i < n - begin; ++i) p.posterior[p.order[begin + i]] = unsigned(i);
+    return p;
+}
+
+/* ------------------------------------------------------------------ */
+/* a6: neighbours of one path node                                     */
+/* ------------------------------------------------------------------ */
+/* Walk the sorted template; accept an offset when the cell is inside the
+ * grid and its path order is <= the node's (the node itself included),
+ * until n cells are accepted (single neighbour count for all variables). */
+int neighbours(const Grid &di, const std::vector<std::vector<int>> &tpl, const unsigned *posterior, unsigned cell,
+               unsigned order, int n, int *out_tpl_index, unsigned *out_cell) {
+    int c0[8], c[8];
+    coords(di, long(cell), c0);
+    int cnt = 0;
+    for (size_t t = 0; t < tpl.size() && cnt < n; ++t) {
+        bool ok = true;
+        for (int d = 0; d < di.nd; ++d) {
+            c[d] = c0[d] + tpl[t][d];
+            ok &= (c[d] >= 0) && (c[d] < int(di.dims[d]));
+        }
+        if (!ok) continue;
+        unsigned nc = unsigned(flat(di, c));
+        if (posterior[nc] <= order) {
+            out_tpl_index[cnt] = int(t);
+            out_cell[cnt] = nc;
+            cnt++;
+        }
+    }
+    return cnt;
+}
+
+/* ------------------------------------------------------------------ */
+/* a8/a9: per-node terms and the map                                   */
+/* ------------------------------------------------------------------ */
+struct Term {
+    long off;      /* flat TI offset of the neighbour (src strides) */
+    int var;       /* variable */
+    int cat;       /* 1 categorical */
+    float a;       /* continuous: -w (TI^2 term); categorical: w */
+    float b;       /* continuous: 2*(w*v) (TI term); categorical: category code v */
+    double w, v;   /* exact weight and value for the FP64 map */
+};
+
+struct Node {
+    std::vector<Term> terms;
+    int mn[8], mx[8];
+};
+
+/* kernel weight for offset o and variable v (uniform 1 when kernel==nullptr);
+ * the weight lookup centres the kernel at dims/2
+ * (quantileSamplingModule.hpp:362-366), unlike the template (dims-1)/2. */
+static inline float kweight(const Grid &kg, const float *kernel, const int *o, int v) {
+    if (!kernel) return 1.f;
+    int c[8];
+    for (int d = 0; d < kg.nd; ++d) {
+        c[d] = int(kg.dims[d] / 2) + o[d];
+        if (c[d] < 0 || c[d] >= int(kg.dims[d])) return 0.f;
+    }
+    return kernel[size_t(flat(kg, c)) * kg.nvar + (v % kg.nvar)];
+}
+
+Node build_node(const Grid &ti, const int *types, const Grid &kg, const float *kernel, int nnb, const int *offs /* nnb*nd */,
+                const float *vals /* nnb*nvar, NaN allowed */) {
+    Node nd;
+    for (int d = 0; d < ti.nd; ++d) nd.mn[d] = nd.mx[d] = 0;
+    for (int j = 0; j < nnb; ++j)
+        for (int d = 0; d < ti.nd; ++d) {
+            nd.mn[d] = std::min(nd.mn[d], offs[j * ti.nd + d]);
+            nd.mx[d] = std::max(nd.mx[d], offs[j * ti.nd + d]);
+        }
+    long strides[8];
+    long s = 1;
+    for (int d = 0; d < ti.nd; ++d) { strides[d] = s; s *= ti.dims[d]; }
+    for (int j = 0; j < nnb; ++j) {
+        long off = 0;
+        for (int d = 0; d < ti.nd; ++d) off += long(offs[j * ti.nd + d]) * strides[d];
+        for (int v = 0; v < ti.nvar; ++v) {
+            float val = vals[j * ti.nvar + v];
+            if (std::isnan(val)) continue;            /* weight 0 (quantileSamplingModule.hpp:378-392) */
+            float w = kweight(kg, kernel, offs + j * ti.nd, v);
+            if (w == 0.f) continue;
+            Term t;
+            t.off = off; t.var = v; t.cat = types[v];
+            t.w = w; t.v = val;
+            if (types[v] == 0) { t.a = -w; t.b = 2.f * (w * val); }
+            else { t.a = w; t.b = val; }
+            nd.terms.push_back(t);
+        }
+    }
+    return nd;
+}
+
+/* scan geometry of the (flipped) correlation space: fft == src here */
+struct Scan {
+    int nd;
+    long fft[8], lo[8], stride[8];
+    long N;
+};
+
+Scan make_scan(const Grid &ti, const Node &nd) {
+    Scan sc;
+    sc.nd = ti.nd;
+    long s = 1;
+    for (int d = 0; d < ti.nd; ++d) {
+        sc.fft[d] = ti.dims[d];
+        sc.stride[d] = s;
+        s *= ti.dims[d];
+        /* first fft-(src-(max-min)) entries along d are invalid (CPUThreadDevice.cpp:454-477) */
+        sc.lo[d] = sc.fft[d] - (long(ti.dims[d]) - (nd.mx[d] - nd.mn[d]));
+    }
+    sc.N = s;
+    return sc;
+}
+
+/* TI flat index of the pattern centre for scan index m (inverse of the
+ * flipped layout, CPUThreadDevice.cpp:257-268 without the wrap). Returns
+ * false when m is masked. */
+static inline bool centre_of(const Scan &sc, const Grid &ti, const Node &nd, long m, long *p) {
+    long pf = 0;
+    bool ok = true;
+    for (int d = sc.nd - 1; d >= 0; --d) {
+        long md = (m / sc.stride[d]) % sc.fft[d];
+        ok &= md >= sc.lo[d];
+        long pd = sc.fft[d] - 1 - nd.mn[d] - md;
+        pf = pf * long(ti.dims[d]) + pd;
+    }
+    *p = pf;
+    return ok;
+}
+
+/* FP32 map in the kernels' fixed term order (terms in neighbour order, each
+ * neighbour's variables in order; continuous: acc=fma(-w,t*t,acc);
+ * acc=fma(2wv,t,acc); categorical: acc+=w when t==v). */
+void map_fp32(const Grid &ti, const float *tival, const Node &nd, const Scan &sc, float *out) {
+    for (long m = 0; m < sc.N; ++m) {
+        long p;
+        if (!centre_of(sc, ti, nd, m, &p)) { out[m] = -INFINITY; continue; }
+        float acc = 0.f;
+        for (const Term &t : nd.terms) {
+            float x = tival[size_t(p + t.off) * ti.nvar + t.var];
+            if (t.cat) {
+                if (x == t.b) acc = acc + t.a;
+            } else {
+                if (std::isnan(x)) x = 0.f;   /* layers store NaN as 0 (DataImage.hpp:554-559) */
+                float x2 = x * x;
+                acc = std::fmaf(t.a, x2, acc);
+                acc = std::fmaf(t.b, x, acc);
+            }
+        }
+        out[m] = acc;
+    }
+}
+
+/* FP64 map: S = sum_j w_j * (2 v_j t - t^2) (continuous, i.e. -w(v-t)^2 without
+ * the constant) and sum_j w_j [t==v_j] (categorical); scale = sum w (v^2+t^2)
+ * or sum w. */
+void map_fp64(const Grid &ti, const float *tival, const Node &nd, const Scan &sc, double *out, double *scale) {
+    for (long m = 0; m < sc.N; ++m) {
+        long p;
+        if (!centre_of(sc, ti, nd, m, &p)) { out[m] = -INFINITY; if (scale) scale[m] = 0; continue; }
+        double acc = 0.0, sc2 = 0.0;
+        for (const Term &t : nd.terms) {
+            double x = tival[size_t(p + t.off) * ti.nvar + t.var];
+            if (t.cat) {
+                if (float(x) == float(t.v)) acc += t.w;
+                sc2 += t.w;
+            } else {
+                if (std::isnan(x)) x = 0.0;
+                acc += t.w * (2.0 * t.v * x - x * x);
+                sc2 += t.w * (t.v * t.v + x * x);
+            }
+        }
+        out[m] = acc;
+        if (scale) scale[m] = sc2;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* a10: k-biggest with the reference's reservoir tie-breaking          */
+/* ------------------------------------------------------------------ */
+static inline unsigned seed_from_unit_float(float seed) {
+    if (!std::isfinite(seed) || seed <= 0.f) return 0;
+    if (seed >= 1.f) return std::numeric_limits<unsigned>::max();
+    return static_cast<unsigned>(std::floor(static_cast<double>(seed) * static_cast<double>(std::numeric_limits<unsigned>::max())));
+}
+
+template <typename R>
+static inline void add_value(const float *data, unsigned short k, float *out, unsigned *pos, R &gen, unsigned &cpt,
+                             unsigned i) {
+    short position = short(k - 2);
+    short likeLast = short(k - 2);
+    while (likeLast > -1 && out[k - 1] == out[likeLast]) likeLast--;
+    int xes = k - likeLast - 1;
+    int x = k - xes + int(std::floor(double(gen() * float(xes))));
+    std::swap(pos[x], pos[k - 1]);
+    if (data[i] > out[k - 1]) {
+        if (xes == 1) cpt = 0;
+        else cpt++;
+        while (position > -1 && data[i] > out[position]) {
+            out[position + 1] = out[position];
+            pos[position + 1] = pos[position];
+            position--;
+        }
+        out[position + 1] = data[i];
+        pos[position + 1] = i;
+    } else {
+        cpt++;
+        if (float(unsigned(xes) + cpt) * gen() < float(xes)) pos[position + 1] = i;
+    }
+}
+
+/* fKst::findKBiggest(data, N, k, out, pos, rng) followed by the merge loop
+ * of quantileSamplingModule.hpp:546-557 for one chunk (threadRatio 1). */
+void kbiggest(const float *data, unsigned N, unsigned short k, float seed, float *out, unsigned *pos) {
+    std::mt19937 generator;
+    generator.seed(seed_from_unit_float(seed) + 0);
+    std::uniform_real_distribution<float> distribution(0.0, 1.0);
+    auto rng = std::bind(distribution, std::ref(generator));
+    std::vector<float> o(k, -INFINITY);
+    std::vector<unsigned> p(k, UINT_MAX);
+    unsigned cpt = 0;
+    for (unsigned i = 0; i < N; ++i)
+        if (data[i] >= o[k - 1]) add_value(data, k, o.data(), p.data(), rng, cpt, i);
+    for (int j = 0; j < k; ++j) {
+        unsigned best = 0;
+        for (unsigned l = 1; l < k; ++l)
+            if (o[l] > o[best]) best = l;
+        out[j] = o[best];
+        pos[j] = p[best];
+        o[best] = -INFINITY;
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* a11-a13: draw                                                       */
+/* ------------------------------------------------------------------ */
+/* quantileSamplingModule.hpp:113 as compiled in the reference (ceil and
+ * floor resolve to the double overloads there). */
+static inline unsigned selected_index(float seed, float localk, unsigned vectorSize) {
+    return unsigned(int(std::floor(double(seed * localk) * (std::ceil(double(float(vectorSize) / localk)) / vectorSize))));
+}
+
+/* CPUThreadDevice.cpp:257-268 */
+static inline unsigned index_to_position(const Scan &sc, const Grid &ti, const Node &nd, unsigned index) {
+    unsigned position = 0;
+    unsigned div = unsigned(sc.N);
+    for (int i = sc.nd - 1; i >= 0; --i) {
+        div /= unsigned(sc.fft[i]);
+        position = position * ti.dims[i] +
+                   ((unsigned(sc.fft[i]) - (index / div) % unsigned(sc.fft[i]) - nd.mn[i] - 1) + ti.dims[i]) % ti.dims[i];
+    }
+    return position;
+}
+
+struct NodeResult {
+    unsigned ti_cell;   /* chosen TI cell */
+    int near_tie;       /* FP64 top-(K+1) adjacent gap within tol*scale */
+    int marginal;       /* drawn from the marginal (no informed neighbour) */
+    double gap_min;     /* smallest relative adjacent gap among the FP64 top-(K+1) */
+    float top_score[8];
+    unsigned top_index[8];
+};
+
+struct Problem {
+    Grid ti, di, kg;
+    const float *tival = nullptr;
+    const int *types = nullptr;
+    const float *kernel = nullptr;
+    int n = 0;
+    float k = 1.f;
+    double tol = 1e-5;
+};
+
+/* one node, given the current state of the grid */
+NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, const Path &path, const float *state,
+                    unsigned idx_path, bool want_fp64, bool own_cell_unknown) {
+    NodeResult r;
+    std::memset(&r, 0, sizeof(r));
+    const Grid &di = P.di;
+    unsigned cell = path.order[path.begin + idx_path];
+    unsigned order = path.posterior[cell];
+    float seed = path.seeds[idx_path];
+    std::vector<int> tix(P.n);
+    std::vector<unsigned> ncell(P.n);
+    int cnt = neighbours(di, tpl, path.posterior.data(), cell, order, P.n, tix.data(), ncell.data());
+    auto value = [&](unsigned c, int v) -> float {
+        if (own_cell_unknown && c == cell) return NAN;
+        return state[size_t(c) * di.nvar + v];
+    };
+    bool withDataInCenter = false;
+    for (int v = 0; v < di.nvar; ++v) withDataInCenter |= !std::isnan(value(cell, v));
+    if (cnt <= 1 && !withDataInCenter) {
+        /* marginal draw (simulation.hpp:586-605), single complete TI */
+        unsigned cells = unsigned(P.ti.cells());
+        r.ti_cell = unsigned(int(std::floor(double(seed * float(cells)))));
+        r.marginal = 1;
+        return r;
+    }
+    std::vector<int> offs(size_t(cnt) * di.nd);
+    std::vector<float> vals(size_t(cnt) * di.nvar);
+    for (int j = 0; j < cnt; ++j) {
+        for (int d = 0; d < di.nd; ++d) offs[j * di.nd + d] = tpl[tix[j]][d];
+        for (int v = 0; v < di.nvar; ++v) vals[j * di.nvar + v] = value(ncell[j], v);
+    }
+    Node nd = build_node(P.ti, P.types, P.kg, P.kernel, cnt, offs.data(), vals.data());
+    Scan sc = make_scan(P.ti, nd);
+    std::vector<float> map(sc.N);
+    map_fp32(P.ti, P.tival, nd, sc, map.data());
+    unsigned short K = (unsigned short)int(std::ceil(P.k));
+    std::vector<float> ev(K);
+    std::vector<unsigned> ep(K);
+    kbiggest(map.data(), unsigned(sc.N), K, seed, ev.data(), ep.data());
+    /* sample(): sort the K candidates by score (std::sort), draw */
+    std::vector<unsigned> lp(K);
+    std::iota(lp.begin(), lp.end(), 0u);
+    const float *errors = ev.data();
+    std::sort(lp.begin(), lp.end(), [errors](unsigned a, unsigned b) { return errors[a] > errors[b]; });
+    unsigned sel = selected_index(seed, P.k, 1);
+    unsigned enc = ep[lp[sel]];
+    r.ti_cell = index_to_position(sc, P.ti, nd, enc);
+    for (int j = 0; j < K && j < 8; ++j) { r.top_score[j] = ev[lp[j]]; r.top_index[j] = ep[lp[j]]; }
+    if (want_fp64) {
+        std::vector<double> m64(sc.N), s64(sc.N);
+        map_fp64(P.ti, P.tival, nd, sc, m64.data(), s64.data());
+        std::vector<long> ord(sc.N);
+        std::iota(ord.begin(), ord.end(), 0L);
+        size_t top = std::min<size_t>(size_t(K) + 1, ord.size());
+        std::partial_sort(ord.begin(), ord.begin() + top, ord.end(),
+                          [&](long a, long b) { return m64[a] > m64[b]; });
+        double scale = 0.0;
+        for (size_t j = 0; j < top; ++j) scale = std::max(scale, s64[ord[j]]);
+        double gmin = INFINITY;
+        for (size_t j = 0; j + 1 < top; ++j) {
+            double g = m64[ord[j]] - m64[ord[j + 1]];
+            gmin = std::min(gmin, scale > 0 ? g / scale : g);
+        }
+        r.gap_min = gmin;
+        r.near_tie = gmin <= P.tol;
+    }
+    return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+/* Sorted search template: writes up to cap offsets (nd ints each); returns count. */
+int orc_template(int nd, const unsigned *kdims, const float *kernel, int knvar, int *out, int cap) {
+    auto tpl = make_template(nd, kdims, kernel, knvar);
+    int n = int(tpl.size());
+    for (int i = 0; i < n && i < cap; ++i)
+        for (int d = 0; d < nd; ++d) out[i * nd + d] = tpl[i][d];
+    return n;
+}
+
+/* Path, seeds and posterior order.  Returns begin (number of informed cells). */
+int orc_path(int nd, const unsigned *dims, int nvar, const float *dival, unsigned seed, unsigned *order, float *seeds,
+             unsigned *posterior) {
+    Grid g;
+    g.nd = nd;
+    g.nvar = nvar;
+    for (int d = 0; d < nd; ++d) g.dims[d] = dims[d];
+    Path p = make_path(g, dival, seed);
+    std::copy(p.order.begin(), p.order.end(), order);
+    std::copy(p.seeds.begin(), p.seeds.end(), seeds);
+    std::copy(p.posterior.begin(), p.posterior.end(), posterior);
+    return int(p.begin);
+}
+
+/* k-biggest with reservoir ties on an arbitrary array (fKb.hpp semantics). */
+void orc_kbiggest(const float *data, unsigned N, unsigned k, float seed, float *out, unsigned *pos) {
+    kbiggest(data, N, (unsigned short)k, seed, out, pos);
+}
+
+/* MT19937 + uniform_real_distribution<float> stream, for RNG unit tests */
+void orc_rng(unsigned s, int n, float *out) {
+    std::mt19937 g;
+    g.seed(s);
+    std::uniform_real_distribution<float> d(0.0, 1.0);
+    for (int i = 0; i < n; ++i) out[i] = d(g);
+}
+
+unsigned orc_seed_from_unit_float(float seed) { return seed_from_unit_float(seed); }
+unsigned orc_selected_index(float seed, float k, unsigned nti) { return selected_index(seed, k, nti); }
+
+/*
+ * Vector QS simulation (mode 0) or teacher-forced per-node evaluation (mode 1).
+ *   ti: nd dims (x first) ti_dims, nvar interleaved variables, types[v] 0/1
+ *   di: di_dims, nvar, NaN = to simulate (mode 0: simulated in place;
+ *       mode 1: the completed grid whose values are used as neighbour values,
+ *       with each node's own cell treated as not yet simulated)
+ *   di_init: mode 1 only, the grid before simulation (defines the path)
+ *   kernel: optional weights (kdims, nvar interleaved); nullptr = uniform 1
+ *           of size min(TI/2+1)
+ * Outputs per path node (size = cells - begin): chosen TI cell, near-tie
+ * flag (if want_fp64), marginal flag.  out_id (mode 0): per DI cell the
+ * reference's index image (TI cell * nTI + TI, nTI = 1).
+ * Returns the number of path nodes.
+ */
+long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
+                  const unsigned *di_dims, float *di, const float *di_init, const unsigned *kdims, const float *kernel, int n, float k,
+                  unsigned seed, int want_fp64, double tol, long node_begin, long node_end, unsigned *out_cell,
+                  int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id) {
+    Problem P;
+    P.ti.nd = P.di.nd = P.kg.nd = nd;
+    P.ti.nvar = P.di.nvar = nvar;
+    for (int d = 0; d < nd; ++d) { P.ti.dims[d] = ti_dims[d]; P.di.dims[d] = di_dims[d]; }
+    P.tival = ti;
+    P.types = types;
+    P.n = n;
+    P.k = k;
+    P.tol = tol;
+    if (kernel) {
+        P.kernel = kernel;
+        P.kg.nvar = nvar;
+        for (int d = 0; d < nd; ++d) P.kg.dims[d] = kdims[d];
+    } else {
+        P.kg.nvar = nvar;
+        for (int d = 0; d < nd; ++d) P.kg.dims[d] = std::min(ti_dims[d] / 2 + 1, ti_dims[d]);
+    }
+    auto tpl = make_template(nd, P.kg.dims, P.kernel, nvar);
+    std::vector<float> state(di, di + P.di.cells() * nvar);
+    /* the path is always built from the grid before simulation (NaN = unknown) */
+    Path path = make_path(P.di, di_init ? di_init : state.data(), seed);
+    long nodes = long(P.di.cells()) - long(path.begin);
+    if (node_end < 0 || node_end > nodes) node_end = nodes;
+    if (mode == 1) {
+        /* teacher forcing: every path cell is "not yet simulated" at its own turn */
+#pragma omp parallel for schedule(dynamic, 16)
+        for (long i = node_begin; i < node_end; ++i) {
+            NodeResult r = run_node(P, tpl, path, state.data(), unsigned(i), want_fp64 != 0, true);
+            long o = i - node_begin;
+            if (out_cell) out_cell[o] = r.ti_cell;
+            if (out_near_tie) out_near_tie[o] = r.near_tie;
+            if (out_marginal) out_marginal[o] = r.marginal;
+            if (out_gap) out_gap[o] = r.gap_min;
+        }
+        return nodes;
+    }
+    for (long i = 0; i < node_end; ++i) {
+        unsigned cell = path.order[path.begin + i];
+        bool active = i >= node_begin;
+        NodeResult r = run_node(P, tpl, path, state.data(), unsigned(i), active && want_fp64 != 0, false);
+        for (int v = 0; v < nvar; ++v)
+            if (std::isnan(state[size_t(cell) * nvar + v])) state[size_t(cell) * nvar + v] = ti[size_t(r.ti_cell) * nvar + v];
+        if (out_id) out_id[cell] = r.ti_cell;
+        if (active) {
+            long o = i - node_begin;
+            if (out_cell) out_cell[o] = r.ti_cell;
+            if (out_near_tie) out_near_tie[o] = r.near_tie;
+            if (out_marginal) out_marginal[o] = r.marginal;
+            if (out_gap) out_gap[o] = r.gap_min;
+        }
+    }
+    std::copy(state.begin(), state.end(), di);
+    return nodes;
+}
+
+/* FP32 and FP64 maps of one explicit pattern (offsets/values) against the TI
+ * in scan (flipped) order, plus the node's min/max; for map-level tests. */
+long orc_pattern_map(int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti, int nnb,
+                     const int *offs, const float *vals, float *out32, double *out64, double *scale, int *mn, int *mx) {
+    Grid g, kg;
+    g.nd = kg.nd = nd;
+    g.nvar = kg.nvar = nvar;
+    for (int d = 0; d < nd; ++d) g.dims[d] = ti_dims[d];
+    Node node = build_node(g, types, kg, nullptr, nnb, offs, vals);
+    Scan sc = make_scan(g, node);
+    if (out32) map_fp32(g, ti, node, sc, out32);
+    if (out64) map_fp64(g, ti, node, sc, out64, scale);
+    for (int d = 0; d < nd; ++d) { mn[d] = node.mn[d]; mx[d] = node.mx[d]; }
+    return sc.N;
+}
+
+}  /* extern "C" */

@@ -1,0 +1,148 @@
+"""Test infrastructure only: Python access to the CPU oracle (qs_oracle.cpp).
+
+The oracle restates the G2S reference QuickSampling path (see the header of
+``qs_oracle.cpp`` for the file:line of every step).  Tests, the smoke check
+and the CPU-baseline leg of bench.py use it as the checker; the product never
+imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libqsoracle.so")
+_lib = None
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_u32p = ctypes.POINTER(ctypes.c_uint)
+_i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(LIB)
+        L.orc_template.argtypes = [ctypes.c_int, _u32p, _f32p, ctypes.c_int, _i32p, ctypes.c_int]
+        L.orc_template.restype = ctypes.c_int
+        L.orc_path.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p, _u32p]
+        L.orc_path.restype = ctypes.c_int
+        L.orc_kbiggest.argtypes = [_f32p, ctypes.c_uint, ctypes.c_uint, ctypes.c_float, _f32p, _u32p]
+        L.orc_rng.argtypes = [ctypes.c_uint, ctypes.c_int, _f32p]
+        L.orc_seed_from_unit_float.argtypes = [ctypes.c_float]
+        L.orc_seed_from_unit_float.restype = ctypes.c_uint
+        L.orc_selected_index.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_uint]
+        L.orc_selected_index.restype = ctypes.c_uint
+        L.orc_simulate.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, _u32p, _f32p, _f32p,
+                                   _u32p,
+                                   _f32p, ctypes.c_int, ctypes.c_float, ctypes.c_uint, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_long, ctypes.c_long, _u32p, _i32p, _i32p, _f64p, _u32p]
+        L.orc_simulate.restype = ctypes.c_long
+        L.orc_pattern_map.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, ctypes.c_int, _i32p, _f32p,
+                                      _f32p, _f64p, _f64p, _i32p, _i32p]
+        L.orc_pattern_map.restype = ctypes.c_long
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def grid_dims(arr: np.ndarray, nvar: int):
+    spatial = arr.shape if nvar == 1 else arr.shape[:-1]
+    return np.array(list(reversed(spatial)), dtype=np.uint32)
+
+
+def template(kdims, kernel=None, nvar=1):
+    kd = np.asarray(kdims, dtype=np.uint32)
+    cap = int(np.prod(kd))
+    out = np.zeros(cap * len(kd), dtype=np.int32)
+    kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
+    n = lib().orc_template(len(kd), _p(kd, _u32p), _p(kern, _f32p), nvar, _p(out, _i32p), cap)
+    return out[: n * len(kd)].reshape(n, len(kd))
+
+
+def path(di: np.ndarray, nvar: int, seed: int):
+    dims = grid_dims(di, nvar)
+    cells = int(np.prod(dims))
+    d = np.ascontiguousarray(di, dtype=np.float32)
+    order = np.zeros(cells, np.uint32)
+    seeds = np.zeros(cells, np.float32)
+    post = np.zeros(cells, np.uint32)
+    begin = lib().orc_path(len(dims), _p(dims, _u32p), nvar, _p(d, _f32p), seed, _p(order, _u32p), _p(seeds, _f32p),
+                           _p(post, _u32p))
+    return order, seeds, post, begin
+
+
+def kbiggest(data: np.ndarray, k: int, seed: float):
+    d = np.ascontiguousarray(data, dtype=np.float32)
+    out = np.zeros(k, np.float32)
+    pos = np.zeros(k, np.uint32)
+    lib().orc_kbiggest(_p(d, _f32p), d.size, k, seed, _p(out, _f32p), _p(pos, _u32p))
+    return out, pos
+
+
+def rng_stream(seed: int, n: int):
+    out = np.zeros(n, np.float32)
+    lib().orc_rng(seed, n, _p(out, _f32p))
+    return out
+
+
+def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp64=False, tol=1e-5,
+             node_begin=0, node_end=-1, di_init=None):
+    """mode 0: sequential vector simulation of ``di`` (NaN = unknown);
+    mode 1: teacher-forced evaluation of every path node against the completed
+    grid ``di``, the path being built from ``di_init`` (the grid before
+    simulation).
+
+    Returns dict(sim, id, cell, near_tie, marginal, gap, begin)."""
+    nvar = len(types)
+    tdims = grid_dims(ti, nvar)
+    ddims = grid_dims(di, nvar)
+    t = np.ascontiguousarray(ti, dtype=np.float32)
+    d = np.ascontiguousarray(di, dtype=np.float32).copy()
+    ty = np.asarray(types, dtype=np.int32)
+    cells = int(np.prod(ddims))
+    init = d if di_init is None else np.ascontiguousarray(di_init, dtype=np.float32)
+    informed = int(np.sum(~np.isnan(init.reshape(cells, nvar)).any(axis=1)))
+    nodes = cells - informed
+    ne = nodes if node_end < 0 else min(node_end, nodes)
+    cnt = max(ne - node_begin, 0)
+    cell = np.zeros(cnt, np.uint32)
+    nt = np.zeros(cnt, np.int32)
+    mg = np.zeros(cnt, np.int32)
+    gap = np.zeros(cnt, np.float64)
+    oid = np.zeros(cells, np.uint32)
+    kd = None if kdims is None else np.asarray(kdims, dtype=np.uint32)
+    kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
+    lib().orc_simulate(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
+                       _p(d, _f32p), None if di_init is None else _p(init, _f32p), _p(kd, _u32p), _p(kern, _f32p), n, k, seed, int(want_fp64), tol, node_begin,
+                       ne, _p(cell, _u32p), _p(nt, _i32p), _p(mg, _i32p), _p(gap, _f64p), _p(oid, _u32p))
+    return dict(sim=d, id=oid, cell=cell, near_tie=nt.astype(bool), marginal=mg.astype(bool), gap=gap)
+
+
+def pattern_map(ti, types, offsets, values):
+    """FP32 and FP64 maps (scan order) of one explicit pattern; returns (m32, m64, scale, mn, mx)."""
+    nvar = len(types)
+    tdims = grid_dims(ti, nvar)
+    t = np.ascontiguousarray(ti, dtype=np.float32)
+    ty = np.asarray(types, dtype=np.int32)
+    offs = np.ascontiguousarray(offsets, dtype=np.int32)
+    vals = np.ascontiguousarray(values, dtype=np.float32)
+    N = int(np.prod(tdims))
+    m32 = np.zeros(N, np.float32)
+    m64 = np.zeros(N, np.float64)
+    sc = np.zeros(N, np.float64)
+    mn = np.zeros(len(tdims), np.int32)
+    mx = np.zeros(len(tdims), np.int32)
+    lib().orc_pattern_map(len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), offs.shape[0],
+                          _p(offs, _i32p), _p(vals, _f32p), _p(m32, _f32p), _p(m64, _f64p), _p(sc, _f64p),
+                          _p(mn, _i32p), _p(mx, _i32p))
+    return m32, m64, sc, mn, mx
