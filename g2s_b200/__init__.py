@@ -1,0 +1,310 @@
+"""g2s_b200: B200-native QuickSampling (QS) hot path.
+
+Python access to ``libg2s_b200.so`` (C ABI declared in ``include/g2s_b200.h``).
+The CUDA library is the only compute path: importing works without a GPU,
+but every call that computes needs the built library and a CUDA device and
+raises ``RuntimeError`` otherwise — there is no CPU fallback.
+
+The high-level call mirrors G2S' QuickSampling interface
+(``g2s('-a','qs','-ti',ti,'-di',di,'-dt',types,'-k',k,'-n',n,'-s',seed)``,
+G2S docs/algorithms/QuickSampling.md:21-37) and returns the simulation and
+the index image like the reference does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libg2s_b200.so")
+
+QSK_OP_LIN, QSK_OP_SQLIN, QSK_OP_EQ = 0, 1, 2
+
+_lib = None
+_f32p = ctypes.POINTER(ctypes.c_float)
+_u32p = ctypes.POINTER(ctypes.c_uint)
+_i32p = ctypes.POINTER(ctypes.c_int)
+
+
+class QskTerm(ctypes.Structure):
+    _fields_ = [("neighbour", ctypes.c_int), ("layer", ctypes.c_int), ("op", ctypes.c_int),
+                ("a", ctypes.c_float), ("b", ctypes.c_float)]
+
+
+class QskParams(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("ti_dims", _u32p), ("nvar", ctypes.c_int), ("types", _i32p),
+                ("ti", _f32p), ("di_dims", _u32p), ("kernel_dims", _u32p), ("kernel", _f32p),
+                ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint)]
+
+
+class QskSimInfo(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_longlong), ("levels", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("template_size", ctypes.c_int), ("ms_setup_neighbours", ctypes.c_float),
+                ("ms_levels", ctypes.c_float), ("ms_batches", ctypes.c_float)]
+
+
+# name -> (restype, argtypes): every entry point of include/g2s_b200.h
+SIGNATURES = {
+    "qsk_last_error": (ctypes.c_char_p, []),
+    "qsk_device_count": (ctypes.c_int, [_i32p]),
+    "qsk_ti_create_layers": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _u32p, ctypes.c_int,
+                                            ctypes.POINTER(_f32p), ctypes.POINTER(ctypes.c_void_p)]),
+    "qsk_ti_create_grid": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "qsk_ti_fft_size": (ctypes.c_int, [ctypes.c_void_p, _u32p]),
+    "qsk_ti_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_worker_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "qsk_worker_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_pattern_kbest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
+                                         ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float, _f32p, _u32p, _i32p]),
+    "qsk_pattern_kbest_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p,
+                                               ctypes.POINTER(QskTerm), ctypes.c_uint, _f32p, _f32p, _u32p, _i32p]),
+    "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
+    "qsk_position_to_index": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
+    "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,
+                                      ctypes.POINTER(ctypes.c_void_p)]),
+    "qsk_sim_run": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_sim_run_teacher": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    "qsk_sim_read": (ctypes.c_int, [ctypes.c_void_p, _f32p, _u32p, _u32p]),
+    "qsk_sim_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskSimInfo)]),
+    "qsk_sim_get_path": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f32p, _u32p]),
+    "qsk_sim_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
+    "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
+    "qsk_qs_path": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p]),
+}
+
+
+def lib():
+    """Load libg2s_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m g2s_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = lib().qsk_last_error()
+        raise RuntimeError(f"{what} failed (status {rc}): {msg.decode() if msg else ''}")
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def device_count() -> int:
+    c = ctypes.c_int(0)
+    rc = lib().qsk_device_count(ctypes.byref(c))
+    return c.value if rc == 0 else 0
+
+
+def search_template(kernel_dims, nvar: int = 1, kernel: Optional[np.ndarray] = None):
+    """Host-only: sorted neighbour search template and kernel weights."""
+    kd = np.asarray(kernel_dims, dtype=np.uint32)
+    cap = int(np.prod(kd))
+    offs = np.zeros(cap * len(kd), np.int32)
+    w = np.zeros(cap * nvar, np.float32)
+    kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
+    n = lib().qsk_qs_template(len(kd), nvar, _p(kd, _u32p), _p(kern, _f32p), _p(offs, _i32p), _p(w, _f32p), cap)
+    if n < 0:
+        raise RuntimeError("qsk_qs_template failed")
+    return offs[: n * len(kd)].reshape(n, len(kd)), w[: n * nvar].reshape(n, nvar)
+
+
+def random_path(di: np.ndarray, nvar: int, seed: int):
+    """Host-only: (order, seeds, begin) of the simulation path for grid di."""
+    d = np.ascontiguousarray(di, dtype=np.float32)
+    cells = d.size // nvar
+    order = np.zeros(cells, np.uint32)
+    seeds = np.zeros(cells, np.float32)
+    b = lib().qsk_qs_path(cells, nvar, _p(d, _f32p), int(seed) & 0xffffffff, _p(order, _u32p), _p(seeds, _f32p))
+    if b < 0:
+        raise RuntimeError("qsk_qs_path failed")
+    return order, seeds, int(b)
+
+
+def _grid_dims(arr: np.ndarray, nvar: int) -> np.ndarray:
+    spatial = arr.shape if nvar == 1 else arr.shape[:-1]
+    return np.array(list(reversed(spatial)), dtype=np.uint32)
+
+
+class TrainingImage:
+    """A training image resident on one GPU (layers built on the device)."""
+
+    def __init__(self, ti: np.ndarray, types: Sequence[int], device: int = 0):
+        self.nvar = len(types)
+        self.dims = _grid_dims(ti, self.nvar)
+        self.data = np.ascontiguousarray(ti, dtype=np.float32)
+        self.types = np.asarray(types, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(lib().qsk_ti_create_grid(device, len(self.dims), _p(self.dims, _u32p), self.nvar,
+                                        _p(self.types, _i32p), _p(self.data, _f32p), ctypes.byref(h)),
+               "qsk_ti_create_grid")
+        self.handle = h
+        self.ndim = len(self.dims)
+
+    @classmethod
+    def from_layers(cls, layers: Sequence[np.ndarray], src_size, fft_size, device: int = 0):
+        """Reference-format layers (flipped, prod(fft_size) floats each)."""
+        self = cls.__new__(cls)
+        self.nvar = 0
+        self.dims = np.asarray(src_size, dtype=np.uint32)
+        fft = np.asarray(fft_size, dtype=np.uint32)
+        arrs = [np.ascontiguousarray(l, dtype=np.float32).ravel() for l in layers]
+        ptrs = (_f32p * len(arrs))(*[a.ctypes.data_as(_f32p) for a in arrs])
+        h = ctypes.c_void_p()
+        _check(lib().qsk_ti_create_layers(device, len(self.dims), _p(self.dims, _u32p), _p(fft, _u32p), len(arrs),
+                                          ptrs, ctypes.byref(h)), "qsk_ti_create_layers")
+        self._keep = arrs
+        self.handle = h
+        self.ndim = len(self.dims)
+        return self
+
+    def fft_size(self) -> np.ndarray:
+        out = np.zeros(self.ndim, np.uint32)
+        _check(lib().qsk_ti_fft_size(self.handle, _p(out, _u32p)), "qsk_ti_fft_size")
+        return out
+
+    def index_to_position(self, mn, index: int) -> int:
+        m = np.asarray(mn, dtype=np.int32)
+        return int(lib().qsk_index_to_position(self.handle, _p(m, _i32p), int(index)))
+
+    def position_to_index(self, mn, position: int) -> int:
+        m = np.asarray(mn, dtype=np.int32)
+        return int(lib().qsk_position_to_index(self.handle, _p(m, _i32p), int(position)))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qsk_ti_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Worker:
+    """Per-thread pattern queries against one TrainingImage."""
+
+    def __init__(self, ti: TrainingImage):
+        self.ti = ti
+        h = ctypes.c_void_p()
+        _check(lib().qsk_worker_create(ti.handle, ctypes.byref(h)), "qsk_worker_create")
+        self.handle = h
+
+    def pattern_kbest(self, offsets: np.ndarray, terms, k: int, seed: float):
+        """offsets: (n, ndim) int; terms: list of (neighbour, layer, op, a, b).
+        Returns (scores[k], scan_indices[k], min_offset[ndim])."""
+        offs = np.ascontiguousarray(offsets, dtype=np.int32).reshape(-1, self.ti.ndim)
+        tarr = (QskTerm * max(len(terms), 1))(*[QskTerm(int(t[0]), int(t[1]), int(t[2]), float(t[3]), float(t[4]))
+                                               for t in terms])
+        sc = np.zeros(k, np.float32)
+        ix = np.zeros(k, np.uint32)
+        mn = np.zeros(self.ti.ndim, np.int32)
+        _check(lib().qsk_pattern_kbest(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
+                                       _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)), "qsk_pattern_kbest")
+        return sc, ix, mn
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qsk_worker_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Simulation:
+    """A QS vector simulation resident on one GPU."""
+
+    def __init__(self, ti: np.ndarray, di: np.ndarray, types: Sequence[int], n: int, k: float, seed: int,
+                 kernel: Optional[np.ndarray] = None, device: int = 0):
+        self.nvar = len(types)
+        self._ti = np.ascontiguousarray(ti, dtype=np.float32)
+        self._di = np.ascontiguousarray(di, dtype=np.float32)
+        self._types = np.asarray(types, dtype=np.int32)
+        self._tdims = _grid_dims(self._ti, self.nvar)
+        self._ddims = _grid_dims(self._di, self.nvar)
+        self._kdims = None if kernel is None else _grid_dims(np.asarray(kernel), self.nvar)
+        self._kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
+        self.params = QskParams(len(self._tdims), _p(self._tdims, _u32p), self.nvar, _p(self._types, _i32p),
+                                _p(self._ti, _f32p), _p(self._ddims, _u32p), _p(self._kdims, _u32p),
+                                _p(self._kern, _f32p), int(n), float(k), int(seed) & 0xffffffff)
+        h = ctypes.c_void_p()
+        _check(lib().qsk_sim_create(device, ctypes.byref(self.params), _p(self._di, _f32p), ctypes.byref(h)),
+               "qsk_sim_create")
+        self.handle = h
+        self.shape = self._di.shape
+
+    def run(self):
+        _check(lib().qsk_sim_run(self.handle), "qsk_sim_run")
+        return self
+
+    def run_teacher(self, completed: np.ndarray):
+        c = np.ascontiguousarray(completed, dtype=np.float32)
+        _check(lib().qsk_sim_run_teacher(self.handle, _p(c, _f32p)), "qsk_sim_run_teacher")
+        return self
+
+    def info(self) -> dict:
+        inf = QskSimInfo()
+        _check(lib().qsk_sim_get_info(self.handle, ctypes.byref(inf)), "qsk_sim_get_info")
+        return {f: getattr(inf, f) for f, _ in QskSimInfo._fields_}
+
+    def path(self):
+        cells = int(np.prod(self._ddims))
+        order = np.zeros(cells, np.uint32)
+        seeds = np.zeros(cells, np.float32)
+        begin = ctypes.c_uint(0)
+        _check(lib().qsk_sim_get_path(self.handle, _p(order, _u32p), _p(seeds, _f32p), ctypes.byref(begin)),
+               "qsk_sim_get_path")
+        return order, seeds, begin.value
+
+    def read(self):
+        """Returns (grid, index_image, node_cells)."""
+        cells = int(np.prod(self._ddims))
+        out = np.empty_like(self._di)
+        idx = np.zeros(cells, np.uint32)
+        nodes = self.info()["nodes"]
+        nc = np.zeros(max(nodes, 1), np.uint32)
+        _check(lib().qsk_sim_read(self.handle, _p(out, _f32p), _p(idx, _u32p), _p(nc, _u32p)), "qsk_sim_read")
+        return out, idx.reshape(self._di.shape[:len(self._ddims)]), nc[:nodes]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qsk_sim_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n: int, s: int,
+       ki: Optional[np.ndarray] = None, device: int = 0):
+    """QuickSampling on one GPU; arguments named after the G2S flags
+    (-ti -di -dt -k -n -s -ki).  Returns (simulation, index) as G2S does."""
+    sim = Simulation(ti, di, dt, n=n, k=k, seed=s, kernel=ki, device=device)
+    try:
+        sim.run()
+        out, idx, _ = sim.read()
+    finally:
+        sim.close()
+    return out, idx

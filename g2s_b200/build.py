@@ -1,0 +1,58 @@
+"""Build recipe for the CUDA extension (sm_100a) and the drop-in device.
+
+    python -m g2s_b200.build          # -> g2s_b200/libg2s_b200.so
+    python -m g2s_b200.build dropin   # -> g2s_b200/dropin/g2s_cuda.so (needs the G2S headers)
+
+nvcc cross-compiles for sm_100a without a GPU.  The shared library is built
+in-tree so that it travels with the repository to the GPU machine.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "libg2s_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+HOSTCXX = "/usr/bin/g++"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+SOURCES = ["qsk_kernels.cu", "qsk_host.cpp"]
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_lib(force: bool = False) -> str:
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "qsk_internal.h"),
+                                                       os.path.join(ROOT, "include", "g2s_b200.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(CSRC, src.rsplit(".", 1)[0] + ".o")
+        cmd = [NVCC, "-ccbin", HOSTCXX, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+               "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+        if src.endswith(".cpp"):
+            cmd[cmd.index("-c"):cmd.index("-c")] = ["-x", "cu"]
+        _run(cmd)
+        objs.append(obj)
+    _run([NVCC, "-ccbin", HOSTCXX, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+if __name__ == "__main__":
+    build_lib(force="--force" in sys.argv)

@@ -1,0 +1,932 @@
+// Host engine of the B200 QuickSampling path: the C ABI of include/g2s_b200.h.
+//
+// Host work mirrors what G2S does on the CPU before its simulation loop
+// (search template, random path, per-node seeds: src/qs.cpp:975-1258,
+// 1604-1641) with the same libstdc++ algorithms, so paths and seeds are
+// identical for a given -s.  Everything per node runs on the GPU.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/g2s_b200.h"
+#include "qsk_internal.h"
+
+using namespace qsk;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(expr)                                                                                          \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) {                                                                          \
+            int code_ = (e_ == cudaErrorMemoryAllocation) ? QSK_ERR_NOMEM : QSK_ERR_CUDA;                  \
+            return fail(code_, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__);         \
+        }                                                                                                 \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    cudaError_t ensure(size_t count) { return count <= n ? cudaSuccess : alloc(count); }
+    cudaError_t upload(const T *h, size_t count, cudaStream_t st) {
+        cudaError_t e = ensure(count);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+    }
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// smallest size >= s of the form 7-smooth times optionally one 11 or 13
+// (G2S src/sharedMemoryManager.cpp:26-58)
+unsigned fft_size_for(unsigned s) {
+    if (s == 1) return 1;
+    unsigned upper = 1u << (32 - __builtin_clz(s - 1));
+    for (unsigned i = s; i <= upper; ++i) {
+        unsigned v = i;
+        for (unsigned p = 2; p < 8; ++p)
+            while (v % p == 0) v /= p;
+        if (v % 11 == 0) v /= 11;
+        else if (v % 13 == 0) v /= 13;
+        if (v == 1) return i;
+    }
+    return s;
+}
+
+Geom make_geom(int nd, const unsigned *src, const unsigned *fft) {
+    Geom g;
+    std::memset(&g, 0, sizeof(g));
+    g.nd = nd;
+    long long s = 1;
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        if (d < nd) {
+            g.fft[d] = int(fft[d]);
+            g.src[d] = int(src[d]);
+            g.sstride[d] = s;
+            s *= fft[d];
+        } else {
+            g.fft[d] = 1;
+            g.src[d] = 1;
+            g.sstride[d] = s;
+        }
+    }
+    g.N = s;
+    g.nseg = int((s + QSK_SEG - 1) / QSK_SEG);
+    return g;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// TI context
+// ---------------------------------------------------------------------------
+struct qsk_ti {
+    int device = 0;
+    Geom g;
+    int nlayers = 0;
+    int nvar = 0;                 // grid-built contexts only
+    std::vector<int> types;       // grid-built contexts only
+    DBuf<float> layers;           // nlayers * N
+    DBuf<float> grid;             // raw TI (grid-built): cells * nvar
+    DBuf<int> dtypes;
+    long long cells = 0;
+};
+
+struct qsk_worker {
+    qsk_ti *ti = nullptr;
+    cudaStream_t st = nullptr;
+    DBuf<Slot> slots;
+    DBuf<Term> terms;
+    DBuf<float> rec_val;
+    DBuf<int> rec_idx;
+    DBuf<int> rec_cnt;
+    DBuf<float> out_val;
+    DBuf<unsigned> out_pos;
+    std::vector<Slot> h_slots;
+    std::vector<Term> h_terms;
+};
+
+namespace {
+
+int smem_configured_device = -1;
+
+cudaError_t ensure_records(const Geom &g, int nslots, DBuf<float> &rv, DBuf<int> &ri, DBuf<int> &rc) {
+    size_t per = size_t(g.nseg) * QSK_SEG;
+    cudaError_t e = rv.ensure(per * nslots);
+    if (e != cudaSuccess) return e;
+    e = ri.ensure(per * nslots);
+    if (e != cudaSuccess) return e;
+    return rc.ensure(size_t(g.nseg) * nslots);
+}
+
+// host-side slot/terms for one explicit pattern
+int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms, const qsk_term *terms, unsigned K,
+                       float seed, int node, Slot &s, std::vector<Term> &out, int *out_min) {
+    const Geom &g = ti->g;
+    const int nd = g.nd;
+    std::memset(&s, 0, sizeof(s));
+    s.node = node;
+    s.seed = seed;
+    s.sel = 0;
+    int mn[QSK_MAXD] = {0}, mx[QSK_MAXD] = {0};
+    for (int j = 0; j < nnb; ++j)
+        for (int d = 0; d < nd; ++d) {
+            mn[d] = std::min(mn[d], offsets[j * nd + d]);
+            mx[d] = std::max(mx[d], offsets[j * nd + d]);
+        }
+    long long nvalid = 1;
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        s.mn[d] = mn[d];
+        int lo = 0;
+        if (d < nd) {
+            lo = g.fft[d] - (g.src[d] - (mx[d] - mn[d]));
+            lo = std::max(0, std::min(lo, g.fft[d]));
+            nvalid *= (g.fft[d] - lo);
+        }
+        s.lo[d] = lo;
+        if (out_min && d < nd) out_min[d] = mn[d];
+    }
+    if (nnb == 0) {
+        s.flags = SLOT_SKIP;  // candidateForPattern returns false on an empty pattern
+        s.nterms = 0;
+        return QSK_OK;
+    }
+    if (nvalid < (long long)K) s.flags |= SLOT_EMIT_MASKED;
+    out.clear();
+    for (int t = 0; t < nterms; ++t) {
+        const qsk_term &q = terms[t];
+        if (q.neighbour < 0 || q.neighbour >= nnb || q.layer < 0 || q.layer >= ti->nlayers || q.op < 0 || q.op > 2)
+            return fail(QSK_ERR_ARG, "pattern term %d out of range", t);
+        long long dflat = 0;
+        for (int d = 0; d < nd; ++d) dflat += (long long)(offsets[q.neighbour * nd + d] - mn[d]) * g.sstride[d];
+        Term tm;
+        tm.base = int((long long)q.layer * g.N - dflat);
+        tm.a = q.a;
+        tm.b = q.b;
+        tm.op = q.op;
+        out.push_back(tm);
+    }
+    s.nterms = int(out.size());
+    return QSK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *qsk_last_error(void) { return g_err.c_str(); }
+
+int qsk_device_count(int *count) {
+    if (!count) return fail(QSK_ERR_ARG, "null count");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        *count = 0;
+        return fail(QSK_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+    }
+    *count = c;
+    return QSK_OK;
+}
+
+static int check_sizes(int ndim, const unsigned *src, const unsigned *fft, int nlayers) {
+    if (ndim < 1 || ndim > QSK_MAXD) return fail(QSK_ERR_UNSUPPORTED, "ndim %d not in [1,%d]", ndim, QSK_MAXD);
+    long long N = 1;
+    for (int d = 0; d < ndim; ++d) {
+        if (src[d] == 0 || fft[d] < src[d]) return fail(QSK_ERR_ARG, "bad size in dimension %d", d);
+        N *= fft[d];
+    }
+    if (N * (long long)std::max(nlayers, 1) >= (1LL << 31))
+        return fail(QSK_ERR_UNSUPPORTED, "layers too large for 32-bit scan offsets (%lld x %d)", N, nlayers);
+    return QSK_OK;
+}
+
+int qsk_ti_create_layers(int device, int ndim, const unsigned *src_size, const unsigned *fft_size, int nlayers,
+                         const float *const *layers, qsk_ti **out) {
+    if (!out || !src_size || !fft_size || !layers || nlayers < 1) return fail(QSK_ERR_ARG, "null argument");
+    int rc = check_sizes(ndim, src_size, fft_size, nlayers);
+    if (rc) return rc;
+    DeviceGuard dgd(device);
+    qsk_ti *t = new qsk_ti();
+    t->device = device;
+    t->g = make_geom(ndim, src_size, fft_size);
+    t->nlayers = nlayers;
+    cudaError_t e = t->layers.alloc(size_t(nlayers) * t->g.N);
+    if (e != cudaSuccess) {
+        delete t;
+        return fail(QSK_ERR_NOMEM, "layers: %s", cudaGetErrorString(e));
+    }
+    for (int l = 0; l < nlayers; ++l) {
+        e = cudaMemcpy(t->layers.p + size_t(l) * t->g.N, layers[l], sizeof(float) * t->g.N, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            delete t;
+            return fail(QSK_ERR_CUDA, "layer upload: %s", cudaGetErrorString(e));
+        }
+    }
+    *out = t;
+    return QSK_OK;
+}
+
+static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int nvar, const int *types,
+                               const float *data, bool data_on_device, qsk_ti **out) {
+    if (!out || !dims || !types || !data || nvar < 1) return fail(QSK_ERR_ARG, "null argument");
+    if (nvar > 4) return fail(QSK_ERR_UNSUPPORTED, "at most 4 variables (got %d)", nvar);
+    std::vector<unsigned> fft(ndim);
+    for (int d = 0; d < ndim && d < QSK_MAXD; ++d) fft[d] = fft_size_for(dims[d]);
+    int rc = check_sizes(ndim, dims, fft.data(), nvar);
+    if (rc) return rc;
+    DeviceGuard dgd(device);
+    qsk_ti *t = new qsk_ti();
+    t->device = device;
+    t->g = make_geom(ndim, dims, fft.data());
+    t->nlayers = nvar;
+    t->nvar = nvar;
+    t->types.assign(types, types + nvar);
+    t->cells = 1;
+    for (int d = 0; d < ndim; ++d) t->cells *= dims[d];
+    auto bail = [&](cudaError_t e) {
+        delete t;
+        return fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "ti upload: %s",
+                    cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    if ((e = t->grid.alloc(size_t(t->cells) * nvar)) != cudaSuccess) return bail(e);
+    if ((e = cudaMemcpy(t->grid.p, data, sizeof(float) * t->cells * nvar,
+                        data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(e);
+    if ((e = t->dtypes.alloc(nvar)) != cudaSuccess) return bail(e);
+    if ((e = cudaMemcpy(t->dtypes.p, types, sizeof(int) * nvar, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
+    if ((e = t->layers.alloc(size_t(nvar) * t->g.N)) != cudaSuccess) return bail(e);
+    if ((e = launch_build_layers(t->grid.p, nvar, t->dtypes.p, t->g, t->layers.p, 0)) != cudaSuccess) return bail(e);
+    if ((e = cudaStreamSynchronize(0)) != cudaSuccess) return bail(e);
+    *out = t;
+    return QSK_OK;
+}
+
+int qsk_ti_create_grid(int device, int ndim, const unsigned *dims, int nvar, const int *types, const float *data,
+                       qsk_ti **out) {
+    return ti_create_grid_impl(device, ndim, dims, nvar, types, data, false, out);
+}
+
+int qsk_ti_fft_size(const qsk_ti *ti, unsigned *fft_size) {
+    if (!ti || !fft_size) return fail(QSK_ERR_ARG, "null argument");
+    for (int d = 0; d < ti->g.nd; ++d) fft_size[d] = unsigned(ti->g.fft[d]);
+    return QSK_OK;
+}
+
+int qsk_ti_destroy(qsk_ti *ti) {
+    if (!ti) return QSK_OK;
+    DeviceGuard dgd(ti->device);
+    delete ti;
+    return QSK_OK;
+}
+
+int qsk_worker_create(qsk_ti *ti, qsk_worker **out) {
+    if (!ti || !out) return fail(QSK_ERR_ARG, "null argument");
+    DeviceGuard dgd(ti->device);
+    qsk_worker *w = new qsk_worker();
+    w->ti = ti;
+    cudaError_t e = cudaStreamCreateWithFlags(&w->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete w;
+        return fail(QSK_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    }
+    *out = w;
+    return QSK_OK;
+}
+
+int qsk_worker_destroy(qsk_worker *w) {
+    if (!w) return QSK_OK;
+    DeviceGuard dgd(w->ti->device);
+    if (w->st) cudaStreamDestroy(w->st);
+    delete w;
+    return QSK_OK;
+}
+
+int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                            const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
+                            unsigned *out_index, int *out_min) {
+    if (!w || B < 0 || !nb_ptr || !term_ptr || !seeds || !out_score || !out_index) return fail(QSK_ERR_ARG, "null argument");
+    if (k < 1 || k > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "k=%u outside [1,%d]", k, QSK_KMAX);
+    if (B == 0) return QSK_OK;
+    if (B > 65535) return fail(QSK_ERR_UNSUPPORTED, "at most 65535 patterns per batch (got %d)", B);
+    qsk_ti *ti = w->ti;
+    DeviceGuard dgd(ti->device);
+    const Geom &g = ti->g;
+    const int nd = g.nd;
+    w->h_slots.resize(B);
+    int maxterms = 1;
+    for (int b = 0; b < B; ++b) maxterms = std::max(maxterms, term_ptr[b + 1] - term_ptr[b]);
+    w->h_terms.assign(size_t(B) * maxterms, Term{0, 0.f, 0.f, 0});
+    std::vector<Term> tmp;
+    for (int b = 0; b < B; ++b) {
+        int nnb = nb_ptr[b + 1] - nb_ptr[b];
+        int nt = term_ptr[b + 1] - term_ptr[b];
+        int rc = build_pattern_slot(ti, nnb, offsets + size_t(nb_ptr[b]) * nd, nt, terms + term_ptr[b], k, seeds[b], b,
+                                    w->h_slots[b], tmp, out_min ? out_min + size_t(b) * nd : nullptr);
+        if (rc) return rc;
+        std::copy(tmp.begin(), tmp.end(), w->h_terms.begin() + size_t(b) * maxterms);
+    }
+    if (smem_configured_device != ti->device) {
+        CK(set_map_smem_limit(200 * 1024));
+        smem_configured_device = ti->device;
+    }
+    if ((size_t)maxterms * sizeof(Term) > 200 * 1024) return fail(QSK_ERR_UNSUPPORTED, "too many terms (%d)", maxterms);
+    CK(w->slots.upload(w->h_slots.data(), B, w->st));
+    CK(w->terms.upload(w->h_terms.data(), w->h_terms.size(), w->st));
+    CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt));
+    CK(w->out_val.ensure(size_t(B) * k));
+    CK(w->out_pos.ensure(size_t(B) * k));
+    MapArgs ma;
+    ma.g = g;
+    ma.layers = ti->layers.p;
+    ma.slots = w->slots.p;
+    ma.terms = w->terms.p;
+    ma.maxterms = maxterms;
+    ma.segs_per_cta = map_segs_per_cta(g, B);
+    ma.rec_val = w->rec_val.p;
+    ma.rec_idx = w->rec_idx.p;
+    ma.rec_cnt = w->rec_cnt.p;
+    CK(launch_map_records(ma, B, int(k), maxterms, w->st));
+    ReplayArgs ra;
+    std::memset(&ra, 0, sizeof(ra));
+    ra.g = g;
+    ra.slots = w->slots.p;
+    ra.nslots = B;
+    ra.K = int(k);
+    ra.rec_val = w->rec_val.p;
+    ra.rec_idx = w->rec_idx.p;
+    ra.rec_cnt = w->rec_cnt.p;
+    ra.out_val = w->out_val.p;
+    ra.out_pos = w->out_pos.p;
+    CK(launch_replay(ra, w->st));
+    CK(cudaMemcpyAsync(out_score, w->out_val.p, sizeof(float) * B * k, cudaMemcpyDeviceToHost, w->st));
+    CK(cudaMemcpyAsync(out_index, w->out_pos.p, sizeof(unsigned) * B * k, cudaMemcpyDeviceToHost, w->st));
+    CK(cudaStreamSynchronize(w->st));
+    // empty patterns keep -inf scores (candidateForPattern returned false)
+    for (int b = 0; b < B; ++b)
+        if (w->h_slots[b].flags & SLOT_SKIP)
+            for (unsigned j = 0; j < k; ++j) {
+                out_score[size_t(b) * k + j] = -INFINITY;
+                out_index[size_t(b) * k + j] = 0xffffffffu;
+            }
+    return QSK_OK;
+}
+
+int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
+                      unsigned k, float seed, float *out_score, unsigned *out_index, int *out_min) {
+    int nb_ptr[2] = {0, n_neighbours};
+    int term_ptr[2] = {0, n_terms};
+    return qsk_pattern_kbest_batch(w, 1, nb_ptr, offsets, term_ptr, terms, k, &seed, out_score, out_index, out_min);
+}
+
+unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index) {
+    const Geom &g = ti->g;
+    unsigned position = 0;
+    unsigned div = unsigned(g.N);
+    for (int i = g.nd - 1; i >= 0; --i) {
+        unsigned f = unsigned(g.fft[i]), s = unsigned(g.src[i]);
+        div /= f;
+        position = position * s + ((f - (index / div) % f - unsigned(min_offset[i]) - 1u) + s) % s;
+    }
+    return position;
+}
+
+unsigned qsk_position_to_index(const qsk_ti *ti, const int *min_offset, unsigned position) {
+    const Geom &g = ti->g;
+    unsigned index = 0;
+    unsigned div = 1;
+    for (int i = g.nd - 1; i >= 0; --i) div *= unsigned(g.src[i]);
+    for (int i = g.nd - 1; i >= 0; --i) {
+        unsigned f = unsigned(g.fft[i]), s = unsigned(g.src[i]);
+        div /= s;
+        index = index * f + (f - (position / div + unsigned(min_offset[i])) % s - 1u);
+    }
+    return index;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// full simulation
+// ---------------------------------------------------------------------------
+struct qsk_sim {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    qsk_ti *ti = nullptr;
+    int nd = 0, nvar = 0, n = 0, K = 1;
+    float k = 1.f;
+    unsigned seed = 0;
+    GridDesc dg;
+    long long cells = 0, nodes = 0;
+    unsigned begin = 0;
+    // host plan
+    std::vector<int> tpl;            // ntpl * nd
+    std::vector<float> wtab;         // ntpl * nvar
+    std::vector<unsigned> order;     // path (all cells)
+    std::vector<float> seeds;        // per path index
+    std::vector<unsigned> posterior; // per cell
+    std::vector<int> node_of_cell;   // per cell
+    std::vector<float> init;         // grid before simulation
+    int ntpl = 0;
+    // device
+    DBuf<int> d_tpl, d_types;
+    DBuf<float> d_wtab, d_seeds, d_init, d_state;
+    DBuf<unsigned> d_path, d_post, d_id, d_node_cell, d_nb_cell;
+    DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_level, d_maxlevel, d_hist, d_start, d_cursor, d_level_nodes,
+        d_status;
+    DBuf<Slot> d_slots;
+    DBuf<Term> d_terms;
+    DBuf<float> d_rec_val;
+    DBuf<int> d_rec_idx, d_rec_cnt;
+    int maxterms = 0;
+    int max_slots = 0;
+    qsk_sim_info info;
+    bool neighbours_ready = false;
+};
+
+namespace {
+
+// a1: sorted search template (src/qs.cpp:1055-1135); fills tpl (ntpl*nd) and
+// the kernel weight of every offset and variable (wtab, ntpl*nvar)
+int make_template(int nd, int nvar, const unsigned *kdims, const float *kernel, std::vector<int> &tpl_out,
+                  std::vector<float> &wtab_out) {
+    std::vector<std::vector<int>> pos;
+    pos.push_back(std::vector<int>());
+    for (int i = 0; i < nd; ++i) {
+        size_t orig = pos.size();
+        int half = (int(kdims[i]) + 1) / 2;
+        pos.resize(orig * (2 * half - 1));
+        for (size_t q = 0; q < orig; ++q) pos[q].push_back(0);
+        for (int j = 1; j < half; ++j) {
+            std::copy(pos.begin(), pos.begin() + orig, pos.begin() + orig * (2 * j - 1));
+            std::copy(pos.begin(), pos.begin() + orig, pos.begin() + orig * (2 * j));
+            for (size_t q = orig * (2 * j - 1); q < orig * (2 * j); ++q) pos[q][i] = j;
+            for (size_t q = orig * (2 * j); q < orig * (2 * j + 1); ++q) pos[q][i] = -j;
+        }
+    }
+    long long kstride[QSK_MAXD];
+    long long ks = 1;
+    for (int d = 0; d < nd; ++d) {
+        kstride[d] = ks;
+        ks *= kdims[d];
+    }
+    if (kernel) {  // remove offsets whose kernel weight (variable 0) is NaN (src/qs.cpp:1107-1128)
+        std::vector<std::vector<int>> kept;
+        for (auto &v : pos) {
+            long long f = 0;
+            for (int d = 0; d < nd; ++d) f += (long long)(int((kdims[d] - 1) / 2) + v[d]) * kstride[d];
+            if (!std::isnan(kernel[size_t(f) * nvar])) kept.push_back(v);
+        }
+        pos.swap(kept);
+    }
+    std::sort(pos.begin(), pos.end(), [](const std::vector<int> &a, const std::vector<int> &b) {
+        float da = 0.f, db = 0.f;
+        for (size_t i = 0; i < a.size(); ++i) da += float(a[i] * a[i]);
+        for (size_t i = 0; i < b.size(); ++i) db += float(b[i] * b[i]);
+        return -da > -db;
+    });
+    const int ntpl = int(pos.size());
+    tpl_out.resize(size_t(ntpl) * nd);
+    wtab_out.resize(size_t(ntpl) * nvar);
+    for (int t = 0; t < ntpl; ++t) {
+        for (int d = 0; d < nd; ++d) tpl_out[size_t(t) * nd + d] = pos[t][d];
+        // weight lookup centred at dims/2 (quantileSamplingModule.hpp:362-366)
+        for (int v = 0; v < nvar; ++v) {
+            float w = 1.f;
+            if (kernel) {
+                long long f = 0;
+                bool ok = true;
+                for (int d = 0; d < nd; ++d) {
+                    int c = int(kdims[d] / 2) + pos[t][d];
+                    ok &= c >= 0 && c < int(kdims[d]);
+                    f += (long long)c * kstride[d];
+                }
+                w = ok ? kernel[size_t(f) * nvar + v] : 0.f;
+            }
+            wtab_out[size_t(t) * nvar + v] = w;
+        }
+    }
+    return ntpl;
+}
+
+void build_template(qsk_sim *s, const unsigned *kdims, const float *kernel) {
+    s->ntpl = make_template(s->nd, s->nvar, kdims, kernel, s->tpl, s->wtab);
+}
+
+// a2: path and per-node seeds (src/qs.cpp:975,1159-1201,1250-1258): informed
+// cells first, the rest shuffled by mt19937(seed); then one U[0,1) float per
+// path position from the same generator.  Returns the number of informed cells.
+unsigned make_path(size_t n, int nvar, const float *init, unsigned seed, std::vector<unsigned> &order,
+                   std::vector<float> &seeds) {
+    std::mt19937 gen(seed);
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0u);
+    unsigned begin = 0;
+    for (size_t i = 0; i < n; ++i) {
+        bool set = true;
+        for (int v = 0; v < nvar; ++v)
+            if (std::isnan(init[i * nvar + v])) set = false;
+        if (set) {
+            std::swap(order[begin], order[i]);
+            begin++;
+        }
+    }
+    std::shuffle(order.begin() + begin, order.end(), gen);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    seeds.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        seeds[i] = u(gen);
+        if (seeds[i] == 1.f) seeds[i] = u(gen);
+    }
+    return begin;
+}
+
+// posterior order (src/qs.cpp:1604-1641)
+void build_path(qsk_sim *s) {
+    const size_t n = size_t(s->cells);
+    unsigned begin = make_path(n, s->nvar, s->init.data(), s->seed, s->order, s->seeds);
+    s->begin = begin;
+    s->nodes = (long long)n - begin;
+    s->posterior.assign(n, std::numeric_limits<unsigned>::max());
+    s->node_of_cell.assign(n, -1);
+    for (size_t i = 0; i < n; ++i) {
+        bool withNan = false;
+        for (int v = 0; v < s->nvar; ++v) withNan |= std::isnan(s->init[i * s->nvar + v]);
+        if (!withNan) s->posterior[i] = 0;
+    }
+    for (long long i = 0; i < s->nodes; ++i) {
+        s->posterior[s->order[begin + i]] = unsigned(i);
+        s->node_of_cell[s->order[begin + i]] = int(i);
+    }
+}
+
+int sim_neighbours(qsk_sim *s) {
+    if (s->neighbours_ready) return QSK_OK;
+    CK(launch_neighbours(s->dg, s->d_tpl.p, s->ntpl, s->d_path.p, s->begin, s->nodes, s->d_post.p, s->n,
+                         s->d_nb_count.p, s->d_nb_tpl.p, s->d_nb_cell.p, s->st));
+    s->neighbours_ready = true;
+    return QSK_OK;
+}
+
+// run the batches of nodes listed in d_level_nodes[start[l]..start[l+1]) for each level
+int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
+    const Geom &g = s->ti->g;
+    for (size_t l = 0; l + 1 < start.size(); ++l) {
+        int a = start[l], e = start[l + 1];
+        for (int off = a; off < e; off += s->max_slots) {
+            int B = std::min(s->max_slots, e - off);
+            SimPrepArgs pa;
+            pa.g = g;
+            pa.dg = s->dg;
+            pa.nvar = s->nvar;
+            pa.types = s->d_types.p;
+            pa.tpl = s->d_tpl.p;
+            pa.wtab = s->d_wtab.p;
+            pa.path = s->d_path.p;
+            pa.begin = s->begin;
+            pa.seeds = s->d_seeds.p;
+            pa.nb_count = s->d_nb_count.p;
+            pa.nb_tpl = s->d_nb_tpl.p;
+            pa.nb_cell = s->d_nb_cell.p;
+            pa.n = s->n;
+            pa.state = s->d_state.p;
+            pa.init = s->d_init.p;
+            pa.nodes = s->d_level_nodes.p + off;
+            pa.nslots = B;
+            pa.k = s->k;
+            pa.K = s->K;
+            pa.nti = 1;
+            pa.slots = s->d_slots.p;
+            pa.terms = s->d_terms.p;
+            pa.maxterms = s->maxterms;
+            pa.status = s->d_status.p;
+            CK(launch_prep_sim(pa, s->st));
+            MapArgs ma;
+            ma.g = g;
+            ma.layers = s->ti->layers.p;
+            ma.slots = s->d_slots.p;
+            ma.terms = s->d_terms.p;
+            ma.maxterms = s->maxterms;
+            ma.segs_per_cta = map_segs_per_cta(g, B);
+            ma.rec_val = s->d_rec_val.p;
+            ma.rec_idx = s->d_rec_idx.p;
+            ma.rec_cnt = s->d_rec_cnt.p;
+            CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+            ReplayArgs ra;
+            std::memset(&ra, 0, sizeof(ra));
+            ra.g = g;
+            ra.slots = s->d_slots.p;
+            ra.nslots = B;
+            ra.K = s->K;
+            ra.rec_val = s->d_rec_val.p;
+            ra.rec_idx = s->d_rec_idx.p;
+            ra.rec_cnt = s->d_rec_cnt.p;
+            ra.nvar = s->nvar;
+            ra.ti = s->ti->grid.p;
+            ra.ti_cells = s->ti->cells;
+            ra.nti = 1;
+            ra.ti_id = 0;
+            ra.state = teacher ? nullptr : s->d_state.p;
+            ra.id_image = teacher ? nullptr : s->d_id.p;
+            ra.node_cell = s->d_node_cell.p;
+            CK(launch_replay(ra, s->st));
+        }
+    }
+    return QSK_OK;
+}
+
+int sim_check_status(qsk_sim *s) {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, s->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (st != DEV_OK) return fail(QSK_ERR_DEVICE, "device status %d (too many terms for a node)", st);
+    return QSK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk_sim **out) {
+    if (!p || !out || !di_init || !p->ti_dims || !p->di_dims || !p->types || !p->ti) return fail(QSK_ERR_ARG, "null argument");
+    if (p->ndim < 1 || p->ndim > QSK_MAXD) return fail(QSK_ERR_UNSUPPORTED, "ndim %d", p->ndim);
+    if (p->n < 1) return fail(QSK_ERR_ARG, "n must be >= 1");
+    if (!(p->k >= 1.f)) return fail(QSK_ERR_UNSUPPORTED, "k must be >= 1 (got %g)", double(p->k));
+    int K = int(std::ceil(double(p->k)));
+    if (K > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "ceil(k)=%d > %d", K, QSK_KMAX);
+    DeviceGuard dgd(device);
+    qsk_sim *s = new qsk_sim();
+    std::memset(&s->info, 0, sizeof(s->info));
+    s->device = device;
+    s->nd = p->ndim;
+    s->nvar = p->nvar;
+    s->n = p->n;
+    s->k = p->k;
+    s->K = K;
+    s->seed = p->seed;
+    auto bail = [&](int rc) {
+        qsk_sim_destroy(s);
+        return rc;
+    };
+    int rc = qsk_ti_create_grid(device, p->ndim, p->ti_dims, p->nvar, p->types, p->ti, &s->ti);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(fail(QSK_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
+    s->cells = 1;
+    std::memset(&s->dg, 0, sizeof(s->dg));
+    s->dg.nd = p->ndim;
+    for (int d = 0; d < p->ndim; ++d) {
+        s->dg.dims[d] = int(p->di_dims[d]);
+        s->dg.stride[d] = s->cells;
+        s->cells *= p->di_dims[d];
+    }
+    if (s->cells >= (1LL << 32) - 1) return bail(fail(QSK_ERR_UNSUPPORTED, "grid too large"));
+    s->init.assign(di_init, di_init + size_t(s->cells) * s->nvar);
+    // kernel: given, or uniform of size min(TI/2+1) (src/qs.cpp:1010-1042)
+    std::vector<unsigned> kd(p->ndim);
+    if (p->kernel && p->kernel_dims) {
+        for (int d = 0; d < p->ndim; ++d) kd[d] = p->kernel_dims[d];
+        build_template(s, kd.data(), p->kernel);
+    } else {
+        for (int d = 0; d < p->ndim; ++d) kd[d] = std::min(p->ti_dims[d] / 2 + 1, p->ti_dims[d]);
+        build_template(s, kd.data(), nullptr);
+    }
+    build_path(s);
+    s->maxterms = std::max(1, s->n * s->nvar);
+    // uploads
+    if ((e = s->d_tpl.upload(s->tpl.data(), s->tpl.size(), s->st)) != cudaSuccess ||
+        (e = s->d_wtab.upload(s->wtab.data(), s->wtab.size(), s->st)) != cudaSuccess ||
+        (e = s->d_types.upload(p->types, size_t(p->nvar), s->st)) != cudaSuccess ||
+        (e = s->d_path.upload(s->order.data(), s->order.size(), s->st)) != cudaSuccess ||
+        (e = s->d_seeds.upload(s->seeds.data(), s->seeds.size(), s->st)) != cudaSuccess ||
+        (e = s->d_post.upload(s->posterior.data(), s->posterior.size(), s->st)) != cudaSuccess ||
+        (e = s->d_node_of_cell.upload(s->node_of_cell.data(), s->node_of_cell.size(), s->st)) != cudaSuccess ||
+        (e = s->d_init.upload(s->init.data(), s->init.size(), s->st)) != cudaSuccess ||
+        (e = s->d_state.alloc(s->init.size())) != cudaSuccess || (e = s->d_id.alloc(size_t(s->cells))) != cudaSuccess ||
+        (e = s->d_node_cell.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_nb_count.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_nb_tpl.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
+        (e = s->d_nb_cell.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
+        (e = s->d_level.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_level_nodes.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_maxlevel.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess)
+        return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "upload: %s",
+                         cudaGetErrorString(e)));
+    // batch scratch: slots up to a record budget of ~2 GiB
+    const Geom &g = s->ti->g;
+    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 4 + sizeof(Term) * s->maxterms;
+    size_t budget = size_t(2) << 30;
+    long long ms = (long long)(budget / per_slot);
+    ms = std::max<long long>(1, std::min<long long>(ms, std::max<long long>(s->nodes, 1)));
+    ms = std::min<long long>(ms, 65535);
+    s->max_slots = int(ms);
+    if ((e = s->d_slots.alloc(size_t(s->max_slots))) != cudaSuccess ||
+        (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess ||
+        (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt)) != cudaSuccess)
+        return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "scratch: %s",
+                         cudaGetErrorString(e)));
+    if ((size_t)s->maxterms * sizeof(Term) > 200 * 1024) return bail(fail(QSK_ERR_UNSUPPORTED, "n*nvar too large"));
+    if (smem_configured_device != device) {
+        if ((e = set_map_smem_limit(200 * 1024)) != cudaSuccess) return bail(fail(QSK_ERR_CUDA, "smem attr"));
+        smem_configured_device = device;
+    }
+    if ((e = cudaStreamSynchronize(s->st)) != cudaSuccess) return bail(fail(QSK_ERR_CUDA, "%s", cudaGetErrorString(e)));
+    s->info.nodes = s->nodes;
+    s->info.template_size = s->ntpl;
+    *out = s;
+    return QSK_OK;
+}
+
+int qsk_sim_run(qsk_sim *s) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    DeviceGuard dgd(s->device);
+    cudaEvent_t ev[4];
+    for (auto &x : ev) CK(cudaEventCreate(&x));
+    CK(cudaMemcpyAsync(s->d_state.p, s->d_init.p, sizeof(float) * s->init.size(), cudaMemcpyDeviceToDevice, s->st));
+    CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells, s->st));
+    CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
+    CK(cudaEventRecord(ev[0], s->st));
+    s->neighbours_ready = false;
+    int rc = sim_neighbours(s);
+    if (rc) return rc;
+    CK(cudaEventRecord(ev[1], s->st));
+    CK(cudaMemsetAsync(s->d_maxlevel.p, 0, sizeof(int), s->st));
+    CK(launch_levels(s->nodes, s->n, s->d_nb_count.p, s->d_nb_cell.p, s->d_node_of_cell.p, s->d_level.p,
+                     s->d_maxlevel.p, s->st));
+    int maxl = 0;
+    CK(cudaMemcpyAsync(&maxl, s->d_maxlevel.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    int nl = s->nodes > 0 ? maxl + 1 : 0;
+    std::vector<int> start(size_t(nl) + 1, 0);
+    if (nl > 0) {
+        CK(s->d_hist.ensure(size_t(nl)));
+        CK(s->d_start.ensure(size_t(nl) + 1));
+        CK(s->d_cursor.ensure(size_t(nl)));
+        CK(cudaMemsetAsync(s->d_hist.p, 0, sizeof(int) * nl, s->st));
+        CK(launch_level_sort(s->nodes, nl, s->d_level.p, s->d_hist.p, s->d_start.p, s->d_cursor.p, s->d_level_nodes.p,
+                             s->st));
+        CK(cudaMemcpyAsync(start.data(), s->d_start.p, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    CK(cudaEventRecord(ev[2], s->st));
+    rc = sim_batches(s, start, false);
+    if (rc) return rc;
+    CK(cudaEventRecord(ev[3], s->st));
+    CK(cudaEventSynchronize(ev[3]));
+    int mb = 0;
+    for (int l = 0; l < nl; ++l) mb = std::max(mb, start[l + 1] - start[l]);
+    s->info.levels = nl;
+    s->info.max_batch = mb;
+    cudaEventElapsedTime(&s->info.ms_setup_neighbours, ev[0], ev[1]);
+    cudaEventElapsedTime(&s->info.ms_levels, ev[1], ev[2]);
+    cudaEventElapsedTime(&s->info.ms_batches, ev[2], ev[3]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    return sim_check_status(s);
+}
+
+int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed) {
+    if (!s || !di_completed) return fail(QSK_ERR_ARG, "null argument");
+    DeviceGuard dgd(s->device);
+    CK(cudaMemcpyAsync(s->d_state.p, di_completed, sizeof(float) * s->init.size(), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
+    int rc = sim_neighbours(s);
+    if (rc) return rc;
+    // every node is independent under teacher forcing: one level of all nodes in path order
+    std::vector<int> ident(size_t(std::max<long long>(s->nodes, 1)));
+    std::iota(ident.begin(), ident.end(), 0);
+    CK(cudaMemcpyAsync(s->d_level_nodes.p, ident.data(), sizeof(int) * s->nodes, cudaMemcpyHostToDevice, s->st));
+    std::vector<int> start = {0, int(s->nodes)};
+    rc = sim_batches(s, start, true);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return sim_check_status(s);
+}
+
+int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    DeviceGuard dgd(s->device);
+    if (di_out)
+        CK(cudaMemcpyAsync(di_out, s->d_state.p, sizeof(float) * s->init.size(), cudaMemcpyDeviceToHost, s->st));
+    if (id_out) CK(cudaMemcpyAsync(id_out, s->d_id.p, sizeof(unsigned) * s->cells, cudaMemcpyDeviceToHost, s->st));
+    if (node_cell_out && s->nodes > 0)
+        CK(cudaMemcpyAsync(node_cell_out, s->d_node_cell.p, sizeof(unsigned) * s->nodes, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return QSK_OK;
+}
+
+int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info) {
+    if (!s || !info) return fail(QSK_ERR_ARG, "null argument");
+    *info = s->info;
+    return QSK_OK;
+}
+
+int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    if (order) std::copy(s->order.begin(), s->order.end(), order);
+    if (seeds) std::copy(s->seeds.begin(), s->seeds.end(), seeds);
+    if (begin) *begin = s->begin;
+    return QSK_OK;
+}
+
+int qsk_sim_destroy(qsk_sim *s) {
+    if (!s) return QSK_OK;
+    {
+        DeviceGuard dgd(s->device);
+        if (s->st) cudaStreamDestroy(s->st);
+        s->st = nullptr;
+        if (s->ti) qsk_ti_destroy(s->ti);
+        s->ti = nullptr;
+        delete s;
+    }
+    return QSK_OK;
+}
+
+int qsk_qs_template(int ndim, int nvar, const unsigned *kernel_dims, const float *kernel, int *offsets, float *weights,
+                    int capacity) {
+    if (!kernel_dims || ndim < 1 || ndim > QSK_MAXD || nvar < 1) return -QSK_ERR_ARG;
+    std::vector<int> tpl;
+    std::vector<float> w;
+    int n = make_template(ndim, nvar, kernel_dims, kernel, tpl, w);
+    for (int t = 0; t < n && t < capacity; ++t) {
+        if (offsets)
+            for (int d = 0; d < ndim; ++d) offsets[t * ndim + d] = tpl[size_t(t) * ndim + d];
+        if (weights)
+            for (int v = 0; v < nvar; ++v) weights[t * nvar + v] = w[size_t(t) * nvar + v];
+    }
+    return n;
+}
+
+long long qsk_qs_path(long long cells, int nvar, const float *di_init, unsigned seed, unsigned *order, float *seeds) {
+    if (!di_init || cells < 1 || nvar < 1) return -QSK_ERR_ARG;
+    std::vector<unsigned> o;
+    std::vector<float> sd;
+    unsigned begin = make_path(size_t(cells), nvar, di_init, seed, o, sd);
+    if (order) std::copy(o.begin(), o.end(), order);
+    if (seeds) std::copy(sd.begin(), sd.end(), seeds);
+    return (long long)begin;
+}
+
+int qsk_simulate(int device, const qsk_qs_params *p, float *di_inout, unsigned *id_out) {
+    qsk_sim *s = nullptr;
+    int rc = qsk_sim_create(device, p, di_inout, &s);
+    if (rc) return rc;
+    rc = qsk_sim_run(s);
+    if (!rc) rc = qsk_sim_read(s, di_inout, id_out, nullptr);
+    qsk_sim_destroy(s);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,148 @@
+// Internal declarations shared by the host engine (qsk_host.cpp) and the
+// CUDA kernels (qsk_kernels.cu) of the B200 QuickSampling path.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime_api.h>
+
+#define QSK_MAXD 4          // grid dimensions supported
+#define QSK_SEG 128         // scan positions per warp segment (32 lanes x 4)
+#define QSK_KMAX 16         // largest extendK handled on device
+
+namespace qsk {
+
+// Operation applied to one gathered layer value x for one term.
+enum TermOp : int {
+    OP_LIN = 0,    // acc = fma(a, x, acc)
+    OP_SQLIN = 1,  // acc = fma(a, x*x, acc); acc = fma(b, x, acc)   (continuous variable)
+    OP_EQ = 2,     // acc = (x == b) ? acc + a : acc                  (categorical variable)
+};
+
+struct Term {
+    int base;   // layer offset minus the neighbour's flat scan offset: address = base + m
+    float a;
+    float b;
+    int op;
+};
+
+// Scan geometry of one training image (the reference's flipped correlation
+// space, G2S src/CPUThreadDevice.cpp:257-284,454-477).
+struct Geom {
+    int nd;
+    int fft[QSK_MAXD];       // fft size per dimension (x first)
+    int src[QSK_MAXD];       // TI size per dimension
+    long long sstride[QSK_MAXD];  // scan (fft) strides
+    long long N;             // prod(fft)
+    int nseg;                // ceil(N / QSK_SEG)
+};
+
+// Per node (batch slot) description written by the prep step.
+struct Slot {
+    int node;                // path index (simulation) or pattern id
+    int nterms;
+    int mn[QSK_MAXD];        // min neighbour offset per dim (init 0)
+    int lo[QSK_MAXD];        // first valid scan coordinate per dim
+    float seed;
+    int sel;                 // drawn candidate rank
+    int flags;               // SLOT_* bits
+    unsigned cell;           // DI cell (simulation)
+};
+
+enum SlotFlags : int {
+    SLOT_SKIP = 1,           // no map: marginal draw or empty pattern
+    SLOT_EMIT_MASKED = 2,    // fewer than K valid positions: masked entries are candidates too
+};
+
+// Status words written by kernels (bounded waits / argument checks).
+enum DevStatus : int {
+    DEV_OK = 0,
+    DEV_BAD_INDEX = 1,
+    DEV_TOO_MANY_TERMS = 2,
+};
+
+// Grid (destination image) description for the neighbour search.
+struct GridDesc {
+    int nd;
+    int dims[QSK_MAXD];
+    long long stride[QSK_MAXD];
+};
+
+struct SimPrepArgs {
+    Geom g;
+    GridDesc dg;
+    int nvar;
+    const int *types;
+    const int *tpl;        // ntpl x nd offsets
+    const float *wtab;     // ntpl x nvar kernel weights
+    const unsigned *path;
+    unsigned begin;
+    const float *seeds;    // per path index
+    const int *nb_count;
+    const int *nb_tpl;
+    const unsigned *nb_cell;
+    int n;
+    const float *state;    // current grid values (cells x nvar)
+    const float *init;     // grid before simulation (centre values)
+    const int *nodes;      // slot -> path index
+    int nslots;
+    float k;
+    int K;
+    unsigned nti;
+    Slot *slots;
+    Term *terms;
+    int maxterms;
+    int *status;
+};
+
+struct MapArgs {
+    Geom g;
+    const float *layers;
+    const Slot *slots;
+    const Term *terms;
+    int maxterms;
+    int segs_per_cta;
+    float *rec_val;   // [slot][nseg*SEG]
+    int *rec_idx;
+    int *rec_cnt;     // [slot][nseg]
+};
+
+struct ReplayArgs {
+    Geom g;
+    const Slot *slots;
+    int nslots;
+    int K;
+    const float *rec_val;
+    const int *rec_idx;
+    const int *rec_cnt;
+    // pattern outputs (may be null)
+    float *out_val;       // [slot][K]
+    unsigned *out_pos;    // [slot][K]
+    // simulation outputs (may be null)
+    int nvar;
+    const float *ti;      // TI grid (cells x nvar)
+    long long ti_cells;
+    unsigned nti, ti_id;
+    float *state;         // grid written in simulation mode (null in teacher-forced mode)
+    unsigned *id_image;   // per grid cell
+    unsigned *node_cell;  // per path index: chosen TI cell
+};
+
+
+// launch wrappers (qsk_kernels.cu)
+cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers,
+                                cudaStream_t st);
+cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
+                              long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
+                              unsigned *nb_cell, cudaStream_t st);
+cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
+                          const int *node_of_cell, int *level, int *max_level, cudaStream_t st);
+cudaError_t launch_level_sort(long long nodes, int nl, const int *level, int *hist, int *start, int *cursor,
+                              int *level_nodes, cudaStream_t st);
+cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);
+int map_segs_per_cta(const Geom &g, int nslots);
+cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
+cudaError_t set_map_smem_limit(int bytes);
+cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
+
+}  // namespace qsk

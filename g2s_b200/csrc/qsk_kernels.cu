@@ -1,0 +1,834 @@
+// CUDA kernels of the B200 QuickSampling (QS) hot path, sm_100a.
+//
+// Per batch of independent path nodes ("slots"):
+//   k_prep_sim     neighbour values -> per-node term list, border bounds
+//                  (G2S include/simulation.hpp:447-537, quantileSamplingModule.hpp:368-457,
+//                   DataImage.hpp:626-710, CPUThreadDevice.cpp:352-366,454-477)
+//   k_map_records  mismatch map of every scan position in FP32 (direct sum in
+//                  the reference's layer decomposition, CPUThreadDevice.cpp:349-490)
+//                  fused with a warp prefix-top-K filter that keeps only the
+//                  positions that can enter the running k-best ("records")
+//   k_replay       exact replay of the reference's k-biggest scan with its
+//                  mt19937 reservoir tie-breaking (fKb.hpp:58-92,121-132,
+//                  quantileSamplingModule.hpp:45-49,525-557) over the records,
+//                  then the draw and the write-back (quantileSamplingModule.hpp:90-126,
+//                  CPUThreadDevice.cpp:257-268, simulation.hpp:586-666)
+// Setup kernels: k_build_layers (DataImage.hpp:538-599), k_neighbours
+// (simulation.hpp:447-511, run for every path node at once), k_levels
+// (dependency levels of the path DAG).
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <cstdint>
+
+#include "qsk_internal.h"
+
+namespace qsk {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// merge two descending top-K lists (register arrays, static indices only):
+// c_t = max_{i=0..t+1} min(a_{i-1}, b_{t-i}), with a_{-1} = b_{-1} = +inf.
+template <int K>
+__device__ __forceinline__ void topk_merge(const float (&a)[K], const float (&b)[K], float (&c)[K]) {
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+        float best = -CUDART_INF_F;
+#pragma unroll
+        for (int i = 0; i <= t + 1; ++i) {
+            float ai = (i == 0) ? CUDART_INF_F : a[i - 1];
+            float bj = (t - i >= 0) ? b[t - i] : CUDART_INF_F;
+            best = fmaxf(best, fminf(ai, bj));
+        }
+        c[t] = best;
+    }
+}
+
+// number of valid scan positions < x (x in [0, N])
+__device__ long long valid_prefix(const Geom &g, const int *lo, long long x) {
+    long long vd[QSK_MAXD];
+    long long acc = 1;
+    for (int d = 0; d < g.nd; ++d) {
+        vd[d] = acc;
+        long long w = g.fft[d] - lo[d];
+        acc *= (w > 0 ? w : 0);
+    }
+    if (x >= g.N) return acc;
+    long long count = 0;
+    for (int d = g.nd - 1; d >= 0; --d) {
+        long long digit = (x / g.sstride[d]) % g.fft[d];
+        long long t = digit - lo[d];
+        if (t > 0) count += t * vd[d];
+        if (digit < lo[d]) break;
+    }
+    return count;
+}
+
+// ---------------------------------------------------------------------------
+// layers: flipped copy of each TI variable (DataImage.hpp:538-599)
+// continuous: value with NaN -> 0 ; categorical: value kept as the category
+// code (NaN stays NaN, so it never equals a code).  Positions of the fft grid
+// outside the TI hold 0 (continuous) / NaN (categorical).
+// ---------------------------------------------------------------------------
+__global__ void k_build_layers(const float *__restrict__ ti, int nvar, const int *__restrict__ types, Geom g,
+                               float *__restrict__ layers) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.N) return;
+    // q is an fft-grid flat index of the flipped array: coord = fft-1-digit
+    long long src_flat = 0, sstr = 1;
+    bool inside = true;
+    for (int d = 0; d < g.nd; ++d) {
+        long long digit = (q / g.sstride[d]) % g.fft[d];
+        long long c = g.fft[d] - 1 - digit;
+        inside &= c < g.src[d];
+        src_flat += c * sstr;
+        sstr *= g.src[d];
+    }
+    for (int v = 0; v < nvar; ++v) {
+        float x;
+        if (inside) {
+            x = ti[src_flat * nvar + v];
+            if (types[v] == 0 && isnan(x)) x = 0.f;
+        } else {
+            x = types[v] == 0 ? 0.f : CUDART_NAN_F;
+        }
+        layers[(long long)v * g.N + q] = x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// neighbour search for every path node (simulation.hpp:447-511, single n,
+// non-strict informed rule: cells with path order <= the node's, the node
+// itself included).
+// ---------------------------------------------------------------------------
+__global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl, const unsigned *__restrict__ path,
+                             unsigned begin, long long nodes, const unsigned *__restrict__ posterior, int n,
+                             int *__restrict__ nb_count, int *__restrict__ nb_tpl, unsigned *__restrict__ nb_cell) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    unsigned cell = path[begin + i];
+    unsigned order = posterior[cell];
+    int c0[QSK_MAXD];
+    long long rem = cell;
+    for (int d = 0; d < dg.nd; ++d) {
+        c0[d] = int(rem % dg.dims[d]);
+        rem /= dg.dims[d];
+    }
+    int cnt = 0;
+    for (int t = 0; t < ntpl && cnt < n; ++t) {
+        bool ok = true;
+        long long nc = 0;
+        for (int d = 0; d < dg.nd; ++d) {
+            int c = c0[d] + tpl[t * dg.nd + d];
+            ok &= (c >= 0) && (c < dg.dims[d]);
+            nc += (long long)c * dg.stride[d];
+        }
+        if (!ok) continue;
+        if (posterior[nc] <= order) {
+            nb_tpl[i * n + cnt] = t;
+            nb_cell[i * n + cnt] = unsigned(nc);
+            cnt++;
+        }
+    }
+    nb_count[i] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// dependency levels: level(i) = 1 + max level(j) over the node's informed
+// neighbours j that are themselves path nodes.  One block walks the path in
+// chunks of blockDim nodes; inside a chunk it relaxes until nothing changes.
+// ---------------------------------------------------------------------------
+__global__ void k_levels(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
+                         const int *__restrict__ node_of_cell, int *__restrict__ level, int *__restrict__ max_level) {
+    __shared__ int changed;
+    int mx = 0;
+    for (long long c0 = 0; c0 < nodes; c0 += blockDim.x) {
+        long long i = c0 + threadIdx.x;
+        bool active = i < nodes;
+        if (active) level[i] = 0;
+        __syncthreads();
+        for (;;) {
+            if (threadIdx.x == 0) changed = 0;
+            __syncthreads();
+            if (active) {
+                int L = 0;
+                int cnt = nb_count[i];
+                for (int j = 0; j < cnt; ++j) {
+                    int dn = node_of_cell[nb_cell[i * n + j]];
+                    if (dn >= 0 && (long long)dn != i) {
+                        int lj = ((volatile int *)level)[dn] + 1;
+                        L = L > lj ? L : lj;
+                    }
+                }
+                if (L != ((volatile int *)level)[i]) {
+                    ((volatile int *)level)[i] = L;
+                    changed = 1;
+                }
+            }
+            __syncthreads();
+            if (!changed) break;
+            __syncthreads();
+        }
+        if (active) mx = mx > level[i] ? mx : level[i];
+    }
+    atomicMax(max_level, mx);
+}
+
+__global__ void k_level_hist(long long nodes, const int *__restrict__ level, int *__restrict__ hist) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nodes) atomicAdd(&hist[level[i]], 1);
+}
+
+// exclusive scan of hist[0..nl) -> start[0..nl]; single block
+__global__ void k_level_scan(int nl, const int *__restrict__ hist, int *__restrict__ start, int *__restrict__ cursor) {
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int l = 0; l < nl; ++l) {
+            start[l] = s;
+            cursor[l] = s;
+            s += hist[l];
+        }
+        start[nl] = s;
+    }
+}
+
+__global__ void k_level_scatter(long long nodes, const int *__restrict__ level, int *__restrict__ cursor,
+                                int *__restrict__ level_nodes) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nodes) level_nodes[atomicAdd(&cursor[level[i]], 1)] = int(i);
+}
+
+// ---------------------------------------------------------------------------
+// selected rank of the draw, exactly as compiled in the reference
+// (quantileSamplingModule.hpp:113 with the double overloads of ceil/floor)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int selected_index(float seed, float k, unsigned nti) {
+    double prod = (double)__fmul_rn(seed, k);
+    double c = ceil((double)__fdiv_rn((float)nti, k));
+    return int(floor(prod * (c / (double)nti)));
+}
+
+// ---------------------------------------------------------------------------
+// prep for the simulation: one warp per slot
+// ---------------------------------------------------------------------------
+__global__ void k_prep_sim(SimPrepArgs A) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= A.nslots) return;
+    const int i = A.nodes[warp];
+    const unsigned cell = A.path[A.begin + i];
+    const int cnt = A.nb_count[i];
+    const int nd = A.g.nd;
+    Slot s;
+    s.node = i;
+    s.cell = cell;
+    s.seed = A.seeds[i];
+    s.sel = selected_index(s.seed, A.k, A.nti);
+    if (s.sel < 0) s.sel = 0;
+    if (s.sel > A.K - 1) s.sel = A.K - 1;   // unreachable for seeds in [0,1)
+    s.flags = 0;
+    s.nterms = 0;
+    bool centreData = false;
+    for (int v = 0; v < A.nvar; ++v) centreData |= !isnan(A.init[(long long)cell * A.nvar + v]);
+    // min / max of the neighbour offsets, starting from 0 (AcceleratorDevice.cpp:95-112)
+    int mn[QSK_MAXD], mx[QSK_MAXD];
+#pragma unroll
+    for (int d = 0; d < QSK_MAXD; ++d) { mn[d] = 0; mx[d] = 0; }
+    for (int j = lane; j < cnt; j += 32) {
+        int t = A.nb_tpl[(long long)i * A.n + j];
+        for (int d = 0; d < nd; ++d) {
+            int o = A.tpl[t * nd + d];
+            mn[d] = min(mn[d], o);
+            mx[d] = max(mx[d], o);
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        for (int off = 16; off > 0; off >>= 1) {
+            mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], off));
+            mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], off));
+        }
+    }
+    long long nvalid = 1;
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        s.mn[d] = mn[d];
+        int lo = 0;
+        if (d < nd) {
+            lo = A.g.fft[d] - (A.g.src[d] - (mx[d] - mn[d]));
+            lo = lo < 0 ? 0 : (lo > A.g.fft[d] ? A.g.fft[d] : lo);
+            nvalid *= (A.g.fft[d] - lo);
+        }
+        s.lo[d] = lo;
+    }
+    if (cnt <= 1 && !centreData) {
+        s.flags |= SLOT_SKIP;   // marginal draw (simulation.hpp:586-605)
+    } else {
+        if (nvalid < A.K) s.flags |= SLOT_EMIT_MASKED;
+        // terms: neighbours in order, variables in order; zero-weight / NaN skipped
+        int base_out = 0;
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            int j = j0 + lane;
+            Term tl[4];
+            int nt = 0;
+            if (j < cnt) {
+                int t = A.nb_tpl[(long long)i * A.n + j];
+                unsigned nc = A.nb_cell[(long long)i * A.n + j];
+                long long d_flat = 0;
+                for (int d = 0; d < nd; ++d) d_flat += (long long)(A.tpl[t * nd + d] - mn[d]) * A.g.sstride[d];
+                for (int v = 0; v < A.nvar && v < 4; ++v) {
+                    float val = (nc == cell) ? A.init[(long long)nc * A.nvar + v] : A.state[(long long)nc * A.nvar + v];
+                    float w = A.wtab[t * A.nvar + v];
+                    if (isnan(val) || w == 0.f) continue;
+                    Term tm;
+                    tm.base = int((long long)v * A.g.N - d_flat);
+                    if (A.types[v] == 0) {
+                        tm.op = OP_SQLIN;
+                        tm.a = -w;
+                        tm.b = 2.f * __fmul_rn(w, val);
+                    } else {
+                        tm.op = OP_EQ;
+                        tm.a = w;
+                        tm.b = val;
+                    }
+                    tl[nt++] = tm;
+                }
+            }
+            // order-preserving compaction across the warp
+            int incl = nt;
+            for (int off = 1; off < 32; off <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
+            }
+            int excl = incl - nt;
+            int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int q = 0; q < nt; ++q) {
+                int o = base_out + excl + q;
+                if (o < A.maxterms) A.terms[(long long)warp * A.maxterms + o] = tl[q];
+            }
+            base_out += total;
+        }
+        if (base_out > A.maxterms) {
+            if (lane == 0) atomicExch(A.status, DEV_TOO_MANY_TERMS);
+            base_out = A.maxterms;
+        }
+        s.nterms = base_out;
+    }
+    if (lane == 0) A.slots[warp] = s;
+}
+
+// ---------------------------------------------------------------------------
+// fused map + record filter
+// ---------------------------------------------------------------------------
+template <int KF>
+__global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
+    extern __shared__ Term sterm[];
+    __shared__ Slot ss;
+    const int b = blockIdx.y;
+    if (threadIdx.x == 0) ss = A.slots[b];
+    __syncthreads();
+    if (ss.flags & SLOT_SKIP) return;
+    const int nt = ss.nterms;
+    const Term *src = A.terms + (long long)b * A.maxterms;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) sterm[t] = src[t];
+    __syncthreads();
+
+    const Geom &g = A.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const bool emit_masked = (ss.flags & SLOT_EMIT_MASKED) != 0;
+    // a valid scan position used for address-safe dummy gathers; with no valid
+    // position at all every entry is masked and no gather is issued
+    long long m_safe = 0;
+    bool any_valid = true;
+    for (int d = 0; d < g.nd; ++d) {
+        m_safe += (long long)ss.lo[d] * g.sstride[d];
+        any_valid &= ss.lo[d] < g.fft[d];
+    }
+    const int nt_eff = any_valid ? nt : 0;
+    if (!any_valid) m_safe = 0;
+    const unsigned usafe = (unsigned)m_safe;
+    const unsigned uN = (unsigned)g.N;
+
+    const int seg_begin = blockIdx.x * A.segs_per_cta;
+    int seg_end = seg_begin + A.segs_per_cta;
+    if (seg_end > g.nseg) seg_end = g.nseg;
+    float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
+    int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
+
+    for (int sg = seg_begin + warp; sg < seg_end; sg += nwarps) {
+        const unsigned base = (unsigned)sg * QSK_SEG;
+        unsigned mm[4];
+        bool valid[4], exists[4];
+        float acc[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            unsigned m = base + 32 * r + lane;
+            exists[r] = m < uN;
+            bool ok = exists[r] && any_valid;
+            if (ok) {
+#pragma unroll
+                for (int d = 0; d < QSK_MAXD; ++d)
+                    if (d < g.nd) ok &= (int)((m / (unsigned)g.sstride[d]) % (unsigned)g.fft[d]) >= ss.lo[d];
+            }
+            valid[r] = ok;
+            mm[r] = ok ? m : usafe;
+            acc[r] = 0.f;
+        }
+        for (int t = 0; t < nt_eff; ++t) {
+            const Term tm = sterm[t];
+            const float *lp = A.layers + tm.base;
+            float x[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) x[r] = __ldg(lp + mm[r]);
+            if (tm.op == OP_SQLIN) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    acc[r] = __fmaf_rn(tm.a, __fmul_rn(x[r], x[r]), acc[r]);
+                    acc[r] = __fmaf_rn(tm.b, x[r], acc[r]);
+                }
+            } else if (tm.op == OP_EQ) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) acc[r] = (x[r] == tm.b) ? __fadd_rn(acc[r], tm.a) : acc[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) acc[r] = __fmaf_rn(tm.a, x[r], acc[r]);
+            }
+        }
+        // warp prefix top-KF over the segment in scan order; records are the
+        // positions not below the K-th best of everything before them in the
+        // segment (a superset of the global triggers).
+        float carry[KF];
+#pragma unroll
+        for (int q = 0; q < KF; ++q) carry[q] = -CUDART_INF_F;
+        int count = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float xval = valid[r] ? acc[r] : -CUDART_INF_F;
+            float st[KF];
+            st[0] = xval;
+#pragma unroll
+            for (int q = 1; q < KF; ++q) st[q] = -CUDART_INF_F;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                float rcv[KF], mrg[KF];
+#pragma unroll
+                for (int q = 0; q < KF; ++q) rcv[q] = __shfl_up_sync(0xffffffffu, st[q], off);
+                if (lane >= off) {
+                    topk_merge<KF>(st, rcv, mrg);
+#pragma unroll
+                    for (int q = 0; q < KF; ++q) st[q] = mrg[q];
+                }
+            }
+            float ex[KF], pre[KF];
+#pragma unroll
+            for (int q = 0; q < KF; ++q) {
+                float y = __shfl_up_sync(0xffffffffu, st[q], 1);
+                ex[q] = lane == 0 ? -CUDART_INF_F : y;
+            }
+            topk_merge<KF>(carry, ex, pre);
+            const float kth = pre[KF - 1];
+            const bool rec = exists[r] && (xval >= kth) && (valid[r] || emit_masked);
+            const unsigned bal = __ballot_sync(0xffffffffu, rec);
+            if (rec) {
+                const int o = count + __popc(bal & lanemask_lt());
+                rv[base + o] = xval;
+                ri[base + o] = int(base + 32 * r + lane);
+            }
+            count += __popc(bal);
+            float last[KF], nc[KF];
+#pragma unroll
+            for (int q = 0; q < KF; ++q) last[q] = __shfl_sync(0xffffffffu, st[q], 31);
+            topk_merge<KF>(carry, last, nc);
+#pragma unroll
+            for (int q = 0; q < KF; ++q) carry[q] = nc[q];
+        }
+        if (lane == 0) A.rec_cnt[(long long)b * g.nseg + sg] = count;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mt19937 (published algorithm: Matsumoto & Nishimura 1998) with the
+// conversion of std::uniform_real_distribution<float>(0,1) in libstdc++
+// (generate_canonical<float,24>: float(u32) * 2^-32, values >= 1 clamped to
+// the largest float below 1).
+// ---------------------------------------------------------------------------
+struct WarpRng {
+    unsigned *mt;   // 624 state words (shared memory)
+    float *buf;     // up to 625 converted draws (shared memory)
+};
+
+__device__ __forceinline__ unsigned mt_temper(unsigned y) {
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+__device__ __forceinline__ float mt_unit(unsigned y) {
+    float u = __fmul_rn(__uint2float_rn(y), 2.3283064365386963e-10f);
+    return u >= 1.f ? 0x1.fffffep-1f : u;
+}
+
+__device__ __forceinline__ unsigned mt_mix(unsigned a, unsigned b, unsigned c) {
+    unsigned y = (a & 0x80000000u) | (b & 0x7fffffffu);
+    return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+}
+
+// warp-cooperative regeneration of the 624-word state (3 dependency phases)
+__device__ void mt_twist(unsigned *mt, int lane) {
+    unsigned nv[8];
+    // phase A: k in [0,227): old x[k], x[k+1], x[k+397]
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        int k = lane + 32 * q;
+        nv[q] = k < 227 ? mt_mix(mt[k], mt[k + 1], mt[k + 397]) : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        int k = lane + 32 * q;
+        if (k < 227) mt[k] = nv[q];
+    }
+    __syncwarp();
+    // phase B: k in [227,454): old x[k], x[k+1]; new x[k-227]
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        int k = 227 + lane + 32 * q;
+        nv[q] = k < 454 ? mt_mix(mt[k], mt[k + 1], mt[k - 227]) : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        int k = 227 + lane + 32 * q;
+        if (k < 454) mt[k] = nv[q];
+    }
+    __syncwarp();
+    // phase C: k in [454,623): old x[k], x[k+1]; new x[k-227]
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        int k = 454 + lane + 32 * q;
+        nv[q] = k < 623 ? mt_mix(mt[k], mt[k + 1], mt[k - 227]) : 0u;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        int k = 454 + lane + 32 * q;
+        if (k < 623) mt[k] = nv[q];
+    }
+    __syncwarp();
+    if (lane == 0) mt[623] = mt_mix(mt[623], mt[0], mt[396]);
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// replay of the k-biggest scan + draw + write-back; one warp per slot
+// ---------------------------------------------------------------------------
+#define RP_WARPS 4
+
+struct WarpShared {
+    unsigned mt[624];
+    float buf[628];
+    int len, rp;
+};
+
+__device__ __forceinline__ void rng_refill(WarpShared &w, int lane) {
+    // keep the unread draws (at most one) at the front, then append 624 new ones
+    __syncwarp();
+    int unread = w.len - w.rp;
+    float keep = unread > 0 ? w.buf[w.rp] : 0.f;
+    __syncwarp();
+    mt_twist(w.mt, lane);
+    for (int i = lane; i < 624; i += 32) w.buf[unread + i] = mt_unit(mt_temper(w.mt[i]));
+    if (lane == 0) {
+        if (unread > 0) w.buf[0] = keep;
+        w.len = unread + 624;
+        w.rp = 0;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void rng_need(WarpShared &w, int lane, int n) {
+    __syncwarp();
+    if (w.len - w.rp < n) rng_refill(w, lane);
+}
+
+__device__ void rng_skip(WarpShared &w, int lane, long long n) {
+    while (n > 0) {
+        __syncwarp();
+        long long avail = w.len - w.rp;
+        long long t = avail < n ? avail : n;
+        __syncwarp();
+        if (lane == 0) w.rp += int(t);
+        n -= t;
+        __syncwarp();
+        if (n > 0) rng_refill(w, lane);
+    }
+}
+
+__global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
+    __shared__ WarpShared wsh[RP_WARPS];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * RP_WARPS + wib;
+    if (b >= A.nslots) return;
+    WarpShared &w = wsh[wib];
+    const Slot s = A.slots[b];
+    const Geom &g = A.g;
+    const int K = A.K;
+
+    float ov[QSK_KMAX];
+    unsigned op[QSK_KMAX];
+    for (int q = 0; q < QSK_KMAX; ++q) { ov[q] = -CUDART_INF_F; op[q] = 0xffffffffu; }
+    unsigned chosen_cell = 0;
+    bool have = false;
+
+    if (s.flags & SLOT_SKIP) {
+        if (A.state || A.node_cell) {
+            // marginal draw over the TI cells (simulation.hpp:586-605; complete TI)
+            chosen_cell = unsigned(int(floor((double)__fmul_rn(s.seed, __uint2float_rn((unsigned)A.ti_cells)))));
+            // float rounding of seed*cells can reach `cells` only for grids above 2^24 cells
+            if ((long long)chosen_cell >= A.ti_cells) chosen_cell = (unsigned)(A.ti_cells - 1);
+            have = true;
+        }
+    } else {
+        // seed: generator.seed(seedFromUnitFloat(seed) + 0)
+        if (lane == 0) {
+            unsigned x;
+            float sd = s.seed;
+            if (!isfinite(sd) || sd <= 0.f) x = 0u;
+            else if (sd >= 1.f) x = 0xffffffffu;
+            else x = (unsigned)floor((double)sd * 4294967295.0);
+            w.mt[0] = x;
+            for (int i = 1; i < 624; ++i) {
+                x = 1812433253u * (x ^ (x >> 30)) + (unsigned)i;
+                w.mt[i] = x;
+            }
+            w.len = 0;
+            w.rp = 0;
+        }
+        __syncwarp();
+        unsigned cpt = 0;
+        long long last = -1;
+        const float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
+        const int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
+        const int *rc = A.rec_cnt + (long long)b * g.nseg;
+        for (int s0 = 0; s0 < g.nseg; s0 += 32) {
+            int myc = (s0 + lane < g.nseg) ? rc[s0 + lane] : 0;
+            unsigned nz = __ballot_sync(0xffffffffu, myc > 0);
+            while (nz) {
+                const int l = __ffs(nz) - 1;
+                nz &= nz - 1;
+                const int sg = s0 + l;
+                const int cnt = __shfl_sync(0xffffffffu, myc, l);
+                const long long base = (long long)sg * QSK_SEG;
+                float cv[4];
+                int ci[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    int j = lane + 32 * q;
+                    cv[q] = j < cnt ? rv[base + j] : -CUDART_INF_F;
+                    ci[q] = j < cnt ? ri[base + j] : -1;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    unsigned lanes_done = 0;
+                    for (;;) {
+                        const float thr = __shfl_sync(0xffffffffu, ov[K - 1], 0);
+                        const bool cand = (ci[q] >= 0) && (cv[q] >= thr);
+                        unsigned bal = __ballot_sync(0xffffffffu, cand) & ~lanes_done;
+                        if (!bal) break;
+                        const int src = __ffs(bal) - 1;
+                        lanes_done |= (2u << src) - 1u;
+                        const float v = __shfl_sync(0xffffffffu, cv[q], src);
+                        const long long m = __shfl_sync(0xffffffffu, ci[q], src);
+                        // masked positions between the last processed one and m are
+                        // -inf ties while fewer than K finite values have been seen
+                        if (thr == -CUDART_INF_F && !(s.flags & SLOT_EMIT_MASKED)) {
+                            long long c = (m - (last + 1)) - (valid_prefix(g, s.lo, m) - valid_prefix(g, s.lo, last + 1));
+                            if (c > 0) {
+                                rng_skip(w, lane, 2 * c);
+                                cpt += unsigned(c);
+                            }
+                        }
+                        last = m;
+                        rng_need(w, lane, 2);
+                        if (lane == 0) {
+                            // fKb.hpp:58-92 (addValueB with generator)
+                            int position = K - 2;
+                            int likeLast = K - 2;
+                            while (likeLast > -1 && ov[K - 1] == ov[likeLast]) likeLast--;
+                            int xes = K - likeLast - 1;
+                            float u1 = w.buf[w.rp++];
+                            int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
+                            if (x > K - 1) x = K - 1;   // u1 < 1 keeps x <= K-1; guard for memory safety
+                            unsigned tp = op[x];
+                            op[x] = op[K - 1];
+                            op[K - 1] = tp;
+                            if (v > ov[K - 1]) {
+                                if (xes == 1) cpt = 0;
+                                else cpt++;
+                                while (position > -1 && v > ov[position]) {
+                                    ov[position + 1] = ov[position];
+                                    op[position + 1] = op[position];
+                                    position--;
+                                }
+                                ov[position + 1] = v;
+                                op[position + 1] = unsigned(m);
+                            } else {
+                                cpt++;
+                                float u2 = w.buf[w.rp++];
+                                if (__fmul_rn(__uint2float_rn(unsigned(xes) + cpt), u2) < (float)xes)
+                                    op[position + 1] = unsigned(m);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+            }
+        }
+        if (lane == 0) {
+            // merge loop (quantileSamplingModule.hpp:546-557): repeated first-max extraction
+            float fv[QSK_KMAX];
+            unsigned fp[QSK_KMAX];
+            for (int j = 0; j < K; ++j) {
+                int best = 0;
+                for (int l2 = 1; l2 < K; ++l2)
+                    if (ov[l2] > ov[best]) best = l2;
+                fv[j] = ov[best];
+                fp[j] = op[best];
+                ov[best] = -CUDART_INF_F;
+            }
+            // sample(): std::sort by score (stable insertion sort for K <= 16)
+            for (int a = 1; a < K; ++a) {
+                float kv = fv[a];
+                unsigned kp = fp[a];
+                int c = a - 1;
+                while (c >= 0 && kv > fv[c]) {
+                    fv[c + 1] = fv[c];
+                    fp[c + 1] = fp[c];
+                    c--;
+                }
+                fv[c + 1] = kv;
+                fp[c + 1] = kp;
+            }
+            if (A.out_val) {
+                for (int j = 0; j < K; ++j) {
+                    A.out_val[(long long)b * K + j] = fv[j];
+                    A.out_pos[(long long)b * K + j] = fp[j];
+                }
+            }
+            if (A.state || A.node_cell) {
+                // cvtIndexToPosition (CPUThreadDevice.cpp:257-268), unsigned arithmetic
+                unsigned index = fp[s.sel];
+                unsigned position = 0;
+                unsigned div = (unsigned)g.N;
+                for (int d = g.nd - 1; d >= 0; --d) {
+                    unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
+                    div /= f;
+                    position = position * sr + ((f - (index / div) % f - (unsigned)s.mn[d] - 1u) + sr) % sr;
+                }
+                chosen_cell = position;
+                have = true;
+            }
+        }
+    }
+    if (lane == 0 && have) {
+        if (A.node_cell) A.node_cell[s.node] = chosen_cell;
+        if (A.state) {
+            for (int v = 0; v < A.nvar; ++v) {
+                float *dst = A.state + (long long)s.cell * A.nvar + v;
+                if (isnan(*dst)) *dst = A.ti[(long long)chosen_cell * A.nvar + v];
+            }
+        }
+        if (A.id_image) A.id_image[s.cell] = chosen_cell * A.nti + A.ti_id;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers (called by the host engine)
+// ---------------------------------------------------------------------------
+cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers,
+                                cudaStream_t st) {
+    long long blocks = (g.N + 255) / 256;
+    k_build_layers<<<(unsigned)blocks, 256, 0, st>>>(ti, nvar, types, g, layers);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
+                              long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
+                              unsigned *nb_cell, cudaStream_t st) {
+    if (nodes <= 0) return cudaSuccess;
+    k_neighbours<<<(unsigned)((nodes + 127) / 128), 128, 0, st>>>(dg, tpl, ntpl, path, begin, nodes, posterior, n,
+                                                                  nb_count, nb_tpl, nb_cell);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
+                          const int *node_of_cell, int *level, int *max_level, cudaStream_t st) {
+    if (nodes <= 0) return cudaSuccess;
+    k_levels<<<1, 1024, 0, st>>>(nodes, n, nb_count, nb_cell, node_of_cell, level, max_level);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level_sort(long long nodes, int nl, const int *level, int *hist, int *start, int *cursor,
+                              int *level_nodes, cudaStream_t st) {
+    unsigned blocks = (unsigned)((nodes + 255) / 256);
+    k_level_hist<<<blocks, 256, 0, st>>>(nodes, level, hist);
+    k_level_scan<<<1, 32, 0, st>>>(nl, hist, start, cursor);
+    k_level_scatter<<<blocks, 256, 0, st>>>(nodes, level, cursor, level_nodes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st) {
+    int threads = 256;
+    long long blocks = ((long long)a.nslots * 32 + threads - 1) / threads;
+    k_prep_sim<<<(unsigned)blocks, threads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+int map_segs_per_cta(const Geom &g, int nslots) {
+    // enough CTAs to fill the GPU several times over, at most 32 segments each
+    long long target = 148LL * 8;
+    long long per = ((long long)g.nseg * nslots + target - 1) / target;
+    if (per < 8) per = 8;
+    if (per > 32) per = 32;
+    return (int)per;
+}
+
+cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st) {
+    int threads = 256;
+    dim3 grid((unsigned)((a.g.nseg + a.segs_per_cta - 1) / a.segs_per_cta), (unsigned)nslots);
+    size_t smem = sizeof(Term) * (size_t)(maxterms_in_batch > 0 ? maxterms_in_batch : 1);
+    if (K <= 1) k_map_records<1><<<grid, threads, smem, st>>>(a);
+    else if (K <= 2) k_map_records<2><<<grid, threads, smem, st>>>(a);
+    else if (K <= 4) k_map_records<4><<<grid, threads, smem, st>>>(a);
+    else if (K <= 8) k_map_records<8><<<grid, threads, smem, st>>>(a);
+    else k_map_records<16><<<grid, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t set_map_smem_limit(int bytes) {
+    cudaError_t e = cudaSuccess;
+    e = cudaFuncSetAttribute(k_map_records<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_map_records<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_map_records<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_map_records<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_map_records<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
+    unsigned blocks = (unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS);
+    k_replay<<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace qsk

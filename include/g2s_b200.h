@@ -1,0 +1,188 @@
+/*
+ * g2s_b200 — B200-native QuickSampling (QS) hot path behind a C ABI.
+ *
+ * Plain C: POD arguments, host pointers, int status codes; no C++ or torch
+ * types cross this boundary.  Shared library: libg2s_b200.so (sm_100a).
+ *
+ * Every entry point names the G2S interface it replaces.  G2S binds its
+ * accelerator device by dlopen("./g2s_cuda.so") and two symbols
+ * (src/qs.cpp:861-911); the drop-in g2s_cuda.so of this project (see
+ * INTEGRATION.md) implements that AcceleratorDevice on top of the functions
+ * below.
+ *
+ * Threading: a qsk_ti is immutable after creation and may be shared; a
+ * qsk_worker or qsk_sim must be used by one host thread at a time.
+ */
+#ifndef G2S_B200_H
+#define G2S_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (G2S has none: CUDA errors call exit(), .cu:45-54) */
+#define QSK_OK 0
+#define QSK_ERR_ARG 1          /* invalid argument / unsupported size */
+#define QSK_ERR_CUDA 2         /* CUDA runtime error (message in qsk_last_error) */
+#define QSK_ERR_NOMEM 3        /* device allocation failed */
+#define QSK_ERR_UNSUPPORTED 4  /* feature outside the implemented path */
+#define QSK_ERR_DEVICE 5       /* a kernel reported an inconsistent input */
+
+/* term operations of a pattern: x = layer value at the neighbour's position */
+#define QSK_OP_LIN 0           /* acc = fma(a, x, acc) */
+#define QSK_OP_SQLIN 1         /* acc = fma(a, x*x, acc); acc = fma(b, x, acc) */
+#define QSK_OP_EQ 2            /* acc = (x == b) ? acc + a : acc */
+
+/* Last error message of the calling thread ("" when none). */
+const char *qsk_last_error(void);
+
+/* Number of usable CUDA devices.
+ * Replaces g2s_cudaGetDeviceCount (G2S src/NvidiaGPUAcceleratorDevice.cu:26-30,
+ * resolved by src/qs.cpp:876). */
+int qsk_device_count(int *count);
+
+/* ------------------------------------------------------------------------
+ * Training image on one GPU (the per-device shared memory of G2S'
+ * SharedMemoryManager + AcceleratorDevice::allocAndInitSharedMemory).
+ * ---------------------------------------------------------------------- */
+typedef struct qsk_ti qsk_ti;
+
+/* Upload nlayers correlation layers, each prod(fft_size) floats in the
+ * reference's flipped layout (DataImage::convertInput4Xcorr).
+ * Replaces NvidiaGPUAcceleratorDevice::allocAndInitSharedMemory
+ * (G2S src/NvidiaGPUAcceleratorDevice.cu:350-390, interface
+ * include/AcceleratorDevice.hpp:46). */
+int qsk_ti_create_layers(int device, int ndim, const unsigned *src_size, const unsigned *fft_size, int nlayers,
+                         const float *const *layers, qsk_ti **out);
+
+/* Upload a raw training image (x fastest, nvar interleaved variables,
+ * types[v] 0 continuous / 1 categorical) and build its layers on the GPU:
+ * one layer per variable (value, NaN->0, for continuous; category code for
+ * categorical).  Replaces DataImage::convertInput4Xcorr + SharedMemoryManager
+ * (G2S include/DataImage.hpp:538-599, src/sharedMemoryManager.cpp:26-58). */
+int qsk_ti_create_grid(int device, int ndim, const unsigned *dims, int nvar, const int *types, const float *data,
+                       qsk_ti **out);
+
+/* Scan (fft) size of a TI context: writes ndim values. */
+int qsk_ti_fft_size(const qsk_ti *ti, unsigned *fft_size);
+
+/* Releases the device copy. Replaces freeSharedMemory (.cu:392-404). */
+int qsk_ti_destroy(qsk_ti *ti);
+
+/* ------------------------------------------------------------------------
+ * Per-thread worker: stream + scratch for pattern queries (one per G2S path
+ * thread, like one NvidiaGPUAcceleratorDevice per thread, src/qs.cpp:1577-1588).
+ * ---------------------------------------------------------------------- */
+typedef struct qsk_worker qsk_worker;
+int qsk_worker_create(qsk_ti *ti, qsk_worker **out);
+int qsk_worker_destroy(qsk_worker *w);
+
+/* One term of a pattern: op applied to layer[layer] at the position of
+ * neighbour `neighbour`, coefficients a, b (see QSK_OP_*). */
+typedef struct {
+    int neighbour;
+    int layer;
+    int op;
+    float a;
+    float b;
+} qsk_term;
+
+/* Mismatch map of one pattern against every TI position (terms summed in
+ * the given order in FP32 with fused multiply-adds), positions whose template
+ * leaves the TI set to -inf, then the k best positions with the reference's
+ * reservoir tie-breaking seeded from `seed`.  Outputs: out_score[k] (map
+ * values S, descending), out_index[k] (scan index in the reference's flipped
+ * space, i.e. its "encodedPosition"), out_min[ndim] (pattern min offset,
+ * needed by cvtIndexToPosition).
+ * Replaces AcceleratorDevice::candidateForPattern + searchKBiggest
+ * (G2S src/AcceleratorDevice.cpp:92-136, include/AcceleratorDevice.hpp:45,68,
+ * src/NvidiaGPUAcceleratorDevice.cu:462-614,688-727), with the k-biggest
+ * semantics of the CPU path (include/fKb.hpp:58-132,907-954,
+ * include/quantileSamplingModule.hpp:525-557). */
+int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
+                      unsigned k, float seed, float *out_score, unsigned *out_index, int *out_min);
+
+/* Batched form: B patterns in CSR form (nb_ptr[B+1] into offsets rows,
+ * term_ptr[B+1] into terms; term.neighbour is relative to its pattern).
+ * Outputs are B*k scores/indices and B*ndim minima. */
+int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                            const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
+                            unsigned *out_index, int *out_min);
+
+/* Reference scan index -> TI cell (CPUThreadDevice::cvtIndexToPosition,
+ * G2S src/CPUThreadDevice.cpp:257-268). */
+unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index);
+/* TI cell -> reference scan index (cvtPositionToIndex, :270-284). */
+unsigned qsk_position_to_index(const qsk_ti *ti, const int *min_offset, unsigned position);
+
+/* ------------------------------------------------------------------------
+ * Whole vector QS simulation on the GPU: the per-node loop of G2S
+ * simulation() (include/simulation.hpp:43-710) with QuantileSamplingModule
+ * (include/quantileSamplingModule.hpp:90-126,342-577), driven by the path,
+ * seeds and search template of g2sQsProgramMain (src/qs.cpp:975-1258,
+ * 1604-1641).  Nodes whose neighbourhoods do not depend on each other run
+ * together; results equal the sequential order.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int ndim;
+    const unsigned *ti_dims;      /* x first */
+    int nvar;
+    const int *types;             /* nvar entries: 0 continuous, 1 categorical */
+    const float *ti;              /* prod(ti_dims) * nvar */
+    const unsigned *di_dims;      /* simulation grid, x first */
+    const unsigned *kernel_dims;  /* NULL: uniform kernel of size min(TI/2+1) (src/qs.cpp:1010-1042) */
+    const float *kernel;          /* prod(kernel_dims) * nvar weights, or NULL */
+    int n;                        /* -n */
+    float k;                      /* -k */
+    unsigned seed;                /* -s */
+} qsk_qs_params;
+
+typedef struct {
+    long long nodes;              /* path nodes simulated */
+    int levels;                   /* dependency levels (batches) */
+    int max_batch;                /* largest level */
+    int template_size;
+    float ms_setup_neighbours;    /* device time of the neighbour search */
+    float ms_levels;              /* device time of the level computation */
+    float ms_batches;             /* device time of all batches */
+} qsk_sim_info;
+
+typedef struct qsk_sim qsk_sim;
+
+/* Host setup (template, path, seeds as src/qs.cpp does) and uploads.
+ * di_init: prod(di_dims)*nvar values, NaN = to simulate. */
+int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk_sim **out);
+/* Simulate on the GPU (device-resident data only; resets the grid first). */
+int qsk_sim_run(qsk_sim *s);
+/* Teacher-forced evaluation: draw every path node against the completed
+ * grid (host array), as the sequential run would at that node's turn. */
+int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed);
+/* Copy results to the host: the grid, the index image (TI cell * nTI + TI,
+ * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL). */
+int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out);
+int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info);
+/* Path (cell order), per-path-index seeds and number of informed cells. */
+int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
+int qsk_sim_destroy(qsk_sim *s);
+
+/* Host-only planning helpers (no GPU needed), identical to what
+ * qsk_sim_create computes.
+ * Sorted search template of a kernel: offsets (nd ints each, nearest first,
+ * G2S src/qs.cpp:1055-1135) and the kernel weight of every offset/variable
+ * (quantileSamplingModule.hpp:362-392); kernel NULL = uniform.  Writes at
+ * most `capacity` offsets and returns the template size (<0: error). */
+int qsk_qs_template(int ndim, int nvar, const unsigned *kernel_dims, const float *kernel, int *offsets, float *weights,
+                    int capacity);
+/* Random path (cell order, informed cells first) and per-path-index seeds
+ * for grid di_init (NaN = unknown), G2S src/qs.cpp:975,1159-1201,1250-1258.
+ * Returns the number of informed cells (<0: error). */
+long long qsk_qs_path(long long cells, int nvar, const float *di_init, unsigned seed, unsigned *order, float *seeds);
+
+/* One call: setup, simulate, read back into di_inout / id_out (host). */
+int qsk_simulate(int device, const qsk_qs_params *p, float *di_inout, unsigned *id_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G2S_B200_H */

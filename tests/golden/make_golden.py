@@ -1,0 +1,67 @@
+"""Generate the golden fixtures of tests/golden/ from the G2S reference.
+
+Runs the reference CPU QuickSampling (compiled from the G2S sources by
+oracle/Makefile, FFTW replaced by the project FFT shim) on seeded synthetic
+inputs and stores inputs + outputs (simulation grid, index image and the
+reference's own reported compute time).  Needs oracle/_ref/libg2sref.so,
+which is built only where the G2S sources are present:
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ref  # noqa: E402
+from g2s_b200 import synthetic as syn  # noqa: E402
+
+CASES = {
+    # name: (ti builder, di shape, types, k, n, seed)
+    "grf2d_small": (lambda: syn.grf((64, 64), (8, 8), seed=1), (40, 40), [0], 1.2, 20, 100),
+    "cat2d_small": (lambda: syn.channels2d((80, 80), n_channels=6, seed=3), (40, 40), [1], 1.5, 20, 100),
+    "bivar2d_small": (lambda: syn.bivariate(syn.grf((64, 64), (8, 8), seed=2), 0.7), (32, 32, 2), [0, 1], 1.2, 16, 7),
+    "grf3d_small": (lambda: syn.grf((16, 20, 24), (5, 6, 6), seed=4), (8, 12, 12), [0], 1.2, 12, 11),
+    "grf2d_k3": (lambda: syn.grf((48, 48), (6, 6), seed=5), (30, 30), [0], 3.0, 12, 3),
+    # configuration 0: 200x200 GRF (range 12), unconditional 200x200, n=50, k=1.2, seed 100
+    "config0": (lambda: syn.grf((200, 200), (12, 12), seed=1), (200, 200), [0], 1.2, 50, 100),
+}
+
+
+def main(names=None):
+    for name, (mk, dshape, types, k, n, seed) in CASES.items():
+        if names and name not in names:
+            continue
+        ti = mk()
+        di = np.full(dshape, np.nan, np.float32)
+        sim, idx, ms, _ = ref.run_qs(ti, di, types, ["-k", str(k), "-n", str(n), "-s", str(seed), "-j", "1"])
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k, n=n,
+                            seed=seed, sim=sim, idx=idx, ref_ms=ms)
+        print(name, ti.shape, dshape, "ref ms", ms)
+
+
+
+
+def oracle_teacher_config0():
+    """Teacher-forced oracle evaluation of every config-0 path node against the
+    reference's completed grid: chosen TI cell and FP64 near-tie flag."""
+    from oracle import qs_oracle as qo
+    g = np.load(os.path.join(HERE, "config0.npz"))
+    di = g["di"]
+    tf = qo.simulate(g["ti"], g["sim"], [0], int(g["n"]), float(g["k"]), int(g["seed"]), mode=1, want_fp64=True,
+                     di_init=di)
+    np.savez_compressed(os.path.join(HERE, "config0_oracle_tf.npz"), cell=tf["cell"], near_tie=tf["near_tie"],
+                        gap=tf["gap"].astype(np.float32))
+    print("config0 oracle teacher-forced: near-ties", int(tf["near_tie"].sum()))
+
+
+if __name__ == "__main__":
+    args = sys.argv[1:]
+    if args == ["teacher"]:
+        oracle_teacher_config0()
+    else:
+        main(args)
