@@ -43,7 +43,9 @@ class QskParams(ctypes.Structure):
 class QskSimInfo(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_longlong), ("levels", ctypes.c_int), ("max_batch", ctypes.c_int),
                 ("template_size", ctypes.c_int), ("ms_setup_neighbours", ctypes.c_float),
-                ("ms_levels", ctypes.c_float), ("ms_batches", ctypes.c_float)]
+                ("ms_levels", ctypes.c_float), ("ms_batches", ctypes.c_float), ("ms_total", ctypes.c_float),
+                ("launches", ctypes.c_longlong), ("map_launches", ctypes.c_longlong), ("ms_map", ctypes.c_float),
+                ("ms_prep", ctypes.c_float), ("ms_replay", ctypes.c_float), ("map_positions", ctypes.c_longlong)]
 
 
 # name -> (restype, argtypes): every entry point of include/g2s_b200.h
@@ -72,6 +74,7 @@ SIGNATURES = {
     "qsk_sim_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskSimInfo)]),
     "qsk_sim_get_path": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f32p, _u32p]),
     "qsk_sim_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_sim_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
     "qsk_qs_path": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p]),
@@ -254,6 +257,10 @@ class Simulation:
 
     def run(self):
         _check(lib().qsk_sim_run(self.handle), "qsk_sim_run")
+        return self
+
+    def set_profiling(self, on: bool = True):
+        _check(lib().qsk_sim_set_profiling(self.handle, int(on)), "qsk_sim_set_profiling")
         return self
 
     def run_teacher(self, completed: np.ndarray):

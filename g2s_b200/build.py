@@ -54,5 +54,27 @@ def build_lib(force: bool = False) -> str:
     return LIB
 
 
+DROPIN = os.path.join(PKG, "dropin")
+
+
+def build_dropin(g2s_tree: str = "/root/reference") -> str:
+    """g2s_cuda.so for G2S `qs -W_CUDA`: compiled with the G2S host compiler
+    against the G2S headers (its AcceleratorDevice class), linked to
+    libg2s_b200.so found next to it ($ORIGIN/..)."""
+    build_lib()
+    out = os.path.join(DROPIN, "g2s_cuda.so")
+    inc = os.path.join(g2s_tree, "include")
+    if not os.path.isdir(inc):
+        raise FileNotFoundError(f"G2S headers not found under {inc}")
+    _run([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-w", "-DG2S_PATH_INDEX_TYPE=unsigned",
+          "-I", inc, "-I", os.path.join(ROOT, "oracle", "fftw_shim"), "-I", os.path.join(ROOT, "oracle", "json_stub"),
+          "-I", os.path.join(ROOT, "include"), os.path.join(DROPIN, "g2s_cuda_device.cpp"), "-o", out,
+          "-L", PKG, "-lg2s_b200", "-Wl,-rpath,$ORIGIN/..:$ORIGIN"])
+    return out
+
+
 if __name__ == "__main__":
-    build_lib(force="--force" in sys.argv)
+    if "dropin" in sys.argv:
+        build_dropin(*[a for a in sys.argv[1:] if a.startswith("/")])
+    else:
+        build_lib(force="--force" in sys.argv)

@@ -150,6 +150,7 @@ struct qsk_worker {
     DBuf<float> rec_val;
     DBuf<int> rec_idx;
     DBuf<int> rec_cnt;
+    DBuf<float> rec_max;
     DBuf<float> out_val;
     DBuf<unsigned> out_pos;
     std::vector<Slot> h_slots;
@@ -160,11 +161,14 @@ namespace {
 
 int smem_configured_device = -1;
 
-cudaError_t ensure_records(const Geom &g, int nslots, DBuf<float> &rv, DBuf<int> &ri, DBuf<int> &rc) {
+cudaError_t ensure_records(const Geom &g, int nslots, DBuf<float> &rv, DBuf<int> &ri, DBuf<int> &rc,
+                           DBuf<float> &rm) {
     size_t per = size_t(g.nseg) * QSK_SEG;
     cudaError_t e = rv.ensure(per * nslots);
     if (e != cudaSuccess) return e;
     e = ri.ensure(per * nslots);
+    if (e != cudaSuccess) return e;
+    e = rm.ensure(size_t(g.nseg) * nslots);
     if (e != cudaSuccess) return e;
     return rc.ensure(size_t(g.nseg) * nslots);
 }
@@ -383,7 +387,7 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     if ((size_t)maxterms * sizeof(Term) > 200 * 1024) return fail(QSK_ERR_UNSUPPORTED, "too many terms (%d)", maxterms);
     CK(w->slots.upload(w->h_slots.data(), B, w->st));
     CK(w->terms.upload(w->h_terms.data(), w->h_terms.size(), w->st));
-    CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt));
+    CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt, w->rec_max));
     CK(w->out_val.ensure(size_t(B) * k));
     CK(w->out_pos.ensure(size_t(B) * k));
     MapArgs ma;
@@ -396,6 +400,7 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     ma.rec_val = w->rec_val.p;
     ma.rec_idx = w->rec_idx.p;
     ma.rec_cnt = w->rec_cnt.p;
+    ma.rec_max = w->rec_max.p;
     CK(launch_map_records(ma, B, int(k), maxterms, w->st));
     ReplayArgs ra;
     std::memset(&ra, 0, sizeof(ra));
@@ -406,6 +411,7 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     ra.rec_val = w->rec_val.p;
     ra.rec_idx = w->rec_idx.p;
     ra.rec_cnt = w->rec_cnt.p;
+    ra.rec_max = w->rec_max.p;
     ra.out_val = w->out_val.p;
     ra.out_pos = w->out_pos.p;
     CK(launch_replay(ra, w->st));
@@ -488,10 +494,14 @@ struct qsk_sim {
     DBuf<Term> d_terms;
     DBuf<float> d_rec_val;
     DBuf<int> d_rec_idx, d_rec_cnt;
+    DBuf<float> d_rec_max;
     int maxterms = 0;
     int max_slots = 0;
     qsk_sim_info info;
     bool neighbours_ready = false;
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev;   // 4 events per batch in profiling mode
+    size_t prof_used = 0;
 };
 
 namespace {
@@ -619,8 +629,18 @@ int sim_neighbours(qsk_sim *s) {
 }
 
 // run the batches of nodes listed in d_level_nodes[start[l]..start[l+1]) for each level
+cudaEvent_t prof_event(qsk_sim *s) {
+    if (s->prof_used == s->prof_ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->prof_ev.push_back(e);
+    }
+    return s->prof_ev[s->prof_used++];
+}
+
 int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     const Geom &g = s->ti->g;
+    s->prof_used = 0;
     for (size_t l = 0; l + 1 < start.size(); ++l) {
         int a = start[l], e = start[l + 1];
         for (int off = a; off < e; off += s->max_slots) {
@@ -650,7 +670,9 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             pa.terms = s->d_terms.p;
             pa.maxterms = s->maxterms;
             pa.status = s->d_status.p;
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             MapArgs ma;
             ma.g = g;
             ma.layers = s->ti->layers.p;
@@ -661,7 +683,12 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ma.rec_val = s->d_rec_val.p;
             ma.rec_idx = s->d_rec_idx.p;
             ma.rec_cnt = s->d_rec_cnt.p;
+            ma.rec_max = s->d_rec_max.p;
             CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
+            s->info.launches += 3;
+            s->info.map_launches += 1;
+            s->info.map_positions += (long long)B * g.N;
             ReplayArgs ra;
             std::memset(&ra, 0, sizeof(ra));
             ra.g = g;
@@ -671,6 +698,7 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.rec_val = s->d_rec_val.p;
             ra.rec_idx = s->d_rec_idx.p;
             ra.rec_cnt = s->d_rec_cnt.p;
+            ra.rec_max = s->d_rec_max.p;
             ra.nvar = s->nvar;
             ra.ti = s->ti->grid.p;
             ra.ti_cells = s->ti->cells;
@@ -680,9 +708,28 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.id_image = teacher ? nullptr : s->d_id.p;
             ra.node_cell = s->d_node_cell.p;
             CK(launch_replay(ra, s->st));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         }
     }
     return QSK_OK;
+}
+
+void collect_profile(qsk_sim *s) {
+    if (!s->profiling || s->prof_used == 0) return;
+    cudaEventSynchronize(s->prof_ev[s->prof_used - 1]);
+    float prep = 0, map = 0, rep = 0;
+    for (size_t i = 0; i + 3 < s->prof_used; i += 4) {
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, s->prof_ev[i], s->prof_ev[i + 1]);
+        cudaEventElapsedTime(&b, s->prof_ev[i + 1], s->prof_ev[i + 2]);
+        cudaEventElapsedTime(&c, s->prof_ev[i + 2], s->prof_ev[i + 3]);
+        prep += a;
+        map += b;
+        rep += c;
+    }
+    s->info.ms_prep = prep;
+    s->info.ms_map = map;
+    s->info.ms_replay = rep;
 }
 
 int sim_check_status(qsk_sim *s) {
@@ -767,7 +814,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
                          cudaGetErrorString(e)));
     // batch scratch: slots up to a record budget of ~2 GiB
     const Geom &g = s->ti->g;
-    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 4 + sizeof(Term) * s->maxterms;
+    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 8 + sizeof(Term) * s->maxterms;
     size_t budget = size_t(2) << 30;
     long long ms = (long long)(budget / per_slot);
     ms = std::max<long long>(1, std::min<long long>(ms, std::max<long long>(s->nodes, 1)));
@@ -775,7 +822,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     s->max_slots = int(ms);
     if ((e = s->d_slots.alloc(size_t(s->max_slots))) != cudaSuccess ||
         (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess ||
-        (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt)) != cudaSuccess)
+        (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "scratch: %s",
                          cudaGetErrorString(e)));
     if ((size_t)s->maxterms * sizeof(Term) > 200 * 1024) return bail(fail(QSK_ERR_UNSUPPORTED, "n*nvar too large"));
@@ -798,6 +845,9 @@ int qsk_sim_run(qsk_sim *s) {
     CK(cudaMemcpyAsync(s->d_state.p, s->d_init.p, sizeof(float) * s->init.size(), cudaMemcpyDeviceToDevice, s->st));
     CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells, s->st));
     CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
+    s->info.launches = 0;
+    s->info.map_launches = 0;
+    s->info.map_positions = 0;
     CK(cudaEventRecord(ev[0], s->st));
     s->neighbours_ready = false;
     int rc = sim_neighbours(s);
@@ -806,6 +856,7 @@ int qsk_sim_run(qsk_sim *s) {
     CK(cudaMemsetAsync(s->d_maxlevel.p, 0, sizeof(int), s->st));
     CK(launch_levels(s->nodes, s->n, s->d_nb_count.p, s->d_nb_cell.p, s->d_node_of_cell.p, s->d_level.p,
                      s->d_maxlevel.p, s->st));
+    s->info.launches += 2;  // neighbours + levels
     int maxl = 0;
     CK(cudaMemcpyAsync(&maxl, s->d_maxlevel.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -818,6 +869,7 @@ int qsk_sim_run(qsk_sim *s) {
         CK(cudaMemsetAsync(s->d_hist.p, 0, sizeof(int) * nl, s->st));
         CK(launch_level_sort(s->nodes, nl, s->d_level.p, s->d_hist.p, s->d_start.p, s->d_cursor.p, s->d_level_nodes.p,
                              s->st));
+        s->info.launches += 3;
         CK(cudaMemcpyAsync(start.data(), s->d_start.p, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
     }
@@ -833,7 +885,9 @@ int qsk_sim_run(qsk_sim *s) {
     cudaEventElapsedTime(&s->info.ms_setup_neighbours, ev[0], ev[1]);
     cudaEventElapsedTime(&s->info.ms_levels, ev[1], ev[2]);
     cudaEventElapsedTime(&s->info.ms_batches, ev[2], ev[3]);
+    cudaEventElapsedTime(&s->info.ms_total, ev[0], ev[3]);
     for (auto &x : ev) cudaEventDestroy(x);
+    collect_profile(s);
     return sim_check_status(s);
 }
 
@@ -881,10 +935,17 @@ int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *
     return QSK_OK;
 }
 
+int qsk_sim_set_profiling(qsk_sim *s, int on) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    s->profiling = on != 0;
+    return QSK_OK;
+}
+
 int qsk_sim_destroy(qsk_sim *s) {
     if (!s) return QSK_OK;
     {
         DeviceGuard dgd(s->device);
+        for (auto e : s->prof_ev) cudaEventDestroy(e);
         if (s->st) cudaStreamDestroy(s->st);
         s->st = nullptr;
         if (s->ti) qsk_ti_destroy(s->ti);

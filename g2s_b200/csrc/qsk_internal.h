@@ -105,6 +105,7 @@ struct MapArgs {
     float *rec_val;   // [slot][nseg*SEG]
     int *rec_idx;
     int *rec_cnt;     // [slot][nseg]
+    float *rec_max;   // [slot][nseg] largest valid score of the segment
 };
 
 struct ReplayArgs {
@@ -115,6 +116,7 @@ struct ReplayArgs {
     const float *rec_val;
     const int *rec_idx;
     const int *rec_cnt;
+    const float *rec_max;
     // pattern outputs (may be null)
     float *out_val;       // [slot][K]
     unsigned *out_pos;    // [slot][K]

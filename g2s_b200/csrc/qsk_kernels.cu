@@ -406,9 +406,11 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
 #pragma unroll
         for (int q = 0; q < KF; ++q) carry[q] = -CUDART_INF_F;
         int count = 0;
+        float segmax = -CUDART_INF_F;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const float xval = valid[r] ? acc[r] : -CUDART_INF_F;
+            segmax = fmaxf(segmax, xval);
             float st[KF];
             st[0] = xval;
 #pragma unroll
@@ -447,7 +449,12 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
 #pragma unroll
             for (int q = 0; q < KF; ++q) carry[q] = nc[q];
         }
-        if (lane == 0) A.rec_cnt[(long long)b * g.nseg + sg] = count;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) segmax = fmaxf(segmax, __shfl_xor_sync(0xffffffffu, segmax, off));
+        if (lane == 0) {
+            A.rec_cnt[(long long)b * g.nseg + sg] = count;
+            A.rec_max[(long long)b * g.nseg + sg] = segmax;
+        }
     }
 }
 
@@ -457,11 +464,6 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
 // (generate_canonical<float,24>: float(u32) * 2^-32, values >= 1 clamped to
 // the largest float below 1).
 // ---------------------------------------------------------------------------
-struct WarpRng {
-    unsigned *mt;   // 624 state words (shared memory)
-    float *buf;     // up to 625 converted draws (shared memory)
-};
-
 __device__ __forceinline__ unsigned mt_temper(unsigned y) {
     y ^= y >> 11;
     y ^= (y << 7) & 0x9d2c5680u;
@@ -530,47 +532,201 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 // replay of the k-biggest scan + draw + write-back; one warp per slot
 // ---------------------------------------------------------------------------
 #define RP_WARPS 4
+#define RNG_BUF 704   // 624 fresh draws + up to 63 unread ones kept across a refill
 
 struct WarpShared {
     unsigned mt[624];
-    float buf[628];
-    int len, rp;
+    float buf[RNG_BUF];
 };
 
-__device__ __forceinline__ void rng_refill(WarpShared &w, int lane) {
-    // keep the unread draws (at most one) at the front, then append 624 new ones
+// Draw buffer with warp-replicated read pointer: rp/len live in registers of
+// every lane (all lanes execute the same control flow).
+__device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int &len) {
+    const int unread = len - rp;   // < 64 by construction, and rp > unread when len >= 624
     __syncwarp();
-    int unread = w.len - w.rp;
-    float keep = unread > 0 ? w.buf[w.rp] : 0.f;
+    float keep0 = 0.f, keep1 = 0.f;
+    if (lane < unread) keep0 = w.buf[rp + lane];
+    if (lane + 32 < unread) keep1 = w.buf[rp + lane + 32];
     __syncwarp();
     mt_twist(w.mt, lane);
     for (int i = lane; i < 624; i += 32) w.buf[unread + i] = mt_unit(mt_temper(w.mt[i]));
-    if (lane == 0) {
-        if (unread > 0) w.buf[0] = keep;
-        w.len = unread + 624;
-        w.rp = 0;
-    }
+    if (lane < unread) w.buf[lane] = keep0;
+    if (lane + 32 < unread) w.buf[lane + 32] = keep1;
     __syncwarp();
+    len = unread + 624;
+    rp = 0;
 }
 
-__device__ __forceinline__ void rng_need(WarpShared &w, int lane, int n) {
-    __syncwarp();
-    if (w.len - w.rp < n) rng_refill(w, lane);
+__device__ __forceinline__ void rng_ensure(WarpShared &w, int lane, int &rp, int &len, int need) {
+    if (len - rp < need) rng_refill(w, lane, rp, len);
 }
 
-__device__ void rng_skip(WarpShared &w, int lane, long long n) {
+__device__ void rng_skip(WarpShared &w, int lane, int &rp, int &len, long long n) {
     while (n > 0) {
-        __syncwarp();
-        long long avail = w.len - w.rp;
+        long long avail = len - rp;
         long long t = avail < n ? avail : n;
-        __syncwarp();
-        if (lane == 0) w.rp += int(t);
+        rp += int(t);
         n -= t;
-        __syncwarp();
-        if (n > 0) rng_refill(w, lane);
+        if (n > 0) rng_refill(w, lane, rp, len);
     }
 }
 
+template <int KM>
+__device__ __forceinline__ float sel_f(const float (&a)[KM], int i) {
+    float r = a[0];
+#pragma unroll
+    for (int s = 1; s < KM; ++s) r = (s == i) ? a[s] : r;
+    return r;
+}
+template <int KM>
+__device__ __forceinline__ int sel_i(const int (&a)[KM], int i) {
+    int r = a[0];
+#pragma unroll
+    for (int s = 1; s < KM; ++s) r = (s == i) ? a[s] : r;
+    return r;
+}
+template <int KM>
+__device__ __forceinline__ unsigned sel_u(const unsigned (&a)[KM], int i) {
+    unsigned r = a[0];
+#pragma unroll
+    for (int s = 1; s < KM; ++s) r = (s == i) ? a[s] : r;
+    return r;
+}
+
+// One step of the reference's k-biggest scan for up to 32 consecutive
+// candidates at once (one per lane, lanes in scan order).  The value state is
+// a prefix top-K (associative merge), the tie counter cpt a composition of
+// "add" / "reset" functions, the draws a prefix count, and the position
+// updates of each trigger (swap of the tail slot, insertion, reservoir
+// replacement) slot maps whose composition is reduced across the warp.
+// State (cv, cp, cpt, rp) is replicated in all lanes.
+template <int KM>
+__device__ __forceinline__ void replay_chunk(int K, bool valid, float v, int m, float (&cv)[KM], unsigned (&cp)[KM],
+                                             unsigned &cpt, int &rp, const float *buf, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    // 1. exclusive prefix top-K of the chunk's values, merged with the state
+    float st[KM];
+    st[0] = valid ? v : -CUDART_INF_F;
+#pragma unroll
+    for (int s = 1; s < KM; ++s) st[s] = -CUDART_INF_F;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        float rcv[KM], mrg[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) rcv[s] = __shfl_up_sync(FULL, st[s], off);
+        if (lane >= off) {
+            topk_merge<KM>(st, rcv, mrg);
+#pragma unroll
+            for (int s = 0; s < KM; ++s) st[s] = mrg[s];
+        }
+    }
+    float ex[KM], pre[KM];
+#pragma unroll
+    for (int s = 0; s < KM; ++s) {
+        float y = __shfl_up_sync(FULL, st[s], 1);
+        ex[s] = lane == 0 ? -CUDART_INF_F : y;
+    }
+    topk_merge<KM>(cv, ex, pre);
+    const float kth = sel_f<KM>(pre, K - 1);
+    const bool trig = valid && (v >= kth);
+    const bool gt = trig && (v > kth);
+    int xes = 0, q = 0;
+#pragma unroll
+    for (int s = 0; s < KM; ++s) {
+        if (s < K && pre[s] == kth) xes++;
+        if (s < K - 1 && pre[s] >= v) q++;
+    }
+    // 2. cpt as functions c -> r ? a : c + a, exclusive scan in lane order
+    int fr = 0, fa = 0;
+    if (trig) {
+        if (gt && xes == 1) { fr = 1; fa = 0; }
+        else { fr = 0; fa = 1; }
+    }
+    int er = 0, ea = 0;   // exclusive composite
+    {
+        int ir = fr, ia = fa;   // inclusive composite (scan)
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            int rr = __shfl_up_sync(FULL, ir, off), ra = __shfl_up_sync(FULL, ia, off);
+            if (lane >= off) {
+                // earlier (rr,ra) then later (ir,ia)
+                if (!ir) { ir = rr; ia = ra + ia; }
+            }
+        }
+        int pr = __shfl_up_sync(FULL, ir, 1), pa = __shfl_up_sync(FULL, ia, 1);
+        if (lane > 0) { er = pr; ea = pa; }
+        // total composite from lane 31 for the state update below
+        int tr = __shfl_sync(FULL, ir, 31), ta = __shfl_sync(FULL, ia, 31);
+        const unsigned before = er ? unsigned(ea) : cpt + unsigned(ea);
+        const unsigned after = fr ? 0u : before + unsigned(fa);
+        // 3. draw offsets: 1 draw per trigger, a second one per tie
+        const unsigned b1 = __ballot_sync(FULL, trig), b2 = __ballot_sync(FULL, trig && !gt);
+        const unsigned lt = lanemask_lt();
+        const int off = __popc(b1 & lt) + __popc(b2 & lt);
+        int o[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) o[s] = s;
+        if (trig) {
+            const float u1 = buf[rp + off];
+            int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
+            if (x > K - 1) x = K - 1;
+            bool write = false;
+            if (!gt) {
+                const float u2 = buf[rp + off + 1];
+                write = __fmul_rn(__uint2float_rn(unsigned(xes) + after), u2) < (float)xes;
+            }
+            int sig[KM];
+#pragma unroll
+            for (int s = 0; s < KM; ++s) sig[s] = (s == x) ? K - 1 : ((s == K - 1) ? x : s);
+            if (gt) {
+#pragma unroll
+                for (int s = 0; s < KM; ++s) {
+                    if (s < K) {
+                        int prevs = s > 0 ? sig[s > 0 ? s - 1 : 0] : 0;
+                        o[s] = s < q ? sig[s] : (s == q ? -(m + 1) : prevs);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < KM; ++s)
+                    if (s < K) o[s] = (write && s == K - 1) ? -(m + 1) : sig[s];
+            }
+        }
+        // 4. compose the slot maps in lane order (tree reduction to lane 0)
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int later[KM];
+#pragma unroll
+            for (int s = 0; s < KM; ++s) later[s] = __shfl_down_sync(FULL, o[s], d);
+            if ((lane & (2 * d - 1)) == 0 && lane + d < 32) {
+                int c[KM];
+#pragma unroll
+                for (int s = 0; s < KM; ++s) c[s] = later[s] < 0 ? later[s] : sel_i<KM>(o, later[s]);
+#pragma unroll
+                for (int s = 0; s < KM; ++s) o[s] = c[s];
+            }
+        }
+        unsigned np[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) {
+            int t = __shfl_sync(FULL, o[s], 0);
+            np[s] = t < 0 ? unsigned(-(t + 1)) : sel_u<KM>(cp, t);
+        }
+#pragma unroll
+        for (int s = 0; s < KM; ++s) cp[s] = np[s];
+        // 5. state values, cpt, draw pointer
+        float last[KM], nv[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) last[s] = __shfl_sync(FULL, st[s], 31);
+        topk_merge<KM>(cv, last, nv);
+#pragma unroll
+        for (int s = 0; s < KM; ++s) cv[s] = nv[s];
+        cpt = tr ? unsigned(ta) : cpt + unsigned(ta);
+        rp += __popc(b1) + __popc(b2);
+    }
+}
+
+template <int KM>
 __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     __shared__ WarpShared wsh[RP_WARPS];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -580,10 +736,12 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     const Slot s = A.slots[b];
     const Geom &g = A.g;
     const int K = A.K;
+    const unsigned FULL = 0xffffffffu;
 
-    float ov[QSK_KMAX];
-    unsigned op[QSK_KMAX];
-    for (int q = 0; q < QSK_KMAX; ++q) { ov[q] = -CUDART_INF_F; op[q] = 0xffffffffu; }
+    float cv[KM];
+    unsigned cp[KM];
+#pragma unroll
+    for (int q = 0; q < KM; ++q) { cv[q] = -CUDART_INF_F; cp[q] = 0xffffffffu; }
     unsigned chosen_cell = 0;
     bool have = false;
 
@@ -596,7 +754,7 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
             have = true;
         }
     } else {
-        // seed: generator.seed(seedFromUnitFloat(seed) + 0)
+        // generator.seed(seedFromUnitFloat(seed) + 0)  (quantileSamplingModule.hpp:45-49,533-534)
         if (lane == 0) {
             unsigned x;
             float sd = s.seed;
@@ -608,133 +766,113 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 x = 1812433253u * (x ^ (x >> 30)) + (unsigned)i;
                 w.mt[i] = x;
             }
-            w.len = 0;
-            w.rp = 0;
         }
         __syncwarp();
+        int rp = 0, len = 0;
         unsigned cpt = 0;
         long long last = -1;
+        const bool emit_masked = (s.flags & SLOT_EMIT_MASKED) != 0;
         const float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
         const int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
         const int *rc = A.rec_cnt + (long long)b * g.nseg;
+        const float *rm = A.rec_max + (long long)b * g.nseg;
         for (int s0 = 0; s0 < g.nseg; s0 += 32) {
-            int myc = (s0 + lane < g.nseg) ? rc[s0 + lane] : 0;
-            unsigned nz = __ballot_sync(0xffffffffu, myc > 0);
+            const int myc = (s0 + lane < g.nseg) ? rc[s0 + lane] : 0;
+            const float mym = (s0 + lane < g.nseg) ? rm[s0 + lane] : -CUDART_INF_F;
+            unsigned nz = __ballot_sync(FULL, myc > 0 && mym >= sel_f<KM>(cv, K - 1));
             while (nz) {
                 const int l = __ffs(nz) - 1;
                 nz &= nz - 1;
                 const int sg = s0 + l;
-                const int cnt = __shfl_sync(0xffffffffu, myc, l);
+                const int cnt = __shfl_sync(FULL, myc, l);
+                const float smax = __shfl_sync(FULL, mym, l);
                 const long long base = (long long)sg * QSK_SEG;
-                float cv[4];
-                int ci[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    int j = lane + 32 * q;
-                    cv[q] = j < cnt ? rv[base + j] : -CUDART_INF_F;
-                    ci[q] = j < cnt ? ri[base + j] : -1;
+                int r0 = 0;
+                while (r0 < cnt) {
+                    const float kth0 = sel_f<KM>(cv, K - 1);
+                    if (smax < kth0) break;   // nothing left in this segment can enter
+                    const bool filling = (kth0 == -CUDART_INF_F);
+                    const int width = filling ? 1 : 32;
+                    const int j = r0 + lane;
+                    const bool valid = lane < width && j < cnt;
+                    const float v = valid ? rv[base + j] : -CUDART_INF_F;
+                    const int m = valid ? ri[base + j] : 0;
+                    if (!filling && __ballot_sync(FULL, valid && v >= kth0) == 0) {
+                        r0 += width;
+                        continue;
+                    }
+                    if (filling && !emit_masked) {
+                        // masked positions between the previous record and this one are
+                        // -inf ties while fewer than K finite values have been seen:
+                        // two draws and one cpt increment each, no visible slot change
+                        const long long mm = __shfl_sync(FULL, (long long)m, 0);
+                        long long c = (mm - (last + 1)) - (valid_prefix(g, s.lo, mm) - valid_prefix(g, s.lo, last + 1));
+                        if (c > 0) {
+                            rng_skip(w, lane, rp, len, 2 * c);
+                            cpt += unsigned(c);
+                        }
+                    }
+                    rng_ensure(w, lane, rp, len, 64);
+                    replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
+                    const unsigned vb = __ballot_sync(FULL, valid);
+                    last = __shfl_sync(FULL, (long long)m, 31 - __clz(vb));
+                    r0 += width;
                 }
+            }
+        }
+        // merge loop (quantileSamplingModule.hpp:546-557): repeated first-max extraction
+        float fv[KM];
+        unsigned fp[KM];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    unsigned lanes_done = 0;
-                    for (;;) {
-                        const float thr = __shfl_sync(0xffffffffu, ov[K - 1], 0);
-                        const bool cand = (ci[q] >= 0) && (cv[q] >= thr);
-                        unsigned bal = __ballot_sync(0xffffffffu, cand) & ~lanes_done;
-                        if (!bal) break;
-                        const int src = __ffs(bal) - 1;
-                        lanes_done |= (2u << src) - 1u;
-                        const float v = __shfl_sync(0xffffffffu, cv[q], src);
-                        const long long m = __shfl_sync(0xffffffffu, ci[q], src);
-                        // masked positions between the last processed one and m are
-                        // -inf ties while fewer than K finite values have been seen
-                        if (thr == -CUDART_INF_F && !(s.flags & SLOT_EMIT_MASKED)) {
-                            long long c = (m - (last + 1)) - (valid_prefix(g, s.lo, m) - valid_prefix(g, s.lo, last + 1));
-                            if (c > 0) {
-                                rng_skip(w, lane, 2 * c);
-                                cpt += unsigned(c);
-                            }
-                        }
-                        last = m;
-                        rng_need(w, lane, 2);
-                        if (lane == 0) {
-                            // fKb.hpp:58-92 (addValueB with generator)
-                            int position = K - 2;
-                            int likeLast = K - 2;
-                            while (likeLast > -1 && ov[K - 1] == ov[likeLast]) likeLast--;
-                            int xes = K - likeLast - 1;
-                            float u1 = w.buf[w.rp++];
-                            int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
-                            if (x > K - 1) x = K - 1;   // u1 < 1 keeps x <= K-1; guard for memory safety
-                            unsigned tp = op[x];
-                            op[x] = op[K - 1];
-                            op[K - 1] = tp;
-                            if (v > ov[K - 1]) {
-                                if (xes == 1) cpt = 0;
-                                else cpt++;
-                                while (position > -1 && v > ov[position]) {
-                                    ov[position + 1] = ov[position];
-                                    op[position + 1] = op[position];
-                                    position--;
-                                }
-                                ov[position + 1] = v;
-                                op[position + 1] = unsigned(m);
-                            } else {
-                                cpt++;
-                                float u2 = w.buf[w.rp++];
-                                if (__fmul_rn(__uint2float_rn(unsigned(xes) + cpt), u2) < (float)xes)
-                                    op[position + 1] = unsigned(m);
-                            }
-                        }
-                        __syncwarp();
+        for (int j = 0; j < KM; ++j) {
+            fv[j] = -CUDART_INF_F;
+            fp[j] = 0xffffffffu;
+            if (j < K) {
+                int best = 0;
+                float bv = cv[0];
+#pragma unroll
+                for (int l2 = 1; l2 < KM; ++l2)
+                    if (l2 < K && cv[l2] > bv) { best = l2; bv = cv[l2]; }
+                fv[j] = bv;
+                fp[j] = sel_u<KM>(cp, best);
+#pragma unroll
+                for (int l2 = 0; l2 < KM; ++l2)
+                    if (l2 == best) cv[l2] = -CUDART_INF_F;
+            }
+        }
+        // sample(): std::sort by score — insertion sort (stable) for K <= 16
+#pragma unroll
+        for (int a2 = 1; a2 < KM; ++a2) {
+            if (a2 < K) {
+#pragma unroll
+                for (int c = a2; c > 0; --c) {
+                    if (fv[c] > fv[c - 1]) {
+                        float tv = fv[c]; fv[c] = fv[c - 1]; fv[c - 1] = tv;
+                        unsigned tp = fp[c]; fp[c] = fp[c - 1]; fp[c - 1] = tp;
                     }
                 }
             }
         }
-        if (lane == 0) {
-            // merge loop (quantileSamplingModule.hpp:546-557): repeated first-max extraction
-            float fv[QSK_KMAX];
-            unsigned fp[QSK_KMAX];
-            for (int j = 0; j < K; ++j) {
-                int best = 0;
-                for (int l2 = 1; l2 < K; ++l2)
-                    if (ov[l2] > ov[best]) best = l2;
-                fv[j] = ov[best];
-                fp[j] = op[best];
-                ov[best] = -CUDART_INF_F;
-            }
-            // sample(): std::sort by score (stable insertion sort for K <= 16)
-            for (int a = 1; a < K; ++a) {
-                float kv = fv[a];
-                unsigned kp = fp[a];
-                int c = a - 1;
-                while (c >= 0 && kv > fv[c]) {
-                    fv[c + 1] = fv[c];
-                    fp[c + 1] = fp[c];
-                    c--;
-                }
-                fv[c + 1] = kv;
-                fp[c + 1] = kp;
-            }
-            if (A.out_val) {
-                for (int j = 0; j < K; ++j) {
+        if (lane == 0 && A.out_val) {
+#pragma unroll
+            for (int j = 0; j < KM; ++j)
+                if (j < K) {
                     A.out_val[(long long)b * K + j] = fv[j];
                     A.out_pos[(long long)b * K + j] = fp[j];
                 }
+        }
+        if (A.state || A.node_cell) {
+            // cvtIndexToPosition (CPUThreadDevice.cpp:257-268), unsigned arithmetic
+            unsigned index = sel_u<KM>(fp, s.sel);
+            unsigned position = 0;
+            unsigned div = (unsigned)g.N;
+            for (int d = g.nd - 1; d >= 0; --d) {
+                unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
+                div /= f;
+                position = position * sr + ((f - (index / div) % f - (unsigned)s.mn[d] - 1u) + sr) % sr;
             }
-            if (A.state || A.node_cell) {
-                // cvtIndexToPosition (CPUThreadDevice.cpp:257-268), unsigned arithmetic
-                unsigned index = fp[s.sel];
-                unsigned position = 0;
-                unsigned div = (unsigned)g.N;
-                for (int d = g.nd - 1; d >= 0; --d) {
-                    unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
-                    div /= f;
-                    position = position * sr + ((f - (index / div) % f - (unsigned)s.mn[d] - 1u) + sr) % sr;
-                }
-                chosen_cell = position;
-                have = true;
-            }
+            chosen_cell = position;
+            have = true;
         }
     }
     if (lane == 0 && have) {
@@ -827,7 +965,11 @@ cudaError_t set_map_smem_limit(int bytes) {
 
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
     unsigned blocks = (unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS);
-    k_replay<<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    if (a.K <= 1) k_replay<1><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    else if (a.K <= 2) k_replay<2><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    else if (a.K <= 4) k_replay<4><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    else if (a.K <= 8) k_replay<8><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    else k_replay<16><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
     return cudaGetLastError();
 }
 

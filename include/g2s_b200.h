@@ -145,6 +145,13 @@ typedef struct {
     float ms_setup_neighbours;    /* device time of the neighbour search */
     float ms_levels;              /* device time of the level computation */
     float ms_batches;             /* device time of all batches */
+    float ms_total;               /* device time of the whole run (first to last kernel) */
+    long long launches;           /* kernels launched by the run */
+    long long map_launches;       /* launches of the fused map kernel */
+    float ms_map;                 /* device time inside the map kernel (profiling mode only) */
+    float ms_prep;                /* ... inside the per-batch prep kernel (profiling mode only) */
+    float ms_replay;              /* ... inside the k-best replay kernel (profiling mode only) */
+    long long map_positions;      /* scan positions evaluated by the map kernel (nodes x N) */
 } qsk_sim_info;
 
 typedef struct qsk_sim qsk_sim;
@@ -161,6 +168,9 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed);
  * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL). */
 int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out);
 int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info);
+/* Profiling mode: record CUDA events around every kernel of the next runs so
+ * that qsk_sim_info reports per-kernel device time (adds event overhead). */
+int qsk_sim_set_profiling(qsk_sim *s, int on);
 /* Path (cell order), per-path-index seeds and number of informed cells. */
 int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
 int qsk_sim_destroy(qsk_sim *s);
