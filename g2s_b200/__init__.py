@@ -77,6 +77,7 @@ SIGNATURES = {
     "qsk_sim_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
+    "qsk_set_map_mode": (ctypes.c_int, [ctypes.c_int]),
     "qsk_qs_path": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p]),
 }
 
@@ -110,6 +111,12 @@ def device_count() -> int:
     c = ctypes.c_int(0)
     rc = lib().qsk_device_count(ctypes.byref(c))
     return c.value if rc == 0 else 0
+
+
+def set_map_mode(mode: int) -> None:
+    """0: automatic (bit-sliced kernel for unit-weight categorical patterns),
+    1: always the FP32 gather kernel.  Identical results either way."""
+    _check(lib().qsk_set_map_mode(int(mode)), "qsk_set_map_mode")
 
 
 def search_template(kernel_dims, nvar: int = 1, kernel: Optional[np.ndarray] = None):

@@ -140,7 +140,18 @@ struct qsk_ti {
     DBuf<float> grid;             // raw TI (grid-built): cells * nvar
     DBuf<int> dtypes;
     long long cells = 0;
+    // bit planes of categorical variables (grid-built, every variable categorical
+    // with at most QSK_CMAX categories)
+    bool planes_ok = false;
+    int pw = 0;
+    DBuf<unsigned> planes;
+    DBuf<int> ncat;
+    DBuf<float> catv;
 };
+
+namespace {
+int g_map_mode = 0;   // 0: automatic, 1: always the FP32 gather kernel
+}
 
 struct qsk_worker {
     qsk_ti *ti = nullptr;
@@ -311,6 +322,39 @@ static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int n
     if ((e = cudaMemcpy(t->dtypes.p, types, sizeof(int) * nvar, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
     if ((e = t->layers.alloc(size_t(nvar) * t->g.N)) != cudaSuccess) return bail(e);
     if ((e = launch_build_layers(t->grid.p, nvar, t->dtypes.p, t->g, t->layers.p, 0)) != cudaSuccess) return bail(e);
+    // categories (distinct non-NaN codes) of categorical variables, for the bit planes
+    bool all_cat = true;
+    std::vector<int> ncat(nvar, 0);
+    std::vector<float> catv(size_t(nvar) * QSK_CMAX, 0.f);
+    if (!data_on_device) {
+        for (int v = 0; v < nvar && all_cat; ++v) {
+            if (types[v] != 1) { all_cat = false; break; }
+            for (long long i = 0; i < t->cells && all_cat; ++i) {
+                float x = data[i * nvar + v];
+                if (std::isnan(x)) continue;
+                bool seen = false;
+                for (int q = 0; q < ncat[v]; ++q) seen |= (catv[size_t(v) * QSK_CMAX + q] == x);
+                if (!seen) {
+                    if (ncat[v] == QSK_CMAX) all_cat = false;
+                    else catv[size_t(v) * QSK_CMAX + ncat[v]++] = x;
+                }
+            }
+        }
+    } else {
+        all_cat = false;
+    }
+    if (all_cat) {
+        t->pw = int((t->g.N + 31) / 32) + 2;
+        if ((e = t->ncat.alloc(nvar)) != cudaSuccess) return bail(e);
+        if ((e = t->catv.alloc(catv.size())) != cudaSuccess) return bail(e);
+        if ((e = t->planes.alloc(size_t(nvar) * QSK_CMAX * t->pw)) != cudaSuccess) return bail(e);
+        if ((e = cudaMemcpy(t->ncat.p, ncat.data(), sizeof(int) * nvar, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
+        if ((e = cudaMemcpy(t->catv.p, catv.data(), sizeof(float) * catv.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return bail(e);
+        if ((e = launch_build_planes(t->layers.p, t->g, nvar, t->ncat.p, t->catv.p, t->pw, t->planes.p, 0)) != cudaSuccess)
+            return bail(e);
+        t->planes_ok = true;
+    }
     if ((e = cudaStreamSynchronize(0)) != cudaSuccess) return bail(e);
     *out = t;
     return QSK_OK;
@@ -390,18 +434,42 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt, w->rec_max));
     CK(w->out_val.ensure(size_t(B) * k));
     CK(w->out_pos.ensure(size_t(B) * k));
-    MapArgs ma;
-    ma.g = g;
-    ma.layers = ti->layers.p;
-    ma.slots = w->slots.p;
-    ma.terms = w->terms.p;
-    ma.maxterms = maxterms;
-    ma.segs_per_cta = map_segs_per_cta(g, B);
-    ma.rec_val = w->rec_val.p;
-    ma.rec_idx = w->rec_idx.p;
-    ma.rec_cnt = w->rec_cnt.p;
-    ma.rec_max = w->rec_max.p;
-    CK(launch_map_records(ma, B, int(k), maxterms, w->st));
+    bool bits = ti->planes_ok && g_map_mode == 0 && maxterms <= 255;
+    for (size_t i = 0; i < w->h_terms.size() && bits; ++i) {
+        int b = int(i / maxterms), t = int(i % maxterms);
+        if (t >= w->h_slots[b].nterms) continue;
+        bits &= (w->h_terms[i].op == OP_EQ && w->h_terms[i].a == 1.f);
+    }
+    if (bits) {
+        BitArgs ba;
+        ba.g = g;
+        ba.planes = ti->planes.p;
+        ba.pw = ti->pw;
+        ba.ncat = ti->ncat.p;
+        ba.catv = ti->catv.p;
+        ba.slots = w->slots.p;
+        ba.terms = w->terms.p;
+        ba.maxterms = maxterms;
+        ba.segs_per_cta = map_bits_segs_per_cta(g, B);
+        ba.rec_val = w->rec_val.p;
+        ba.rec_idx = w->rec_idx.p;
+        ba.rec_cnt = w->rec_cnt.p;
+        ba.rec_max = w->rec_max.p;
+        CK(launch_map_bits(ba, B, int(k), maxterms, w->st));
+    } else {
+        MapArgs ma;
+        ma.g = g;
+        ma.layers = ti->layers.p;
+        ma.slots = w->slots.p;
+        ma.terms = w->terms.p;
+        ma.maxterms = maxterms;
+        ma.segs_per_cta = map_segs_per_cta(g, B);
+        ma.rec_val = w->rec_val.p;
+        ma.rec_idx = w->rec_idx.p;
+        ma.rec_cnt = w->rec_cnt.p;
+        ma.rec_max = w->rec_max.p;
+        CK(launch_map_records(ma, B, int(k), maxterms, w->st));
+    }
     ReplayArgs ra;
     std::memset(&ra, 0, sizeof(ra));
     ra.g = g;
@@ -497,6 +565,7 @@ struct qsk_sim {
     DBuf<float> d_rec_max;
     int maxterms = 0;
     int max_slots = 0;
+    bool use_bits = false;
     qsk_sim_info info;
     bool neighbours_ready = false;
     bool profiling = false;
@@ -673,18 +742,36 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            MapArgs ma;
-            ma.g = g;
-            ma.layers = s->ti->layers.p;
-            ma.slots = s->d_slots.p;
-            ma.terms = s->d_terms.p;
-            ma.maxterms = s->maxterms;
-            ma.segs_per_cta = map_segs_per_cta(g, B);
-            ma.rec_val = s->d_rec_val.p;
-            ma.rec_idx = s->d_rec_idx.p;
-            ma.rec_cnt = s->d_rec_cnt.p;
-            ma.rec_max = s->d_rec_max.p;
-            CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+            if (s->use_bits && g_map_mode == 0) {
+                BitArgs ba;
+                ba.g = g;
+                ba.planes = s->ti->planes.p;
+                ba.pw = s->ti->pw;
+                ba.ncat = s->ti->ncat.p;
+                ba.catv = s->ti->catv.p;
+                ba.slots = s->d_slots.p;
+                ba.terms = s->d_terms.p;
+                ba.maxterms = s->maxterms;
+                ba.segs_per_cta = map_bits_segs_per_cta(g, B);
+                ba.rec_val = s->d_rec_val.p;
+                ba.rec_idx = s->d_rec_idx.p;
+                ba.rec_cnt = s->d_rec_cnt.p;
+                ba.rec_max = s->d_rec_max.p;
+                CK(launch_map_bits(ba, B, s->K, s->maxterms, s->st));
+            } else {
+                MapArgs ma;
+                ma.g = g;
+                ma.layers = s->ti->layers.p;
+                ma.slots = s->d_slots.p;
+                ma.terms = s->d_terms.p;
+                ma.maxterms = s->maxterms;
+                ma.segs_per_cta = map_segs_per_cta(g, B);
+                ma.rec_val = s->d_rec_val.p;
+                ma.rec_idx = s->d_rec_idx.p;
+                ma.rec_cnt = s->d_rec_cnt.p;
+                ma.rec_max = s->d_rec_max.p;
+                CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+            }
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             s->info.launches += 3;
             s->info.map_launches += 1;
@@ -793,6 +880,9 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     }
     build_path(s);
     s->maxterms = std::max(1, s->n * s->nvar);
+    // bit-sliced map: every variable categorical with bit planes, unit weights
+    s->use_bits = s->ti->planes_ok && s->maxterms <= 255;
+    for (float wv : s->wtab) s->use_bits &= (wv == 1.f);
     // uploads
     if ((e = s->d_tpl.upload(s->tpl.data(), s->tpl.size(), s->st)) != cudaSuccess ||
         (e = s->d_wtab.upload(s->wtab.data(), s->wtab.size(), s->st)) != cudaSuccess ||
@@ -952,6 +1042,12 @@ int qsk_sim_destroy(qsk_sim *s) {
         s->ti = nullptr;
         delete s;
     }
+    return QSK_OK;
+}
+
+int qsk_set_map_mode(int mode) {
+    if (mode < 0 || mode > 1) return fail(QSK_ERR_ARG, "map mode %d", mode);
+    g_map_mode = mode;
     return QSK_OK;
 }
 

@@ -9,6 +9,7 @@
 #define QSK_MAXD 4          // grid dimensions supported
 #define QSK_SEG 128         // scan positions per warp segment (32 lanes x 4)
 #define QSK_KMAX 16         // largest extendK handled on device
+#define QSK_CMAX 32         // categories per variable with bit planes
 
 namespace qsk {
 
@@ -108,6 +109,22 @@ struct MapArgs {
     float *rec_max;   // [slot][nseg] largest valid score of the segment
 };
 
+struct BitArgs {
+    Geom g;
+    const unsigned *planes;   // [var][QSK_CMAX][pw] words
+    int pw;                   // words per plane (ceil(N/32) + 2)
+    const int *ncat;          // categories per variable
+    const float *catv;        // [var][QSK_CMAX] category codes
+    const Slot *slots;
+    const Term *terms;
+    int maxterms;
+    int segs_per_cta;         // 1024-position segments per CTA
+    float *rec_val;
+    int *rec_idx;
+    int *rec_cnt;
+    float *rec_max;
+};
+
 struct ReplayArgs {
     Geom g;
     const Slot *slots;
@@ -145,6 +162,10 @@ cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);
 int map_segs_per_cta(const Geom &g, int nslots);
 cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
 cudaError_t set_map_smem_limit(int bytes);
+cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, const int *ncat, const float *catv,
+                                int pw, unsigned *planes, cudaStream_t st);
+int map_bits_segs_per_cta(const Geom &g, int nslots);
+cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
 
 }  // namespace qsk

@@ -888,6 +888,215 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// bit-sliced map for categorical patterns with unit weights
+//
+// One bit plane per (categorical variable, category) in the flipped scan
+// order: bit q of plane (v,c) = [layer_v[q] == c].  For 32 consecutive scan
+// positions m0..m0+31 the matches of term t are bits m0-d_t.. of its plane,
+// read as one funnel-shifted 32-bit word; an 8-plane bit-sliced counter adds
+// them.  With every weight equal to 1 the reference's sum of weights is the
+// match count, exact in FP32 (< 2^24), so the scores equal the FP32 map bit
+// for bit.  Records, counts and maxima are written in the same 128-position
+// segment layout as k_map_records.
+// ---------------------------------------------------------------------------
+__global__ void k_build_planes(const float *__restrict__ layers, Geom g, int nvar, const int *__restrict__ ncat,
+                               const float *__restrict__ catv, int pw, unsigned *__restrict__ planes) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long total = (long long)nvar * QSK_CMAX * pw;
+    if (idx >= total) return;
+    int w = int(idx % pw);
+    int vc = int(idx / pw);
+    int c = vc % QSK_CMAX, v = vc / QSK_CMAX;
+    unsigned word = 0;
+    if (c < ncat[v]) {
+        float cv = catv[v * QSK_CMAX + c];
+        for (int b = 0; b < 32; ++b) {
+            long long q = (long long)w * 32 + b;
+            if (q < g.N && layers[(long long)v * g.N + q] == cv) word |= 1u << b;
+        }
+    }
+    planes[idx] = word;
+}
+
+template <int KF>
+__device__ __forceinline__ void topk_insert(float (&st)[KF], float x) {
+    // insert x into the descending list st, dropping the smallest
+#pragma unroll
+    for (int s = KF - 1; s >= 0; --s) {
+        float prev = (s > 0) ? st[s > 0 ? s - 1 : 0] : CUDART_INF_F;
+        // new st[s] = max(min(prev, x), st[s])
+        st[s] = fmaxf(st[s], fminf(prev, x));
+    }
+}
+
+template <int KF>
+__global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
+    extern __shared__ int2 bterm[];
+    __shared__ Slot ss;
+    __shared__ int nbt;
+    const int b = blockIdx.y;
+    if (threadIdx.x == 0) ss = A.slots[b];
+    __syncthreads();
+    if (ss.flags & SLOT_SKIP) return;
+    const Geom &g = A.g;
+    if (threadIdx.x == 0) {
+        // terms -> (plane offset, flat offset); a code that is no category of
+        // the TI never matches and is dropped
+        const Term *src = A.terms + (long long)b * A.maxterms;
+        int k = 0;
+        for (int t = 0; t < ss.nterms; ++t) {
+            const Term tm = src[t];
+            long long base = tm.base;
+            int v = int((base + g.N - 1) / g.N);   // base = v*N - d with 0 <= d < N
+            if (base <= 0) v = 0;
+            long long d = (long long)v * g.N - base;
+            int c = -1;
+            for (int q = 0; q < A.ncat[v]; ++q)
+                if (A.catv[v * QSK_CMAX + q] == tm.b) { c = q; break; }
+            if (c >= 0) bterm[k++] = make_int2((v * QSK_CMAX + c) * A.pw, int(d));
+        }
+        nbt = k;
+    }
+    __syncthreads();
+    const int nt = nbt;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const bool emit_masked = (ss.flags & SLOT_EMIT_MASKED) != 0;
+    const int nseg1k = (int)((g.N + 1023) / 1024);
+    const int seg_begin = blockIdx.x * A.segs_per_cta;
+    int seg_end = seg_begin + A.segs_per_cta;
+    if (seg_end > nseg1k) seg_end = nseg1k;
+    float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
+    int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
+
+    for (int sg = seg_begin + warp; sg < seg_end; sg += nwarps) {
+        const long long m0 = (long long)sg * 1024 + 32 * lane;
+        // validity of the lane's 32 positions (incremental digits)
+        unsigned vmask = 0, emask = 0;
+        if (m0 < g.N) {
+            int dig[QSK_MAXD];
+#pragma unroll
+            for (int d = 0; d < QSK_MAXD; ++d) dig[d] = d < g.nd ? int((m0 / g.sstride[d]) % g.fft[d]) : 0;
+            bool rowok = true;
+#pragma unroll
+            for (int d = 1; d < QSK_MAXD; ++d)
+                if (d < g.nd) rowok &= dig[d] >= ss.lo[d];
+            for (int bit = 0; bit < 32; ++bit) {
+                if (m0 + bit >= g.N) break;
+                emask |= 1u << bit;
+                if (rowok && dig[0] >= ss.lo[0]) vmask |= 1u << bit;
+                if (++dig[0] == g.fft[0]) {
+                    dig[0] = 0;
+                    for (int d = 1; d < g.nd; ++d) {
+                        if (++dig[d] < g.fft[d]) break;
+                        dig[d] = 0;
+                    }
+                    rowok = true;
+                    for (int d = 1; d < g.nd; ++d) rowok &= dig[d] >= ss.lo[d];
+                }
+            }
+        }
+        unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
+        if (vmask) {
+            const int im0 = int(m0);
+            for (int t = 0; t < nt; ++t) {
+                const int2 bt = bterm[t];
+                const unsigned *P = A.planes + bt.x;
+                const int q0 = im0 - bt.y;
+                const int wi = q0 >> 5;
+                const unsigned w0 = wi >= 0 ? __ldg(P + wi) : 0u;
+                const unsigned w1 = wi + 1 >= 0 ? __ldg(P + wi + 1) : 0u;
+                unsigned x = __funnelshift_r(w0, w1, unsigned(q0) & 31u);
+                unsigned t0;
+                t0 = c0 & x; c0 ^= x; x = t0;
+                t0 = c1 & x; c1 ^= x; x = t0;
+                t0 = c2 & x; c2 ^= x; x = t0;
+                t0 = c3 & x; c3 ^= x; x = t0;
+                t0 = c4 & x; c4 ^= x; x = t0;
+                t0 = c5 & x; c5 ^= x; x = t0;
+                t0 = c6 & x; c6 ^= x; x = t0;
+                c7 ^= x;
+            }
+        }
+        // scores in scan order; lane-local top-K
+        float sc[32];
+        float lst[KF];
+#pragma unroll
+        for (int q = 0; q < KF; ++q) lst[q] = -CUDART_INF_F;
+        float lmax = -CUDART_INF_F;
+#pragma unroll
+        for (int bit = 0; bit < 32; ++bit) {
+            unsigned cnt = ((c0 >> bit) & 1u) | (((c1 >> bit) & 1u) << 1) | (((c2 >> bit) & 1u) << 2) |
+                           (((c3 >> bit) & 1u) << 3) | (((c4 >> bit) & 1u) << 4) | (((c5 >> bit) & 1u) << 5) |
+                           (((c6 >> bit) & 1u) << 6) | (((c7 >> bit) & 1u) << 7);
+            float x = ((vmask >> bit) & 1u) ? (float)cnt : -CUDART_INF_F;
+            sc[bit] = x;
+            lmax = fmaxf(lmax, x);
+            topk_insert<KF>(lst, x);
+        }
+        // exclusive prefix of the lane states across the 1024-position segment
+        float inc[KF];
+#pragma unroll
+        for (int q = 0; q < KF; ++q) inc[q] = lst[q];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            float rcv[KF], mrg[KF];
+#pragma unroll
+            for (int q = 0; q < KF; ++q) rcv[q] = __shfl_up_sync(0xffffffffu, inc[q], off);
+            if (lane >= off) {
+                topk_merge<KF>(inc, rcv, mrg);
+#pragma unroll
+                for (int q = 0; q < KF; ++q) inc[q] = mrg[q];
+            }
+        }
+        float st[KF];
+#pragma unroll
+        for (int q = 0; q < KF; ++q) {
+            float y = __shfl_up_sync(0xffffffffu, inc[q], 1);
+            st[q] = lane == 0 ? -CUDART_INF_F : y;
+        }
+        // record flags (value not below the K-th best of everything before it)
+        unsigned rmask = 0;
+#pragma unroll
+        for (int bit = 0; bit < 32; ++bit) {
+            const float x = sc[bit];
+            const bool ex = (emask >> bit) & 1u;
+            const bool val = (vmask >> bit) & 1u;
+            if (ex && x >= st[KF - 1] && (val || emit_masked)) rmask |= 1u << bit;
+            topk_insert<KF>(st, x);
+        }
+        // offsets inside each 128-position sub-segment (4 lanes)
+        const int rc = __popc(rmask);
+        int pre = rc;
+        int y1 = __shfl_up_sync(0xffffffffu, pre, 1);
+        if ((lane & 3) >= 1) pre += y1;
+        int y2 = __shfl_up_sync(0xffffffffu, pre, 2);
+        if ((lane & 3) >= 2) pre += y2;
+        const int excl = pre - rc;
+        const int tot = __shfl_sync(0xffffffffu, pre, (lane | 3));
+        float gmax = lmax;
+        gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, 1));
+        gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, 2));
+        const long long sub = (long long)sg * 8 + (lane >> 2);
+        if (sub < g.nseg) {
+            const long long rb = sub * QSK_SEG + excl;
+            int o = 0;
+#pragma unroll
+            for (int bit = 0; bit < 32; ++bit) {
+                if ((rmask >> bit) & 1u) {
+                    rv[rb + o] = sc[bit];
+                    ri[rb + o] = int(m0 + bit);
+                    o++;
+                }
+            }
+            if ((lane & 3) == 0) {
+                A.rec_cnt[(long long)b * g.nseg + sub] = tot;
+                A.rec_max[(long long)b * g.nseg + sub] = gmax;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // launch wrappers (called by the host engine)
 // ---------------------------------------------------------------------------
 cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers,
@@ -947,6 +1156,35 @@ cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms
     else if (K <= 4) k_map_records<4><<<grid, threads, smem, st>>>(a);
     else if (K <= 8) k_map_records<8><<<grid, threads, smem, st>>>(a);
     else k_map_records<16><<<grid, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, const int *ncat, const float *catv,
+                                int pw, unsigned *planes, cudaStream_t st) {
+    long long total = (long long)nvar * QSK_CMAX * pw;
+    k_build_planes<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(layers, g, nvar, ncat, catv, pw, planes);
+    return cudaGetLastError();
+}
+
+int map_bits_segs_per_cta(const Geom &g, int nslots) {
+    long long nseg1k = (g.N + 1023) / 1024;
+    long long target = 148LL * 8;
+    long long per = (nseg1k * nslots + target - 1) / target;
+    if (per < 8) per = 8;
+    if (per > 16) per = 16;
+    return (int)per;
+}
+
+cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st) {
+    int threads = 256;
+    long long nseg1k = (a.g.N + 1023) / 1024;
+    dim3 grid((unsigned)((nseg1k + a.segs_per_cta - 1) / a.segs_per_cta), (unsigned)nslots);
+    size_t smem = sizeof(int2) * (size_t)(maxterms_in_batch > 0 ? maxterms_in_batch : 1);
+    if (K <= 1) k_map_bits<1><<<grid, threads, smem, st>>>(a);
+    else if (K <= 2) k_map_bits<2><<<grid, threads, smem, st>>>(a);
+    else if (K <= 4) k_map_bits<4><<<grid, threads, smem, st>>>(a);
+    else if (K <= 8) k_map_bits<8><<<grid, threads, smem, st>>>(a);
+    else k_map_bits<16><<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

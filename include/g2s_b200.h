@@ -188,6 +188,12 @@ int qsk_qs_template(int ndim, int nvar, const unsigned *kernel_dims, const float
  * Returns the number of informed cells (<0: error). */
 long long qsk_qs_path(long long cells, int nvar, const float *di_init, unsigned seed, unsigned *order, float *seeds);
 
+/* Map kernel selection, process-wide: 0 (default) picks the bit-sliced
+ * kernel for categorical patterns with unit weights and the FP32 gather
+ * kernel otherwise; 1 always uses the FP32 gather kernel.  Both give the same
+ * scores bit for bit; the switch exists to test exactly that. */
+int qsk_set_map_mode(int mode);
+
 /* One call: setup, simulate, read back into di_inout / id_out (host). */
 int qsk_simulate(int device, const qsk_qs_params *p, float *di_inout, unsigned *id_out);
 

@@ -179,3 +179,25 @@ def test_batch_equals_single(g2s, gpu):
     for b, (sc, ix, mn) in enumerate(single):
         assert np.array_equal(out_s[2 * b:2 * b + 2], sc) and np.array_equal(out_i[2 * b:2 * b + 2], ix)
         assert np.array_equal(out_m[2 * b:2 * b + 2], mn)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_categorical_bit_and_float_kernels_agree(g2s, gpu, oracle, mode):
+    """Unit-weight categorical patterns run on the bit-sliced kernel (mode 0)
+    or the FP32 gather kernel (mode 1); both equal the oracle bit for bit."""
+    ti = syn.channels2d((100, 130), n_channels=9, seed=7)
+    T = g2s.TrainingImage(ti, [1])
+    W = g2s.Worker(T)
+    rng = np.random.default_rng(42)
+    g2s.set_map_mode(mode)
+    try:
+        for trial in range(8):
+            n = int(rng.integers(2, 90))
+            offs, vals = random_pattern(rng, ti, [1], n, radius=7, nd=2)
+            seed = float(np.float32(rng.random()))
+            for k in (1, 2, 4):
+                sc, ix, mn = W.pattern_kbest(offs, make_terms(offs, vals, [1]), k, seed)
+                v, p, *_ = oracle_kbest(oracle, ti, [1], offs, vals, k, seed)
+                assert np.array_equal(sc, v) and np.array_equal(ix, p), (trial, k)
+    finally:
+        g2s.set_map_mode(0)

@@ -119,3 +119,14 @@ def test_conditioning_data_kept(g2s, gpu, oracle):
     assert np.array_equal(out.reshape(-1)[cells], di.reshape(-1)[cells])
     o = oracle.simulate(ti, di, [0], 15, 1.2, 9, mode=0)
     assert np.array_equal(out, o["sim"])
+
+
+def test_categorical_simulation_bit_and_float_kernels_agree(g2s, gpu):
+    g = golden("cat2d_small")
+    g2s.set_map_mode(1)
+    try:
+        (sim1, idx1, _), _ = run_gpu(g2s, g)
+    finally:
+        g2s.set_map_mode(0)
+    (sim0, idx0, _), _ = run_gpu(g2s, g)
+    assert np.array_equal(sim0, sim1) and np.array_equal(idx0, idx1)
