@@ -995,18 +995,44 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                 }
             }
         }
+        // bit-sliced counter: c0 (ones), c1 (twos), c2 (fours) fed by
+        // carry-save adders over groups of 8 match words, c3..c7 count eights
         unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
         if (vmask) {
             const int im0 = int(m0);
-            for (int t = 0; t < nt; ++t) {
+            auto match = [&](int t) -> unsigned {
                 const int2 bt = bterm[t];
                 const unsigned *P = A.planes + bt.x;
                 const int q0 = im0 - bt.y;
                 const int wi = q0 >> 5;
                 const unsigned w0 = wi >= 0 ? __ldg(P + wi) : 0u;
                 const unsigned w1 = wi + 1 >= 0 ? __ldg(P + wi + 1) : 0u;
-                unsigned x = __funnelshift_r(w0, w1, unsigned(q0) & 31u);
-                unsigned t0;
+                return __funnelshift_r(w0, w1, unsigned(q0) & 31u);
+            };
+            auto csa = [](unsigned &h, unsigned &l, unsigned a, unsigned b, unsigned c) {
+                const unsigned u = a ^ b;
+                h = (a & b) | (u & c);
+                l = u ^ c;
+            };
+            int t = 0;
+            for (; t + 8 <= nt; t += 8) {
+                unsigned twosA, twosB, foursA, foursB, eights;
+                csa(twosA, c0, c0, match(t), match(t + 1));
+                csa(twosB, c0, c0, match(t + 2), match(t + 3));
+                csa(foursA, c1, c1, twosA, twosB);
+                csa(twosA, c0, c0, match(t + 4), match(t + 5));
+                csa(twosB, c0, c0, match(t + 6), match(t + 7));
+                csa(foursB, c1, c1, twosA, twosB);
+                csa(eights, c2, c2, foursA, foursB);
+                unsigned x = eights, t0;
+                t0 = c3 & x; c3 ^= x; x = t0;
+                t0 = c4 & x; c4 ^= x; x = t0;
+                t0 = c5 & x; c5 ^= x; x = t0;
+                t0 = c6 & x; c6 ^= x; x = t0;
+                c7 ^= x;
+            }
+            for (; t < nt; ++t) {
+                unsigned x = match(t), t0;
                 t0 = c0 & x; c0 ^= x; x = t0;
                 t0 = c1 & x; c1 ^= x; x = t0;
                 t0 = c2 & x; c2 ^= x; x = t0;
