@@ -1,6 +1,8 @@
 """Per-pattern parity: map + k-best of the CUDA path against the oracle (bit
 for bit: same FP32 term order, same reservoir tie-breaking), against FP64
 (tolerance 1e-5 of the term scale) and the reference's self-match KAT."""
+import zlib
+
 import numpy as np
 import pytest
 
@@ -30,7 +32,7 @@ def make_terms(offsets, values, types):
 
 def random_pattern(rng, ti, types, n, radius, nd):
     nvar = len(types)
-    shape = ti.shape if nvar == 1 else ti.shape[:-1]
+    n = min(n, (2 * radius + 1) ** nd)   # distinct offsets available in the box
     offs = [np.zeros(nd, np.int32)]
     seen = {tuple(offs[0])}
     while len(offs) < n:
@@ -66,7 +68,7 @@ CASES = [
 @pytest.mark.parametrize("k", [1, 2, 3, 5, 16])
 def test_pattern_kbest_bit_exact(g2s, gpu, oracle, name, mk, types, nd, k):
     ti = mk()
-    rng = np.random.default_rng(abs(hash((name, k))) % 2**32)
+    rng = np.random.default_rng(zlib.crc32(f"{name}-{k}".encode()))
     T = g2s.TrainingImage(ti, types)
     W = g2s.Worker(T)
     for trial in range(6):
