@@ -106,6 +106,26 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def replica_seed(base: int, rank: int) -> int:
+    """Replicas only: rank r simulates its own realisation with seed base + r."""
+    return base + rank
+
+
+def slowest(value: float, dist=None, device=None) -> float:
+    """Max over ranks (device time of the slowest rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(nodes_per_rank: int, steps: int, world: int, slowest_ms: float) -> float:
+    """Nodes of all ranks divided by the slowest rank's time."""
+    return nodes_per_rank * steps * world / (slowest_ms / 1000.0)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -192,7 +212,7 @@ def main():
 
     ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
     di = np.full(DI_SHAPE, np.nan, np.float32)
-    seed = SEED + rank
+    seed = replica_seed(SEED, rank)
     sim = g2s.Simulation(ti, di, [1], n=N_NB, k=K_CAND, seed=seed, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")  # > 126 MB L2
 
@@ -221,11 +241,8 @@ def main():
     clocks = clk.summary()
     total_ms = float(sum(step_ms))
     nodes = int(sim.info()["nodes"])
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = nodes * args.steps * ws / (total_ms / 1000.0)
+    total_ms = slowest(total_ms, dist, f"cuda:{dev}")
+    value = whole_job_rate(nodes, args.steps, ws, total_ms)
 
     # roofline of the dominant kernel (fused map + record filter): one extra
     # profiled step records events around every launch
@@ -254,10 +271,7 @@ def main():
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_vals))
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = slowest(e2e_s, dist, f"cuda:{dev}")
     e2e = {"value": nodes * ws / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": int(ti.nbytes + di.nbytes),
            "d2h_bytes_per_step": int(di.nbytes + di.size * 4)}
