@@ -193,6 +193,7 @@ def main():
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--ref-side", type=int, default=120)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -250,6 +251,7 @@ def main():
     sim.run()
     pinf = sim.info()
     sim.set_profiling(False)
+    map_kernel = "bits"   # categorical TI with a uniform kernel: bit-sliced map kernel
     N = TI_SHAPE[0] * TI_SHAPE[1]
     L = 2  # categorical variable with 2 classes: 2 indicator layers
     bytes_per_node = 4 * N * L
@@ -263,16 +265,16 @@ def main():
     # e2e: the public one-call API with host buffers (H2D of TI+grid, D2H of
     # grid+index image inside the timed region), wall clock around the call
     e2e_vals = []
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
         d = np.full(DI_SHAPE, np.nan, np.float32)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g2s.qs(ti, d, [1], k=K_CAND, n=N_NB, s=seed, device=dev)
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(e2e_vals))
+    e2e_s = float(np.mean(e2e_vals)) if e2e_vals else float("nan")
     e2e_s = slowest(e2e_s, dist, f"cuda:{dev}")
-    e2e = {"value": nodes * ws / e2e_s, "unit": UNIT,
+    e2e = {"value": nodes * ws / e2e_s if e2e_vals else None, "unit": UNIT,
            "h2d_bytes_per_step": int(ti.nbytes + di.nbytes),
            "d2h_bytes_per_step": int(di.nbytes + di.size * 4)}
 
@@ -289,10 +291,13 @@ def main():
                        "nodes_per_step": nodes, "levels": out_info["levels"], "max_batch": out_info["max_batch"],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "k_map_records",
+                         "traffic": None, "kernel": "k_map_bits" if map_kernel == "bits" else "k_map_records",
                          "algorithmic_bytes": f"4*N*L per node, N={N}, L={L}", "peak_kind": f"{peak_kind} hbm_gbs",
                          "map_ms_avg": map_avg_ms, "nodes_per_launch": nodes_per_launch,
                          "share_of_step": pinf["ms_map"] / max(pinf["ms_total"], 1e-9)},
+            "breakdown_ms": {"neighbours": pinf["ms_setup_neighbours"], "levels": pinf["ms_levels"],
+                             "prep": pinf["ms_prep"], "map": pinf["ms_map"], "replay": pinf["ms_replay"],
+                             "total": pinf["ms_total"]},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

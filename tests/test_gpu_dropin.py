@@ -15,11 +15,22 @@ QS = os.path.join(ROOT, "oracle", "_ref", "qs")
 DROPIN_DIR = os.path.join(ROOT, "g2s_b200", "dropin")
 
 
+def _cleanup(names):
+    for name in names:
+        for ext in (".bgrid", ".bgrid.gz"):
+            try:
+                os.remove(f"/tmp/G2S/data/{name}{ext}")
+            except OSError:
+                pass
+
+
 def run_qs_dropin(g, job):
     from oracle import ref
     if not (os.path.exists(QS) and os.path.exists(os.path.join(DROPIN_DIR, "g2s_cuda.so"))):
         pytest.fail("oracle/_ref/qs or g2s_b200/dropin/g2s_cuda.so missing (build them with __graft_entry__.build)")
     types = [int(t) for t in g["types"]]
+    outputs = [str(job), f"id_{job}", f"im_1_{job}", f"im_2_{job}"]
+    _cleanup(outputs)
     ref.write_image(f"dropin_ti_{job}", g["ti"], types)
     ref.write_image(f"dropin_di_{job}", g["di"], types)
     log = f"/tmp/G2S/logs/dropin_{job}.log"
@@ -30,8 +41,10 @@ def run_qs_dropin(g, job):
     assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:], text[-2000:])
     sim = ref.read_image(str(job))
     idx = ref.read_image("id_" + str(job))
+    _cleanup(outputs + [f"dropin_ti_{job}", f"dropin_di_{job}"])
     if idx.dtype != np.uint32:
         idx = idx.view(np.uint32)
+    assert sim.shape == g["di"].shape
     return sim, idx, text
 
 
@@ -47,7 +60,8 @@ def test_qs_w_cuda_equals_reference_cpu():
 def test_qs_w_cuda_equals_oracle(oracle, name):
     g = golden(name)
     types = [int(t) for t in g["types"]]
-    sim, idx, log = run_qs_dropin(g, 31002 + len(name))
+    job = {"cat2d_small": 31011, "bivar2d_small": 31012, "grf3d_small": 31013}[name]
+    sim, idx, log = run_qs_dropin(g, job)
     o = oracle.simulate(g["ti"], g["di"], types, int(g["n"]), float(g["k"]), int(g["seed"]), mode=0)
     assert np.array_equal(sim, o["sim"])
     assert np.array_equal(idx.ravel(), o["id"])
