@@ -726,6 +726,59 @@ __device__ __forceinline__ void replay_chunk(int K, bool valid, float v, int m, 
     }
 }
 
+// Steady-state fast path: every value of the state equals the K-th (so
+// xes = K and a trigger can only tie) and no candidate of the chunk exceeds
+// it.  Each tie uses two draws and increments cpt; lane ranks give both.
+template <int KM>
+__device__ __forceinline__ void replay_chunk_ties(int K, bool tie, int m, unsigned (&cp)[KM], unsigned &cpt, int &rp,
+                                                  const float *buf, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned bt = __ballot_sync(FULL, tie);
+    const int rank = __popc(bt & lanemask_lt());
+    int o[KM];
+#pragma unroll
+    for (int s = 0; s < KM; ++s) o[s] = s;
+    if (tie) {
+        const float u1 = buf[rp + 2 * rank];
+        const float u2 = buf[rp + 2 * rank + 1];
+        int x = int(floorf(__fmul_rn(u1, (float)K)));
+        if (x > K - 1) x = K - 1;
+        const unsigned after = cpt + unsigned(rank) + 1u;
+        const bool write = __fmul_rn(__uint2float_rn(unsigned(K) + after), u2) < (float)K;
+#pragma unroll
+        for (int s = 0; s < KM; ++s) {
+            if (s < K) {
+                int sig = (s == x) ? K - 1 : ((s == K - 1) ? x : s);
+                o[s] = (write && s == K - 1) ? -(m + 1) : sig;
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int later[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) later[s] = __shfl_down_sync(FULL, o[s], d);
+        if ((lane & (2 * d - 1)) == 0) {
+            int c[KM];
+#pragma unroll
+            for (int s = 0; s < KM; ++s) c[s] = later[s] < 0 ? later[s] : sel_i<KM>(o, later[s]);
+#pragma unroll
+            for (int s = 0; s < KM; ++s) o[s] = c[s];
+        }
+    }
+    unsigned np[KM];
+#pragma unroll
+    for (int s = 0; s < KM; ++s) {
+        int t = __shfl_sync(FULL, o[s], 0);
+        np[s] = t < 0 ? unsigned(-(t + 1)) : sel_u<KM>(cp, t);
+    }
+#pragma unroll
+    for (int s = 0; s < KM; ++s) cp[s] = np[s];
+    const int nt = __popc(bt);
+    cpt += unsigned(nt);
+    rp += 2 * nt;
+}
+
 template <int KM>
 __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     __shared__ WarpShared wsh[RP_WARPS];
@@ -813,7 +866,13 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                         }
                     }
                     rng_ensure(w, lane, rp, len, 64);
-                    replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
+                    // all K state values equal and nothing above them in the chunk
+                    if (!filling && sel_f<KM>(cv, 0) == kth0 &&
+                        __ballot_sync(FULL, valid && v > kth0) == 0) {
+                        replay_chunk_ties<KM>(K, valid && v == kth0, m, cp, cpt, rp, w.buf, lane);
+                    } else {
+                        replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
+                    }
                     const unsigned vb = __ballot_sync(FULL, valid);
                     last = __shfl_sync(FULL, (long long)m, 31 - __clz(vb));
                     r0 += width;
