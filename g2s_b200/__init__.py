@@ -21,7 +21,7 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libg2s_b200.so")
 
-QSK_OP_LIN, QSK_OP_SQLIN, QSK_OP_EQ = 0, 1, 2
+QSK_OP_LIN, QSK_OP_SQLIN, QSK_OP_EQ, QSK_OP_LIN_CROSS = 0, 1, 2, 3
 
 _lib = None
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -37,7 +37,11 @@ class QskTerm(ctypes.Structure):
 class QskParams(ctypes.Structure):
     _fields_ = [("ndim", ctypes.c_int), ("ti_dims", _u32p), ("nvar", ctypes.c_int), ("types", _i32p),
                 ("ti", _f32p), ("di_dims", _u32p), ("kernel_dims", _u32p), ("kernel", _f32p),
-                ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint)]
+                ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint), ("no_verbatim", ctypes.c_int)]
+
+
+class QskPatternOpts(ctypes.Structure):
+    _fields_ = [("exclude_index", ctypes.c_int), ("missing_data", ctypes.c_int), ("centre_mask_layer", ctypes.c_int)]
 
 
 class QskSimInfo(ctypes.Structure):
@@ -62,6 +66,9 @@ SIGNATURES = {
     "qsk_worker_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_pattern_kbest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
                                          ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float, _f32p, _u32p, _i32p]),
+    "qsk_pattern_kbest_ex": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
+                                            ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float,
+                                            ctypes.POINTER(QskPatternOpts), _f32p, _u32p, _i32p]),
     "qsk_pattern_kbest_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p,
                                                ctypes.POINTER(QskTerm), ctypes.c_uint, _f32p, _f32p, _u32p, _i32p]),
     "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
@@ -69,7 +76,7 @@ SIGNATURES = {
     "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,
                                       ctypes.POINTER(ctypes.c_void_p)]),
     "qsk_sim_run": (ctypes.c_int, [ctypes.c_void_p]),
-    "qsk_sim_run_teacher": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    "qsk_sim_run_teacher": (ctypes.c_int, [ctypes.c_void_p, _f32p, _u32p]),
     "qsk_sim_read": (ctypes.c_int, [ctypes.c_void_p, _f32p, _u32p, _u32p]),
     "qsk_sim_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskSimInfo)]),
     "qsk_sim_get_path": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f32p, _u32p]),
@@ -215,7 +222,8 @@ class Worker:
         _check(lib().qsk_worker_create(ti.handle, ctypes.byref(h)), "qsk_worker_create")
         self.handle = h
 
-    def pattern_kbest(self, offsets: np.ndarray, terms, k: int, seed: float):
+    def pattern_kbest(self, offsets: np.ndarray, terms, k: int, seed: float, exclude_index: int = -1,
+                      missing_data: bool = False, centre_mask_layer: int = -1):
         """offsets: (n, ndim) int; terms: list of (neighbour, layer, op, a, b).
         Returns (scores[k], scan_indices[k], min_offset[ndim])."""
         offs = np.ascontiguousarray(offsets, dtype=np.int32).reshape(-1, self.ti.ndim)
@@ -224,8 +232,14 @@ class Worker:
         sc = np.zeros(k, np.float32)
         ix = np.zeros(k, np.uint32)
         mn = np.zeros(self.ti.ndim, np.int32)
-        _check(lib().qsk_pattern_kbest(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
-                                       _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)), "qsk_pattern_kbest")
+        if exclude_index < 0 and not missing_data:
+            _check(lib().qsk_pattern_kbest(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
+                                           _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)), "qsk_pattern_kbest")
+        else:
+            opts = QskPatternOpts(int(exclude_index), int(missing_data), int(centre_mask_layer))
+            _check(lib().qsk_pattern_kbest_ex(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
+                                              ctypes.byref(opts), _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)),
+                   "qsk_pattern_kbest_ex")
         return sc, ix, mn
 
     def close(self):
@@ -244,7 +258,7 @@ class Simulation:
     """A QS vector simulation resident on one GPU."""
 
     def __init__(self, ti: np.ndarray, di: np.ndarray, types: Sequence[int], n: int, k: float, seed: int,
-                 kernel: Optional[np.ndarray] = None, device: int = 0):
+                 kernel: Optional[np.ndarray] = None, device: int = 0, no_verbatim: bool = False):
         self.nvar = len(types)
         self._ti = np.ascontiguousarray(ti, dtype=np.float32)
         self._di = np.ascontiguousarray(di, dtype=np.float32)
@@ -255,7 +269,7 @@ class Simulation:
         self._kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
         self.params = QskParams(len(self._tdims), _p(self._tdims, _u32p), self.nvar, _p(self._types, _i32p),
                                 _p(self._ti, _f32p), _p(self._ddims, _u32p), _p(self._kdims, _u32p),
-                                _p(self._kern, _f32p), int(n), float(k), int(seed) & 0xffffffff)
+                                _p(self._kern, _f32p), int(n), float(k), int(seed) & 0xffffffff, int(no_verbatim))
         h = ctypes.c_void_p()
         _check(lib().qsk_sim_create(device, ctypes.byref(self.params), _p(self._di, _f32p), ctypes.byref(h)),
                "qsk_sim_create")
@@ -270,9 +284,10 @@ class Simulation:
         _check(lib().qsk_sim_set_profiling(self.handle, int(on)), "qsk_sim_set_profiling")
         return self
 
-    def run_teacher(self, completed: np.ndarray):
+    def run_teacher(self, completed: np.ndarray, index: Optional[np.ndarray] = None):
         c = np.ascontiguousarray(completed, dtype=np.float32)
-        _check(lib().qsk_sim_run_teacher(self.handle, _p(c, _f32p)), "qsk_sim_run_teacher")
+        ix = None if index is None else np.ascontiguousarray(index, dtype=np.uint32).ravel()
+        _check(lib().qsk_sim_run_teacher(self.handle, _p(c, _f32p), _p(ix, _u32p)), "qsk_sim_run_teacher")
         return self
 
     def info(self) -> dict:
@@ -312,10 +327,10 @@ class Simulation:
 
 
 def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n: int, s: int,
-       ki: Optional[np.ndarray] = None, device: int = 0):
+       ki: Optional[np.ndarray] = None, nV: bool = False, device: int = 0):
     """QuickSampling on one GPU; arguments named after the G2S flags
-    (-ti -di -dt -k -n -s -ki).  Returns (simulation, index) as G2S does."""
-    sim = Simulation(ti, di, dt, n=n, k=k, seed=s, kernel=ki, device=device)
+    (-ti -di -dt -k -n -s -ki -nV).  Returns (simulation, index) as G2S does."""
+    sim = Simulation(ti, di, dt, n=n, k=k, seed=s, kernel=ki, device=device, no_verbatim=nV)
     try:
         sim.run()
         out, idx, _ = sim.read()

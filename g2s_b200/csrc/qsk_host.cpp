@@ -140,6 +140,10 @@ struct qsk_ti {
     DBuf<float> grid;             // raw TI (grid-built): cells * nvar
     DBuf<int> dtypes;
     long long cells = 0;
+    // missing values (grid-built): cells with any NaN variable are all-NaN, an
+    // extra mask layer (index nvar) and complete-cell prefix counts
+    bool missing = false;
+    DBuf<int> complete_prefix;
     // bit planes of categorical variables (grid-built, every variable categorical
     // with at most QSK_CMAX categories)
     bool planes_ok = false;
@@ -186,13 +190,15 @@ cudaError_t ensure_records(const Geom &g, int nslots, DBuf<float> &rv, DBuf<int>
 
 // host-side slot/terms for one explicit pattern
 int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms, const qsk_term *terms, unsigned K,
-                       float seed, int node, Slot &s, std::vector<Term> &out, int *out_min) {
+                       float seed, int node, Slot &s, std::vector<Term> &out, int *out_min,
+                       const qsk_pattern_opts *opts = nullptr) {
     const Geom &g = ti->g;
     const int nd = g.nd;
     std::memset(&s, 0, sizeof(s));
     s.node = node;
     s.seed = seed;
     s.sel = 0;
+    s.excl = -1;
     int mn[QSK_MAXD] = {0}, mx[QSK_MAXD] = {0};
     for (int j = 0; j < nnb; ++j)
         for (int d = 0; d < nd; ++d) {
@@ -217,10 +223,21 @@ int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms
         return QSK_OK;
     }
     if (nvalid < (long long)K) s.flags |= SLOT_EMIT_MASKED;
+    if (opts) {
+        if (opts->exclude_index >= 0 && (long long)opts->exclude_index < g.N) s.excl = opts->exclude_index;
+        if (opts->missing_data) {
+            if (opts->centre_mask_layer < 0 || opts->centre_mask_layer >= ti->nlayers)
+                return fail(QSK_ERR_ARG, "centre_mask_layer %d out of range", opts->centre_mask_layer);
+            s.flags |= SLOT_MISSING;
+            long long fmn = 0;
+            for (int d = 0; d < nd; ++d) fmn += (long long)mn[d] * g.sstride[d];
+            s.cmask_base = int((long long)opts->centre_mask_layer * g.N + fmn);
+        }
+    }
     out.clear();
     for (int t = 0; t < nterms; ++t) {
         const qsk_term &q = terms[t];
-        if (q.neighbour < 0 || q.neighbour >= nnb || q.layer < 0 || q.layer >= ti->nlayers || q.op < 0 || q.op > 2)
+        if (q.neighbour < 0 || q.neighbour >= nnb || q.layer < 0 || q.layer >= ti->nlayers || q.op < 0 || q.op > 3)
             return fail(QSK_ERR_ARG, "pattern term %d out of range", t);
         long long dflat = 0;
         for (int d = 0; d < nd; ++d) dflat += (long long)(offsets[q.neighbour * nd + d] - mn[d]) * g.sstride[d];
@@ -228,7 +245,7 @@ int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms
         tm.base = int((long long)q.layer * g.N - dflat);
         tm.a = q.a;
         tm.b = q.b;
-        tm.op = q.op;
+        tm.op = q.op == QSK_OP_LIN_CROSS ? OP_LINX : q.op;
         out.push_back(tm);
     }
     s.nterms = int(out.size());
@@ -292,22 +309,43 @@ int qsk_ti_create_layers(int device, int ndim, const unsigned *src_size, const u
 }
 
 static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int nvar, const int *types,
-                               const float *data, bool data_on_device, qsk_ti **out) {
-    if (!out || !dims || !types || !data || nvar < 1) return fail(QSK_ERR_ARG, "null argument");
+                               const float *data_in, bool data_on_device, qsk_ti **out) {
+    if (!out || !dims || !types || !data_in || nvar < 1) return fail(QSK_ERR_ARG, "null argument");
     if (nvar > 4) return fail(QSK_ERR_UNSUPPORTED, "at most 4 variables (got %d)", nvar);
+    if (data_on_device) return fail(QSK_ERR_UNSUPPORTED, "device-resident TI");
     std::vector<unsigned> fft(ndim);
     for (int d = 0; d < ndim && d < QSK_MAXD; ++d) fft[d] = fft_size_for(dims[d]);
-    int rc = check_sizes(ndim, dims, fft.data(), nvar);
+    int rc = check_sizes(ndim, dims, fft.data(), nvar + 1);
     if (rc) return rc;
+    long long cells = 1;
+    for (int d = 0; d < ndim; ++d) cells *= dims[d];
+    // missing values: for vector simulation a cell with any NaN variable is
+    // treated as missing in every variable (src/qs.cpp:1436-1467)
+    std::vector<float> data(data_in, data_in + size_t(cells) * nvar);
+    bool missing = false;
+    for (long long c = 0; c < cells; ++c) {
+        bool hasNan = false;
+        for (int v = 0; v < nvar; ++v) hasNan |= std::isnan(data[size_t(c) * nvar + v]);
+        if (hasNan) {
+            missing = true;
+            for (int v = 0; v < nvar; ++v) data[size_t(c) * nvar + v] = NAN;
+        }
+    }
+    if (missing)
+        for (int v = 0; v < nvar; ++v)
+            if (types[v] != 0)
+                return fail(QSK_ERR_UNSUPPORTED,
+                            "categorical variables with missing training-image values are undefined in G2S "
+                            "(its converted neighbour values misalign, quantileSamplingModule.hpp:368-410)");
     DeviceGuard dgd(device);
     qsk_ti *t = new qsk_ti();
     t->device = device;
     t->g = make_geom(ndim, dims, fft.data());
-    t->nlayers = nvar;
+    t->missing = missing;
+    t->nlayers = nvar + (missing ? 1 : 0);
     t->nvar = nvar;
     t->types.assign(types, types + nvar);
-    t->cells = 1;
-    for (int d = 0; d < ndim; ++d) t->cells *= dims[d];
+    t->cells = cells;
     auto bail = [&](cudaError_t e) {
         delete t;
         return fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "ti upload: %s",
@@ -315,39 +353,47 @@ static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int n
     };
     cudaError_t e;
     if ((e = t->grid.alloc(size_t(t->cells) * nvar)) != cudaSuccess) return bail(e);
-    if ((e = cudaMemcpy(t->grid.p, data, sizeof(float) * t->cells * nvar,
-                        data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice)) != cudaSuccess)
+    if ((e = cudaMemcpy(t->grid.p, data.data(), sizeof(float) * t->cells * nvar, cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(e);
     if ((e = t->dtypes.alloc(nvar)) != cudaSuccess) return bail(e);
     if ((e = cudaMemcpy(t->dtypes.p, types, sizeof(int) * nvar, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
-    if ((e = t->layers.alloc(size_t(nvar) * t->g.N)) != cudaSuccess) return bail(e);
-    if ((e = launch_build_layers(t->grid.p, nvar, t->dtypes.p, t->g, t->layers.p, 0)) != cudaSuccess) return bail(e);
+    if ((e = t->layers.alloc(size_t(t->nlayers) * t->g.N)) != cudaSuccess) return bail(e);
+    if ((e = launch_build_layers(t->grid.p, nvar, t->dtypes.p, t->g, t->layers.p, missing ? 1 : 0, 0)) != cudaSuccess)
+        return bail(e);
+    if (missing) {
+        std::vector<int> prefix(static_cast<size_t>(cells));
+        int run = 0;
+        for (long long c = 0; c < cells; ++c) {
+            run += std::isnan(data[size_t(c) * nvar]) ? 0 : 1;
+            prefix[size_t(c)] = run;
+        }
+        if ((e = t->complete_prefix.alloc(size_t(cells))) != cudaSuccess) return bail(e);
+        if ((e = cudaMemcpy(t->complete_prefix.p, prefix.data(), sizeof(int) * cells, cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return bail(e);
+    }
     // categories (distinct non-NaN codes) of categorical variables, for the bit planes
-    bool all_cat = true;
+    bool all_cat = !missing;
     std::vector<int> ncat(nvar, 0);
     std::vector<float> catv(size_t(nvar) * QSK_CMAX, 0.f);
-    if (!data_on_device) {
-        for (int v = 0; v < nvar && all_cat; ++v) {
-            if (types[v] != 1) { all_cat = false; break; }
-            for (long long i = 0; i < t->cells && all_cat; ++i) {
-                float x = data[i * nvar + v];
-                if (std::isnan(x)) continue;
-                bool seen = false;
-                for (int q = 0; q < ncat[v]; ++q) seen |= (catv[size_t(v) * QSK_CMAX + q] == x);
-                if (!seen) {
-                    if (ncat[v] == QSK_CMAX) all_cat = false;
-                    else catv[size_t(v) * QSK_CMAX + ncat[v]++] = x;
-                }
+    for (int v = 0; v < nvar && all_cat; ++v) {
+        if (types[v] != 1) { all_cat = false; break; }
+        for (long long i = 0; i < t->cells && all_cat; ++i) {
+            float x = data[size_t(i) * nvar + v];
+            if (std::isnan(x)) continue;
+            bool seen = false;
+            for (int q = 0; q < ncat[v]; ++q) seen |= (catv[size_t(v) * QSK_CMAX + q] == x);
+            if (!seen) {
+                if (ncat[v] == QSK_CMAX) all_cat = false;
+                else catv[size_t(v) * QSK_CMAX + ncat[v]++] = x;
             }
         }
-    } else {
-        all_cat = false;
     }
     if (all_cat) {
         t->pw = int((t->g.N + 31) / 32) + 2;
         if ((e = t->ncat.alloc(nvar)) != cudaSuccess) return bail(e);
         if ((e = t->catv.alloc(catv.size())) != cudaSuccess) return bail(e);
-        if ((e = t->planes.alloc(size_t(nvar) * QSK_CMAX * t->pw)) != cudaSuccess) return bail(e);
+        if ((e = t->planes.alloc(size_t(nvar) * (QSK_CMAX + 1) * t->pw)) != cudaSuccess) return bail(e);
         if ((e = cudaMemcpy(t->ncat.p, ncat.data(), sizeof(int) * nvar, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e);
         if ((e = cudaMemcpy(t->catv.p, catv.data(), sizeof(float) * catv.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return bail(e);
@@ -400,9 +446,9 @@ int qsk_worker_destroy(qsk_worker *w) {
     return QSK_OK;
 }
 
-int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
-                            const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
-                            unsigned *out_index, int *out_min) {
+static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                              const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
+                              unsigned *out_index, int *out_min, const qsk_pattern_opts *opts) {
     if (!w || B < 0 || !nb_ptr || !term_ptr || !seeds || !out_score || !out_index) return fail(QSK_ERR_ARG, "null argument");
     if (k < 1 || k > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "k=%u outside [1,%d]", k, QSK_KMAX);
     if (B == 0) return QSK_OK;
@@ -420,7 +466,7 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
         int nnb = nb_ptr[b + 1] - nb_ptr[b];
         int nt = term_ptr[b + 1] - term_ptr[b];
         int rc = build_pattern_slot(ti, nnb, offsets + size_t(nb_ptr[b]) * nd, nt, terms + term_ptr[b], k, seeds[b], b,
-                                    w->h_slots[b], tmp, out_min ? out_min + size_t(b) * nd : nullptr);
+                                    w->h_slots[b], tmp, out_min ? out_min + size_t(b) * nd : nullptr, opts);
         if (rc) return rc;
         std::copy(tmp.begin(), tmp.end(), w->h_terms.begin() + size_t(b) * maxterms);
     }
@@ -434,7 +480,7 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt, w->rec_max));
     CK(w->out_val.ensure(size_t(B) * k));
     CK(w->out_pos.ensure(size_t(B) * k));
-    bool bits = ti->planes_ok && g_map_mode == 0 && maxterms <= 255;
+    bool bits = ti->planes_ok && g_map_mode == 0 && maxterms <= 255 && !opts;
     for (size_t i = 0; i < w->h_terms.size() && bits; ++i) {
         int b = int(i / maxterms), t = int(i % maxterms);
         if (t >= w->h_slots[b].nterms) continue;
@@ -496,11 +542,26 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
     return QSK_OK;
 }
 
+int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                            const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
+                            unsigned *out_index, int *out_min) {
+    return pattern_batch_impl(w, B, nb_ptr, offsets, term_ptr, terms, k, seeds, out_score, out_index, out_min, nullptr);
+}
+
 int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
                       unsigned k, float seed, float *out_score, unsigned *out_index, int *out_min) {
     int nb_ptr[2] = {0, n_neighbours};
     int term_ptr[2] = {0, n_terms};
-    return qsk_pattern_kbest_batch(w, 1, nb_ptr, offsets, term_ptr, terms, k, &seed, out_score, out_index, out_min);
+    return pattern_batch_impl(w, 1, nb_ptr, offsets, term_ptr, terms, k, &seed, out_score, out_index, out_min,
+                              nullptr);
+}
+
+int qsk_pattern_kbest_ex(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
+                         unsigned k, float seed, const qsk_pattern_opts *opts, float *out_score, unsigned *out_index,
+                         int *out_min) {
+    int nb_ptr[2] = {0, n_neighbours};
+    int term_ptr[2] = {0, n_terms};
+    return pattern_batch_impl(w, 1, nb_ptr, offsets, term_ptr, terms, k, &seed, out_score, out_index, out_min, opts);
 }
 
 unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index) {
@@ -540,6 +601,7 @@ struct qsk_sim {
     int nd = 0, nvar = 0, n = 0, K = 1;
     float k = 1.f;
     unsigned seed = 0;
+    int no_verbatim = 0;
     GridDesc dg;
     long long cells = 0, nodes = 0;
     unsigned begin = 0;
@@ -556,7 +618,7 @@ struct qsk_sim {
     DBuf<int> d_tpl, d_types;
     DBuf<float> d_wtab, d_seeds, d_init, d_state;
     DBuf<unsigned> d_path, d_post, d_id, d_node_cell, d_nb_cell;
-    DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_level, d_maxlevel, d_hist, d_start, d_cursor, d_level_nodes,
+    DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_dep, d_level, d_maxlevel, d_hist, d_start, d_cursor, d_level_nodes,
         d_status;
     DBuf<Slot> d_slots;
     DBuf<Term> d_terms;
@@ -739,6 +801,10 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             pa.terms = s->d_terms.p;
             pa.maxterms = s->maxterms;
             pa.status = s->d_status.p;
+            pa.missing = s->ti->missing ? 1 : 0;
+            pa.mask_layer = s->nvar;
+            pa.no_verbatim = s->no_verbatim;
+            pa.id_image = s->d_id.p;
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
@@ -789,6 +855,7 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.nvar = s->nvar;
             ra.ti = s->ti->grid.p;
             ra.ti_cells = s->ti->cells;
+            ra.complete_prefix = s->ti->missing ? s->ti->complete_prefix.p : nullptr;
             ra.nti = 1;
             ra.ti_id = 0;
             ra.state = teacher ? nullptr : s->d_state.p;
@@ -848,6 +915,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     s->k = p->k;
     s->K = K;
     s->seed = p->seed;
+    s->no_verbatim = p->no_verbatim;
     auto bail = [&](int rc) {
         qsk_sim_destroy(s);
         return rc;
@@ -879,7 +947,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         build_template(s, kd.data(), nullptr);
     }
     build_path(s);
-    s->maxterms = std::max(1, s->n * s->nvar);
+    s->maxterms = std::max(1, s->n * s->nvar * (s->ti->missing ? 2 : 1));
     // bit-sliced map: every variable categorical with bit planes, unit weights
     s->use_bits = s->ti->planes_ok && s->maxterms <= 255;
     for (float wv : s->wtab) s->use_bits &= (wv == 1.f);
@@ -897,6 +965,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_nb_count.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_nb_tpl.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
         (e = s->d_nb_cell.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
+        (e = s->d_dep.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
         (e = s->d_level.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_level_nodes.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_maxlevel.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess)
@@ -944,9 +1013,9 @@ int qsk_sim_run(qsk_sim *s) {
     if (rc) return rc;
     CK(cudaEventRecord(ev[1], s->st));
     CK(cudaMemsetAsync(s->d_maxlevel.p, 0, sizeof(int), s->st));
-    CK(launch_levels(s->nodes, s->n, s->d_nb_count.p, s->d_nb_cell.p, s->d_node_of_cell.p, s->d_level.p,
+    CK(launch_levels(s->nodes, s->n, s->d_nb_count.p, s->d_nb_cell.p, s->d_node_of_cell.p, s->d_dep.p, s->d_level.p,
                      s->d_maxlevel.p, s->st));
-    s->info.launches += 2;  // neighbours + levels
+    s->info.launches += 3;  // neighbours + dependency nodes + levels
     int maxl = 0;
     CK(cudaMemcpyAsync(&maxl, s->d_maxlevel.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -981,10 +1050,15 @@ int qsk_sim_run(qsk_sim *s) {
     return sim_check_status(s);
 }
 
-int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed) {
+int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *id_completed) {
     if (!s || !di_completed) return fail(QSK_ERR_ARG, "null argument");
+    if (s->no_verbatim && !id_completed) return fail(QSK_ERR_ARG, "-nV teacher forcing needs the index image");
     DeviceGuard dgd(s->device);
     CK(cudaMemcpyAsync(s->d_state.p, di_completed, sizeof(float) * s->init.size(), cudaMemcpyHostToDevice, s->st));
+    if (id_completed)
+        CK(cudaMemcpyAsync(s->d_id.p, id_completed, sizeof(unsigned) * s->cells, cudaMemcpyHostToDevice, s->st));
+    else
+        CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells, s->st));
     CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
     int rc = sim_neighbours(s);
     if (rc) return rc;

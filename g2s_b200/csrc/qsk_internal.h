@@ -18,6 +18,12 @@ enum TermOp : int {
     OP_LIN = 0,    // acc = fma(a, x, acc)
     OP_SQLIN = 1,  // acc = fma(a, x*x, acc); acc = fma(b, x, acc)   (continuous variable)
     OP_EQ = 2,     // acc = (x == b) ? acc + a : acc                  (categorical variable)
+    OP_LINX = 3,   // cross = fma(a, x, cross)                       (overlap output, missing data)
+    OP_SQLINM = 4, // missing data: mask = !isnan(x), x0 = mask ? x : 0:
+                   //   acc = fma(a, x0*x0, acc); acc = fma(b, x0, acc);
+                   //   acc = fma(next.a, mask, acc); cross = fma(next.b, mask, cross)
+                   // (the next term carries the two mask coefficients and is skipped)
+    OP_NOP = 5,    // payload of the previous term
 };
 
 struct Term {
@@ -48,11 +54,14 @@ struct Slot {
     int sel;                 // drawn candidate rank
     int flags;               // SLOT_* bits
     unsigned cell;           // DI cell (simulation)
+    int excl;                // scan index forced to -inf (-nV), -1 for none
+    int cmask_base;          // missing data: centre-mask layer address minus m
 };
 
 enum SlotFlags : int {
     SLOT_SKIP = 1,           // no map: marginal draw or empty pattern
     SLOT_EMIT_MASKED = 2,    // fewer than K valid positions: masked entries are candidates too
+    SLOT_MISSING = 4,        // TI with missing values: score -|S/c^4| with the overlap c, border NaN
 };
 
 // Status words written by kernels (bounded waits / argument checks).
@@ -94,6 +103,10 @@ struct SimPrepArgs {
     Term *terms;
     int maxterms;
     int *status;
+    int missing;           // TI with missing values (terms OP_SQLINM + payload)
+    int mask_layer;        // layer index of the TI mask (missing data)
+    int no_verbatim;       // -nV
+    const unsigned *id_image;  // index image of the grid (-nV)
 };
 
 struct MapArgs {
@@ -111,7 +124,7 @@ struct MapArgs {
 
 struct BitArgs {
     Geom g;
-    const unsigned *planes;   // [var][QSK_CMAX][pw] words
+    const unsigned *planes;   // [var][QSK_CMAX+1][pw] words (slot QSK_CMAX all zero)
     int pw;                   // words per plane (ceil(N/32) + 2)
     const int *ncat;          // categories per variable
     const float *catv;        // [var][QSK_CMAX] category codes
@@ -142,6 +155,7 @@ struct ReplayArgs {
     const float *ti;      // TI grid (cells x nvar)
     long long ti_cells;
     unsigned nti, ti_id;
+    const int *complete_prefix;  // missing data: complete TI cells in [0..c]; null for a complete TI
     float *state;         // grid written in simulation mode (null in teacher-forced mode)
     unsigned *id_image;   // per grid cell
     unsigned *node_cell;  // per path index: chosen TI cell
@@ -149,13 +163,13 @@ struct ReplayArgs {
 
 
 // launch wrappers (qsk_kernels.cu)
-cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers,
+cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers, int missing,
                                 cudaStream_t st);
 cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
                               unsigned *nb_cell, cudaStream_t st);
 cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
-                          const int *node_of_cell, int *level, int *max_level, cudaStream_t st);
+                          const int *node_of_cell, int *dep, int *level, int *max_level, cudaStream_t st);
 cudaError_t launch_level_sort(long long nodes, int nl, const int *level, int *hist, int *start, int *cursor,
                               int *level_nodes, cudaStream_t st);
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);

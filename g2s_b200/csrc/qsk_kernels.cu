@@ -77,7 +77,7 @@ __device__ long long valid_prefix(const Geom &g, const int *lo, long long x) {
 // outside the TI hold 0 (continuous) / NaN (categorical).
 // ---------------------------------------------------------------------------
 __global__ void k_build_layers(const float *__restrict__ ti, int nvar, const int *__restrict__ types, Geom g,
-                               float *__restrict__ layers) {
+                               float *__restrict__ layers, int missing) {
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= g.N) return;
     // q is an fft-grid flat index of the flipped array: coord = fft-1-digit
@@ -94,11 +94,15 @@ __global__ void k_build_layers(const float *__restrict__ ti, int nvar, const int
         float x;
         if (inside) {
             x = ti[src_flat * nvar + v];
-            if (types[v] == 0 && isnan(x)) x = 0.f;
+            if (types[v] == 0 && isnan(x) && !missing) x = 0.f;
         } else {
             x = types[v] == 0 ? 0.f : CUDART_NAN_F;
         }
         layers[(long long)v * g.N + q] = x;
+    }
+    if (missing) {
+        // mask layer (DataImage.hpp:582-595): 1 where the TI cell is informed
+        layers[(long long)nvar * g.N + q] = (inside && !isnan(ti[src_flat * nvar])) ? 1.f : 0.f;
     }
 }
 
@@ -144,29 +148,50 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
 // neighbours j that are themselves path nodes.  One block walks the path in
 // chunks of blockDim nodes; inside a chunk it relaxes until nothing changes.
 // ---------------------------------------------------------------------------
-__global__ void k_levels(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                         const int *__restrict__ node_of_cell, int *__restrict__ level, int *__restrict__ max_level) {
+// dependency node of each neighbour slot (-1: none / the node itself)
+__global__ void k_dep_nodes(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
+                            const int *__restrict__ node_of_cell, int *__restrict__ dep) {
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nodes * n) return;
+    long long i = idx / n;
+    int j = int(idx % n);
+    int dn = -1;
+    if (j < nb_count[i]) {
+        dn = node_of_cell[nb_cell[idx]];
+        if ((long long)dn == i) dn = -1;
+    }
+    dep[idx] = dn;
+}
+
+__global__ void k_levels(long long nodes, int n, const int *__restrict__ dep, int *__restrict__ level,
+                         int *__restrict__ max_level) {
     __shared__ int changed;
     int mx = 0;
     for (long long c0 = 0; c0 < nodes; c0 += blockDim.x) {
-        long long i = c0 + threadIdx.x;
-        bool active = i < nodes;
-        if (active) level[i] = 0;
+        const long long i = c0 + threadIdx.x;
+        const bool active = i < nodes;
+        int L = 0;
+        // dependencies before this chunk are final: one pass over them
+        if (active) {
+            for (int j = 0; j < n; ++j) {
+                const int dn = dep[i * n + j];
+                if (dn >= 0 && dn < c0) L = max(L, level[dn] + 1);
+            }
+            level[i] = L;
+        }
         __syncthreads();
+        // dependencies inside the chunk: relax to the fixed point
         for (;;) {
             if (threadIdx.x == 0) changed = 0;
             __syncthreads();
             if (active) {
-                int L = 0;
-                int cnt = nb_count[i];
-                for (int j = 0; j < cnt; ++j) {
-                    int dn = node_of_cell[nb_cell[i * n + j]];
-                    if (dn >= 0 && (long long)dn != i) {
-                        int lj = ((volatile int *)level)[dn] + 1;
-                        L = L > lj ? L : lj;
-                    }
+                int L2 = L;
+                for (int j = 0; j < n; ++j) {
+                    const int dn = dep[i * n + j];
+                    if (dn >= c0) L2 = max(L2, ((volatile int *)level)[dn] + 1);
                 }
-                if (L != ((volatile int *)level)[i]) {
+                if (L2 != L) {
+                    L = L2;
                     ((volatile int *)level)[i] = L;
                     changed = 1;
                 }
@@ -175,7 +200,7 @@ __global__ void k_levels(long long nodes, int n, const int *__restrict__ nb_coun
             if (!changed) break;
             __syncthreads();
         }
-        if (active) mx = mx > level[i] ? mx : level[i];
+        if (active) mx = mx > L ? mx : L;
     }
     atomicMax(max_level, mx);
 }
@@ -234,6 +259,8 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     if (s.sel > A.K - 1) s.sel = A.K - 1;   // unreachable for seeds in [0,1)
     s.flags = 0;
     s.nterms = 0;
+    s.excl = -1;
+    s.cmask_base = 0;
     bool centreData = false;
     for (int v = 0; v < A.nvar; ++v) centreData |= !isnan(A.init[(long long)cell * A.nvar + v]);
     // min / max of the neighbour offsets, starting from 0 (AcceleratorDevice.cpp:95-112)
@@ -274,7 +301,7 @@ __global__ void k_prep_sim(SimPrepArgs A) {
         int base_out = 0;
         for (int j0 = 0; j0 < cnt; j0 += 32) {
             int j = j0 + lane;
-            Term tl[4];
+            Term tl[8];
             int nt = 0;
             if (j < cnt) {
                 int t = A.nb_tpl[(long long)i * A.n + j];
@@ -287,6 +314,20 @@ __global__ void k_prep_sim(SimPrepArgs A) {
                     if (isnan(val) || w == 0.f) continue;
                     Term tm;
                     tm.base = int((long long)v * A.g.N - d_flat);
+                    if (A.types[v] == 0 && A.missing) {
+                        // regular output: -w TI^2 + 2wv TI - ((w v) v) mask; overlap: w mask
+                        tm.op = OP_SQLINM;
+                        tm.a = -w;
+                        tm.b = 2.f * __fmul_rn(w, val);
+                        tl[nt++] = tm;
+                        Term pl;
+                        pl.base = tm.base;
+                        pl.op = OP_NOP;
+                        pl.a = -__fmul_rn(__fmul_rn(w, val), val);
+                        pl.b = w;
+                        tl[nt++] = pl;
+                        continue;
+                    }
                     if (A.types[v] == 0) {
                         tm.op = OP_SQLIN;
                         tm.a = -w;
@@ -318,6 +359,37 @@ __global__ void k_prep_sim(SimPrepArgs A) {
             base_out = A.maxterms;
         }
         s.nterms = base_out;
+        if (A.missing) {
+            s.flags |= SLOT_MISSING;
+            long long fmn = 0;
+            for (int d = 0; d < nd; ++d) fmn += (long long)mn[d] * A.g.sstride[d];
+            s.cmask_base = int((long long)A.mask_layer * A.g.N + fmn);
+        }
+        if (A.no_verbatim && cnt > 1) {
+            // the TI cell continuing neighbour 1's source is excluded
+            // (simulation.hpp:556-583, quantileSamplingModule.hpp:518-523)
+            const int t1 = A.nb_tpl[(long long)i * A.n + 1];
+            const unsigned c1 = A.nb_cell[(long long)i * A.n + 1];
+            unsigned src = A.id_image[c1];
+            long long pf = 0, st = 1;
+            for (int d = 0; d < nd; ++d) {
+                int dim = A.g.src[d];
+                int c = int(src % (unsigned)dim) - A.tpl[t1 * nd + d];
+                src /= (unsigned)dim;
+                c = ((c % dim) + dim) % dim;
+                pf += (long long)c * st;
+                st *= dim;
+            }
+            // cvtPositionToIndex (CPUThreadDevice.cpp:270-284), unsigned arithmetic
+            unsigned position = (unsigned)pf, index = 0, div = 1;
+            for (int d = nd - 1; d >= 0; --d) div *= (unsigned)A.g.src[d];
+            for (int d = nd - 1; d >= 0; --d) {
+                unsigned f = (unsigned)A.g.fft[d], sr = (unsigned)A.g.src[d];
+                div /= sr;
+                index = index * f + (f - (position / div + (unsigned)mn[d]) % sr - 1u);
+            }
+            s.excl = index < (unsigned)A.g.N ? int(index) : -1;
+        }
     }
     if (lane == 0) A.slots[warp] = s;
 }
@@ -379,6 +451,9 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
             mm[r] = ok ? m : usafe;
             acc[r] = 0.f;
         }
+        float crs[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) crs[r] = 0.f;
         for (int t = 0; t < nt_eff; ++t) {
             const Term tm = sterm[t];
             const float *lp = A.layers + tm.base;
@@ -394,10 +469,45 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
             } else if (tm.op == OP_EQ) {
 #pragma unroll
                 for (int r = 0; r < 4; ++r) acc[r] = (x[r] == tm.b) ? __fadd_rn(acc[r], tm.a) : acc[r];
-            } else {
+            } else if (tm.op == OP_LIN) {
 #pragma unroll
                 for (int r = 0; r < 4; ++r) acc[r] = __fmaf_rn(tm.a, x[r], acc[r]);
+            } else if (tm.op == OP_LINX) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) crs[r] = __fmaf_rn(tm.a, x[r], crs[r]);
+            } else if (tm.op == OP_SQLINM) {
+                const Term pl = sterm[t + 1];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const bool in = !isnan(x[r]);
+                    const float x0 = in ? x[r] : 0.f;
+                    const float mk = in ? 1.f : 0.f;
+                    acc[r] = __fmaf_rn(tm.a, __fmul_rn(x0, x0), acc[r]);
+                    acc[r] = __fmaf_rn(tm.b, x0, acc[r]);
+                    acc[r] = __fmaf_rn(pl.a, mk, acc[r]);
+                    crs[r] = __fmaf_rn(pl.b, mk, crs[r]);
+                }
+                ++t;
             }
+        }
+        if (ss.flags & SLOT_MISSING) {
+            // overlap masked by the centre, then -|S/c^4| (-inf where c == 0);
+            // positions outside the border are NaN in the reference
+            // (quantileSamplingModule.hpp:507-516, CPUThreadDevice.cpp:501-524)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const float cm = valid[r] ? __ldg(A.layers + ss.cmask_base + (long long)mm[r]) : 0.f;
+                const float c = __fmul_rn(crs[r], cm);
+                const float c4 = __fmul_rn(__fmul_rn(__fmul_rn(c, c), c), c);
+                float e = -fabsf(__fdiv_rn(acc[r], c4));
+                if (c == 0.f) e = -CUDART_INF_F;
+                acc[r] = valid[r] ? e : CUDART_NAN_F;
+            }
+        }
+        if (ss.excl >= 0) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if ((int)(base + 32 * r + lane) == ss.excl && valid[r]) acc[r] = -CUDART_INF_F;
         }
         // warp prefix top-KF over the segment in scan order; records are the
         // positions not below the K-th best of everything before them in the
@@ -409,7 +519,7 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
         float segmax = -CUDART_INF_F;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const float xval = valid[r] ? acc[r] : -CUDART_INF_F;
+            const float xval = valid[r] ? acc[r] : ((ss.flags & SLOT_MISSING) ? CUDART_NAN_F : -CUDART_INF_F);
             segmax = fmaxf(segmax, xval);
             float st[KF];
             st[0] = xval;
@@ -804,6 +914,25 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
             chosen_cell = unsigned(int(floor((double)__fmul_rn(s.seed, __uint2float_rn((unsigned)A.ti_cells)))));
             // float rounding of seed*cells can reach `cells` only for grids above 2^24 cells
             if ((long long)chosen_cell >= A.ti_cells) chosen_cell = (unsigned)(A.ti_cells - 1);
+            if (A.complete_prefix) {
+                bool hasNaN = false;
+                for (int v = 0; v < A.nvar; ++v) hasNaN |= isnan(A.ti[(long long)chosen_cell * A.nvar + v]);
+                if (hasNaN) {
+                    // NaN-safe draw (simulation.hpp:616-652): the first cell whose
+                    // running count of complete cells reaches floor(seed*(complete/nvar))*nvar
+                    const unsigned complete = (unsigned)A.complete_prefix[A.ti_cells - 1];
+                    const unsigned pos2 = unsigned(int(floor((double)__fmul_rn(
+                                              s.seed, __uint2float_rn(complete / (unsigned)A.nvar))))) *
+                                          (unsigned)A.nvar;
+                    long long lo2 = 0, hi2 = A.ti_cells;   // first index with prefix >= pos2
+                    while (lo2 < hi2) {
+                        long long mid = (lo2 + hi2) >> 1;
+                        if ((unsigned)A.complete_prefix[mid] < pos2) lo2 = mid + 1;
+                        else hi2 = mid;
+                    }
+                    chosen_cell = (unsigned)(lo2 < A.ti_cells ? lo2 : A.ti_cells - 1);
+                }
+            }
             have = true;
         }
     } else {
@@ -824,7 +953,7 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
         int rp = 0, len = 0;
         unsigned cpt = 0;
         long long last = -1;
-        const bool emit_masked = (s.flags & SLOT_EMIT_MASKED) != 0;
+        const bool emit_masked = (s.flags & (SLOT_EMIT_MASKED | SLOT_MISSING)) != 0;
         const float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
         const int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
         const int *rc = A.rec_cnt + (long long)b * g.nseg;
@@ -961,11 +1090,11 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
 __global__ void k_build_planes(const float *__restrict__ layers, Geom g, int nvar, const int *__restrict__ ncat,
                                const float *__restrict__ catv, int pw, unsigned *__restrict__ planes) {
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    long long total = (long long)nvar * QSK_CMAX * pw;
+    long long total = (long long)nvar * (QSK_CMAX + 1) * pw;
     if (idx >= total) return;
     int w = int(idx % pw);
     int vc = int(idx / pw);
-    int c = vc % QSK_CMAX, v = vc / QSK_CMAX;
+    int c = vc % (QSK_CMAX + 1), v = vc / (QSK_CMAX + 1);
     unsigned word = 0;
     if (c < ncat[v]) {
         float cv = catv[v * QSK_CMAX + c];
@@ -998,23 +1127,23 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
     __syncthreads();
     if (ss.flags & SLOT_SKIP) return;
     const Geom &g = A.g;
-    if (threadIdx.x == 0) {
-        // terms -> (plane offset, flat offset); a code that is no category of
-        // the TI never matches and is dropped
+    {
+        // terms -> (plane offset, flat offset), one thread per term; a code that
+        // is no category of the TI reads the all-zero plane QSK_CMAX
         const Term *src = A.terms + (long long)b * A.maxterms;
-        int k = 0;
-        for (int t = 0; t < ss.nterms; ++t) {
+        const int N32 = (int)g.N;
+        for (int t = threadIdx.x; t < ss.nterms; t += blockDim.x) {
             const Term tm = src[t];
-            long long base = tm.base;
-            int v = int((base + g.N - 1) / g.N);   // base = v*N - d with 0 <= d < N
-            if (base <= 0) v = 0;
-            long long d = (long long)v * g.N - base;
-            int c = -1;
-            for (int q = 0; q < A.ncat[v]; ++q)
+            const int base = tm.base;   // v*N - d with 0 <= d < N
+            const int v = base > 0 ? (base + N32 - 1) / N32 : 0;
+            const int d = v * N32 - base;
+            int c = QSK_CMAX;
+            const int nc = A.ncat[v];
+            for (int q = 0; q < nc; ++q)
                 if (A.catv[v * QSK_CMAX + q] == tm.b) { c = q; break; }
-            if (c >= 0) bterm[k++] = make_int2((v * QSK_CMAX + c) * A.pw, int(d));
+            bterm[t] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw, d);
         }
-        nbt = k;
+        if (threadIdx.x == 0) nbt = ss.nterms;
     }
     __syncthreads();
     const int nt = nbt;
@@ -1114,6 +1243,7 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                            (((c3 >> bit) & 1u) << 3) | (((c4 >> bit) & 1u) << 4) | (((c5 >> bit) & 1u) << 5) |
                            (((c6 >> bit) & 1u) << 6) | (((c7 >> bit) & 1u) << 7);
             float x = ((vmask >> bit) & 1u) ? (float)cnt : -CUDART_INF_F;
+            if ((long long)ss.excl == m0 + bit && ((vmask >> bit) & 1u)) x = -CUDART_INF_F;
             sc[bit] = x;
             lmax = fmaxf(lmax, x);
             topk_insert<KF>(lst, x);
@@ -1184,10 +1314,10 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
 // ---------------------------------------------------------------------------
 // launch wrappers (called by the host engine)
 // ---------------------------------------------------------------------------
-cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers,
+cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers, int missing,
                                 cudaStream_t st) {
     long long blocks = (g.N + 255) / 256;
-    k_build_layers<<<(unsigned)blocks, 256, 0, st>>>(ti, nvar, types, g, layers);
+    k_build_layers<<<(unsigned)blocks, 256, 0, st>>>(ti, nvar, types, g, layers, missing);
     return cudaGetLastError();
 }
 
@@ -1201,9 +1331,11 @@ cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, cons
 }
 
 cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
-                          const int *node_of_cell, int *level, int *max_level, cudaStream_t st) {
+                          const int *node_of_cell, int *dep, int *level, int *max_level, cudaStream_t st) {
     if (nodes <= 0) return cudaSuccess;
-    k_levels<<<1, 1024, 0, st>>>(nodes, n, nb_count, nb_cell, node_of_cell, level, max_level);
+    long long tot = nodes * n;
+    k_dep_nodes<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nodes, n, nb_count, nb_cell, node_of_cell, dep);
+    k_levels<<<1, 1024, 0, st>>>(nodes, n, dep, level, max_level);
     return cudaGetLastError();
 }
 
@@ -1246,7 +1378,7 @@ cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms
 
 cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, const int *ncat, const float *catv,
                                 int pw, unsigned *planes, cudaStream_t st) {
-    long long total = (long long)nvar * QSK_CMAX * pw;
+    long long total = (long long)nvar * (QSK_CMAX + 1) * pw;
     k_build_planes<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(layers, g, nvar, ncat, catv, pw, planes);
     return cudaGetLastError();
 }

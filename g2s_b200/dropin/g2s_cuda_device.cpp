@@ -18,7 +18,10 @@
 //  * searchKBiggest runs the fused map + k-best on the GPU with the CPU
 //    path's tie-breaking (fKb.hpp) and returns scores scaled like the device
 //    that qs asked for (setTrueMismatch(true): S/N·N + delta, i.e. S + delta;
-//    otherwise the unnormalised N·S of the CPU device).
+//    otherwise the unnormalised N·S of the CPU device);
+//  * training images with missing values: the overlap ("cross") output of the
+//    XMeasurement matrix, its centre mask and the -|S/c^4| compensation are
+//    applied on the GPU (qsk_pattern_opts); -nV excludes one candidate.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -45,8 +48,6 @@ public:
     B200QsDevice(int deviceId, SharedMemoryManager *smm, std::vector<g2s::OperationMatrix> coefficientMatrix,
                  unsigned threadRatio, bool withCrossMeasurement, bool circularTI)
         : AcceleratorDevice(smm, coefficientMatrix, threadRatio, withCrossMeasurement, circularTI) {
-        if (withCrossMeasurement)
-            throw std::runtime_error("g2s_b200: training images with missing values (cross measurement) are not supported");
         if (circularTI) throw std::runtime_error("g2s_b200: circular training images are not supported");
         _deviceType = DT_gpuCuda;
         _deviceID = unsigned(deviceId);
@@ -101,7 +102,9 @@ public:
                 _max[d] = std::max(_max[d], o[d]);
             }
         // terms: neighbour j, its converted value var, every layer varA with a
-        // non-zero coefficient in the regular operation matrix
+        // non-zero coefficient in the regular operation matrix; with missing
+        // training-image values also the overlap terms of the XMeasurement
+        // matrix (DataImage.hpp:626-710, CPUThreadDevice.cpp:426-444)
         g2s::OperationMatrix &M = _coefficientMatrix[0];
         const int nvar = int(M.getNumberOfVariable());
         _terms.clear();
@@ -109,21 +112,27 @@ public:
             const std::vector<float> &vals = neighborValueArrayVector[j];
             for (int var = 0; var < nvar && var < int(vals.size()); ++var) {
                 if (std::isnan(vals[var])) continue;
-                for (int varA = 0; varA < nvar; ++varA) {
-                    float c = M.getVariableAt(varA, var);
-                    if (c == 0.f) continue;
-                    float coef = c * vals[var];
-                    if (coef == 0.f) continue;
-                    qsk_term t;
-                    t.neighbour = int(j);
-                    t.layer = varA;
-                    t.op = QSK_OP_LIN;
-                    t.a = coef;
-                    t.b = 0.f;
-                    _terms.push_back(t);
+                for (size_t mi = 0; mi < _coefficientMatrix.size() && mi < 2; ++mi) {
+                    g2s::OperationMatrix &Mi = _coefficientMatrix[mi];
+                    for (int varA = 0; varA < nvar; ++varA) {
+                        float c = Mi.getVariableAt(varA, var);
+                        if (c == 0.f) continue;
+                        float coef = c * vals[var];
+                        if (coef == 0.f) continue;
+                        qsk_term t;
+                        t.neighbour = int(j);
+                        t.layer = varA;
+                        t.op = mi == 0 ? QSK_OP_LIN : QSK_OP_LIN_CROSS;
+                        t.a = coef;
+                        t.b = 0.f;
+                        _terms.push_back(t);
+                    }
                 }
             }
         }
+        _opts.exclude_index = -1;
+        _opts.missing_data = 0;
+        _opts.centre_mask_layer = -1;
         _delta = delta0.empty() ? 0.f : delta0[0];
         _nnb = int(neighborArrayVector.size());
         return true;
@@ -131,11 +140,15 @@ public:
 
     void searchKBiggest(float *errors, unsigned *encodedPosition, unsigned extendK, float seed) override {
         std::vector<int> mn(_fftSize.size());
-        check(qsk_pattern_kbest(_worker, _nnb, _offsets.data(), int(_terms.size()), _terms.data(), extendK, seed, errors,
-                                encodedPosition, mn.data()),
-              "qsk_pattern_kbest");
-        const float N = float(_realSpaceSize);
-        for (unsigned j = 0; j < extendK; ++j) errors[j] = _trueMismatch ? errors[j] + _delta : errors[j] * N;
+        check(qsk_pattern_kbest_ex(_worker, _nnb, _offsets.data(), int(_terms.size()), _terms.data(), extendK, seed,
+                                   &_opts, errors, encodedPosition, mn.data()),
+              "qsk_pattern_kbest_ex");
+        if (!_opts.missing_data) {
+            // the reference CUDA device reports S + delta, the CPU device N*S
+            const float N = float(_realSpaceSize);
+            for (unsigned j = 0; j < extendK; ++j) errors[j] = _trueMismatch ? errors[j] + _delta : errors[j] * N;
+        }
+        _opts.exclude_index = -1;
     }
 
     unsigned getErrorsArraySize() override { return _realSpaceSize; }
@@ -149,18 +162,34 @@ public:
         return qsk_position_to_index(_ti, _min.data(), position);
     }
 
-    void maskLayerWithVariable(unsigned, unsigned) override {
-        throw std::runtime_error("g2s_b200: masking layers (incomplete training images) is not supported");
+    // cross output masked by the TI mask at the candidate centre
+    // (CPUThreadDevice.cpp:501-524): the mask layer is the first layer with a
+    // non-zero row in the XMeasurement matrix
+    void maskLayerWithVariable(unsigned, unsigned variable) override {
+        if (_coefficientMatrix.size() < 2) throw std::runtime_error("g2s_b200: no cross-measurement matrix");
+        g2s::OperationMatrix &X = _coefficientMatrix[1];
+        int tmp = int(variable), conv = 0;
+        for (unsigned var = 0; var < X.getNumberOfVariable(); ++var) {
+            tmp -= X.needVariableAlongA(int(var));
+            if (tmp < 0) {
+                conv = int(var);
+                break;
+            }
+        }
+        _opts.centre_mask_layer = conv;
     }
-    void setValueInErrorArray(unsigned, float) override {
-        throw std::runtime_error("g2s_b200: -nV (no verbatim) is not supported");
+    // -nV: the excluded candidate (quantileSamplingModule.hpp:566-571); the
+    // reference only ever writes -inf here
+    void setValueInErrorArray(unsigned position, float) override { _opts.exclude_index = int(position); }
+    void setValueInErrorArrayWithRadius(unsigned position, float value, float radius) override {
+        if (radius < 1.f) {
+            setValueInErrorArray(position, value);
+            return;
+        }
+        throw std::runtime_error("g2s_b200: a verbatim exclusion radius >= 1 is not supported");
     }
-    void setValueInErrorArrayWithRadius(unsigned, float, float) override {
-        throw std::runtime_error("g2s_b200: -nV (no verbatim) is not supported");
-    }
-    void compensateMissingData() override {
-        throw std::runtime_error("g2s_b200: incomplete training images are not supported");
-    }
+    // -|S / c^4|, -inf where c == 0 (NvidiaGPUAcceleratorDevice.cu:199-206,677-686)
+    void compensateMissingData() override { _opts.missing_data = 1; }
 
     // the FFT pipeline steps are replaced by the fused candidateForPattern
     void zerosFrenquencySpaceOutputArray(unsigned) override {}
@@ -173,6 +202,7 @@ private:
     qsk_worker *_worker = nullptr;
     std::vector<int> _offsets;
     std::vector<qsk_term> _terms;
+    qsk_pattern_opts _opts{-1, 0, -1};
     int _nnb = 0;
     float _delta = 0.f;
 };

@@ -32,6 +32,7 @@ extern "C" {
 #define QSK_OP_LIN 0           /* acc = fma(a, x, acc) */
 #define QSK_OP_SQLIN 1         /* acc = fma(a, x*x, acc); acc = fma(b, x, acc) */
 #define QSK_OP_EQ 2            /* acc = (x == b) ? acc + a : acc */
+#define QSK_OP_LIN_CROSS 3     /* cross = fma(a, x, cross): the overlap output of a TI with missing values */
 
 /* Last error message of the calling thread ("" when none). */
 const char *qsk_last_error(void);
@@ -102,6 +103,26 @@ typedef struct {
 int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
                       unsigned k, float seed, float *out_score, unsigned *out_index, int *out_min);
 
+/* Options of a pattern query beyond the plain map (zero-initialise):
+ *   exclude_index      scan index forced to -inf before the k-best (-nV:
+ *                      AcceleratorDevice::setValueInErrorArray, G2S
+ *                      include/quantileSamplingModule.hpp:566-571); -1 none
+ *   missing_data       1 when the TI has missing values: the score becomes
+ *                      -|S / c^4| with c the QSK_OP_LIN_CROSS sum times the
+ *                      centre mask, -inf where c == 0, NaN outside the border
+ *                      (maskCroossErrorWithVariable + compensateMissingData,
+ *                      quantileSamplingModule.hpp:559-564, .cu:617-686)
+ *   centre_mask_layer  layer holding the TI mask (1 informed, 0 missing) */
+typedef struct {
+    int exclude_index;
+    int missing_data;
+    int centre_mask_layer;
+} qsk_pattern_opts;
+
+int qsk_pattern_kbest_ex(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
+                         unsigned k, float seed, const qsk_pattern_opts *opts, float *out_score, unsigned *out_index,
+                         int *out_min);
+
 /* Batched form: B patterns in CSR form (nb_ptr[B+1] into offsets rows,
  * term_ptr[B+1] into terms; term.neighbour is relative to its pattern).
  * Outputs are B*k scores/indices and B*ndim minima. */
@@ -135,6 +156,7 @@ typedef struct {
     int n;                        /* -n */
     float k;                      /* -k */
     unsigned seed;                /* -s */
+    int no_verbatim;              /* -nV */
 } qsk_qs_params;
 
 typedef struct {
@@ -162,8 +184,9 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
 /* Simulate on the GPU (device-resident data only; resets the grid first). */
 int qsk_sim_run(qsk_sim *s);
 /* Teacher-forced evaluation: draw every path node against the completed
- * grid (host array), as the sequential run would at that node's turn. */
-int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed);
+ * grid (host array), as the sequential run would at that node's turn.
+ * id_completed (the run's index image) is needed with -nV, else may be NULL. */
+int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *id_completed);
 /* Copy results to the host: the grid, the index image (TI cell * nTI + TI,
  * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL). */
 int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out);

@@ -186,12 +186,15 @@ struct Term {
     int cat;       /* 1 categorical */
     float a;       /* continuous: -w (TI^2 term); categorical: w */
     float b;       /* continuous: 2*(w*v) (TI term); categorical: category code v */
+    float cm;      /* missing-data mode: coefficient of the mask layer, -((w*v)*v) */
+    float cw;      /* missing-data mode: weight added to the overlap ("cross") sum */
     double w, v;   /* exact weight and value for the FP64 map */
 };
 
 struct Node {
     std::vector<Term> terms;
     int mn[8], mx[8];
+    bool incomplete = false;   /* the TI has missing values: cross-measurement scoring */
 };
 
 /* kernel weight for offset o and variable v (uniform 1 when kernel==nullptr);
@@ -232,6 +235,11 @@ Node build_node(const Grid &ti, const int *types, const Grid &kg, const float *k
             t.w = w; t.v = val;
             if (types[v] == 0) { t.a = -w; t.b = 2.f * (w * val); }
             else { t.a = w; t.b = val; }
+            /* P2 = (w*v)*v on the mask layer with coefficient -1, and the
+             * XMeasurement matrix adds P0 = w on the mask layer
+             * (DataImage.hpp:640-660, quantileSamplingModule.hpp:398-402) */
+            t.cm = -((w * val) * val);
+            t.cw = w;
             nd.terms.push_back(t);
         }
     }
@@ -282,7 +290,28 @@ static inline bool centre_of(const Scan &sc, const Grid &ti, const Node &nd, lon
 void map_fp32(const Grid &ti, const float *tival, const Node &nd, const Scan &sc, float *out) {
     for (long m = 0; m < sc.N; ++m) {
         long p;
-        if (!centre_of(sc, ti, nd, m, &p)) { out[m] = -INFINITY; continue; }
+        if (!centre_of(sc, ti, nd, m, &p)) { out[m] = nd.incomplete ? NAN : -INFINITY; continue; }
+        if (nd.incomplete) {
+            /* regular and cross outputs (CPUThreadDevice.cpp:426-444), the cross
+             * output masked by the centre (CPUThreadDevice.cpp:501-524), then
+             * -|S / c^4|, -inf where c == 0 (quantileSamplingModule.hpp:507-516) */
+            float reg = 0.f, cross = 0.f;
+            for (const Term &t : nd.terms) {
+                float xr = tival[size_t(p + t.off) * ti.nvar + t.var];
+                float mask = std::isnan(xr) ? 0.f : 1.f;
+                float x = std::isnan(xr) ? 0.f : xr;
+                reg = std::fmaf(t.a, x * x, reg);
+                reg = std::fmaf(t.b, x, reg);
+                reg = std::fmaf(t.cm, mask, reg);
+                cross = std::fmaf(t.cw, mask, cross);
+            }
+            float cmask = std::isnan(tival[size_t(p) * ti.nvar + 0]) ? 0.f : 1.f;
+            float c = cross * cmask;
+            float e = -std::fabs(reg / (((c * c) * c) * c));
+            if (c == 0.0f) e = -INFINITY;
+            out[m] = e;
+            continue;
+        }
         float acc = 0.f;
         for (const Term &t : nd.terms) {
             float x = tival[size_t(p + t.off) * ti.nvar + t.var];
@@ -306,6 +335,20 @@ void map_fp64(const Grid &ti, const float *tival, const Node &nd, const Scan &sc
     for (long m = 0; m < sc.N; ++m) {
         long p;
         if (!centre_of(sc, ti, nd, m, &p)) { out[m] = -INFINITY; if (scale) scale[m] = 0; continue; }
+        if (nd.incomplete) {
+            double reg = 0.0, cross = 0.0;
+            for (const Term &t : nd.terms) {
+                double xr = tival[size_t(p + t.off) * ti.nvar + t.var];
+                if (std::isnan(xr)) continue;
+                reg += t.w * (2.0 * t.v * xr - xr * xr - t.v * t.v);
+                cross += t.w;
+            }
+            if (std::isnan(tival[size_t(p) * ti.nvar + 0])) cross = 0.0;
+            double e = cross == 0.0 ? -INFINITY : -std::fabs(reg / (cross * cross * cross * cross));
+            out[m] = e;
+            if (scale) scale[m] = std::fabs(e);
+            continue;
+        }
         double acc = 0.0, sc2 = 0.0;
         for (const Term &t : nd.terms) {
             double x = tival[size_t(p + t.off) * ti.nvar + t.var];
@@ -401,6 +444,7 @@ static inline unsigned index_to_position(const Scan &sc, const Grid &ti, const N
 }
 
 struct NodeResult {
+    double probe_cross; /* missing-data mode: overlap weight sum at a probed TI cell */
     unsigned ti_cell;   /* chosen TI cell */
     int near_tie;       /* FP64 top-(K+1) adjacent gap within tol*scale */
     int marginal;       /* drawn from the marginal (no informed neighbour) */
@@ -417,11 +461,28 @@ struct Problem {
     int n = 0;
     float k = 1.f;
     double tol = 1e-5;
+    bool incomplete = false;   /* some TI value is NaN */
+    bool no_verbatim = false;  /* -nV */
+    std::vector<long> complete_prefix;  /* complete TI cells in [0..c] (missing-data marginal draw) */
 };
+
+/* CPUThreadDevice::cvtPositionToIndex (CPUThreadDevice.cpp:270-284), unsigned arithmetic */
+static inline unsigned position_to_index(const Scan &sc, const Grid &ti, const Node &nd, unsigned position) {
+    unsigned index = 0;
+    unsigned div = 1;
+    for (int i = sc.nd - 1; i >= 0; --i) div *= ti.dims[i];
+    for (int i = sc.nd - 1; i >= 0; --i) {
+        div /= ti.dims[i];
+        index = index * unsigned(sc.fft[i]) +
+                (unsigned(sc.fft[i]) - (position / div + unsigned(nd.mn[i])) % ti.dims[i] - 1u);
+    }
+    return index;
+}
 
 /* one node, given the current state of the grid */
 NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, const Path &path, const float *state,
-                    unsigned idx_path, bool want_fp64, bool own_cell_unknown) {
+                    const unsigned *id_state, unsigned idx_path, bool want_fp64, bool own_cell_unknown,
+                    long probe_cell = -1) {
     NodeResult r;
     std::memset(&r, 0, sizeof(r));
     const Grid &di = P.di;
@@ -438,9 +499,22 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
     bool withDataInCenter = false;
     for (int v = 0; v < di.nvar; ++v) withDataInCenter |= !std::isnan(value(cell, v));
     if (cnt <= 1 && !withDataInCenter) {
-        /* marginal draw (simulation.hpp:586-605), single complete TI */
+        /* marginal draw (simulation.hpp:586-655), single TI */
         unsigned cells = unsigned(P.ti.cells());
-        r.ti_cell = unsigned(int(std::floor(double(seed * float(cells)))));
+        unsigned position = unsigned(int(std::floor(double(seed * float(cells)))));
+        bool hasNaN = false;
+        for (int v = 0; v < P.ti.nvar; ++v) hasNaN |= std::isnan(P.tival[size_t(position) * P.ti.nvar + v]);
+        if (hasNaN) {
+            /* NaN-safe draw: position = floor(seed*(complete/nvar))*nvar, first cell
+             * whose running count of complete cells reaches it */
+            unsigned complete = unsigned(P.complete_prefix.back());
+            unsigned pos2 = unsigned(int(std::floor(double(seed * float(complete / unsigned(P.ti.nvar)))))) *
+                            unsigned(P.ti.nvar);
+            long k = std::lower_bound(P.complete_prefix.begin(), P.complete_prefix.end(), long(pos2)) -
+                     P.complete_prefix.begin();
+            position = unsigned(k);
+        }
+        r.ti_cell = position;
         r.marginal = 1;
         return r;
     }
@@ -451,9 +525,55 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
         for (int v = 0; v < di.nvar; ++v) vals[j * di.nvar + v] = value(ncell[j], v);
     }
     Node nd = build_node(P.ti, P.types, P.kg, P.kernel, cnt, offs.data(), vals.data());
+    nd.incomplete = P.incomplete;
     Scan sc = make_scan(P.ti, nd);
+    if (probe_cell >= 0 && P.incomplete) {
+        /* exact overlap weight (cross output times the centre mask) at the
+         * probed candidate centre */
+        double cross = 0.0;
+        long pc = probe_cell;
+        bool inside = true;
+        long rem = pc;
+        int cc[8];
+        for (int d = 0; d < P.ti.nd; ++d) { cc[d] = int(rem % P.ti.dims[d]); rem /= P.ti.dims[d]; }
+        for (int j = 0; j < cnt && inside; ++j) {
+            bool in = true;
+            long f = 0, st = 1;
+            for (int d = 0; d < P.ti.nd; ++d) {
+                int c = cc[d] + offs[j * di.nd + d];
+                in &= c >= 0 && c < int(P.ti.dims[d]);
+                f += long(c) * st;
+                st *= P.ti.dims[d];
+            }
+            if (!in) { inside = false; break; }
+            for (int v = 0; v < P.ti.nvar; ++v) {
+                float val = vals[j * di.nvar + v];
+                if (std::isnan(val)) continue;
+                if (!std::isnan(P.tival[size_t(f) * P.ti.nvar + v])) cross += kweight(P.kg, P.kernel, offs.data() + j * di.nd, v);
+            }
+        }
+        if (std::isnan(P.tival[size_t(pc) * P.ti.nvar])) cross = 0.0;
+        r.probe_cross = inside ? cross : -1.0;
+    }
     std::vector<float> map(sc.N);
     map_fp32(P.ti, P.tival, nd, sc, map.data());
+    if (P.no_verbatim && cnt > 1) {
+        /* the TI position continuing neighbour 1's own source is excluded
+         * (simulation.hpp:556-583, quantileSamplingModule.hpp:518-523) */
+        unsigned src = id_state[ncell[1]];
+        long rem = long(src);
+        long pf = 0, stride = 1;
+        for (int d = 0; d < P.ti.nd; ++d) {
+            int dim = int(P.ti.dims[d]);
+            int c = int(rem % dim) - offs[1 * di.nd + d];
+            rem /= dim;
+            c = ((c % dim) + dim) % dim;
+            pf += long(c) * stride;
+            stride *= dim;
+        }
+        unsigned ex = position_to_index(sc, P.ti, nd, unsigned(pf));
+        if (ex < unsigned(sc.N)) map[ex] = -INFINITY;
+    }
     unsigned short K = (unsigned short)int(std::ceil(P.k));
     std::vector<float> ev(K);
     std::vector<unsigned> ep(K);
@@ -481,6 +601,16 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
         for (size_t j = 0; j + 1 < top; ++j) {
             double g = m64[ord[j]] - m64[ord[j + 1]];
             gmin = std::min(gmin, scale > 0 ? g / scale : g);
+        }
+        if (nd.incomplete) {
+            /* scores are -|S/c^4|: relative gaps */
+            gmin = INFINITY;
+            for (size_t j = 0; j + 1 < top; ++j) {
+                double a = m64[ord[j]], b2 = m64[ord[j + 1]];
+                double g = a - b2;
+                double sc2 = std::max(std::fabs(a), std::fabs(b2));
+                gmin = std::min(gmin, std::isfinite(g) && sc2 > 0 ? g / sc2 : (a == b2 ? 0.0 : INFINITY));
+            }
         }
         r.gap_min = gmin;
         r.near_tie = gmin <= P.tol;
@@ -548,16 +678,38 @@ unsigned orc_selected_index(float seed, float k, unsigned nti) { return selected
 long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
                   const unsigned *di_dims, float *di, const float *di_init, const unsigned *kdims, const float *kernel, int n, float k,
                   unsigned seed, int want_fp64, double tol, long node_begin, long node_end, unsigned *out_cell,
-                  int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id) {
+                  int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id, int no_verbatim,
+                  const unsigned *id_init, const unsigned *probe, double *probe_cross) {
     Problem P;
     P.ti.nd = P.di.nd = P.kg.nd = nd;
     P.ti.nvar = P.di.nvar = nvar;
     for (int d = 0; d < nd; ++d) { P.ti.dims[d] = ti_dims[d]; P.di.dims[d] = di_dims[d]; }
-    P.tival = ti;
+    /* missing values: cells with any NaN variable become all-NaN for vector
+     * simulation (src/qs.cpp:1436-1467) */
+    std::vector<float> tiw(ti, ti + P.ti.cells() * nvar);
+    for (size_t c = 0; c < P.ti.cells(); ++c) {
+        bool hasNan = false;
+        for (int v = 0; v < nvar; ++v) hasNan |= std::isnan(tiw[c * nvar + v]);
+        if (hasNan) {
+            P.incomplete = true;
+            for (int v = 0; v < nvar; ++v) tiw[c * nvar + v] = NAN;
+        }
+    }
+    if (P.incomplete)
+        for (int v = 0; v < nvar; ++v)
+            if (types[v] != 0) return -2;  /* categorical + missing values: undefined in the reference */
+    P.complete_prefix.resize(P.ti.cells());
+    long run = 0;
+    for (size_t c = 0; c < P.ti.cells(); ++c) {
+        run += std::isnan(tiw[c * nvar]) ? 0 : 1;
+        P.complete_prefix[c] = run;
+    }
+    P.tival = tiw.data();
     P.types = types;
     P.n = n;
     P.k = k;
     P.tol = tol;
+    P.no_verbatim = no_verbatim != 0;
     if (kernel) {
         P.kernel = kernel;
         P.kg.nvar = nvar;
@@ -572,12 +724,16 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
     Path path = make_path(P.di, di_init ? di_init : state.data(), seed);
     long nodes = long(P.di.cells()) - long(path.begin);
     if (node_end < 0 || node_end > nodes) node_end = nodes;
+    std::vector<unsigned> idw(P.di.cells(), 0u);
+    if (id_init) std::copy(id_init, id_init + P.di.cells(), idw.begin());
     if (mode == 1) {
         /* teacher forcing: every path cell is "not yet simulated" at its own turn */
 #pragma omp parallel for schedule(dynamic, 16)
         for (long i = node_begin; i < node_end; ++i) {
-            NodeResult r = run_node(P, tpl, path, state.data(), unsigned(i), want_fp64 != 0, true);
             long o = i - node_begin;
+            NodeResult r = run_node(P, tpl, path, state.data(), idw.data(), unsigned(i), want_fp64 != 0, true,
+                                    probe ? long(probe[o]) : -1L);
+            if (probe_cross) probe_cross[o] = r.probe_cross;
             if (out_cell) out_cell[o] = r.ti_cell;
             if (out_near_tie) out_near_tie[o] = r.near_tie;
             if (out_marginal) out_marginal[o] = r.marginal;
@@ -588,9 +744,10 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
     for (long i = 0; i < node_end; ++i) {
         unsigned cell = path.order[path.begin + i];
         bool active = i >= node_begin;
-        NodeResult r = run_node(P, tpl, path, state.data(), unsigned(i), active && want_fp64 != 0, false);
+        NodeResult r = run_node(P, tpl, path, state.data(), idw.data(), unsigned(i), active && want_fp64 != 0, false);
         for (int v = 0; v < nvar; ++v)
-            if (std::isnan(state[size_t(cell) * nvar + v])) state[size_t(cell) * nvar + v] = ti[size_t(r.ti_cell) * nvar + v];
+            if (std::isnan(state[size_t(cell) * nvar + v])) state[size_t(cell) * nvar + v] = P.tival[size_t(r.ti_cell) * nvar + v];
+        idw[cell] = r.ti_cell;
         if (out_id) out_id[cell] = r.ti_cell;
         if (active) {
             long o = i - node_begin;

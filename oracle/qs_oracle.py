@@ -42,7 +42,8 @@ def lib():
         L.orc_simulate.argtypes = [ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, _u32p, _f32p, _f32p,
                                    _u32p,
                                    _f32p, ctypes.c_int, ctypes.c_float, ctypes.c_uint, ctypes.c_int, ctypes.c_double,
-                                   ctypes.c_long, ctypes.c_long, _u32p, _i32p, _i32p, _f64p, _u32p]
+                                   ctypes.c_long, ctypes.c_long, _u32p, _i32p, _i32p, _f64p, _u32p, ctypes.c_int,
+                                   _u32p, _u32p, _f64p]
         L.orc_simulate.restype = ctypes.c_long
         L.orc_pattern_map.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, ctypes.c_int, _i32p, _f32p,
                                       _f32p, _f64p, _f64p, _i32p, _i32p]
@@ -96,11 +97,12 @@ def rng_stream(seed: int, n: int):
 
 
 def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp64=False, tol=1e-5,
-             node_begin=0, node_end=-1, di_init=None):
+             node_begin=0, node_end=-1, di_init=None, no_verbatim=False, id_init=None, probe=None):
     """mode 0: sequential vector simulation of ``di`` (NaN = unknown);
     mode 1: teacher-forced evaluation of every path node against the completed
     grid ``di``, the path being built from ``di_init`` (the grid before
-    simulation).
+    simulation).  ``no_verbatim`` is -nV; in mode 1 it needs ``id_init``, the
+    index image of the completed grid.
 
     Returns dict(sim, id, cell, near_tie, marginal, gap, begin)."""
     nvar = len(types)
@@ -122,10 +124,17 @@ def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp
     oid = np.zeros(cells, np.uint32)
     kd = None if kdims is None else np.asarray(kdims, dtype=np.uint32)
     kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
-    lib().orc_simulate(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
+    idi = None if id_init is None else np.ascontiguousarray(id_init, dtype=np.uint32).ravel()
+    prb = None if probe is None else np.ascontiguousarray(probe, dtype=np.uint32).ravel()
+    pcross = np.full(cnt, np.nan, np.float64)
+    rc = lib().orc_simulate(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
                        _p(d, _f32p), None if di_init is None else _p(init, _f32p), _p(kd, _u32p), _p(kern, _f32p), n, k, seed, int(want_fp64), tol, node_begin,
-                       ne, _p(cell, _u32p), _p(nt, _i32p), _p(mg, _i32p), _p(gap, _f64p), _p(oid, _u32p))
-    return dict(sim=d, id=oid, cell=cell, near_tie=nt.astype(bool), marginal=mg.astype(bool), gap=gap)
+                       ne, _p(cell, _u32p), _p(nt, _i32p), _p(mg, _i32p), _p(gap, _f64p), _p(oid, _u32p),
+                       int(no_verbatim), _p(idi, _u32p), _p(prb, _u32p), _p(pcross, _f64p))
+    if rc < 0:
+        raise ValueError("oracle: categorical variables with missing training-image values are undefined")
+    return dict(sim=d, id=oid, cell=cell, near_tie=nt.astype(bool), marginal=mg.astype(bool), gap=gap,
+                probe_cross=pcross)
 
 
 def pattern_map(ti, types, offsets, values):

@@ -31,16 +31,36 @@ CASES = {
     "config0": (lambda: syn.grf((200, 200), (12, 12), seed=1), (200, 200), [0], 1.2, 50, 100),
 }
 
+# cases with extra qs flags: name -> (ti builder, di shape, types, k, n, seed, extra flags)
+EXTRA = {
+    "grf2d_nv": (lambda: syn.grf((64, 64), (8, 8), seed=1), (40, 40), [0], 1.2, 20, 100, ["-nV"]),
+    "grf2d_holes": (lambda: holes(syn.grf((64, 64), (8, 8), seed=6), seed=6), (40, 40), [0], 1.2, 20, 100, []),
+    "grf2d_holes_nv": (lambda: holes(syn.grf((60, 70), (7, 7), seed=8), seed=8), (36, 44), [0], 1.5, 16, 5, ["-nV"]),
+}
+
+
+def holes(field, seed):
+    """Missing training-image values: a few NaN rectangles."""
+    rng = np.random.default_rng(seed)
+    f = field.copy()
+    ny, nx = f.shape
+    for _ in range(6):
+        y, x = rng.integers(0, ny - 8), rng.integers(0, nx - 8)
+        f[y:y + int(rng.integers(2, 8)), x:x + int(rng.integers(2, 8))] = np.nan
+    return f
+
 
 def main(names=None):
-    for name, (mk, dshape, types, k, n, seed) in CASES.items():
+    cases = {k: v + ([],) for k, v in CASES.items()}
+    cases.update(EXTRA)
+    for name, (mk, dshape, types, k, n, seed, extra) in cases.items():
         if names and name not in names:
             continue
         ti = mk()
         di = np.full(dshape, np.nan, np.float32)
-        sim, idx, ms, _ = ref.run_qs(ti, di, types, ["-k", str(k), "-n", str(n), "-s", str(seed), "-j", "1"])
+        sim, idx, ms, _ = ref.run_qs(ti, di, types, ["-k", str(k), "-n", str(n), "-s", str(seed), "-j", "1"] + extra)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k, n=n,
-                            seed=seed, sim=sim, idx=idx, ref_ms=ms)
+                            seed=seed, sim=sim, idx=idx, ref_ms=ms, nv=("-nV" in extra))
         print(name, ti.shape, dshape, "ref ms", ms)
 
 

@@ -65,3 +65,29 @@ def test_qs_w_cuda_equals_oracle(oracle, name):
     o = oracle.simulate(g["ti"], g["di"], types, int(g["n"]), float(g["k"]), int(g["seed"]), mode=0)
     assert np.array_equal(sim, o["sim"])
     assert np.array_equal(idx.ravel(), o["id"])
+
+
+def test_qs_w_cuda_no_verbatim_equals_reference():
+    g = golden("grf2d_nv")
+    from oracle import ref
+    types = [0]
+    job = 31020
+    outputs = [str(job), f"id_{job}", f"im_1_{job}", f"im_2_{job}"]
+    _cleanup(outputs)
+    ref.write_image(f"dropin_ti_{job}", g["ti"], types)
+    ref.write_image(f"dropin_di_{job}", g["di"], types)
+    log = f"/tmp/G2S/logs/dropin_{job}.log"
+    cmd = [QS, "-ti", f"dropin_ti_{job}", "-di", f"dropin_di_{job}", "-k", str(float(g["k"])), "-n", str(int(g["n"])),
+           "-s", str(int(g["seed"])), "-j", "1", "-nV", "-W_CUDA", "0", "-id", str(job), "-r", log]
+    r = subprocess.run(cmd, cwd=DROPIN_DIR, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    sim = ref.read_image(str(job))
+    _cleanup(outputs + [f"dropin_ti_{job}", f"dropin_di_{job}"])
+    assert np.array_equal(sim, g["sim"])
+
+
+def test_qs_w_cuda_missing_data_equals_oracle(oracle):
+    g = golden("grf2d_holes")
+    sim, idx, log = run_qs_dropin(g, 31021)
+    o = oracle.simulate(g["ti"], g["di"], [0], int(g["n"]), float(g["k"]), int(g["seed"]), mode=0)
+    assert np.array_equal(sim, o["sim"]) and np.array_equal(idx.ravel(), o["id"])
