@@ -642,7 +642,7 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 // replay of the k-biggest scan + draw + write-back; one warp per slot
 // ---------------------------------------------------------------------------
 #define RP_WARPS 4
-#define RNG_BUF 704   // 624 fresh draws + up to 63 unread ones kept across a refill
+#define RNG_BUF 896   // 624 fresh draws + up to 255 unread ones kept across a refill
 
 struct WarpShared {
     unsigned mt[624];
@@ -652,16 +652,17 @@ struct WarpShared {
 // Draw buffer with warp-replicated read pointer: rp/len live in registers of
 // every lane (all lanes execute the same control flow).
 __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int &len) {
-    const int unread = len - rp;   // < 64 by construction, and rp > unread when len >= 624
+    const int unread = len - rp;   // < 256 by construction
     __syncwarp();
-    float keep0 = 0.f, keep1 = 0.f;
-    if (lane < unread) keep0 = w.buf[rp + lane];
-    if (lane + 32 < unread) keep1 = w.buf[rp + lane + 32];
+    float keep[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) keep[q] = (lane + 32 * q < unread) ? w.buf[rp + lane + 32 * q] : 0.f;
     __syncwarp();
     mt_twist(w.mt, lane);
     for (int i = lane; i < 624; i += 32) w.buf[unread + i] = mt_unit(mt_temper(w.mt[i]));
-    if (lane < unread) w.buf[lane] = keep0;
-    if (lane + 32 < unread) w.buf[lane + 32] = keep1;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (lane + 32 * q < unread) w.buf[lane + 32 * q] = keep[q];
     __syncwarp();
     len = unread + 624;
     rp = 0;
@@ -889,6 +890,84 @@ __device__ __forceinline__ void replay_chunk_ties(int K, bool tie, int m, unsign
     rp += 2 * nt;
 }
 
+// Segment-wide tie path: the state's K values are all equal to the K-th
+// value V and nothing in the segment exceeds V, so every record equal to V is
+// a tie (xes = K, two draws, cpt + 1) and the others are no-ops.  Lane l
+// composes the slot maps of records 4l..4l+3 on its own; one warp reduction
+// per segment combines them.
+template <int KM>
+__device__ __forceinline__ void replay_segment_ties(int K, float V, int cnt, const float *rv, const int *ri,
+                                                    unsigned (&cp)[KM], unsigned &cpt, int &rp, const float *buf,
+                                                    int lane) {
+    const unsigned FULL = 0xffffffffu;
+    float vv[4];
+    int mi[4];
+    int mine = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = 4 * lane + q;
+        vv[q] = j < cnt ? rv[j] : -CUDART_INF_F;
+        mi[q] = j < cnt ? ri[j] : 0;
+        mine += (j < cnt && vv[q] == V) ? 1 : 0;
+    }
+    // exclusive prefix of the per-lane tie counts (0..4) from three ballots
+    const unsigned lt = lanemask_lt();
+    const unsigned b0 = __ballot_sync(FULL, mine & 1), b1 = __ballot_sync(FULL, mine & 2),
+                   b2 = __ballot_sync(FULL, mine & 4);
+    int rank = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+    const int total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+    int o[KM];
+#pragma unroll
+    for (int s = 0; s < KM; ++s) o[s] = s;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (4 * lane + q < cnt && vv[q] == V) {
+            const float u1 = buf[rp + 2 * rank];
+            const float u2 = buf[rp + 2 * rank + 1];
+            int x = int(floorf(__fmul_rn(u1, (float)K)));
+            if (x > K - 1) x = K - 1;
+            const unsigned after = cpt + unsigned(rank) + 1u;
+            const bool write = __fmul_rn(__uint2float_rn(unsigned(K) + after), u2) < (float)K;
+            // op = (write at K-1) o (swap x, K-1); compose after the lane's earlier ops
+            int c[KM];
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) {
+                int src = (s2 == x) ? K - 1 : ((s2 == K - 1) ? x : s2);
+                if (s2 >= K) src = s2;
+                int val = sel_i<KM>(o, src);
+                if (write && s2 == K - 1) val = -(mi[q] + 1);
+                c[s2] = val;
+            }
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) o[s2] = c[s2];
+            ++rank;
+        }
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int later[KM];
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) later[s2] = __shfl_down_sync(FULL, o[s2], d);
+        if ((lane & (2 * d - 1)) == 0) {
+            int c[KM];
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) c[s2] = later[s2] < 0 ? later[s2] : sel_i<KM>(o, later[s2]);
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) o[s2] = c[s2];
+        }
+    }
+    unsigned np[KM];
+#pragma unroll
+    for (int s2 = 0; s2 < KM; ++s2) {
+        int t = __shfl_sync(FULL, o[s2], 0);
+        np[s2] = t < 0 ? unsigned(-(t + 1)) : sel_u<KM>(cp, t);
+    }
+#pragma unroll
+    for (int s2 = 0; s2 < KM; ++s2) cp[s2] = np[s2];
+    cpt += unsigned(total);
+    rp += 2 * total;
+}
+
 template <int KM>
 __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     __shared__ WarpShared wsh[RP_WARPS];
@@ -969,6 +1048,17 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 const int cnt = __shfl_sync(FULL, myc, l);
                 const float smax = __shfl_sync(FULL, mym, l);
                 const long long base = (long long)sg * QSK_SEG;
+                {
+                    const float kth0 = sel_f<KM>(cv, K - 1);
+                    if (kth0 != -CUDART_INF_F && sel_f<KM>(cv, 0) == kth0 && smax <= kth0) {
+                        // the whole segment is ties or no-ops
+                        if (smax == kth0) {
+                            rng_ensure(w, lane, rp, len, 256);
+                            replay_segment_ties<KM>(K, kth0, cnt, rv + base, ri + base, cp, cpt, rp, w.buf, lane);
+                        }
+                        continue;
+                    }
+                }
                 int r0 = 0;
                 while (r0 < cnt) {
                     const float kth0 = sel_f<KM>(cv, K - 1);
