@@ -111,13 +111,16 @@ __global__ void k_build_layers(const float *__restrict__ ti, int nvar, const int
 // non-strict informed rule: cells with path order <= the node's, the node
 // itself included).
 // ---------------------------------------------------------------------------
+// one warp per node: 32 template offsets tested per step, accepted ones
+// appended in template order
 __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl, const unsigned *__restrict__ path,
                              unsigned begin, long long nodes, const unsigned *__restrict__ posterior, int n,
                              int *__restrict__ nb_count, int *__restrict__ nb_tpl, unsigned *__restrict__ nb_cell) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (i >= nodes) return;
-    unsigned cell = path[begin + i];
-    unsigned order = posterior[cell];
+    const unsigned cell = path[begin + i];
+    const unsigned order = posterior[cell];
     int c0[QSK_MAXD];
     long long rem = cell;
     for (int d = 0; d < dg.nd; ++d) {
@@ -125,22 +128,28 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
         rem /= dg.dims[d];
     }
     int cnt = 0;
-    for (int t = 0; t < ntpl && cnt < n; ++t) {
-        bool ok = true;
+    for (int t0 = 0; t0 < ntpl && cnt < n; t0 += 32) {
+        const int t = t0 + lane;
+        bool acc = false;
         long long nc = 0;
-        for (int d = 0; d < dg.nd; ++d) {
-            int c = c0[d] + tpl[t * dg.nd + d];
-            ok &= (c >= 0) && (c < dg.dims[d]);
-            nc += (long long)c * dg.stride[d];
+        if (t < ntpl) {
+            bool ok = true;
+            for (int d = 0; d < dg.nd; ++d) {
+                int c = c0[d] + tpl[t * dg.nd + d];
+                ok &= (c >= 0) && (c < dg.dims[d]);
+                nc += (long long)c * dg.stride[d];
+            }
+            acc = ok && posterior[nc] <= order;
         }
-        if (!ok) continue;
-        if (posterior[nc] <= order) {
-            nb_tpl[i * n + cnt] = t;
-            nb_cell[i * n + cnt] = unsigned(nc);
-            cnt++;
+        const unsigned bal = __ballot_sync(0xffffffffu, acc);
+        const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
+        if (acc && pos < n) {
+            nb_tpl[i * n + pos] = t;
+            nb_cell[i * n + pos] = unsigned(nc);
         }
+        cnt += __popc(bal);
     }
-    nb_count[i] = cnt;
+    if (lane == 0) nb_count[i] = cnt < n ? cnt : n;
 }
 
 // ---------------------------------------------------------------------------
@@ -1415,8 +1424,8 @@ cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, cons
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
                               unsigned *nb_cell, cudaStream_t st) {
     if (nodes <= 0) return cudaSuccess;
-    k_neighbours<<<(unsigned)((nodes + 127) / 128), 128, 0, st>>>(dg, tpl, ntpl, path, begin, nodes, posterior, n,
-                                                                  nb_count, nb_tpl, nb_cell);
+    k_neighbours<<<(unsigned)((nodes * 32 + 255) / 256), 256, 0, st>>>(dg, tpl, ntpl, path, begin, nodes, posterior, n,
+                                                                       nb_count, nb_tpl, nb_cell);
     return cudaGetLastError();
 }
 
