@@ -194,6 +194,8 @@ def main():
     ap.add_argument("--ref-side", type=int, default=120)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--workload", default="config1", choices=["config1", "config0"],
+                    help="config1 (default, the benchmark line) or config0 (continuous GRF 200x200, n=50, k=1.2)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -202,6 +204,7 @@ def main():
     import g2s_b200 as g2s
     from g2s_b200 import synthetic as syn
 
+    global TI_SHAPE, DI_SHAPE, N_NB, K_CAND, WORKLOAD
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = None
@@ -211,10 +214,17 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = local
 
-    ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
+    types = [1]
+    if args.workload == "config0":
+        TI_SHAPE, DI_SHAPE, N_NB, K_CAND = (200, 200), (200, 200), 50, 1.2
+        WORKLOAD = "config0-continuous-grf-200x200-to-200x200-n50-k1.2"
+        ti = syn.grf(TI_SHAPE, (12, 12), seed=1)
+        types = [0]
+    else:
+        ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
     di = np.full(DI_SHAPE, np.nan, np.float32)
     seed = replica_seed(SEED, rank)
-    sim = g2s.Simulation(ti, di, [1], n=N_NB, k=K_CAND, seed=seed, device=dev)
+    sim = g2s.Simulation(ti, di, types, n=N_NB, k=K_CAND, seed=seed, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")  # > 126 MB L2
 
     for _ in range(max(args.warmup, 0)):
@@ -251,9 +261,10 @@ def main():
     sim.run()
     pinf = sim.info()
     sim.set_profiling(False)
-    map_kernel = "bits"   # categorical TI with a uniform kernel: bit-sliced map kernel
+    # categorical TI with a uniform kernel: bit-sliced map kernel
+    map_kernel = "bits" if types == [1] else "fp32"
     N = TI_SHAPE[0] * TI_SHAPE[1]
-    L = 2  # categorical variable with 2 classes: 2 indicator layers
+    L = 2  # 2 correlation layers: TI^2 and TI (continuous) / 2 class indicators (binary categorical)
     bytes_per_node = 4 * N * L
     map_avg_ms = pinf["ms_map"] / max(pinf["map_launches"], 1)
     nodes_per_launch = pinf["map_positions"] / max(pinf["map_launches"], 1) / N
@@ -269,7 +280,7 @@ def main():
         d = np.full(DI_SHAPE, np.nan, np.float32)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        g2s.qs(ti, d, [1], k=K_CAND, n=N_NB, s=seed, device=dev)
+        g2s.qs(ti, d, types, k=K_CAND, n=N_NB, s=seed, device=dev)
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_vals)) if e2e_vals else float("nan")
@@ -279,7 +290,7 @@ def main():
            "d2h_bytes_per_step": int(di.nbytes + di.size * 4)}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "config1":
         cpu = cpu_baseline_leg(args.ref_side)
 
     if rank == 0:
