@@ -203,3 +203,50 @@ def test_categorical_bit_and_float_kernels_agree(g2s, gpu, oracle, mode):
                 assert np.array_equal(sc, v) and np.array_equal(ix, p), (trial, k)
     finally:
         g2s.set_map_mode(0)
+
+
+def test_missing_data_pattern_scores(g2s, gpu):
+    """Training image with missing values: every valid position's score
+    -|S / c^4| (S the masked squared mismatch, c the informed overlap times
+    the centre mask; -inf where c == 0) against a direct numpy evaluation."""
+    rng = np.random.default_rng(3)
+    ti = rng.standard_normal((7, 9)).astype(np.float32)
+    ti[2, 3] = np.nan
+    ti[5, 6] = np.nan
+    T = g2s.TrainingImage(ti, [0])
+    W = g2s.Worker(T)
+    offs = np.array([[0, 0], [1, 0], [-1, 2]], np.int32)
+    vals = np.array([np.nan, 0.4, -1.1], np.float32)
+    # reference-format layers: TI^2 (NaN->0), TI (NaN->0), mask; flipped (fft == src)
+    flat = ti.reshape(-1)
+    m = (~np.isnan(flat)).astype(np.float32)
+    t0 = np.where(np.isnan(flat), 0, flat).astype(np.float32)
+    L = g2s.TrainingImage.from_layers([(t0 * t0)[::-1].copy(), t0[::-1].copy(), m[::-1].copy()],
+                                      src_size=[9, 7], fft_size=[9, 7])
+    WL = g2s.Worker(L)
+    terms = []
+    for j in (1, 2):
+        w, v = np.float32(1), vals[j]
+        terms += [(j, 0, g2s.QSK_OP_LIN, float(-w), 0.0), (j, 1, g2s.QSK_OP_LIN, float(2 * w * v), 0.0),
+                  (j, 2, g2s.QSK_OP_LIN, float(-(w * v) * v), 0.0), (j, 2, g2s.QSK_OP_LIN_CROSS, float(w), 0.0)]
+    K = 16
+    sc, ix, mn = WL.pattern_kbest(offs, terms, K, 0.5, missing_data=True, centre_mask_layer=2)
+    expect = []
+    for py in range(7):
+        for px in range(9):
+            ok = all(0 <= px + ox < 9 and 0 <= py + oy < 7 for ox, oy in offs)
+            if not ok:
+                continue
+            reg, c = 0.0, 0.0
+            for (ox, oy), v in zip(offs[1:], vals[1:]):
+                t = ti[py + oy, px + ox]
+                if np.isnan(t):
+                    continue
+                reg += -(t - v) ** 2
+                c += 1
+            if np.isnan(ti[py, px]):
+                c = 0
+            expect.append(-np.inf if c == 0 else -abs(reg / c ** 4))
+    expect = np.sort(np.array(expect, np.float64))[::-1][:K]
+    got = sc.astype(np.float64)
+    assert np.allclose(got[np.isfinite(expect)], expect[np.isfinite(expect)], rtol=1e-5, atol=1e-7), (got, expect)
