@@ -530,8 +530,11 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
         for (int r = 0; r < 4; ++r) {
             const float xval = valid[r] ? acc[r] : ((ss.flags & SLOT_MISSING) ? CUDART_NAN_F : -CUDART_INF_F);
             segmax = fmaxf(segmax, xval);
+            // a NaN score never compares true in the reservoir (fKb.hpp), so it
+            // is never a record and must not raise the prefix K-th best: it
+            // enters the scan as -inf (fminf/fmaxf would turn it into +inf)
             float st[KF];
-            st[0] = xval;
+            st[0] = isnan(xval) ? -CUDART_INF_F : xval;
 #pragma unroll
             for (int q = 1; q < KF; ++q) st[q] = -CUDART_INF_F;
 #pragma unroll
