@@ -71,6 +71,9 @@ SIGNATURES = {
                                             ctypes.POINTER(QskPatternOpts), _f32p, _u32p, _i32p]),
     "qsk_pattern_kbest_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p,
                                                ctypes.POINTER(QskTerm), ctypes.c_uint, _f32p, _f32p, _u32p, _i32p]),
+    "qsk_pattern_kbest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
+                                                 ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float, _f32p, _u32p,
+                                                 _i32p]),
     "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_position_to_index": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <string>
@@ -1158,6 +1159,211 @@ int qsk_simulate(int device, const qsk_qs_params *p, float *di_inout, unsigned *
     if (!rc) rc = qsk_sim_read(s, di_inout, id_out, nullptr);
     qsk_sim_destroy(s);
     return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// qsk_pattern_kbest_noalloc: the map + k-best of qsk_pattern_kbest for callers
+// that cannot allocate (their device memory is held by another allocator, or
+// they must not stall the device's other streams with cudaFree's implicit
+// synchronisation).  Its device scratch is the fixed array below; the host
+// side stages the slot and the terms on the stack.  Nothing in it calls
+// cudaMalloc, cudaFree or an allocating library routine.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QSK_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_addr[kMaxDevices] = {};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// scratch layout of one call; every region 256-byte aligned
+struct NoallocLayout {
+    size_t slot, terms, rec_val, rec_idx, rec_cnt, rec_max, out_val, out_pos, total;
+};
+
+NoallocLayout noalloc_layout(const Geom &g, int nterms, unsigned k) {
+    NoallocLayout L;
+    const size_t recs = size_t(g.nseg) * QSK_SEG;
+    size_t o = 0;
+    L.slot = o;
+    o = align256(o + sizeof(Slot));
+    L.terms = o;
+    o = align256(o + sizeof(Term) * size_t(std::max(nterms, 1)));
+    L.rec_val = o;
+    o = align256(o + sizeof(float) * recs);
+    L.rec_idx = o;
+    o = align256(o + sizeof(int) * recs);
+    L.rec_cnt = o;
+    o = align256(o + sizeof(int) * size_t(g.nseg));
+    L.rec_max = o;
+    o = align256(o + sizeof(float) * size_t(g.nseg));
+    L.out_val = o;
+    o = align256(o + sizeof(float) * k);
+    L.out_pos = o;
+    o = align256(o + sizeof(unsigned) * k);
+    L.total = o;
+    return L;
+}
+
+// address of the scratch array on `device` (current), looked up once per device
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= kMaxDevices) return fail(QSK_ERR_UNSUPPORTED, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(QSK_ERR_CUDA, "cudaGetSymbolAddress(scratch) on device %d: %s", device, cudaGetErrorString(e));
+        g_noalloc_addr[device] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return QSK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, const int *offsets, int n_terms,
+                              const qsk_term *terms, unsigned k, float seed, float *out_score, unsigned *out_index,
+                              int *out_min) {
+    if (!ti || n_neighbours < 0 || n_terms < 0 || !out_score || !out_index || (n_neighbours > 0 && !offsets) ||
+        (n_terms > 0 && !terms))
+        return fail(QSK_ERR_ARG, "null argument");
+    if (k < 1 || k > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "k=%u outside [1,%d]", k, QSK_KMAX);
+    if (n_terms > QSK_NOALLOC_MAX_TERMS)
+        return fail(QSK_ERR_UNSUPPORTED, "qsk_pattern_kbest_noalloc: %d terms, at most %d", n_terms,
+                    QSK_NOALLOC_MAX_TERMS);
+    const Geom &g = ti->g;
+    const int nd = g.nd;
+    const NoallocLayout L = noalloc_layout(g, n_terms, k);
+    if (L.total > size_t(QSK_NOALLOC_SCRATCH_BYTES))
+        return fail(QSK_ERR_UNSUPPORTED,
+                    "qsk_pattern_kbest_noalloc: a training image of %lld positions with %d terms needs %zu bytes of "
+                    "scratch; the fixed scratch holds %zu (use qsk_pattern_kbest)",
+                    g.N, n_terms, L.total, size_t(QSK_NOALLOC_SCRATCH_BYTES));
+    DeviceGuard dgd(ti->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned char *base = nullptr;
+    int rc = noalloc_scratch(ti->device, &base);
+    if (rc) return rc;
+
+    // slot and terms on the stack (same rules as build_pattern_slot)
+    Slot s;
+    std::memset(&s, 0, sizeof(s));
+    s.node = 0;
+    s.seed = seed;
+    s.excl = -1;
+    int mn[QSK_MAXD] = {0}, mx[QSK_MAXD] = {0};
+    for (int j = 0; j < n_neighbours; ++j)
+        for (int d = 0; d < nd; ++d) {
+            mn[d] = std::min(mn[d], offsets[j * nd + d]);
+            mx[d] = std::max(mx[d], offsets[j * nd + d]);
+        }
+    long long nvalid = 1;
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        s.mn[d] = mn[d];
+        int lo = 0;
+        if (d < nd) {
+            lo = g.fft[d] - (g.src[d] - (mx[d] - mn[d]));
+            lo = std::max(0, std::min(lo, g.fft[d]));
+            nvalid *= (g.fft[d] - lo);
+        }
+        s.lo[d] = lo;
+        if (out_min && d < nd) out_min[d] = mn[d];
+    }
+    if (n_neighbours == 0) {
+        // candidateForPattern returns false on an empty pattern
+        for (unsigned j = 0; j < k; ++j) {
+            out_score[j] = -INFINITY;
+            out_index[j] = 0xffffffffu;
+        }
+        return QSK_OK;
+    }
+    if (nvalid < (long long)k) s.flags |= SLOT_EMIT_MASKED;
+    Term h_terms[QSK_NOALLOC_MAX_TERMS];
+    bool bits = ti->planes_ok && g_map_mode == 0 && n_terms <= 255;
+    for (int t = 0; t < n_terms; ++t) {
+        const qsk_term &q = terms[t];
+        if (q.neighbour < 0 || q.neighbour >= n_neighbours || q.layer < 0 || q.layer >= ti->nlayers || q.op < 0 ||
+            q.op > 3)
+            return fail(QSK_ERR_ARG, "pattern term %d out of range", t);
+        long long dflat = 0;
+        for (int d = 0; d < nd; ++d) dflat += (long long)(offsets[q.neighbour * nd + d] - mn[d]) * g.sstride[d];
+        Term &tm = h_terms[t];
+        tm.base = int((long long)q.layer * g.N - dflat);
+        tm.a = q.a;
+        tm.b = q.b;
+        tm.op = q.op == QSK_OP_LIN_CROSS ? OP_LINX : q.op;
+        bits &= (tm.op == OP_EQ && tm.a == 1.f);
+    }
+    s.nterms = n_terms;
+    const int maxterms = std::max(n_terms, 1);
+
+    Slot *d_slot = reinterpret_cast<Slot *>(base + L.slot);
+    Term *d_terms = reinterpret_cast<Term *>(base + L.terms);
+    float *rec_val = reinterpret_cast<float *>(base + L.rec_val);
+    int *rec_idx = reinterpret_cast<int *>(base + L.rec_idx);
+    int *rec_cnt = reinterpret_cast<int *>(base + L.rec_cnt);
+    float *rec_max = reinterpret_cast<float *>(base + L.rec_max);
+    float *out_val = reinterpret_cast<float *>(base + L.out_val);
+    unsigned *out_pos = reinterpret_cast<unsigned *>(base + L.out_pos);
+
+    CK(set_map_smem_limit(200 * 1024));
+    CK(cudaMemcpyAsync(d_slot, &s, sizeof(Slot), cudaMemcpyHostToDevice, st));
+    if (n_terms > 0) CK(cudaMemcpyAsync(d_terms, h_terms, sizeof(Term) * n_terms, cudaMemcpyHostToDevice, st));
+    if (bits) {
+        BitArgs ba;
+        ba.g = g;
+        ba.planes = ti->planes.p;
+        ba.pw = ti->pw;
+        ba.ncat = ti->ncat.p;
+        ba.catv = ti->catv.p;
+        ba.slots = d_slot;
+        ba.terms = d_terms;
+        ba.maxterms = maxterms;
+        ba.segs_per_cta = map_bits_segs_per_cta(g, 1);
+        ba.rec_val = rec_val;
+        ba.rec_idx = rec_idx;
+        ba.rec_cnt = rec_cnt;
+        ba.rec_max = rec_max;
+        CK(launch_map_bits(ba, 1, int(k), maxterms, st));
+    } else {
+        MapArgs ma;
+        ma.g = g;
+        ma.layers = ti->layers.p;
+        ma.slots = d_slot;
+        ma.terms = d_terms;
+        ma.maxterms = maxterms;
+        ma.segs_per_cta = map_segs_per_cta(g, 1);
+        ma.rec_val = rec_val;
+        ma.rec_idx = rec_idx;
+        ma.rec_cnt = rec_cnt;
+        ma.rec_max = rec_max;
+        CK(launch_map_records(ma, 1, int(k), maxterms, st));
+    }
+    ReplayArgs ra;
+    std::memset(&ra, 0, sizeof(ra));
+    ra.g = g;
+    ra.slots = d_slot;
+    ra.nslots = 1;
+    ra.K = int(k);
+    ra.rec_val = rec_val;
+    ra.rec_idx = rec_idx;
+    ra.rec_cnt = rec_cnt;
+    ra.rec_max = rec_max;
+    ra.out_val = out_val;
+    ra.out_pos = out_pos;
+    CK(launch_replay(ra, st));
+    CK(cudaMemcpyAsync(out_score, out_val, sizeof(float) * k, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(out_index, out_pos, sizeof(unsigned) * k, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return QSK_OK;
 }
 
 }  // extern "C"

@@ -130,6 +130,44 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
                             const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
                             unsigned *out_index, int *out_min);
 
+/* qsk_pattern_kbest without any allocation.  No counterpart in the reference
+ * (G2S' devices allocate their buffers when they are created).
+ *
+ * Same arguments (a qsk_ti instead of a worker), same results as
+ * qsk_pattern_kbest, for callers that cannot allocate device memory:
+ *  - a process whose device memory is already held by another allocator
+ *    (a caching allocator that reserved the HBM, or a host program that
+ *    sized its training images to fill the GPU), where cudaMalloc fails;
+ *  - a caller that must not stall the other streams of the device:
+ *    qsk_pattern_kbest grows its worker's buffers with cudaFree + cudaMalloc,
+ *    and cudaFree waits for the whole device.
+ * The call makes no cudaMalloc, cudaFree or other allocating call.  Its
+ * device scratch (the pattern's slot and terms, the map's records, the k
+ * results) lives in one fixed array of QSK_NOALLOC_SCRATCH_BYTES bytes in the
+ * library's device code, one per device; the host side stages on the stack.
+ *
+ * Limit: the scratch needs, each region rounded up to 256 bytes, 8 bytes per
+ * TI scan position (positions rounded up to a multiple of 128), 8 bytes per
+ * 128 positions, 16 bytes per term and 8*k bytes: training images of up to
+ * about 2 million scan positions fit.  A larger request, or more than
+ * QSK_NOALLOC_MAX_TERMS terms, returns QSK_ERR_UNSUPPORTED before any GPU
+ * work, with the sizes in qsk_last_error().
+ * Nothing in the scratch needs to start at zero: every byte a call reads was
+ * written earlier in the same call.
+ * One scratch per device: calls on the same device that overlap in time
+ * (from several threads, or on several streams) race on it and give wrong
+ * results; serialise them.
+ * The first call on a device looks the scratch address up with
+ * cudaGetSymbolAddress (with that device current, the return code checked);
+ * make that first call before any stream capture begins.
+ * `stream` is a cudaStream_t of ti's device (NULL: the legacy default
+ * stream); the call returns after its work on that stream has finished. */
+#define QSK_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define QSK_NOALLOC_MAX_TERMS 2048
+int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, const int *offsets, int n_terms,
+                              const qsk_term *terms, unsigned k, float seed, float *out_score, unsigned *out_index,
+                              int *out_min);
+
 /* Reference scan index -> TI cell (CPUThreadDevice::cvtIndexToPosition,
  * G2S src/CPUThreadDevice.cpp:257-268). */
 unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index);
