@@ -619,8 +619,9 @@ struct qsk_sim {
     DBuf<int> d_tpl, d_types;
     DBuf<float> d_wtab, d_seeds, d_init, d_state;
     DBuf<unsigned> d_path, d_post, d_id, d_node_cell, d_nb_cell;
-    DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_dep, d_level, d_maxlevel, d_hist, d_start, d_cursor, d_level_nodes,
-        d_status;
+    DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_level_nodes, d_status;
+    // dependency levels (Kahn frontiers over the reverse edges)
+    DBuf<int> d_adj, d_deg, d_outcnt, d_outstart, d_cursor, d_tile_sum, d_lcnt, d_start, d_nl;
     DBuf<Slot> d_slots;
     DBuf<Term> d_terms;
     DBuf<float> d_rec_val;
@@ -966,10 +967,16 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_nb_count.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_nb_tpl.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
         (e = s->d_nb_cell.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
-        (e = s->d_dep.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
-        (e = s->d_level.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_adj.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
+        (e = s->d_deg.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_outcnt.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_outstart.alloc(size_t(s->nodes) + 1)) != cudaSuccess ||
+        (e = s->d_cursor.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
+        (e = s->d_tile_sum.alloc(size_t((s->nodes + 1023) / 1024) + 2)) != cudaSuccess ||
+        (e = s->d_lcnt.alloc(size_t(s->nodes) + 2)) != cudaSuccess ||
+        (e = s->d_start.alloc(size_t(s->nodes) + 1)) != cudaSuccess ||
         (e = s->d_level_nodes.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
-        (e = s->d_maxlevel.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess)
+        (e = s->d_nl.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "upload: %s",
                          cudaGetErrorString(e)));
     // batch scratch: slots up to a record budget of ~2 GiB
@@ -1013,26 +1020,36 @@ int qsk_sim_run(qsk_sim *s) {
     int rc = sim_neighbours(s);
     if (rc) return rc;
     CK(cudaEventRecord(ev[1], s->st));
-    CK(cudaMemsetAsync(s->d_maxlevel.p, 0, sizeof(int), s->st));
-    CK(launch_levels(s->nodes, s->n, s->d_nb_count.p, s->d_nb_cell.p, s->d_node_of_cell.p, s->d_dep.p, s->d_level.p,
-                     s->d_maxlevel.p, s->st));
-    s->info.launches += 3;  // neighbours + dependency nodes + levels
-    int maxl = 0;
-    CK(cudaMemcpyAsync(&maxl, s->d_maxlevel.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    LevelArgs la;
+    la.nodes = s->nodes;
+    la.n = s->n;
+    la.nb_count = s->d_nb_count.p;
+    la.nb_cell = s->d_nb_cell.p;
+    la.node_of_cell = s->d_node_of_cell.p;
+    la.deg = s->d_deg.p;
+    la.outcnt = s->d_outcnt.p;
+    la.outstart = s->d_outstart.p;
+    la.cursor = s->d_cursor.p;
+    la.tile_sum = s->d_tile_sum.p;
+    la.adj = s->d_adj.p;
+    la.cnt = s->d_lcnt.p;
+    la.level_nodes = s->d_level_nodes.p;
+    la.start = s->d_start.p;
+    la.nl_out = s->d_nl.p;
+    CK(cudaMemsetAsync(s->d_nl.p, 0, sizeof(int), s->st));
+    CK(launch_levels(la, s->st));
+    s->info.launches += 7;  // neighbours + count, 3 scan passes, reverse edges, frontiers
+    int nl = 0;
+    CK(cudaMemcpyAsync(&nl, s->d_nl.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    int nl = s->nodes > 0 ? maxl + 1 : 0;
     std::vector<int> start(size_t(nl) + 1, 0);
     if (nl > 0) {
-        CK(s->d_hist.ensure(size_t(nl)));
-        CK(s->d_start.ensure(size_t(nl) + 1));
-        CK(s->d_cursor.ensure(size_t(nl)));
-        CK(cudaMemsetAsync(s->d_hist.p, 0, sizeof(int) * nl, s->st));
-        CK(launch_level_sort(s->nodes, nl, s->d_level.p, s->d_hist.p, s->d_start.p, s->d_cursor.p, s->d_level_nodes.p,
-                             s->st));
-        s->info.launches += 3;
         CK(cudaMemcpyAsync(start.data(), s->d_start.p, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
     }
+    if (s->nodes > 0 && (nl < 1 || start[size_t(nl)] != s->nodes))
+        return fail(QSK_ERR_DEVICE, "dependency levels cover %d of %lld nodes", nl > 0 ? start[size_t(nl)] : 0,
+                    s->nodes);
     CK(cudaEventRecord(ev[2], s->st));
     rc = sim_batches(s, start, false);
     if (rc) return rc;

@@ -168,10 +168,25 @@ cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, con
 cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
                               unsigned *nb_cell, cudaStream_t st);
-cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
-                          const int *node_of_cell, int *dep, int *level, int *max_level, cudaStream_t st);
-cudaError_t launch_level_sort(long long nodes, int nl, const int *level, int *hist, int *start, int *cursor,
-                              int *level_nodes, cudaStream_t st);
+// dependency levels of the path DAG (Kahn frontiers)
+struct LevelArgs {
+    long long nodes;
+    int n;
+    const int *nb_count;
+    const unsigned *nb_cell;
+    const int *node_of_cell;
+    int *deg;           // nodes
+    int *outcnt;        // nodes
+    int *outstart;      // nodes + 1
+    int *cursor;        // nodes
+    int *tile_sum;      // ceil(nodes / 1024) + 1
+    int *adj;           // nodes * n
+    int *cnt;           // nodes + 2
+    int *level_nodes;   // nodes: grouped by level
+    int *start;         // nodes + 1: level L is level_nodes[start[L] .. start[L+1])
+    int *nl_out;        // 1: number of levels
+};
+cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st);
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);
 int map_segs_per_cta(const Geom &g, int nslots);
 cudaError_t launch_map_records(const MapArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);

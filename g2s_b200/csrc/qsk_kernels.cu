@@ -13,9 +13,12 @@
 //                  quantileSamplingModule.hpp:45-49,525-557) over the records,
 //                  then the draw and the write-back (quantileSamplingModule.hpp:90-126,
 //                  CPUThreadDevice.cpp:257-268, simulation.hpp:586-666)
+//   k_map_bits     the same map for categorical patterns with unit weights,
+//                  bit-sliced (one bit plane per category), same records
 // Setup kernels: k_build_layers (DataImage.hpp:538-599), k_neighbours
-// (simulation.hpp:447-511, run for every path node at once), k_levels
-// (dependency levels of the path DAG).
+// (simulation.hpp:447-511, run for every path node at once), k_dep_count /
+// k_adj_fill / k_kahn (dependency levels of the path DAG, grouped by level).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <cstdint>
@@ -154,88 +157,134 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
 
 // ---------------------------------------------------------------------------
 // dependency levels: level(i) = 1 + max level(j) over the node's informed
-// neighbours j that are themselves path nodes.  One block walks the path in
-// chunks of blockDim nodes; inside a chunk it relaxes until nothing changes.
+// neighbours j that are themselves path nodes (0 without any) -- the longest
+// path to i in the path DAG (dependencies always point to smaller path
+// indices).  Kahn's frontier algorithm over the reverse edges: the nodes of
+// level L are those whose last dependency finished in level L-1, so the
+// frontiers come out already grouped by level.
 // ---------------------------------------------------------------------------
-// dependency node of each neighbour slot (-1: none / the node itself)
-__global__ void k_dep_nodes(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                            const int *__restrict__ node_of_cell, int *__restrict__ dep) {
-    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nodes * n) return;
-    long long i = idx / n;
-    int j = int(idx % n);
-    int dn = -1;
-    if (j < nb_count[i]) {
-        dn = node_of_cell[nb_cell[idx]];
-        if ((long long)dn == i) dn = -1;
-    }
-    dep[idx] = dn;
-}
-
-__global__ void k_levels(long long nodes, int n, const int *__restrict__ dep, int *__restrict__ level,
-                         int *__restrict__ max_level) {
-    __shared__ int changed;
-    int mx = 0;
-    for (long long c0 = 0; c0 < nodes; c0 += blockDim.x) {
-        const long long i = c0 + threadIdx.x;
-        const bool active = i < nodes;
-        int L = 0;
-        // dependencies before this chunk are final: one pass over them
-        if (active) {
-            for (int j = 0; j < n; ++j) {
-                const int dn = dep[i * n + j];
-                if (dn >= 0 && dn < c0) L = max(L, level[dn] + 1);
-            }
-            level[i] = L;
+// in-degree of every node and out-degree count of every dependency
+__global__ void k_dep_count(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
+                            const int *__restrict__ node_of_cell, int *__restrict__ deg, int *__restrict__ outcnt) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const int c = nb_count[i];
+    int dg = 0;
+    for (int j = 0; j < c; ++j) {
+        const int d = node_of_cell[nb_cell[i * n + j]];
+        if (d >= 0 && (long long)d != i) {
+            ++dg;
+            atomicAdd(&outcnt[d], 1);
         }
-        __syncthreads();
-        // dependencies inside the chunk: relax to the fixed point
-        for (;;) {
-            if (threadIdx.x == 0) changed = 0;
-            __syncthreads();
-            if (active) {
-                int L2 = L;
-                for (int j = 0; j < n; ++j) {
-                    const int dn = dep[i * n + j];
-                    if (dn >= c0) L2 = max(L2, ((volatile int *)level)[dn] + 1);
-                }
-                if (L2 != L) {
-                    L = L2;
-                    ((volatile int *)level)[i] = L;
-                    changed = 1;
-                }
-            }
-            __syncthreads();
-            if (!changed) break;
-            __syncthreads();
-        }
-        if (active) mx = mx > L ? mx : L;
     }
-    atomicMax(max_level, mx);
+    deg[i] = dg;
 }
 
-__global__ void k_level_hist(long long nodes, const int *__restrict__ level, int *__restrict__ hist) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nodes) atomicAdd(&hist[level[i]], 1);
+// exclusive scan in three passes: 1024-element tiles, tile sums, add
+__global__ void __launch_bounds__(1024) k_scan_tiles(long long count, const int *__restrict__ in, int *__restrict__ out,
+                                                     int *__restrict__ tile_sum) {
+    __shared__ int warp_sum[32];
+    const long long i = (long long)blockIdx.x * 1024 + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x = i < count ? in[i] : 0;
+    int incl = x;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) warp_sum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int ws = warp_sum[lane];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, ws, off);
+            if (lane >= off) ws += y;
+        }
+        warp_sum[lane] = ws;   // inclusive
+    }
+    __syncthreads();
+    const int base = w > 0 ? warp_sum[w - 1] : 0;
+    if (i < count) out[i] = base + incl - x;
+    if (threadIdx.x == 1023) tile_sum[blockIdx.x] = base + incl;
 }
 
-// exclusive scan of hist[0..nl) -> start[0..nl]; single block
-__global__ void k_level_scan(int nl, const int *__restrict__ hist, int *__restrict__ start, int *__restrict__ cursor) {
+__global__ void k_scan_sums(int ntiles, int *__restrict__ tile_sum) {
     if (threadIdx.x == 0) {
         int s = 0;
-        for (int l = 0; l < nl; ++l) {
-            start[l] = s;
-            cursor[l] = s;
-            s += hist[l];
+        for (int t = 0; t < ntiles; ++t) {
+            const int v = tile_sum[t];
+            tile_sum[t] = s;
+            s += v;
         }
-        start[nl] = s;
+        tile_sum[ntiles] = s;
     }
 }
 
-__global__ void k_level_scatter(long long nodes, const int *__restrict__ level, int *__restrict__ cursor,
-                                int *__restrict__ level_nodes) {
-    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nodes) level_nodes[atomicAdd(&cursor[level[i]], 1)] = int(i);
+__global__ void k_scan_add(long long count, int *__restrict__ out, int *__restrict__ cursor,
+                           const int *__restrict__ tile_sum) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const int v = out[i] + tile_sum[i / 1024];
+        out[i] = v;
+        cursor[i] = v;
+    } else if (i == count) {
+        const int v = tile_sum[(count + 1023) / 1024];
+        out[i] = v;
+    }
+}
+
+// reverse edges: adj[outstart[d] ..] lists the nodes that depend on d
+__global__ void k_adj_fill(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
+                           const int *__restrict__ node_of_cell, int *__restrict__ cursor, int *__restrict__ adj) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const int c = nb_count[i];
+    for (int j = 0; j < c; ++j) {
+        const int d = node_of_cell[nb_cell[i * n + j]];
+        if (d >= 0 && (long long)d != i) adj[atomicAdd(&cursor[d], 1)] = int(i);
+    }
+}
+
+// Frontier pass (cooperative launch, one grid barrier per level).  Level L's
+// nodes are level_nodes[start[L] .. start[L] + cnt[L]); a node joins level
+// L+1 when its remaining in-degree drops to zero.  cnt (levels + 2 ints) starts
+// at zero.  Writes start[0..nl] and *nl_out.
+__global__ void k_kahn(long long nodes, int *__restrict__ deg, const int *__restrict__ outstart,
+                       const int *__restrict__ adj, int *level_nodes, int *cnt, int *__restrict__ start,
+                       int *__restrict__ nl_out) {
+    namespace cg = cooperative_groups;
+    cg::grid_group grid = cg::this_grid();
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long wid = tid >> 5, nwarps = stride >> 5;
+    const int lane = threadIdx.x & 31;
+    for (long long i = tid; i < nodes; i += stride)
+        if (deg[i] == 0) level_nodes[atomicAdd(&cnt[0], 1)] = int(i);
+    grid.sync();
+    long long st = 0;
+    for (long long L = 0; L <= nodes; ++L) {
+        const int c = ((volatile int *)cnt)[L];
+        if (tid == 0) start[L] = int(st);
+        if (c == 0) {
+            if (tid == 0) *nl_out = int(L);
+            break;
+        }
+        const long long nst = st + c;
+        // one warp per frontier node, lanes over its dependents (out-degrees
+        // are skewed: early path nodes are neighbours of many later ones)
+        for (long long q = wid; q < c; q += nwarps) {
+            const int i = ((volatile int *)level_nodes)[st + q];
+            const int e1 = outstart[i + 1];
+            for (int e = outstart[i] + lane; e < e1; e += 32) {
+                const int d = adj[e];
+                if (atomicSub(&deg[d], 1) == 1) level_nodes[nst + atomicAdd(&cnt[L + 1], 1)] = d;
+            }
+        }
+        st = nst;
+        grid.sync();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -604,8 +653,10 @@ __device__ __forceinline__ unsigned mt_mix(unsigned a, unsigned b, unsigned c) {
     return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
 }
 
-// warp-cooperative regeneration of the 624-word state (3 dependency phases)
-__device__ void mt_twist(unsigned *mt, int lane) {
+// warp-cooperative regeneration of the 624-word state (3 dependency phases);
+// with OUT, draw k of the new block (tempered, converted) goes to out[k]
+template <bool OUT>
+__device__ void mt_twist(unsigned *mt, int lane, float *out) {
     unsigned nv[8];
     // phase A: k in [0,227): old x[k], x[k+1], x[k+397]
 #pragma unroll
@@ -617,7 +668,10 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         int k = lane + 32 * q;
-        if (k < 227) mt[k] = nv[q];
+        if (k < 227) {
+            mt[k] = nv[q];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[q]));
+        }
     }
     __syncwarp();
     // phase B: k in [227,454): old x[k], x[k+1]; new x[k-227]
@@ -630,7 +684,10 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         int k = 227 + lane + 32 * q;
-        if (k < 454) mt[k] = nv[q];
+        if (k < 454) {
+            mt[k] = nv[q];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[q]));
+        }
     }
     __syncwarp();
     // phase C: k in [454,623): old x[k], x[k+1]; new x[k-227]
@@ -643,10 +700,17 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         int k = 454 + lane + 32 * q;
-        if (k < 623) mt[k] = nv[q];
+        if (k < 623) {
+            mt[k] = nv[q];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[q]));
+        }
     }
     __syncwarp();
-    if (lane == 0) mt[623] = mt_mix(mt[623], mt[0], mt[396]);
+    if (lane == 0) {
+        const unsigned y = mt_mix(mt[623], mt[0], mt[396]);
+        mt[623] = y;
+        if (OUT) out[623] = mt_unit(mt_temper(y));
+    }
     __syncwarp();
 }
 
@@ -654,28 +718,31 @@ __device__ void mt_twist(unsigned *mt, int lane) {
 // replay of the k-biggest scan + draw + write-back; one warp per slot
 // ---------------------------------------------------------------------------
 #define RP_WARPS 4
-#define RNG_BUF 896   // 624 fresh draws + up to 255 unread ones kept across a refill
+#define RNG_KEEP 512  // unread draws kept across a refill (rng_ensure asks for at most this many)
+#define RNG_BUF (RNG_KEEP + 640)
+#define RUN_RECORDS 256   // records of one multi-segment tie run (8 per lane)
 
 struct WarpShared {
     unsigned mt[624];
     float buf[RNG_BUF];
+    int run_seg[32];      // segments of the current tie run
+    int run_pre[32];      // their first record's rank in the run
 };
 
 // Draw buffer with warp-replicated read pointer: rp/len live in registers of
 // every lane (all lanes execute the same control flow).
 __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int &len) {
-    const int unread = len - rp;   // < 256 by construction
+    const int unread = len - rp;   // < RNG_KEEP by construction
+    // move the unread draws to the front (destinations never overtake sources)
     __syncwarp();
-    float keep[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) keep[q] = (lane + 32 * q < unread) ? w.buf[rp + lane + 32 * q] : 0.f;
-    __syncwarp();
-    mt_twist(w.mt, lane);
-    for (int i = lane; i < 624; i += 32) w.buf[unread + i] = mt_unit(mt_temper(w.mt[i]));
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-        if (lane + 32 * q < unread) w.buf[lane + 32 * q] = keep[q];
-    __syncwarp();
+    for (int q = 0; 32 * q < unread; ++q) {
+        const int i = lane + 32 * q;
+        const float v = i < unread ? w.buf[rp + i] : 0.f;
+        __syncwarp();
+        if (i < unread) w.buf[i] = v;
+        __syncwarp();
+    }
+    mt_twist<true>(w.mt, lane, w.buf + unread);
     len = unread + 624;
     rp = 0;
 }
@@ -684,14 +751,21 @@ __device__ __forceinline__ void rng_ensure(WarpShared &w, int lane, int &rp, int
     if (len - rp < need) rng_refill(w, lane, rp, len);
 }
 
+// advance the stream by n draws; whole blocks of 624 only regenerate the state
 __device__ void rng_skip(WarpShared &w, int lane, int &rp, int &len, long long n) {
-    while (n > 0) {
-        long long avail = len - rp;
-        long long t = avail < n ? avail : n;
-        rp += int(t);
-        n -= t;
-        if (n > 0) rng_refill(w, lane, rp, len);
+    const long long avail = len - rp;
+    if (n <= avail) {
+        rp += int(n);
+        return;
     }
+    n -= avail;
+    rp = len;
+    while (n > 624) {
+        mt_twist<false>(w.mt, lane, nullptr);
+        n -= 624;
+    }
+    rng_refill(w, lane, rp, len);
+    rp += int(n);
 }
 
 template <int KM>
@@ -902,56 +976,73 @@ __device__ __forceinline__ void replay_chunk_ties(int K, bool tie, int m, unsign
     rp += 2 * nt;
 }
 
-// Segment-wide tie path: the state's K values are all equal to the K-th
-// value V and nothing in the segment exceeds V, so every record equal to V is
-// a tie (xes = K, two draws, cpt + 1) and the others are no-ops.  Lane l
-// composes the slot maps of records 4l..4l+3 on its own; one warp reduction
-// per segment combines them.
+// Multi-segment tie path: the state's K values all equal the K-th value V
+// and nothing in the run exceeds V, so every record equal to V is a tie
+// (xes = K, two draws, cpt + 1) and the others are no-ops.  The run is up to
+// RUN_RECORDS records of consecutive candidate segments (tables in w.run_*);
+// lane l composes the slot maps of run records 8l..8l+7 on its own and one
+// warp reduction per run combines them.
 template <int KM>
-__device__ __forceinline__ void replay_segment_ties(int K, float V, int cnt, const float *rv, const int *ri,
-                                                    unsigned (&cp)[KM], unsigned &cpt, int &rp, const float *buf,
-                                                    int lane) {
+__device__ __forceinline__ void replay_run_ties(int K, float V, int T, int r, const WarpShared &w, const float *rv,
+                                                const int *ri, unsigned (&cp)[KM], unsigned &cpt, int &rp,
+                                                WarpShared &wm, int &len, int lane) {
     const unsigned FULL = 0xffffffffu;
-    float vv[4];
-    int mi[4];
+    const int j0 = 8 * lane;
+    int seg = 0;
+    if (j0 < T) {
+        // last run segment whose first record is at or before j0
+        int lo = 0, hi = r - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (w.run_pre[mid] <= j0) lo = mid;
+            else hi = mid - 1;
+        }
+        seg = lo;
+    }
+    float vv[8];
+    int mi[8];
     int mine = 0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = 4 * lane + q;
-        vv[q] = j < cnt ? rv[j] : -CUDART_INF_F;
-        mi[q] = j < cnt ? ri[j] : 0;
-        mine += (j < cnt && vv[q] == V) ? 1 : 0;
+    for (int q = 0; q < 8; ++q) {
+        const int j = j0 + q;
+        vv[q] = -CUDART_INF_F;
+        mi[q] = 0;
+        if (j < T) {
+            while (seg + 1 < r && w.run_pre[seg + 1] <= j) ++seg;
+            const long long a = (long long)w.run_seg[seg] * QSK_SEG + (j - w.run_pre[seg]);
+            vv[q] = rv[a];
+            mi[q] = ri[a];
+        }
     }
-    // exclusive prefix of the per-lane tie counts (0..4) from three ballots
+#pragma unroll
+    for (int q = 0; q < 8; ++q) mine += (vv[q] == V) ? 1 : 0;
+    // exclusive prefix of the per-lane tie counts (0..8) from four ballots
     const unsigned lt = lanemask_lt();
     const unsigned b0 = __ballot_sync(FULL, mine & 1), b1 = __ballot_sync(FULL, mine & 2),
-                   b2 = __ballot_sync(FULL, mine & 4);
-    int rank = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
-    const int total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
+                   b2 = __ballot_sync(FULL, mine & 4), b3 = __ballot_sync(FULL, mine & 8);
+    int rank = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt) + 8 * __popc(b3 & lt);
+    const int total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2) + 8 * __popc(b3);
+    rng_ensure(wm, lane, rp, len, 2 * total);
+    const float *buf = wm.buf;
     int o[KM];
 #pragma unroll
     for (int s = 0; s < KM; ++s) o[s] = s;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        if (4 * lane + q < cnt && vv[q] == V) {
+    for (int q = 0; q < 8; ++q) {
+        if (vv[q] == V) {
             const float u1 = buf[rp + 2 * rank];
             const float u2 = buf[rp + 2 * rank + 1];
             int x = int(floorf(__fmul_rn(u1, (float)K)));
             if (x > K - 1) x = K - 1;
             const unsigned after = cpt + unsigned(rank) + 1u;
             const bool write = __fmul_rn(__uint2float_rn(unsigned(K) + after), u2) < (float)K;
-            // op = (write at K-1) o (swap x, K-1); compose after the lane's earlier ops
-            int c[KM];
+            // op = (write at K-1) o (swap x, K-1); composed after the lane's earlier ops
+            const int ox = sel_i<KM>(o, x), ok1 = sel_i<KM>(o, K - 1);
 #pragma unroll
             for (int s2 = 0; s2 < KM; ++s2) {
-                int src = (s2 == x) ? K - 1 : ((s2 == K - 1) ? x : s2);
-                if (s2 >= K) src = s2;
-                int val = sel_i<KM>(o, src);
-                if (write && s2 == K - 1) val = -(mi[q] + 1);
-                c[s2] = val;
+                if (s2 == x) o[s2] = ok1;
+                if (s2 == K - 1) o[s2] = write ? -(mi[q] + 1) : ox;
             }
-#pragma unroll
-            for (int s2 = 0; s2 < KM; ++s2) o[s2] = c[s2];
             ++rank;
         }
     }
@@ -1049,9 +1140,17 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
         const int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
         const int *rc = A.rec_cnt + (long long)b * g.nseg;
         const float *rm = A.rec_max + (long long)b * g.nseg;
+        // segment counts and maxima, 32 segments per group, loaded two groups ahead
+        int c1 = lane < g.nseg ? rc[lane] : 0, c2 = 32 + lane < g.nseg ? rc[32 + lane] : 0;
+        float m1 = lane < g.nseg ? rm[lane] : -CUDART_INF_F, m2 = 32 + lane < g.nseg ? rm[32 + lane] : -CUDART_INF_F;
         for (int s0 = 0; s0 < g.nseg; s0 += 32) {
-            const int myc = (s0 + lane < g.nseg) ? rc[s0 + lane] : 0;
-            const float mym = (s0 + lane < g.nseg) ? rm[s0 + lane] : -CUDART_INF_F;
+            const int myc = c1;
+            const float mym = m1;
+            c1 = c2;
+            m1 = m2;
+            const int s2 = s0 + 64 + lane;
+            c2 = s2 < g.nseg ? rc[s2] : 0;
+            m2 = s2 < g.nseg ? rm[s2] : -CUDART_INF_F;
             unsigned nz = __ballot_sync(FULL, myc > 0 && mym >= sel_f<KM>(cv, K - 1));
             while (nz) {
                 const int l = __ffs(nz) - 1;
@@ -1065,8 +1164,33 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                     if (kth0 != -CUDART_INF_F && sel_f<KM>(cv, 0) == kth0 && smax <= kth0) {
                         // the whole segment is ties or no-ops
                         if (smax == kth0) {
-                            rng_ensure(w, lane, rp, len, 256);
-                            replay_segment_ties<KM>(K, kth0, cnt, rv + base, ri + base, cp, cpt, rp, w.buf, lane);
+                            // run: this segment and the group's next candidates up to the
+                            // first one above V, at most RUN_RECORDS records
+                            const bool in_rest = (((nz | (1u << l)) >> lane) & 1u) != 0;
+                            const unsigned above = __ballot_sync(FULL, in_rest && mym > kth0);
+                            const unsigned below = above ? ((1u << (__ffs(above) - 1)) - 1u) : FULL;
+                            const bool cand = in_rest && ((below >> lane) & 1u) && myc > 0 && mym == kth0;
+                            const int c = cand ? myc : 0;
+                            int incl = c;
+#pragma unroll
+                            for (int off = 1; off < 32; off <<= 1) {
+                                const int y = __shfl_up_sync(FULL, incl, off);
+                                if (lane >= off) incl += y;
+                            }
+                            const bool take = cand && incl <= RUN_RECORDS;
+                            const unsigned R = __ballot_sync(FULL, take);
+                            if (take) {
+                                const int pos = __popc(R & lanemask_lt());
+                                w.run_seg[pos] = s0 + lane;
+                                w.run_pre[pos] = incl - c;
+                            }
+                            const int hi = 31 - __clz(R);
+                            const int T = __shfl_sync(FULL, incl, hi);
+                            __syncwarp();
+                            replay_run_ties<KM>(K, kth0, T, __popc(R), w, rv, ri, cp, cpt, rp, w, len, lane);
+                            __syncwarp();
+                            // the run's segments and the no-op ones between them are done
+                            nz &= (hi >= 31) ? 0u : ~((2u << hi) - 1u);
                         }
                         continue;
                     }
@@ -1333,22 +1457,45 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                 c7 ^= x;
             }
         }
-        // scores in scan order; lane-local top-K
-        float sc[32];
+        // Scores stay bit-sliced: position p of the lane holds the count
+        // sum_b ((c_b >> p) & 1) << b where it is valid and not excluded, -inf
+        // elsewhere.  Lane top-K by repeated bit-sliced maximum extraction.
+        unsigned vm = vmask;
+        if (ss.excl >= 0 && (long long)ss.excl >= m0 && (long long)ss.excl < m0 + 32)
+            vm &= ~(1u << unsigned(ss.excl - m0));
+        auto count_at = [&](int p) -> int {
+            return int(((c0 >> p) & 1u) | (((c1 >> p) & 1u) << 1) | (((c2 >> p) & 1u) << 2) |
+                       (((c3 >> p) & 1u) << 3) | (((c4 >> p) & 1u) << 4) | (((c5 >> p) & 1u) << 5) |
+                       (((c6 >> p) & 1u) << 6) | (((c7 >> p) & 1u) << 7));
+        };
         float lst[KF];
 #pragma unroll
         for (int q = 0; q < KF; ++q) lst[q] = -CUDART_INF_F;
         float lmax = -CUDART_INF_F;
+        {
+            unsigned rest = vm;
+            int filled = 0;
+            for (int q = 0; q < KF && rest != 0u && filled < KF; ++q) {
+                unsigned cand = rest;
+                int val = 0;
+                const unsigned cb[8] = {c0, c1, c2, c3, c4, c5, c6, c7};
 #pragma unroll
-        for (int bit = 0; bit < 32; ++bit) {
-            unsigned cnt = ((c0 >> bit) & 1u) | (((c1 >> bit) & 1u) << 1) | (((c2 >> bit) & 1u) << 2) |
-                           (((c3 >> bit) & 1u) << 3) | (((c4 >> bit) & 1u) << 4) | (((c5 >> bit) & 1u) << 5) |
-                           (((c6 >> bit) & 1u) << 6) | (((c7 >> bit) & 1u) << 7);
-            float x = ((vmask >> bit) & 1u) ? (float)cnt : -CUDART_INF_F;
-            if ((long long)ss.excl == m0 + bit && ((vmask >> bit) & 1u)) x = -CUDART_INF_F;
-            sc[bit] = x;
-            lmax = fmaxf(lmax, x);
-            topk_insert<KF>(lst, x);
+                for (int bb = 7; bb >= 0; --bb) {
+                    const unsigned t = cand & cb[bb];
+                    if (t) {
+                        cand = t;
+                        val |= 1 << bb;
+                    }
+                }
+                const int mult = __popc(cand);
+                const float fv = (float)val;
+#pragma unroll
+                for (int q2 = 0; q2 < KF; ++q2)
+                    if (q2 >= filled && q2 < filled + mult) lst[q2] = fv;
+                if (q == 0) lmax = fv;
+                filled += mult;
+                rest &= ~cand;
+            }
         }
         // exclusive prefix of the lane states across the 1024-position segment
         float inc[KF];
@@ -1371,15 +1518,43 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             float y = __shfl_up_sync(0xffffffffu, inc[q], 1);
             st[q] = lane == 0 ? -CUDART_INF_F : y;
         }
-        // record flags (value not below the K-th best of everything before it)
+        // record flags: value not below the K-th best of everything before it
+        // (earlier lanes, then earlier positions of this lane)
         unsigned rmask = 0;
+        const float T0 = st[KF - 1];
+        if (T0 == -CUDART_INF_F) {
+            // every existing position may qualify: exact scan of the 32 positions
+            if (vm != 0u || emit_masked) {
+                for (int bit = 0; bit < 32; ++bit) {
+                    if (!((emask >> bit) & 1u)) continue;
+                    const float x = ((vm >> bit) & 1u) ? (float)count_at(bit) : -CUDART_INF_F;
+                    if (x >= st[KF - 1] && (((vmask >> bit) & 1u) || emit_masked)) rmask |= 1u << bit;
+                    topk_insert<KF>(st, x);
+                }
+            }
+        } else {
+            // only positions with count >= T0 can be records (the running K-th
+            // never drops below T0; a smaller value leaves the state unchanged)
+            const int T = (int)T0;
+            unsigned gt = 0u, eq = vm;
+            const unsigned cb[8] = {c0, c1, c2, c3, c4, c5, c6, c7};
 #pragma unroll
-        for (int bit = 0; bit < 32; ++bit) {
-            const float x = sc[bit];
-            const bool ex = (emask >> bit) & 1u;
-            const bool val = (vmask >> bit) & 1u;
-            if (ex && x >= st[KF - 1] && (val || emit_masked)) rmask |= 1u << bit;
-            topk_insert<KF>(st, x);
+            for (int bb = 7; bb >= 0; --bb) {
+                if ((T >> bb) & 1) {
+                    eq &= cb[bb];
+                } else {
+                    gt |= eq & cb[bb];
+                    eq &= ~cb[bb];
+                }
+            }
+            unsigned cand = (T > 255) ? 0u : (gt | eq);
+            while (cand) {
+                const int bit = __ffs(cand) - 1;
+                cand &= cand - 1u;
+                const float x = (float)count_at(bit);
+                if (x >= st[KF - 1]) rmask |= 1u << bit;
+                topk_insert<KF>(st, x);
+            }
         }
         // offsets inside each 128-position sub-segment (4 lanes)
         const int rc = __popc(rmask);
@@ -1397,13 +1572,13 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         if (sub < g.nseg) {
             const long long rb = sub * QSK_SEG + excl;
             int o = 0;
-#pragma unroll
-            for (int bit = 0; bit < 32; ++bit) {
-                if ((rmask >> bit) & 1u) {
-                    rv[rb + o] = sc[bit];
-                    ri[rb + o] = int(m0 + bit);
-                    o++;
-                }
+            unsigned rm = rmask;
+            while (rm) {
+                const int bit = __ffs(rm) - 1;
+                rm &= rm - 1u;
+                rv[rb + o] = ((vm >> bit) & 1u) ? (float)count_at(bit) : -CUDART_INF_F;
+                ri[rb + o] = int(m0 + bit);
+                o++;
             }
             if ((lane & 3) == 0) {
                 A.rec_cnt[(long long)b * g.nseg + sub] = tot;
@@ -1432,22 +1607,32 @@ cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, cons
     return cudaGetLastError();
 }
 
-cudaError_t launch_levels(long long nodes, int n, const int *nb_count, const unsigned *nb_cell,
-                          const int *node_of_cell, int *dep, int *level, int *max_level, cudaStream_t st) {
+cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
+    long long nodes = a.nodes;
     if (nodes <= 0) return cudaSuccess;
-    long long tot = nodes * n;
-    k_dep_nodes<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(nodes, n, nb_count, nb_cell, node_of_cell, dep);
-    k_levels<<<1, 1024, 0, st>>>(nodes, n, dep, level, max_level);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_level_sort(long long nodes, int nl, const int *level, int *hist, int *start, int *cursor,
-                              int *level_nodes, cudaStream_t st) {
-    unsigned blocks = (unsigned)((nodes + 255) / 256);
-    k_level_hist<<<blocks, 256, 0, st>>>(nodes, level, hist);
-    k_level_scan<<<1, 32, 0, st>>>(nl, hist, start, cursor);
-    k_level_scatter<<<blocks, 256, 0, st>>>(nodes, level, cursor, level_nodes);
-    return cudaGetLastError();
+    const unsigned nb = (unsigned)((nodes + 255) / 256);
+    const long long ntiles = (nodes + 1023) / 1024;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(a.outcnt, 0, sizeof(int) * size_t(nodes), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.cnt, 0, sizeof(int) * size_t(nodes + 2), st)) != cudaSuccess) return e;
+    k_dep_count<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.node_of_cell, a.deg, a.outcnt);
+    k_scan_tiles<<<(unsigned)ntiles, 1024, 0, st>>>(nodes, a.outcnt, a.outstart, a.tile_sum);
+    k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);
+    k_scan_add<<<(unsigned)((nodes + 1 + 255) / 256), 256, 0, st>>>(nodes, a.outstart, a.cursor, a.tile_sum);
+    k_adj_fill<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.node_of_cell, a.cursor, a.adj);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kahn, 256, 0)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+    // one or two co-resident blocks per SM: per-level work is small, barriers cheap
+    long long blocks = (long long)sms * (per_sm < 2 ? per_sm : 2);
+    if (blocks > (long long)nb) blocks = nb;
+    int *deg = a.deg, *level_nodes = a.level_nodes, *cnt = a.cnt, *start = a.start, *nl_out = a.nl_out;
+    const int *outstart = a.outstart, *adj = a.adj;
+    void *args[] = {&nodes, &deg, &outstart, &adj, &level_nodes, &cnt, &start, &nl_out};
+    return cudaLaunchCooperativeKernel((const void *)k_kahn, dim3((unsigned)blocks), dim3(256), args, 0, st);
 }
 
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st) {
