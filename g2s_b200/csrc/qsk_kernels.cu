@@ -718,21 +718,24 @@ __device__ void mt_twist(unsigned *mt, int lane, float *out) {
 // replay of the k-biggest scan + draw + write-back; one warp per slot
 // ---------------------------------------------------------------------------
 #define RP_WARPS 4
-#define RNG_KEEP 512  // unread draws kept across a refill (rng_ensure asks for at most this many)
-#define RNG_BUF (RNG_KEEP + 640)
-#define RUN_RECORDS 256   // records of one multi-segment tie run (8 per lane)
+#define REC_CAP 1024          // records (padded to 4 per segment) of one tie super-run
+#define TAB_CAP 128           // segments of one tie super-run
+#define RNG_BUF (2 * REC_CAP + 640)   // draws of one super-run + one block
 
-struct WarpShared {
+struct __align__(16) WarpShared {
+    float rv_s[REC_CAP];      // super-run records (values), 16-byte aligned for cp.async
+    int ri_s[REC_CAP];        // and their scan indices
     unsigned mt[624];
     float buf[RNG_BUF];
-    int run_seg[32];      // segments of the current tie run
-    int run_pre[32];      // their first record's rank in the run
+    int tseg[TAB_CAP];        // super-run segments, their first padded record, record count
+    int tpre[TAB_CAP];
+    int tcnt[TAB_CAP];
 };
 
 // Draw buffer with warp-replicated read pointer: rp/len live in registers of
 // every lane (all lanes execute the same control flow).
 __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int &len) {
-    const int unread = len - rp;   // < RNG_KEEP by construction
+    const int unread = len - rp;   // <= 2 * REC_CAP by construction
     // move the unread draws to the front (destinations never overtake sources)
     __syncwarp();
     for (int q = 0; 32 * q < unread; ++q) {
@@ -749,6 +752,26 @@ __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int
 
 __device__ __forceinline__ void rng_ensure(WarpShared &w, int lane, int &rp, int &len, int need) {
     if (len - rp < need) rng_refill(w, lane, rp, len);
+}
+
+// at least `need` (<= 2 * REC_CAP) unread draws in the buffer
+__device__ void rng_ensure_many(WarpShared &w, int lane, int &rp, int &len, int need) {
+    if (len - rp >= need) return;
+    const int unread = len - rp;
+    __syncwarp();
+    for (int q = 0; 32 * q < unread; ++q) {
+        const int i = lane + 32 * q;
+        const float v = i < unread ? w.buf[rp + i] : 0.f;
+        __syncwarp();
+        if (i < unread) w.buf[i] = v;
+        __syncwarp();
+    }
+    len = unread;
+    rp = 0;
+    while (len < need) {
+        mt_twist<true>(w.mt, lane, w.buf + len);
+        len += 624;
+    }
 }
 
 // advance the stream by n draws; whole blocks of 624 only regenerate the state
@@ -976,75 +999,73 @@ __device__ __forceinline__ void replay_chunk_ties(int K, bool tie, int m, unsign
     rp += 2 * nt;
 }
 
-// Multi-segment tie path: the state's K values all equal the K-th value V
-// and nothing in the run exceeds V, so every record equal to V is a tie
-// (xes = K, two draws, cpt + 1) and the others are no-ops.  The run is up to
-// RUN_RECORDS records of consecutive candidate segments (tables in w.run_*);
-// lane l composes the slot maps of run records 8l..8l+7 on its own and one
-// warp reduction per run combines them.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One tie super-run: no record of the run exceeds the K-th value V of the
+// state, so the state's values stay as they are, every record equal to V is a
+// tie (two draws, cpt + 1, a swap inside the xes tail slots that hold V and a
+// possible replacement at K-1) and the others are no-ops.  The run's segments
+// (w.tseg/tpre/tcnt, E entries, Tp padded records) are copied to shared memory
+// with 16-byte asynchronous copies; lane l then owns a contiguous range of
+// the run, counts its ties, composes the slot maps of its ties on its own,
+// and one warp reduction combines the 32 lane maps in order.
 template <int KM>
-__device__ __forceinline__ void replay_run_ties(int K, float V, int T, int r, const WarpShared &w, const float *rv,
-                                                const int *ri, unsigned (&cp)[KM], unsigned &cpt, int &rp,
-                                                WarpShared &wm, int &len, int lane) {
+__device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const float *rv, const int *ri, unsigned (&cp)[KM],
+                                 unsigned &cpt, int &rp, int &len, WarpShared &w, int lane) {
     const unsigned FULL = 0xffffffffu;
-    const int j0 = 8 * lane;
-    int seg = 0;
-    if (j0 < T) {
-        // last run segment whose first record is at or before j0
-        int lo = 0, hi = r - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (w.run_pre[mid] <= j0) lo = mid;
-            else hi = mid - 1;
+    for (int e = 0; e < E; ++e) {
+        const int sgm = w.tseg[e], pre = w.tpre[e], c = w.tcnt[e];
+        if (4 * lane < c) {
+            const long long src = (long long)sgm * QSK_SEG + 4 * lane;
+            cp_async16(&w.rv_s[pre + 4 * lane], rv + src);
+            cp_async16(&w.ri_s[pre + 4 * lane], ri + src);
         }
-        seg = lo;
     }
-    float vv[8];
-    int mi[8];
+    cp_async_wait_all();
+    __syncwarp();
+    for (int e = lane; e < E; e += 32) {
+        const int c = w.tcnt[e], pre = w.tpre[e];
+        for (int k = c; k < ((c + 3) & ~3); ++k) w.rv_s[pre + k] = -CUDART_INF_F;
+    }
+    __syncwarp();
+    const int P = (Tp + 31) >> 5;
+    const int j0 = lane * P;
+    const int j1 = min(Tp, j0 + P);
     int mine = 0;
+    for (int j = j0; j < j1; ++j) mine += (w.rv_s[j] == V) ? 1 : 0;
+    int incl = mine;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int j = j0 + q;
-        vv[q] = -CUDART_INF_F;
-        mi[q] = 0;
-        if (j < T) {
-            while (seg + 1 < r && w.run_pre[seg + 1] <= j) ++seg;
-            const long long a = (long long)w.run_seg[seg] * QSK_SEG + (j - w.run_pre[seg]);
-            vv[q] = rv[a];
-            mi[q] = ri[a];
-        }
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, off);
+        if (lane >= off) incl += y;
     }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) mine += (vv[q] == V) ? 1 : 0;
-    // exclusive prefix of the per-lane tie counts (0..8) from four ballots
-    const unsigned lt = lanemask_lt();
-    const unsigned b0 = __ballot_sync(FULL, mine & 1), b1 = __ballot_sync(FULL, mine & 2),
-                   b2 = __ballot_sync(FULL, mine & 4), b3 = __ballot_sync(FULL, mine & 8);
-    int rank = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt) + 8 * __popc(b3 & lt);
-    const int total = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2) + 8 * __popc(b3);
-    rng_ensure(wm, lane, rp, len, 2 * total);
-    const float *buf = wm.buf;
+    const int total = __shfl_sync(FULL, incl, 31);
+    int rank = incl - mine;
+    rng_ensure_many(w, lane, rp, len, 2 * total);
     int o[KM];
 #pragma unroll
-    for (int s = 0; s < KM; ++s) o[s] = s;
+    for (int s2 = 0; s2 < KM; ++s2) o[s2] = s2;
+    for (int j = j0; j < j1; ++j) {
+        if (w.rv_s[j] != V) continue;
+        const float u1 = w.buf[rp + 2 * rank];
+        const float u2 = w.buf[rp + 2 * rank + 1];
+        int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
+        if (x > K - 1) x = K - 1;
+        const unsigned after = cpt + unsigned(rank) + 1u;
+        const bool write = __fmul_rn(__uint2float_rn(unsigned(xes) + after), u2) < (float)xes;
+        // op = (write at K-1) o (swap x, K-1); composed after the lane's earlier ops
+        const int ox = sel_i<KM>(o, x), ok1 = sel_i<KM>(o, K - 1);
+        const int wr = -(w.ri_s[j] + 1);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        if (vv[q] == V) {
-            const float u1 = buf[rp + 2 * rank];
-            const float u2 = buf[rp + 2 * rank + 1];
-            int x = int(floorf(__fmul_rn(u1, (float)K)));
-            if (x > K - 1) x = K - 1;
-            const unsigned after = cpt + unsigned(rank) + 1u;
-            const bool write = __fmul_rn(__uint2float_rn(unsigned(K) + after), u2) < (float)K;
-            // op = (write at K-1) o (swap x, K-1); composed after the lane's earlier ops
-            const int ox = sel_i<KM>(o, x), ok1 = sel_i<KM>(o, K - 1);
-#pragma unroll
-            for (int s2 = 0; s2 < KM; ++s2) {
-                if (s2 == x) o[s2] = ok1;
-                if (s2 == K - 1) o[s2] = write ? -(mi[q] + 1) : ox;
-            }
-            ++rank;
+        for (int s2 = 0; s2 < KM; ++s2) {
+            if (s2 == x) o[s2] = ok1;
+            if (s2 == K - 1) o[s2] = write ? wr : ox;
         }
+        ++rank;
     }
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -1069,11 +1090,78 @@ __device__ __forceinline__ void replay_run_ties(int K, float V, int T, int r, co
     for (int s2 = 0; s2 < KM; ++s2) cp[s2] = np[s2];
     cpt += unsigned(total);
     rp += 2 * total;
+    __syncwarp();
+}
+
+// Tie stream (the state holds K finite values, the K-th is V, xes of them
+// equal V): segments from `sg` on whose maximum is V are ties or no-ops,
+// those below V are skipped, and the first segment above V ends the stream.  Segments are gathered into super-runs of
+// at most REC_CAP padded records and TAB_CAP segments.  Returns the first
+// segment above V, or nseg.
+template <int KM>
+__device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, const float *rv, const int *ri, const int *rc,
+                                 const float *rm, unsigned (&cp)[KM], unsigned &cpt, int &rp, int &len, WarpShared &w,
+                                 int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lt = lanemask_lt();
+    for (;;) {
+        int E = 0, Tp = 0, stop = -1;
+        for (;;) {
+            if (sg >= nseg) {
+                stop = nseg;
+                break;
+            }
+            const int q = sg + lane;
+            const int c = q < nseg ? rc[q] : 0;
+            const float m = q < nseg ? rm[q] : -CUDART_INF_F;
+            const unsigned brk = __ballot_sync(FULL, c > 0 && m > V);
+            const unsigned lim = brk ? ((1u << (__ffs(brk) - 1)) - 1u) : FULL;
+            const bool elig = ((lim >> lane) & 1u) && c > 0 && m == V;
+            const int pc = elig ? ((c + 3) & ~3) : 0;
+            int incl = pc;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, off);
+                if (lane >= off) incl += y;
+            }
+            const unsigned EL = __ballot_sync(FULL, elig);
+            const int epos = E + __popc(EL & lt);
+            // the limits are monotone in lane order: the taken lanes are a prefix of EL
+            const bool take = elig && Tp + incl <= REC_CAP && epos < TAB_CAP;
+            const unsigned TK = __ballot_sync(FULL, take);
+            if (take) {
+                w.tseg[epos] = q;
+                w.tpre[epos] = Tp + incl - pc;
+                w.tcnt[epos] = c;
+            }
+            const int hi = TK ? 31 - __clz(TK) : 0;
+            const int add = __shfl_sync(FULL, incl, hi);
+            if (TK) {
+                Tp += add;
+                E += __popc(TK);
+            }
+            const unsigned left = EL & ~TK;
+            if (left) {   // capacity reached: the next run starts at the first segment left out
+                sg += __ffs(left) - 1;
+                break;
+            }
+            if (brk) {
+                sg += __ffs(brk) - 1;
+                stop = sg;
+                break;
+            }
+            sg += 32;
+        }
+        __syncwarp();
+        if (E > 0) replay_super_run<KM>(K, V, xes, E, Tp, rv, ri, cp, cpt, rp, len, w, lane);
+        if (stop >= 0) return stop;
+    }
 }
 
 template <int KM>
 __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
-    __shared__ WarpShared wsh[RP_WARPS];
+    extern __shared__ __align__(16) unsigned char rp_smem[];
+    WarpShared *wsh = reinterpret_cast<WarpShared *>(rp_smem);
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * RP_WARPS + wib;
     if (b >= A.nslots) return;
@@ -1140,99 +1228,75 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
         const int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
         const int *rc = A.rec_cnt + (long long)b * g.nseg;
         const float *rm = A.rec_max + (long long)b * g.nseg;
-        // segment counts and maxima, 32 segments per group, loaded two groups ahead
-        int c1 = lane < g.nseg ? rc[lane] : 0, c2 = 32 + lane < g.nseg ? rc[32 + lane] : 0;
-        float m1 = lane < g.nseg ? rm[lane] : -CUDART_INF_F, m2 = 32 + lane < g.nseg ? rm[32 + lane] : -CUDART_INF_F;
-        for (int s0 = 0; s0 < g.nseg; s0 += 32) {
-            const int myc = c1;
-            const float mym = m1;
-            c1 = c2;
-            m1 = m2;
-            const int s2 = s0 + 64 + lane;
-            c2 = s2 < g.nseg ? rc[s2] : 0;
-            m2 = s2 < g.nseg ? rm[s2] : -CUDART_INF_F;
-            unsigned nz = __ballot_sync(FULL, myc > 0 && mym >= sel_f<KM>(cv, K - 1));
+        // general replay of one segment's records, 32 per step
+        auto general_segment = [&](int sg, int cnt, float smax) {
+            const long long base = (long long)sg * QSK_SEG;
+            int r0 = 0;
+            while (r0 < cnt) {
+                const float kth0 = sel_f<KM>(cv, K - 1);
+                if (smax < kth0) break;   // nothing left in this segment can enter
+                const bool filling = (kth0 == -CUDART_INF_F);
+                const int width = filling ? 1 : 32;
+                const int j = r0 + lane;
+                const bool valid = lane < width && j < cnt;
+                const float v = valid ? rv[base + j] : -CUDART_INF_F;
+                const int m = valid ? ri[base + j] : 0;
+                if (!filling && __ballot_sync(FULL, valid && v >= kth0) == 0) {
+                    r0 += width;
+                    continue;
+                }
+                if (filling && !emit_masked) {
+                    // masked positions between the previous record and this one are
+                    // -inf ties while fewer than K finite values have been seen:
+                    // two draws and one cpt increment each, no visible slot change
+                    const long long mm = __shfl_sync(FULL, (long long)m, 0);
+                    long long c = (mm - (last + 1)) - (valid_prefix(g, s.lo, mm) - valid_prefix(g, s.lo, last + 1));
+                    if (c > 0) {
+                        rng_skip(w, lane, rp, len, 2 * c);
+                        cpt += unsigned(c);
+                    }
+                }
+                rng_ensure(w, lane, rp, len, 64);
+                // all K state values equal and nothing above them in the chunk
+                if (!filling && sel_f<KM>(cv, 0) == kth0 && __ballot_sync(FULL, valid && v > kth0) == 0) {
+                    replay_chunk_ties<KM>(K, valid && v == kth0, m, cp, cpt, rp, w.buf, lane);
+                } else {
+                    replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
+                }
+                const unsigned vb = __ballot_sync(FULL, valid);
+                last = __shfl_sync(FULL, (long long)m, 31 - __clz(vb));
+                r0 += width;
+            }
+        };
+        int sg = 0;
+        while (sg < g.nseg) {
+            const float kth_s = sel_f<KM>(cv, K - 1);
+            if (kth_s != -CUDART_INF_F) {
+                // K finite values: tie super-runs up to the first segment above V
+                int xes = 0;
+#pragma unroll
+                for (int q = 0; q < KM; ++q) xes += (q < K && cv[q] == kth_s) ? 1 : 0;
+                sg = replay_tie_stream<KM>(K, kth_s, xes, sg, g.nseg, rv, ri, rc, rm, cp, cpt, rp, len, w, lane);
+                if (sg >= g.nseg) break;
+                general_segment(sg, rc[sg], rm[sg]);
+                ++sg;
+                continue;
+            }
+            // general replay, 32 segments at a time, until K finite values are held
+            const int myc = sg + lane < g.nseg ? rc[sg + lane] : 0;
+            const float mym = sg + lane < g.nseg ? rm[sg + lane] : -CUDART_INF_F;
+            unsigned nz = __ballot_sync(FULL, myc > 0 && mym >= kth_s);
+            int next = sg + 32;
             while (nz) {
                 const int l = __ffs(nz) - 1;
                 nz &= nz - 1;
-                const int sg = s0 + l;
-                const int cnt = __shfl_sync(FULL, myc, l);
-                const float smax = __shfl_sync(FULL, mym, l);
-                const long long base = (long long)sg * QSK_SEG;
-                {
-                    const float kth0 = sel_f<KM>(cv, K - 1);
-                    if (kth0 != -CUDART_INF_F && sel_f<KM>(cv, 0) == kth0 && smax <= kth0) {
-                        // the whole segment is ties or no-ops
-                        if (smax == kth0) {
-                            // run: this segment and the group's next candidates up to the
-                            // first one above V, at most RUN_RECORDS records
-                            const bool in_rest = (((nz | (1u << l)) >> lane) & 1u) != 0;
-                            const unsigned above = __ballot_sync(FULL, in_rest && mym > kth0);
-                            const unsigned below = above ? ((1u << (__ffs(above) - 1)) - 1u) : FULL;
-                            const bool cand = in_rest && ((below >> lane) & 1u) && myc > 0 && mym == kth0;
-                            const int c = cand ? myc : 0;
-                            int incl = c;
-#pragma unroll
-                            for (int off = 1; off < 32; off <<= 1) {
-                                const int y = __shfl_up_sync(FULL, incl, off);
-                                if (lane >= off) incl += y;
-                            }
-                            const bool take = cand && incl <= RUN_RECORDS;
-                            const unsigned R = __ballot_sync(FULL, take);
-                            if (take) {
-                                const int pos = __popc(R & lanemask_lt());
-                                w.run_seg[pos] = s0 + lane;
-                                w.run_pre[pos] = incl - c;
-                            }
-                            const int hi = 31 - __clz(R);
-                            const int T = __shfl_sync(FULL, incl, hi);
-                            __syncwarp();
-                            replay_run_ties<KM>(K, kth0, T, __popc(R), w, rv, ri, cp, cpt, rp, w, len, lane);
-                            __syncwarp();
-                            // the run's segments and the no-op ones between them are done
-                            nz &= (hi >= 31) ? 0u : ~((2u << hi) - 1u);
-                        }
-                        continue;
-                    }
-                }
-                int r0 = 0;
-                while (r0 < cnt) {
-                    const float kth0 = sel_f<KM>(cv, K - 1);
-                    if (smax < kth0) break;   // nothing left in this segment can enter
-                    const bool filling = (kth0 == -CUDART_INF_F);
-                    const int width = filling ? 1 : 32;
-                    const int j = r0 + lane;
-                    const bool valid = lane < width && j < cnt;
-                    const float v = valid ? rv[base + j] : -CUDART_INF_F;
-                    const int m = valid ? ri[base + j] : 0;
-                    if (!filling && __ballot_sync(FULL, valid && v >= kth0) == 0) {
-                        r0 += width;
-                        continue;
-                    }
-                    if (filling && !emit_masked) {
-                        // masked positions between the previous record and this one are
-                        // -inf ties while fewer than K finite values have been seen:
-                        // two draws and one cpt increment each, no visible slot change
-                        const long long mm = __shfl_sync(FULL, (long long)m, 0);
-                        long long c = (mm - (last + 1)) - (valid_prefix(g, s.lo, mm) - valid_prefix(g, s.lo, last + 1));
-                        if (c > 0) {
-                            rng_skip(w, lane, rp, len, 2 * c);
-                            cpt += unsigned(c);
-                        }
-                    }
-                    rng_ensure(w, lane, rp, len, 64);
-                    // all K state values equal and nothing above them in the chunk
-                    if (!filling && sel_f<KM>(cv, 0) == kth0 &&
-                        __ballot_sync(FULL, valid && v > kth0) == 0) {
-                        replay_chunk_ties<KM>(K, valid && v == kth0, m, cp, cpt, rp, w.buf, lane);
-                    } else {
-                        replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
-                    }
-                    const unsigned vb = __ballot_sync(FULL, valid);
-                    last = __shfl_sync(FULL, (long long)m, 31 - __clz(vb));
-                    r0 += width;
+                general_segment(sg + l, __shfl_sync(FULL, myc, l), __shfl_sync(FULL, mym, l));
+                if (sel_f<KM>(cv, K - 1) != -CUDART_INF_F) {
+                    next = sg + l + 1;
+                    break;
                 }
             }
+            sg = next;
         }
         // merge loop (quantileSamplingModule.hpp:546-557): repeated first-max extraction
         float fv[KM];
@@ -1706,12 +1770,27 @@ cudaError_t set_map_smem_limit(int bytes) {
 }
 
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
+    static bool configured[64] = {};
+    const size_t smem = sizeof(WarpShared) * RP_WARPS;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!configured[dev]) {
+        if ((e = cudaFuncSetAttribute(k_replay<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+            return e;
+        configured[dev] = true;
+    }
     unsigned blocks = (unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS);
-    if (a.K <= 1) k_replay<1><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
-    else if (a.K <= 2) k_replay<2><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
-    else if (a.K <= 4) k_replay<4><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
-    else if (a.K <= 8) k_replay<8><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
-    else k_replay<16><<<blocks, 32 * RP_WARPS, 0, st>>>(a);
+    if (a.K <= 1) k_replay<1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 2) k_replay<2><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 4) k_replay<4><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 8) k_replay<8><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else k_replay<16><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
