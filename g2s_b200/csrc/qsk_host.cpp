@@ -391,7 +391,7 @@ static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int n
         }
     }
     if (all_cat) {
-        t->pw = int((t->g.N + 31) / 32) + 2;
+        t->pw = plane_words(t->g.N);
         if ((e = t->ncat.alloc(nvar)) != cudaSuccess) return bail(e);
         if ((e = t->catv.alloc(catv.size())) != cudaSuccess) return bail(e);
         if ((e = t->planes.alloc(size_t(nvar) * (QSK_CMAX + 1) * t->pw)) != cudaSuccess) return bail(e);

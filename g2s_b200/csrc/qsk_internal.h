@@ -122,10 +122,17 @@ struct MapArgs {
     float *rec_max;   // [slot][nseg] largest valid score of the segment
 };
 
+// Bit-plane layout: every plane is `plane_words(N)` words, of which the
+// first `plane_guard(N)` are zero and word plane_guard(N) + w holds positions
+// 32w..32w+31; the guard and the zero tail make every funnel-shifted read of
+// the map kernel, for any term offset, an in-bounds read without a test.
+__host__ __device__ inline int plane_guard(long long N) { return int((N + 31) / 32) + 1; }
+__host__ __device__ inline int plane_words(long long N) { return plane_guard(N) + int((N + 31) / 32) + 34; }
+
 struct BitArgs {
     Geom g;
     const unsigned *planes;   // [var][QSK_CMAX+1][pw] words (slot QSK_CMAX all zero)
-    int pw;                   // words per plane (ceil(N/32) + 2)
+    int pw;                   // words per plane: plane_words(N)
     const int *ncat;          // categories per variable
     const float *catv;        // [var][QSK_CMAX] category codes
     const Slot *slots;

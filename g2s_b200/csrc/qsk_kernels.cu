@@ -1382,11 +1382,11 @@ __global__ void k_build_planes(const float *__restrict__ layers, Geom g, int nva
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long total = (long long)nvar * (QSK_CMAX + 1) * pw;
     if (idx >= total) return;
-    int w = int(idx % pw);
+    const int w = int(idx % pw) - plane_guard(g.N);   // data word (negative: guard)
     int vc = int(idx / pw);
     int c = vc % (QSK_CMAX + 1), v = vc / (QSK_CMAX + 1);
     unsigned word = 0;
-    if (c < ncat[v]) {
+    if (w >= 0 && c < ncat[v]) {
         float cv = catv[v * QSK_CMAX + c];
         for (int b = 0; b < 32; ++b) {
             long long q = (long long)w * 32 + b;
@@ -1431,7 +1431,9 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             const int nc = A.ncat[v];
             for (int q = 0; q < nc; ++q)
                 if (A.catv[v * QSK_CMAX + q] == tm.b) { c = q; break; }
-            bterm[t] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw, d);
+            // positions 32k..32k+31 read source bits from word k + floor(-d/32),
+            // shifted right by (-d) mod 32
+            bterm[t] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw + plane_guard(g.N) + ((-d) >> 5), (-d) & 31);
         }
         if (threadIdx.x == 0) nbt = ss.nterms;
     }
@@ -1448,9 +1450,34 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
 
     for (int sg = seg_begin + warp; sg < seg_end; sg += nwarps) {
         const long long m0 = (long long)sg * 1024 + 32 * lane;
-        // validity of the lane's 32 positions (incremental digits)
+        // validity of the lane's 32 positions
         unsigned vmask = 0, emask = 0;
-        if (m0 < g.N) {
+        if (m0 < g.N && g.fft[0] >= 32) {
+            // the 32 positions lie in at most two rows of the x dimension
+            const long long rem = g.N - m0;
+            emask = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
+            const int X = g.fft[0];
+            const long long r0 = m0 / X;
+            const int x0 = int(m0 - r0 * X);
+            auto row_ok = [&](long long r) {
+                bool ok = true;
+#pragma unroll
+                for (int d = 1; d < QSK_MAXD; ++d)
+                    if (d < g.nd) ok &= int((r / (g.sstride[d] / X)) % g.fft[d]) >= ss.lo[d];
+                return ok;
+            };
+            auto range = [](int a, int b) -> unsigned {   // bits [a, b), 0 <= a, b <= 32
+                if (a >= b) return 0u;
+                const unsigned hi = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+                return hi & ~((1u << a) - 1u);
+            };
+            const int first = X - x0;   // positions p < first are in row r0
+            unsigned m = 0;
+            if (row_ok(r0)) m |= range(max(0, ss.lo[0] - x0), min(32, first));
+            if (first < 32 && row_ok(r0 + 1)) m |= range(min(32, first + ss.lo[0]), 32);
+            vmask = m & emask;
+        } else if (m0 < g.N) {
+            // narrow x dimension: incremental digits
             int dig[QSK_MAXD];
 #pragma unroll
             for (int d = 0; d < QSK_MAXD; ++d) dig[d] = d < g.nd ? int((m0 / g.sstride[d]) % g.fft[d]) : 0;
@@ -1478,14 +1505,10 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
         if (vmask) {
             const int im0 = int(m0);
+            const unsigned *P = A.planes + (im0 >> 5);
             auto match = [&](int t) -> unsigned {
                 const int2 bt = bterm[t];
-                const unsigned *P = A.planes + bt.x;
-                const int q0 = im0 - bt.y;
-                const int wi = q0 >> 5;
-                const unsigned w0 = wi >= 0 ? __ldg(P + wi) : 0u;
-                const unsigned w1 = wi + 1 >= 0 ? __ldg(P + wi + 1) : 0u;
-                return __funnelshift_r(w0, w1, unsigned(q0) & 31u);
+                return __funnelshift_r(__ldg(P + bt.x), __ldg(P + bt.x + 1), unsigned(bt.y));
             };
             auto csa = [](unsigned &h, unsigned &l, unsigned a, unsigned b, unsigned c) {
                 const unsigned u = a ^ b;
