@@ -42,6 +42,10 @@ DI_SHAPE = (500, 500)
 N_NB, K_CAND, SEED = 80, 1.5, 100
 WORKLOAD = "config1-categorical-channels-250x250-to-500x500-n80-k1.5"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes (read + write) per launch, averaged over every launch of one
+# step of the default workload, from one ncu capture of this script
+# (dram__bytes_read.sum + dram__bytes_write.sum; cold-cache, launches serialised)
+TRAFFIC_PER_LAUNCH = {("config1", "k_replay"): 13.70e6, ("config1", "k_map_bits"): 11.50e6}
 
 
 def peaks():
@@ -196,6 +200,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--workload", default="config1", choices=["config1", "config0"],
                     help="config1 (default, the benchmark line) or config0 (continuous GRF 200x200, n=50, k=1.2)")
+    ap.add_argument("--di-side", type=int, default=0,
+                    help="simulate an SxS grid instead of the workload's (small cases for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -222,6 +228,9 @@ def main():
         types = [0]
     else:
         ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
+    if args.di_side > 0:
+        DI_SHAPE = (args.di_side, args.di_side)
+        WORKLOAD += f"-grid{args.di_side}x{args.di_side}"
     di = np.full(DI_SHAPE, np.nan, np.float32)
     seed = replica_seed(SEED, rank)
     sim = g2s.Simulation(ti, di, types, n=N_NB, k=K_CAND, seed=seed, device=dev)
@@ -255,21 +264,34 @@ def main():
     total_ms = slowest(total_ms, dist, f"cuda:{dev}")
     value = whole_job_rate(nodes, args.steps, ws, total_ms)
 
-    # roofline of the dominant kernel (fused map + record filter): one extra
-    # profiled step records events around every launch
+    # roofline of the dominant kernel: one extra profiled step records events
+    # around every launch.  Algorithmic bytes per node (survey of the
+    # reference path): the fused map reads 4*N*L bytes of correlation layers,
+    # the k-best scan 4*N bytes of scores.
     sim.set_profiling(True)
     sim.run()
     pinf = sim.info()
     sim.set_profiling(False)
-    # categorical TI with a uniform kernel: bit-sliced map kernel
-    map_kernel = "bits" if types == [1] else "fp32"
+    map_kernel = "k_map_bits" if types == [1] else "k_map_records"
     N = TI_SHAPE[0] * TI_SHAPE[1]
-    L = 2  # 2 correlation layers: TI^2 and TI (continuous) / 2 class indicators (binary categorical)
-    bytes_per_node = 4 * N * L
-    map_avg_ms = pinf["ms_map"] / max(pinf["map_launches"], 1)
-    nodes_per_launch = pinf["map_positions"] / max(pinf["map_launches"], 1) / N
-    achieved = bytes_per_node * nodes_per_launch / (map_avg_ms / 1000.0) / 1e9
+    L = 2  # continuous: TI^2 and TI; binary categorical: 2 class indicators
+    launches_l = max(pinf["map_launches"], 1)
+    nodes_per_launch = pinf["map_positions"] / launches_l / N
     peak, peak_kind = peaks()
+    kernels = {}
+    for name, ms, bpn in ((map_kernel, pinf["ms_map"], 4 * N * L), ("k_replay", pinf["ms_replay"], 4 * N)):
+        avg_ms = ms / launches_l
+        ach = bpn * nodes_per_launch / (avg_ms / 1000.0) / 1e9
+        kernels[name] = {"ms_per_step": ms, "launches": launches_l, "avg_launch_ms": avg_ms,
+                         "algorithmic_bytes_per_node": bpn, "achieved": ach, "frac": ach / peak,
+                         "share_of_step": ms / max(pinf["ms_total"], 1e-9),
+                         "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, name)) if args.di_side == 0 else None}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    roofline = {"bound": "hbm", "achieved": kernels[dom]["achieved"], "peak": peak, "unit": "GB/s",
+                "frac": kernels[dom]["frac"], "traffic": kernels[dom]["traffic"], "kernel": dom,
+                "peak_kind": f"{peak_kind} hbm_gbs", "nodes_per_launch": nodes_per_launch,
+                "algorithmic_bytes": f"{map_kernel}: 4*N*L per node, k_replay: 4*N per node (N={N}, L={L})",
+                "kernels": kernels}
     out_info = sim.info()
     sim.close()
 
@@ -297,15 +319,13 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "path": "plain FP32 map + exact reservoir k-best (CUDA cores)",
+            "dtype": "u8" if types == [1] else "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD,
+                       "path": ("bit-sliced categorical match counts (equal to the FP32 map)" if types == [1] else
+                                "FP32 direct-sum map") + " + exact reservoir k-best replay (CUDA cores)",
                        "nodes_per_step": nodes, "levels": out_info["levels"], "max_batch": out_info["max_batch"],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "k_map_bits" if map_kernel == "bits" else "k_map_records",
-                         "algorithmic_bytes": f"4*N*L per node, N={N}, L={L}", "peak_kind": f"{peak_kind} hbm_gbs",
-                         "map_ms_avg": map_avg_ms, "nodes_per_launch": nodes_per_launch,
-                         "share_of_step": pinf["ms_map"] / max(pinf["ms_total"], 1e-9)},
+            "roofline": roofline,
             "breakdown_ms": {"neighbours": pinf["ms_setup_neighbours"], "levels": pinf["ms_levels"],
                              "prep": pinf["ms_prep"], "map": pinf["ms_map"], "replay": pinf["ms_replay"],
                              "total": pinf["ms_total"]},
