@@ -37,7 +37,10 @@ class QskTerm(ctypes.Structure):
 class QskParams(ctypes.Structure):
     _fields_ = [("ndim", ctypes.c_int), ("ti_dims", _u32p), ("nvar", ctypes.c_int), ("types", _i32p),
                 ("ti", _f32p), ("di_dims", _u32p), ("kernel_dims", _u32p), ("kernel", _f32p),
-                ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint), ("no_verbatim", ctypes.c_int)]
+                ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint), ("no_verbatim", ctypes.c_int),
+                ("n_counts", ctypes.c_int), ("n_per_variable", _i32p), ("n_image_vars", ctypes.c_int),
+                ("n_image", _f32p), ("k_image", _f32p), ("n_kernels", ctypes.c_int), ("kernels_dims", _u32p),
+                ("kernels", ctypes.POINTER(_f32p)), ("kernel_index_image", _f32p)]
 
 
 class QskPatternOpts(ctypes.Structure):
@@ -261,7 +264,13 @@ class Simulation:
     """A QS vector simulation resident on one GPU."""
 
     def __init__(self, ti: np.ndarray, di: np.ndarray, types: Sequence[int], n: int, k: float, seed: int,
-                 kernel: Optional[np.ndarray] = None, device: int = 0, no_verbatim: bool = False):
+                 kernel: Optional[np.ndarray] = None, device: int = 0, no_verbatim: bool = False,
+                 n_per_var: Optional[Sequence[int]] = None, ni: Optional[np.ndarray] = None,
+                 kvi: Optional[np.ndarray] = None, kernels: Optional[Sequence[np.ndarray]] = None,
+                 kii: Optional[np.ndarray] = None):
+        """Local controls as in G2S: ``n_per_var`` (-n n1 n2 ...), ``ni``
+        (-ni image, grid shape [+ counts]), ``kvi`` (-kvi image), ``kernels``
+        (the -ki list) with ``kii`` (-kii image of kernel indices)."""
         self.nvar = len(types)
         self._ti = np.ascontiguousarray(ti, dtype=np.float32)
         self._di = np.ascontiguousarray(di, dtype=np.float32)
@@ -273,6 +282,34 @@ class Simulation:
         self.params = QskParams(len(self._tdims), _p(self._tdims, _u32p), self.nvar, _p(self._types, _i32p),
                                 _p(self._ti, _f32p), _p(self._ddims, _u32p), _p(self._kdims, _u32p),
                                 _p(self._kern, _f32p), int(n), float(k), int(seed) & 0xffffffff, int(no_verbatim))
+        cells = int(np.prod(self._ddims))
+        self._keep = []
+
+        def keep(a, dt):
+            x = np.ascontiguousarray(a, dtype=dt).ravel()
+            self._keep.append(x)
+            return x
+
+        if n_per_var is not None:
+            a = keep(n_per_var, np.int32)
+            self.params.n_counts = a.size
+            self.params.n_per_variable = _p(a, _i32p)
+        if ni is not None:
+            a = keep(ni, np.float32)
+            self.params.n_image_vars = max(1, a.size // cells)
+            self.params.n_image = _p(a, _f32p)
+        if kvi is not None:
+            self.params.k_image = _p(keep(kvi, np.float32), _f32p)
+        if kernels is not None:
+            arrs = [keep(kq, np.float32) for kq in kernels]
+            dims = keep(np.concatenate([_grid_dims(np.asarray(kq), self.nvar) for kq in kernels]), np.uint32)
+            ptrs = (_f32p * len(arrs))(*[_p(a, _f32p) for a in arrs])
+            self._keep.append(ptrs)
+            self.params.n_kernels = len(arrs)
+            self.params.kernels_dims = _p(dims, _u32p)
+            self.params.kernels = ptrs
+        if kii is not None:
+            self.params.kernel_index_image = _p(keep(kii, np.float32), _f32p)
         h = ctypes.c_void_p()
         _check(lib().qsk_sim_create(device, ctypes.byref(self.params), _p(self._di, _f32p), ctypes.byref(h)),
                "qsk_sim_create")
@@ -329,11 +366,22 @@ class Simulation:
             pass
 
 
-def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n: int, s: int,
-       ki: Optional[np.ndarray] = None, nV: bool = False, device: int = 0):
+def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
+       ki=None, nV: bool = False, ni: Optional[np.ndarray] = None, kvi: Optional[np.ndarray] = None,
+       kii: Optional[np.ndarray] = None, device: int = 0):
     """QuickSampling on one GPU; arguments named after the G2S flags
-    (-ti -di -dt -k -n -s -ki -nV).  Returns (simulation, index) as G2S does."""
-    sim = Simulation(ti, di, dt, n=n, k=k, seed=s, kernel=ki, device=device, no_verbatim=nV)
+    (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii).  ``n`` is one count or one
+    per variable; ``ki`` one kernel or a list of kernels (selected per cell by
+    ``kii``).  Returns (simulation, index) as G2S does."""
+    n_list = None
+    if np.ndim(n) > 0:
+        n_list = [int(x) for x in np.ravel(n)]
+        n = max(n_list)
+    kernel, kernels = ki, None
+    if isinstance(ki, (list, tuple)):
+        kernel, kernels = None, list(ki)
+    sim = Simulation(ti, di, dt, n=n if n is not None else 0, k=k, seed=s, kernel=kernel, device=device,
+                     no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii)
     try:
         sim.run()
         out, idx, _ = sim.read()

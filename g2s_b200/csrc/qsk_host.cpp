@@ -200,6 +200,7 @@ int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms
     s.seed = seed;
     s.sel = 0;
     s.excl = -1;
+    s.K = int(K);
     int mn[QSK_MAXD] = {0}, mx[QSK_MAXD] = {0};
     for (int j = 0; j < nnb; ++j)
         for (int d = 0; d < nd; ++d) {
@@ -615,6 +616,12 @@ struct qsk_sim {
     std::vector<int> node_of_cell;   // per cell
     std::vector<float> init;         // grid before simulation
     int ntpl = 0;
+    // local controls: per kernel template range (begin, count); per path
+    // node kernel, neighbour limit, neighbour count per variable, k
+    std::vector<int> tpl_range;
+    std::vector<int> node_kernel, node_lim, node_nv;
+    std::vector<float> node_k;
+    bool local = false;
     // device
     DBuf<int> d_tpl, d_types;
     DBuf<float> d_wtab, d_seeds, d_init, d_state;
@@ -627,6 +634,8 @@ struct qsk_sim {
     DBuf<float> d_rec_val;
     DBuf<int> d_rec_idx, d_rec_cnt;
     DBuf<float> d_rec_max;
+    DBuf<int> d_tpl_range, d_node_kernel, d_node_lim, d_node_nv;
+    DBuf<float> d_node_k;
     int maxterms = 0;
     int max_slots = 0;
     bool use_bits = false;
@@ -702,8 +711,16 @@ int make_template(int nd, int nvar, const unsigned *kdims, const float *kernel, 
     return ntpl;
 }
 
-void build_template(qsk_sim *s, const unsigned *kdims, const float *kernel) {
-    s->ntpl = make_template(s->nd, s->nvar, kdims, kernel, s->tpl, s->wtab);
+// append one kernel's template and weights to the concatenated tables
+void add_template(qsk_sim *s, const unsigned *kdims, const float *kernel) {
+    std::vector<int> t;
+    std::vector<float> w;
+    int nt = make_template(s->nd, s->nvar, kdims, kernel, t, w);
+    s->tpl_range.push_back(s->ntpl);
+    s->tpl_range.push_back(nt);
+    s->tpl.insert(s->tpl.end(), t.begin(), t.end());
+    s->wtab.insert(s->wtab.end(), w.begin(), w.end());
+    s->ntpl += nt;
 }
 
 // a2: path and per-node seeds (src/qs.cpp:975,1159-1201,1250-1258): informed
@@ -755,8 +772,10 @@ void build_path(qsk_sim *s) {
 
 int sim_neighbours(qsk_sim *s) {
     if (s->neighbours_ready) return QSK_OK;
-    CK(launch_neighbours(s->dg, s->d_tpl.p, s->ntpl, s->d_path.p, s->begin, s->nodes, s->d_post.p, s->n,
-                         s->d_nb_count.p, s->d_nb_tpl.p, s->d_nb_cell.p, s->st));
+    CK(launch_neighbours(s->dg, s->d_tpl.p, s->ntpl, s->d_path.p, s->begin, s->nodes,
+                         s->d_post.p, s->n, s->d_nb_count.p, s->d_nb_tpl.p, s->d_nb_cell.p,
+                         s->local ? s->d_node_kernel.p : nullptr, s->local ? s->d_tpl_range.p : nullptr,
+                         s->local ? s->d_node_lim.p : nullptr, s->st));
     s->neighbours_ready = true;
     return QSK_OK;
 }
@@ -807,6 +826,8 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             pa.mask_layer = s->nvar;
             pa.no_verbatim = s->no_verbatim;
             pa.id_image = s->d_id.p;
+            pa.node_nv = s->local ? s->d_node_nv.p : nullptr;
+            pa.node_k = s->local ? s->d_node_k.p : nullptr;
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
@@ -903,9 +924,24 @@ extern "C" {
 int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk_sim **out) {
     if (!p || !out || !di_init || !p->ti_dims || !p->di_dims || !p->types || !p->ti) return fail(QSK_ERR_ARG, "null argument");
     if (p->ndim < 1 || p->ndim > QSK_MAXD) return fail(QSK_ERR_UNSUPPORTED, "ndim %d", p->ndim);
-    if (p->n < 1) return fail(QSK_ERR_ARG, "n must be >= 1");
-    if (!(p->k >= 1.f)) return fail(QSK_ERR_UNSUPPORTED, "k must be >= 1 (got %g)", double(p->k));
-    int K = int(std::ceil(double(p->k)));
+    const bool counts_given = (p->n_counts > 0 && p->n_per_variable) || (p->n_image_vars > 0 && p->n_image);
+    if (p->n < 1 && !counts_given) return fail(QSK_ERR_ARG, "n must be >= 1");
+    if (p->n_counts > 0 && p->n_per_variable)
+        for (int q = 0; q < p->n_counts; ++q)
+            if (p->n_per_variable[q] < 0) return fail(QSK_ERR_ARG, "negative neighbour count");
+    if (p->n_kernels > 1 && !p->kernel_index_image)
+        return fail(QSK_ERR_ARG, "several kernels need a kernel index image (-kii)");
+    if (p->n_kernels > 0 && (!p->kernels_dims || !p->kernels)) return fail(QSK_ERR_ARG, "null kernel list");
+    // -kvi: the module's k becomes max(k, max k_image) (src/qs.cpp:1281-1292)
+    float kbase = p->k;
+    if (p->k_image) {
+        if (!(kbase > 0.f)) kbase = 1.f;
+        long long cells = 1;
+        for (int d = 0; d < p->ndim; ++d) cells *= p->di_dims[d];
+        for (long long c = 0; c < cells; ++c) kbase = std::max(kbase, p->k_image[c]);
+    }
+    if (!(kbase > 0.f)) return fail(QSK_ERR_UNSUPPORTED, "k must be > 0 (got %g)", double(p->k));
+    int K = int(std::ceil(double(kbase)));
     if (K > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "ceil(k)=%d > %d", K, QSK_KMAX);
     DeviceGuard dgd(device);
     qsk_sim *s = new qsk_sim();
@@ -914,7 +950,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     s->nd = p->ndim;
     s->nvar = p->nvar;
     s->n = p->n;
-    s->k = p->k;
+    s->k = kbase;
     s->K = K;
     s->seed = p->seed;
     s->no_verbatim = p->no_verbatim;
@@ -939,16 +975,63 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     }
     if (s->cells >= (1LL << 32) - 1) return bail(fail(QSK_ERR_UNSUPPORTED, "grid too large"));
     s->init.assign(di_init, di_init + size_t(s->cells) * s->nvar);
-    // kernel: given, or uniform of size min(TI/2+1) (src/qs.cpp:1010-1042)
+    // kernels: the -ki list, the given one, or uniform of size min(TI/2+1)
+    // (src/qs.cpp:1000-1042); one sorted template per kernel
     std::vector<unsigned> kd(p->ndim);
-    if (p->kernel && p->kernel_dims) {
+    if (p->n_kernels > 0) {
+        for (int q = 0; q < p->n_kernels; ++q) add_template(s, p->kernels_dims + size_t(q) * p->ndim, p->kernels[q]);
+    } else if (p->kernel && p->kernel_dims) {
         for (int d = 0; d < p->ndim; ++d) kd[d] = p->kernel_dims[d];
-        build_template(s, kd.data(), p->kernel);
+        add_template(s, kd.data(), p->kernel);
     } else {
         for (int d = 0; d < p->ndim; ++d) kd[d] = std::min(p->ti_dims[d] / 2 + 1, p->ti_dims[d]);
-        build_template(s, kd.data(), nullptr);
+        add_template(s, kd.data(), nullptr);
     }
     build_path(s);
+    // local controls per path node (simulation.hpp:337-358,447-507)
+    s->local = counts_given || p->k_image || p->kernel_index_image || p->n_kernels > 1;
+    if (s->local) {
+        const long long nn = std::max<long long>(s->nodes, 1);
+        s->node_kernel.assign(size_t(nn), 0);
+        s->node_lim.assign(size_t(nn), 0);
+        s->node_nv.assign(size_t(nn) * s->nvar, 0);
+        s->node_k.assign(size_t(nn), kbase);
+        const int nk = int(s->tpl_range.size() / 2);
+        int nmax_all = 0;
+        float kmax = kbase;
+        std::vector<int> counts;
+        for (long long i = 0; i < s->nodes; ++i) {
+            const unsigned cell = s->order[s->begin + i];
+            if (p->n_image_vars > 0 && p->n_image) {
+                counts.assign(size_t(p->n_image_vars), 0);
+                for (int q = 0; q < p->n_image_vars; ++q)
+                    counts[q] = int(p->n_image[size_t(cell) * p->n_image_vars + q]);
+            } else if (p->n_counts > 0 && p->n_per_variable) {
+                counts.assign(p->n_per_variable, p->n_per_variable + p->n_counts);
+            } else {
+                counts.assign(1, p->n);
+            }
+            int nmax = 0;
+            for (int v = 0; v < s->nvar; ++v) {
+                int c = std::max(0, counts[size_t(v) % counts.size()]);
+                s->node_nv[size_t(i) * s->nvar + v] = c;
+                nmax = std::max(nmax, c);
+            }
+            // with one count per variable the walk also keeps the next informed cell
+            s->node_lim[size_t(i)] = nmax + (counts.size() > 1 ? 1 : 0);
+            nmax_all = std::max(nmax_all, s->node_lim[size_t(i)]);
+            if (p->kernel_index_image) {
+                int q = int(p->kernel_index_image[cell]);
+                if (q < 0 || q >= nk) return bail(fail(QSK_ERR_ARG, "kernel index %d at cell %u outside [0,%d)", q, cell, nk));
+                s->node_kernel[size_t(i)] = q;
+            }
+            if (p->k_image && p->k_image[cell] > 0.f) s->node_k[size_t(i)] = p->k_image[cell];
+            kmax = std::max(kmax, s->node_k[size_t(i)]);
+        }
+        s->n = std::max(1, nmax_all);
+        s->K = int(std::ceil(double(kmax)));
+        if (s->K > QSK_KMAX) return bail(fail(QSK_ERR_UNSUPPORTED, "ceil(k)=%d > %d", s->K, QSK_KMAX));
+    }
     s->maxterms = std::max(1, s->n * s->nvar * (s->ti->missing ? 2 : 1));
     // bit-sliced map: every variable categorical with bit planes, unit weights
     s->use_bits = s->ti->planes_ok && s->maxterms <= 255;
@@ -976,7 +1059,12 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_lcnt.alloc(size_t(s->nodes) + 2)) != cudaSuccess ||
         (e = s->d_start.alloc(size_t(s->nodes) + 1)) != cudaSuccess ||
         (e = s->d_level_nodes.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
-        (e = s->d_nl.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess)
+        (e = s->d_nl.alloc(1)) != cudaSuccess || (e = s->d_status.alloc(1)) != cudaSuccess ||
+        (s->local && ((e = s->d_tpl_range.upload(s->tpl_range.data(), s->tpl_range.size(), s->st)) != cudaSuccess ||
+                      (e = s->d_node_kernel.upload(s->node_kernel.data(), s->node_kernel.size(), s->st)) != cudaSuccess ||
+                      (e = s->d_node_lim.upload(s->node_lim.data(), s->node_lim.size(), s->st)) != cudaSuccess ||
+                      (e = s->d_node_nv.upload(s->node_nv.data(), s->node_nv.size(), s->st)) != cudaSuccess ||
+                      (e = s->d_node_k.upload(s->node_k.data(), s->node_k.size(), s->st)) != cudaSuccess)))
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "upload: %s",
                          cudaGetErrorString(e)));
     // batch scratch: slots up to a record budget of ~2 GiB
@@ -1276,6 +1364,7 @@ int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, 
     s.node = 0;
     s.seed = seed;
     s.excl = -1;
+    s.K = int(k);
     int mn[QSK_MAXD] = {0}, mx[QSK_MAXD] = {0};
     for (int j = 0; j < n_neighbours; ++j)
         for (int d = 0; d < nd; ++d) {

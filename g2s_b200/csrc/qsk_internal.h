@@ -56,6 +56,7 @@ struct Slot {
     unsigned cell;           // DI cell (simulation)
     int excl;                // scan index forced to -inf (-nV), -1 for none
     int cmask_base;          // missing data: centre-mask layer address minus m
+    int K;                   // candidates kept (extendK = ceil(k) of this node)
 };
 
 enum SlotFlags : int {
@@ -107,6 +108,10 @@ struct SimPrepArgs {
     int mask_layer;        // layer index of the TI mask (missing data)
     int no_verbatim;       // -nV
     const unsigned *id_image;  // index image of the grid (-nV)
+    // local controls (nullable): neighbour count per path node and variable,
+    // candidate count per path node
+    const int *node_nv;
+    const float *node_k;
 };
 
 struct MapArgs {
@@ -172,9 +177,12 @@ struct ReplayArgs {
 // launch wrappers (qsk_kernels.cu)
 cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers, int missing,
                                 cudaStream_t st);
+// node_kernel / tpl_range / node_lim: optional per-node kernel (template
+// range [begin, begin+count) of the concatenated templates) and neighbour limit
 cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
-                              unsigned *nb_cell, cudaStream_t st);
+                              unsigned *nb_cell, const int *node_kernel, const int *tpl_range, const int *node_lim,
+                              cudaStream_t st);
 // dependency levels of the path DAG (Kahn frontiers)
 struct LevelArgs {
     long long nodes;

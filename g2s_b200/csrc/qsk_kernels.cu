@@ -118,7 +118,9 @@ __global__ void k_build_layers(const float *__restrict__ ti, int nvar, const int
 // appended in template order
 __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl, const unsigned *__restrict__ path,
                              unsigned begin, long long nodes, const unsigned *__restrict__ posterior, int n,
-                             int *__restrict__ nb_count, int *__restrict__ nb_tpl, unsigned *__restrict__ nb_cell) {
+                             int *__restrict__ nb_count, int *__restrict__ nb_tpl, unsigned *__restrict__ nb_cell,
+                             const int *__restrict__ node_kernel, const int *__restrict__ tpl_range,
+                             const int *__restrict__ node_lim) {
     const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= nodes) return;
@@ -130,15 +132,23 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
         c0[d] = int(rem % dg.dims[d]);
         rem /= dg.dims[d];
     }
+    // template of this node's kernel (-kii) and its neighbour limit (-n per variable / -ni)
+    int tb = 0, tn = ntpl, lim = n;
+    if (node_kernel) {
+        const int q = node_kernel[i];
+        tb = tpl_range[2 * q];
+        tn = tpl_range[2 * q + 1];
+    }
+    if (node_lim) lim = min(node_lim[i], n);
     int cnt = 0;
-    for (int t0 = 0; t0 < ntpl && cnt < n; t0 += 32) {
+    for (int t0 = 0; t0 < tn && cnt < lim; t0 += 32) {
         const int t = t0 + lane;
         bool acc = false;
         long long nc = 0;
-        if (t < ntpl) {
+        if (t < tn) {
             bool ok = true;
             for (int d = 0; d < dg.nd; ++d) {
-                int c = c0[d] + tpl[t * dg.nd + d];
+                int c = c0[d] + tpl[(tb + t) * dg.nd + d];
                 ok &= (c >= 0) && (c < dg.dims[d]);
                 nc += (long long)c * dg.stride[d];
             }
@@ -146,13 +156,13 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
         }
         const unsigned bal = __ballot_sync(0xffffffffu, acc);
         const int pos = cnt + __popc(bal & ((1u << lane) - 1u));
-        if (acc && pos < n) {
-            nb_tpl[i * n + pos] = t;
+        if (acc && pos < lim) {
+            nb_tpl[i * n + pos] = tb + t;
             nb_cell[i * n + pos] = unsigned(nc);
         }
         cnt += __popc(bal);
     }
-    if (lane == 0) nb_count[i] = cnt < n ? cnt : n;
+    if (lane == 0) nb_count[i] = cnt < lim ? cnt : lim;
 }
 
 // ---------------------------------------------------------------------------
@@ -312,9 +322,14 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     s.node = i;
     s.cell = cell;
     s.seed = A.seeds[i];
-    s.sel = selected_index(s.seed, A.k, A.nti);
+    // candidate count of this node: -kvi or k (quantileSamplingModule.hpp:90-113)
+    const float lk = A.node_k ? A.node_k[i] : A.k;
+    int Ki = int(ceilf(lk));
+    Ki = Ki < 1 ? 1 : (Ki > QSK_KMAX ? QSK_KMAX : Ki);
+    s.K = Ki;
+    s.sel = selected_index(s.seed, lk, A.nti);
     if (s.sel < 0) s.sel = 0;
-    if (s.sel > A.K - 1) s.sel = A.K - 1;   // unreachable for seeds in [0,1)
+    if (s.sel > Ki - 1) s.sel = Ki - 1;   // unreachable for k >= 1 and seeds in [0,1)
     s.flags = 0;
     s.nterms = 0;
     s.excl = -1;
@@ -354,7 +369,7 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     if (cnt <= 1 && !centreData) {
         s.flags |= SLOT_SKIP;   // marginal draw (simulation.hpp:586-605)
     } else {
-        if (nvalid < A.K) s.flags |= SLOT_EMIT_MASKED;
+        if (nvalid < Ki) s.flags |= SLOT_EMIT_MASKED;
         // terms: neighbours in order, variables in order; zero-weight / NaN skipped
         int base_out = 0;
         for (int j0 = 0; j0 < cnt; j0 += 32) {
@@ -367,6 +382,9 @@ __global__ void k_prep_sim(SimPrepArgs A) {
                 long long d_flat = 0;
                 for (int d = 0; d < nd; ++d) d_flat += (long long)(A.tpl[t * nd + d] - mn[d]) * A.g.sstride[d];
                 for (int v = 0; v < A.nvar && v < 4; ++v) {
+                    // a variable takes values from its first n_v neighbours only
+                    // (simulation.hpp:476-497)
+                    if (A.node_nv && j >= A.node_nv[(long long)i * A.nvar + v]) continue;
                     float val = (nc == cell) ? A.init[(long long)nc * A.nvar + v] : A.state[(long long)nc * A.nvar + v];
                     float w = A.wtab[t * A.nvar + v];
                     if (isnan(val) || w == 0.f) continue;
@@ -1168,7 +1186,7 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     WarpShared &w = wsh[wib];
     const Slot s = A.slots[b];
     const Geom &g = A.g;
-    const int K = A.K;
+    const int K = s.K;
     const unsigned FULL = 0xffffffffu;
 
     float cv[KM];
@@ -1687,10 +1705,12 @@ cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, con
 
 cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
-                              unsigned *nb_cell, cudaStream_t st) {
+                              unsigned *nb_cell, const int *node_kernel, const int *tpl_range, const int *node_lim,
+                              cudaStream_t st) {
     if (nodes <= 0) return cudaSuccess;
     k_neighbours<<<(unsigned)((nodes * 32 + 255) / 256), 256, 0, st>>>(dg, tpl, ntpl, path, begin, nodes, posterior, n,
-                                                                       nb_count, nb_tpl, nb_cell);
+                                                                       nb_count, nb_tpl, nb_cell, node_kernel,
+                                                                       tpl_range, node_lim);
     return cudaGetLastError();
 }
 

@@ -6,9 +6,9 @@
  *
  * Every entry point names the G2S interface it replaces.  G2S binds its
  * accelerator device by dlopen("./g2s_cuda.so") and two symbols
- * (src/qs.cpp:861-911); the drop-in g2s_cuda.so of this project (see
- * INTEGRATION.md) implements that AcceleratorDevice on top of the functions
- * below.
+ * (src/qs.cpp:861-911); the drop-in g2s_cuda.so of this project
+ * (g2s_b200/dropin/) implements that AcceleratorDevice on top of the
+ * functions below.
  *
  * Threading: a qsk_ti is immutable after creation and may be shared; a
  * qsk_worker or qsk_sim must be used by one host thread at a time.
@@ -195,6 +195,18 @@ typedef struct {
     float k;                      /* -k */
     unsigned seed;                /* -s */
     int no_verbatim;              /* -nV */
+    /* Local controls (G2S include/simulation.hpp:337-358,447-507,
+     * src/qs.cpp:1264-1292); zero / NULL when unused.  Images hold values per
+     * grid cell, x fastest. */
+    int n_counts;                 /* -n n1 n2 ...: entries of n_per_variable (0: n for every variable) */
+    const int *n_per_variable;
+    int n_image_vars;             /* -ni: counts per cell (0: no image) */
+    const float *n_image;
+    const float *k_image;         /* -kvi: candidate count per cell (<= 0: k); k becomes max(k, max k_image) */
+    int n_kernels;                /* -ki list (0: kernel_dims / kernel above) */
+    const unsigned *kernels_dims; /* n_kernels * ndim */
+    const float *const *kernels;  /* n_kernels weight arrays, prod(dims) * nvar each */
+    const float *kernel_index_image; /* -kii: kernel index per cell (required when n_kernels > 1) */
 } qsk_qs_params;
 
 typedef struct {

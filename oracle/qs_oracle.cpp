@@ -14,6 +14,10 @@
  *                            include/quantileSamplingModule.hpp:45-49,525-557
  *   draw                     G2S include/quantileSamplingModule.hpp:90-126,
  *                            src/CPUThreadDevice.cpp:257-268, include/simulation.hpp:556-666
+ *   local controls           G2S include/simulation.hpp:337-358,447-507 (-n per variable,
+ *                            -ni, -kii with one template and weight kernel per -ki file,
+ *                            -kvi), include/quantileSamplingModule.hpp:90-113,
+ *                            src/qs.cpp:1010-1137,1281-1292
  *
  * The FP32 map uses exactly the term order and the fused multiply-adds that
  * the CUDA kernels use, so the GPU path can be checked bit for bit; the FP64
@@ -453,11 +457,24 @@ struct NodeResult {
     unsigned top_index[8];
 };
 
+/* one weight kernel and its sorted search template */
+struct KernelTpl {
+    Grid kg;
+    const float *kernel = nullptr;   /* nullptr: uniform 1 */
+    std::vector<std::vector<int>> tpl;
+};
+
 struct Problem {
     Grid ti, di, kg;
     const float *tival = nullptr;
     const int *types = nullptr;
     const float *kernel = nullptr;
+    std::vector<KernelTpl> kernels;      /* index 0: the main kernel; -kii selects one */
+    std::vector<int> n_per_var;          /* -n n1 n2 ... (size 1: one count for all variables) */
+    int ni_vars = 0;                     /* -ni: counts per cell */
+    const float *ni = nullptr;
+    const float *kvi = nullptr;          /* -kvi: candidate count per cell (<= 0: k) */
+    const float *kii = nullptr;          /* -kii: kernel index per cell */
     int n = 0;
     float k = 1.f;
     double tol = 1e-5;
@@ -480,18 +497,35 @@ static inline unsigned position_to_index(const Scan &sc, const Grid &ti, const N
 }
 
 /* one node, given the current state of the grid */
-NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, const Path &path, const float *state,
-                    const unsigned *id_state, unsigned idx_path, bool want_fp64, bool own_cell_unknown,
-                    long probe_cell = -1) {
+NodeResult run_node(const Problem &P, const Path &path, const float *state, const unsigned *id_state,
+                    unsigned idx_path, bool want_fp64, bool own_cell_unknown, long probe_cell = -1) {
     NodeResult r;
     std::memset(&r, 0, sizeof(r));
     const Grid &di = P.di;
     unsigned cell = path.order[path.begin + idx_path];
     unsigned order = path.posterior[cell];
     float seed = path.seeds[idx_path];
-    std::vector<int> tix(P.n);
-    std::vector<unsigned> ncell(P.n);
-    int cnt = neighbours(di, tpl, path.posterior.data(), cell, order, P.n, tix.data(), ncell.data());
+    /* local controls (simulation.hpp:337-358): neighbour count per variable,
+     * kernel (template + weights), candidate count */
+    std::vector<int> nnb = P.n_per_var;
+    if (P.ni) {
+        nnb.assign(size_t(P.ni_vars), 0);
+        for (int q = 0; q < P.ni_vars; ++q) nnb[q] = int(P.ni[size_t(cell) * P.ni_vars + q]);
+    }
+    int ki = P.kii ? int(P.kii[cell]) : 0;
+    const KernelTpl &KT = P.kernels[size_t(ki)];
+    float localk = P.kvi ? P.kvi[cell] : 0.f;
+    if (localk <= 0.f) localk = P.k;
+    /* every accepted cell counts for each variable still below its count;
+     * with more than one count the walk also keeps the next informed cell
+     * (values all dropped) before it stops (simulation.hpp:447-507) */
+    int nmax = 0;
+    for (int v = 0; v < di.nvar; ++v) nmax = std::max(nmax, nnb[size_t(v) % nnb.size()]);
+    const int nlim = nmax + (nnb.size() > 1 ? 1 : 0);
+    const std::vector<std::vector<int>> &tpl = KT.tpl;
+    std::vector<int> tix(size_t(std::max(nlim, 1)));
+    std::vector<unsigned> ncell(size_t(std::max(nlim, 1)));
+    int cnt = neighbours(di, tpl, path.posterior.data(), cell, order, nlim, tix.data(), ncell.data());
     auto value = [&](unsigned c, int v) -> float {
         if (own_cell_unknown && c == cell) return NAN;
         return state[size_t(c) * di.nvar + v];
@@ -522,9 +556,10 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
     std::vector<float> vals(size_t(cnt) * di.nvar);
     for (int j = 0; j < cnt; ++j) {
         for (int d = 0; d < di.nd; ++d) offs[j * di.nd + d] = tpl[tix[j]][d];
-        for (int v = 0; v < di.nvar; ++v) vals[j * di.nvar + v] = value(ncell[j], v);
+        for (int v = 0; v < di.nvar; ++v)
+            vals[j * di.nvar + v] = j < nnb[size_t(v) % nnb.size()] ? value(ncell[j], v) : NAN;
     }
-    Node nd = build_node(P.ti, P.types, P.kg, P.kernel, cnt, offs.data(), vals.data());
+    Node nd = build_node(P.ti, P.types, KT.kg, KT.kernel, cnt, offs.data(), vals.data());
     nd.incomplete = P.incomplete;
     Scan sc = make_scan(P.ti, nd);
     if (probe_cell >= 0 && P.incomplete) {
@@ -549,7 +584,7 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
             for (int v = 0; v < P.ti.nvar; ++v) {
                 float val = vals[j * di.nvar + v];
                 if (std::isnan(val)) continue;
-                if (!std::isnan(P.tival[size_t(f) * P.ti.nvar + v])) cross += kweight(P.kg, P.kernel, offs.data() + j * di.nd, v);
+                if (!std::isnan(P.tival[size_t(f) * P.ti.nvar + v])) cross += kweight(KT.kg, KT.kernel, offs.data() + j * di.nd, v);
             }
         }
         if (std::isnan(P.tival[size_t(pc) * P.ti.nvar])) cross = 0.0;
@@ -574,7 +609,7 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
         unsigned ex = position_to_index(sc, P.ti, nd, unsigned(pf));
         if (ex < unsigned(sc.N)) map[ex] = -INFINITY;
     }
-    unsigned short K = (unsigned short)int(std::ceil(P.k));
+    unsigned short K = (unsigned short)int(std::ceil(localk));
     std::vector<float> ev(K);
     std::vector<unsigned> ep(K);
     kbiggest(map.data(), unsigned(sc.N), K, seed, ev.data(), ep.data());
@@ -583,7 +618,7 @@ NodeResult run_node(const Problem &P, const std::vector<std::vector<int>> &tpl, 
     std::iota(lp.begin(), lp.end(), 0u);
     const float *errors = ev.data();
     std::sort(lp.begin(), lp.end(), [errors](unsigned a, unsigned b) { return errors[a] > errors[b]; });
-    unsigned sel = selected_index(seed, P.k, 1);
+    unsigned sel = selected_index(seed, localk, 1);
     unsigned enc = ep[lp[sel]];
     r.ti_cell = index_to_position(sc, P.ti, nd, enc);
     for (int j = 0; j < K && j < 8; ++j) { r.top_score[j] = ev[lp[j]]; r.top_index[j] = ep[lp[j]]; }
@@ -675,11 +710,25 @@ unsigned orc_selected_index(float seed, float k, unsigned nti) { return selected
  * reference's index image (TI cell * nTI + TI, nTI = 1).
  * Returns the number of path nodes.
  */
-long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
-                  const unsigned *di_dims, float *di, const float *di_init, const unsigned *kdims, const float *kernel, int n, float k,
-                  unsigned seed, int want_fp64, double tol, long node_begin, long node_end, unsigned *out_cell,
-                  int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id, int no_verbatim,
-                  const unsigned *id_init, const unsigned *probe, double *probe_cross) {
+/* local controls of orc_simulate_ex (all optional, per DI cell where noted) */
+struct OrcControls {
+    int n_counts;                  /* entries of n_per_var (-n n1 n2 ...); 0: n for every variable */
+    const int *n_per_var;
+    int ni_vars;                   /* -ni: counts per cell (0: none) */
+    const float *ni;
+    const float *kvi;              /* -kvi */
+    int n_kernels;                 /* kernels for -kii (0: the main kernel only) */
+    const unsigned *kernels_dims;  /* n_kernels * nd */
+    const float *const *kernels;
+    const float *kii;              /* -kii */
+};
+
+long orc_simulate_ex(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
+                     const unsigned *di_dims, float *di, const float *di_init, const unsigned *kdims, const float *kernel,
+                     int n, float k, unsigned seed, int want_fp64, double tol, long node_begin, long node_end,
+                     unsigned *out_cell, int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id,
+                     int no_verbatim, const unsigned *id_init, const unsigned *probe, double *probe_cross,
+                     const OrcControls *ctl) {
     Problem P;
     P.ti.nd = P.di.nd = P.kg.nd = nd;
     P.ti.nvar = P.di.nvar = nvar;
@@ -718,7 +767,43 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
         P.kg.nvar = nvar;
         for (int d = 0; d < nd; ++d) P.kg.dims[d] = std::min(ti_dims[d] / 2 + 1, ti_dims[d]);
     }
-    auto tpl = make_template(nd, P.kg.dims, P.kernel, nvar);
+    /* kernels: the main one, or the -kii list (src/qs.cpp:1000-1042) */
+    if (ctl && ctl->n_kernels > 0) {
+        for (int q = 0; q < ctl->n_kernels; ++q) {
+            KernelTpl kt;
+            kt.kg.nd = nd;
+            kt.kg.nvar = nvar;
+            for (int d = 0; d < nd; ++d) kt.kg.dims[d] = ctl->kernels_dims[q * nd + d];
+            kt.kernel = ctl->kernels[q];
+            P.kernels.push_back(kt);
+        }
+    } else {
+        KernelTpl kt;
+        kt.kg = P.kg;
+        kt.kernel = P.kernel;
+        P.kernels.push_back(kt);
+    }
+    for (auto &kt : P.kernels) kt.tpl = make_template(nd, kt.kg.dims, kt.kernel, nvar);
+    P.n_per_var.assign(1, n);
+    if (ctl && ctl->n_counts > 0) P.n_per_var.assign(ctl->n_per_var, ctl->n_per_var + ctl->n_counts);
+    if (ctl && ctl->ni_vars > 0 && ctl->ni) {
+        P.ni_vars = ctl->ni_vars;
+        P.ni = ctl->ni;
+    }
+    if (ctl && ctl->kii) {
+        P.kii = ctl->kii;
+        for (size_t c = 0; c < P.di.cells(); ++c) {
+            int q = int(P.kii[c]);
+            if (q < 0 || q >= int(P.kernels.size())) return -3;
+        }
+    }
+    if (ctl && ctl->kvi) {
+        /* -kvi: the module's k becomes max(k, max kvi) (src/qs.cpp:1281-1292) */
+        P.kvi = ctl->kvi;
+        float kb = std::isnan(k) || k <= 0.f ? 1.f : k;
+        for (size_t c = 0; c < P.di.cells(); ++c) kb = std::max(kb, P.kvi[c]);
+        P.k = kb;
+    }
     std::vector<float> state(di, di + P.di.cells() * nvar);
     /* the path is always built from the grid before simulation (NaN = unknown) */
     Path path = make_path(P.di, di_init ? di_init : state.data(), seed);
@@ -731,7 +816,7 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
 #pragma omp parallel for schedule(dynamic, 16)
         for (long i = node_begin; i < node_end; ++i) {
             long o = i - node_begin;
-            NodeResult r = run_node(P, tpl, path, state.data(), idw.data(), unsigned(i), want_fp64 != 0, true,
+            NodeResult r = run_node(P, path, state.data(), idw.data(), unsigned(i), want_fp64 != 0, true,
                                     probe ? long(probe[o]) : -1L);
             if (probe_cross) probe_cross[o] = r.probe_cross;
             if (out_cell) out_cell[o] = r.ti_cell;
@@ -744,7 +829,7 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
     for (long i = 0; i < node_end; ++i) {
         unsigned cell = path.order[path.begin + i];
         bool active = i >= node_begin;
-        NodeResult r = run_node(P, tpl, path, state.data(), idw.data(), unsigned(i), active && want_fp64 != 0, false);
+        NodeResult r = run_node(P, path, state.data(), idw.data(), unsigned(i), active && want_fp64 != 0, false);
         for (int v = 0; v < nvar; ++v)
             if (std::isnan(state[size_t(cell) * nvar + v])) state[size_t(cell) * nvar + v] = P.tival[size_t(r.ti_cell) * nvar + v];
         idw[cell] = r.ti_cell;
@@ -759,6 +844,16 @@ long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int
     }
     std::copy(state.begin(), state.end(), di);
     return nodes;
+}
+
+long orc_simulate(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
+                  const unsigned *di_dims, float *di, const float *di_init, const unsigned *kdims, const float *kernel, int n, float k,
+                  unsigned seed, int want_fp64, double tol, long node_begin, long node_end, unsigned *out_cell,
+                  int *out_near_tie, int *out_marginal, double *out_gap, unsigned *out_id, int no_verbatim,
+                  const unsigned *id_init, const unsigned *probe, double *probe_cross) {
+    return orc_simulate_ex(mode, nd, ti_dims, nvar, types, ti, di_dims, di, di_init, kdims, kernel, n, k, seed, want_fp64,
+                           tol, node_begin, node_end, out_cell, out_near_tie, out_marginal, out_gap, out_id, no_verbatim,
+                           id_init, probe, probe_cross, nullptr);
 }
 
 /* FP32 and FP64 maps of one explicit pattern (offsets/values) against the TI

@@ -45,6 +45,8 @@ def lib():
                                    ctypes.c_long, ctypes.c_long, _u32p, _i32p, _i32p, _f64p, _u32p, ctypes.c_int,
                                    _u32p, _u32p, _f64p]
         L.orc_simulate.restype = ctypes.c_long
+        L.orc_simulate_ex.argtypes = L.orc_simulate.argtypes + [ctypes.c_void_p]
+        L.orc_simulate_ex.restype = ctypes.c_long
         L.orc_pattern_map.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, ctypes.c_int, _i32p, _f32p,
                                       _f32p, _f64p, _f64p, _i32p, _i32p]
         L.orc_pattern_map.restype = ctypes.c_long
@@ -96,13 +98,62 @@ def rng_stream(seed: int, n: int):
     return out
 
 
+class _Controls(ctypes.Structure):
+    _fields_ = [("n_counts", ctypes.c_int), ("n_per_var", ctypes.c_void_p), ("ni_vars", ctypes.c_int),
+                ("ni", ctypes.c_void_p), ("kvi", ctypes.c_void_p), ("n_kernels", ctypes.c_int),
+                ("kernels_dims", ctypes.c_void_p), ("kernels", ctypes.c_void_p), ("kii", ctypes.c_void_p)]
+
+
+def _controls(cells, n_per_var=None, ni=None, kvi=None, kernels=None, kii=None):
+    """Local controls (-n per variable, -ni, -kvi, -kii with its kernels);
+    returns (struct, keep-alive list) or (None, []) when none is given."""
+    if n_per_var is None and ni is None and kvi is None and kernels is None and kii is None:
+        return None, []
+    c = _Controls()
+    keep = []
+
+    def arr(a, dt):
+        x = np.ascontiguousarray(a, dtype=dt)
+        keep.append(x)
+        return x.ctypes.data
+
+    if n_per_var is not None:
+        c.n_counts = len(n_per_var)
+        c.n_per_var = arr(n_per_var, np.int32)
+    if ni is not None:
+        ni = np.asarray(ni, np.float32)
+        c.ni_vars = max(1, ni.size // cells)
+        c.ni = arr(ni, np.float32)
+    if kvi is not None:
+        c.kvi = arr(kvi, np.float32)
+    if kernels is not None:
+        # list of (weights array with numpy shape (..., ky, kx[, nvar]), dims x-first)
+        dims = []
+        ptrs = (ctypes.c_void_p * len(kernels))()
+        for q, (w, kd) in enumerate(kernels):
+            ptrs[q] = arr(w, np.float32)
+            dims += list(kd)
+        keep.append(ptrs)
+        c.n_kernels = len(kernels)
+        c.kernels_dims = arr(dims, np.uint32)
+        c.kernels = ctypes.cast(ptrs, ctypes.c_void_p).value
+    if kii is not None:
+        c.kii = arr(kii, np.float32)
+    keep.append(c)
+    return c, keep
+
+
 def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp64=False, tol=1e-5,
-             node_begin=0, node_end=-1, di_init=None, no_verbatim=False, id_init=None, probe=None):
+             node_begin=0, node_end=-1, di_init=None, no_verbatim=False, id_init=None, probe=None,
+             n_per_var=None, ni=None, kvi=None, kernels=None, kii=None):
     """mode 0: sequential vector simulation of ``di`` (NaN = unknown);
     mode 1: teacher-forced evaluation of every path node against the completed
     grid ``di``, the path being built from ``di_init`` (the grid before
     simulation).  ``no_verbatim`` is -nV; in mode 1 it needs ``id_init``, the
-    index image of the completed grid.
+    index image of the completed grid.  Local controls: ``n_per_var`` (-n
+    with one count per variable), ``ni`` (-ni image, numpy shape of the grid
+    [, counts]), ``kvi`` (-kvi image), ``kernels`` (list of (weights, dims
+    x-first), the -ki files) with ``kii`` (-kii image of kernel indices).
 
     Returns dict(sim, id, cell, near_tie, marginal, gap, begin)."""
     nvar = len(types)
@@ -127,12 +178,16 @@ def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp
     idi = None if id_init is None else np.ascontiguousarray(id_init, dtype=np.uint32).ravel()
     prb = None if probe is None else np.ascontiguousarray(probe, dtype=np.uint32).ravel()
     pcross = np.full(cnt, np.nan, np.float64)
-    rc = lib().orc_simulate(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
+    ctl, keep = _controls(cells, n_per_var, ni, kvi, kernels, kii)
+    rc = lib().orc_simulate_ex(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
                        _p(d, _f32p), None if di_init is None else _p(init, _f32p), _p(kd, _u32p), _p(kern, _f32p), n, k, seed, int(want_fp64), tol, node_begin,
                        ne, _p(cell, _u32p), _p(nt, _i32p), _p(mg, _i32p), _p(gap, _f64p), _p(oid, _u32p),
-                       int(no_verbatim), _p(idi, _u32p), _p(prb, _u32p), _p(pcross, _f64p))
-    if rc < 0:
+                       int(no_verbatim), _p(idi, _u32p), _p(prb, _u32p), _p(pcross, _f64p),
+                       None if ctl is None else ctypes.addressof(ctl))
+    if rc == -2:
         raise ValueError("oracle: categorical variables with missing training-image values are undefined")
+    if rc == -3:
+        raise ValueError("oracle: kernel index image out of range")
     return dict(sim=d, id=oid, cell=cell, near_tie=nt.astype(bool), marginal=mg.astype(bool), gap=gap,
                 probe_cross=pcross)
 

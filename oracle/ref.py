@@ -66,18 +66,31 @@ def read_image(name: str):
     return out
 
 
-def run_qs(ti: np.ndarray, di: np.ndarray, types, args, job_id: int = 4242, tag: str = "g2sb200"):
+def run_qs(ti: np.ndarray, di: np.ndarray, types, args, job_id: int = 4242, tag: str = "g2sb200", images=None):
     """Run reference ``qs`` with ``-ti``/``-di`` set; returns (sim, index, compute_ms, log_text).
 
     ``args`` is a list of extra qs flags, e.g. ``['-dt','0','-k','1.2','-n','50','-s','100','-j','8']``.
+    ``images`` maps further image flags to lists of (array, types), e.g.
+    ``{'-ni': [(ni, [0])], '-ki': [(k1, [0]), (k2, [0])]}``; each array is
+    written as a ``.bgrid`` and its name passed after the flag.
     ``compute_ms`` is the reference's own "compuattion time" (G2S src/qs.cpp:2229-2235).
     """
     ti_name = f"{tag}_ti_{job_id}"
     di_name = f"{tag}_di_{job_id}"
     write_image(ti_name, ti, types)
     write_image(di_name, di, types)
+    extra_names = []
+    extra_args = []
+    for flag, items in (images or {}).items():
+        extra_args.append(flag)
+        for q, (arr, ty) in enumerate(items):
+            name = f"{tag}_{flag.strip('-')}{q}_{job_id}"
+            write_image(name, arr, ty)
+            extra_names.append(name)
+            extra_args.append(name)
     log = f"/tmp/G2S/logs/{tag}_{job_id}.log"
-    argv = ["qs", "-ti", ti_name, "-di", di_name, "-id", str(job_id), "-r", log] + [str(a) for a in args]
+    argv = (["qs", "-ti", ti_name, "-di", di_name, "-id", str(job_id), "-r", log] + [str(a) for a in args] +
+            extra_args)
     arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
     rc = lib().g2sref_qs_main(len(argv), arr)
     if rc != 0:
@@ -89,7 +102,8 @@ def run_qs(ti: np.ndarray, di: np.ndarray, types, args, job_id: int = 4242, tag:
     text = open(log).read() if os.path.exists(log) else ""
     m = re.findall(r"compuattion time: (\d+) ms", text)
     ms = float(m[-1]) if m else float("nan")
-    for name in (ti_name, di_name, str(job_id), "id_" + str(job_id), "im_1_" + str(job_id), "im_2_" + str(job_id)):
+    for name in [ti_name, di_name, str(job_id), "id_" + str(job_id), "im_1_" + str(job_id),
+                 "im_2_" + str(job_id)] + extra_names:
         for ext in (".bgrid", ".bgrid.gz"):
             try:
                 os.remove(f"/tmp/G2S/data/{name}{ext}")

@@ -39,6 +39,62 @@ EXTRA = {
 }
 
 
+def _local_arrays(dshape, seed, what):
+    """Seeded local-control images for a grid of numpy shape dshape."""
+    rng = np.random.default_rng(seed)
+    sp = dshape[:2]
+    out = {}
+    if "ni" in what:
+        out["ni"] = rng.integers(3, 30, sp).astype(np.float32)
+    if "ni2" in what:
+        out["ni"] = np.stack([rng.integers(2, 20, sp), rng.integers(2, 20, sp)], -1).astype(np.float32)
+    if "kvi" in what:
+        out["kvi"] = rng.choice(np.array([1.0, 1.5, 2.0, 3.0, 0.0], np.float32), sp)
+    if "kii" in what:
+        out["k0"] = np.ones((15, 15), np.float32)
+        yy, xx = np.meshgrid(np.arange(21) - 10, np.arange(21) - 10, indexing="ij")
+        out["k1"] = np.exp(-np.hypot(yy, xx) / 4).astype(np.float32)
+        out["kii"] = rng.integers(0, 2, sp).astype(np.float32)
+    return out
+
+
+# local controls (-n per variable, -ni, -kvi, -kii with a -ki list):
+# name -> (ti builder, di shape, types, k, n (int or list), seed, images wanted)
+LOCAL = {
+    "grf2d_ni": (lambda: syn.grf((60, 70), (6, 6), seed=3), (24, 28), [0], 1.2, None, 100, ["ni"]),
+    "grf2d_kvi": (lambda: syn.grf((60, 70), (6, 6), seed=3), (24, 28), [0], 1.2, 20, 100, ["kvi"]),
+    "grf2d_kii": (lambda: syn.grf((60, 70), (6, 6), seed=3), (24, 28), [0], 1.2, 20, 100, ["kii"]),
+    "grf2d_local": (lambda: syn.grf((60, 70), (6, 6), seed=3), (24, 28), [0], 1.2, None, 100, ["ni", "kvi", "kii"]),
+    "bivar2d_n2": (lambda: syn.bivariate(syn.grf((60, 70), (6, 6), seed=5)), (20, 22, 2), [0, 1], 1.2, [12, 25], 100, []),
+    "bivar2d_ni2": (lambda: syn.bivariate(syn.grf((60, 70), (6, 6), seed=5)), (20, 22, 2), [0, 1], 1.2, None, 100,
+                    ["ni2"]),
+}
+
+
+def make_local(names=None):
+    for name, (mk, dshape, types, k, n, seed, what) in LOCAL.items():
+        if names and name not in names:
+            continue
+        ti = mk()
+        di = np.full(dshape, np.nan, np.float32)
+        arrs = _local_arrays(dshape, seed + len(name), what)
+        args = ["-k", str(k), "-s", str(seed), "-j", "1"]
+        if n is not None:
+            args += ["-n"] + [str(x) for x in np.ravel(n)]
+        images = {}
+        if "ni" in arrs:
+            images["-ni"] = [(arrs["ni"], [0] * (1 if arrs["ni"].ndim == 2 else arrs["ni"].shape[-1]))]
+        if "kvi" in arrs:
+            images["-kvi"] = [(arrs["kvi"], [0])]
+        if "kii" in arrs:
+            images["-ki"] = [(arrs["k0"], [0]), (arrs["k1"], [0])]
+            images["-kii"] = [(arrs["kii"], [0])]
+        sim, idx, ms, _ = ref.run_qs(ti, di, types, args, images=images, job_id=3100 + len(name))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k,
+                            n=np.array(-1 if n is None else n), seed=seed, sim=sim, idx=idx, ref_ms=ms, **arrs)
+        print(name, ti.shape, dshape, sorted(arrs))
+
+
 def holes(field, seed):
     """Missing training-image values: a few NaN rectangles."""
     rng = np.random.default_rng(seed)
@@ -83,5 +139,7 @@ if __name__ == "__main__":
     args = sys.argv[1:]
     if args == ["teacher"]:
         oracle_teacher_config0()
+    elif args[:1] == ["local"]:
+        make_local(args[1:])
     else:
         main(args)

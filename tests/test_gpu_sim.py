@@ -182,3 +182,86 @@ def test_missing_data_teacher_forced_vs_reference(g2s, gpu, oracle, name):
     mism = cells != ref_cells
     noise = tf["probe_cross"] == 0.0
     assert not np.any(mism & ~tf["near_tie"] & ~noise)
+
+
+# ---------------------------------------------------------------------------
+# local controls: -n per variable, -ni, -kvi, -kii with a -ki list
+# ---------------------------------------------------------------------------
+LOCAL = ["grf2d_ni", "grf2d_kvi", "grf2d_kii", "grf2d_local", "bivar2d_n2", "bivar2d_ni2"]
+
+
+def local_args(g):
+    kw = {}
+    n = np.asarray(g["n"])
+    if n.ndim > 0:
+        kw["n_per_var"] = [int(x) for x in n]
+    if "ni" in g:
+        kw["ni"] = g["ni"]
+    if "kvi" in g:
+        kw["kvi"] = g["kvi"]
+    if "kii" in g:
+        kw["kii"] = g["kii"]
+    nmax = int(n.max()) if n.ndim > 0 else max(int(n), 0)
+    return nmax, kw
+
+
+def run_gpu_local(g2s, g, teacher=None):
+    types = [int(t) for t in g["types"]]
+    nmax, kw = local_args(g)
+    kernels = [g["k0"], g["k1"]] if "kii" in g else None
+    sim = g2s.Simulation(g["ti"], g["di"], types, n=nmax, k=float(g["k"]), seed=int(g["seed"]), kernels=kernels, **kw)
+    if teacher is None:
+        sim.run()
+    else:
+        sim.run_teacher(teacher)
+    out = sim.read()
+    sim.close()
+    return out
+
+
+def oracle_local(oracle, g, mode=0):
+    types = [int(t) for t in g["types"]]
+    nmax, kw = local_args(g)
+    if "kii" in g:
+        kw["kernels"] = [(g["k0"], g["k0"].shape[::-1]), (g["k1"], g["k1"].shape[::-1])]
+    if mode == 0:
+        return oracle.simulate(g["ti"], g["di"], types, nmax, float(g["k"]), int(g["seed"]), mode=0, **kw)
+    return oracle.simulate(g["ti"], g["sim"], types, nmax, float(g["k"]), int(g["seed"]), mode=1, want_fp64=True,
+                           di_init=g["di"], **kw)
+
+
+@pytest.mark.parametrize("name", LOCAL)
+def test_local_controls_equal_oracle(g2s, gpu, oracle, name):
+    g = golden(name)
+    sim, idx, _ = run_gpu_local(g2s, g)
+    o = oracle_local(oracle, g)
+    assert np.array_equal(idx.ravel(), o["id"])
+    assert np.array_equal(sim, o["sim"], equal_nan=True)
+
+
+@pytest.mark.parametrize("name", ["grf2d_ni", "grf2d_kvi"])
+def test_local_controls_equal_reference(g2s, gpu, name):
+    g = golden(name)
+    sim, idx, _ = run_gpu_local(g2s, g)
+    assert np.array_equal(idx.ravel(), g["idx"].ravel())
+    assert np.array_equal(sim, g["sim"])
+
+
+@pytest.mark.parametrize("name", LOCAL)
+def test_local_controls_teacher_forced(g2s, gpu, oracle, name):
+    g = golden(name)
+    _, _, cells = run_gpu_local(g2s, g, teacher=g["sim"])
+    tf = oracle_local(oracle, g, mode=1)
+    assert np.array_equal(cells, tf["cell"])
+    types = [int(t) for t in g["types"]]
+    order, seeds, post, begin = oracle.path(g["di"], len(types), int(g["seed"]))
+    ref_cells = g["idx"].ravel()[order[begin:]]
+    assert not np.any((cells != ref_cells) & ~tf["near_tie"])
+
+
+def test_local_controls_rejects_bad_kernel_index(g2s, gpu):
+    g = golden("grf2d_kii")
+    bad = g["kii"].copy()
+    bad[3, 4] = 2
+    with pytest.raises(RuntimeError, match="kernel index"):
+        g2s.Simulation(g["ti"], g["di"], [0], n=20, k=1.2, seed=100, kernels=[g["k0"], g["k1"]], kii=bad)
