@@ -40,7 +40,7 @@ class QskParams(ctypes.Structure):
                 ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint), ("no_verbatim", ctypes.c_int),
                 ("n_counts", ctypes.c_int), ("n_per_variable", _i32p), ("n_image_vars", ctypes.c_int),
                 ("n_image", _f32p), ("k_image", _f32p), ("n_kernels", ctypes.c_int), ("kernels_dims", _u32p),
-                ("kernels", ctypes.POINTER(_f32p)), ("kernel_index_image", _f32p)]
+                ("kernels", ctypes.POINTER(_f32p)), ("kernel_index_image", _f32p), ("full_simulation", ctypes.c_int)]
 
 
 class QskPatternOpts(ctypes.Structure):
@@ -267,10 +267,12 @@ class Simulation:
                  kernel: Optional[np.ndarray] = None, device: int = 0, no_verbatim: bool = False,
                  n_per_var: Optional[Sequence[int]] = None, ni: Optional[np.ndarray] = None,
                  kvi: Optional[np.ndarray] = None, kernels: Optional[Sequence[np.ndarray]] = None,
-                 kii: Optional[np.ndarray] = None):
+                 kii: Optional[np.ndarray] = None, full: bool = False):
         """Local controls as in G2S: ``n_per_var`` (-n n1 n2 ...), ``ni``
         (-ni image, grid shape [+ counts]), ``kvi`` (-kvi image), ``kernels``
-        (the -ki list) with ``kii`` (-kii image of kernel indices)."""
+        (the -ki list) with ``kii`` (-kii image of kernel indices); ``full``
+        is -fs (one path node per cell value; the index image then has one
+        entry per value)."""
         self.nvar = len(types)
         self._ti = np.ascontiguousarray(ti, dtype=np.float32)
         self._di = np.ascontiguousarray(di, dtype=np.float32)
@@ -284,6 +286,8 @@ class Simulation:
                                 _p(self._kern, _f32p), int(n), float(k), int(seed) & 0xffffffff, int(no_verbatim))
         cells = int(np.prod(self._ddims))
         self._keep = []
+        self.full = bool(full)
+        self.params.full_simulation = int(full)
 
         def keep(a, dt):
             x = np.ascontiguousarray(a, dtype=dt).ravel()
@@ -348,11 +352,12 @@ class Simulation:
         """Returns (grid, index_image, node_cells)."""
         cells = int(np.prod(self._ddims))
         out = np.empty_like(self._di)
-        idx = np.zeros(cells, np.uint32)
+        idx = np.zeros(cells * (self.nvar if self.full else 1), np.uint32)
         nodes = self.info()["nodes"]
         nc = np.zeros(max(nodes, 1), np.uint32)
         _check(lib().qsk_sim_read(self.handle, _p(out, _f32p), _p(idx, _u32p), _p(nc, _u32p)), "qsk_sim_read")
-        return out, idx.reshape(self._di.shape[:len(self._ddims)]), nc[:nodes]
+        shape = self._di.shape if self.full else self._di.shape[:len(self._ddims)]
+        return out, idx.reshape(shape), nc[:nodes]
 
     def close(self):
         if getattr(self, "handle", None):
@@ -368,9 +373,9 @@ class Simulation:
 
 def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
        ki=None, nV: bool = False, ni: Optional[np.ndarray] = None, kvi: Optional[np.ndarray] = None,
-       kii: Optional[np.ndarray] = None, device: int = 0):
+       kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0):
     """QuickSampling on one GPU; arguments named after the G2S flags
-    (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii).  ``n`` is one count or one
+    (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii -fs).  ``n`` is one count or one
     per variable; ``ki`` one kernel or a list of kernels (selected per cell by
     ``kii``).  Returns (simulation, index) as G2S does."""
     n_list = None
@@ -381,7 +386,7 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     if isinstance(ki, (list, tuple)):
         kernel, kernels = None, list(ki)
     sim = Simulation(ti, di, dt, n=n if n is not None else 0, k=k, seed=s, kernel=kernel, device=device,
-                     no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii)
+                     no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii, full=fs)
     try:
         sim.run()
         out, idx, _ = sim.read()

@@ -622,6 +622,7 @@ struct qsk_sim {
     std::vector<int> node_kernel, node_lim, node_nv;
     std::vector<float> node_k;
     bool local = false;
+    bool full = false;               // -fs: nodes are (cell, variable) values
     // device
     DBuf<int> d_tpl, d_types;
     DBuf<float> d_wtab, d_seeds, d_init, d_state;
@@ -635,6 +636,7 @@ struct qsk_sim {
     DBuf<int> d_rec_idx, d_rec_cnt;
     DBuf<float> d_rec_max;
     DBuf<int> d_tpl_range, d_node_kernel, d_node_lim, d_node_nv;
+    DBuf<unsigned char> d_nb_mask;
     DBuf<float> d_node_k;
     int maxterms = 0;
     int max_slots = 0;
@@ -751,6 +753,38 @@ unsigned make_path(size_t n, int nvar, const float *init, unsigned seed, std::ve
     return begin;
 }
 
+// -fs: path over the cells*nvar values, informed values first
+// (src/qs.cpp:1159-1183,1250-1258,1614-1638)
+void build_path_full(qsk_sim *s) {
+    const size_t n = size_t(s->cells) * s->nvar;
+    std::mt19937 gen(s->seed);
+    s->order.resize(n);
+    std::iota(s->order.begin(), s->order.end(), 0u);
+    unsigned begin = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isnan(s->init[i])) {
+            std::swap(s->order[begin], s->order[i]);
+            begin++;
+        }
+    std::shuffle(s->order.begin() + begin, s->order.end(), gen);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    s->seeds.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        s->seeds[i] = u(gen);
+        if (s->seeds[i] == 1.f) s->seeds[i] = u(gen);
+    }
+    s->begin = begin;
+    s->nodes = (long long)n - begin;
+    s->posterior.assign(n, std::numeric_limits<unsigned>::max());
+    s->node_of_cell.assign(n, -1);   // per value
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isnan(s->init[i])) s->posterior[i] = 0;
+    for (long long i = 0; i < s->nodes; ++i) {
+        s->posterior[s->order[begin + i]] = unsigned(i);
+        s->node_of_cell[s->order[begin + i]] = int(i);
+    }
+}
+
 // posterior order (src/qs.cpp:1604-1641)
 void build_path(qsk_sim *s) {
     const size_t n = size_t(s->cells);
@@ -772,6 +806,14 @@ void build_path(qsk_sim *s) {
 
 int sim_neighbours(qsk_sim *s) {
     if (s->neighbours_ready) return QSK_OK;
+    if (s->full) {
+        CK(launch_neighbours_full(s->dg, s->d_tpl.p, s->ntpl, s->d_path.p, s->begin, s->nodes, s->d_post.p, s->nvar,
+                                  s->n, s->local ? s->d_node_nv.p : nullptr, s->d_nb_count.p, s->d_nb_tpl.p,
+                                  s->d_nb_cell.p, s->d_nb_mask.p, s->local ? s->d_node_kernel.p : nullptr,
+                                  s->local ? s->d_tpl_range.p : nullptr, s->st));
+        s->neighbours_ready = true;
+        return QSK_OK;
+    }
     CK(launch_neighbours(s->dg, s->d_tpl.p, s->ntpl, s->d_path.p, s->begin, s->nodes,
                          s->d_post.p, s->n, s->d_nb_count.p, s->d_nb_tpl.p, s->d_nb_cell.p,
                          s->local ? s->d_node_kernel.p : nullptr, s->local ? s->d_tpl_range.p : nullptr,
@@ -828,6 +870,8 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             pa.id_image = s->d_id.p;
             pa.node_nv = s->local ? s->d_node_nv.p : nullptr;
             pa.node_k = s->local ? s->d_node_k.p : nullptr;
+            pa.full = s->full ? 1 : 0;
+            pa.nb_mask = s->full ? s->d_nb_mask.p : nullptr;
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
@@ -884,6 +928,7 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.state = teacher ? nullptr : s->d_state.p;
             ra.id_image = teacher ? nullptr : s->d_id.p;
             ra.node_cell = s->d_node_cell.p;
+            ra.full = s->full ? 1 : 0;
             CK(launch_replay(ra, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         }
@@ -932,6 +977,9 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     if (p->n_kernels > 1 && !p->kernel_index_image)
         return fail(QSK_ERR_ARG, "several kernels need a kernel index image (-kii)");
     if (p->n_kernels > 0 && (!p->kernels_dims || !p->kernels)) return fail(QSK_ERR_ARG, "null kernel list");
+    if (p->full_simulation && p->nvar > 4) return fail(QSK_ERR_UNSUPPORTED, "-fs with more than 4 variables");
+    if (p->full_simulation && p->k_image && p->nvar > 1)
+        return fail(QSK_ERR_UNSUPPORTED, "-fs with -kvi needs one value per cell and variable (G2S indexes it so)");
     // -kvi: the module's k becomes max(k, max k_image) (src/qs.cpp:1281-1292)
     float kbase = p->k;
     if (p->k_image) {
@@ -953,7 +1001,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     s->k = kbase;
     s->K = K;
     s->seed = p->seed;
-    s->no_verbatim = p->no_verbatim;
+    s->full = p->full_simulation != 0;
+    s->no_verbatim = s->full ? 0 : p->no_verbatim;   // -fs has no verbatim record
     auto bail = [&](int rc) {
         qsk_sim_destroy(s);
         return rc;
@@ -963,6 +1012,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         delete s;
         return rc;
     }
+    if (s->full && s->ti->missing)
+        return bail(fail(QSK_ERR_UNSUPPORTED, "-fs with missing training-image values is not implemented"));
     cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(fail(QSK_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
     s->cells = 1;
@@ -987,9 +1038,10 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         for (int d = 0; d < p->ndim; ++d) kd[d] = std::min(p->ti_dims[d] / 2 + 1, p->ti_dims[d]);
         add_template(s, kd.data(), nullptr);
     }
-    build_path(s);
-    // local controls per path node (simulation.hpp:337-358,447-507)
-    s->local = counts_given || p->k_image || p->kernel_index_image || p->n_kernels > 1;
+    if (s->full) build_path_full(s);
+    else build_path(s);
+    // local controls per path node (simulation.hpp:337-358,447-507; -fs 793-815)
+    s->local = counts_given || p->k_image || p->kernel_index_image || p->n_kernels > 1 || s->full;
     if (s->local) {
         const long long nn = std::max<long long>(s->nodes, 1);
         s->node_kernel.assign(size_t(nn), 0);
@@ -1001,7 +1053,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         float kmax = kbase;
         std::vector<int> counts;
         for (long long i = 0; i < s->nodes; ++i) {
-            const unsigned cell = s->order[s->begin + i];
+            const unsigned pv = s->order[s->begin + i];
+            const unsigned cell = s->full ? pv / unsigned(s->nvar) : pv;
             if (p->n_image_vars > 0 && p->n_image) {
                 counts.assign(size_t(p->n_image_vars), 0);
                 for (int q = 0; q < p->n_image_vars; ++q)
@@ -1011,21 +1064,24 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
             } else {
                 counts.assign(1, p->n);
             }
-            int nmax = 0;
+            int nmax = 0, nsum = 0;
             for (int v = 0; v < s->nvar; ++v) {
                 int c = std::max(0, counts[size_t(v) % counts.size()]);
                 s->node_nv[size_t(i) * s->nvar + v] = c;
                 nmax = std::max(nmax, c);
+                nsum += c;
             }
-            // with one count per variable the walk also keeps the next informed cell
-            s->node_lim[size_t(i)] = nmax + (counts.size() > 1 ? 1 : 0);
+            // with one count per variable the vector walk also keeps the next
+            // informed cell; under -fs a cell may serve a single variable, so up
+            // to the sum of the counts are taken
+            s->node_lim[size_t(i)] = s->full ? nsum : nmax + (counts.size() > 1 ? 1 : 0);
             nmax_all = std::max(nmax_all, s->node_lim[size_t(i)]);
             if (p->kernel_index_image) {
                 int q = int(p->kernel_index_image[cell]);
                 if (q < 0 || q >= nk) return bail(fail(QSK_ERR_ARG, "kernel index %d at cell %u outside [0,%d)", q, cell, nk));
                 s->node_kernel[size_t(i)] = q;
             }
-            if (p->k_image && p->k_image[cell] > 0.f) s->node_k[size_t(i)] = p->k_image[cell];
+            if (p->k_image && p->k_image[cell] > 0.f) s->node_k[size_t(i)] = p->k_image[cell];   // nvar 1 under -fs
             kmax = std::max(kmax, s->node_k[size_t(i)]);
         }
         s->n = std::max(1, nmax_all);
@@ -1045,12 +1101,14 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_post.upload(s->posterior.data(), s->posterior.size(), s->st)) != cudaSuccess ||
         (e = s->d_node_of_cell.upload(s->node_of_cell.data(), s->node_of_cell.size(), s->st)) != cudaSuccess ||
         (e = s->d_init.upload(s->init.data(), s->init.size(), s->st)) != cudaSuccess ||
-        (e = s->d_state.alloc(s->init.size())) != cudaSuccess || (e = s->d_id.alloc(size_t(s->cells))) != cudaSuccess ||
+        (e = s->d_state.alloc(s->init.size())) != cudaSuccess ||
+        (e = s->d_id.alloc(size_t(s->cells) * (s->full ? s->nvar : 1))) != cudaSuccess ||
+        (s->full && (e = s->d_nb_mask.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess) ||
         (e = s->d_node_cell.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_nb_count.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_nb_tpl.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
         (e = s->d_nb_cell.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
-        (e = s->d_adj.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
+        (e = s->d_adj.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n * (s->full ? s->nvar : 1))) != cudaSuccess ||
         (e = s->d_deg.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_outcnt.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_outstart.alloc(size_t(s->nodes) + 1)) != cudaSuccess ||
@@ -1098,7 +1156,7 @@ int qsk_sim_run(qsk_sim *s) {
     cudaEvent_t ev[4];
     for (auto &x : ev) CK(cudaEventCreate(&x));
     CK(cudaMemcpyAsync(s->d_state.p, s->d_init.p, sizeof(float) * s->init.size(), cudaMemcpyDeviceToDevice, s->st));
-    CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells, s->st));
+    CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells * (s->full ? s->nvar : 1), s->st));
     CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
     s->info.launches = 0;
     s->info.map_launches = 0;
@@ -1113,6 +1171,8 @@ int qsk_sim_run(qsk_sim *s) {
     la.n = s->n;
     la.nb_count = s->d_nb_count.p;
     la.nb_cell = s->d_nb_cell.p;
+    la.nb_mask = s->full ? s->d_nb_mask.p : nullptr;
+    la.nvar = s->nvar;
     la.node_of_cell = s->d_node_of_cell.p;
     la.deg = s->d_deg.p;
     la.outcnt = s->d_outcnt.p;
@@ -1164,7 +1224,7 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
     if (id_completed)
         CK(cudaMemcpyAsync(s->d_id.p, id_completed, sizeof(unsigned) * s->cells, cudaMemcpyHostToDevice, s->st));
     else
-        CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells, s->st));
+        CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells * (s->full ? s->nvar : 1), s->st));
     CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
     int rc = sim_neighbours(s);
     if (rc) return rc;
@@ -1184,7 +1244,9 @@ int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cel
     DeviceGuard dgd(s->device);
     if (di_out)
         CK(cudaMemcpyAsync(di_out, s->d_state.p, sizeof(float) * s->init.size(), cudaMemcpyDeviceToHost, s->st));
-    if (id_out) CK(cudaMemcpyAsync(id_out, s->d_id.p, sizeof(unsigned) * s->cells, cudaMemcpyDeviceToHost, s->st));
+    if (id_out)
+        CK(cudaMemcpyAsync(id_out, s->d_id.p, sizeof(unsigned) * s->cells * (s->full ? s->nvar : 1),
+                           cudaMemcpyDeviceToHost, s->st));
     if (node_cell_out && s->nodes > 0)
         CK(cudaMemcpyAsync(node_cell_out, s->d_node_cell.p, sizeof(unsigned) * s->nodes, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));

@@ -57,6 +57,7 @@ struct Slot {
     int excl;                // scan index forced to -inf (-nV), -1 for none
     int cmask_base;          // missing data: centre-mask layer address minus m
     int K;                   // candidates kept (extendK = ceil(k) of this node)
+    int var;                 // -fs: the node's variable (the only one written)
 };
 
 enum SlotFlags : int {
@@ -112,6 +113,8 @@ struct SimPrepArgs {
     // candidate count per path node
     const int *node_nv;
     const float *node_k;
+    int full;                       // -fs: path entries are cell values, neighbours carry nb_mask
+    const unsigned char *nb_mask;
 };
 
 struct MapArgs {
@@ -169,8 +172,9 @@ struct ReplayArgs {
     unsigned nti, ti_id;
     const int *complete_prefix;  // missing data: complete TI cells in [0..c]; null for a complete TI
     float *state;         // grid written in simulation mode (null in teacher-forced mode)
-    unsigned *id_image;   // per grid cell
+    unsigned *id_image;   // per grid cell (-fs: per cell value)
     unsigned *node_cell;  // per path index: chosen TI cell
+    int full;             // -fs: write the slot's variable only
 };
 
 
@@ -183,13 +187,20 @@ cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, cons
                               long long nodes, const unsigned *posterior, int n, int *nb_count, int *nb_tpl,
                               unsigned *nb_cell, const int *node_kernel, const int *tpl_range, const int *node_lim,
                               cudaStream_t st);
+cudaError_t launch_neighbours_full(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
+                                   long long nodes, const unsigned *posterior, int nvar, int n, const int *node_nv,
+                                   int *nb_count, int *nb_tpl, unsigned *nb_cell, unsigned char *nb_mask,
+                                   const int *node_kernel, const int *tpl_range, cudaStream_t st);
+
 // dependency levels of the path DAG (Kahn frontiers)
 struct LevelArgs {
     long long nodes;
     int n;
     const int *nb_count;
     const unsigned *nb_cell;
-    const int *node_of_cell;
+    const unsigned char *nb_mask;  // -fs: variables each neighbour contributes (null otherwise)
+    int nvar;
+    const int *node_of_cell;       // per cell, or (-fs) per cell value
     int *deg;           // nodes
     int *outcnt;        // nodes
     int *outstart;      // nodes + 1

@@ -165,6 +165,76 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
     if (lane == 0) nb_count[i] = cnt < lim ? cnt : lim;
 }
 
+// -fs: one warp per (cell, variable) node.  A cell is taken when a variable
+// that still needs neighbours was simulated there strictly before the node
+// (posterior < order, simulation.hpp:822-872); the variables it contributes
+// are recorded in nb_mask.  The 32 offsets of a step are tested in parallel,
+// then taken in template order with the per-variable counts.
+__global__ void k_neighbours_full(GridDesc dg, const int *__restrict__ tpl, int ntpl, const unsigned *__restrict__ path,
+                                  unsigned begin, long long nodes, const unsigned *__restrict__ posterior, int nvar,
+                                  int n, const int *__restrict__ node_nv, int *__restrict__ nb_count,
+                                  int *__restrict__ nb_tpl, unsigned *__restrict__ nb_cell,
+                                  unsigned char *__restrict__ nb_mask, const int *__restrict__ node_kernel,
+                                  const int *__restrict__ tpl_range) {
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= nodes) return;
+    const unsigned value = path[begin + i];
+    const unsigned cell = value / unsigned(nvar);
+    const unsigned order = posterior[value];
+    int c0[QSK_MAXD];
+    long long rem = cell;
+    for (int d = 0; d < dg.nd; ++d) {
+        c0[d] = int(rem % dg.dims[d]);
+        rem /= dg.dims[d];
+    }
+    int tb = 0, tn = ntpl;
+    if (node_kernel) {
+        const int q = node_kernel[i];
+        tb = tpl_range[2 * q];
+        tn = tpl_range[2 * q + 1];
+    }
+    int need[4] = {0, 0, 0, 0};   // remaining count per variable
+    unsigned needm = 0;
+    for (int v = 0; v < nvar && v < 4; ++v) {
+        need[v] = node_nv ? node_nv[i * nvar + v] : n;
+        if (need[v] > 0) needm |= 1u << v;
+    }
+    int cnt = 0;
+    for (int t0 = 0; t0 < tn && needm && cnt < n; t0 += 32) {
+        const int t = t0 + lane;
+        unsigned im = 0;
+        long long nc = 0;
+        if (t < tn) {
+            bool ok = true;
+            for (int d = 0; d < dg.nd; ++d) {
+                int c = c0[d] + tpl[(tb + t) * dg.nd + d];
+                ok &= (c >= 0) && (c < dg.dims[d]);
+                nc += (long long)c * dg.stride[d];
+            }
+            if (ok)
+                for (int v = 0; v < nvar && v < 4; ++v)
+                    if (posterior[nc * nvar + v] < order) im |= 1u << v;
+        }
+        unsigned cand = __ballot_sync(0xffffffffu, (im & needm) != 0u);
+        while (cand && needm && cnt < n) {
+            const int l = __ffs(cand) - 1;
+            cand &= cand - 1u;
+            const unsigned m = __shfl_sync(0xffffffffu, im, l) & needm;
+            if (!m) continue;
+            if (lane == l) {
+                nb_tpl[i * n + cnt] = tb + t;
+                nb_cell[i * n + cnt] = unsigned(nc);
+                nb_mask[i * n + cnt] = (unsigned char)m;
+            }
+            for (int v = 0; v < 4; ++v)
+                if ((m >> v) & 1u && --need[v] == 0) needm &= ~(1u << v);
+            ++cnt;
+        }
+    }
+    if (lane == 0) nb_count[i] = cnt;
+}
+
 // ---------------------------------------------------------------------------
 // dependency levels: level(i) = 1 + max level(j) over the node's informed
 // neighbours j that are themselves path nodes (0 without any) -- the longest
@@ -173,20 +243,39 @@ __global__ void k_neighbours(GridDesc dg, const int *__restrict__ tpl, int ntpl,
 // level L are those whose last dependency finished in level L-1, so the
 // frontiers come out already grouped by level.
 // ---------------------------------------------------------------------------
+// dependency nodes of neighbour j of node i: the cell's node, or (-fs, with
+// nb_mask) the nodes of the cell's values that the neighbour contributes
+template <class F>
+__device__ __forceinline__ void for_each_dep(long long i, int j, int n, const unsigned *__restrict__ nb_cell,
+                                             const unsigned char *__restrict__ nb_mask, int nvar,
+                                             const int *__restrict__ node_of, F f) {
+    const unsigned c = nb_cell[i * n + j];
+    if (!nb_mask) {
+        const int d = node_of[c];
+        if (d >= 0 && (long long)d != i) f(d);
+        return;
+    }
+    const unsigned m = nb_mask[i * n + j];
+    for (int v = 0; v < nvar; ++v)
+        if ((m >> v) & 1u) {
+            const int d = node_of[(long long)c * nvar + v];
+            if (d >= 0 && (long long)d != i) f(d);
+        }
+}
+
 // in-degree of every node and out-degree count of every dependency
 __global__ void k_dep_count(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                            const int *__restrict__ node_of_cell, int *__restrict__ deg, int *__restrict__ outcnt) {
+                            const unsigned char *__restrict__ nb_mask, int nvar, const int *__restrict__ node_of,
+                            int *__restrict__ deg, int *__restrict__ outcnt) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nodes) return;
     const int c = nb_count[i];
     int dg = 0;
-    for (int j = 0; j < c; ++j) {
-        const int d = node_of_cell[nb_cell[i * n + j]];
-        if (d >= 0 && (long long)d != i) {
+    for (int j = 0; j < c; ++j)
+        for_each_dep(i, j, n, nb_cell, nb_mask, nvar, node_of, [&](int d) {
             ++dg;
             atomicAdd(&outcnt[d], 1);
-        }
-    }
+        });
     deg[i] = dg;
 }
 
@@ -247,14 +336,13 @@ __global__ void k_scan_add(long long count, int *__restrict__ out, int *__restri
 
 // reverse edges: adj[outstart[d] ..] lists the nodes that depend on d
 __global__ void k_adj_fill(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                           const int *__restrict__ node_of_cell, int *__restrict__ cursor, int *__restrict__ adj) {
+                           const unsigned char *__restrict__ nb_mask, int nvar, const int *__restrict__ node_of,
+                           int *__restrict__ cursor, int *__restrict__ adj) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nodes) return;
     const int c = nb_count[i];
-    for (int j = 0; j < c; ++j) {
-        const int d = node_of_cell[nb_cell[i * n + j]];
-        if (d >= 0 && (long long)d != i) adj[atomicAdd(&cursor[d], 1)] = int(i);
-    }
+    for (int j = 0; j < c; ++j)
+        for_each_dep(i, j, n, nb_cell, nb_mask, nvar, node_of, [&](int d) { adj[atomicAdd(&cursor[d], 1)] = int(i); });
 }
 
 // Frontier pass (cooperative launch, one grid barrier per level).  Level L's
@@ -315,12 +403,15 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     const int lane = threadIdx.x & 31;
     if (warp >= A.nslots) return;
     const int i = A.nodes[warp];
-    const unsigned cell = A.path[A.begin + i];
+    const unsigned pv = A.path[A.begin + i];
+    // -fs: the path entry is a cell value (cell * nvar + variable)
+    const unsigned cell = A.full ? pv / unsigned(A.nvar) : pv;
     const int cnt = A.nb_count[i];
     const int nd = A.g.nd;
     Slot s;
     s.node = i;
     s.cell = cell;
+    s.var = A.full ? int(pv % unsigned(A.nvar)) : 0;
     s.seed = A.seeds[i];
     // candidate count of this node: -kvi or k (quantileSamplingModule.hpp:90-113)
     const float lk = A.node_k ? A.node_k[i] : A.k;
@@ -334,8 +425,12 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     s.nterms = 0;
     s.excl = -1;
     s.cmask_base = 0;
+    // vector simulation: data at the centre also forces a search
+    // (simulation.hpp:565-584); -fs draws from the marginal below two
+    // neighbours (simulation.hpp:952-965)
     bool centreData = false;
-    for (int v = 0; v < A.nvar; ++v) centreData |= !isnan(A.init[(long long)cell * A.nvar + v]);
+    if (!A.full)
+        for (int v = 0; v < A.nvar; ++v) centreData |= !isnan(A.init[(long long)cell * A.nvar + v]);
     // min / max of the neighbour offsets, starting from 0 (AcceleratorDevice.cpp:95-112)
     int mn[QSK_MAXD], mx[QSK_MAXD];
 #pragma unroll
@@ -384,8 +479,13 @@ __global__ void k_prep_sim(SimPrepArgs A) {
                 for (int v = 0; v < A.nvar && v < 4; ++v) {
                     // a variable takes values from its first n_v neighbours only
                     // (simulation.hpp:476-497)
-                    if (A.node_nv && j >= A.node_nv[(long long)i * A.nvar + v]) continue;
-                    float val = (nc == cell) ? A.init[(long long)nc * A.nvar + v] : A.state[(long long)nc * A.nvar + v];
+                    if (A.full) {
+                        if (!((A.nb_mask[(long long)i * A.n + j] >> v) & 1u)) continue;
+                    } else if (A.node_nv && j >= A.node_nv[(long long)i * A.nvar + v]) {
+                        continue;
+                    }
+                    float val = (nc == cell && !A.full) ? A.init[(long long)nc * A.nvar + v]
+                                                        : A.state[(long long)nc * A.nvar + v];
                     float w = A.wtab[t * A.nvar + v];
                     if (isnan(val) || w == 0.f) continue;
                     Term tm;
@@ -441,7 +541,7 @@ __global__ void k_prep_sim(SimPrepArgs A) {
             for (int d = 0; d < nd; ++d) fmn += (long long)mn[d] * A.g.sstride[d];
             s.cmask_base = int((long long)A.mask_layer * A.g.N + fmn);
         }
-        if (A.no_verbatim && cnt > 1) {
+        if (A.no_verbatim && cnt > 1 && !A.full) {
             // the TI cell continuing neighbour 1's source is excluded
             // (simulation.hpp:556-583, quantileSamplingModule.hpp:518-523)
             const int t1 = A.nb_tpl[(long long)i * A.n + 1];
@@ -1373,13 +1473,20 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
     }
     if (lane == 0 && have) {
         if (A.node_cell) A.node_cell[s.node] = chosen_cell;
-        if (A.state) {
-            for (int v = 0; v < A.nvar; ++v) {
-                float *dst = A.state + (long long)s.cell * A.nvar + v;
-                if (isnan(*dst)) *dst = A.ti[(long long)chosen_cell * A.nvar + v];
+        if (A.full) {
+            // -fs: the node's variable only (simulation.hpp:1016-1024)
+            const long long val = (long long)s.cell * A.nvar + s.var;
+            if (A.state && isnan(A.state[val])) A.state[val] = A.ti[(long long)chosen_cell * A.nvar + s.var];
+            if (A.id_image) A.id_image[val] = chosen_cell * A.nti + A.ti_id;
+        } else {
+            if (A.state) {
+                for (int v = 0; v < A.nvar; ++v) {
+                    float *dst = A.state + (long long)s.cell * A.nvar + v;
+                    if (isnan(*dst)) *dst = A.ti[(long long)chosen_cell * A.nvar + v];
+                }
             }
+            if (A.id_image) A.id_image[s.cell] = chosen_cell * A.nti + A.ti_id;
         }
-        if (A.id_image) A.id_image[s.cell] = chosen_cell * A.nti + A.ti_id;
     }
 }
 
@@ -1714,6 +1821,17 @@ cudaError_t launch_neighbours(const GridDesc &dg, const int *tpl, int ntpl, cons
     return cudaGetLastError();
 }
 
+cudaError_t launch_neighbours_full(const GridDesc &dg, const int *tpl, int ntpl, const unsigned *path, unsigned begin,
+                                   long long nodes, const unsigned *posterior, int nvar, int n, const int *node_nv,
+                                   int *nb_count, int *nb_tpl, unsigned *nb_cell, unsigned char *nb_mask,
+                                   const int *node_kernel, const int *tpl_range, cudaStream_t st) {
+    if (nodes <= 0) return cudaSuccess;
+    k_neighbours_full<<<(unsigned)((nodes * 32 + 255) / 256), 256, 0, st>>>(dg, tpl, ntpl, path, begin, nodes, posterior,
+                                                                            nvar, n, node_nv, nb_count, nb_tpl, nb_cell,
+                                                                            nb_mask, node_kernel, tpl_range);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
     long long nodes = a.nodes;
     if (nodes <= 0) return cudaSuccess;
@@ -1722,11 +1840,13 @@ cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(a.outcnt, 0, sizeof(int) * size_t(nodes), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.cnt, 0, sizeof(int) * size_t(nodes + 2), st)) != cudaSuccess) return e;
-    k_dep_count<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.node_of_cell, a.deg, a.outcnt);
+    k_dep_count<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell, a.deg,
+                                    a.outcnt);
     k_scan_tiles<<<(unsigned)ntiles, 1024, 0, st>>>(nodes, a.outcnt, a.outstart, a.tile_sum);
     k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);
     k_scan_add<<<(unsigned)((nodes + 1 + 255) / 256), 256, 0, st>>>(nodes, a.outstart, a.cursor, a.tile_sum);
-    k_adj_fill<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.node_of_cell, a.cursor, a.adj);
+    k_adj_fill<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell, a.cursor,
+                                   a.adj);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;

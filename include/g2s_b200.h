@@ -207,6 +207,8 @@ typedef struct {
     const unsigned *kernels_dims; /* n_kernels * ndim */
     const float *const *kernels;  /* n_kernels weight arrays, prod(dims) * nvar each */
     const float *kernel_index_image; /* -kii: kernel index per cell (required when n_kernels > 1) */
+    int full_simulation;          /* -fs: one path node per (cell, variable) value (simulationFull,
+                                     include/simulation.hpp:712-1066); index image per value */
 } qsk_qs_params;
 
 typedef struct {

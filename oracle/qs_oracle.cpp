@@ -153,6 +153,36 @@ Path make_path(const Grid &di, const float *dival, unsigned seed) {
     return p;
 }
 
+/* -fs: the path runs over (cell, variable) values: informed values first,
+ * the rest shuffled by the same generator, one seed per value
+ * (src/qs.cpp:1159-1183,1250-1258,1614-1638) */
+Path make_path_full(const Grid &di, const float *dival, unsigned seed) {
+    Path p;
+    std::mt19937 gen(seed);
+    const size_t n = di.cells() * size_t(di.nvar);
+    p.order.resize(n);
+    std::iota(p.order.begin(), p.order.end(), 0u);
+    unsigned begin = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isnan(dival[i])) {
+            std::swap(p.order[begin], p.order[i]);
+            begin++;
+        }
+    std::shuffle(p.order.begin() + begin, p.order.end(), gen);
+    std::uniform_real_distribution<float> u(0.f, 1.f);
+    p.seeds.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+        p.seeds[i] = u(gen);
+        if (p.seeds[i] == 1.f) p.seeds[i] = u(gen);
+    }
+    p.begin = begin;
+    p.posterior.assign(n, UINT_MAX);
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isnan(dival[i])) p.posterior[i] = 0;
+    for (size_t i = begin; i < n; ++i) p.posterior[p.order[i]] = unsigned(i - begin);
+    return p;
+}
+
 /* ------------------------------------------------------------------ */
 /* a6: neighbours of one path node                                     */
 /* ------------------------------------------------------------------ */
@@ -496,6 +526,8 @@ static inline unsigned position_to_index(const Scan &sc, const Grid &ti, const N
     return index;
 }
 
+void fp64_gap(const Problem &P, const Node &nd, const Scan &sc, int K, NodeResult &r);
+
 /* one node, given the current state of the grid */
 NodeResult run_node(const Problem &P, const Path &path, const float *state, const unsigned *id_state,
                     unsigned idx_path, bool want_fp64, bool own_cell_unknown, long probe_cell = -1) {
@@ -622,7 +654,14 @@ NodeResult run_node(const Problem &P, const Path &path, const float *state, cons
     unsigned enc = ep[lp[sel]];
     r.ti_cell = index_to_position(sc, P.ti, nd, enc);
     for (int j = 0; j < K && j < 8; ++j) { r.top_score[j] = ev[lp[j]]; r.top_index[j] = ep[lp[j]]; }
-    if (want_fp64) {
+    if (want_fp64) fp64_gap(P, nd, sc, K, r);
+    return r;
+}
+
+/* FP64 map of the node: smallest adjacent gap among its top-(K+1) scores,
+ * relative to the term scale (continuous) or the scores (missing data) */
+void fp64_gap(const Problem &P, const Node &nd, const Scan &sc, int K, NodeResult &r) {
+    {
         std::vector<double> m64(sc.N), s64(sc.N);
         map_fp64(P.ti, P.tival, nd, sc, m64.data(), s64.data());
         std::vector<long> ord(sc.N);
@@ -650,6 +689,84 @@ NodeResult run_node(const Problem &P, const Path &path, const float *state, cons
         r.gap_min = gmin;
         r.near_tie = gmin <= P.tol;
     }
+}
+
+/* -fs: one value (cell, variable) per path node (simulation.hpp:712-1024).
+ * A cell is taken when some variable still needs neighbours and its value
+ * there was simulated strictly before this node (posterior < order); only
+ * those variables carry values.  The draw writes the node's variable only;
+ * without two neighbours it draws from the marginal. */
+NodeResult run_node_full(const Problem &P, const Path &path, const float *state, unsigned idx_path, bool want_fp64) {
+    NodeResult r;
+    std::memset(&r, 0, sizeof(r));
+    const Grid &di = P.di;
+    const int nvar = di.nvar;
+    unsigned value = path.order[path.begin + idx_path];
+    unsigned cell = value / unsigned(nvar), var = value % unsigned(nvar);
+    unsigned order = path.posterior[value];
+    float seed = path.seeds[idx_path];
+    std::vector<int> nnb = P.n_per_var;
+    if (P.ni) {
+        nnb.assign(size_t(P.ni_vars), 0);
+        for (int q = 0; q < P.ni_vars; ++q) nnb[q] = int(P.ni[size_t(cell) * P.ni_vars + q]);
+    }
+    int ki = P.kii ? int(P.kii[cell]) : 0;
+    const KernelTpl &KT = P.kernels[size_t(ki)];
+    float localk = P.kvi ? P.kvi[size_t(cell) * nvar + var] : 0.f;
+    if (localk <= 0.f) localk = P.k;
+    std::vector<int> count(size_t(nvar), 0);
+    std::vector<int> offs;
+    std::vector<float> vals;
+    int c0[8], c[8];
+    coords(di, long(cell), c0);
+    int cnt = 0;
+    for (size_t t = 0; t < KT.tpl.size(); ++t) {
+        bool need = false;
+        for (int v = 0; v < nvar; ++v) need |= count[v] < nnb[size_t(v) % nnb.size()];
+        if (!need && nnb.size() == 1) break;
+        bool ok = true;
+        for (int d = 0; d < di.nd; ++d) {
+            c[d] = c0[d] + KT.tpl[t][d];
+            ok &= (c[d] >= 0) && (c[d] < int(di.dims[d]));
+        }
+        if (!ok) continue;
+        unsigned nc = unsigned(flat(di, c));
+        bool add = false;
+        for (int v = 0; v < nvar; ++v)
+            add |= count[v] < nnb[size_t(v) % nnb.size()] && path.posterior[size_t(nc) * nvar + v] < order;
+        if (!add) continue;
+        for (int d = 0; d < di.nd; ++d) offs.push_back(KT.tpl[t][d]);
+        for (int v = 0; v < nvar; ++v) {
+            if (count[v] < nnb[size_t(v) % nnb.size()] && path.posterior[size_t(nc) * nvar + v] < order) {
+                vals.push_back(state[size_t(nc) * nvar + v]);
+                count[v]++;
+            } else {
+                vals.push_back(NAN);
+            }
+        }
+        cnt++;
+    }
+    if (cnt <= 1) {
+        /* marginal draw of the node's variable (simulation.hpp:965-1014), complete TI */
+        r.ti_cell = unsigned(int(std::floor(double(seed * float(unsigned(P.ti.cells()))))));
+        r.marginal = 1;
+        return r;
+    }
+    Node nd = build_node(P.ti, P.types, KT.kg, KT.kernel, cnt, offs.data(), vals.data());
+    Scan sc = make_scan(P.ti, nd);
+    std::vector<float> map(sc.N);
+    map_fp32(P.ti, P.tival, nd, sc, map.data());
+    unsigned short K = (unsigned short)int(std::ceil(localk));
+    std::vector<float> ev(K);
+    std::vector<unsigned> ep(K);
+    kbiggest(map.data(), unsigned(sc.N), K, seed, ev.data(), ep.data());
+    std::vector<unsigned> lp(K);
+    std::iota(lp.begin(), lp.end(), 0u);
+    const float *errors = ev.data();
+    std::sort(lp.begin(), lp.end(), [errors](unsigned a, unsigned b) { return errors[a] > errors[b]; });
+    unsigned sel = selected_index(seed, localk, 1);
+    r.ti_cell = index_to_position(sc, P.ti, nd, ep[lp[sel]]);
+    if (want_fp64) fp64_gap(P, nd, sc, K, r);
     return r;
 }
 
@@ -674,6 +791,20 @@ int orc_path(int nd, const unsigned *dims, int nvar, const float *dival, unsigne
     g.nvar = nvar;
     for (int d = 0; d < nd; ++d) g.dims[d] = dims[d];
     Path p = make_path(g, dival, seed);
+    std::copy(p.order.begin(), p.order.end(), order);
+    std::copy(p.seeds.begin(), p.seeds.end(), seeds);
+    std::copy(p.posterior.begin(), p.posterior.end(), posterior);
+    return int(p.begin);
+}
+
+/* -fs path over (cell, variable) values; arrays of cells*nvar entries. */
+int orc_path_full(int nd, const unsigned *dims, int nvar, const float *dival, unsigned seed, unsigned *order,
+                  float *seeds, unsigned *posterior) {
+    Grid g;
+    g.nd = nd;
+    g.nvar = nvar;
+    for (int d = 0; d < nd; ++d) g.dims[d] = dims[d];
+    Path p = make_path_full(g, dival, seed);
     std::copy(p.order.begin(), p.order.end(), order);
     std::copy(p.seeds.begin(), p.seeds.end(), seeds);
     std::copy(p.posterior.begin(), p.posterior.end(), posterior);
@@ -721,6 +852,7 @@ struct OrcControls {
     const unsigned *kernels_dims;  /* n_kernels * nd */
     const float *const *kernels;
     const float *kii;              /* -kii */
+    int full;                      /* -fs: one path node per (cell, variable) value */
 };
 
 long orc_simulate_ex(int mode, int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
@@ -805,6 +937,43 @@ long orc_simulate_ex(int mode, int nd, const unsigned *ti_dims, int nvar, const 
         P.k = kb;
     }
     std::vector<float> state(di, di + P.di.cells() * nvar);
+    if (ctl && ctl->full) {
+        /* -fs (complete TIs only here); out_id holds one index per value.
+         * mode 1: every node against the completed grid (values visible by
+         * posterior order only, so no masking is needed) */
+        if (P.incomplete) return -4;
+        Path fp = make_path_full(P.di, di_init ? di_init : state.data(), seed);
+        long fnodes = long(P.di.cells()) * nvar - long(fp.begin);
+        if (node_end < 0 || node_end > fnodes) node_end = fnodes;
+        if (mode == 1) {
+#pragma omp parallel for schedule(dynamic, 16)
+            for (long i = node_begin; i < node_end; ++i) {
+                NodeResult r = run_node_full(P, fp, state.data(), unsigned(i), want_fp64 != 0);
+                long o = i - node_begin;
+                if (out_cell) out_cell[o] = r.ti_cell;
+                if (out_near_tie) out_near_tie[o] = r.near_tie;
+                if (out_marginal) out_marginal[o] = r.marginal;
+                if (out_gap) out_gap[o] = r.gap_min;
+            }
+            return fnodes;
+        }
+        for (long i = 0; i < node_end; ++i) {
+            unsigned value = fp.order[fp.begin + i];
+            NodeResult r = run_node_full(P, fp, state.data(), unsigned(i), i >= node_begin && want_fp64 != 0);
+            unsigned var = value % unsigned(nvar);
+            if (std::isnan(state[value])) state[value] = P.tival[size_t(r.ti_cell) * nvar + var];
+            if (out_id) out_id[value] = r.ti_cell;
+            if (i >= node_begin) {
+                long o = i - node_begin;
+                if (out_cell) out_cell[o] = r.ti_cell;
+                if (out_near_tie) out_near_tie[o] = r.near_tie;
+                if (out_marginal) out_marginal[o] = r.marginal;
+                if (out_gap) out_gap[o] = r.gap_min;
+            }
+        }
+        std::copy(state.begin(), state.end(), di);
+        return fnodes;
+    }
     /* the path is always built from the grid before simulation (NaN = unknown) */
     Path path = make_path(P.di, di_init ? di_init : state.data(), seed);
     long nodes = long(P.di.cells()) - long(path.begin);

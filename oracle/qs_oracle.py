@@ -33,6 +33,8 @@ def lib():
         L.orc_template.restype = ctypes.c_int
         L.orc_path.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p, _u32p]
         L.orc_path.restype = ctypes.c_int
+        L.orc_path_full.argtypes = L.orc_path.argtypes
+        L.orc_path_full.restype = ctypes.c_int
         L.orc_kbiggest.argtypes = [_f32p, ctypes.c_uint, ctypes.c_uint, ctypes.c_float, _f32p, _u32p]
         L.orc_rng.argtypes = [ctypes.c_uint, ctypes.c_int, _f32p]
         L.orc_seed_from_unit_float.argtypes = [ctypes.c_float]
@@ -72,15 +74,18 @@ def template(kdims, kernel=None, nvar=1):
     return out[: n * len(kd)].reshape(n, len(kd))
 
 
-def path(di: np.ndarray, nvar: int, seed: int):
+def path(di: np.ndarray, nvar: int, seed: int, full: bool = False):
+    """(order, seeds, posterior, begin); with ``full`` (-fs) over the
+    cells*nvar values instead of the cells."""
     dims = grid_dims(di, nvar)
-    cells = int(np.prod(dims))
+    cells = int(np.prod(dims)) * (nvar if full else 1)
     d = np.ascontiguousarray(di, dtype=np.float32)
     order = np.zeros(cells, np.uint32)
     seeds = np.zeros(cells, np.float32)
     post = np.zeros(cells, np.uint32)
-    begin = lib().orc_path(len(dims), _p(dims, _u32p), nvar, _p(d, _f32p), seed, _p(order, _u32p), _p(seeds, _f32p),
-                           _p(post, _u32p))
+    fn = lib().orc_path_full if full else lib().orc_path
+    begin = fn(len(dims), _p(dims, _u32p), nvar, _p(d, _f32p), seed, _p(order, _u32p), _p(seeds, _f32p),
+               _p(post, _u32p))
     return order, seeds, post, begin
 
 
@@ -101,15 +106,17 @@ def rng_stream(seed: int, n: int):
 class _Controls(ctypes.Structure):
     _fields_ = [("n_counts", ctypes.c_int), ("n_per_var", ctypes.c_void_p), ("ni_vars", ctypes.c_int),
                 ("ni", ctypes.c_void_p), ("kvi", ctypes.c_void_p), ("n_kernels", ctypes.c_int),
-                ("kernels_dims", ctypes.c_void_p), ("kernels", ctypes.c_void_p), ("kii", ctypes.c_void_p)]
+                ("kernels_dims", ctypes.c_void_p), ("kernels", ctypes.c_void_p), ("kii", ctypes.c_void_p),
+                ("full", ctypes.c_int)]
 
 
-def _controls(cells, n_per_var=None, ni=None, kvi=None, kernels=None, kii=None):
-    """Local controls (-n per variable, -ni, -kvi, -kii with its kernels);
+def _controls(cells, n_per_var=None, ni=None, kvi=None, kernels=None, kii=None, full=False):
+    """Local controls (-n per variable, -ni, -kvi, -kii with its kernels, -fs);
     returns (struct, keep-alive list) or (None, []) when none is given."""
-    if n_per_var is None and ni is None and kvi is None and kernels is None and kii is None:
+    if n_per_var is None and ni is None and kvi is None and kernels is None and kii is None and not full:
         return None, []
     c = _Controls()
+    c.full = int(full)
     keep = []
 
     def arr(a, dt):
@@ -145,7 +152,7 @@ def _controls(cells, n_per_var=None, ni=None, kvi=None, kernels=None, kii=None):
 
 def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp64=False, tol=1e-5,
              node_begin=0, node_end=-1, di_init=None, no_verbatim=False, id_init=None, probe=None,
-             n_per_var=None, ni=None, kvi=None, kernels=None, kii=None):
+             n_per_var=None, ni=None, kvi=None, kernels=None, kii=None, full=False):
     """mode 0: sequential vector simulation of ``di`` (NaN = unknown);
     mode 1: teacher-forced evaluation of every path node against the completed
     grid ``di``, the path being built from ``di_init`` (the grid before
@@ -178,7 +185,16 @@ def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp
     idi = None if id_init is None else np.ascontiguousarray(id_init, dtype=np.uint32).ravel()
     prb = None if probe is None else np.ascontiguousarray(probe, dtype=np.uint32).ravel()
     pcross = np.full(cnt, np.nan, np.float64)
-    ctl, keep = _controls(cells, n_per_var, ni, kvi, kernels, kii)
+    ctl, keep = _controls(cells, n_per_var, ni, kvi, kernels, kii, full)
+    if full:
+        oid = np.zeros(cells * nvar, np.uint32)
+        nodes = int(np.sum(np.isnan(init)))
+        ne = nodes if node_end < 0 else min(node_end, nodes)
+        cnt = max(ne - node_begin, 0)
+        cell = np.zeros(cnt, np.uint32)
+        nt = np.zeros(cnt, np.int32)
+        mg = np.zeros(cnt, np.int32)
+        gap = np.zeros(cnt, np.float64)
     rc = lib().orc_simulate_ex(mode, len(tdims), _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(ddims, _u32p),
                        _p(d, _f32p), None if di_init is None else _p(init, _f32p), _p(kd, _u32p), _p(kern, _f32p), n, k, seed, int(want_fp64), tol, node_begin,
                        ne, _p(cell, _u32p), _p(nt, _i32p), _p(mg, _i32p), _p(gap, _f64p), _p(oid, _u32p),
@@ -188,6 +204,8 @@ def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp
         raise ValueError("oracle: categorical variables with missing training-image values are undefined")
     if rc == -3:
         raise ValueError("oracle: kernel index image out of range")
+    if rc == -4:
+        raise ValueError("oracle: -fs is restated for complete training images and mode 0 only")
     return dict(sim=d, id=oid, cell=cell, near_tie=nt.astype(bool), marginal=mg.astype(bool), gap=gap,
                 probe_cross=pcross)
 

@@ -71,6 +71,28 @@ LOCAL = {
 }
 
 
+# -fs (one path node per cell value): name -> (ti builder, di shape, types, k, n (int or list), seed)
+FULL = {
+    "grf2d_fs": (lambda: syn.grf((60, 70), (6, 6), seed=3), (24, 28), [0], 1.2, 20, 100),
+    "bivar2d_fs": (lambda: syn.bivariate(syn.grf((60, 70), (6, 6), seed=5)), (16, 18, 2), [0, 1], 1.2, 15, 100),
+    "bivar2d_fs_n2": (lambda: syn.bivariate(syn.grf((60, 70), (6, 6), seed=5)), (16, 18, 2), [0, 1], 1.2, [10, 20],
+                      100),
+}
+
+
+def make_full(names=None):
+    for name, (mk, dshape, types, k, n, seed) in FULL.items():
+        if names and name not in names:
+            continue
+        ti = mk()
+        di = np.full(dshape, np.nan, np.float32)
+        args = ["-k", str(k), "-s", str(seed), "-j", "1", "-fs", "-n"] + [str(x) for x in np.ravel(n)]
+        sim, idx, ms, _ = ref.run_qs(ti, di, types, args, job_id=3300 + len(name))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k,
+                            n=np.array(n), seed=seed, sim=sim, idx=idx, ref_ms=ms)
+        print(name, ti.shape, dshape, idx.shape)
+
+
 def make_local(names=None):
     for name, (mk, dshape, types, k, n, seed, what) in LOCAL.items():
         if names and name not in names:
@@ -141,5 +163,7 @@ if __name__ == "__main__":
         oracle_teacher_config0()
     elif args[:1] == ["local"]:
         make_local(args[1:])
+    elif args[:1] == ["full"]:
+        make_full(args[1:])
     else:
         main(args)

@@ -265,3 +265,59 @@ def test_local_controls_rejects_bad_kernel_index(g2s, gpu):
     bad[3, 4] = 2
     with pytest.raises(RuntimeError, match="kernel index"):
         g2s.Simulation(g["ti"], g["di"], [0], n=20, k=1.2, seed=100, kernels=[g["k0"], g["k1"]], kii=bad)
+
+
+# ---------------------------------------------------------------------------
+# -fs: one path node per (cell, variable) value
+# ---------------------------------------------------------------------------
+FULL = ["grf2d_fs", "bivar2d_fs", "bivar2d_fs_n2"]
+
+
+def full_args(g):
+    n = np.asarray(g["n"])
+    return (int(n.max()), {"n_per_var": [int(x) for x in n]}) if n.ndim > 0 else (int(n), {})
+
+
+def run_gpu_full(g2s, g, teacher=None):
+    types = [int(t) for t in g["types"]]
+    n, kw = full_args(g)
+    sim = g2s.Simulation(g["ti"], g["di"], types, n=n, k=float(g["k"]), seed=int(g["seed"]), full=True, **kw)
+    if teacher is None:
+        sim.run()
+    else:
+        sim.run_teacher(teacher)
+    out = sim.read()
+    sim.close()
+    return out
+
+
+@pytest.mark.parametrize("name", FULL)
+def test_full_simulation_equals_oracle(g2s, gpu, oracle, name):
+    g = golden(name)
+    types = [int(t) for t in g["types"]]
+    sim, idx, _ = run_gpu_full(g2s, g)
+    n, kw = full_args(g)
+    o = oracle.simulate(g["ti"], g["di"], types, n, float(g["k"]), int(g["seed"]), full=True, **kw)
+    assert np.array_equal(idx.ravel(), o["id"])
+    assert np.array_equal(sim, o["sim"], equal_nan=True)
+
+
+def test_full_simulation_equals_reference(g2s, gpu):
+    g = golden("grf2d_fs")
+    sim, idx, _ = run_gpu_full(g2s, g)
+    assert np.array_equal(idx.ravel(), g["idx"].ravel())
+    assert np.array_equal(sim, g["sim"])
+
+
+@pytest.mark.parametrize("name", FULL)
+def test_full_simulation_teacher_forced(g2s, gpu, oracle, name):
+    g = golden(name)
+    types = [int(t) for t in g["types"]]
+    _, _, cells = run_gpu_full(g2s, g, teacher=g["sim"])
+    n, kw = full_args(g)
+    tf = oracle.simulate(g["ti"], g["sim"], types, n, float(g["k"]), int(g["seed"]), mode=1, want_fp64=True,
+                         di_init=g["di"], full=True, **kw)
+    assert np.array_equal(cells, tf["cell"])
+    order, seeds, post, begin = oracle.path(g["di"], len(types), int(g["seed"]), full=True)
+    ref_cells = g["idx"].ravel()[order[begin:]]
+    assert not np.any((cells != ref_cells) & ~tf["near_tie"])

@@ -114,3 +114,32 @@ def test_oracle_local_controls_teacher_forced(oracle, name):
     mismatch = tf["cell"] != ref_cells
     assert not np.any(mismatch & ~tf["near_tie"])
     assert mismatch.sum() <= 0.05 * mismatch.size
+
+
+def full_kwargs(g):
+    n = np.asarray(g["n"])
+    return (int(n.max()), {"n_per_var": [int(x) for x in n]}) if n.ndim > 0 else (int(n), {})
+
+
+def test_oracle_full_simulation_equals_reference(oracle):
+    """-fs, one variable: the whole simulation equals the reference's."""
+    g = golden("grf2d_fs")
+    out = oracle.simulate(g["ti"], g["di"], [0], int(g["n"]), float(g["k"]), int(g["seed"]), full=True)
+    assert np.array_equal(out["id"], g["idx"].ravel())
+    assert np.array_equal(out["sim"], g["sim"])
+
+
+@pytest.mark.parametrize("name", ["grf2d_fs", "bivar2d_fs", "bivar2d_fs_n2"])
+def test_oracle_full_simulation_teacher_forced(oracle, name):
+    """-fs teacher-forced on the reference's output: identical outside FP64
+    near-ties (the bivariate cases have a categorical variable)."""
+    g = golden(name)
+    types = [int(t) for t in g["types"]]
+    n, kw = full_kwargs(g)
+    tf = oracle.simulate(g["ti"], g["sim"], types, n, float(g["k"]), int(g["seed"]), mode=1, want_fp64=True,
+                         di_init=g["di"], full=True, **kw)
+    order, seeds, post, begin = oracle.path(g["di"], len(types), int(g["seed"]), full=True)
+    ref_cells = g["idx"].ravel()[order[begin:]]
+    mismatch = tf["cell"] != ref_cells
+    assert not np.any(mismatch & ~tf["near_tie"])
+    assert mismatch.sum() <= 0.05 * mismatch.size
