@@ -92,6 +92,10 @@ SIGNATURES = {
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
     "qsk_set_map_mode": (ctypes.c_int, [ctypes.c_int]),
     "qsk_qs_path": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, _f32p, ctypes.c_uint, _u32p, _f32p]),
+    "qsk_bgrid_read": (ctypes.c_int, [ctypes.c_char_p, _i32p, _u32p, _i32p, _i32p, ctypes.c_int, _i32p,
+                                      ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
+    "qsk_bgrid_write": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _u32p, ctypes.c_int, _i32p, ctypes.c_int,
+                                       ctypes.c_void_p, ctypes.c_int]),
 }
 
 
@@ -393,3 +397,36 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     finally:
         sim.close()
     return out, idx
+
+
+def read_bgrid(path: str):
+    """Read a G2S .bgrid(.gz) grid: returns (array with numpy shape
+    (..., ny, nx[, nvar]), types).  Unsigned-integer grids (index images)
+    come back as uint32."""
+    nd, nv, enc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    dims = (ctypes.c_uint * 16)()
+    types = (ctypes.c_int * 4096)()
+    count = ctypes.c_longlong()
+    _check(lib().qsk_bgrid_read(path.encode(), ctypes.byref(nd), dims, ctypes.byref(nv), types, 4096,
+                                ctypes.byref(enc), None, 0, ctypes.byref(count)), "qsk_bgrid_read")
+    dt = {0: np.float32, 1: np.int32, 2: np.uint32}[enc.value]
+    out = np.empty(count.value, dt)
+    _check(lib().qsk_bgrid_read(path.encode(), ctypes.byref(nd), dims, ctypes.byref(nv), types, 4096,
+                                ctypes.byref(enc), out.ctypes.data, count.value, ctypes.byref(count)),
+           "qsk_bgrid_read")
+    shape = tuple(reversed([dims[i] for i in range(nd.value)])) + ((nv.value,) if nv.value > 1 else ())
+    return out.reshape(shape), [types[i] for i in range(nv.value)]
+
+
+def write_bgrid(path: str, arr: np.ndarray, types: Sequence[int], compress: bool = False) -> None:
+    """Write a G2S .bgrid grid; ``arr`` has numpy shape (..., ny, nx[, nvar])
+    with nvar = len(types) > 1; float32 (encoding 0) or uint32 (encoding 2)."""
+    a = np.ascontiguousarray(arr)
+    enc = 2 if a.dtype == np.uint32 else (1 if a.dtype == np.int32 else 0)
+    if enc == 0:
+        a = np.ascontiguousarray(a, dtype=np.float32)
+    nvar = len(types)
+    dims = _grid_dims(a, nvar)
+    ty = np.asarray(types, np.int32)
+    _check(lib().qsk_bgrid_write(path.encode(), len(dims), _p(dims, _u32p), nvar, _p(ty, _i32p), enc, a.ctypes.data,
+                                 int(compress)), "qsk_bgrid_write")

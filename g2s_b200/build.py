@@ -2,6 +2,7 @@
 
     python -m g2s_b200.build          # -> g2s_b200/libg2s_b200.so
     python -m g2s_b200.build dropin   # -> g2s_b200/dropin/g2s_cuda.so (needs the G2S headers)
+    python -m g2s_b200.build cli      # -> g2s_b200/qs_b200 (the G2S `qs` command line)
 
 nvcc cross-compiles for sm_100a without a GPU.  The shared library is built
 in-tree so that it travels with the repository to the GPU machine.
@@ -19,7 +20,7 @@ LIB = os.path.join(PKG, "libg2s_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["qsk_kernels.cu", "qsk_host.cpp"]
+SOURCES = ["qsk_kernels.cu", "qsk_host.cpp", "qsk_bgrid.cpp"]
 
 
 def _run(cmd):
@@ -48,10 +49,21 @@ def build_lib(force: bool = False) -> str:
             cmd[cmd.index("-c"):cmd.index("-c")] = ["-x", "cu"]
         _run(cmd)
         objs.append(obj)
-    _run([NVCC, "-ccbin", HOSTCXX, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"])
+    _run([NVCC, "-ccbin", HOSTCXX, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lz"])
     for o in objs:
         os.remove(o)
     return LIB
+
+
+CLI = os.path.join(PKG, "qs_b200")
+
+
+def build_cli() -> str:
+    """qs_b200: the G2S `qs` command line on this library (host C++)."""
+    build_lib()
+    _run([HOSTCXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), os.path.join(PKG, "cli", "qs_b200.cpp"),
+          "-o", CLI, "-L", PKG, "-lg2s_b200", "-Wl,-rpath,$ORIGIN"])
+    return CLI
 
 
 DROPIN = os.path.join(PKG, "dropin")
@@ -76,5 +88,7 @@ def build_dropin(g2s_tree: str = "/root/reference") -> str:
 if __name__ == "__main__":
     if "dropin" in sys.argv:
         build_dropin(*[a for a in sys.argv[1:] if a.startswith("/")])
+    elif "cli" in sys.argv:
+        build_cli()
     else:
         build_lib(force="--force" in sys.argv)

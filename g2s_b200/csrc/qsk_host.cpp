@@ -37,6 +37,22 @@ int fail(int code, const char *fmt, ...) {
     return code;
 }
 
+}  // namespace
+
+namespace qsk {
+int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+}  // namespace qsk
+
+namespace {
+
 #define CK(expr)                                                                                          \
     do {                                                                                                  \
         cudaError_t e_ = (expr);                                                                          \

@@ -178,6 +178,9 @@ struct ReplayArgs {
 };
 
 
+// record the calling thread's error message (qsk_last_error) and return code
+int set_error(int code, const char *fmt, ...);
+
 // launch wrappers (qsk_kernels.cu)
 cudaError_t launch_build_layers(const float *ti, int nvar, const int *types, const Geom &g, float *layers, int missing,
                                 cudaStream_t st);

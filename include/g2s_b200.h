@@ -272,6 +272,23 @@ int qsk_set_map_mode(int mode);
 /* One call: setup, simulate, read back into di_inout / id_out (host). */
 int qsk_simulate(int device, const qsk_qs_params *p, float *di_inout, unsigned *id_out);
 
+/* ------------------------------------------------------------------------
+ * G2S grid files (.bgrid, optionally gzip-compressed .bgrid.gz): the
+ * serialised DataImage of the G2S data directory.  Replace
+ * DataImage::createFromFile / write (G2S include/DataImage.hpp:96-104,143-223,
+ * 281-323; src/DataImage.cpp:35-165) so that grids move between G2S and this
+ * library unchanged.
+ * ---------------------------------------------------------------------- */
+/* Read `path`.  Writes ndim, dims[ndim] (x first, up to 16), nvar, up to
+ * types_capacity variable types, the encoding (0 float, 1 int, 2 uint) and
+ * *count = prod(dims) * nvar; copies the 32-bit values (variables
+ * interleaved) to data when data is not NULL (capacity in values). */
+int qsk_bgrid_read(const char *path, int *ndim, unsigned *dims, int *nvar, int *types, int types_capacity,
+                   int *encoding, void *data, long long capacity, long long *count);
+/* Write a grid to `path` (gzip when compress != 0). */
+int qsk_bgrid_write(const char *path, int ndim, const unsigned *dims, int nvar, const int *types, int encoding,
+                    const void *data, int compress);
+
 #ifdef __cplusplus
 }
 #endif

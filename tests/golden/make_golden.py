@@ -93,6 +93,22 @@ def make_full(names=None):
         print(name, ti.shape, dshape, idx.shape)
 
 
+def make_bgrid():
+    """Grids written by the reference's own DataImage::write (gzip and plain),
+    copied out of its data directory, for the .bgrid reader tests."""
+    import shutil
+    rng = np.random.default_rng(12)
+    a = rng.standard_normal((5, 7, 2)).astype(np.float32)
+    a[1, 2, 0] = np.nan
+    for compressed, ext in ((True, ".bgrid.gz"), (False, ".bgrid")):
+        name = f"g2sb200_bgrid_{int(compressed)}"
+        ref.write_image(name, a, [0, 1], compressed=compressed)
+        src = os.path.realpath(f"/tmp/G2S/data/{name}{ext}")
+        shutil.copyfile(src, os.path.join(HERE, f"ref_written{ext}"))
+    np.save(os.path.join(HERE, "ref_written_values.npy"), a)
+    print("bgrid fixtures", a.shape)
+
+
 def make_local(names=None):
     for name, (mk, dshape, types, k, n, seed, what) in LOCAL.items():
         if names and name not in names:
@@ -165,5 +181,7 @@ if __name__ == "__main__":
         make_local(args[1:])
     elif args[:1] == ["full"]:
         make_full(args[1:])
+    elif args == ["bgrid"]:
+        make_bgrid()
     else:
         main(args)
