@@ -1734,6 +1734,8 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         // (earlier lanes, then earlier positions of this lane)
         unsigned rmask = 0;
         const float T0 = st[KF - 1];
+        unsigned eqm = 0u;       // records whose value is tval (no count extraction)
+        float tval = 0.f;
         if (T0 == -CUDART_INF_F) {
             // every existing position may qualify: exact scan of the 32 positions
             if (vm != 0u || emit_masked) {
@@ -1759,14 +1761,24 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                     eq &= ~cb[bb];
                 }
             }
-            unsigned cand = (T > 255) ? 0u : (gt | eq);
-            while (cand) {
-                const int bit = __ffs(cand) - 1;
-                cand &= cand - 1u;
+            if (T > 255) gt = eq = 0u;
+            // Positions equal to T0 are records while the running K-th is still
+            // T0 and never change the state; only positions above T0 need their
+            // count and an insertion.  The first insertion that lifts the K-th
+            // above T0 ends the equal records.
+            unsigned eqcut = 0xffffffffu;
+            unsigned g = gt;
+            while (g) {
+                const int bit = __ffs(g) - 1;
+                g &= g - 1u;
                 const float x = (float)count_at(bit);
                 if (x >= st[KF - 1]) rmask |= 1u << bit;
                 topk_insert<KF>(st, x);
+                if (eqcut == 0xffffffffu && st[KF - 1] > T0) eqcut = bit >= 31 ? 0xffffffffu : ((2u << bit) - 1u);
             }
+            rmask |= eq & eqcut;
+            eqm = eq;
+            tval = T0;
         }
         // offsets inside each 128-position sub-segment (4 lanes)
         const int rc = __popc(rmask);
@@ -1788,7 +1800,7 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             while (rm) {
                 const int bit = __ffs(rm) - 1;
                 rm &= rm - 1u;
-                rv[rb + o] = ((vm >> bit) & 1u) ? (float)count_at(bit) : -CUDART_INF_F;
+                rv[rb + o] = ((eqm >> bit) & 1u) ? tval : (((vm >> bit) & 1u) ? (float)count_at(bit) : -CUDART_INF_F);
                 ri[rb + o] = int(m0 + bit);
                 o++;
             }
