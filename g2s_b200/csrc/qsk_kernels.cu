@@ -1528,6 +1528,13 @@ __global__ void k_build_planes(const float *__restrict__ layers, Geom g, int nva
     planes[idx] = word;
 }
 
+// bits [a, b) of a word, 0 <= a, b <= 32
+__device__ __forceinline__ unsigned bits_range(int a, int b) {
+    if (a >= b) return 0u;
+    const unsigned hi = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
+    return hi & ~((1u << a) - 1u);
+}
+
 template <int KF>
 __device__ __forceinline__ void topk_insert(float (&st)[KF], float x) {
     // insert x into the descending list st, dropping the smallest
@@ -1740,20 +1747,36 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         // record flags: value not below the K-th best of everything before it
         // (earlier lanes, then earlier positions of this lane)
         unsigned rmask = 0;
-        const float T0 = st[KF - 1];
+        const float T0s = st[KF - 1];
         unsigned eqm = 0u;       // records whose value is tval (no count extraction)
         float tval = 0.f;
+        unsigned from = 0xffffffffu;   // positions decided by the threshold path below
+        float T0 = T0s;
         if (T0 == -CUDART_INF_F) {
-            // every existing position may qualify: exact scan of the 32 positions
-            if (vm != 0u || emit_masked) {
-                for (int bit = 0; bit < 32; ++bit) {
-                    if (!((emask >> bit) & 1u)) continue;
-                    const float x = ((vm >> bit) & 1u) ? (float)count_at(bit) : -CUDART_INF_F;
-                    if (x >= st[KF - 1] && (((vmask >> bit) & 1u) || emit_masked)) rmask |= 1u << bit;
-                    topk_insert<KF>(st, x);
-                }
+            // Fewer than K finite values before this lane: every position is a
+            // record until K finite values are held (masked ones only when they
+            // can be candidates).  Only the valid positions up to that point are
+            // visited one by one; the rest of the lane takes the threshold path.
+            const unsigned recok = emit_masked ? emask : (emask & vmask);
+            unsigned vv = vm;
+            int cur = 0;
+            while (vv && st[KF - 1] == -CUDART_INF_F) {
+                const int bit = __ffs(vv) - 1;
+                vv &= vv - 1u;
+                rmask |= recok & bits_range(cur, bit);
+                rmask |= 1u << bit;
+                topk_insert<KF>(st, (float)count_at(bit));
+                cur = bit + 1;
             }
-        } else {
+            if (st[KF - 1] == -CUDART_INF_F) {
+                rmask |= recok & bits_range(cur, 32);
+                from = 0u;
+            } else {
+                from = bits_range(cur, 32);
+            }
+            T0 = st[KF - 1];
+        }
+        if (from) {
             // only positions with count >= T0 can be records (the running K-th
             // never drops below T0; a smaller value leaves the state unchanged)
             const int T = (int)T0;
@@ -1769,6 +1792,8 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                 }
             }
             if (T > 255) gt = eq = 0u;
+            gt &= from;
+            eq &= from;
             // Positions equal to T0 are records while the running K-th is still
             // T0 and never change the state; only positions above T0 need their
             // count and an insertion.  The first insertion that lifts the K-th
