@@ -615,6 +615,9 @@ unsigned qsk_position_to_index(const qsk_ti *ti, const int *min_offset, unsigned
 struct qsk_sim {
     int device = 0;
     cudaStream_t st = nullptr;
+    // generator states are prepared on st_rng while st runs the map
+    cudaStream_t st_rng = nullptr;
+    cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
     qsk_ti *ti = nullptr;
     int nd = 0, nvar = 0, n = 0, K = 1;
     float k = 1.f;
@@ -651,6 +654,8 @@ struct qsk_sim {
     DBuf<float> d_rec_val;
     DBuf<int> d_rec_idx, d_rec_cnt;
     DBuf<float> d_rec_max;
+    DBuf<unsigned> d_mt_state;       // [2][slot][624]: two batches
+    DBuf<int> d_mt_pre;
     DBuf<int> d_tpl_range, d_node_kernel, d_node_lim, d_node_nv;
     DBuf<unsigned char> d_nb_mask;
     DBuf<float> d_node_k;
@@ -851,43 +856,68 @@ cudaEvent_t prof_event(qsk_sim *s) {
 int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     const Geom &g = s->ti->g;
     s->prof_used = 0;
-    for (size_t l = 0; l + 1 < start.size(); ++l) {
-        int a = start[l], e = start[l + 1];
-        for (int off = a; off < e; off += s->max_slots) {
-            int B = std::min(s->max_slots, e - off);
-            SimPrepArgs pa;
-            pa.g = g;
-            pa.dg = s->dg;
-            pa.nvar = s->nvar;
-            pa.types = s->d_types.p;
-            pa.tpl = s->d_tpl.p;
-            pa.wtab = s->d_wtab.p;
-            pa.path = s->d_path.p;
-            pa.begin = s->begin;
-            pa.seeds = s->d_seeds.p;
-            pa.nb_count = s->d_nb_count.p;
-            pa.nb_tpl = s->d_nb_tpl.p;
-            pa.nb_cell = s->d_nb_cell.p;
-            pa.n = s->n;
-            pa.state = s->d_state.p;
-            pa.init = s->d_init.p;
-            pa.nodes = s->d_level_nodes.p + off;
-            pa.nslots = B;
-            pa.k = s->k;
-            pa.K = s->K;
-            pa.nti = 1;
-            pa.slots = s->d_slots.p;
-            pa.terms = s->d_terms.p;
-            pa.maxterms = s->maxterms;
-            pa.status = s->d_status.p;
-            pa.missing = s->ti->missing ? 1 : 0;
-            pa.mask_layer = s->nvar;
-            pa.no_verbatim = s->no_verbatim;
-            pa.id_image = s->d_id.p;
-            pa.node_nv = s->local ? s->d_node_nv.p : nullptr;
-            pa.node_k = s->local ? s->d_node_k.p : nullptr;
-            pa.full = s->full ? 1 : 0;
-            pa.nb_mask = s->full ? s->d_nb_mask.p : nullptr;
+    // batches: (first entry in the level node list, slots), levels in order
+    std::vector<std::pair<int, int>> batches;
+    for (size_t l = 0; l + 1 < start.size(); ++l)
+        for (int off = start[l]; off < start[l + 1]; off += s->max_slots)
+            batches.emplace_back(off, std::min(s->max_slots, start[l + 1] - off));
+    auto prep_args = [&](int off, int B) {
+        SimPrepArgs pa;
+        pa.g = g;
+        pa.dg = s->dg;
+        pa.nvar = s->nvar;
+        pa.types = s->d_types.p;
+        pa.tpl = s->d_tpl.p;
+        pa.wtab = s->d_wtab.p;
+        pa.path = s->d_path.p;
+        pa.begin = s->begin;
+        pa.seeds = s->d_seeds.p;
+        pa.nb_count = s->d_nb_count.p;
+        pa.nb_tpl = s->d_nb_tpl.p;
+        pa.nb_cell = s->d_nb_cell.p;
+        pa.n = s->n;
+        pa.state = s->d_state.p;
+        pa.init = s->d_init.p;
+        pa.nodes = s->d_level_nodes.p + off;
+        pa.nslots = B;
+        pa.k = s->k;
+        pa.K = s->K;
+        pa.nti = 1;
+        pa.slots = s->d_slots.p;
+        pa.terms = s->d_terms.p;
+        pa.maxterms = s->maxterms;
+        pa.status = s->d_status.p;
+        pa.missing = s->ti->missing ? 1 : 0;
+        pa.mask_layer = s->nvar;
+        pa.no_verbatim = s->no_verbatim;
+        pa.id_image = s->d_id.p;
+        pa.node_nv = s->local ? s->d_node_nv.p : nullptr;
+        pa.node_k = s->local ? s->d_node_k.p : nullptr;
+        pa.full = s->full ? 1 : 0;
+        pa.nb_mask = s->full ? s->d_nb_mask.p : nullptr;
+        return pa;
+    };
+    // Generator states of batch j go to buffer j % 2 on st_rng, one batch
+    // ahead of the simulation on st; buffer p is rewritten only after the
+    // replay that read it (ev_used[p]).
+    const size_t mt_words = size_t(s->max_slots) * 624;
+    auto launch_rng = [&](size_t j) -> int {
+        const int p = int(j & 1);
+        CK(cudaStreamWaitEvent(s->st_rng, s->ev_used[p], 0));
+        CK(launch_mt_prep(prep_args(batches[j].first, batches[j].second), s->d_mt_state.p + p * mt_words,
+                          s->d_mt_pre.p + size_t(p) * s->max_slots, s->st_rng));
+        CK(cudaEventRecord(s->ev_ready[p], s->st_rng));
+        return QSK_OK;
+    };
+    CK(cudaEventRecord(s->ev_used[0], s->st));   // after everything queued so far on st
+    CK(cudaEventRecord(s->ev_used[1], s->st));
+    int rc = batches.empty() ? QSK_OK : launch_rng(0);
+    if (rc) return rc;
+    for (size_t j = 0; j < batches.size(); ++j) {
+        const int B = batches[j].second, p = int(j & 1);
+        if (j + 1 < batches.size() && (rc = launch_rng(j + 1)) != QSK_OK) return rc;
+        {
+            const SimPrepArgs pa = prep_args(batches[j].first, B);
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             CK(launch_prep_sim(pa, s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
@@ -922,7 +952,7 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
                 CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
             }
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            s->info.launches += 3;
+            s->info.launches += 4;
             s->info.map_launches += 1;
             s->info.map_positions += (long long)B * g.N;
             ReplayArgs ra;
@@ -945,7 +975,11 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.id_image = teacher ? nullptr : s->d_id.p;
             ra.node_cell = s->d_node_cell.p;
             ra.full = s->full ? 1 : 0;
+            ra.mt_state = s->d_mt_state.p + p * mt_words;
+            ra.mt_pre = s->d_mt_pre.p + size_t(p) * s->max_slots;
+            CK(cudaStreamWaitEvent(s->st, s->ev_ready[p], 0));
             CK(launch_replay(ra, s->st));
+            CK(cudaEventRecord(s->ev_used[p], s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         }
     }
@@ -1031,6 +1065,11 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     if (s->full && s->ti->missing)
         return bail(fail(QSK_ERR_UNSUPPORTED, "-fs with missing training-image values is not implemented"));
     cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st_rng, cudaStreamNonBlocking);
+    for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
+        e = cudaEventCreateWithFlags(&s->ev_ready[p], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_used[p], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) return bail(fail(QSK_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
     s->cells = 1;
     std::memset(&s->dg, 0, sizeof(s->dg));
@@ -1150,6 +1189,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     ms = std::min<long long>(ms, 65535);
     s->max_slots = int(ms);
     if ((e = s->d_slots.alloc(size_t(s->max_slots))) != cudaSuccess ||
+        (e = s->d_mt_state.alloc(size_t(2) * s->max_slots * 624)) != cudaSuccess ||
+        (e = s->d_mt_pre.alloc(size_t(2) * s->max_slots)) != cudaSuccess ||
         (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess ||
         (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "scratch: %s",
@@ -1294,6 +1335,11 @@ int qsk_sim_destroy(qsk_sim *s) {
     {
         DeviceGuard dgd(s->device);
         for (auto e : s->prof_ev) cudaEventDestroy(e);
+        for (int p = 0; p < 2; ++p) {
+            if (s->ev_ready[p]) cudaEventDestroy(s->ev_ready[p]);
+            if (s->ev_used[p]) cudaEventDestroy(s->ev_used[p]);
+        }
+        if (s->st_rng) cudaStreamDestroy(s->st_rng);
         if (s->st) cudaStreamDestroy(s->st);
         s->st = nullptr;
         if (s->ti) qsk_ti_destroy(s->ti);

@@ -175,6 +175,10 @@ struct ReplayArgs {
     unsigned *id_image;   // per grid cell (-fs: per cell value)
     unsigned *node_cell;  // per path index: chosen TI cell
     int full;             // -fs: write the slot's variable only
+    // generator states from k_mt_prep ([slot][624]) and the draws their
+    // skipped blocks stand for; null: each slot is seeded in the replay
+    const unsigned *mt_state;
+    const int *mt_pre;
 };
 
 
@@ -225,5 +229,6 @@ cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, co
 int map_bits_segs_per_cta(const Geom &g, int nslots);
 cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
+cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cudaStream_t st);
 
 }  // namespace qsk

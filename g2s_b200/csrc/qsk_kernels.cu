@@ -398,33 +398,27 @@ __device__ __forceinline__ int selected_index(float seed, float k, unsigned nti)
 // ---------------------------------------------------------------------------
 // prep for the simulation: one warp per slot
 // ---------------------------------------------------------------------------
-__global__ void k_prep_sim(SimPrepArgs A) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= A.nslots) return;
-    const int i = A.nodes[warp];
-    const unsigned pv = A.path[A.begin + i];
-    // -fs: the path entry is a cell value (cell * nvar + variable)
-    const unsigned cell = A.full ? pv / unsigned(A.nvar) : pv;
+// The part of a node's slot that follows from the neighbour lists and the
+// initial grid alone (not from simulated values), shared by k_prep_sim and
+// k_mt_prep: candidate count, neighbour offset minima, first valid scan
+// coordinate per dimension, number of valid positions, marginal draw.
+struct NodeGeom {
+    float lk;
+    int Ki;
+    int mn[QSK_MAXD];
+    int lo[QSK_MAXD];
+    long long nvalid;
+    bool skip;
+};
+
+__device__ NodeGeom node_geometry(const SimPrepArgs &A, int i, unsigned cell, int lane) {
+    NodeGeom r;
     const int cnt = A.nb_count[i];
     const int nd = A.g.nd;
-    Slot s;
-    s.node = i;
-    s.cell = cell;
-    s.var = A.full ? int(pv % unsigned(A.nvar)) : 0;
-    s.seed = A.seeds[i];
     // candidate count of this node: -kvi or k (quantileSamplingModule.hpp:90-113)
-    const float lk = A.node_k ? A.node_k[i] : A.k;
-    int Ki = int(ceilf(lk));
-    Ki = Ki < 1 ? 1 : (Ki > QSK_KMAX ? QSK_KMAX : Ki);
-    s.K = Ki;
-    s.sel = selected_index(s.seed, lk, A.nti);
-    if (s.sel < 0) s.sel = 0;
-    if (s.sel > Ki - 1) s.sel = Ki - 1;   // unreachable for k >= 1 and seeds in [0,1)
-    s.flags = 0;
-    s.nterms = 0;
-    s.excl = -1;
-    s.cmask_base = 0;
+    r.lk = A.node_k ? A.node_k[i] : A.k;
+    int Ki = int(ceilf(r.lk));
+    r.Ki = Ki < 1 ? 1 : (Ki > QSK_KMAX ? QSK_KMAX : Ki);
     // vector simulation: data at the centre also forces a search
     // (simulation.hpp:565-584); -fs draws from the marginal below two
     // neighbours (simulation.hpp:952-965)
@@ -450,21 +444,58 @@ __global__ void k_prep_sim(SimPrepArgs A) {
             mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], off));
         }
     }
-    long long nvalid = 1;
+    r.nvalid = 1;
     for (int d = 0; d < QSK_MAXD; ++d) {
-        s.mn[d] = mn[d];
+        r.mn[d] = mn[d];
         int lo = 0;
         if (d < nd) {
             lo = A.g.fft[d] - (A.g.src[d] - (mx[d] - mn[d]));
             lo = lo < 0 ? 0 : (lo > A.g.fft[d] ? A.g.fft[d] : lo);
-            nvalid *= (A.g.fft[d] - lo);
+            r.nvalid *= (A.g.fft[d] - lo);
         }
-        s.lo[d] = lo;
+        r.lo[d] = lo;
     }
-    if (cnt <= 1 && !centreData) {
-        s.flags |= SLOT_SKIP;   // marginal draw (simulation.hpp:586-605)
+    r.skip = cnt <= 1 && !centreData;   // marginal draw (simulation.hpp:586-605)
+    return r;
+}
+
+__global__ void k_prep_sim(SimPrepArgs A) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= A.nslots) return;
+    const int i = A.nodes[warp];
+    const unsigned pv = A.path[A.begin + i];
+    // -fs: the path entry is a cell value (cell * nvar + variable)
+    const unsigned cell = A.full ? pv / unsigned(A.nvar) : pv;
+    const int cnt = A.nb_count[i];
+    const int nd = A.g.nd;
+    const NodeGeom ng = node_geometry(A, i, cell, lane);
+    Slot s;
+    s.node = i;
+    s.cell = cell;
+    s.var = A.full ? int(pv % unsigned(A.nvar)) : 0;
+    s.seed = A.seeds[i];
+    const float lk = ng.lk;
+    const int Ki = ng.Ki;
+    s.K = Ki;
+    s.sel = selected_index(s.seed, lk, A.nti);
+    if (s.sel < 0) s.sel = 0;
+    if (s.sel > Ki - 1) s.sel = Ki - 1;   // unreachable for k >= 1 and seeds in [0,1)
+    s.flags = 0;
+    s.nterms = 0;
+    s.excl = -1;
+    s.cmask_base = 0;
+    int mn[QSK_MAXD];
+#pragma unroll
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        mn[d] = ng.mn[d];
+        s.mn[d] = ng.mn[d];
+        s.lo[d] = ng.lo[d];
+    }
+    if (ng.skip) {
+        s.flags |= SLOT_SKIP;
     } else {
-        if (nvalid < Ki) s.flags |= SLOT_EMIT_MASKED;
+        if (ng.nvalid < Ki) s.flags |= SLOT_EMIT_MASKED;
         // terms: neighbours in order, variables in order; zero-weight / NaN skipped
         int base_out = 0;
         for (int j0 = 0; j0 < cnt; j0 += 32) {
@@ -838,6 +869,20 @@ __device__ __forceinline__ void mt_twist(unsigned *mt, int lane, float *out, flo
     __syncwarp();
 }
 
+// generator.seed(seedFromUnitFloat(seed) + 0)  (quantileSamplingModule.hpp:45-49,533-534):
+// the standard mt19937 initialisation, serial, on the calling thread
+__device__ __forceinline__ void mt_seed(unsigned *mt, float sd) {
+    unsigned x;
+    if (!isfinite(sd) || sd <= 0.f) x = 0u;
+    else if (sd >= 1.f) x = 0xffffffffu;
+    else x = (unsigned)floor((double)sd * 4294967295.0);
+    mt[0] = x;
+    for (int i = 1; i < 624; ++i) {
+        x = 1812433253u * (x ^ (x >> 30)) + (unsigned)i;
+        mt[i] = x;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // replay of the k-biggest scan + draw + write-back; one warp per slot
 // ---------------------------------------------------------------------------
@@ -845,6 +890,7 @@ __device__ __forceinline__ void mt_twist(unsigned *mt, int lane, float *out, flo
 #define REC_CAP 1024          // records (padded to 4 per segment) of one tie super-run
 #define TAB_CAP 128           // segments of one tie super-run
 #define RNG_BUF (2 * REC_CAP + 640)   // draws of one super-run + one block
+#define SEG_WIN 256           // record counts and maxima of SEG_WIN segments staged per warp
 
 struct __align__(16) WarpShared {
     float rv_s[REC_CAP];      // super-run records (values), 16-byte aligned for cp.async
@@ -855,7 +901,32 @@ struct __align__(16) WarpShared {
     int tseg[TAB_CAP];        // super-run segments, their first padded record, record count
     int tpre[TAB_CAP];
     int tcnt[TAB_CAP];
+    int wc[SEG_WIN];          // record counts and maxima of segments [wbase, wbase + SEG_WIN)
+    float wm[SEG_WIN];
 };
+
+// Make segments [q0, q0 + 32) readable from the window (w.wc / w.wm at q - wbase).
+// The scan only moves forward, so a miss restages the window from q0 on.
+__device__ __forceinline__ void win_cover(WarpShared &w, int &wbase, int q0, int nseg, const int *rc, const float *rm,
+                                          int lane) {
+    if (q0 >= wbase && q0 + 32 <= wbase + SEG_WIN) return;
+    __syncwarp();
+    wbase = q0;
+    int c[SEG_WIN / 32];
+    float m[SEG_WIN / 32];
+#pragma unroll
+    for (int i = 0; i < SEG_WIN / 32; ++i) {
+        const int q = q0 + lane + 32 * i;
+        c[i] = q < nseg ? rc[q] : 0;
+        m[i] = q < nseg ? rm[q] : -CUDART_INF_F;
+    }
+#pragma unroll
+    for (int i = 0; i < SEG_WIN / 32; ++i) {
+        w.wc[lane + 32 * i] = c[i];
+        w.wm[lane + 32 * i] = m[i];
+    }
+    __syncwarp();
+}
 
 // Draw buffer with warp-replicated read pointer: rp/len live in registers of
 // every lane (all lanes execute the same control flow).
@@ -1142,13 +1213,18 @@ template <int KM>
 __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const float *rv, const int *ri, unsigned (&cp)[KM],
                                  unsigned &cpt, int &rp, int &len, WarpShared &w, int lane) {
     const unsigned FULL = 0xffffffffu;
-    for (int e = 0; e < E; ++e) {
-        const int sgm = w.tseg[e], pre = w.tpre[e], c = w.tcnt[e];
-        if (4 * lane < c) {
-            const long long src = (long long)sgm * QSK_SEG + 4 * lane;
-            cp_async16(&w.rv_s[pre + 4 * lane], rv + src);
-            cp_async16(&w.ri_s[pre + 4 * lane], ri + src);
+    // 16-byte chunk t (records 4t..4t+3 of the run) lies in the last entry e
+    // with tpre[e] <= 4t (tpre strictly increasing)
+    for (int t = lane; 4 * t < Tp; t += 32) {
+        int lo = 0, hi = E - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (w.tpre[mid] <= 4 * t) lo = mid;
+            else hi = mid - 1;
         }
+        const long long src = (long long)w.tseg[lo] * QSK_SEG + (4 * t - w.tpre[lo]);
+        cp_async16(&w.rv_s[4 * t], rv + src);
+        cp_async16(&w.ri_s[4 * t], ri + src);
     }
     cp_async_wait_all();
     __syncwarp();
@@ -1157,11 +1233,14 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
         for (int k = c; k < ((c + 3) & ~3); ++k) w.rv_s[pre + k] = -CUDART_INF_F;
     }
     __syncwarp();
-    const int P = (Tp + 31) >> 5;
-    const int j0 = lane * P;
+    // lane l owns records [l*P, l*P + P); P odd keeps the lanes' reads on
+    // distinct shared-memory banks (P <= 33 fits a 64-bit tie mask)
+    const int P = ((Tp + 31) >> 5) | 1;
+    const int j0 = min(Tp, lane * P);
     const int j1 = min(Tp, j0 + P);
-    int mine = 0;
-    for (int j = j0; j < j1; ++j) mine += (w.rv_s[j] == V) ? 1 : 0;
+    unsigned long long tmask = 0ull;
+    for (int j = j0; j < j1; ++j) tmask |= (unsigned long long)(w.rv_s[j] == V) << (j - j0);
+    const int mine = __popcll(tmask);
     int incl = mine;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -1174,8 +1253,9 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
     int o[KM];
 #pragma unroll
     for (int s2 = 0; s2 < KM; ++s2) o[s2] = s2;
-    for (int j = j0; j < j1; ++j) {
-        if (w.rv_s[j] != V) continue;
+    while (tmask) {
+        const int j = j0 + __ffsll((long long)tmask) - 1;
+        tmask &= tmask - 1ull;
         const float u1 = w.buf[rp + 2 * rank];
         const float u2 = w.buf[rp + 2 * rank + 1];
         int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
@@ -1225,8 +1305,8 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
 // segment above V, or nseg.
 template <int KM>
 __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, const float *rv, const int *ri, const int *rc,
-                                 const float *rm, unsigned (&cp)[KM], unsigned &cpt, int &rp, int &len, WarpShared &w,
-                                 int lane) {
+                                 const float *rm, int &wbase, unsigned (&cp)[KM], unsigned &cpt, int &rp, int &len,
+                                 WarpShared &w, int lane) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lt = lanemask_lt();
     for (;;) {
@@ -1236,9 +1316,10 @@ __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, cons
                 stop = nseg;
                 break;
             }
+            win_cover(w, wbase, sg, nseg, rc, rm, lane);
             const int q = sg + lane;
-            const int c = q < nseg ? rc[q] : 0;
-            const float m = q < nseg ? rm[q] : -CUDART_INF_F;
+            const int c = w.wc[q - wbase];
+            const float m = w.wm[q - wbase];
             const unsigned brk = __ballot_sync(FULL, c > 0 && m > V);
             const unsigned lim = brk ? ((1u << (__ffs(brk) - 1)) - 1u) : FULL;
             const bool elig = ((lim >> lane) & 1u) && c > 0 && m == V;
@@ -1331,18 +1412,14 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
             have = true;
         }
     } else {
-        // generator.seed(seedFromUnitFloat(seed) + 0)  (quantileSamplingModule.hpp:45-49,533-534)
-        if (lane == 0) {
-            unsigned x;
-            float sd = s.seed;
-            if (!isfinite(sd) || sd <= 0.f) x = 0u;
-            else if (sd >= 1.f) x = 0xffffffffu;
-            else x = (unsigned)floor((double)sd * 4294967295.0);
-            w.mt[0] = x;
-            for (int i = 1; i < 624; ++i) {
-                x = 1812433253u * (x ^ (x >> 30)) + (unsigned)i;
-                w.mt[i] = x;
-            }
+        // generator state: seeded here, or prepared by k_mt_prep together with
+        // the blocks that the first masked stretch of the scan skips
+        long long preskip = 0;
+        if (A.mt_state) {
+            for (int i = lane; i < 624; i += 32) w.mt[i] = A.mt_state[(long long)b * 624 + i];
+            preskip = A.mt_pre[b];
+        } else if (lane == 0) {
+            mt_seed(w.mt, s.seed);
         }
         __syncwarp();
         int rp = 0, len = 0;
@@ -1377,7 +1454,10 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                     const long long mm = __shfl_sync(FULL, (long long)m, 0);
                     long long c = (mm - (last + 1)) - (valid_prefix(g, s.lo, mm) - valid_prefix(g, s.lo, last + 1));
                     if (c > 0) {
-                        rng_skip(w, lane, rp, len, 2 * c);
+                        // the first skip covers the prepared blocks (c >= the masked
+                        // positions before the first valid one, so 2c > preskip)
+                        rng_skip(w, lane, rp, len, 2 * c - preskip);
+                        preskip = 0;
                         cpt += unsigned(c);
                     }
                 }
@@ -1393,7 +1473,7 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 r0 += width;
             }
         };
-        int sg = 0;
+        int sg = 0, wbase = -SEG_WIN;
         while (sg < g.nseg) {
             const float kth_s = sel_f<KM>(cv, K - 1);
             if (kth_s != -CUDART_INF_F) {
@@ -1401,15 +1481,17 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 int xes = 0;
 #pragma unroll
                 for (int q = 0; q < KM; ++q) xes += (q < K && cv[q] == kth_s) ? 1 : 0;
-                sg = replay_tie_stream<KM>(K, kth_s, xes, sg, g.nseg, rv, ri, rc, rm, cp, cpt, rp, len, w, lane);
+                sg = replay_tie_stream<KM>(K, kth_s, xes, sg, g.nseg, rv, ri, rc, rm, wbase, cp, cpt, rp, len, w, lane);
                 if (sg >= g.nseg) break;
-                general_segment(sg, rc[sg], rm[sg]);
+                win_cover(w, wbase, sg, g.nseg, rc, rm, lane);
+                general_segment(sg, w.wc[sg - wbase], w.wm[sg - wbase]);
                 ++sg;
                 continue;
             }
             // general replay, 32 segments at a time, until K finite values are held
-            const int myc = sg + lane < g.nseg ? rc[sg + lane] : 0;
-            const float mym = sg + lane < g.nseg ? rm[sg + lane] : -CUDART_INF_F;
+            win_cover(w, wbase, sg, g.nseg, rc, rm, lane);
+            const int myc = w.wc[sg - wbase + lane];
+            const float mym = w.wm[sg - wbase + lane];
             unsigned nz = __ballot_sync(FULL, myc > 0 && mym >= kth_s);
             int next = sg + 32;
             while (nz) {
@@ -1844,6 +1926,43 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
     }
 }
 
+// MT19937 state of each slot ahead of its replay (one warp per slot; the
+// host runs it for the next batch while the current one is simulated, as it
+// reads the neighbour lists only): the seeding, and with masked positions
+// not emitted as records
+// the state-only blocks of the replay's first skip.  That skip covers the c
+// masked positions before the first record (two draws each); c is at least
+// the number c0 of masked positions before the first valid one, so the
+// blocks that rng_skip regenerates without output for 2*c0 draws,
+// (2*c0 - 1) / 624 of them, are the first blocks of the real skip too.
+__global__ void __launch_bounds__(32 * RP_WARPS) k_mt_prep(SimPrepArgs A, unsigned *__restrict__ state,
+                                                           int *__restrict__ pre) {
+    __shared__ unsigned mt[RP_WARPS][624 + 32];
+    __shared__ float dummy[RP_WARPS][32];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * RP_WARPS + wib;
+    if (b >= A.nslots) return;
+    const int i = A.nodes[b];
+    const unsigned pv = A.path[A.begin + i];
+    const unsigned cell = A.full ? pv / unsigned(A.nvar) : pv;
+    const NodeGeom ng = node_geometry(A, i, cell, lane);
+    if (ng.skip) return;
+    if (lane == 0) mt_seed(mt[wib], A.seeds[i]);
+    __syncwarp();
+    int blocks = 0;
+    const Geom &g = A.g;
+    if (ng.nvalid >= ng.Ki && !A.missing && ng.nvalid > 0) {
+        long long m0 = 0;
+        for (int d = 0; d < g.nd; ++d) m0 += (long long)ng.lo[d] * g.sstride[d];
+        const long long n = 2 * (m0 - valid_prefix(g, ng.lo, m0));
+        if (n > 624) blocks = int((n - 1) / 624);
+    }
+    for (int t = 0; t < blocks; ++t) mt_twist<false>(mt[wib], lane, nullptr, dummy[wib]);
+    __syncwarp();
+    for (int i = lane; i < 624; i += 32) state[(long long)b * 624 + i] = mt[wib][i];
+    if (lane == 0) pre[b] = 624 * blocks;
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers (called by the host engine)
 // ---------------------------------------------------------------------------
@@ -1974,6 +2093,11 @@ cudaError_t set_map_smem_limit(int bytes) {
     e = cudaFuncSetAttribute(k_map_records<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_map_records<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cudaStream_t st) {
+    k_mt_prep<<<(unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS), 32 * RP_WARPS, 0, st>>>(a, state, pre);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
