@@ -1205,28 +1205,16 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // state, so the state's values stay as they are, every record equal to V is a
 // tie (two draws, cpt + 1, a swap inside the xes tail slots that hold V and a
 // possible replacement at K-1) and the others are no-ops.  The run's segments
-// (w.tseg/tpre/tcnt, E entries, Tp padded records) are copied to shared memory
-// with 16-byte asynchronous copies; lane l then owns a contiguous range of
-// the run, counts its ties, composes the slot maps of its ties on its own,
-// and one warp reduction combines the 32 lane maps in order.
+// (w.tseg/tpre/tcnt, E entries, Tp padded records) arrive in shared memory by
+// the 16-byte asynchronous copies issued while they were gathered; lane l
+// then owns a contiguous range of the run, counts its ties, composes the slot
+// maps of its ties on its own, and one warp reduction combines the 32 lane
+// maps in order.
 template <int KM>
 __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const float *rv, const int *ri, unsigned (&cp)[KM],
                                  unsigned &cpt, int &rp, int &len, WarpShared &w, int lane) {
     const unsigned FULL = 0xffffffffu;
-    // 16-byte chunk t (records 4t..4t+3 of the run) lies in the last entry e
-    // with tpre[e] <= 4t (tpre strictly increasing)
-    for (int t = lane; 4 * t < Tp; t += 32) {
-        int lo = 0, hi = E - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (w.tpre[mid] <= 4 * t) lo = mid;
-            else hi = mid - 1;
-        }
-        const long long src = (long long)w.tseg[lo] * QSK_SEG + (4 * t - w.tpre[lo]);
-        cp_async16(&w.rv_s[4 * t], rv + src);
-        cp_async16(&w.ri_s[4 * t], ri + src);
-    }
-    cp_async_wait_all();
+    cp_async_wait_all();   // the copies issued while the run was gathered
     __syncwarp();
     for (int e = lane; e < E; e += 32) {
         const int c = w.tcnt[e], pre = w.tpre[e];
@@ -1336,9 +1324,17 @@ __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, cons
             const bool take = elig && Tp + incl <= REC_CAP && epos < TAB_CAP;
             const unsigned TK = __ballot_sync(FULL, take);
             if (take) {
+                // the segment's records go to the run's buffers right away, so
+                // the copies overlap the rest of the gathering
+                const int dst = Tp + incl - pc;
                 w.tseg[epos] = q;
-                w.tpre[epos] = Tp + incl - pc;
+                w.tpre[epos] = dst;
                 w.tcnt[epos] = c;
+                const long long src = (long long)q * QSK_SEG;
+                for (int k = 0; k < pc; k += 4) {
+                    cp_async16(&w.rv_s[dst + k], rv + src + k);
+                    cp_async16(&w.ri_s[dst + k], ri + src + k);
+                }
             }
             const int hi = TK ? 31 - __clz(TK) : 0;
             const int add = __shfl_sync(FULL, incl, hi);
@@ -1416,7 +1412,9 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
         // the blocks that the first masked stretch of the scan skips
         long long preskip = 0;
         if (A.mt_state) {
-            for (int i = lane; i < 624; i += 32) w.mt[i] = A.mt_state[(long long)b * 624 + i];
+            // 156 16-byte copies (state rows and w.mt are 16-byte aligned)
+            for (int i = lane; i < 156; i += 32) cp_async16(&w.mt[4 * i], A.mt_state + (long long)b * 624 + 4 * i);
+            cp_async_wait_all();
             preskip = A.mt_pre[b];
         } else if (lane == 0) {
             mt_seed(w.mt, s.seed);
