@@ -53,6 +53,17 @@ __device__ __forceinline__ void topk_merge(const float (&a)[K], const float (&b)
     }
 }
 
+template <int KF>
+__device__ __forceinline__ void topk_insert(float (&st)[KF], float x) {
+    // insert x into the descending list st, dropping the smallest
+#pragma unroll
+    for (int s = KF - 1; s >= 0; --s) {
+        float prev = (s > 0) ? st[s > 0 ? s - 1 : 0] : CUDART_INF_F;
+        // new st[s] = max(min(prev, x), st[s])
+        st[s] = fmaxf(st[s], fminf(prev, x));
+    }
+}
+
 // number of valid scan positions < x (x in [0, N])
 __device__ long long valid_prefix(const Geom &g, const int *lo, long long x) {
     long long vd[QSK_MAXD];
@@ -1195,6 +1206,55 @@ __device__ __forceinline__ void replay_chunk_ties(int K, bool tie, int m, unsign
     rp += 2 * nt;
 }
 
+// A few candidates (the lanes of cand, in scan order): the reference's scan
+// step (fKb.hpp) applied to one trigger after the other, warp-uniformly.
+// A trigger v >= K-th draws x among the xes tail slots holding the K-th and
+// swaps it with slot K-1; above the K-th it is inserted after the values
+// >= v (the last slot drops out, cpt restarts at 0 when the K-th was unique
+// and counts on otherwise); equal to the K-th it replaces slot K-1 with
+// probability xes / (xes + cpt + 1) (a second draw) and cpt counts on.
+template <int KM>
+__device__ __forceinline__ void replay_scalar(int K, unsigned cand, float v, int m, float (&cv)[KM],
+                                              unsigned (&cp)[KM], unsigned &cpt, int &rp, const float *buf) {
+    const unsigned FULL = 0xffffffffu;
+    while (cand) {
+        const int l = __ffs(cand) - 1;
+        cand &= cand - 1u;
+        const float xv = __shfl_sync(FULL, v, l);
+        const unsigned xm = (unsigned)__shfl_sync(FULL, m, l);
+        const float kth = sel_f<KM>(cv, K - 1);
+        if (!(xv >= kth)) continue;
+        const bool gt = xv > kth;
+        int xes = 0, q = 0;
+#pragma unroll
+        for (int s = 0; s < KM; ++s) {
+            if (s < K && cv[s] == kth) xes++;
+            if (s < K - 1 && cv[s] >= xv) q++;
+        }
+        int x = K - xes + int(floorf(__fmul_rn(buf[rp], (float)xes)));
+        if (x > K - 1) x = K - 1;
+        const unsigned px = sel_u<KM>(cp, x), pk = sel_u<KM>(cp, K - 1);
+        unsigned sw[KM];
+#pragma unroll
+        for (int s = 0; s < KM; ++s) sw[s] = (s == x) ? pk : ((s == K - 1) ? px : cp[s]);
+        if (gt) {
+#pragma unroll
+            for (int s = 0; s < KM; ++s)
+                if (s < K) cp[s] = s < q ? sw[s] : (s == q ? xm : sw[s > 0 ? s - 1 : 0]);
+            topk_insert<KM>(cv, xv);
+            cpt = (xes == 1) ? 0u : cpt + 1u;
+            rp += 1;
+        } else {
+            const unsigned after = cpt + 1u;
+            const bool write = __fmul_rn(__uint2float_rn(unsigned(xes) + after), buf[rp + 1]) < (float)xes;
+#pragma unroll
+            for (int s = 0; s < KM; ++s) cp[s] = (write && s == K - 1) ? xm : sw[s];
+            cpt = after;
+            rp += 2;
+        }
+    }
+}
+
 __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
@@ -1441,7 +1501,8 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 const bool valid = lane < width && j < cnt;
                 const float v = valid ? rv[base + j] : -CUDART_INF_F;
                 const int m = valid ? ri[base + j] : 0;
-                if (!filling && __ballot_sync(FULL, valid && v >= kth0) == 0) {
+                const unsigned cand = __ballot_sync(FULL, valid && v >= kth0);
+                if (cand == 0u) {
                     r0 += width;
                     continue;
                 }
@@ -1463,6 +1524,8 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 // all K state values equal and nothing above them in the chunk
                 if (!filling && sel_f<KM>(cv, 0) == kth0 && __ballot_sync(FULL, valid && v > kth0) == 0) {
                     replay_chunk_ties<KM>(K, valid && v == kth0, m, cp, cpt, rp, w.buf, lane);
+                } else if (__popc(cand) <= 4) {
+                    replay_scalar<KM>(K, cand, v, m, cv, cp, cpt, rp, w.buf);
                 } else {
                     replay_chunk<KM>(K, valid, v, m, cv, cp, cpt, rp, w.buf, lane);
                 }
@@ -1613,17 +1676,6 @@ __device__ __forceinline__ unsigned bits_range(int a, int b) {
     if (a >= b) return 0u;
     const unsigned hi = b >= 32 ? 0xffffffffu : ((1u << b) - 1u);
     return hi & ~((1u << a) - 1u);
-}
-
-template <int KF>
-__device__ __forceinline__ void topk_insert(float (&st)[KF], float x) {
-    // insert x into the descending list st, dropping the smallest
-#pragma unroll
-    for (int s = KF - 1; s >= 0; --s) {
-        float prev = (s > 0) ? st[s > 0 ? s - 1 : 0] : CUDART_INF_F;
-        // new st[s] = max(min(prev, x), st[s])
-        st[s] = fmaxf(st[s], fminf(prev, x));
-    }
 }
 
 template <int KF>
