@@ -1876,15 +1876,56 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             float y = __shfl_up_sync(0xffffffffu, inc[q], 1);
             st[q] = lane == 0 ? -CUDART_INF_F : y;
         }
+        // Lane 0 has no earlier lane, so its running K-th starts from nothing
+        // and most of its positions would be visited one by one below.  The
+        // warp decides them instead: position p of lane 0 on lane p, and an
+        // exclusive prefix top-K over the lanes gives the K-th before each.
+        float x0v;
+        unsigned rmask0;
+        {
+            const unsigned vm0 = __shfl_sync(0xffffffffu, vm, 0);
+            const unsigned recok0 = __shfl_sync(0xffffffffu, emit_masked ? emask : (emask & vmask), 0);
+            const unsigned cnt = ((__shfl_sync(0xffffffffu, c0, 0) >> lane) & 1u) |
+                                 (((__shfl_sync(0xffffffffu, c1, 0) >> lane) & 1u) << 1) |
+                                 (((__shfl_sync(0xffffffffu, c2, 0) >> lane) & 1u) << 2) |
+                                 (((__shfl_sync(0xffffffffu, c3, 0) >> lane) & 1u) << 3) |
+                                 (((__shfl_sync(0xffffffffu, c4, 0) >> lane) & 1u) << 4) |
+                                 (((__shfl_sync(0xffffffffu, c5, 0) >> lane) & 1u) << 5) |
+                                 (((__shfl_sync(0xffffffffu, c6, 0) >> lane) & 1u) << 6) |
+                                 (((__shfl_sync(0xffffffffu, c7, 0) >> lane) & 1u) << 7);
+            const bool val = (vm0 >> lane) & 1u;
+            x0v = val ? (float)cnt : -CUDART_INF_F;
+            float in0[KF];
+            in0[0] = x0v;
+#pragma unroll
+            for (int q = 1; q < KF; ++q) in0[q] = -CUDART_INF_F;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                float rcv[KF], mrg[KF];
+#pragma unroll
+                for (int q = 0; q < KF; ++q) rcv[q] = __shfl_up_sync(0xffffffffu, in0[q], off);
+                if (lane >= off) {
+                    topk_merge<KF>(in0, rcv, mrg);
+#pragma unroll
+                    for (int q = 0; q < KF; ++q) in0[q] = mrg[q];
+                }
+            }
+            const float y = __shfl_up_sync(0xffffffffu, in0[KF - 1], 1);
+            const float kth = lane == 0 ? -CUDART_INF_F : y;
+            // before K finite values every position that can be a candidate is
+            // a record; afterwards the valid ones not below the K-th
+            const bool rec = kth == -CUDART_INF_F ? ((recok0 >> lane) & 1u) != 0u : (val && x0v >= kth);
+            rmask0 = __ballot_sync(0xffffffffu, rec);
+        }
         // record flags: value not below the K-th best of everything before it
         // (earlier lanes, then earlier positions of this lane)
-        unsigned rmask = 0;
+        unsigned rmask = lane == 0 ? rmask0 : 0u;
         const float T0s = st[KF - 1];
         unsigned eqm = 0u;       // records whose value is tval (no count extraction)
         float tval = 0.f;
-        unsigned from = 0xffffffffu;   // positions decided by the threshold path below
+        unsigned from = lane == 0 ? 0u : 0xffffffffu;   // positions decided by the threshold path below
         float T0 = T0s;
-        if (T0 == -CUDART_INF_F) {
+        if (lane != 0 && T0 == -CUDART_INF_F) {
             // Fewer than K finite values before this lane: every position is a
             // record until K finite values are held (masked ones only when they
             // can be candidates).  Only the valid positions up to that point are
@@ -1957,10 +1998,16 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, 1));
         gmax = fmaxf(gmax, __shfl_xor_sync(0xffffffffu, gmax, 2));
         const long long sub = (long long)sg * 8 + (lane >> 2);
+        // lane 0's records, one per lane (the first ones of its sub-segment)
+        if ((rmask0 >> lane) & 1u) {
+            const long long r0 = (long long)sg * 8 * QSK_SEG + __popc(rmask0 & lanemask_lt());
+            rv[r0] = x0v;
+            ri[r0] = int((long long)sg * 1024 + lane);
+        }
         if (sub < g.nseg) {
             const long long rb = sub * QSK_SEG + excl;
             int o = 0;
-            unsigned rm = rmask;
+            unsigned rm = lane == 0 ? 0u : rmask;
             while (rm) {
                 const int bit = __ffs(rm) - 1;
                 rm &= rm - 1u;
@@ -1978,9 +2025,9 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
 
 // MT19937 state of each slot ahead of its replay (one warp per slot; the
 // host runs it for the next batch while the current one is simulated, as it
-// reads the neighbour lists only): the seeding, and with masked positions
-// not emitted as records
-// the state-only blocks of the replay's first skip.  That skip covers the c
+// reads the neighbour lists only): the seeding and, with masked positions
+// not emitted as records, the state-only blocks of the replay's first
+// skip.  That skip covers the c
 // masked positions before the first record (two draws each); c is at least
 // the number c0 of masked positions before the first valid one, so the
 // blocks that rng_skip regenerates without output for 2*c0 draws,
