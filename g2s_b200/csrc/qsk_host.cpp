@@ -655,6 +655,8 @@ struct qsk_sim {
     DBuf<int> d_rec_idx, d_rec_cnt;
     DBuf<float> d_rec_max;
     DBuf<unsigned> d_mt_state;       // [2][slot][624]: two batches
+    DBuf<Slot> d_sslots;             // bit-sliced path: [2][slot] slots written one batch ahead
+    DBuf<StaticTerm> d_sterms;       // and their terms without values [2][slot][maxterms]
     DBuf<int> d_mt_pre;
     DBuf<int> d_tpl_range, d_node_kernel, d_node_lim, d_node_nv;
     DBuf<unsigned char> d_nb_mask;
@@ -901,11 +903,20 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     // ahead of the simulation on st; buffer p is rewritten only after the
     // replay that read it (ev_used[p]).
     const size_t mt_words = size_t(s->max_slots) * 624;
+    // bit-sliced map: slots and value-free terms also come one batch ahead
+    // (k_mt_prep); the map reads the neighbour values itself, so nothing
+    // runs before it on st
+    const bool bits = s->use_bits && g_map_mode == 0;
+    const size_t st_words = size_t(s->max_slots) * s->maxterms;
     auto launch_rng = [&](size_t j) -> int {
         const int p = int(j & 1);
         CK(cudaStreamWaitEvent(s->st_rng, s->ev_used[p], 0));
-        CK(launch_mt_prep(prep_args(batches[j].first, batches[j].second), s->d_mt_state.p + p * mt_words,
-                          s->d_mt_pre.p + size_t(p) * s->max_slots, s->st_rng));
+        SimPrepArgs pa = prep_args(batches[j].first, batches[j].second);
+        if (bits) {
+            pa.slots = s->d_sslots.p + size_t(p) * s->max_slots;
+            pa.sterms = s->d_sterms.p + p * st_words;
+        }
+        CK(launch_mt_prep(pa, s->d_mt_state.p + p * mt_words, s->d_mt_pre.p + size_t(p) * s->max_slots, s->st_rng));
         CK(cudaEventRecord(s->ev_ready[p], s->st_rng));
         return QSK_OK;
     };
@@ -917,19 +928,27 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
         const int B = batches[j].second, p = int(j & 1);
         if (j + 1 < batches.size() && (rc = launch_rng(j + 1)) != QSK_OK) return rc;
         {
-            const SimPrepArgs pa = prep_args(batches[j].first, B);
+            Slot *slots = bits ? s->d_sslots.p + size_t(p) * s->max_slots : s->d_slots.p;
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            CK(launch_prep_sim(pa, s->st));
+            if (!bits) CK(launch_prep_sim(prep_args(batches[j].first, B), s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            if (s->use_bits && g_map_mode == 0) {
+            if (bits) {
+                // the slots and static terms of this batch come from k_mt_prep
+                CK(cudaStreamWaitEvent(s->st, s->ev_ready[p], 0));
                 BitArgs ba;
                 ba.g = g;
                 ba.planes = s->ti->planes.p;
                 ba.pw = s->ti->pw;
                 ba.ncat = s->ti->ncat.p;
                 ba.catv = s->ti->catv.p;
-                ba.slots = s->d_slots.p;
-                ba.terms = s->d_terms.p;
+                ba.slots = slots;
+                ba.terms = nullptr;
+                ba.sterms = s->d_sterms.p + p * st_words;
+                ba.state = s->d_state.p;
+                ba.init = s->d_init.p;
+                ba.id_image = s->d_id.p;
+                ba.tpl = s->d_tpl.p;
+                ba.no_verbatim = s->no_verbatim;
                 ba.maxterms = s->maxterms;
                 ba.segs_per_cta = map_bits_segs_per_cta(g, B);
                 ba.rec_val = s->d_rec_val.p;
@@ -952,13 +971,13 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
                 CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
             }
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            s->info.launches += 4;
+            s->info.launches += bits ? 3 : 4;
             s->info.map_launches += 1;
             s->info.map_positions += (long long)B * g.N;
             ReplayArgs ra;
             std::memset(&ra, 0, sizeof(ra));
             ra.g = g;
-            ra.slots = s->d_slots.p;
+            ra.slots = slots;
             ra.nslots = B;
             ra.K = s->K;
             ra.rec_val = s->d_rec_val.p;
@@ -1182,7 +1201,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
                          cudaGetErrorString(e)));
     // batch scratch: slots up to a record budget of ~2 GiB
     const Geom &g = s->ti->g;
-    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 8 + sizeof(Term) * s->maxterms;
+    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 8 + sizeof(Term) * s->maxterms +
+                      (s->use_bits ? 2 * (sizeof(StaticTerm) * s->maxterms + sizeof(Slot)) : 0);
     size_t budget = size_t(2) << 30;
     long long ms = (long long)(budget / per_slot);
     ms = std::max<long long>(1, std::min<long long>(ms, std::max<long long>(s->nodes, 1)));
@@ -1191,6 +1211,8 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     if ((e = s->d_slots.alloc(size_t(s->max_slots))) != cudaSuccess ||
         (e = s->d_mt_state.alloc(size_t(2) * s->max_slots * 624)) != cudaSuccess ||
         (e = s->d_mt_pre.alloc(size_t(2) * s->max_slots)) != cudaSuccess ||
+        (s->use_bits && ((e = s->d_sslots.alloc(size_t(2) * s->max_slots)) != cudaSuccess ||
+                         (e = s->d_sterms.alloc(size_t(2) * s->max_slots * s->maxterms)) != cudaSuccess)) ||
         (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess ||
         (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "scratch: %s",

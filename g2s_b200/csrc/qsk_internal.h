@@ -58,6 +58,19 @@ struct Slot {
     int cmask_base;          // missing data: centre-mask layer address minus m
     int K;                   // candidates kept (extendK = ceil(k) of this node)
     int var;                 // -fs: the node's variable (the only one written)
+    // -nV with static terms: neighbour 1's cell and template index, from
+    // which the map derives excl (vtpl < 0: no exclusion)
+    unsigned vcell;
+    int vtpl;
+};
+
+// A simulation term whose value is read when the map runs: the layer offset
+// (as Term::base) and where the neighbour's value lives (src >= 0: the grid
+// state at src, src < 0: the initial grid at -src - 1).  A NaN value there
+// contributes nothing (the reference leaves it out of the pattern).
+struct StaticTerm {
+    int base;
+    int src;
 };
 
 enum SlotFlags : int {
@@ -115,6 +128,7 @@ struct SimPrepArgs {
     const float *node_k;
     int full;                       // -fs: path entries are cell values, neighbours carry nb_mask
     const unsigned char *nb_mask;
+    StaticTerm *sterms = nullptr;   // k_mt_prep: slots + static terms of the batch (null: none)
 };
 
 struct MapArgs {
@@ -151,6 +165,14 @@ struct BitArgs {
     int *rec_idx;
     int *rec_cnt;
     float *rec_max;
+    // simulation with static terms (null sterms: the terms above are used):
+    // values from state / init, -nV exclusion from the index image
+    const StaticTerm *sterms = nullptr;
+    const float *state = nullptr;
+    const float *init = nullptr;
+    const unsigned *id_image = nullptr;
+    const int *tpl = nullptr;           // template offsets (ntpl x nd)
+    int no_verbatim = 0;
 };
 
 struct ReplayArgs {

@@ -470,6 +470,32 @@ __device__ NodeGeom node_geometry(const SimPrepArgs &A, int i, unsigned cell, in
     return r;
 }
 
+// -nV: scan index of the TI cell that continues neighbour 1's source (cell
+// id_src, template offset tpl1) (simulation.hpp:556-583,
+// quantileSamplingModule.hpp:518-523), or -1 outside the scan
+__device__ int verbatim_excl(const Geom &g, const int *tpl1, unsigned id_src, const int *mn) {
+    const int nd = g.nd;
+    unsigned src = id_src;
+    long long pf = 0, st = 1;
+    for (int d = 0; d < nd; ++d) {
+        int dim = g.src[d];
+        int c = int(src % (unsigned)dim) - tpl1[d];
+        src /= (unsigned)dim;
+        c = ((c % dim) + dim) % dim;
+        pf += (long long)c * st;
+        st *= dim;
+    }
+    // cvtPositionToIndex (CPUThreadDevice.cpp:270-284), unsigned arithmetic
+    unsigned position = (unsigned)pf, index = 0, div = 1;
+    for (int d = nd - 1; d >= 0; --d) div *= (unsigned)g.src[d];
+    for (int d = nd - 1; d >= 0; --d) {
+        unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
+        div /= sr;
+        index = index * f + (f - (position / div + (unsigned)mn[d]) % sr - 1u);
+    }
+    return index < (unsigned)g.N ? int(index) : -1;
+}
+
 __global__ void k_prep_sim(SimPrepArgs A) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -585,30 +611,13 @@ __global__ void k_prep_sim(SimPrepArgs A) {
         }
         if (A.no_verbatim && cnt > 1 && !A.full) {
             // the TI cell continuing neighbour 1's source is excluded
-            // (simulation.hpp:556-583, quantileSamplingModule.hpp:518-523)
             const int t1 = A.nb_tpl[(long long)i * A.n + 1];
             const unsigned c1 = A.nb_cell[(long long)i * A.n + 1];
-            unsigned src = A.id_image[c1];
-            long long pf = 0, st = 1;
-            for (int d = 0; d < nd; ++d) {
-                int dim = A.g.src[d];
-                int c = int(src % (unsigned)dim) - A.tpl[t1 * nd + d];
-                src /= (unsigned)dim;
-                c = ((c % dim) + dim) % dim;
-                pf += (long long)c * st;
-                st *= dim;
-            }
-            // cvtPositionToIndex (CPUThreadDevice.cpp:270-284), unsigned arithmetic
-            unsigned position = (unsigned)pf, index = 0, div = 1;
-            for (int d = nd - 1; d >= 0; --d) div *= (unsigned)A.g.src[d];
-            for (int d = nd - 1; d >= 0; --d) {
-                unsigned f = (unsigned)A.g.fft[d], sr = (unsigned)A.g.src[d];
-                div /= sr;
-                index = index * f + (f - (position / div + (unsigned)mn[d]) % sr - 1u);
-            }
-            s.excl = index < (unsigned)A.g.N ? int(index) : -1;
+            s.excl = verbatim_excl(A.g, A.tpl + t1 * nd, A.id_image[c1], mn);
         }
     }
+    s.vcell = 0;
+    s.vtpl = -1;
     if (lane == 0) A.slots[warp] = s;
 }
 
@@ -1287,6 +1296,7 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
     const int j0 = min(Tp, lane * P);
     const int j1 = min(Tp, j0 + P);
     unsigned long long tmask = 0ull;
+#pragma unroll 4
     for (int j = j0; j < j1; ++j) tmask |= (unsigned long long)(w.rv_s[j] == V) << (j - j0);
     const int mine = __popcll(tmask);
     int incl = mine;
@@ -1690,23 +1700,38 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
     const Geom &g = A.g;
     {
         // terms -> (plane offset, flat offset), one thread per term; a code that
-        // is no category of the TI reads the all-zero plane QSK_CMAX
+        // is no category of the TI (or a NaN value) reads the all-zero plane QSK_CMAX
         const Term *src = A.terms + (long long)b * A.maxterms;
+        const StaticTerm *ssrc = A.sterms ? A.sterms + (long long)b * A.maxterms : nullptr;
         const int N32 = (int)g.N;
         for (int t = threadIdx.x; t < ss.nterms; t += blockDim.x) {
-            const Term tm = src[t];
-            const int base = tm.base;   // v*N - d with 0 <= d < N
+            int base;
+            float val;
+            if (ssrc) {
+                const StaticTerm st = ssrc[t];
+                base = st.base;
+                val = st.src >= 0 ? A.state[st.src] : A.init[-(long long)st.src - 1];
+            } else {
+                const Term tm = src[t];
+                base = tm.base;
+                val = tm.b;
+            }
+            // base = v*N - d with 0 <= d < N
             const int v = base > 0 ? (base + N32 - 1) / N32 : 0;
             const int d = v * N32 - base;
             int c = QSK_CMAX;
             const int nc = A.ncat[v];
             for (int q = 0; q < nc; ++q)
-                if (A.catv[v * QSK_CMAX + q] == tm.b) { c = q; break; }
+                if (A.catv[v * QSK_CMAX + q] == val) { c = q; break; }
             // positions 32k..32k+31 read source bits from word k + floor(-d/32),
             // shifted right by (-d) mod 32
             bterm[t] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw + plane_guard(g.N) + ((-d) >> 5), (-d) & 31);
         }
-        if (threadIdx.x == 0) nbt = ss.nterms;
+        if (threadIdx.x == 0) {
+            nbt = ss.nterms;
+            if (ssrc && A.no_verbatim && ss.vtpl >= 0)
+                ss.excl = verbatim_excl(g, A.tpl + ss.vtpl * g.nd, A.id_image[ss.vcell], ss.mn);
+        }
     }
     __syncthreads();
     const int nt = nbt;
@@ -2023,6 +2048,88 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
     }
 }
 
+// The slot of path node i and its terms without their values (bit-sliced
+// simulations: unit weights, categorical variables, complete TI): everything
+// k_prep_sim derives from the neighbour lists, computed one batch ahead.
+// The map reads the values (and derives the -nV exclusion) when it runs.
+__device__ void write_static_slot(const SimPrepArgs &A, int b, int i, unsigned pv, unsigned cell, const NodeGeom &ng,
+                                  int lane) {
+    const int cnt = A.nb_count[i];
+    const int nd = A.g.nd;
+    Slot s;
+    s.node = i;
+    s.cell = cell;
+    s.var = A.full ? int(pv % unsigned(A.nvar)) : 0;
+    s.seed = A.seeds[i];
+    s.K = ng.Ki;
+    s.sel = selected_index(s.seed, ng.lk, A.nti);
+    if (s.sel < 0) s.sel = 0;
+    if (s.sel > ng.Ki - 1) s.sel = ng.Ki - 1;
+    s.flags = 0;
+    s.nterms = 0;
+    s.excl = -1;
+    s.cmask_base = 0;
+    s.vcell = 0;
+    s.vtpl = -1;
+#pragma unroll
+    for (int d = 0; d < QSK_MAXD; ++d) {
+        s.mn[d] = ng.mn[d];
+        s.lo[d] = ng.lo[d];
+    }
+    if (ng.skip) {
+        s.flags |= SLOT_SKIP;
+    } else {
+        if (ng.nvalid < ng.Ki) s.flags |= SLOT_EMIT_MASKED;
+        int base_out = 0;
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            const int j = j0 + lane;
+            StaticTerm tl[4];
+            int nt = 0;
+            if (j < cnt) {
+                const int t = A.nb_tpl[(long long)i * A.n + j];
+                const unsigned nc = A.nb_cell[(long long)i * A.n + j];
+                long long d_flat = 0;
+                for (int d = 0; d < nd; ++d) d_flat += (long long)(A.tpl[t * nd + d] - ng.mn[d]) * A.g.sstride[d];
+                for (int v = 0; v < A.nvar && v < 4; ++v) {
+                    if (A.full) {
+                        if (!((A.nb_mask[(long long)i * A.n + j] >> v) & 1u)) continue;
+                    } else if (A.node_nv && j >= A.node_nv[(long long)i * A.nvar + v]) {
+                        continue;
+                    }
+                    if (A.wtab[t * A.nvar + v] == 0.f) continue;
+                    const long long sidx = (long long)nc * A.nvar + v;
+                    StaticTerm st;
+                    st.base = int((long long)v * A.g.N - d_flat);
+                    st.src = (nc == cell && !A.full) ? int(-sidx - 1) : int(sidx);
+                    tl[nt++] = st;
+                }
+            }
+            int incl = nt;
+            for (int off = 1; off < 32; off <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += y;
+            }
+            const int excl = incl - nt;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int q = 0; q < nt; ++q) {
+                const int o = base_out + excl + q;
+                if (o < A.maxterms) A.sterms[(long long)b * A.maxterms + o] = tl[q];
+            }
+            base_out += total;
+        }
+        if (base_out > A.maxterms) {
+            if (lane == 0) atomicExch(A.status, DEV_TOO_MANY_TERMS);
+            base_out = A.maxterms;
+        }
+        s.nterms = base_out;
+        if (A.no_verbatim && cnt > 1 && !A.full) {
+            s.vtpl = A.nb_tpl[(long long)i * A.n + 1];
+            s.vcell = A.nb_cell[(long long)i * A.n + 1];
+        }
+    }
+    if (lane == 0) A.slots[b] = s;
+}
+
 // MT19937 state of each slot ahead of its replay (one warp per slot; the
 // host runs it for the next batch while the current one is simulated, as it
 // reads the neighbour lists only): the seeding and, with masked positions
@@ -2043,6 +2150,7 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_mt_prep(SimPrepArgs A, unsign
     const unsigned pv = A.path[A.begin + i];
     const unsigned cell = A.full ? pv / unsigned(A.nvar) : pv;
     const NodeGeom ng = node_geometry(A, i, cell, lane);
+    if (A.sterms) write_static_slot(A, b, i, pv, cell, ng, lane);
     if (ng.skip) return;
     if (lane == 0) mt_seed(mt[wib], A.seeds[i]);
     __syncwarp();
