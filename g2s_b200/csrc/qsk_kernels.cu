@@ -74,11 +74,13 @@ __device__ long long valid_prefix(const Geom &g, const int *lo, long long x) {
         acc *= (w > 0 ? w : 0);
     }
     if (x >= g.N) return acc;
+    // scan indices are below 2^31 (int record indices): 32-bit digits
     long long count = 0;
+    const unsigned ux = (unsigned)x;
     for (int d = g.nd - 1; d >= 0; --d) {
-        long long digit = (x / g.sstride[d]) % g.fft[d];
-        long long t = digit - lo[d];
-        if (t > 0) count += t * vd[d];
+        const int digit = int((ux / (unsigned)g.sstride[d]) % (unsigned)g.fft[d]);
+        const int t = digit - lo[d];
+        if (t > 0) count += (long long)t * vd[d];
         if (digit < lo[d]) break;
     }
     return count;
@@ -1296,6 +1298,7 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
     const int j0 = min(Tp, lane * P);
     const int j1 = min(Tp, j0 + P);
     unsigned long long tmask = 0ull;
+#pragma unroll 4
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) tmask |= (unsigned long long)(w.rv_s[j] == V) << (j - j0);
     const int mine = __popcll(tmask);
