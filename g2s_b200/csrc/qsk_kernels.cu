@@ -1755,14 +1755,19 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             // the 32 positions lie in at most two rows of the x dimension
             const long long rem = g.N - m0;
             emask = rem >= 32 ? 0xffffffffu : ((1u << rem) - 1u);
-            const int X = g.fft[0];
-            const long long r0 = m0 / X;
-            const int x0 = int(m0 - r0 * X);
-            auto row_ok = [&](long long r) {
+            // scan indices are below 2^31: 32-bit digits (row r holds digits 1..)
+            const unsigned X = (unsigned)g.fft[0];
+            const unsigned r0 = (unsigned)m0 / X;
+            const int x0 = int((unsigned)m0 - r0 * X);
+            auto row_ok = [&](unsigned r) {
                 bool ok = true;
 #pragma unroll
                 for (int d = 1; d < QSK_MAXD; ++d)
-                    if (d < g.nd) ok &= int((r / (g.sstride[d] / X)) % g.fft[d]) >= ss.lo[d];
+                    if (d < g.nd) {
+                        const unsigned f = (unsigned)g.fft[d];
+                        ok &= int(r % f) >= ss.lo[d];
+                        r /= f;
+                    }
                 return ok;
             };
             auto range = [](int a, int b) -> unsigned {   // bits [a, b), 0 <= a, b <= 32
@@ -1779,7 +1784,8 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             // narrow x dimension: incremental digits
             int dig[QSK_MAXD];
 #pragma unroll
-            for (int d = 0; d < QSK_MAXD; ++d) dig[d] = d < g.nd ? int((m0 / g.sstride[d]) % g.fft[d]) : 0;
+            for (int d = 0; d < QSK_MAXD; ++d)
+                dig[d] = d < g.nd ? int(((unsigned)m0 / (unsigned)g.sstride[d]) % (unsigned)g.fft[d]) : 0;
             bool rowok = true;
 #pragma unroll
             for (int d = 1; d < QSK_MAXD; ++d)
