@@ -47,6 +47,15 @@ class QskPatternOpts(ctypes.Structure):
     _fields_ = [("exclude_index", ctypes.c_int), ("missing_data", ctypes.c_int), ("centre_mask_layer", ctypes.c_int)]
 
 
+class QskCalibParams(ctypes.Structure):
+    _fields_ = [("ndim", ctypes.c_int), ("ti_dims", _u32p), ("nvar", ctypes.c_int), ("types", _i32p),
+                ("ti", _f32p), ("n_kernels", ctypes.c_int), ("kernel_dims", _u32p), ("kernel_nvar", _i32p),
+                ("kernels", ctypes.POINTER(_f32p)), ("n_configs", ctypes.c_int), ("n_counts", ctypes.c_int),
+                ("counts", _u32p), ("n_densities", ctypes.c_int), ("densities", _f32p), ("max_k", ctypes.c_uint),
+                ("power", ctypes.c_float), ("noise", ctypes.c_float), ("max_iterations", ctypes.c_uint),
+                ("min_iterations", ctypes.c_uint), ("max_seconds", ctypes.c_float), ("seed", ctypes.c_uint)]
+
+
 class QskSimInfo(ctypes.Structure):
     _fields_ = [("nodes", ctypes.c_longlong), ("levels", ctypes.c_int), ("max_batch", ctypes.c_int),
                 ("template_size", ctypes.c_int), ("ms_setup_neighbours", ctypes.c_float),
@@ -74,6 +83,11 @@ SIGNATURES = {
                                             ctypes.POINTER(QskPatternOpts), _f32p, _u32p, _i32p]),
     "qsk_pattern_kbest_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p,
                                                ctypes.POINTER(QskTerm), ctypes.c_uint, _f32p, _f32p, _u32p, _i32p]),
+    "qsk_pattern_kbest_batch_verbatim": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _i32p, _i32p, _i32p,
+                                                        ctypes.POINTER(QskTerm), ctypes.c_uint, _f32p, _u32p, _f32p,
+                                                        _f32p, _u32p, _i32p]),
+    "qsk_calibrate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskCalibParams), _f32p, _f32p, _u32p,
+                                     ctypes.POINTER(ctypes.c_longlong)]),
     "qsk_pattern_kbest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
                                                  ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float, _f32p, _u32p,
                                                  _i32p]),
@@ -252,6 +266,38 @@ class Worker:
                    "qsk_pattern_kbest_ex")
         return sc, ix, mn
 
+    def pattern_kbest_verbatim(self, patterns, k: int, seeds, origins, radii=None):
+        """Batched queries with the verbatim exclusion of distribution():
+        patterns is a list of (offsets (n, ndim), terms); origins the TI cell
+        each pattern came from (0xffffffff: none); radii the exclusion radius
+        (< 1: the cell's index only).  Returns (scores[B,k], scan_indices[B,k],
+        min_offsets[B,ndim])."""
+        nd = self.ti.ndim
+        B = len(patterns)
+        nb_ptr = np.zeros(B + 1, np.int32)
+        term_ptr = np.zeros(B + 1, np.int32)
+        offs, tl = [], []
+        for b, (o, terms) in enumerate(patterns):
+            o = np.asarray(o, np.int32).reshape(-1, nd)
+            offs.append(o)
+            nb_ptr[b + 1] = nb_ptr[b] + o.shape[0]
+            tl.extend(terms)
+            term_ptr[b + 1] = term_ptr[b] + len(terms)
+        offs = np.ascontiguousarray(np.concatenate(offs) if offs else np.zeros((0, nd), np.int32), np.int32)
+        tarr = (QskTerm * max(len(tl), 1))(*[QskTerm(int(t[0]), int(t[1]), int(t[2]), float(t[3]), float(t[4]))
+                                            for t in tl])
+        sd = np.ascontiguousarray(seeds, np.float32)
+        org = np.ascontiguousarray(origins, np.uint32)
+        rad = None if radii is None else np.ascontiguousarray(radii, np.float32)
+        sc = np.zeros((B, k), np.float32)
+        ix = np.zeros((B, k), np.uint32)
+        mn = np.zeros((B, nd), np.int32)
+        _check(lib().qsk_pattern_kbest_batch_verbatim(self.handle, B, _p(nb_ptr, _i32p), _p(offs, _i32p),
+                                                      _p(term_ptr, _i32p), tarr, k, _p(sd, _f32p), _p(org, _u32p),
+                                                      _p(rad, _f32p), _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)),
+               "qsk_pattern_kbest_batch_verbatim")
+        return sc, ix, mn
+
     def close(self):
         if getattr(self, "handle", None):
             lib().qsk_worker_destroy(self.handle)
@@ -397,6 +443,63 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     finally:
         sim.close()
     return out, idx
+
+
+def default_neighbour_counts(max_n) -> np.ndarray:
+    """auto_qs' configurations without -nl: for i in 1..max_n[0]-1 the counts
+    i * max_n[j] / max_n[0] in unsigned integer arithmetic (the round() there
+    applies to an integer quotient; G2S src/auto_qs.cpp:650-661)."""
+    mx = [int(m) for m in np.atleast_1d(max_n)]
+    rows = [[(i * mx[j]) // mx[0] for j in range(len(mx))] for i in range(1, mx[0])]
+    return np.array(rows, np.uint32).reshape(-1, len(mx))
+
+
+def calibrate(ti: np.ndarray, types: Sequence[int], kernels, counts=None, densities=None, max_k: int = 1,
+              power: float = 2.0, noise: float = 0.0, max_iterations: int = 25000, min_iterations: int = 1000,
+              max_seconds: float = float("inf"), seed: int = 0, device: int = 0, max_n=80):
+    """auto_qs calibration (G2S src/auto_qs.cpp) on the GPU.  kernels: list of
+    weight kernels (numpy spatial shape [+ (nvar,)]); counts: (n_configs,
+    n_counts) neighbours per variable (default: auto_qs' list for max_n);
+    densities: default auto_qs' 7 values.  Returns (mean_error, deviation,
+    sample_count, searches) with the arrays shaped (n_densities, n_kernels,
+    n_configs, max_k)."""
+    nvar = len(types)
+    t = np.ascontiguousarray(ti, dtype=np.float32)
+    tdims = _grid_dims(t, nvar)
+    nd = len(tdims)
+    if counts is None:
+        counts = default_neighbour_counts(max_n)
+    cnt = np.ascontiguousarray(np.atleast_2d(np.asarray(counts, np.uint32)))
+    if densities is None:
+        densities = [0.0078, 0.0156, 0.0312, 0.0625, 0.1250, 0.2500, 0.5000]
+    den = np.ascontiguousarray(densities, np.float32)
+    karr, kd, knv = [], [], []
+    for k in kernels:
+        kk = np.ascontiguousarray(k, dtype=np.float32)
+        if kk.ndim == nd + 1:
+            knv.append(kk.shape[-1])
+            kd.extend(reversed(kk.shape[:-1]))
+        else:
+            knv.append(1)
+            kd.extend(reversed(kk.shape))
+        karr.append(kk)
+    kd = np.ascontiguousarray(kd, np.uint32)
+    knv = np.ascontiguousarray(knv, np.int32)
+    kptrs = (_f32p * len(karr))(*[_p(k, _f32p) for k in karr])
+    ty = np.ascontiguousarray(types, np.int32)
+    p = QskCalibParams(nd, _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), len(karr), _p(kd, _u32p),
+                       _p(knv, _i32p), kptrs, cnt.shape[0], cnt.shape[1], _p(cnt, _u32p), den.size, _p(den, _f32p),
+                       int(max_k), float(power), float(noise), int(max_iterations), int(min_iterations),
+                       float(max_seconds), int(seed))
+    S = cnt.shape[0] * len(karr) * den.size
+    mean = np.zeros(S * max_k, np.float32)
+    dev = np.zeros(S * max_k, np.float32)
+    ns = np.zeros(S * max_k, np.uint32)
+    nsearch = ctypes.c_longlong(0)
+    _check(lib().qsk_calibrate(device, ctypes.byref(p), _p(mean, _f32p), _p(dev, _f32p), _p(ns, _u32p),
+                               ctypes.byref(nsearch)), "qsk_calibrate")
+    shape = (den.size, len(karr), cnt.shape[0], max_k)
+    return mean.reshape(shape), dev.reshape(shape), ns.reshape(shape), int(nsearch.value)
 
 
 def read_bgrid(path: str):

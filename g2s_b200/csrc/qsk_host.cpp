@@ -12,6 +12,7 @@
 #include <limits>
 #include <mutex>
 #include <numeric>
+#include <chrono>
 #include <random>
 #include <string>
 #include <vector>
@@ -185,6 +186,9 @@ struct qsk_worker {
     DBuf<float> rec_max;
     DBuf<float> out_val;
     DBuf<unsigned> out_pos;
+    DBuf<int> xcenter;        // verbatim exclusion with a radius: scan index per pattern
+    DBuf<float> xradius;
+    DBuf<unsigned> xmask;     // [pattern][ceil(N/32)] excluded positions
     std::vector<Slot> h_slots;
     std::vector<Term> h_terms;
 };
@@ -466,7 +470,8 @@ int qsk_worker_destroy(qsk_worker *w) {
 
 static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
                               const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
-                              unsigned *out_index, int *out_min, const qsk_pattern_opts *opts) {
+                              unsigned *out_index, int *out_min, const qsk_pattern_opts *opts,
+                              const unsigned *origin = nullptr, const float *radius = nullptr) {
     if (!w || B < 0 || !nb_ptr || !term_ptr || !seeds || !out_score || !out_index) return fail(QSK_ERR_ARG, "null argument");
     if (k < 1 || k > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "k=%u outside [1,%d]", k, QSK_KMAX);
     if (B == 0) return QSK_OK;
@@ -488,6 +493,29 @@ static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int
         if (rc) return rc;
         std::copy(tmp.begin(), tmp.end(), w->h_terms.begin() + size_t(b) * maxterms);
     }
+    // verbatim exclusion of each pattern's origin (the TI cell the pattern was
+    // taken from): one scan index, or every index within the radius
+    std::vector<int> xc;
+    std::vector<float> xr;
+    bool any_radius = false;
+    if (origin) {
+        xc.assign(B, -1);
+        xr.assign(B, 0.f);
+        for (int b = 0; b < B; ++b) {
+            Slot &sl = w->h_slots[b];
+            if (origin[b] == 0xffffffffu || (sl.flags & SLOT_SKIP)) continue;
+            if ((long long)origin[b] >= ti->cells) return fail(QSK_ERR_ARG, "origin %u of pattern %d outside the TI", origin[b], b);
+            const unsigned idx = qsk_position_to_index(ti, sl.mn, origin[b]);
+            const float rad = radius ? radius[b] : 0.f;
+            if (rad >= 1.f) {
+                xc[b] = int(idx);
+                xr[b] = rad;
+                any_radius = true;
+            } else if ((long long)idx < g.N) {
+                sl.excl = int(idx);
+            }
+        }
+    }
     if (smem_configured_device != ti->device) {
         CK(set_map_smem_limit(200 * 1024));
         smem_configured_device = ti->device;
@@ -498,7 +526,9 @@ static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int
     CK(ensure_records(g, B, w->rec_val, w->rec_idx, w->rec_cnt, w->rec_max));
     CK(w->out_val.ensure(size_t(B) * k));
     CK(w->out_pos.ensure(size_t(B) * k));
-    bool bits = ti->planes_ok && g_map_mode == 0 && maxterms <= 255 && !opts;
+    // the radius masks are applied by the FP32 kernel (the bit-sliced one gives
+    // the same scores, so the choice changes no result)
+    bool bits = ti->planes_ok && g_map_mode == 0 && maxterms <= 255 && !opts && !any_radius;
     for (size_t i = 0; i < w->h_terms.size() && bits; ++i) {
         int b = int(i / maxterms), t = int(i % maxterms);
         if (t >= w->h_slots[b].nterms) continue;
@@ -532,6 +562,15 @@ static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int
         ma.rec_idx = w->rec_idx.p;
         ma.rec_cnt = w->rec_cnt.p;
         ma.rec_max = w->rec_max.p;
+        if (any_radius) {
+            const long long xwords = (g.N + 31) / 32;
+            CK(w->xcenter.upload(xc.data(), size_t(B), w->st));
+            CK(w->xradius.upload(xr.data(), size_t(B), w->st));
+            CK(w->xmask.ensure(size_t(B) * size_t(xwords)));
+            CK(launch_radius_mask(w->xcenter.p, w->xradius.p, B, g, w->xmask.p, xwords, w->st));
+            ma.xmask = w->xmask.p;
+            ma.xwords = xwords;
+        }
         CK(launch_map_records(ma, B, int(k), maxterms, w->st));
     }
     ReplayArgs ra;
@@ -564,6 +603,14 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
                             const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
                             unsigned *out_index, int *out_min) {
     return pattern_batch_impl(w, B, nb_ptr, offsets, term_ptr, terms, k, seeds, out_score, out_index, out_min, nullptr);
+}
+
+int qsk_pattern_kbest_batch_verbatim(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                                     const qsk_term *terms, unsigned k, const float *seeds, const unsigned *origin,
+                                     const float *radius, float *out_score, unsigned *out_index, int *out_min) {
+    if (!origin) return fail(QSK_ERR_ARG, "null origin");
+    return pattern_batch_impl(w, B, nb_ptr, offsets, term_ptr, terms, k, seeds, out_score, out_index, out_min, nullptr,
+                              origin, radius);
 }
 
 int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
@@ -1616,6 +1663,265 @@ int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, 
     CK(cudaMemcpyAsync(out_index, out_pos, sizeof(unsigned) * k, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return QSK_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// f3: auto_qs calibration (G2S include/calibration.hpp:30-284, src/auto_qs.cpp:
+// 640-700) on the batched engine.  Setup s = (neighbour configuration, kernel,
+// density), configurations fastest, draws its samples from its own
+// std::mt19937(seed + s).  Every iteration tests all setups against the
+// statistics as they stood when it began, searches the samples of the unpruned
+// ones in one batched query (verbatim exclusion of the sample's own cell with
+// the reference's radius), then accumulates their errors and updates the best
+// mean error per density in setup order.  The reference draws from one
+// generator per OpenMP thread (seeded from the clock) and tests each setup
+// after the updates of the setups before it in the same iteration; its
+// results depend on the thread schedule and the clock, so the order here is
+// this engine's (the oracle restates the same order).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct CalibSample {
+    unsigned cell = 0;
+    std::vector<int> offs;
+    std::vector<float> vals;
+    float seed = 0.f;
+    bool search = false;
+};
+
+// the sample of one setup (include/calibration.hpp:113-224 up to the search)
+CalibSample calib_draw(const qsk_calib_params *p, const std::vector<int> &tpl, int ntpl, const unsigned *nn, int ncounts,
+                       float density, std::mt19937 &gen) {
+    std::uniform_real_distribution<float> U(0.f, 1.f);
+    const int nd = p->ndim, nvar = p->nvar;
+    CalibSample S;
+    unsigned cells = 1;
+    for (int d = 0; d < nd; ++d) cells *= p->ti_dims[d];
+    (void)int(std::floor(U(gen) * 1.f));   // TI index (one TI)
+    S.cell = unsigned(std::floor(U(gen) * float(cells * unsigned(nvar)) / float(unsigned(nvar))));
+    int c0[QSK_MAXD];
+    unsigned rest = S.cell;
+    for (int d = 0; d < nd; ++d) {
+        c0[d] = int(rest % p->ti_dims[d]);
+        rest /= p->ti_dims[d];
+    }
+    std::vector<unsigned> per(size_t(nvar), 0u);
+    int ps = 0;
+    while ((ncounts > 1 || S.offs.size() / size_t(nd) < nn[0]) && ps < ntpl) {
+        bool take = U(gen) < density;
+        long long dataIndex = 0;
+        if (take) {
+            long long stride = 1;
+            for (int d = 0; d < nd; ++d) {
+                const int c = c0[d] + tpl[size_t(ps) * nd + d];
+                if (c < 0 || c >= int(p->ti_dims[d])) take = false;
+                dataIndex += (long long)c * stride;
+                stride *= p->ti_dims[d];
+            }
+        }
+        if (take) {
+            unsigned cpt = 0;
+            for (int v = 0; v < nvar; ++v) {
+                if (per[v] < nn[v % ncounts]) {
+                    S.vals.push_back(p->ti[size_t(dataIndex) * nvar + v]);
+                    cpt++;
+                    per[v]++;
+                } else {
+                    S.vals.push_back(NAN);
+                }
+            }
+            for (int d = 0; d < nd; ++d) S.offs.push_back(tpl[size_t(ps) * nd + d]);
+            if (cpt == 0) break;
+        }
+        ps++;
+    }
+    if (ps >= ntpl) return S;
+    const size_t n = S.offs.size() / size_t(nd);
+    if (n > 1 && p->noise > 0.f) {
+        float fraction = p->noise / float(n) / 2.f;
+        if (p->noise < 1.0f) fraction = p->noise / 2.f;
+        for (size_t j = 0; j < n; ++j)
+            if (U(gen) < fraction) {
+                const size_t a = size_t(std::floor(U(gen) * float(n)));
+                const size_t b = size_t(std::floor(U(gen) * float(n)));
+                for (int d = 0; d < nd; ++d) std::swap(S.offs[a * nd + d], S.offs[b * nd + d]);
+            }
+    }
+    if (n > 1) {
+        S.seed = U(gen);
+        S.search = true;
+    }
+    return S;
+}
+
+// kernel weight of offset o for variable v, centred at dims/2 (0 outside)
+float calib_weight(int nd, const unsigned *kd, int knvar, const float *k, const int *o, int v) {
+    long long f = 0, stride = 1;
+    for (int d = 0; d < nd; ++d) {
+        const int c = int(kd[d] / 2) + o[d];
+        if (c < 0 || c >= int(kd[d])) return 0.f;
+        f += (long long)c * stride;
+        stride *= kd[d];
+    }
+    return k[size_t(f) * knvar + (v % knvar)];
+}
+
+}  // namespace
+
+extern "C" {
+
+int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, float *dev_error, unsigned *n_samples,
+                  long long *n_searches) {
+    if (!p || !p->ti_dims || !p->types || !p->ti || !p->kernel_dims || !p->kernels || !p->counts || !p->densities ||
+        !mean_error || !dev_error || !n_samples)
+        return fail(QSK_ERR_ARG, "null argument");
+    if (p->ndim < 1 || p->ndim > QSK_MAXD || p->nvar < 1 || p->n_kernels < 1 || p->n_configs < 1 || p->n_counts < 1 ||
+        p->n_densities < 1 || !(p->power > 0.f))
+        return fail(QSK_ERR_ARG, "invalid calibration parameters");
+    if (p->max_k < 1 || p->max_k > QSK_KMAX) return fail(QSK_ERR_UNSUPPORTED, "max_k=%u outside [1,%d]", p->max_k, QSK_KMAX);
+    for (int i = 0; i < p->n_kernels; ++i)
+        if (!p->kernels[i] || !p->kernel_nvar || p->kernel_nvar[i] < 1)
+            return fail(QSK_ERR_ARG, "kernel %d missing", i);
+    const int nd = p->ndim, nvar = p->nvar;
+    size_t cells = 1;
+    for (int d = 0; d < nd; ++d) cells *= p->ti_dims[d];
+    for (size_t i = 0; i < cells * size_t(nvar); ++i)
+        if (std::isnan(p->ti[i]))
+            return fail(QSK_ERR_UNSUPPORTED, "calibration with missing training-image values is not implemented");
+    // pathPosition: the box of kernel 0, nearest first (src/auto_qs.cpp:452-492)
+    std::vector<int> tpl;
+    std::vector<float> wtab_unused;
+    int ntpl = make_template(nd, 1, p->kernel_dims, nullptr, tpl, wtab_unused);
+    if (ntpl <= 0) return fail(QSK_ERR_ARG, "empty template");
+    // exclusion radius of the sample's own cell (include/calibration.hpp:33)
+    const float radius = float(std::pow(double(unsigned(cells) * unsigned(nvar) / unsigned(nvar)) * 0.005,
+                                        1.f / float(nd)));
+    qsk_ti *ti = nullptr;
+    int rc = qsk_ti_create_grid(device, nd, p->ti_dims, nvar, p->types, p->ti, &ti);
+    if (rc) return rc;
+    qsk_worker *w = nullptr;
+    if ((rc = qsk_worker_create(ti, &w)) != QSK_OK) {
+        qsk_ti_destroy(ti);
+        return rc;
+    }
+    const size_t setups = size_t(p->n_configs) * p->n_kernels * p->n_densities;
+    const size_t K = p->max_k;
+    std::vector<double> cum(setups * K, 0.0), cum2(setups * K, 0.0);
+    std::vector<uint16_t> ns(setups * K, 0);
+    std::vector<float> best(p->n_densities, INFINITY), devBest(p->n_densities, 0.f);
+    std::vector<std::mt19937> gens;
+    gens.reserve(setups);
+    for (size_t s = 0; s < setups; ++s) gens.emplace_back(p->seed + unsigned(s));
+    std::vector<size_t> koff(p->n_kernels);
+    const float nbSigmas = 1.f / p->power;
+    std::vector<CalibSample> samples(setups);
+    std::vector<float> before(setups);
+    std::vector<int> nb_ptr, offs, term_ptr, mins;
+    std::vector<qsk_term> terms;
+    std::vector<float> seeds, radii, scores;
+    std::vector<unsigned> origins, index, which;
+    long long searches = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned it = 0; it < p->max_iterations && rc == QSK_OK; ++it) {
+        nb_ptr.assign(1, 0);
+        term_ptr.assign(1, 0);
+        offs.clear();
+        terms.clear();
+        seeds.clear();
+        radii.clear();
+        origins.clear();
+        which.clear();
+        for (size_t s = 0; s < setups; ++s) {
+            samples[s].search = false;
+            const size_t ni = s % p->n_configs, ki = (s / p->n_configs) % p->n_kernels,
+                         di = s / (size_t(p->n_configs) * p->n_kernels);
+            const float eb = float(cum[s * K] / ns[s * K]);
+            const float db = float(std::sqrt(cum2[s * K] / ns[s * K] - eb * eb));
+            before[s] = eb;
+            if (ns[s * K] > p->min_iterations && (eb - nbSigmas * db) > (best[di] + nbSigmas * devBest[di])) continue;
+            samples[s] = calib_draw(p, tpl, ntpl, p->counts + ni * p->n_counts, p->n_counts, p->densities[di], gens[s]);
+            const CalibSample &S = samples[s];
+            if (!S.search) continue;
+            // the sample's pattern as terms (the simulation's conversion)
+            const unsigned *kd = p->kernel_dims + ki * nd;
+            const int n = int(S.offs.size() / size_t(nd));
+            for (int j = 0; j < n; ++j) {
+                for (int v = 0; v < nvar; ++v) {
+                    const float val = S.vals[size_t(j) * nvar + v];
+                    if (std::isnan(val)) continue;
+                    const float wgt = calib_weight(nd, kd, p->kernel_nvar[ki], p->kernels[ki], &S.offs[size_t(j) * nd], v);
+                    if (wgt == 0.f) continue;
+                    qsk_term t;
+                    t.neighbour = j;
+                    t.layer = v;
+                    if (p->types[v] == 0) {
+                        t.op = QSK_OP_SQLIN;
+                        t.a = -wgt;
+                        t.b = 2.f * (wgt * val);
+                    } else {
+                        t.op = QSK_OP_EQ;
+                        t.a = wgt;
+                        t.b = val;
+                    }
+                    terms.push_back(t);
+                }
+            }
+            offs.insert(offs.end(), S.offs.begin(), S.offs.end());
+            nb_ptr.push_back(int(offs.size() / size_t(nd)));
+            term_ptr.push_back(int(terms.size()));
+            seeds.push_back(S.seed);
+            origins.push_back(S.cell);
+            radii.push_back(radius);
+            which.push_back(unsigned(s));
+        }
+        const int B = int(which.size());
+        if (B > 0) {
+            scores.resize(size_t(B) * K);
+            index.resize(size_t(B) * K);
+            mins.resize(size_t(B) * nd);
+            rc = pattern_batch_impl(w, B, nb_ptr.data(), offs.data(), term_ptr.data(), terms.data(), unsigned(K),
+                                    seeds.data(), scores.data(), index.data(), mins.data(), nullptr, origins.data(),
+                                    radii.data());
+            if (rc != QSK_OK) break;
+            searches += B;
+        }
+        for (int b = 0; b < B; ++b) {
+            const size_t s = which[b];
+            const size_t di = s / (size_t(p->n_configs) * p->n_kernels);
+            const CalibSample &S = samples[s];
+            for (size_t i = 0; i < K; ++i) {
+                const unsigned pos = qsk_index_to_position(ti, &mins[size_t(b) * nd], index[size_t(b) * K + i]);
+                // the reference reads _data[index] of the raw array (one value per
+                // cell for single-variable TIs)
+                const double e = double(std::pow(std::fabs(p->ti[pos] - p->ti[S.cell]), p->power));
+                cum[s * K + i] += e;
+                cum2[s * K + i] += e * e;
+                ns[s * K + i]++;
+            }
+            const float ea = float(cum[s * K] / ns[s * K]);
+            if (before[s] > ea && best[di] > ea) {
+                best[di] = ea;
+                devBest[di] = float(std::sqrt(cum2[s * K] / ns[s * K] - ea * ea));
+            }
+        }
+        if (p->max_seconds > 0.f && std::isfinite(p->max_seconds) &&
+            std::chrono::duration_cast<std::chrono::seconds>(std::chrono::steady_clock::now() - t0).count() > p->max_seconds)
+            break;
+    }
+    if (rc == QSK_OK) {
+        for (size_t i = 0; i < setups * K; ++i) {
+            const float m = float(cum[i] / ns[i]);
+            mean_error[i] = std::pow(m, 1.f / p->power);
+            dev_error[i] = float(std::pow(cum2[i] / ns[i] - m * m, 0.5 / double(p->power)));
+            n_samples[i] = ns[i];
+        }
+        if (n_searches) *n_searches = searches;
+    }
+    qsk_worker_destroy(w);
+    qsk_ti_destroy(ti);
+    return rc;
 }
 
 }  // extern "C"

@@ -142,6 +142,10 @@ struct MapArgs {
     int *rec_idx;
     int *rec_cnt;     // [slot][nseg]
     float *rec_max;   // [slot][nseg] largest valid score of the segment
+    // verbatim exclusion with a radius: bit m of slot b's mask
+    // (xmask[b * xwords + m / 32]) forces valid position m to -inf; null: none
+    const unsigned *xmask = nullptr;
+    long long xwords = 0;
 };
 
 // Bit-plane layout: every plane is `plane_words(N)` words, of which the
@@ -251,6 +255,9 @@ cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, co
 int map_bits_segs_per_cta(const Geom &g, int nslots);
 cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
+// exclusion masks: slot b's positions around scan index center[b] (radius[b] >= 1)
+cudaError_t launch_radius_mask(const int *center, const float *radius, int nslots, const Geom &g, unsigned *mask,
+                               long long xwords, cudaStream_t st);
 cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cudaStream_t st);
 
 }  // namespace qsk

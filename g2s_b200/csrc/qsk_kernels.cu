@@ -738,6 +738,14 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
             for (int r = 0; r < 4; ++r)
                 if ((int)(base + 32 * r + lane) == ss.excl && valid[r]) acc[r] = -CUDART_INF_F;
         }
+        if (A.xmask) {
+            const unsigned *xm = A.xmask + (long long)b * A.xwords;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const unsigned m = base + 32 * r + lane;
+                if (exists[r] && valid[r] && ((xm[m >> 5] >> (m & 31)) & 1u)) acc[r] = -CUDART_INF_F;
+            }
+        }
         // warp prefix top-KF over the segment in scan order; records are the
         // positions not below the K-th best of everything before them in the
         // segment (a superset of the global triggers).
@@ -2177,6 +2185,54 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_mt_prep(SimPrepArgs A, unsign
     if (lane == 0) pre[b] = 624 * blocks;
 }
 
+// Verbatim exclusion with a radius (CPUThreadDevice::setValueInErrorArrayWithRadius,
+// G2S src/CPUThreadDevice.cpp:310-342): from the scan index c, level L = nd..2
+// steps i_L in [-r, r] with r = ceil(sqrt(R2 - d2)) by fft[L-1] (d2 the sum of
+// the squares of the outer steps, a level entered only while d2 <= R2), and
+// level 1 steps by fft[0], marking (c + offset + N) mod N in 32-bit unsigned
+// arithmetic as the reference does.  One CTA per slot: the outer steps are a
+// box [-R, R]^(nd-1) enumerated by the threads, each thread runs the level-1
+// loop of its tuples.
+__global__ void k_radius_mask(const int *__restrict__ center, const float *__restrict__ radius, Geom g,
+                              unsigned *__restrict__ mask, long long xwords) {
+    const int b = blockIdx.x;
+    unsigned *xm = mask + (long long)b * xwords;
+    for (long long q = threadIdx.x; q < xwords; q += blockDim.x) xm[q] = 0u;
+    __syncthreads();
+    const int c = center[b];
+    const float rad = radius[b];
+    if (c < 0 || !(rad >= 1.f)) return;
+    const float R2 = rad * rad;
+    const int R = int(ceil(sqrt((double)R2)));
+    const unsigned s = (unsigned)g.N;
+    const int nouter = g.nd - 1;
+    long long box = 1;
+    for (int L = 0; L < nouter; ++L) box *= 2 * R + 1;
+    for (long long t = threadIdx.x; t < box; t += blockDim.x) {
+        // outer tuple (i_nd, ..., i_2), outermost first
+        long long rest = t;
+        unsigned pos = (unsigned)c;
+        unsigned d2 = 0;
+        bool ok = true;
+        for (int L = g.nd; L >= 2 && ok; --L) {
+            const int i = int(rest % (2 * R + 1)) - R;
+            rest /= (2 * R + 1);
+            // level L is entered with d2 <= R2 and runs i in [-r, r]
+            if (!((float)d2 <= R2)) { ok = false; break; }
+            const int r = int(ceil(sqrt((double)(R2 - (float)d2))));
+            if (i < -r || i > r) { ok = false; break; }
+            pos += (unsigned)(i * (int)g.fft[L - 1]);
+            d2 += (unsigned)(i * i);
+        }
+        if (!ok || !((float)d2 <= R2)) continue;
+        const int r1 = int(ceil(sqrt((double)(R2 - (float)d2))));
+        for (int i = -r1; i <= r1; ++i) {
+            const unsigned m = (pos + (unsigned)(i * (int)g.fft[0]) + s) % s;
+            atomicOr(xm + (m >> 5), 1u << (m & 31));
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers (called by the host engine)
 // ---------------------------------------------------------------------------
@@ -2307,6 +2363,13 @@ cudaError_t set_map_smem_limit(int bytes) {
     e = cudaFuncSetAttribute(k_map_records<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_map_records<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_radius_mask(const int *center, const float *radius, int nslots, const Geom &g, unsigned *mask,
+                               long long xwords, cudaStream_t st) {
+    if (nslots <= 0) return cudaSuccess;
+    k_radius_mask<<<(unsigned)nslots, 256, 0, st>>>(center, radius, g, mask, xwords);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cudaStream_t st) {

@@ -130,6 +130,65 @@ int qsk_pattern_kbest_batch(qsk_worker *w, int B, const int *nb_ptr, const int *
                             const qsk_term *terms, unsigned k, const float *seeds, float *out_score,
                             unsigned *out_index, int *out_min);
 
+/* Batched form with the verbatim exclusion of QuantileSamplingModule::
+ * distribution (G2S include/quantileSamplingModule.hpp:128-175,518-523,
+ * 566-571): pattern b was taken from TI cell origin[b] (0xffffffff: none);
+ * with radius[b] < 1 the scan index of that cell is excluded
+ * (setValueInErrorArray), otherwise every index that
+ * CPUThreadDevice::setValueInErrorArrayWithRadius marks around it
+ * (src/CPUThreadDevice.cpp:310-342).  radius may be null (all < 1).  The
+ * auto_qs calibration queries its samples this way (include/calibration.hpp:
+ * 221-224). */
+int qsk_pattern_kbest_batch_verbatim(qsk_worker *w, int B, const int *nb_ptr, const int *offsets, const int *term_ptr,
+                                     const qsk_term *terms, unsigned k, const float *seeds, const unsigned *origin,
+                                     const float *radius, float *out_score, unsigned *out_index, int *out_min);
+
+/* auto_qs calibration (G2S src/auto_qs.cpp:640-700, include/calibration.hpp:
+ * 30-284) on the batched engine: for every setup (neighbour configuration,
+ * kernel, density) samples are drawn from the TI itself (a random cell, its
+ * template neighbours kept with probability `density`, optional position
+ * noise), searched with the verbatim exclusion of the cell's own
+ * neighbourhood (radius (cells*0.005)^(1/ndim)), and the error
+ * |TI[match] - TI[cell]|^power of each of the max_k candidates is
+ * accumulated; setups whose mean error is worse than the density's best by
+ * more than 1/power deviations (after min_iterations samples) stop drawing.
+ *   counts        [n_configs][n_counts] neighbours per variable (v % n_counts)
+ *   kernels       n_kernels weight kernels (kernel_dims: n_kernels*ndim, x
+ *                 first; kernel_nvar[i] weights per cell)
+ * Outputs (n_densities*n_kernels*n_configs*max_k, configurations fastest and
+ * candidate rank innermost, the reference's im_1/im_2/im_3 images): mean
+ * error^(1/power), deviation^(0.5/power), 16-bit sample counts.  Each setup
+ * draws from std::mt19937(seed + setup); one iteration tests all setups on
+ * the statistics it began with, searches the unpruned samples in one batch,
+ * then accumulates in setup order (the reference's OpenMP order depends on
+ * the thread schedule; its seed on the clock).  Complete TIs only. */
+typedef struct {
+    int ndim;
+    const unsigned *ti_dims;
+    int nvar;
+    const int *types;
+    const float *ti;
+    int n_kernels;
+    const unsigned *kernel_dims;
+    const int *kernel_nvar;
+    const float *const *kernels;
+    int n_configs;
+    int n_counts;
+    const unsigned *counts;
+    int n_densities;
+    const float *densities;
+    unsigned max_k;
+    float power;
+    float noise;
+    unsigned max_iterations;
+    unsigned min_iterations;
+    float max_seconds;
+    unsigned seed;
+} qsk_calib_params;
+
+int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, float *dev_error, unsigned *n_samples,
+                  long long *n_searches);
+
 /* qsk_pattern_kbest without any allocation.  No counterpart in the reference
  * (G2S' devices allocate their buffers when they are created).
  *

@@ -1042,3 +1042,276 @@ long orc_pattern_map(int nd, const unsigned *ti_dims, int nvar, const int *types
 }
 
 }  /* extern "C" */
+
+/* ------------------------------------------------------------------ */
+/* f3: auto_qs calibration                                             */
+/* ------------------------------------------------------------------ */
+namespace {
+
+/* scan indices marked by CPUThreadDevice::setValueInErrorArrayWithRadius
+ * (src/CPUThreadDevice.cpp:310-342): level L > 1 steps i in [-r, r],
+ * r = ceil(sqrt(R2 - d2)), by fft[L-1]; level 1 steps by fft[0] and marks
+ * (pos + i*fft[0] + N) % N; unsigned 32-bit arithmetic throughout. */
+void radius_marks(const Scan &sc, unsigned pos, float R2, int level, unsigned d2, std::vector<unsigned> &out) {
+    if (!(float(d2) <= R2)) return;
+    const int r = int(std::ceil(std::sqrt(double(R2 - float(d2)))));
+    const unsigned s = unsigned(sc.N);
+    for (int i = -r; i <= r; ++i) {
+        if (level == 1) out.push_back((pos + unsigned(i * int(sc.fft[0])) + s) % s);
+        else radius_marks(sc, pos + unsigned(i * int(sc.fft[level - 1])), R2, level - 1, d2 + unsigned(i * i), out);
+    }
+}
+
+/* QuantileSamplingModule::distribution for one TI on the CPU device
+ * (include/quantileSamplingModule.hpp:128-175,342-600): the weighted map, the
+ * verbatim exclusion of the origin (one index, or the radius marks), the
+ * k-biggest with reservoir ties, the stable order by score, TI positions. */
+struct Dist {
+    std::vector<float> score;
+    std::vector<unsigned> index, position;
+    int mn[8];
+};
+
+Dist distribution(const Grid &g, const int *types, const float *ti, const Grid &kg, const float *kernel, int nnb,
+                  const int *offs, const float *vals, unsigned k, float seed, unsigned origin, float radius,
+                  std::vector<float> *map_out = nullptr, std::vector<double> *m64 = nullptr,
+                  std::vector<double> *scale = nullptr) {
+    Node node = build_node(g, types, kg, kernel, nnb, offs, vals);
+    Scan sc = make_scan(g, node);
+    std::vector<float> m(size_t(sc.N));
+    map_fp32(g, ti, node, sc, m.data());
+    if (origin != UINT_MAX) {
+        const unsigned idx = position_to_index(sc, g, node, origin);
+        if (radius < 1.f) {
+            if (idx < unsigned(sc.N)) m[idx] = -INFINITY;
+        } else {
+            std::vector<unsigned> marks;
+            radius_marks(sc, idx, radius * radius, sc.nd, 0, marks);
+            for (unsigned q : marks) m[q] = -INFINITY;
+        }
+    }
+    Dist d;
+    d.score.resize(k);
+    d.index.resize(k);
+    kbiggest(m.data(), unsigned(sc.N), (unsigned short)k, seed, d.score.data(), d.index.data());
+    d.position.resize(k);
+    for (unsigned i = 0; i < k; ++i) d.position[i] = index_to_position(sc, g, node, d.index[i]);
+    for (int i = 0; i < g.nd; ++i) d.mn[i] = node.mn[i];
+    if (map_out) *map_out = m;
+    if (m64) {
+        m64->resize(size_t(sc.N));
+        scale->resize(size_t(sc.N));
+        map_fp64(g, ti, node, sc, m64->data(), scale->data());
+    }
+    return d;
+}
+
+}  /* namespace */
+
+extern "C" {
+
+/* One distribution() query: TI (x fastest, variables interleaved), weight
+ * kernel (kdims, knvar variables), nnb neighbour offsets and values (NaN:
+ * left out), k candidates, seed, origin TI cell (0xffffffff: none) and
+ * exclusion radius.  Outputs k scores, scan indices, TI positions and the
+ * pattern minimum; map32 (N floats, after the exclusion) and map64/scale
+ * (N doubles) when not null.  Returns N. */
+long orc_distribution(int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti,
+                      const unsigned *kdims, int knvar, const float *kernel, int nnb, const int *offs,
+                      const float *vals, unsigned k, float seed, unsigned origin, float radius, float *out_score,
+                      unsigned *out_index, unsigned *out_position, int *out_min, float *map32, double *map64,
+                      double *scale) {
+    Grid g, kg;
+    g.nd = kg.nd = nd;
+    g.nvar = nvar;
+    kg.nvar = knvar;
+    for (int d = 0; d < nd; ++d) {
+        g.dims[d] = ti_dims[d];
+        kg.dims[d] = kdims[d];
+    }
+    std::vector<float> m32;
+    std::vector<double> m64, sc;
+    Dist r = distribution(g, types, ti, kg, kernel, nnb, offs, vals, k, seed, origin, radius, map32 ? &m32 : nullptr,
+                          map64 ? &m64 : nullptr, map64 ? &sc : nullptr);
+    for (unsigned i = 0; i < k; ++i) {
+        out_score[i] = r.score[i];
+        out_index[i] = r.index[i];
+        out_position[i] = r.position[i];
+    }
+    for (int d = 0; d < nd; ++d) out_min[d] = r.mn[d];
+    if (map32) std::copy(m32.begin(), m32.end(), map32);
+    if (map64) {
+        std::copy(m64.begin(), m64.end(), map64);
+        if (scale) std::copy(sc.begin(), sc.end(), scale);
+    }
+    long N = 1;
+    for (int d = 0; d < nd; ++d) N *= long(ti_dims[d]);
+    return N;
+}
+
+}  /* extern "C" */
+
+namespace {
+
+/* One calibration sample of setup (neighbour counts nn, density), drawn from
+ * the setup's generator: the body of the reference's loop in
+ * include/calibration.hpp:113-224 up to the distribution() call. */
+struct Sample {
+    unsigned cell = 0;
+    std::vector<int> offs;
+    std::vector<float> vals;
+    float seed = 0.f;
+    bool search = false;
+};
+
+Sample draw_sample(const Grid &g, const float *ti, const std::vector<std::vector<int>> &tpl,
+                   const std::vector<unsigned> &nn, float density, float noise, std::mt19937 &gen) {
+    std::uniform_real_distribution<float> U(0.f, 1.f);
+    Sample S;
+    (void)int(std::floor(U(gen) * 1.f));   /* TI index: one TI */
+    const unsigned dataSize = unsigned(g.cells()) * unsigned(g.nvar);
+    S.cell = unsigned(std::floor(U(gen) * float(dataSize) / float(unsigned(g.nvar))));
+    std::vector<unsigned> per(g.nvar, 0);
+    size_t P = tpl.size(), ps = 0;
+    int c0[8];
+    coords(g, long(S.cell), c0);
+    while ((nn.size() > 1 || S.offs.size() / size_t(g.nd) < nn[0]) && ps < P) {
+        bool take = U(gen) < density;
+        long dataIndex = 0;
+        if (take) {
+            int c[8];
+            for (int d = 0; d < g.nd; ++d) {
+                c[d] = c0[d] + tpl[ps][d];
+                if (c[d] < 0 || c[d] >= int(g.dims[d])) take = false;
+            }
+            if (take) dataIndex = flat(g, c);
+        }
+        if (take) {
+            unsigned cpt = 0;
+            for (int v = 0; v < g.nvar; ++v) {
+                if (per[v] < nn[v % nn.size()]) {
+                    S.vals.push_back(ti[size_t(dataIndex) * g.nvar + v]);
+                    cpt++;
+                    per[v]++;
+                } else {
+                    S.vals.push_back(NAN);
+                }
+            }
+            for (int d = 0; d < g.nd; ++d) S.offs.push_back(tpl[ps][d]);
+            if (cpt == 0) break;
+        }
+        ps++;
+    }
+    if (ps >= P) return S;   /* not enough neighbours: no search */
+    const size_t n = S.offs.size() / size_t(g.nd);
+    if (n > 1 && noise > 0.f) {
+        float fraction = noise / float(n) / 2.f;
+        if (noise < 1.0f) fraction = noise / 2.f;
+        for (size_t j = 0; j < n; ++j)
+            if (U(gen) < fraction) {
+                /* the two indices of iter_swap; a swap is symmetric, so their
+                 * order of evaluation does not matter */
+                const size_t a = size_t(std::floor(U(gen) * float(n)));
+                const size_t b = size_t(std::floor(U(gen) * float(n)));
+                for (int d = 0; d < g.nd; ++d) std::swap(S.offs[a * g.nd + d], S.offs[b * g.nd + d]);
+            }
+    }
+    if (n > 1) {
+        S.seed = U(gen);
+        S.search = true;
+    }
+    return S;
+}
+
+}  /* namespace */
+
+extern "C" {
+
+/* auto_qs calibration (include/calibration.hpp:30-284, src/auto_qs.cpp:640-
+ * 700), restated with the batched order of this project's GPU driver:
+ * setup s = (neighbour configuration, kernel, density), x fastest, draws
+ * from its own std::mt19937(seed + s); in every iteration the pruning test of
+ * all setups uses the statistics as they stood when the iteration began, the
+ * samples of all unpruned setups are searched, and their errors are then
+ * accumulated (and the best mean error per density updated) in setup order.
+ * Outputs per setup and candidate rank (max_k of them): mean error^(1/p),
+ * deviation^(0.5/p) and the 16-bit sample count.  Returns the number of
+ * searches. */
+long orc_calibrate(int nd, const unsigned *ti_dims, int nvar, const int *types, const float *ti, int n_kernels,
+                   const unsigned *kdims, const int *knvar, const float *kernels, int n_configs, int n_counts,
+                   const unsigned *counts, int n_densities, const float *densities, unsigned max_k, float power,
+                   float noise, unsigned max_iter, unsigned min_iter, unsigned seed, float *mean, float *dev,
+                   unsigned *nsamp) {
+    Grid g;
+    g.nd = nd;
+    g.nvar = nvar;
+    for (int d = 0; d < nd; ++d) g.dims[d] = ti_dims[d];
+    std::vector<Grid> kg(n_kernels);
+    std::vector<const float *> kp(n_kernels);
+    size_t koff = 0;
+    for (int i = 0; i < n_kernels; ++i) {
+        kg[i].nd = nd;
+        kg[i].nvar = knvar[i];
+        for (int d = 0; d < nd; ++d) kg[i].dims[d] = kdims[i * nd + d];
+        kp[i] = kernels + koff;
+        koff += kg[i].cells() * size_t(knvar[i]);
+    }
+    /* pathPosition: the box of kernel 0 nearest first (src/auto_qs.cpp:452-492) */
+    const auto tpl = make_template(nd, kdims, nullptr, 1);
+    const float radius = float(std::pow(double(unsigned(g.cells()) * unsigned(nvar) / unsigned(nvar)) * 0.005,
+                                        1.f / float(nd)));
+    const size_t setups = size_t(n_configs) * n_kernels * n_densities;
+    const size_t K = max_k;
+    std::vector<double> cum(setups * K, 0.0), cum2(setups * K, 0.0);
+    std::vector<uint16_t> ns(setups * K, 0);
+    std::vector<float> best(n_densities, INFINITY), devBest(n_densities, 0.f);
+    std::vector<std::mt19937> gens;
+    gens.reserve(setups);
+    for (size_t s = 0; s < setups; ++s) gens.emplace_back(seed + unsigned(s));
+    const float nbSigmas = 1.f / power;
+    long searches = 0;
+    std::vector<Sample> samples(setups);
+    std::vector<float> before(setups);
+    for (unsigned it = 0; it < max_iter; ++it) {
+        for (size_t s = 0; s < setups; ++s) {
+            samples[s].search = false;
+            const size_t ni = s % n_configs, ki = (s / n_configs) % n_kernels, di = s / (size_t(n_configs) * n_kernels);
+            (void)ki;
+            const float eb = float(cum[s * K] / ns[s * K]);
+            const float db = float(std::sqrt(cum2[s * K] / ns[s * K] - eb * eb));
+            before[s] = eb;
+            if (ns[s * K] > min_iter && (eb - nbSigmas * db) > (best[di] + nbSigmas * devBest[di])) continue;
+            std::vector<unsigned> nn(counts + ni * n_counts, counts + (ni + 1) * n_counts);
+            samples[s] = draw_sample(g, ti, tpl, nn, densities[di], noise, gens[s]);
+        }
+        for (size_t s = 0; s < setups; ++s) {
+            const Sample &S = samples[s];
+            if (!S.search) continue;
+            const size_t ki = (s / n_configs) % n_kernels, di = s / (size_t(n_configs) * n_kernels);
+            const int n = int(S.offs.size() / size_t(nd));
+            Dist r = distribution(g, types, ti, kg[ki], kp[ki], n, S.offs.data(), S.vals.data(), max_k, S.seed, S.cell,
+                                  radius);
+            searches++;
+            for (size_t i = 0; i < K; ++i) {
+                const double e = double(std::pow(std::fabs(ti[r.position[i]] - ti[S.cell]), power));
+                cum[s * K + i] += e;
+                cum2[s * K + i] += e * e;
+                ns[s * K + i]++;
+            }
+            const float ea = float(cum[s * K] / ns[s * K]);
+            if (before[s] > ea && best[di] > ea) {
+                best[di] = ea;
+                devBest[di] = float(std::sqrt(cum2[s * K] / ns[s * K] - ea * ea));
+            }
+        }
+    }
+    for (size_t i = 0; i < setups * K; ++i) {
+        const float m = float(cum[i] / ns[i]);
+        mean[i] = std::pow(m, 1.f / power);
+        dev[i] = float(std::pow(cum2[i] / ns[i] - m * m, 0.5 / double(power)));
+        nsamp[i] = ns[i];
+    }
+    return searches;
+}
+
+}  /* extern "C" */

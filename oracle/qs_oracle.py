@@ -228,3 +228,90 @@ def pattern_map(ti, types, offsets, values):
                           _p(offs, _i32p), _p(vals, _f32p), _p(m32, _f32p), _p(m64, _f64p), _p(sc, _f64p),
                           _p(mn, _i32p), _p(mx, _i32p))
     return m32, m64, sc, mn, mx
+
+
+def _kernel_arrays(kernel, nd, nvar):
+    """(kdims x-first uint32, knvar, float32 data) of a weight kernel given as
+    a numpy array of spatial shape (.., ny, nx) [+ (nvar,) when it has one
+    weight per variable]."""
+    k = np.ascontiguousarray(kernel, dtype=np.float32)
+    if k.ndim == nd + 1:
+        knvar = k.shape[-1]
+        spatial = k.shape[:-1]
+    else:
+        knvar = 1
+        spatial = k.shape
+    return np.array(list(reversed(spatial)), np.uint32), knvar, k
+
+
+def distribution(ti, types, kernel, offsets, values, k, seed, origin=0xFFFFFFFF, radius=0.0, maps=False):
+    """QuantileSamplingModule::distribution on one TI (auto_qs' per-sample search):
+    returns (scores, scan indices, TI positions, pattern min) and, with maps=True,
+    (map32 after the exclusion, map64, scale)."""
+    nvar = len(types)
+    tdims = grid_dims(ti, nvar)
+    nd = len(tdims)
+    t = np.ascontiguousarray(ti, dtype=np.float32)
+    ty = np.asarray(types, dtype=np.int32)
+    kd, knvar, kk = _kernel_arrays(kernel, nd, nvar)
+    offs = np.ascontiguousarray(offsets, dtype=np.int32)
+    vals = np.ascontiguousarray(values, dtype=np.float32)
+    sc = np.zeros(k, np.float32)
+    ix = np.zeros(k, np.uint32)
+    pos = np.zeros(k, np.uint32)
+    mn = np.zeros(nd, np.int32)
+    N = int(np.prod(tdims))
+    m32 = np.zeros(N, np.float32) if maps else None
+    m64 = np.zeros(N, np.float64) if maps else None
+    scl = np.zeros(N, np.float64) if maps else None
+    L = lib()
+    L.orc_distribution.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, _u32p, ctypes.c_int, _f32p,
+                                   ctypes.c_int, _i32p, _f32p, ctypes.c_uint, ctypes.c_float, ctypes.c_uint,
+                                   ctypes.c_float, _f32p, _u32p, _u32p, _i32p, _f32p, _f64p, _f64p]
+    L.orc_distribution.restype = ctypes.c_long
+    L.orc_distribution(nd, _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), _p(kd, _u32p), knvar, _p(kk, _f32p),
+                       offs.shape[0], _p(offs, _i32p), _p(vals, _f32p), k, seed, int(origin), float(radius),
+                       _p(sc, _f32p), _p(ix, _u32p), _p(pos, _u32p), _p(mn, _i32p),
+                       _p(m32, _f32p) if maps else None, _p(m64, _f64p) if maps else None,
+                       _p(scl, _f64p) if maps else None)
+    if maps:
+        return sc, ix, pos, mn, m32, m64, scl
+    return sc, ix, pos, mn
+
+
+def calibrate(ti, types, kernels, counts, densities, max_k=1, power=2.0, noise=0.0, max_iter=10, min_iter=1000,
+              seed=0):
+    """The auto_qs calibration loop (batched setup order, per-setup generators);
+    returns (mean, dev, nsamp) shaped (n_densities, n_kernels, n_configs, max_k)
+    and the number of searches."""
+    nvar = len(types)
+    tdims = grid_dims(ti, nvar)
+    nd = len(tdims)
+    t = np.ascontiguousarray(ti, dtype=np.float32)
+    ty = np.asarray(types, dtype=np.int32)
+    kds, knv, kdata = [], [], []
+    for kern in kernels:
+        kd, knvar, kk = _kernel_arrays(kern, nd, nvar)
+        kds.append(kd)
+        knv.append(knvar)
+        kdata.append(kk.ravel())
+    kds = np.ascontiguousarray(np.concatenate(kds), np.uint32)
+    knv = np.asarray(knv, np.int32)
+    kdata = np.ascontiguousarray(np.concatenate(kdata), np.float32)
+    cnt = np.ascontiguousarray(np.atleast_2d(np.asarray(counts, np.uint32)))
+    den = np.ascontiguousarray(densities, np.float32)
+    S = cnt.shape[0] * len(kernels) * den.size
+    mean = np.zeros(S * max_k, np.float32)
+    dev = np.zeros(S * max_k, np.float32)
+    ns = np.zeros(S * max_k, np.uint32)
+    L = lib()
+    L.orc_calibrate.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, ctypes.c_int, _u32p, _i32p, _f32p,
+                                ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int, _f32p, ctypes.c_uint, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, _f32p, _f32p, _u32p]
+    L.orc_calibrate.restype = ctypes.c_long
+    n = L.orc_calibrate(nd, _p(tdims, _u32p), nvar, _p(ty, _i32p), _p(t, _f32p), len(kernels), _p(kds, _u32p),
+                        _p(knv, _i32p), _p(kdata, _f32p), cnt.shape[0], cnt.shape[1], _p(cnt, _u32p), den.size,
+                        _p(den, _f32p), max_k, power, noise, max_iter, min_iter, seed, _p(mean, _f32p),
+                        _p(dev, _f32p), _p(ns, _u32p))
+    shape = (den.size, len(kernels), cnt.shape[0], max_k)
+    return mean.reshape(shape), dev.reshape(shape), ns.reshape(shape), n

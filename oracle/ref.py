@@ -110,3 +110,34 @@ def run_qs(ti: np.ndarray, di: np.ndarray, types, args, job_id: int = 4242, tag:
             except OSError:
                 pass
     return sim, idx, ms, text
+
+
+def distribution(ti, types, kernel, offsets, values, k, seed, origin, radius):
+    """The reference's QuantileSamplingModule::distribution (auto_qs' per-sample
+    search) on a CPU device: the k TI positions it returns."""
+    nvar = len(types)
+    a = np.ascontiguousarray(ti, dtype=np.float32)
+    spatial = a.shape if nvar == 1 else a.shape[:-1]
+    nd = len(spatial)
+    dims = np.array(list(reversed(spatial)), np.uint32)
+    kk = np.ascontiguousarray(kernel, dtype=np.float32)
+    if kk.ndim == nd + 1:
+        knvar, kspatial = kk.shape[-1], kk.shape[:-1]
+    else:
+        knvar, kspatial = 1, kk.shape
+    kdims = np.array(list(reversed(kspatial)), np.uint32)
+    ty = np.asarray(types, np.int32)
+    offs = np.ascontiguousarray(offsets, np.int32)
+    vals = np.ascontiguousarray(values, np.float32)
+    out = np.zeros(k, np.uint32)
+    L = lib()
+    u32 = ctypes.POINTER(ctypes.c_uint)
+    i32 = ctypes.POINTER(ctypes.c_int)
+    f32 = ctypes.POINTER(ctypes.c_float)
+    L.g2sref_distribution.argtypes = [ctypes.c_int, u32, ctypes.c_int, i32, f32, u32, ctypes.c_int, f32, ctypes.c_int,
+                                      i32, f32, ctypes.c_uint, ctypes.c_float, ctypes.c_uint, ctypes.c_float, u32]
+    L.g2sref_distribution(nd, dims.ctypes.data_as(u32), nvar, ty.ctypes.data_as(i32), a.ctypes.data_as(f32),
+                          kdims.ctypes.data_as(u32), knvar, kk.ctypes.data_as(f32), offs.shape[0],
+                          offs.ctypes.data_as(i32), vals.ctypes.data_as(f32), k, seed, int(origin), float(radius),
+                          out.ctypes.data_as(u32))
+    return out
