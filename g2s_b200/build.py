@@ -63,6 +63,10 @@ def build_cli() -> str:
     build_lib()
     _run([HOSTCXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), os.path.join(PKG, "cli", "qs_b200.cpp"),
           "-o", CLI, "-L", PKG, "-lg2s_b200", "-Wl,-rpath,$ORIGIN"])
+    # auto_qs_b200: the G2S `auto_qs` calibration command line
+    _run([HOSTCXX, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+          os.path.join(PKG, "cli", "auto_qs_b200.cpp"), "-o", os.path.join(PKG, "auto_qs_b200"), "-L", PKG,
+          "-lg2s_b200", "-Wl,-rpath,$ORIGIN"])
     return CLI
 
 

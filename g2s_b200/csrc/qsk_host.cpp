@@ -14,6 +14,7 @@
 #include <numeric>
 #include <chrono>
 #include <random>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1824,17 +1825,14 @@ int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, floa
     std::vector<unsigned> origins, index, which;
     long long searches = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    for (unsigned it = 0; it < p->max_iterations && rc == QSK_OK; ++it) {
-        nb_ptr.assign(1, 0);
-        term_ptr.assign(1, 0);
-        offs.clear();
-        terms.clear();
-        seeds.clear();
-        radii.clear();
-        origins.clear();
-        which.clear();
-        for (size_t s = 0; s < setups; ++s) {
+    // samples are drawn on host threads (each setup owns its generator, so the
+    // draws do not depend on the thread count), then gathered in setup order
+    std::vector<std::vector<qsk_term>> sterms(setups);
+    const unsigned nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    auto draw_range = [&](size_t s0, size_t s1) {
+        for (size_t s = s0; s < s1; ++s) {
             samples[s].search = false;
+            sterms[s].clear();
             const size_t ni = s % p->n_configs, ki = (s / p->n_configs) % p->n_kernels,
                          di = s / (size_t(p->n_configs) * p->n_kernels);
             const float eb = float(cum[s * K] / ns[s * K]);
@@ -1865,9 +1863,35 @@ int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, floa
                         t.a = wgt;
                         t.b = val;
                     }
-                    terms.push_back(t);
+                    sterms[s].push_back(t);
                 }
             }
+        }
+    };
+    for (unsigned it = 0; it < p->max_iterations && rc == QSK_OK; ++it) {
+        nb_ptr.assign(1, 0);
+        term_ptr.assign(1, 0);
+        offs.clear();
+        terms.clear();
+        seeds.clear();
+        radii.clear();
+        origins.clear();
+        which.clear();
+        if (nthreads > 1 && setups >= 64) {
+            std::vector<std::thread> pool;
+            const size_t chunk = (setups + nthreads - 1) / nthreads;
+            for (unsigned t = 0; t < nthreads; ++t) {
+                const size_t s0 = size_t(t) * chunk, s1 = std::min(setups, s0 + chunk);
+                if (s0 < s1) pool.emplace_back(draw_range, s0, s1);
+            }
+            for (auto &th : pool) th.join();
+        } else {
+            draw_range(0, setups);
+        }
+        for (size_t s = 0; s < setups; ++s) {
+            const CalibSample &S = samples[s];
+            if (!S.search) continue;
+            terms.insert(terms.end(), sterms[s].begin(), sterms[s].end());
             offs.insert(offs.end(), S.offs.begin(), S.offs.end());
             nb_ptr.push_back(int(offs.size() / size_t(nd)));
             term_ptr.push_back(int(terms.size()));

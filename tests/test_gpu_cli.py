@@ -57,3 +57,30 @@ def test_cli_full_simulation_equals_reference(g2s, gpu, tmp_path):
     sim, idx = run_cli(g2s, tmp_path, g, ["-k", "1.2", "-n", "20", "-s", "100", "-fs"], {})
     assert np.array_equal(idx.ravel(), g["idx"].ravel())
     assert np.array_equal(sim, g["sim"])
+
+
+def test_auto_qs_cli_equals_calibrate(g2s, gpu, oracle, tmp_path):
+    """auto_qs_b200 (the G2S auto_qs command line): im_1/2/3 images equal to the
+    oracle's calibration for the same setups, seed and iteration counts."""
+    from g2s_b200 import synthetic as syn
+    exe = os.path.join(ROOT, "g2s_b200", "auto_qs_b200")
+    ti = syn.grf((48, 48), (5, 5), seed=4)
+    r = np.arange(9) - 4
+    k = np.exp(-(r[:, None] ** 2 + r[None, :] ** 2) / 10.0).astype(np.float32)
+    g2s.write_bgrid(str(tmp_path / "ti.bgrid"), ti, [0])
+    g2s.write_bgrid(str(tmp_path / "k.bgrid"), k, [0])
+    env = dict(os.environ, G2S_DATA_DIR=str(tmp_path))
+    res = subprocess.run([exe, "-ti", "ti", "-ki", "k", "-maxk", "2", "-maxn", "8", "-densities", "0.1", "0.5",
+                          "-maxIter", "20", "-minIter", "6", "-s", "9", "-id", "cal", "-W_CUDA", "0"],
+                         capture_output=True, text=True, env=env, timeout=300)
+    assert res.returncode == 0, res.stderr
+    assert "compuattion time" in res.stderr
+    m, _ = g2s.read_bgrid(str(tmp_path / "im_1_cal.bgrid"))
+    d, _ = g2s.read_bgrid(str(tmp_path / "im_2_cal.bgrid"))
+    n, _ = g2s.read_bgrid(str(tmp_path / "im_3_cal.bgrid"))
+    om, od, on, _ = oracle.calibrate(ti, [0], [k], g2s.default_neighbour_counts(8), [0.1, 0.5], max_k=2, power=2.0,
+                                     max_iter=20, min_iter=6, seed=9)
+    assert np.array_equal(np.asarray(n).view(np.uint32).reshape(on.shape) if np.asarray(n).dtype == np.float32
+                          else np.asarray(n).reshape(on.shape), on)
+    assert np.array_equal(np.asarray(m).reshape(om.shape), om, equal_nan=True)
+    assert np.array_equal(np.asarray(d).reshape(od.shape), od, equal_nan=True)
