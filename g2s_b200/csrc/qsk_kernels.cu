@@ -921,6 +921,8 @@ __device__ __forceinline__ void mt_seed(unsigned *mt, float sd) {
 #define TAB_CAP 128           // segments of one tie super-run
 #define RNG_BUF (2 * REC_CAP + 640)   // draws of one super-run + one block
 #define SEG_WIN 256           // record counts and maxima of SEG_WIN segments staged per warp
+#define TEAM_MAX 8            // warps of one slot's team (small batches)
+#define TEAM_SLOTS 296        // batches up to this many slots get a team of TEAM_MAX warps per slot
 
 struct __align__(16) WarpShared {
     float rv_s[REC_CAP];      // super-run records (values), 16-byte aligned for cp.async
@@ -933,7 +935,77 @@ struct __align__(16) WarpShared {
     int tcnt[TAB_CAP];
     int wc[SEG_WIN];          // record counts and maxima of segments [wbase, wbase + SEG_WIN)
     float wm[SEG_WIN];
+    // a team of warps on one slot (k_replay with W > 1): the command warp 0
+    // posts, and the per-warp tie counts and slot maps of a super-run
+    int cmd, cmd_off, cmd_tp, cmd_xes, cmd_k, cmd_rp;
+    unsigned cmd_cpt;
+    float cmd_v;
+    int tw_sum[TEAM_MAX];
+    int tw_map[TEAM_MAX][QSK_KMAX];
 };
+
+enum TeamCommand : int { CMD_EXIT = 0, CMD_TWIST = 1, CMD_TWIST_OUT = 2, CMD_SUPER = 3 };
+
+// barrier 1 over the team's threads (barrier 0 stays free for __syncthreads)
+__device__ __forceinline__ void team_bar(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+
+// mt_twist with the elements of each dependency phase spread over the NT
+// (>= 128) threads of a team
+template <bool OUT>
+__device__ void mt_twist_team(unsigned *mt, int tid, int NT, float *out) {
+    unsigned nv[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = tid + i * NT;
+        nv[i] = k < 227 ? mt_mix(mt[k], mt[k + 1], mt[k + 397]) : 0u;
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = tid + i * NT;
+        if (k < 227) {
+            mt[k] = nv[i];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[i]));
+        }
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = 227 + tid + i * NT;
+        nv[i] = k < 454 ? mt_mix(mt[k], mt[k + 1], mt[k - 227]) : 0u;
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = 227 + tid + i * NT;
+        if (k < 454) {
+            mt[k] = nv[i];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[i]));
+        }
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = 454 + tid + i * NT;
+        nv[i] = k < 623 ? mt_mix(mt[k], mt[k + 1], mt[k - 227]) : 0u;
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int k = 454 + tid + i * NT;
+        if (k < 623) {
+            mt[k] = nv[i];
+            if (OUT) out[k] = mt_unit(mt_temper(nv[i]));
+        }
+    }
+    team_bar(NT);
+    if (tid == 0) {
+        const unsigned y = mt_mix(mt[623], mt[0], mt[396]);
+        mt[623] = y;
+        if (OUT) out[623] = mt_unit(mt_temper(y));
+    }
+    team_bar(NT);
+}
 
 // Make segments [q0, q0 + 32) readable from the window (w.wc / w.wm at q - wbase).
 // The scan only moves forward, so a miss restages the window from q0 on.
@@ -958,8 +1030,26 @@ __device__ __forceinline__ void win_cover(WarpShared &w, int &wbase, int q0, int
     __syncwarp();
 }
 
+// One MT19937 block of the slot's stream: regenerated by warp 0 alone (W ==
+// 1), or by the whole team, which warp 0 wakes with a command (W > 1).
+template <int W, bool OUT>
+__device__ __forceinline__ void rng_block(WarpShared &w, int lane, float *out) {
+    if constexpr (W == 1) {
+        mt_twist<OUT>(w.mt, lane, out, w.dummy);
+    } else {
+        __syncwarp();
+        if (lane == 0) {
+            w.cmd = OUT ? CMD_TWIST_OUT : CMD_TWIST;
+            w.cmd_off = OUT ? int(out - w.buf) : 0;
+        }
+        team_bar(32 * W);
+        mt_twist_team<OUT>(w.mt, threadIdx.x, 32 * W, out);
+    }
+}
+
 // Draw buffer with warp-replicated read pointer: rp/len live in registers of
 // every lane (all lanes execute the same control flow).
+template <int W>
 __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int &len) {
     const int unread = len - rp;   // <= 2 * REC_CAP by construction
     // move the unread draws to the front (destinations never overtake sources)
@@ -971,16 +1061,18 @@ __device__ __forceinline__ void rng_refill(WarpShared &w, int lane, int &rp, int
         if (i < unread) w.buf[i] = v;
         __syncwarp();
     }
-    mt_twist<true>(w.mt, lane, w.buf + unread, w.dummy);
+    rng_block<W, true>(w, lane, w.buf + unread);
     len = unread + 624;
     rp = 0;
 }
 
+template <int W>
 __device__ __forceinline__ void rng_ensure(WarpShared &w, int lane, int &rp, int &len, int need) {
-    if (len - rp < need) rng_refill(w, lane, rp, len);
+    if (len - rp < need) rng_refill<W>(w, lane, rp, len);
 }
 
 // at least `need` (<= 2 * REC_CAP) unread draws in the buffer
+template <int W>
 __device__ void rng_ensure_many(WarpShared &w, int lane, int &rp, int &len, int need) {
     if (len - rp >= need) return;
     const int unread = len - rp;
@@ -995,12 +1087,13 @@ __device__ void rng_ensure_many(WarpShared &w, int lane, int &rp, int &len, int 
     len = unread;
     rp = 0;
     while (len < need) {
-        mt_twist<true>(w.mt, lane, w.buf + len, w.dummy);
+        rng_block<W, true>(w, lane, w.buf + len);
         len += 624;
     }
 }
 
 // advance the stream by n draws; whole blocks of 624 only regenerate the state
+template <int W>
 __device__ void rng_skip(WarpShared &w, int lane, int &rp, int &len, long long n) {
     const long long avail = len - rp;
     if (n <= avail) {
@@ -1010,10 +1103,10 @@ __device__ void rng_skip(WarpShared &w, int lane, int &rp, int &len, long long n
     n -= avail;
     rp = len;
     while (n > 624) {
-        mt_twist<false>(w.mt, lane, nullptr, w.dummy);
+        rng_block<W, false>(w, lane, nullptr);
         n -= 624;
     }
-    rng_refill(w, lane, rp, len);
+    rng_refill<W>(w, lane, rp, len);
     rp += int(n);
 }
 
@@ -1289,7 +1382,115 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // then owns a contiguous range of the run, counts its ties, composes the slot
 // maps of its ties on its own, and one warp reduction combines the 32 lane
 // maps in order.
-template <int KM>
+// A super-run on a team of W warps (W > 1): thread t of the team owns
+// records [t*P, t*P + P) of the staged run (the parameters warp 0 posted),
+// the team's tie counts are scanned through shared memory, every thread
+// composes the slot maps of its ties, and the warp maps are composed in warp
+// order.  Returns the tie count and the composed map (in every thread).
+template <int KM, int W>
+__device__ void super_team(WarpShared &w, int tid, int &total, int (&o)[KM]) {
+    const unsigned FULL = 0xffffffffu;
+    constexpr int NT = 32 * W;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int Tp = w.cmd_tp, xes = w.cmd_xes, K = w.cmd_k, rp = w.cmd_rp;
+    const unsigned cpt = w.cmd_cpt;
+    const float V = w.cmd_v;
+    // P odd keeps a warp's reads on distinct banks; P <= REC_CAP / NT + 1 bits
+    const int P = ((Tp + NT - 1) / NT) | 1;
+    const int j0 = min(Tp, tid * P);
+    const int j1 = min(Tp, j0 + P);
+    unsigned tm = 0u;
+    for (int j = j0; j < j1; ++j) tm |= unsigned(w.rv_s[j] == V) << (j - j0);
+    const int mine = __popc(tm);
+    int incl = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, off);
+        if (lane >= off) incl += y;
+    }
+    if (lane == 31) w.tw_sum[wid] = incl;
+    team_bar(NT);
+    int before = 0;
+    total = 0;
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        const int t = w.tw_sum[q];
+        before += q < wid ? t : 0;
+        total += t;
+    }
+    int rank = before + incl - mine;
+#pragma unroll
+    for (int s2 = 0; s2 < KM; ++s2) o[s2] = s2;
+    while (tm) {
+        const int j = j0 + __ffs(tm) - 1;
+        tm &= tm - 1u;
+        const float u1 = w.buf[rp + 2 * rank];
+        const float u2 = w.buf[rp + 2 * rank + 1];
+        int x = K - xes + int(floorf(__fmul_rn(u1, (float)xes)));
+        if (x > K - 1) x = K - 1;
+        const unsigned after = cpt + unsigned(rank) + 1u;
+        const bool write = __fmul_rn(__uint2float_rn(unsigned(xes) + after), u2) < (float)xes;
+        const int ox = sel_i<KM>(o, x), ok1 = sel_i<KM>(o, K - 1);
+        const int wr = -(w.ri_s[j] + 1);
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) {
+            if (s2 == x) o[s2] = ok1;
+            if (s2 == K - 1) o[s2] = write ? wr : ox;
+        }
+        ++rank;
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        int later[KM];
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) later[s2] = __shfl_down_sync(FULL, o[s2], d);
+        if ((lane & (2 * d - 1)) == 0) {
+            int c[KM];
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) c[s2] = later[s2] < 0 ? later[s2] : sel_i<KM>(o, later[s2]);
+#pragma unroll
+            for (int s2 = 0; s2 < KM; ++s2) o[s2] = c[s2];
+        }
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) w.tw_map[wid][s2] = o[s2];
+    }
+    team_bar(NT);
+#pragma unroll
+    for (int s2 = 0; s2 < KM; ++s2) o[s2] = w.tw_map[0][s2];
+#pragma unroll
+    for (int q = 1; q < W; ++q) {
+        int c[KM];
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) {
+            const int later = w.tw_map[q][s2];
+            c[s2] = later < 0 ? later : sel_i<KM>(o, later);
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) o[s2] = c[s2];
+    }
+}
+
+// warps 1..W-1 of a team: run the commands warp 0 posts until it is done
+template <int KM, int W>
+__device__ void team_helper(WarpShared &w) {
+    for (;;) {
+        team_bar(32 * W);
+        const int c = w.cmd;
+        if (c == CMD_EXIT) return;
+        if (c == CMD_TWIST_OUT) {
+            mt_twist_team<true>(w.mt, threadIdx.x, 32 * W, w.buf + w.cmd_off);
+        } else if (c == CMD_TWIST) {
+            mt_twist_team<false>(w.mt, threadIdx.x, 32 * W, nullptr);
+        } else {
+            int tot, o[KM];
+            super_team<KM, W>(w, threadIdx.x, tot, o);
+        }
+    }
+}
+
+template <int KM, int W>
 __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const float *rv, const int *ri, unsigned (&cp)[KM],
                                  unsigned &cpt, int &rp, int &len, WarpShared &w, int lane) {
     const unsigned FULL = 0xffffffffu;
@@ -1300,13 +1501,38 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
         for (int k = c; k < ((c + 3) & ~3); ++k) w.rv_s[pre + k] = -CUDART_INF_F;
     }
     __syncwarp();
+    if constexpr (W > 1) {
+        // draws for every record (at most two per tie), then the team
+        rng_ensure_many<W>(w, lane, rp, len, 2 * Tp);
+        __syncwarp();
+        if (lane == 0) {
+            w.cmd = CMD_SUPER;
+            w.cmd_tp = Tp;
+            w.cmd_v = V;
+            w.cmd_xes = xes;
+            w.cmd_k = K;
+            w.cmd_rp = rp;
+            w.cmd_cpt = cpt;
+        }
+        team_bar(32 * W);
+        int total, o[KM];
+        super_team<KM, W>(w, threadIdx.x, total, o);
+        unsigned np[KM];
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) np[s2] = o[s2] < 0 ? unsigned(-(o[s2] + 1)) : sel_u<KM>(cp, o[s2]);
+#pragma unroll
+        for (int s2 = 0; s2 < KM; ++s2) cp[s2] = np[s2];
+        cpt += unsigned(total);
+        rp += 2 * total;
+        __syncwarp();
+        return;
+    }
     // lane l owns records [l*P, l*P + P); P odd keeps the lanes' reads on
     // distinct shared-memory banks (P <= 33 fits a 64-bit tie mask)
     const int P = ((Tp + 31) >> 5) | 1;
     const int j0 = min(Tp, lane * P);
     const int j1 = min(Tp, j0 + P);
     unsigned long long tmask = 0ull;
-#pragma unroll 4
 #pragma unroll 4
     for (int j = j0; j < j1; ++j) tmask |= (unsigned long long)(w.rv_s[j] == V) << (j - j0);
     const int mine = __popcll(tmask);
@@ -1318,7 +1544,7 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
     }
     const int total = __shfl_sync(FULL, incl, 31);
     int rank = incl - mine;
-    rng_ensure_many(w, lane, rp, len, 2 * total);
+    rng_ensure_many<W>(w, lane, rp, len, 2 * total);
     int o[KM];
 #pragma unroll
     for (int s2 = 0; s2 < KM; ++s2) o[s2] = s2;
@@ -1372,7 +1598,7 @@ __device__ void replay_super_run(int K, float V, int xes, int E, int Tp, const f
 // those below V are skipped, and the first segment above V ends the stream.  Segments are gathered into super-runs of
 // at most REC_CAP padded records and TAB_CAP segments.  Returns the first
 // segment above V, or nseg.
-template <int KM>
+template <int KM, int W>
 __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, const float *rv, const int *ri, const int *rc,
                                  const float *rm, int &wbase, unsigned (&cp)[KM], unsigned &cpt, int &rp, int &len,
                                  WarpShared &w, int lane) {
@@ -1436,19 +1662,28 @@ __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, cons
             sg += 32;
         }
         __syncwarp();
-        if (E > 0) replay_super_run<KM>(K, V, xes, E, Tp, rv, ri, cp, cpt, rp, len, w, lane);
+        if (E > 0) replay_super_run<KM, W>(K, V, xes, E, Tp, rv, ri, cp, cpt, rp, len, w, lane);
         if (stop >= 0) return stop;
     }
 }
 
-template <int KM>
-__global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
+// W == 1: RP_WARPS slots per CTA, one warp each.  W > 1: one slot per CTA;
+// warp 0 replays it and the other W-1 warps join it for the MT19937 blocks
+// and the tie super-runs (small batches, where the GPU would idle otherwise).
+template <int KM, int W>
+__global__ void __launch_bounds__(W == 1 ? 32 * RP_WARPS : 32 * W) k_replay(ReplayArgs A) {
     extern __shared__ __align__(16) unsigned char rp_smem[];
     WarpShared *wsh = reinterpret_cast<WarpShared *>(rp_smem);
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * RP_WARPS + wib;
+    const int b = W == 1 ? blockIdx.x * RP_WARPS + wib : blockIdx.x;
     if (b >= A.nslots) return;
-    WarpShared &w = wsh[wib];
+    WarpShared &w = wsh[W == 1 ? wib : 0];
+    if constexpr (W > 1) {
+        if (wib > 0) {
+            team_helper<KM, W>(w);
+            return;
+        }
+    }
     const Slot s = A.slots[b];
     const Geom &g = A.g;
     const int K = s.K;
@@ -1536,12 +1771,12 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                     if (c > 0) {
                         // the first skip covers the prepared blocks (c >= the masked
                         // positions before the first valid one, so 2c > preskip)
-                        rng_skip(w, lane, rp, len, 2 * c - preskip);
+                        rng_skip<W>(w, lane, rp, len, 2 * c - preskip);
                         preskip = 0;
                         cpt += unsigned(c);
                     }
                 }
-                rng_ensure(w, lane, rp, len, 64);
+                rng_ensure<W>(w, lane, rp, len, 64);
                 // all K state values equal and nothing above them in the chunk
                 if (!filling && sel_f<KM>(cv, 0) == kth0 && __ballot_sync(FULL, valid && v > kth0) == 0) {
                     replay_chunk_ties<KM>(K, valid && v == kth0, m, cp, cpt, rp, w.buf, lane);
@@ -1563,7 +1798,8 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
                 int xes = 0;
 #pragma unroll
                 for (int q = 0; q < KM; ++q) xes += (q < K && cv[q] == kth_s) ? 1 : 0;
-                sg = replay_tie_stream<KM>(K, kth_s, xes, sg, g.nseg, rv, ri, rc, rm, wbase, cp, cpt, rp, len, w, lane);
+                sg = replay_tie_stream<KM, W>(K, kth_s, xes, sg, g.nseg, rv, ri, rc, rm, wbase, cp, cpt, rp, len, w,
+                                              lane);
                 if (sg >= g.nseg) break;
                 win_cover(w, wbase, sg, g.nseg, rc, rm, lane);
                 general_segment(sg, w.wc[sg - wbase], w.wm[sg - wbase]);
@@ -1641,6 +1877,12 @@ __global__ void __launch_bounds__(32 * RP_WARPS) k_replay(ReplayArgs A) {
             chosen_cell = position;
             have = true;
         }
+    }
+    if constexpr (W > 1) {
+        // the team's work is done (every path of warp 0 reaches this point once)
+        __syncwarp();
+        if (lane == 0) w.cmd = CMD_EXIT;
+        team_bar(32 * W);
     }
     if (lane == 0 && have) {
         if (A.node_cell) A.node_cell[s.node] = chosen_cell;
@@ -2380,25 +2622,37 @@ cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cuda
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
     static bool configured[64] = {};
     const size_t smem = sizeof(WarpShared) * RP_WARPS;
+    const size_t smem_team = sizeof(WarpShared);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!configured[dev]) {
-        if ((e = cudaFuncSetAttribute(k_replay<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+        if ((e = cudaFuncSetAttribute(k_replay<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
+            (e = cudaFuncSetAttribute(k_replay<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
             return e;
         configured[dev] = true;
     }
+    if (a.nslots <= TEAM_SLOTS) {
+        // small batch: a team of TEAM_MAX warps per slot
+        const unsigned blocks = (unsigned)a.nslots;
+        constexpr int T = TEAM_MAX;
+        if (a.K <= 1) k_replay<1, T><<<blocks, 32 * T, smem_team, st>>>(a);
+        else if (a.K <= 2) k_replay<2, T><<<blocks, 32 * T, smem_team, st>>>(a);
+        else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem_team, st>>>(a);
+        else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem_team, st>>>(a);
+        else k_replay<16, T><<<blocks, 32 * T, smem_team, st>>>(a);
+        return cudaGetLastError();
+    }
     unsigned blocks = (unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS);
-    if (a.K <= 1) k_replay<1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 2) k_replay<2><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 4) k_replay<4><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 8) k_replay<8><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else k_replay<16><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    if (a.K <= 1) k_replay<1, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 2) k_replay<2, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 4) k_replay<4, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else if (a.K <= 8) k_replay<8, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    else k_replay<16, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
