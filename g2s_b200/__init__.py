@@ -44,7 +44,8 @@ class QskParams(ctypes.Structure):
 
 
 class QskPatternOpts(ctypes.Structure):
-    _fields_ = [("exclude_index", ctypes.c_int), ("missing_data", ctypes.c_int), ("centre_mask_layer", ctypes.c_int)]
+    _fields_ = [("exclude_index", ctypes.c_int), ("missing_data", ctypes.c_int), ("centre_mask_layer", ctypes.c_int),
+                ("exclude_radius", ctypes.c_float)]
 
 
 class QskCalibParams(ctypes.Structure):
@@ -247,9 +248,11 @@ class Worker:
         self.handle = h
 
     def pattern_kbest(self, offsets: np.ndarray, terms, k: int, seed: float, exclude_index: int = -1,
-                      missing_data: bool = False, centre_mask_layer: int = -1):
+                      missing_data: bool = False, centre_mask_layer: int = -1, exclude_radius: float = 0.0):
         """offsets: (n, ndim) int; terms: list of (neighbour, layer, op, a, b).
-        Returns (scores[k], scan_indices[k], min_offset[ndim])."""
+        ``exclude_index`` (scan index) is forced to -inf, with
+        ``exclude_radius`` >= 1 every index the reference's radius exclusion
+        marks around it.  Returns (scores[k], scan_indices[k], min_offset[ndim])."""
         offs = np.ascontiguousarray(offsets, dtype=np.int32).reshape(-1, self.ti.ndim)
         tarr = (QskTerm * max(len(terms), 1))(*[QskTerm(int(t[0]), int(t[1]), int(t[2]), float(t[3]), float(t[4]))
                                                for t in terms])
@@ -260,7 +263,7 @@ class Worker:
             _check(lib().qsk_pattern_kbest(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
                                            _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)), "qsk_pattern_kbest")
         else:
-            opts = QskPatternOpts(int(exclude_index), int(missing_data), int(centre_mask_layer))
+            opts = QskPatternOpts(int(exclude_index), int(missing_data), int(centre_mask_layer), float(exclude_radius))
             _check(lib().qsk_pattern_kbest_ex(self.handle, offs.shape[0], _p(offs, _i32p), len(terms), tarr, k, seed,
                                               ctypes.byref(opts), _p(sc, _f32p), _p(ix, _u32p), _p(mn, _i32p)),
                    "qsk_pattern_kbest_ex")

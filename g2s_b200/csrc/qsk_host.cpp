@@ -247,7 +247,9 @@ int build_pattern_slot(const qsk_ti *ti, int nnb, const int *offsets, int nterms
     }
     if (nvalid < (long long)K) s.flags |= SLOT_EMIT_MASKED;
     if (opts) {
-        if (opts->exclude_index >= 0 && (long long)opts->exclude_index < g.N) s.excl = opts->exclude_index;
+        // a radius exclusion is a mask made by the caller (k_radius_mask)
+        if (opts->exclude_index >= 0 && (long long)opts->exclude_index < g.N && !(opts->exclude_radius >= 1.f))
+            s.excl = opts->exclude_index;
         if (opts->missing_data) {
             if (opts->centre_mask_layer < 0 || opts->centre_mask_layer >= ti->nlayers)
                 return fail(QSK_ERR_ARG, "centre_mask_layer %d out of range", opts->centre_mask_layer);
@@ -499,7 +501,16 @@ static int pattern_batch_impl(qsk_worker *w, int B, const int *nb_ptr, const int
     std::vector<int> xc;
     std::vector<float> xr;
     bool any_radius = false;
-    if (origin) {
+    if (opts && opts->exclude_radius >= 1.f && opts->exclude_index >= 0 && (long long)opts->exclude_index < g.N) {
+        xc.assign(B, -1);
+        xr.assign(B, 0.f);
+        for (int b = 0; b < B; ++b) {
+            if (w->h_slots[b].flags & SLOT_SKIP) continue;
+            xc[b] = opts->exclude_index;
+            xr[b] = opts->exclude_radius;
+            any_radius = true;
+        }
+    } else if (origin) {
         xc.assign(B, -1);
         xr.assign(B, 0.f);
         for (int b = 0; b < B; ++b) {
@@ -1362,6 +1373,9 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
     std::vector<int> start = {0, int(s->nodes)};
     rc = sim_batches(s, start, true);
     if (rc) return rc;
+    s->info.nodes = s->nodes;
+    s->info.levels = 1;
+    s->info.max_batch = int(s->nodes);
     CK(cudaStreamSynchronize(s->st));
     return sim_check_status(s);
 }

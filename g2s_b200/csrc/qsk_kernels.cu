@@ -733,19 +733,25 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
                 acc[r] = valid[r] ? e : CUDART_NAN_F;
             }
         }
-        if (ss.excl >= 0) {
+        // verbatim exclusion (one index, or the radius mask): -inf written over
+        // the map after the compensation, at masked positions too, where it
+        // replaces the NaN border of a missing-data map
+        // (quantileSamplingModule.hpp:518-523, CPUThreadDevice.cpp:310-342)
+        bool hit[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if ((int)(base + 32 * r + lane) == ss.excl && valid[r]) acc[r] = -CUDART_INF_F;
-        }
+        for (int r = 0; r < 4; ++r) hit[r] = exists[r] && (int)(base + 32 * r + lane) == ss.excl;
         if (A.xmask) {
             const unsigned *xm = A.xmask + (long long)b * A.xwords;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const unsigned m = base + 32 * r + lane;
-                if (exists[r] && valid[r] && ((xm[m >> 5] >> (m & 31)) & 1u)) acc[r] = -CUDART_INF_F;
+                if (exists[r] && ((xm[m >> 5] >> (m & 31)) & 1u)) hit[r] = true;
             }
         }
+        // a masked position is an explicit record when the slot emits masked
+        // entries, or when it is an excluded one of a missing-data map (-inf
+        // instead of NaN); otherwise the replay counts it as an implicit -inf
+        const bool missing = (ss.flags & SLOT_MISSING) != 0;
         // warp prefix top-KF over the segment in scan order; records are the
         // positions not below the K-th best of everything before them in the
         // segment (a superset of the global triggers).
@@ -756,7 +762,7 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
         float segmax = -CUDART_INF_F;
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const float xval = valid[r] ? acc[r] : ((ss.flags & SLOT_MISSING) ? CUDART_NAN_F : -CUDART_INF_F);
+            const float xval = hit[r] ? -CUDART_INF_F : valid[r] ? acc[r] : (missing ? CUDART_NAN_F : -CUDART_INF_F);
             segmax = fmaxf(segmax, xval);
             // a NaN score never compares true in the reservoir (fKb.hpp), so it
             // is never a record and must not raise the prefix K-th best: it
@@ -784,7 +790,7 @@ __global__ void __launch_bounds__(256) k_map_records(MapArgs A) {
             }
             topk_merge<KF>(carry, ex, pre);
             const float kth = pre[KF - 1];
-            const bool rec = exists[r] && (xval >= kth) && (valid[r] || emit_masked);
+            const bool rec = exists[r] && (xval >= kth) && (valid[r] || emit_masked || (hit[r] && missing));
             const unsigned bal = __ballot_sync(0xffffffffu, rec);
             if (rec) {
                 const int o = count + __popc(bal & lanemask_lt());

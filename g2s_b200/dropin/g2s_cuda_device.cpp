@@ -21,7 +21,11 @@
 //    otherwise the unnormalised N·S of the CPU device);
 //  * training images with missing values: the overlap ("cross") output of the
 //    XMeasurement matrix, its centre mask and the -|S/c^4| compensation are
-//    applied on the GPU (qsk_pattern_opts); -nV excludes one candidate.
+//    applied on the GPU (qsk_pattern_opts); -nV excludes one candidate, or,
+//    with a verbatim radius (auto_qs' distribution() queries), every index
+//    that the CPU device's setValueInErrorArrayWithRadius marks
+//    (CPUThreadDevice.cpp:310-342; the reference CUDA device leaves that
+//    method empty, NvidiaGPUAcceleratorDevice.cu:646-670).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -131,6 +135,7 @@ public:
             }
         }
         _opts.exclude_index = -1;
+        _opts.exclude_radius = 0.f;
         _opts.missing_data = 0;
         _opts.centre_mask_layer = -1;
         _delta = delta0.empty() ? 0.f : delta0[0];
@@ -149,6 +154,7 @@ public:
             for (unsigned j = 0; j < extendK; ++j) errors[j] = _trueMismatch ? errors[j] + _delta : errors[j] * N;
         }
         _opts.exclude_index = -1;
+        _opts.exclude_radius = 0.f;
     }
 
     unsigned getErrorsArraySize() override { return _realSpaceSize; }
@@ -180,13 +186,13 @@ public:
     }
     // -nV: the excluded candidate (quantileSamplingModule.hpp:566-571); the
     // reference only ever writes -inf here
-    void setValueInErrorArray(unsigned position, float) override { _opts.exclude_index = int(position); }
-    void setValueInErrorArrayWithRadius(unsigned position, float value, float radius) override {
-        if (radius < 1.f) {
-            setValueInErrorArray(position, value);
-            return;
-        }
-        throw std::runtime_error("g2s_b200: a verbatim exclusion radius >= 1 is not supported");
+    void setValueInErrorArray(unsigned position, float) override {
+        _opts.exclude_index = int(position);
+        _opts.exclude_radius = 0.f;
+    }
+    void setValueInErrorArrayWithRadius(unsigned position, float, float radius) override {
+        _opts.exclude_index = int(position);
+        _opts.exclude_radius = radius;
     }
     // -|S / c^4|, -inf where c == 0 (NvidiaGPUAcceleratorDevice.cu:199-206,677-686)
     void compensateMissingData() override { _opts.missing_data = 1; }
@@ -202,7 +208,7 @@ private:
     qsk_worker *_worker = nullptr;
     std::vector<int> _offsets;
     std::vector<qsk_term> _terms;
-    qsk_pattern_opts _opts{-1, 0, -1};
+    qsk_pattern_opts _opts{-1, 0, -1, 0.f};
     int _nnb = 0;
     float _delta = 0.f;
 };

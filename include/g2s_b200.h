@@ -112,11 +112,20 @@ int qsk_pattern_kbest(qsk_worker *w, int n_neighbours, const int *offsets, int n
  *                      centre mask, -inf where c == 0, NaN outside the border
  *                      (maskCroossErrorWithVariable + compensateMissingData,
  *                      quantileSamplingModule.hpp:559-564, .cu:617-686)
- *   centre_mask_layer  layer holding the TI mask (1 informed, 0 missing) */
+ *   centre_mask_layer  layer holding the TI mask (1 informed, 0 missing)
+ *   exclude_radius     >= 1: instead of exclude_index alone, every scan index
+ *                      that CPUThreadDevice::setValueInErrorArrayWithRadius
+ *                      (G2S src/CPUThreadDevice.cpp:310-342) marks around it
+ *                      is forced to -inf (distribution() with a verbatim
+ *                      radius, quantileSamplingModule.hpp:518-523); < 1: the
+ *                      single index
+ * The exclusion is written after the missing-data score, over the NaN border
+ * too, as the reference writes it into its error array. */
 typedef struct {
     int exclude_index;
     int missing_data;
     int centre_mask_layer;
+    float exclude_radius;
 } qsk_pattern_opts;
 
 int qsk_pattern_kbest_ex(qsk_worker *w, int n_neighbours, const int *offsets, int n_terms, const qsk_term *terms,
@@ -272,8 +281,8 @@ typedef struct {
 
 typedef struct {
     long long nodes;              /* path nodes simulated */
-    int levels;                   /* dependency levels (batches) */
-    int max_batch;                /* largest level */
+    int levels;                   /* dependency levels (1 under teacher forcing) */
+    int max_batch;                /* largest level (batches are cut at the slot budget) */
     int template_size;
     float ms_setup_neighbours;    /* device time of the neighbour search */
     float ms_levels;              /* device time of the level computation */

@@ -104,6 +104,33 @@ def test_verbatim_batch_equals_oracle(g2s, gpu, oracle, name, mk, types, k):
     T.close()
 
 
+@pytest.mark.parametrize("k", [1, 4])
+def test_single_query_radius_option_equals_oracle(g2s, gpu, oracle, k):
+    """qsk_pattern_kbest_ex with exclude_radius (what the drop-in device does
+    for setValueInErrorArrayWithRadius under auto_qs -W_CUDA): the scan index
+    of the origin and every index the reference's radius recursion marks
+    around it are -inf; equal to the oracle's distribution()."""
+    ti = syn.grf((64, 64), (6, 6), seed=2)
+    rng = np.random.default_rng(100 + k)
+    kernel = gauss_kernel(21, 60.0)
+    T = g2s.TrainingImage(ti, [0])
+    W = g2s.Worker(T)
+    for trial in range(12):
+        origin, offs, vals = sample_pattern(rng, ti, 1, int(rng.integers(2, 40)), 10)
+        radius = [1.0, 2.5, 4.5, 11.0][trial % 4]
+        seed = float(np.float32(rng.random()))
+        mn = np.minimum(offs.min(axis=0), 0).astype(np.int32)
+        idx = g2s.lib().qsk_position_to_index(T.handle, g2s._p(mn, g2s._i32p), origin)
+        sc, ix, gmn = W.pattern_kbest(offs, terms_of(offs, vals, [0], kernel, g2s), k, seed, exclude_index=idx,
+                                      exclude_radius=radius)
+        osc, oix, opos, omn = oracle.distribution(ti, [0], kernel, offs, vals, k, seed, origin, radius)
+        assert np.array_equal(gmn, omn)
+        assert np.array_equal(sc, osc), (trial, sc, osc)
+        assert np.array_equal(ix, oix), (trial, ix, oix)
+    W.close()
+    T.close()
+
+
 @pytest.mark.parametrize("noise", [0.0, 0.4])
 def test_calibrate_equals_oracle(g2s, gpu, oracle, noise):
     ti = syn.grf((64, 64), (6, 6), seed=12)

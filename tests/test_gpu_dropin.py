@@ -91,3 +91,51 @@ def test_qs_w_cuda_missing_data_equals_oracle(oracle):
     sim, idx, log = run_qs_dropin(g, 31021)
     o = oracle.simulate(g["ti"], g["di"], [0], int(g["n"]), float(g["k"]), int(g["seed"]), mode=0)
     assert np.array_equal(sim, o["sim"]) and np.array_equal(idx.ravel(), o["id"])
+
+
+def test_auto_qs_w_cuda_calibration_agrees_with_oracle(oracle):
+    """The unmodified G2S auto_qs (oracle/_ref/auto_qs_cuda: src/auto_qs.cpp
+    with its -W_CUDA dlopen path) calibrating on the drop-in device: every
+    distribution() query, with the verbatim exclusion of the sample's
+    neighbourhood (radius (cells*0.005)^(1/2) here), runs on the GPU.  The
+    program seeds its generators from the clock, so its estimates are
+    compared statistically with the oracle's calibration: without pruning
+    every setup collects the same number of samples, and every mean error
+    agrees within a few standard errors."""
+    from oracle import ref
+    from g2s_b200 import synthetic as syn
+    exe = os.path.join(ROOT, "oracle", "_ref", "auto_qs_cuda")
+    if not (os.path.exists(exe) and os.path.exists(os.path.join(DROPIN_DIR, "g2s_cuda.so"))):
+        pytest.fail("oracle/_ref/auto_qs_cuda or g2s_b200/dropin/g2s_cuda.so missing (__graft_entry__.build)")
+    ti = syn.grf((48, 48), (5, 5), seed=21)
+    r = np.arange(11) - 5
+    kernel = np.exp(-(r[:, None] ** 2 + r[None, :] ** 2) / 20.0).astype(np.float32)
+    max_n, dens, max_k, iters = 6, [0.1, 0.5], 2, 1500
+    job = 31030
+    outputs = [f"im_{i}_{job}" for i in (1, 2, 3)]
+    _cleanup(outputs)
+    ref.write_image(f"dropin_ti_{job}", ti, [0])
+    ref.write_image(f"dropin_k_{job}", kernel, [0])
+    log = f"/tmp/G2S/logs/dropin_{job}.log"
+    cmd = [exe, "-ti", f"dropin_ti_{job}", "-ki", f"dropin_k_{job}", "-maxk", str(max_k), "-maxn", str(max_n),
+           "-densities"] + [str(d) for d in dens] + ["-maxIter", str(iters), "-minIter", str(iters), "-j", "1",
+                                                   "-W_CUDA", "0", "-id", str(job), "-r", log]
+    p = subprocess.run(cmd, cwd=DROPIN_DIR, capture_output=True, text=True, timeout=600)
+    text = open(log).read() if os.path.exists(log) else ""
+    assert p.returncode == 0, (p.stdout[-2000:], p.stderr[-2000:], text[-2000:])
+    assert "could not load" not in text
+    rm = ref.read_image(f"im_1_{job}").astype(np.float64)
+    rd = ref.read_image(f"im_2_{job}").astype(np.float64)
+    rn = ref.read_image(f"im_3_{job}")
+    rn = (rn.view(np.uint32) if rn.dtype == np.float32 else rn).astype(np.float64)
+    _cleanup(outputs + [f"dropin_ti_{job}", f"dropin_k_{job}"])
+    counts = np.arange(1, max_n, dtype=np.uint32)[:, None]
+    om, od, on, _ = oracle.calibrate(ti, [0], [kernel], counts, dens, max_k=max_k, power=2.0, max_iter=iters,
+                                     min_iter=iters, seed=5)
+    rm, rd, rn = (a.reshape(om.shape) for a in (rm, rd, rn))
+    assert np.abs(rn - on).max() <= 0.02 * iters, (rn, on)
+    ok = (rn > 30) & (on > 30)
+    m1, m2 = om[ok].astype(np.float64) ** 2, rm[ok] ** 2
+    z = np.abs(m1 - m2) / np.sqrt(od[ok].astype(np.float64) ** 4 / on[ok] + rd[ok] ** 4 / rn[ok])
+    assert ok.sum() >= 10
+    assert np.all(z < 5.0), (z.max(), m1, m2)

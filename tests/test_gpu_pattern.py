@@ -250,3 +250,73 @@ def test_missing_data_pattern_scores(g2s, gpu):
     expect = np.sort(np.array(expect, np.float64))[::-1][:K]
     got = sc.astype(np.float64)
     assert np.allclose(got[np.isfinite(expect)], expect[np.isfinite(expect)], rtol=1e-5, atol=1e-7), (got, expect)
+
+
+def test_missing_data_exclusion_over_masked_positions(g2s, gpu, oracle):
+    """-nV with a training image with missing values: the excluded scan index
+    is -inf after the -|S/c^4| compensation, also where it falls on the NaN
+    border (quantileSamplingModule.hpp:559-571 writes it into the error
+    array).  A -inf there takes part in the reservoir's ties while fewer than
+    K finite values have been seen, a NaN never does.  Integer TI values and
+    pattern values make every score exact in FP32, so the expected map is
+    built here and run through the oracle's k-biggest; every scan index is
+    tried as the excluded one."""
+    rng = np.random.default_rng(11)
+    ti = rng.integers(0, 3, (7, 9)).astype(np.float32)
+    ti[2, 3] = np.nan
+    ti[5, 6] = np.nan
+    ti[0, 1] = np.nan
+    ny, nx = ti.shape
+    offs = np.array([[0, 0], [1, 0], [-1, 2]], np.int32)
+    vals = np.array([np.nan, 1.0, 2.0], np.float32)
+    flat = ti.reshape(-1)
+    m = (~np.isnan(flat)).astype(np.float32)
+    t0 = np.where(np.isnan(flat), 0, flat).astype(np.float32)
+    L = g2s.TrainingImage.from_layers([(t0 * t0)[::-1].copy(), t0[::-1].copy(), m[::-1].copy()],
+                                      src_size=[nx, ny], fft_size=[nx, ny])
+    W = g2s.Worker(L)
+    terms = []
+    for j in (1, 2):
+        v = float(vals[j])
+        terms += [(j, 0, g2s.QSK_OP_LIN, -1.0, 0.0), (j, 1, g2s.QSK_OP_LIN, 2.0 * v, 0.0),
+                  (j, 2, g2s.QSK_OP_LIN, -v * v, 0.0), (j, 2, g2s.QSK_OP_LIN_CROSS, 1.0, 0.0)]
+    mn = offs.min(axis=0)
+    mx = offs.max(axis=0)
+    N = nx * ny
+    base = np.full(N, np.nan, np.float32)
+    valid = np.zeros(N, bool)
+    for i in range(N):
+        ix, iy = i % nx, i // nx
+        # scan index -> TI cell (cvtIndexToPosition with fft == src)
+        px = (nx - ix - mn[0] - 1 + nx) % nx
+        py = (ny - iy - mn[1] - 1 + ny) % ny
+        if ix < mx[0] - mn[0] or iy < mx[1] - mn[1]:
+            continue
+        valid[i] = True
+        S, c = 0.0, 0.0
+        for (ox, oy), v in zip(offs[1:], vals[1:]):
+            t = ti[py + oy, px + ox]
+            if np.isnan(t):
+                continue
+            S -= (float(t) - float(v)) ** 2
+            c += 1.0
+        if np.isnan(ti[py, px]):
+            c = 0.0
+        base[i] = -np.inf if c == 0 else -abs(np.float32(S) / np.float32(c ** 4))
+    sensitive = 0
+    for K in (1, 3, 8):
+        for seed in (0.25, 0.8125):
+            for x in range(N):
+                ref = base.copy()
+                ref[x] = -np.inf
+                ev, ep = oracle.kbiggest(ref, K, seed)
+                sc, ix, _ = W.pattern_kbest(offs, terms, K, seed, exclude_index=x, missing_data=True,
+                                            centre_mask_layer=2)
+                assert np.array_equal(sc, ev) and np.array_equal(ix, ep), (K, seed, x, sc, ev, ix, ep)
+                if not valid[x]:
+                    nv, npos = oracle.kbiggest(base, K, seed)
+                    sensitive += int(not (np.array_equal(nv, ev) and np.array_equal(npos, ep)))
+    # the case where -inf and NaN differ is met
+    assert sensitive > 0
+    W.close()
+    L.close()
