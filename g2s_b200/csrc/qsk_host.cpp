@@ -707,7 +707,7 @@ struct qsk_sim {
     DBuf<unsigned> d_path, d_post, d_id, d_node_cell, d_nb_cell;
     DBuf<int> d_node_of_cell, d_nb_count, d_nb_tpl, d_level_nodes, d_status;
     // dependency levels (Kahn frontiers over the reverse edges)
-    DBuf<int> d_adj, d_deg, d_outcnt, d_outstart, d_cursor, d_tile_sum, d_lcnt, d_start, d_nl;
+    DBuf<int> d_level, d_cursor, d_tile_sum, d_lcnt, d_start, d_nl;
     DBuf<Slot> d_slots;
     DBuf<Term> d_terms;
     DBuf<float> d_rec_val;
@@ -1086,7 +1086,12 @@ int sim_check_status(qsk_sim *s) {
     int st = 0;
     CK(cudaMemcpyAsync(&st, s->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    if (st != DEV_OK) return fail(QSK_ERR_DEVICE, "device status %d (too many terms for a node)", st);
+    if (st != DEV_OK)
+        return fail(QSK_ERR_DEVICE, "device status %d (%s)", st,
+                    st == DEV_TOO_MANY_TERMS ? "too many terms for a node"
+                    : st == DEV_LEVEL_WAIT   ? "a dependency level did not appear within the wait limit"
+                    : st == DEV_BAD_INDEX    ? "index out of range"
+                                             : "unknown");
     return QSK_OK;
 }
 
@@ -1241,10 +1246,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_nb_count.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_nb_tpl.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
         (e = s->d_nb_cell.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n)) != cudaSuccess ||
-        (e = s->d_adj.alloc(size_t(std::max<long long>(s->nodes, 1)) * s->n * (s->full ? s->nvar : 1))) != cudaSuccess ||
-        (e = s->d_deg.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
-        (e = s->d_outcnt.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
-        (e = s->d_outstart.alloc(size_t(s->nodes) + 1)) != cudaSuccess ||
+        (e = s->d_level.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_cursor.alloc(size_t(std::max<long long>(s->nodes, 1)))) != cudaSuccess ||
         (e = s->d_tile_sum.alloc(size_t((s->nodes + 1023) / 1024) + 2)) != cudaSuccess ||
         (e = s->d_lcnt.alloc(size_t(s->nodes) + 2)) != cudaSuccess ||
@@ -1312,22 +1314,21 @@ int qsk_sim_run(qsk_sim *s) {
     la.nb_mask = s->full ? s->d_nb_mask.p : nullptr;
     la.nvar = s->nvar;
     la.node_of_cell = s->d_node_of_cell.p;
-    la.deg = s->d_deg.p;
-    la.outcnt = s->d_outcnt.p;
-    la.outstart = s->d_outstart.p;
+    la.level = s->d_level.p;
     la.cursor = s->d_cursor.p;
     la.tile_sum = s->d_tile_sum.p;
-    la.adj = s->d_adj.p;
     la.cnt = s->d_lcnt.p;
+    la.status = s->d_status.p;
     la.level_nodes = s->d_level_nodes.p;
     la.start = s->d_start.p;
     la.nl_out = s->d_nl.p;
     CK(cudaMemsetAsync(s->d_nl.p, 0, sizeof(int), s->st));
     CK(launch_levels(la, s->st));
-    s->info.launches += 7;  // neighbours + count, 3 scan passes, reverse edges, frontiers
+    s->info.launches += 7;  // neighbours, level pass, count, 3 scan passes, scatter
     int nl = 0;
     CK(cudaMemcpyAsync(&nl, s->d_nl.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CK(cudaStreamSynchronize(s->st));
+    rc = sim_check_status(s);
+    if (rc) return rc;
     std::vector<int> start(size_t(nl) + 1, 0);
     if (nl > 0) {
         CK(cudaMemcpyAsync(start.data(), s->d_start.p, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, s->st));

@@ -84,6 +84,7 @@ enum DevStatus : int {
     DEV_OK = 0,
     DEV_BAD_INDEX = 1,
     DEV_TOO_MANY_TERMS = 2,
+    DEV_LEVEL_WAIT = 3,       // a dependency level did not appear within the wait limit
 };
 
 // Grid (destination image) description for the neighbour search.
@@ -177,6 +178,7 @@ struct BitArgs {
     const unsigned *id_image = nullptr;
     const int *tpl = nullptr;           // template offsets (ntpl x nd)
     int no_verbatim = 0;
+    int stage_words = 0;                // shared-memory words for staged planes (set by the launcher)
 };
 
 struct ReplayArgs {
@@ -234,16 +236,14 @@ struct LevelArgs {
     const unsigned char *nb_mask;  // -fs: variables each neighbour contributes (null otherwise)
     int nvar;
     const int *node_of_cell;       // per cell, or (-fs) per cell value
-    int *deg;           // nodes
-    int *outcnt;        // nodes
-    int *outstart;      // nodes + 1
+    int *level;         // nodes: level of each path node
     int *cursor;        // nodes
     int *tile_sum;      // ceil(nodes / 1024) + 1
-    int *adj;           // nodes * n
-    int *cnt;           // nodes + 2
+    int *cnt;           // nodes + 2: nodes per level, then the node ticket
     int *level_nodes;   // nodes: grouped by level
     int *start;         // nodes + 1: level L is level_nodes[start[L] .. start[L+1])
     int *nl_out;        // 1: number of levels
+    int *status;        // DevStatus
 };
 cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st);
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);

@@ -16,9 +16,9 @@
 //   k_map_bits     the same map for categorical patterns with unit weights,
 //                  bit-sliced (one bit plane per category), same records
 // Setup kernels: k_build_layers (DataImage.hpp:538-599), k_neighbours
-// (simulation.hpp:447-511, run for every path node at once), k_dep_count /
-// k_adj_fill / k_kahn (dependency levels of the path DAG, grouped by level).
-#include <cooperative_groups.h>
+// (simulation.hpp:447-511, run for every path node at once), k_level_flow /
+// k_level_count / k_level_scatter (dependency levels of the path DAG, nodes
+// grouped by level).
 #include <cuda_runtime.h>
 #include <math_constants.h>
 #include <cstdint>
@@ -252,9 +252,8 @@ __global__ void k_neighbours_full(GridDesc dg, const int *__restrict__ tpl, int 
 // dependency levels: level(i) = 1 + max level(j) over the node's informed
 // neighbours j that are themselves path nodes (0 without any) -- the longest
 // path to i in the path DAG (dependencies always point to smaller path
-// indices).  Kahn's frontier algorithm over the reverse edges: the nodes of
-// level L are those whose last dependency finished in level L-1, so the
-// frontiers come out already grouped by level.
+// indices).  One pass in path order (k_level_flow), then a counting sort of
+// the nodes by level (k_level_count, the scan, k_level_scatter).
 // ---------------------------------------------------------------------------
 // dependency nodes of neighbour j of node i: the cell's node, or (-fs, with
 // nb_mask) the nodes of the cell's values that the neighbour contributes
@@ -276,20 +275,62 @@ __device__ __forceinline__ void for_each_dep(long long i, int j, int n, const un
         }
 }
 
-// in-degree of every node and out-degree count of every dependency
-__global__ void k_dep_count(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                            const unsigned char *__restrict__ nb_mask, int nvar, const int *__restrict__ node_of,
-                            int *__restrict__ deg, int *__restrict__ outcnt) {
+#define LEVEL_SPIN_LIMIT (1u << 22)   // polls of one dependency (about a second with the back-off)
+
+// One warp per node, nodes taken in path order from a ticket.  A node's
+// dependencies have smaller path indices, so they were taken earlier by warps
+// that are running; the smallest unfinished node waits on finished nodes only,
+// so every wait ends.  The waits are bounded all the same: past the limit the
+// kernel records DEV_LEVEL_WAIT and moves on (the host then fails the run).
+// The level words start at -1; a level is published with one volatile store
+// and read with volatile loads (it carries no other data).
+__global__ void k_level_flow(long long nodes, int n, const int *__restrict__ nb_count,
+                             const unsigned *__restrict__ nb_cell, const unsigned char *__restrict__ nb_mask, int nvar,
+                             const int *__restrict__ node_of, int *level, int *ticket, int *nl_out, int *status) {
+    const int lane = threadIdx.x & 31;
+    volatile int *vlevel = level;
+    for (;;) {
+        int i = 0;
+        if (lane == 0) i = atomicAdd(ticket, 1);
+        i = __shfl_sync(0xffffffffu, i, 0);
+        if ((long long)i >= nodes) return;
+        const int c = nb_count[i];
+        int mx = -1;
+        bool bad = false, late = false;
+        for (int j = lane; j < c; j += 32)
+            for_each_dep(i, j, n, nb_cell, nb_mask, nvar, node_of, [&](int d) {
+                if (d >= i) {
+                    bad = true;
+                    return;
+                }
+                int lv = vlevel[d];
+                unsigned spins = 0;
+                while (lv < 0) {
+                    if (++spins > LEVEL_SPIN_LIMIT) {
+                        late = true;
+                        lv = 0;
+                        break;
+                    }
+                    __nanosleep(128);
+                    lv = vlevel[d];
+                }
+                mx = max(mx, lv);
+            });
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        const bool any_bad = __any_sync(0xffffffffu, bad), any_late = __any_sync(0xffffffffu, late);
+        if (lane == 0) {
+            if (any_bad) atomicExch(status, DEV_BAD_INDEX);
+            if (any_late) atomicExch(status, DEV_LEVEL_WAIT);
+            vlevel[i] = mx + 1;
+            atomicMax(nl_out, mx + 2);
+        }
+    }
+}
+
+__global__ void k_level_count(long long nodes, const int *__restrict__ level, int *__restrict__ cnt) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nodes) return;
-    const int c = nb_count[i];
-    int dg = 0;
-    for (int j = 0; j < c; ++j)
-        for_each_dep(i, j, n, nb_cell, nb_mask, nvar, node_of, [&](int d) {
-            ++dg;
-            atomicAdd(&outcnt[d], 1);
-        });
-    deg[i] = dg;
+    if (i < nodes) atomicAdd(&cnt[level[i]], 1);
 }
 
 // exclusive scan in three passes: 1024-element tiles, tile sums, add
@@ -347,55 +388,11 @@ __global__ void k_scan_add(long long count, int *__restrict__ out, int *__restri
     }
 }
 
-// reverse edges: adj[outstart[d] ..] lists the nodes that depend on d
-__global__ void k_adj_fill(long long nodes, int n, const int *__restrict__ nb_count, const unsigned *__restrict__ nb_cell,
-                           const unsigned char *__restrict__ nb_mask, int nvar, const int *__restrict__ node_of,
-                           int *__restrict__ cursor, int *__restrict__ adj) {
+// nodes grouped by level (order inside a level is free: its nodes are independent)
+__global__ void k_level_scatter(long long nodes, const int *__restrict__ level, int *__restrict__ cursor,
+                                int *__restrict__ level_nodes) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nodes) return;
-    const int c = nb_count[i];
-    for (int j = 0; j < c; ++j)
-        for_each_dep(i, j, n, nb_cell, nb_mask, nvar, node_of, [&](int d) { adj[atomicAdd(&cursor[d], 1)] = int(i); });
-}
-
-// Frontier pass (cooperative launch, one grid barrier per level).  Level L's
-// nodes are level_nodes[start[L] .. start[L] + cnt[L]); a node joins level
-// L+1 when its remaining in-degree drops to zero.  cnt (levels + 2 ints) starts
-// at zero.  Writes start[0..nl] and *nl_out.
-__global__ void k_kahn(long long nodes, int *__restrict__ deg, const int *__restrict__ outstart,
-                       const int *__restrict__ adj, int *level_nodes, int *cnt, int *__restrict__ start,
-                       int *__restrict__ nl_out) {
-    namespace cg = cooperative_groups;
-    cg::grid_group grid = cg::this_grid();
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long wid = tid >> 5, nwarps = stride >> 5;
-    const int lane = threadIdx.x & 31;
-    for (long long i = tid; i < nodes; i += stride)
-        if (deg[i] == 0) level_nodes[atomicAdd(&cnt[0], 1)] = int(i);
-    grid.sync();
-    long long st = 0;
-    for (long long L = 0; L <= nodes; ++L) {
-        const int c = ((volatile int *)cnt)[L];
-        if (tid == 0) start[L] = int(st);
-        if (c == 0) {
-            if (tid == 0) *nl_out = int(L);
-            break;
-        }
-        const long long nst = st + c;
-        // one warp per frontier node, lanes over its dependents (out-degrees
-        // are skewed: early path nodes are neighbours of many later ones)
-        for (long long q = wid; q < c; q += nwarps) {
-            const int i = ((volatile int *)level_nodes)[st + q];
-            const int e1 = outstart[i + 1];
-            for (int e = outstart[i] + lane; e < e1; e += 32) {
-                const int d = adj[e];
-                if (atomicSub(&deg[d], 1) == 1) level_nodes[nst + atomicAdd(&cnt[L + 1], 1)] = d;
-            }
-        }
-        st = nst;
-        grid.sync();
-    }
+    if (i < nodes) level_nodes[atomicAdd(&cursor[level[i]], 1)] = int(i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1951,15 +1948,32 @@ template <int KF>
 __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
     extern __shared__ int2 bterm[];
     __shared__ Slot ss;
-    __shared__ int nbt;
+    __shared__ int nbt, s_multi, s_total;
+    // staged plane windows of a single-variable slot, per category: lowest and
+    // highest word offset of its terms, and where its window starts
+    __shared__ int s_lo[QSK_CMAX], s_hi[QSK_CMAX], s_base[QSK_CMAX];
     const int b = blockIdx.y;
-    if (threadIdx.x == 0) ss = A.slots[b];
+    if (threadIdx.x == 0) {
+        ss = A.slots[b];
+        nbt = 0;
+        s_multi = 0;
+    }
+    if (threadIdx.x < QSK_CMAX) {
+        s_lo[threadIdx.x] = INT_MAX;
+        s_hi[threadIdx.x] = INT_MIN;
+    }
     __syncthreads();
     if (ss.flags & SLOT_SKIP) return;
     const Geom &g = A.g;
+    const int seg_begin = blockIdx.x * A.segs_per_cta;
+    const int nseg1k = (int)((g.N + 1023) / 1024);
+    int seg_end = seg_begin + A.segs_per_cta;
+    if (seg_end > nseg1k) seg_end = nseg1k;
     {
-        // terms -> (plane offset, flat offset), one thread per term; a code that
-        // is no category of the TI (or a NaN value) reads the all-zero plane QSK_CMAX
+        // terms -> (category, word offset), one thread per term; a code that is
+        // no category of the TI (or a NaN value) matches nowhere and adds
+        // nothing to the counts, so the term is dropped (the count is a sum of
+        // 0/1 matches: its order is free)
         const Term *src = A.terms + (long long)b * A.maxterms;
         const StaticTerm *ssrc = A.sterms ? A.sterms + (long long)b * A.maxterms : nullptr;
         const int N32 = (int)g.N;
@@ -1982,24 +1996,64 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
             const int nc = A.ncat[v];
             for (int q = 0; q < nc; ++q)
                 if (A.catv[v * QSK_CMAX + q] == val) { c = q; break; }
+            if (c == QSK_CMAX) continue;
             // positions 32k..32k+31 read source bits from word k + floor(-d/32),
             // shifted right by (-d) mod 32
-            bterm[t] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw + plane_guard(g.N) + ((-d) >> 5), (-d) & 31);
+            const int off = plane_guard(g.N) + ((-d) >> 5);
+            const int o = atomicAdd(&nbt, 1);
+            if (v > 0) {
+                s_multi = 1;
+                bterm[o] = make_int2((v * (QSK_CMAX + 1) + c) * A.pw + off, (-d) & 31);
+            } else {
+                atomicMin(&s_lo[c], off);
+                atomicMax(&s_hi[c], off);
+                bterm[o] = make_int2(c * A.pw + off, ((-d) & 31) | (c << 8));
+            }
         }
-        if (threadIdx.x == 0) {
-            nbt = ss.nterms;
-            if (ssrc && A.no_verbatim && ss.vtpl >= 0)
-                ss.excl = verbatim_excl(g, A.tpl + ss.vtpl * g.nd, A.id_image[ss.vcell], ss.mn);
-        }
+        if (threadIdx.x == 0 && ssrc && A.no_verbatim && ss.vtpl >= 0)
+            ss.excl = verbatim_excl(g, A.tpl + ss.vtpl * g.nd, A.id_image[ss.vcell], ss.mn);
     }
     __syncthreads();
     const int nt = nbt;
+    // Staging: the words of each category plane that this CTA's segments read
+    // ([lo + 32*seg_begin, hi + 32*seg_end + 1)) go to shared memory, where a
+    // warp's 32 consecutive words are one conflict-free access at any word
+    // alignment (from global memory they span two cache lines).
+    unsigned *stage = reinterpret_cast<unsigned *>(bterm + A.maxterms);
+    if (threadIdx.x < 32) {
+        const int c = threadIdx.x;
+        const int len = s_lo[c] <= s_hi[c] ? s_hi[c] - s_lo[c] + 32 * (seg_end - seg_begin) + 1 : 0;
+        int inc = len;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, inc, off);
+            if (c >= off) inc += y;
+        }
+        s_base[c] = inc - len;
+        if (c == 31) s_total = inc;
+    }
+    __syncthreads();
+    const bool staged = !s_multi && s_total <= A.stage_words && A.stage_words > 0;
+    if (staged) {
+        for (int c = 0; c < QSK_CMAX; ++c) {
+            if (s_lo[c] > s_hi[c]) continue;
+            const int len = s_hi[c] - s_lo[c] + 32 * (seg_end - seg_begin) + 1;
+            const unsigned *src = A.planes + (long long)c * A.pw + s_lo[c] + 32 * seg_begin;
+            unsigned *dst = stage + s_base[c];
+            for (int w = threadIdx.x; w < len; w += blockDim.x) dst[w] = __ldg(src + w);
+        }
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+            const int2 bt = bterm[t];
+            const int c = bt.y >> 8;
+            const int off = bt.x - c * A.pw;
+            bterm[t] = make_int2(s_base[c] + off - s_lo[c] - 32 * seg_begin, bt.y & 31);
+        }
+    } else {
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) bterm[t].y &= 31;
+    }
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const bool emit_masked = (ss.flags & SLOT_EMIT_MASKED) != 0;
-    const int nseg1k = (int)((g.N + 1023) / 1024);
-    const int seg_begin = blockIdx.x * A.segs_per_cta;
-    int seg_end = seg_begin + A.segs_per_cta;
-    if (seg_end > nseg1k) seg_end = nseg1k;
     float *rv = A.rec_val + (long long)b * g.nseg * QSK_SEG;
     int *ri = A.rec_idx + (long long)b * g.nseg * QSK_SEG;
 
@@ -2065,44 +2119,54 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
         // carry-save adders over groups of 8 match words, c3..c7 count eights
         unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
         if (vmask) {
-            const int im0 = int(m0);
-            const unsigned *P = A.planes + (im0 >> 5);
-            auto match = [&](int t) -> unsigned {
-                const int2 bt = bterm[t];
-                return __funnelshift_r(__ldg(P + bt.x), __ldg(P + bt.x + 1), unsigned(bt.y));
+            const int mw = int(m0) >> 5;
+            auto count = [&](auto match) {
+                auto csa = [](unsigned &h, unsigned &l, unsigned a, unsigned b, unsigned c) {
+                    const unsigned u = a ^ b;
+                    h = (a & b) | (u & c);
+                    l = u ^ c;
+                };
+                int t = 0;
+                for (; t + 8 <= nt; t += 8) {
+                    unsigned twosA, twosB, foursA, foursB, eights;
+                    csa(twosA, c0, c0, match(t), match(t + 1));
+                    csa(twosB, c0, c0, match(t + 2), match(t + 3));
+                    csa(foursA, c1, c1, twosA, twosB);
+                    csa(twosA, c0, c0, match(t + 4), match(t + 5));
+                    csa(twosB, c0, c0, match(t + 6), match(t + 7));
+                    csa(foursB, c1, c1, twosA, twosB);
+                    csa(eights, c2, c2, foursA, foursB);
+                    unsigned x = eights, t0;
+                    t0 = c3 & x; c3 ^= x; x = t0;
+                    t0 = c4 & x; c4 ^= x; x = t0;
+                    t0 = c5 & x; c5 ^= x; x = t0;
+                    t0 = c6 & x; c6 ^= x; x = t0;
+                    c7 ^= x;
+                }
+                for (; t < nt; ++t) {
+                    unsigned x = match(t), t0;
+                    t0 = c0 & x; c0 ^= x; x = t0;
+                    t0 = c1 & x; c1 ^= x; x = t0;
+                    t0 = c2 & x; c2 ^= x; x = t0;
+                    t0 = c3 & x; c3 ^= x; x = t0;
+                    t0 = c4 & x; c4 ^= x; x = t0;
+                    t0 = c5 & x; c5 ^= x; x = t0;
+                    t0 = c6 & x; c6 ^= x; x = t0;
+                    c7 ^= x;
+                }
             };
-            auto csa = [](unsigned &h, unsigned &l, unsigned a, unsigned b, unsigned c) {
-                const unsigned u = a ^ b;
-                h = (a & b) | (u & c);
-                l = u ^ c;
-            };
-            int t = 0;
-            for (; t + 8 <= nt; t += 8) {
-                unsigned twosA, twosB, foursA, foursB, eights;
-                csa(twosA, c0, c0, match(t), match(t + 1));
-                csa(twosB, c0, c0, match(t + 2), match(t + 3));
-                csa(foursA, c1, c1, twosA, twosB);
-                csa(twosA, c0, c0, match(t + 4), match(t + 5));
-                csa(twosB, c0, c0, match(t + 6), match(t + 7));
-                csa(foursB, c1, c1, twosA, twosB);
-                csa(eights, c2, c2, foursA, foursB);
-                unsigned x = eights, t0;
-                t0 = c3 & x; c3 ^= x; x = t0;
-                t0 = c4 & x; c4 ^= x; x = t0;
-                t0 = c5 & x; c5 ^= x; x = t0;
-                t0 = c6 & x; c6 ^= x; x = t0;
-                c7 ^= x;
-            }
-            for (; t < nt; ++t) {
-                unsigned x = match(t), t0;
-                t0 = c0 & x; c0 ^= x; x = t0;
-                t0 = c1 & x; c1 ^= x; x = t0;
-                t0 = c2 & x; c2 ^= x; x = t0;
-                t0 = c3 & x; c3 ^= x; x = t0;
-                t0 = c4 & x; c4 ^= x; x = t0;
-                t0 = c5 & x; c5 ^= x; x = t0;
-                t0 = c6 & x; c6 ^= x; x = t0;
-                c7 ^= x;
+            if (staged) {
+                const unsigned *S = stage + mw;
+                count([&](int t) -> unsigned {
+                    const int2 bt = bterm[t];
+                    return __funnelshift_r(S[bt.x], S[bt.x + 1], unsigned(bt.y));
+                });
+            } else {
+                const unsigned *P = A.planes + mw;
+                count([&](int t) -> unsigned {
+                    const int2 bt = bterm[t];
+                    return __funnelshift_r(__ldg(P + bt.x), __ldg(P + bt.x + 1), unsigned(bt.y));
+                });
             }
         }
         // Scores stay bit-sliced: position p of the lane holds the count
@@ -2519,28 +2583,22 @@ cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
     const unsigned nb = (unsigned)((nodes + 255) / 256);
     const long long ntiles = (nodes + 1023) / 1024;
     cudaError_t e;
-    if ((e = cudaMemsetAsync(a.outcnt, 0, sizeof(int) * size_t(nodes), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(a.level, 0xff, sizeof(int) * size_t(nodes), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(a.cnt, 0, sizeof(int) * size_t(nodes + 2), st)) != cudaSuccess) return e;
-    k_dep_count<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell, a.deg,
-                                    a.outcnt);
-    k_scan_tiles<<<(unsigned)ntiles, 1024, 0, st>>>(nodes, a.outcnt, a.outstart, a.tile_sum);
-    k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);
-    k_scan_add<<<(unsigned)((nodes + 1 + 255) / 256), 256, 0, st>>>(nodes, a.outstart, a.cursor, a.tile_sum);
-    k_adj_fill<<<nb, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell, a.cursor,
-                                   a.adj);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    int dev = 0, sms = 0, per_sm = 0;
+    int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kahn, 256, 0)) != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-    // one or two co-resident blocks per SM: per-level work is small, barriers cheap
-    long long blocks = (long long)sms * (per_sm < 2 ? per_sm : 2);
-    if (blocks > (long long)nb) blocks = nb;
-    int *deg = a.deg, *level_nodes = a.level_nodes, *cnt = a.cnt, *start = a.start, *nl_out = a.nl_out;
-    const int *outstart = a.outstart, *adj = a.adj;
-    void *args[] = {&nodes, &deg, &outstart, &adj, &level_nodes, &cnt, &start, &nl_out};
-    return cudaLaunchCooperativeKernel((const void *)k_kahn, dim3((unsigned)blocks), dim3(256), args, 0, st);
+    long long blocks = (long long)sms * 8;
+    const long long need = (nodes * 32 + 255) / 256;
+    if (blocks > need) blocks = need;
+    k_level_flow<<<(unsigned)blocks, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell,
+                                                   a.level, a.cnt + nodes + 1, a.nl_out, a.status);
+    k_level_count<<<nb, 256, 0, st>>>(nodes, a.level, a.cnt);
+    k_scan_tiles<<<(unsigned)ntiles, 1024, 0, st>>>(nodes, a.cnt, a.start, a.tile_sum);
+    k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);
+    k_scan_add<<<(unsigned)((nodes + 1 + 255) / 256), 256, 0, st>>>(nodes, a.start, a.cursor, a.tile_sum);
+    k_level_scatter<<<nb, 256, 0, st>>>(nodes, a.level, a.cursor, a.level_nodes);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st) {
@@ -2578,6 +2636,9 @@ cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, co
     return cudaGetLastError();
 }
 
+// shared-memory words for the staged plane windows of k_map_bits (24 KB)
+#define MAP_BITS_STAGE_WORDS 6144
+
 int map_bits_segs_per_cta(const Geom &g, int nslots) {
     long long nseg1k = (g.N + 1023) / 1024;
     long long target = 148LL * 8;
@@ -2587,11 +2648,14 @@ int map_bits_segs_per_cta(const Geom &g, int nslots) {
     return (int)per;
 }
 
-cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st) {
+cudaError_t launch_map_bits(const BitArgs &args, int nslots, int K, int maxterms_in_batch, cudaStream_t st) {
     int threads = 256;
+    BitArgs a = args;
+    if (a.maxterms < maxterms_in_batch) return cudaErrorInvalidValue;
+    a.stage_words = MAP_BITS_STAGE_WORDS;
     long long nseg1k = (a.g.N + 1023) / 1024;
     dim3 grid((unsigned)((nseg1k + a.segs_per_cta - 1) / a.segs_per_cta), (unsigned)nslots);
-    size_t smem = sizeof(int2) * (size_t)(maxterms_in_batch > 0 ? maxterms_in_batch : 1);
+    size_t smem = sizeof(int2) * (size_t)(a.maxterms > 0 ? a.maxterms : 1) + sizeof(unsigned) * (size_t)a.stage_words;
     if (K <= 1) k_map_bits<1><<<grid, threads, smem, st>>>(a);
     else if (K <= 2) k_map_bits<2><<<grid, threads, smem, st>>>(a);
     else if (K <= 4) k_map_bits<4><<<grid, threads, smem, st>>>(a);

@@ -112,21 +112,26 @@ def test_auto_qs_w_cuda_calibration_agrees_with_oracle(oracle):
     kernel = np.exp(-(r[:, None] ** 2 + r[None, :] ** 2) / 20.0).astype(np.float32)
     max_n, dens, max_k, iters = 6, [0.1, 0.5], 2, 1500
     job = 31030
-    outputs = [f"im_{i}_{job}" for i in (1, 2, 3)]
+    # auto_qs ignores -id: its outputs are im_1/2/3_4294967295 (src/auto_qs.cpp:758-760)
+    outputs = [f"im_{i}_4294967295" for i in (1, 2, 3)]
     _cleanup(outputs)
     ref.write_image(f"dropin_ti_{job}", ti, [0])
     ref.write_image(f"dropin_k_{job}", kernel, [0])
     log = f"/tmp/G2S/logs/dropin_{job}.log"
     cmd = [exe, "-ti", f"dropin_ti_{job}", "-ki", f"dropin_k_{job}", "-maxk", str(max_k), "-maxn", str(max_n),
            "-densities"] + [str(d) for d in dens] + ["-maxIter", str(iters), "-minIter", str(iters), "-j", "1",
-                                                   "-W_CUDA", "0", "-id", str(job), "-r", log]
-    p = subprocess.run(cmd, cwd=DROPIN_DIR, capture_output=True, text=True, timeout=600)
+                                                   "-W_CUDA", "0", "-r", log]
+    # auto_qs falls back to CPU devices without a word when the dlopen fails:
+    # the loader's own trace shows that the drop-in and this library were loaded
+    env = dict(os.environ, LD_DEBUG="files")
+    p = subprocess.run(cmd, cwd=DROPIN_DIR, capture_output=True, text=True, timeout=600, env=env)
     text = open(log).read() if os.path.exists(log) else ""
     assert p.returncode == 0, (p.stdout[-2000:], p.stderr[-2000:], text[-2000:])
     assert "could not load" not in text
-    rm = ref.read_image(f"im_1_{job}").astype(np.float64)
-    rd = ref.read_image(f"im_2_{job}").astype(np.float64)
-    rn = ref.read_image(f"im_3_{job}")
+    inits = [ln for ln in p.stderr.splitlines() if "calling init:" in ln]
+    assert any("g2s_cuda.so" in ln for ln in inits) and any("libg2s_b200.so" in ln for ln in inits), inits[-20:]
+    rm, rd, rn = (ref.read_image(name) for name in outputs)
+    rm, rd = rm.astype(np.float64), rd.astype(np.float64)
     rn = (rn.view(np.uint32) if rn.dtype == np.float32 else rn).astype(np.float64)
     _cleanup(outputs + [f"dropin_ti_{job}", f"dropin_k_{job}"])
     counts = np.arange(1, max_n, dtype=np.uint32)[:, None]
