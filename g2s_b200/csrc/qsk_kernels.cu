@@ -924,8 +924,7 @@ __device__ __forceinline__ void mt_seed(unsigned *mt, float sd) {
 #define TAB_CAP 128           // segments of one tie super-run
 #define RNG_BUF (2 * REC_CAP + 640)   // draws of one super-run + one block
 #define SEG_WIN 256           // record counts and maxima of SEG_WIN segments staged per warp
-#define TEAM_MAX 8            // warps of one slot's team (small batches)
-#define TEAM_SLOTS 296        // batches up to this many slots get a team of TEAM_MAX warps per slot
+#define TEAM_MAX 8            // warps of one slot's team
 
 struct __align__(16) WarpShared {
     float rv_s[REC_CAP];      // super-run records (values), 16-byte aligned for cp.async
@@ -1670,9 +1669,9 @@ __device__ int replay_tie_stream(int K, float V, int xes, int sg, int nseg, cons
     }
 }
 
-// W == 1: RP_WARPS slots per CTA, one warp each.  W > 1: one slot per CTA;
-// warp 0 replays it and the other W-1 warps join it for the MT19937 blocks
-// and the tie super-runs (small batches, where the GPU would idle otherwise).
+// W == 1: RP_WARPS slots per CTA, one warp each.  W > 1 (what the launcher
+// uses): one slot per CTA; warp 0 replays it and the other W-1 warps join it
+// for the MT19937 blocks and the tie super-runs.
 template <int KM, int W>
 __global__ void __launch_bounds__(W == 1 ? 32 * RP_WARPS : 32 * W) k_replay(ReplayArgs A) {
     extern __shared__ __align__(16) unsigned char rp_smem[];
@@ -2115,8 +2114,9 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                 }
             }
         }
-        // bit-sliced counter: c0 (ones), c1 (twos), c2 (fours) fed by
-        // carry-save adders over groups of 8 match words, c3..c7 count eights
+        // bit-sliced counter: c0 (ones), c1 (twos), c2 (fours), c3 (eights)
+        // fed by carry-save adders (Harley-Seal) over groups of 16 match
+        // words, c4..c7 count sixteens; a tail of 8 and single words ripples
         unsigned c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0, c6 = 0, c7 = 0;
         if (vmask) {
             const int mw = int(m0) >> 5;
@@ -2127,6 +2127,29 @@ __global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
                     l = u ^ c;
                 };
                 int t = 0;
+                for (; t + 16 <= nt; t += 16) {
+                    unsigned twosA, twosB, foursA, foursB, eightsA, eightsB, sixteens;
+                    csa(twosA, c0, c0, match(t), match(t + 1));
+                    csa(twosB, c0, c0, match(t + 2), match(t + 3));
+                    csa(foursA, c1, c1, twosA, twosB);
+                    csa(twosA, c0, c0, match(t + 4), match(t + 5));
+                    csa(twosB, c0, c0, match(t + 6), match(t + 7));
+                    csa(foursB, c1, c1, twosA, twosB);
+                    csa(eightsA, c2, c2, foursA, foursB);
+                    csa(twosA, c0, c0, match(t + 8), match(t + 9));
+                    csa(twosB, c0, c0, match(t + 10), match(t + 11));
+                    csa(foursA, c1, c1, twosA, twosB);
+                    csa(twosA, c0, c0, match(t + 12), match(t + 13));
+                    csa(twosB, c0, c0, match(t + 14), match(t + 15));
+                    csa(foursB, c1, c1, twosA, twosB);
+                    csa(eightsB, c2, c2, foursA, foursB);
+                    csa(sixteens, c3, c3, eightsA, eightsB);
+                    unsigned x = sixteens, t0;
+                    t0 = c4 & x; c4 ^= x; x = t0;
+                    t0 = c5 & x; c5 ^= x; x = t0;
+                    t0 = c6 & x; c6 ^= x; x = t0;
+                    c7 ^= x;
+                }
                 for (; t + 8 <= nt; t += 8) {
                     unsigned twosA, twosB, foursA, foursB, eights;
                     csa(twosA, c0, c0, match(t), match(t + 1));
@@ -2690,39 +2713,20 @@ cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cuda
 }
 
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
-    static bool configured[64] = {};
-    const size_t smem = sizeof(WarpShared) * RP_WARPS;
+    // One CTA per slot: a team of TEAM_MAX warps (warp 0 replays, the others
+    // help with the generator blocks and the tie super-runs) around one
+    // shared state of ~25 KB.  Eight teams fit an SM; one warp per slot with
+    // a state of its own fits only eight warps on an SM, and measured slower
+    // at every batch size of the simulations.
     const size_t smem_team = sizeof(WarpShared);
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!configured[dev]) {
-        if ((e = cudaFuncSetAttribute(k_replay<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) ||
-            (e = cudaFuncSetAttribute(k_replay<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
-            return e;
-        configured[dev] = true;
-    }
-    if (a.nslots <= TEAM_SLOTS) {
-        // small batch: a team of TEAM_MAX warps per slot
-        const unsigned blocks = (unsigned)a.nslots;
-        constexpr int T = TEAM_MAX;
-        if (a.K <= 1) k_replay<1, T><<<blocks, 32 * T, smem_team, st>>>(a);
-        else if (a.K <= 2) k_replay<2, T><<<blocks, 32 * T, smem_team, st>>>(a);
-        else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem_team, st>>>(a);
-        else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem_team, st>>>(a);
-        else k_replay<16, T><<<blocks, 32 * T, smem_team, st>>>(a);
-        return cudaGetLastError();
-    }
-    unsigned blocks = (unsigned)((a.nslots + RP_WARPS - 1) / RP_WARPS);
-    if (a.K <= 1) k_replay<1, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 2) k_replay<2, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 4) k_replay<4, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else if (a.K <= 8) k_replay<8, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
-    else k_replay<16, 1><<<blocks, 32 * RP_WARPS, smem, st>>>(a);
+    if (a.nslots <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)a.nslots;
+    constexpr int T = TEAM_MAX;
+    if (a.K <= 1) k_replay<1, T><<<blocks, 32 * T, smem_team, st>>>(a);
+    else if (a.K <= 2) k_replay<2, T><<<blocks, 32 * T, smem_team, st>>>(a);
+    else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem_team, st>>>(a);
+    else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem_team, st>>>(a);
+    else k_replay<16, T><<<blocks, 32 * T, smem_team, st>>>(a);
     return cudaGetLastError();
 }
 
