@@ -1943,8 +1943,10 @@ __device__ __forceinline__ unsigned bits_range(int a, int b) {
     return hi & ~((1u << a) - 1u);
 }
 
+// K <= 4: at most 42 registers, 48 warps per SM (measured faster than 48
+// registers and 40 warps); the wider top-K states would spill under that cap
 template <int KF>
-__global__ void __launch_bounds__(256) k_map_bits(BitArgs A) {
+__global__ void __launch_bounds__(256, KF <= 4 ? 6 : 1) k_map_bits(BitArgs A) {
     extern __shared__ int2 bterm[];
     __shared__ Slot ss;
     __shared__ int nbt, s_multi, s_total;
@@ -2712,21 +2714,46 @@ cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cuda
     return cudaGetLastError();
 }
 
-cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
-    // One CTA per slot: a team of TEAM_MAX warps (warp 0 replays, the others
-    // help with the generator blocks and the tie super-runs) around one
-    // shared state of ~25 KB.  Eight teams fit an SM; one warp per slot with
-    // a state of its own fits only eight warps on an SM, and measured slower
-    // at every batch size of the simulations.
-    const size_t smem_team = sizeof(WarpShared);
-    if (a.nslots <= 0) return cudaSuccess;
+template <int T>
+static void launch_replay_team(const ReplayArgs &a, size_t smem, cudaStream_t st) {
     const unsigned blocks = (unsigned)a.nslots;
-    constexpr int T = TEAM_MAX;
-    if (a.K <= 1) k_replay<1, T><<<blocks, 32 * T, smem_team, st>>>(a);
-    else if (a.K <= 2) k_replay<2, T><<<blocks, 32 * T, smem_team, st>>>(a);
-    else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem_team, st>>>(a);
-    else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem_team, st>>>(a);
-    else k_replay<16, T><<<blocks, 32 * T, smem_team, st>>>(a);
+    if (a.K <= 1) k_replay<1, T><<<blocks, 32 * T, smem, st>>>(a);
+    else if (a.K <= 2) k_replay<2, T><<<blocks, 32 * T, smem, st>>>(a);
+    else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem, st>>>(a);
+    else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem, st>>>(a);
+    else k_replay<16, T><<<blocks, 32 * T, smem, st>>>(a);
+}
+
+cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
+    // One CTA per slot: a team of warps (warp 0 replays, the others help
+    // with the generator blocks and the tie super-runs) around one shared
+    // state of ~25 KB.  Teams of eight while every slot of the batch gets an
+    // SM slot at once (registers allow 4 such CTAs per SM); larger batches
+    // take teams of four, 8 CTAs per SM, so that they still run in one wave
+    // up to 1184 slots.  A warp per slot with a state of its own (8 warps per
+    // SM) measured slower at every batch size of the simulations.
+    static int wave8[64][5] = {};
+    const size_t smem = sizeof(WarpShared);
+    if (a.nslots <= 0) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    const int kc = a.K <= 1 ? 0 : a.K <= 2 ? 1 : a.K <= 4 ? 2 : a.K <= 8 ? 3 : 4;
+    if (wave8[dev][kc] == 0) {
+        int sms = 0, per_sm = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        const void *fn = kc == 0   ? (const void *)k_replay<1, TEAM_MAX>
+                         : kc == 1 ? (const void *)k_replay<2, TEAM_MAX>
+                         : kc == 2 ? (const void *)k_replay<4, TEAM_MAX>
+                         : kc == 3 ? (const void *)k_replay<8, TEAM_MAX>
+                                   : (const void *)k_replay<16, TEAM_MAX>;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * TEAM_MAX, smem)) != cudaSuccess)
+            return e;
+        wave8[dev][kc] = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    if (a.nslots <= wave8[dev][kc]) launch_replay_team<TEAM_MAX>(a, smem, st);
+    else launch_replay_team<TEAM_MAX / 2>(a, smem, st);
     return cudaGetLastError();
 }
 
