@@ -45,7 +45,7 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) per launch, averaged over every launch of one
 # step of the default workload, from one ncu capture of this script
 # (dram__bytes_read.sum + dram__bytes_write.sum; cold-cache, launches serialised)
-TRAFFIC_PER_LAUNCH = {("config1", "k_replay"): 14.51e6, ("config1", "k_map_bits"): 11.91e6}
+TRAFFIC_PER_LAUNCH = {("config1", "k_replay"): 14.54e6, ("config1", "k_map_bits"): 12.07e6}
 
 
 def peaks():
