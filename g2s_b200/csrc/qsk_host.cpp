@@ -1082,6 +1082,17 @@ void collect_profile(qsk_sim *s) {
     s->info.ms_replay = rep;
 }
 
+// records for the largest batch a run launches (its largest level, cut at
+// the slot budget), allocated when the levels are known: a run that needs
+// fewer slots than the budget allows never maps the whole budget
+int sim_records(qsk_sim *s, long long slots) {
+    const int n = int(std::max<long long>(1, std::min<long long>(slots, s->max_slots)));
+    cudaError_t e = ensure_records(s->ti->g, n, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "records: %s", cudaGetErrorString(e));
+    return QSK_OK;
+}
+
 int sim_check_status(qsk_sim *s) {
     int st = 0;
     CK(cudaMemcpyAsync(&st, s->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, s->st));
@@ -1274,8 +1285,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         (e = s->d_mt_pre.alloc(size_t(2) * s->max_slots)) != cudaSuccess ||
         (s->use_bits && ((e = s->d_sslots.alloc(size_t(2) * s->max_slots)) != cudaSuccess ||
                          (e = s->d_sterms.alloc(size_t(2) * s->max_slots * s->maxterms)) != cudaSuccess)) ||
-        (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess ||
-        (e = ensure_records(g, s->max_slots, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max)) != cudaSuccess)
+        (e = s->d_terms.alloc(size_t(s->max_slots) * s->maxterms)) != cudaSuccess)
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "scratch: %s",
                          cudaGetErrorString(e)));
     if ((size_t)s->maxterms * sizeof(Term) > 200 * 1024) return bail(fail(QSK_ERR_UNSUPPORTED, "n*nvar too large"));
@@ -1337,13 +1347,15 @@ int qsk_sim_run(qsk_sim *s) {
     if (s->nodes > 0 && (nl < 1 || start[size_t(nl)] != s->nodes))
         return fail(QSK_ERR_DEVICE, "dependency levels cover %d of %lld nodes", nl > 0 ? start[size_t(nl)] : 0,
                     s->nodes);
+    int mb = 0;
+    for (int l = 0; l < nl; ++l) mb = std::max(mb, start[l + 1] - start[l]);
+    rc = sim_records(s, mb);
+    if (rc) return rc;
     CK(cudaEventRecord(ev[2], s->st));
     rc = sim_batches(s, start, false);
     if (rc) return rc;
     CK(cudaEventRecord(ev[3], s->st));
     CK(cudaEventSynchronize(ev[3]));
-    int mb = 0;
-    for (int l = 0; l < nl; ++l) mb = std::max(mb, start[l + 1] - start[l]);
     s->info.levels = nl;
     s->info.max_batch = mb;
     cudaEventElapsedTime(&s->info.ms_setup_neighbours, ev[0], ev[1]);
@@ -1372,6 +1384,8 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
     std::iota(ident.begin(), ident.end(), 0);
     CK(cudaMemcpyAsync(s->d_level_nodes.p, ident.data(), sizeof(int) * s->nodes, cudaMemcpyHostToDevice, s->st));
     std::vector<int> start = {0, int(s->nodes)};
+    rc = sim_records(s, s->nodes);
+    if (rc) return rc;
     rc = sim_batches(s, start, true);
     if (rc) return rc;
     s->info.nodes = s->nodes;
