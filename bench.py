@@ -28,6 +28,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -63,7 +64,7 @@ class ClockSampler:
     def __init__(self, index: int = 0):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(os.environ.get("QSK_CLOCKS_DIR", tempfile.gettempdir()), f"clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -265,9 +266,9 @@ def main():
     value = whole_job_rate(nodes, args.steps, ws, total_ms)
 
     # roofline of the dominant kernel: one extra profiled step records events
-    # around every launch.  Algorithmic bytes per node (survey of the
-    # reference path): the fused map reads 4*N*L bytes of correlation layers,
-    # the k-best scan 4*N bytes of scores.
+    # around every launch.  Algorithmic bytes per node of the reference
+    # path: the fused map reads 4*N*L bytes of correlation layers, the k-best
+    # scan 4*N bytes of scores.
     sim.set_profiling(True)
     sim.run()
     pinf = sim.info()
