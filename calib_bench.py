@@ -6,7 +6,7 @@ kernel, max_k 1, power 2) and pruning off (min iterations = max
 iterations), so both arms search every setup every iteration.  Prints one
 JSON line: searches per second of each arm.
 
-    python -m g2s_b200.calib_bench [--iterations 200] [--ref-iterations 100]
+    python calib_bench.py [--iterations 200] [--ref-iterations 100]
 
 The reference needs at least 100 iterations (its progress report divides the
 iteration counter by max_iterations/100).
@@ -17,9 +17,12 @@ import os
 import subprocess
 import time
 
+import sys
+
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
 
 
 def main():

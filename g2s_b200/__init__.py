@@ -92,6 +92,9 @@ SIGNATURES = {
     "qsk_pattern_kbest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_int,
                                                  ctypes.POINTER(QskTerm), ctypes.c_uint, ctypes.c_float, _f32p, _u32p,
                                                  _i32p]),
+    "qsk_tc_topk": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
+                                   ctypes.c_void_p, ctypes.c_void_p, _f32p, _f32p, _f32p, _u32p, _i32p, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _u32p]),
     "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_position_to_index": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,
@@ -103,6 +106,7 @@ SIGNATURES = {
     "qsk_sim_get_path": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f32p, _u32p]),
     "qsk_sim_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_sim_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "qsk_sim_set_level_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_longlong]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
     "qsk_set_map_mode": (ctypes.c_int, [ctypes.c_int]),
@@ -381,6 +385,12 @@ class Simulation:
         _check(lib().qsk_sim_set_profiling(self.handle, int(on)), "qsk_sim_set_profiling")
         return self
 
+    def set_level_wait(self, spin_limit: int = 0, hold_node: int = -1):
+        """Bound of the dependency-level waits (polls; 0 = default) and, for
+        failure-path tests, a path node whose level is never published."""
+        _check(lib().qsk_sim_set_level_wait(self.handle, int(spin_limit), int(hold_node)), "qsk_sim_set_level_wait")
+        return self
+
     def run_teacher(self, completed: np.ndarray, index: Optional[np.ndarray] = None):
         c = np.ascontiguousarray(completed, dtype=np.float32)
         ix = None if index is None else np.ascontiguousarray(index, dtype=np.uint32).ravel()
@@ -422,6 +432,30 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+def tc_topk(queries: np.ndarray, rows: np.ndarray, fmt: int, X: int, Y: int, box: np.ndarray, W: int = 8,
+            ranges: int = 1, q_scale=None, q_bias=None, p_scale=None, q_seed=None, device: int = 0):
+    """Top-W inner products on the tensor cores (qsk_tc_topk).  ``queries``
+    (B x K) and ``rows`` (N x K) hold bit patterns: uint16 BF16 (fmt 0) or
+    uint8 FP8 E4M3 (fmt 1).  Returns (keys, positions), each [B, ranges, W]."""
+    q = np.ascontiguousarray(queries)
+    r = np.ascontiguousarray(rows)
+    want = np.uint16 if fmt == 0 else np.uint8
+    if q.dtype != want or r.dtype != want or q.ndim != 2 or r.ndim != 2 or q.shape[1] != r.shape[1]:
+        raise ValueError("queries/rows: 2-D bit-pattern arrays of one K (uint16 BF16 or uint8 FP8)")
+    B, K = q.shape
+    N = r.shape[0]
+    bx = np.ascontiguousarray(box, dtype=np.int32).reshape(B, 6)
+    f = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+    qs_, qb_, ps_ = f(q_scale), f(q_bias), f(p_scale)
+    sd = None if q_seed is None else np.ascontiguousarray(q_seed, dtype=np.uint32)
+    keys = np.zeros((B, ranges, W), np.uint64)
+    pos = np.zeros((B, ranges, W), np.uint32)
+    _check(lib().qsk_tc_topk(device, fmt, B, N, K, q.ctypes.data, r.ctypes.data, _p(qs_, _f32p), _p(qb_, _f32p),
+                             _p(ps_, _f32p), _p(sd, _u32p), _p(bx, _i32p), X, Y, W, ranges,
+                             keys.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)), _p(pos, _u32p)), "qsk_tc_topk")
+    return keys, pos
 
 
 def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,

@@ -20,7 +20,7 @@ LIB = os.path.join(PKG, "libg2s_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["qsk_kernels.cu", "qsk_host.cpp", "qsk_bgrid.cpp"]
+SOURCES = ["qsk_kernels.cu", "qsk_tc.cu", "qsk_host.cpp", "qsk_tensor.cpp", "qsk_bgrid.cpp"]
 
 
 def _run(cmd):
@@ -37,6 +37,7 @@ def _stale(target, deps):
 
 def build_lib(force: bool = False) -> str:
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "qsk_internal.h"),
+                                                       os.path.join(CSRC, "qsk_host_util.h"),
                                                        os.path.join(ROOT, "include", "g2s_b200.h")]
     if not force and not _stale(LIB, deps):
         return LIB
@@ -73,13 +74,19 @@ def build_cli() -> str:
 DROPIN = os.path.join(PKG, "dropin")
 
 
-def build_dropin(g2s_tree: str = "/root/reference") -> str:
+def g2s_sources() -> str:
+    """The G2S source tree: $G2S_SOURCES, else a `reference` directory beside
+    this repository (where it lies when the build runs next to it)."""
+    return os.environ.get("G2S_SOURCES") or os.path.join(os.path.dirname(ROOT), "reference")
+
+
+def build_dropin(g2s_tree: str = "") -> str:
     """g2s_cuda.so for G2S `qs -W_CUDA`: compiled with the G2S host compiler
     against the G2S headers (its AcceleratorDevice class), linked to
     libg2s_b200.so found next to it ($ORIGIN/..)."""
     build_lib()
     out = os.path.join(DROPIN, "g2s_cuda.so")
-    inc = os.path.join(g2s_tree, "include")
+    inc = os.path.join(g2s_tree or g2s_sources(), "include")
     if not os.path.isdir(inc):
         raise FileNotFoundError(f"G2S headers not found under {inc}")
     _run([HOSTCXX, "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-w", "-DG2S_PATH_INDEX_TYPE=unsigned",

@@ -22,6 +22,7 @@
 
 #include "../../include/g2s_b200.h"
 #include "qsk_internal.h"
+#include "qsk_host_util.h"
 
 using namespace qsk;
 
@@ -64,47 +65,6 @@ namespace {
         }                                                                                                 \
     } while (0)
 
-template <typename T>
-struct DBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    DBuf() = default;
-    DBuf(const DBuf &) = delete;
-    DBuf &operator=(const DBuf &) = delete;
-    ~DBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    cudaError_t alloc(size_t count) {
-        release();
-        if (count == 0) count = 1;
-        cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
-        if (e == cudaSuccess) n = count;
-        else p = nullptr;
-        return e;
-    }
-    cudaError_t ensure(size_t count) { return count <= n ? cudaSuccess : alloc(count); }
-    cudaError_t upload(const T *h, size_t count, cudaStream_t st) {
-        cudaError_t e = ensure(count);
-        if (e != cudaSuccess) return e;
-        return cudaMemcpyAsync(p, h, sizeof(T) * count, cudaMemcpyHostToDevice, st);
-    }
-};
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 // smallest size >= s of the form 7-smooth times optionally one 11 or 13
 // (G2S src/sharedMemoryManager.cpp:26-58)
@@ -726,6 +686,8 @@ struct qsk_sim {
     qsk_sim_info info;
     bool neighbours_ready = false;
     bool profiling = false;
+    unsigned level_spin_limit = 0;      // 0: the kernel's default
+    long long level_hold = -1;          // failure-path test: a node whose level is never published
     std::vector<cudaEvent_t> prof_ev;   // 4 events per batch in profiling mode
     size_t prof_used = 0;
 };
@@ -1332,6 +1294,8 @@ int qsk_sim_run(qsk_sim *s) {
     la.level_nodes = s->d_level_nodes.p;
     la.start = s->d_start.p;
     la.nl_out = s->d_nl.p;
+    la.spin_limit = s->level_spin_limit;
+    la.hold = s->level_hold;
     CK(cudaMemsetAsync(s->d_nl.p, 0, sizeof(int), s->st));
     CK(launch_levels(la, s->st));
     s->info.launches += 7;  // neighbours, level pass, count, 3 scan passes, scatter
@@ -1426,6 +1390,14 @@ int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *
 int qsk_sim_set_profiling(qsk_sim *s, int on) {
     if (!s) return fail(QSK_ERR_ARG, "null sim");
     s->profiling = on != 0;
+    return QSK_OK;
+}
+
+int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    if (hold_node < -1 || hold_node >= s->nodes) return fail(QSK_ERR_ARG, "hold node %lld of %lld", hold_node, s->nodes);
+    s->level_spin_limit = spin_limit;
+    s->level_hold = hold_node;
     return QSK_OK;
 }
 

@@ -85,6 +85,7 @@ enum DevStatus : int {
     DEV_BAD_INDEX = 1,
     DEV_TOO_MANY_TERMS = 2,
     DEV_LEVEL_WAIT = 3,       // a dependency level did not appear within the wait limit
+    DEV_TC_WAIT = 4,          // a tensor-core kernel's pipeline wait ran out (kernel returned early)
 };
 
 // Grid (destination image) description for the neighbour search.
@@ -244,6 +245,8 @@ struct LevelArgs {
     int *start;         // nodes + 1: level L is level_nodes[start[L] .. start[L+1])
     int *nl_out;        // 1: number of levels
     int *status;        // DevStatus
+    unsigned spin_limit = 0;   // polls of one dependency before DEV_LEVEL_WAIT (0: 2^22)
+    long long hold = -1;       // node whose level is never published (failure-path test), -1 none
 };
 cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st);
 cudaError_t launch_prep_sim(const SimPrepArgs &a, cudaStream_t st);
@@ -259,5 +262,133 @@ cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
 cudaError_t launch_radius_mask(const int *center, const float *radius, int nslots, const Geom &g, unsigned *mask,
                                long long xwords, cudaStream_t st);
 cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// tensor-core shortlist (qsk_tc.cu): D = A * P^T on tcgen05 for 128-row tiles
+// of A (nodes / queries) against 256-row tiles of P (TI positions), K in
+// 128-byte blocks (64 BF16 or 128 FP8 E4M3 values); per A row and position
+// range the W largest scores (acc * node_scale * pos_scale + node_bias) whose
+// position lies in the row's validity box are kept.
+// ---------------------------------------------------------------------------
+struct TcArgs {
+    int n_nodes;               // live rows of A
+    long long n_pos;           // live rows of P
+    long long n_tiles;         // position tiles of 256 rows
+    int ranges;                // position ranges (grid.y)
+    int tiles_per_range;
+    int kblocks;               // K blocks of A and P
+    const int *tile_kblocks;   // per 128-row tile of A: K blocks used (null: kblocks)
+    int k_per_block;           // elements per K block (set by the launcher)
+    const float *node_scale;   // per A row (null: 1)
+    const float *node_bias;    // per A row (null: 0)
+    const float *pos_scale;    // per P row (null: 1)
+    const unsigned *node_seed; // per A row tie-break seed (null: 0)
+    const int *node_box;       // per A row: x0, x1, y0, y1, z0, z1 (p valid iff x0 <= x < x1, ...)
+    int X, Y;                  // P row p is TI cell (x, y, z), x fastest
+    unsigned long long *out_key;   // [row][range][W]: (ordered score << 32) | tie hash; 0 = empty
+    unsigned *out_pos;             // [row][range][W]
+    int *status;
+};
+int tc_supported_width(int w);
+// kind 0: BF16 (kind::f16), 1: FP8 E4M3 (kind::f8f6f4); a_rows % 128 == 0,
+// p_rows % 256 == 0, k_elems * element size % 128 == 0
+cudaError_t launch_tc_shortlist(int kind, int W, const void *a_mat, long long a_rows, const void *p_mat,
+                                long long p_rows, long long k_elems, const TcArgs &args, cudaStream_t st);
+// Tensor-core form inside the simulation.  Pattern matrix P: one row per TI
+// cell p (natural order, x fastest; rows padded to 256), row length Kp with
+// column j * L + l = layer l at cell p + o_j for the first T template
+// offsets (0 outside the TI), in BF16 or FP8 E4M3 (rows scaled to their
+// largest magnitude).  Layers: a continuous variable gives t^2 and t, a
+// categorical one an indicator per category code.
+#define QSK_TC_MAXL 64
+struct TcLayer {
+    int var;
+    int kind;     // 0: t^2, 1: t, 2: [t == code]
+    float code;
+};
+struct TcPatternArgs {
+    const float *ti;           // raw TI, cells x nvar
+    int nvar, nd;
+    int src[QSK_MAXD];
+    long long N;               // TI cells
+    long long rows;            // padded rows
+    const int *tpl;            // template offsets (ntpl x nd)
+    int T, L;
+    TcLayer layer[QSK_TC_MAXL];
+    long long Kp;
+    int fmt;                   // 0 BF16, 1 FP8 E4M3
+    void *P;
+    float *pos_scale;          // FP8: per row
+};
+struct TcNodeArgs {
+    int nd, nvar;
+    int src[QSK_MAXD];
+    const int *nodes;          // slot -> path index
+    int nslots;
+    const unsigned *path;
+    unsigned begin;
+    const int *nb_count;
+    const int *nb_tpl;
+    const unsigned *nb_cell;
+    int n;
+    const int *tpl;
+    const float *wtab;
+    const float *state, *init, *seeds;
+    const int *types;
+    const int *var_layer0;     // first pattern layer of each variable
+    const int *var_ncat;       // categorical: codes per variable
+    const float *var_catv;     // [var][QSK_CMAX]
+    int L;
+    long long Kp;
+    int fmt;
+    void *A;                   // slot rows x Kp (zeroed by the caller)
+    float *node_scale;
+    int *node_box;
+    unsigned *node_seed;
+};
+struct TcSelectArgs {
+    Geom g;
+    const Slot *slots;
+    const Term *terms;
+    int maxterms;
+    int nslots;
+    const float *layers;                 // FP32 flipped layers (exact scores)
+    const unsigned long long *cand_key;  // [slot][ncand]
+    const unsigned *cand_pos;
+    int ncand;                           // ranges x W
+    int S;                               // candidates scored exactly (<= 64)
+    int fp64;                            // rank by the FP64 exact score
+    const float *ti;
+    int nvar;
+    unsigned nti, ti_id;
+    float *state;
+    unsigned *id_image;
+    unsigned *node_cell;
+    float *drawn_score;                  // per path node: FP32 exact score of the draw
+    float *drawn_scale;                  // per path node: its term scale
+    unsigned *err_max;                   // float bits: largest |approx - FP64| / scale
+    double *err_sum;
+    unsigned long long *err_n;
+    int *status;
+};
+cudaError_t launch_tc_pattern(const TcPatternArgs &a, cudaStream_t st);
+cudaError_t launch_tc_tmax(long long nodes, int n, const int *nb_count, const int *nb_tpl, int *tmax, cudaStream_t st);
+cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st);
+cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st);
+cudaError_t launch_tc_audit(int n, const int *nodes, int K, const float *plain_val, const float *drawn_score,
+                            const float *drawn_scale, float tol, unsigned long long *counts, cudaStream_t st);
+
+// 32-bit mix of a node seed and a position: the tie-break part of a
+// shortlist key (equal scores are ordered by it, uniformly at random over
+// positions for a given seed)
+__host__ __device__ inline unsigned tie_hash(unsigned seed, unsigned pos) {
+    unsigned x = seed ^ (pos * 0x9E3779B9u);
+    x ^= x >> 16;
+    x *= 0x7FEB352Du;
+    x ^= x >> 15;
+    x *= 0x846CA68Bu;
+    x ^= x >> 16;
+    return x;
+}
 
 }  // namespace qsk

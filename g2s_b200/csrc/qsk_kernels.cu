@@ -275,18 +275,21 @@ __device__ __forceinline__ void for_each_dep(long long i, int j, int n, const un
         }
 }
 
-#define LEVEL_SPIN_LIMIT (1u << 22)   // polls of one dependency (about a second with the back-off)
-
 // One warp per node, nodes taken in path order from a ticket.  A node's
 // dependencies have smaller path indices, so they were taken earlier by warps
 // that are running; the smallest unfinished node waits on finished nodes only,
-// so every wait ends.  The waits are bounded all the same: past the limit the
-// kernel records DEV_LEVEL_WAIT and moves on (the host then fails the run).
+// so every wait ends.  The waits are bounded all the same: past `spin_limit`
+// polls of one dependency (2^22 by default, about a second with the back-off)
+// the kernel records DEV_LEVEL_WAIT and moves on (the host then fails the
+// run).  `hold` (normally -1) names a node whose level is never published:
+// a host-side injection that makes its dependants' waits run out, so that the
+// failure path can be exercised without a fault.
 // The level words start at -1; a level is published with one volatile store
 // and read with volatile loads (it carries no other data).
 __global__ void k_level_flow(long long nodes, int n, const int *__restrict__ nb_count,
                              const unsigned *__restrict__ nb_cell, const unsigned char *__restrict__ nb_mask, int nvar,
-                             const int *__restrict__ node_of, int *level, int *ticket, int *nl_out, int *status) {
+                             const int *__restrict__ node_of, int *level, int *ticket, int *nl_out, int *status,
+                             unsigned spin_limit, long long hold) {
     const int lane = threadIdx.x & 31;
     volatile int *vlevel = level;
     for (;;) {
@@ -306,7 +309,7 @@ __global__ void k_level_flow(long long nodes, int n, const int *__restrict__ nb_
                 int lv = vlevel[d];
                 unsigned spins = 0;
                 while (lv < 0) {
-                    if (++spins > LEVEL_SPIN_LIMIT) {
+                    if (++spins > spin_limit) {
                         late = true;
                         lv = 0;
                         break;
@@ -322,15 +325,17 @@ __global__ void k_level_flow(long long nodes, int n, const int *__restrict__ nb_
         if (lane == 0) {
             if (any_bad) atomicExch(status, DEV_BAD_INDEX);
             if (any_late) atomicExch(status, DEV_LEVEL_WAIT);
-            vlevel[i] = mx + 1;
-            atomicMax(nl_out, mx + 2);
+            if ((long long)i != hold) {
+                vlevel[i] = mx + 1;
+                atomicMax(nl_out, mx + 2);
+            }
         }
     }
 }
 
 __global__ void k_level_count(long long nodes, const int *__restrict__ level, int *__restrict__ cnt) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nodes) atomicAdd(&cnt[level[i]], 1);
+    if (i < nodes && level[i] >= 0) atomicAdd(&cnt[level[i]], 1);   // < 0: held back (the run fails)
 }
 
 // exclusive scan in three passes: 1024-element tiles, tile sums, add
@@ -392,7 +397,7 @@ __global__ void k_scan_add(long long count, int *__restrict__ out, int *__restri
 __global__ void k_level_scatter(long long nodes, const int *__restrict__ level, int *__restrict__ cursor,
                                 int *__restrict__ level_nodes) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nodes) level_nodes[atomicAdd(&cursor[level[i]], 1)] = int(i);
+    if (i < nodes && level[i] >= 0) level_nodes[atomicAdd(&cursor[level[i]], 1)] = int(i);
 }
 
 // ---------------------------------------------------------------------------
@@ -2617,7 +2622,8 @@ cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
     const long long need = (nodes * 32 + 255) / 256;
     if (blocks > need) blocks = need;
     k_level_flow<<<(unsigned)blocks, 256, 0, st>>>(nodes, a.n, a.nb_count, a.nb_cell, a.nb_mask, a.nvar, a.node_of_cell,
-                                                   a.level, a.cnt + nodes + 1, a.nl_out, a.status);
+                                                   a.level, a.cnt + nodes + 1, a.nl_out, a.status,
+                                                   a.spin_limit ? a.spin_limit : (1u << 22), a.hold);
     k_level_count<<<nb, 256, 0, st>>>(nodes, a.level, a.cnt);
     k_scan_tiles<<<(unsigned)ntiles, 1024, 0, st>>>(nodes, a.cnt, a.start, a.tile_sum);
     k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);

@@ -1,0 +1,880 @@
+// Tensor-core form of the QuickSampling mismatch map (sm_100a, tcgen05).
+//
+// The cross-correlation part of a node's map, S_b(p) = sum_j sum_l
+// c_{b,j,l} * layer_l(p + o_j), is, for a batch of nodes over a shared
+// template prefix o_0..o_{T-1}, the product of a node matrix A (nodes x K,
+// K = T x L coefficients, zero where a node has no neighbour) with the
+// pattern matrix P (TI positions x K, the layers gathered at every prefix
+// offset: an im2col of the training image).  One launch computes
+// D = A * P^T for a node tile of 128 rows against a range of position tiles
+// and keeps, per node, the W best scores of its range in a heap (the
+// shortlist); nothing of D leaves the SM.
+//
+//   warp 0      TMA producer: A and P tiles (128-byte swizzled K blocks) into
+//               a ring of shared-memory stages, completion on mbarriers
+//   warp 1      TMEM allocation and the MMA issuer: tcgen05.mma (kind::f16
+//               for BF16, kind::f8f6f4 for FP8 E4M3) of M=128 nodes x N=256
+//               positions x K=16/32, FP32 accumulators in TMEM, two buffers
+//               of 256 columns so that the epilogue of tile t overlaps the
+//               MMAs of tile t+1; tcgen05.commit frees stages and buffers
+//   warps 2-5   epilogue: one thread per node (TMEM lane), 32 columns per
+//               tcgen05.ld; score = acc * node_scale * pos_scale + node_bias;
+//               scores at least the heap's minimum go through the full key
+//               (ordered score, 32-bit tie hash of node seed and position),
+//               the node's validity box (the template inside the TI) and a
+//               replace-root/sift-down in shared memory
+//
+// Every mbarrier wait is bounded by a clock budget; on expiry the kernel
+// records DEV_TC_WAIT, drains the copies it issued (bounded too), frees its
+// TMEM and returns.  No cluster, no multicast: every TMA load reads this
+// GPU's own memory into the issuing CTA.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+
+#include "qsk_internal.h"
+
+namespace qsk {
+namespace tc {
+
+constexpr int BM = 128;                  // nodes per CTA tile (TMEM lanes)
+constexpr int BN = 256;                  // positions per tile (accumulator columns)
+constexpr int BKB = 128;                 // bytes of K per block: one 128-byte swizzle row
+constexpr int A_BYTES = BM * BKB;        // 16 KB
+constexpr int B_BYTES = BN * BKB;        // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int THREADS = 192;             // producer, MMA, 4 epilogue warps
+constexpr long long WAIT_CYCLES = 4000000000LL;   // about two seconds at 1.9 GHz
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// wait for the phase of `parity` to complete, at most WAIT_CYCLES; false on expiry
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (abort_flag && *abort_flag) return false;
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major operand tile in the 128-byte swizzle layout written by TMA:
+// rows of 128 bytes, 8-row groups 1024 bytes apart (stride byte offset),
+// leading byte offset unused for this layout, descriptor version 1 (sm_100)
+__device__ __forceinline__ uint64_t sw128_desc(unsigned saddr) {
+    uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// instruction descriptor: FP32 accumulator, A and B of format `fmt`
+// (kind::f16: 1 = BF16; kind::f8f6f4: 0 = E4M3), both K-major, M x N
+__host__ __device__ constexpr unsigned make_idesc(unsigned fmt, int M, int N) {
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | (unsigned(N >> 3) << 17) | (unsigned(M >> 4) << 24);
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma(unsigned tmem_d, uint64_t adesc, uint64_t bdesc, unsigned idesc, unsigned acc) {
+    if constexpr (KIND == 0) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
+            : "memory");
+    }
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 32 consecutive 32-bit columns of TMEM into registers
+__device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32]) {
+    unsigned r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// monotone map of a float to an unsigned (NaN and -inf lowest)
+__device__ __forceinline__ unsigned ordered(float f) {
+    if (f != f) return 0u;
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unordered(unsigned o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+
+template <int KIND, int W, int STAGES>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_tc_shortlist(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_p, TcArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned stage ring (the swizzle atom), then heap and barriers
+    const unsigned raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    uint8_t *sA = smem;                                   // STAGES x A_BYTES
+    uint8_t *sB = smem + STAGES * A_BYTES;                // STAGES x B_BYTES
+    unsigned long long *hk = reinterpret_cast<unsigned long long *>(smem + STAGES * STAGE_BYTES);  // W x BM keys
+    unsigned *hp = reinterpret_cast<unsigned *>(hk + W * BM);                                       // W x BM positions
+    uint64_t *bar = reinterpret_cast<uint64_t *>(hp + W * BM);
+    uint64_t *full = bar, *empty = bar + STAGES, *tfull = bar + 2 * STAGES, *tempty = tfull + 2, *done = tempty + 2;
+    __shared__ unsigned tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile_m = blockIdx.x, range = blockIdx.y;
+    const long long t_begin = (long long)range * a.tiles_per_range;
+    long long t_end = t_begin + a.tiles_per_range;
+    if (t_end > a.n_tiles) t_end = a.n_tiles;
+    const int nkb = a.tile_kblocks ? a.tile_kblocks[tile_m] : a.kblocks;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], 4);
+        }
+        mbar_init(done, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_base_s))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // heap keys start at 0: below every real key (ordered() of a real score is > 0)
+    for (int i = threadIdx.x; i < W * BM; i += THREADS) {
+        hk[i] = 0ull;
+        hp[i] = 0xFFFFFFFFu;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_base_s;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0 && t_begin < t_end && nkb > 0) {
+            int s = 0;
+            unsigned ph = 0;
+            unsigned issued_ph[STAGES];
+            bool pending[STAGES];
+            for (int i = 0; i < STAGES; ++i) pending[i] = false;
+            bool ok = true;
+            for (long long t = t_begin; t < t_end && ok; ++t) {
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(&empty[s], ph ^ 1u, &abort_s)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], STAGE_BYTES);
+                    tma_load_2d(sA + s * A_BYTES, &map_a, &full[s], kb * a.k_per_block, tile_m * BM);
+                    tma_load_2d(sB + s * B_BYTES, &map_p, &full[s], kb * a.k_per_block, (int)(t * BN));
+                    pending[s] = true;
+                    issued_ph[s] = ph;
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicExch(a.status, DEV_TC_WAIT);
+                abort_s = 1;
+            }
+            // every copy issued has landed before the CTA may leave
+            for (int i = 0; i < STAGES; ++i)
+                if (pending[i]) mbar_wait(&full[i], issued_ph[i], nullptr);
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0 && t_begin < t_end && nkb > 0) {
+            constexpr unsigned idesc = make_idesc(KIND == 0 ? 1u : 0u, BM, BN);
+            constexpr int KSTEPS = 4;   // 128-byte K block / 32 bytes per MMA
+            int s = 0;
+            unsigned ph = 0;
+            bool ok = true;
+            int i = 0;
+            for (long long t = t_begin; t < t_end && ok; ++t, ++i) {
+                const int b = i & 1;
+                const unsigned tph = (unsigned)(i >> 1) & 1u;
+                if (!mbar_wait(&tempty[b], tph ^ 1u, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const unsigned dcol = tmem + (unsigned)(b * BN);
+                for (int kb = 0; kb < nkb; ++kb) {
+                    if (!mbar_wait(&full[s], ph, &abort_s)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint64_t ad = sw128_desc(smem_u32(sA + s * A_BYTES));
+                    const uint64_t bd = sw128_desc(smem_u32(sB + s * B_BYTES));
+#pragma unroll
+                    for (int k = 0; k < KSTEPS; ++k)
+                        mma<KIND>(dcol, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), idesc, (kb | k) != 0);
+                    mma_commit(&empty[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                if (ok) mma_commit(&tfull[b]);
+            }
+            if (!ok) {
+                atomicExch(a.status, DEV_TC_WAIT);
+                abort_s = 1;
+            }
+            // every MMA issued has completed before the TMEM is freed
+            mma_commit(done);
+            mbar_wait(done, 0, nullptr);
+        }
+    } else {
+        // ---------------- epilogue: one thread per node ----------------
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        const int node = tile_m * BM + row;
+        const bool live = node < a.n_nodes;
+        float nscale = 1.f, nbias = 0.f;
+        unsigned nseed = 0;
+        int box[6] = {0, 0, 0, 0, 0, 0};
+        if (live) {
+            if (a.node_scale) nscale = a.node_scale[node];
+            if (a.node_bias) nbias = a.node_bias[node];
+            nseed = a.node_seed ? a.node_seed[node] : 0u;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) box[d] = a.node_box[node * 6 + d];
+        }
+        unsigned long long *myk = hk + row;
+        unsigned *myp = hp + row;
+        unsigned long long root = 0ull;
+        float thr = -INFINITY;
+        int i = 0;
+        for (long long t = t_begin; t < t_end; ++t, ++i) {
+            const int b = i & 1;
+            const unsigned tph = (unsigned)(i >> 1) & 1u;
+            bool ok = mbar_wait(&tfull[b], tph, &abort_s);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) {
+                if (lane == 0) {
+                    atomicExch(a.status, DEV_TC_WAIT);
+                    abort_s = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            const long long pos0 = t * BN;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                float v[32];
+                tmem_ld32(tmem + ((unsigned)(q * 32) << 16) + (unsigned)(b * BN + c * 32), v);
+                if (!live) continue;
+                const long long pc = pos0 + c * 32;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const long long p = pc + j;
+                    if (p >= a.n_pos) break;
+                    const float ps = a.pos_scale ? __ldg(a.pos_scale + p) : 1.f;
+                    const float sc = fmaf(v[j], nscale * ps, nbias);
+                    if (sc >= thr) {
+                        const unsigned long long key =
+                            ((unsigned long long)ordered(sc) << 32) | tie_hash(nseed, (unsigned)p);
+                        if (key > root) {
+                            // validity: the node's template lies inside the TI at p
+                            const int x = (int)(p % a.X);
+                            const long long yz = p / a.X;
+                            const int y = (int)(yz % a.Y), z = (int)(yz / a.Y);
+                            if (x >= box[0] && x < box[1] && y >= box[2] && y < box[3] && z >= box[4] && z < box[5]) {
+                                // replace the root, sift down (min-heap, entry e of this node at e*BM)
+                                int e = 0;
+                                for (;;) {
+                                    int l = 2 * e + 1;
+                                    if (l >= W) break;
+                                    unsigned long long kl = myk[l * BM];
+                                    if (l + 1 < W) {
+                                        const unsigned long long kr = myk[(l + 1) * BM];
+                                        if (kr < kl) {
+                                            kl = kr;
+                                            ++l;
+                                        }
+                                    }
+                                    if (kl >= key) break;
+                                    myk[e * BM] = kl;
+                                    myp[e * BM] = myp[l * BM];
+                                    e = l;
+                                }
+                                myk[e * BM] = key;
+                                myp[e * BM] = (unsigned)p;
+                                root = myk[0];
+                                thr = root ? unordered((unsigned)(root >> 32)) : -INFINITY;
+                            }
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+        if (live) {
+            const size_t o = ((size_t)node * a.ranges + range) * W;
+            for (int e = 0; e < W; ++e) {
+                a.out_key[o + e] = myk[e * BM];
+                a.out_pos[o + e] = myp[e * BM];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
+}
+
+}  // namespace tc
+
+// ---------------------------------------------------------------------------
+// host side: tensor maps and launch
+// ---------------------------------------------------------------------------
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// rows x k_elems operand, row-major (K contiguous), element of `elem` bytes,
+// boxes of one 128-byte K block x box_rows rows, 128-byte swizzle
+cudaError_t make_map(CUtensorMap *m, const void *base, int elem, long long k_elems, long long rows, int box_rows) {
+    auto enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    cuuint64_t dims[2] = {(cuuint64_t)k_elems, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(k_elems * elem)};
+    cuuint32_t box[2] = {(cuuint32_t)(tc::BKB / elem), (cuuint32_t)box_rows};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, elem == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 2,
+                     const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int KIND, int W>
+cudaError_t launch_w(const CUtensorMap &ma, const CUtensorMap &mp, const TcArgs &a, int node_tiles,
+                     cudaStream_t st) {
+    constexpr int HEAP = W * tc::BM * 12;
+    constexpr int STAGES = (W <= 16) ? 4 : 3;
+    constexpr int SMEM = 1024 + STAGES * tc::STAGE_BYTES + HEAP + (2 * STAGES + 5) * 8;
+    static_assert(SMEM <= 232448, "shared memory");
+    auto kern = tc::k_tc_shortlist<KIND, W, STAGES>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned)node_tiles, (unsigned)a.ranges);
+    kern<<<grid, tc::THREADS, SMEM, st>>>(ma, mp, a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int tc_supported_width(int w) { return w == 8 || w == 16 || w == 32; }
+
+cudaError_t launch_tc_shortlist(int kind, int W, const void *a_mat, long long a_rows, const void *p_mat,
+                                long long p_rows, long long k_elems, const TcArgs &args, cudaStream_t st) {
+    const int elem = kind == 0 ? 2 : 1;
+    if ((k_elems * elem) % tc::BKB != 0) return cudaErrorInvalidValue;
+    if (a_rows % tc::BM != 0 || p_rows % tc::BN != 0) return cudaErrorInvalidValue;
+    CUtensorMap ma, mp;
+    cudaError_t e;
+    if ((e = make_map(&ma, a_mat, elem, k_elems, a_rows, tc::BM)) != cudaSuccess) return e;
+    if ((e = make_map(&mp, p_mat, elem, k_elems, p_rows, tc::BN)) != cudaSuccess) return e;
+    TcArgs a = args;
+    a.k_per_block = tc::BKB / elem;
+    const int node_tiles = (int)(a_rows / tc::BM);
+    if (kind == 0) {
+        if (W == 8) return launch_w<0, 8>(ma, mp, a, node_tiles, st);
+        if (W == 16) return launch_w<0, 16>(ma, mp, a, node_tiles, st);
+        if (W == 32) return launch_w<0, 32>(ma, mp, a, node_tiles, st);
+    } else {
+        if (W == 8) return launch_w<1, 8>(ma, mp, a, node_tiles, st);
+        if (W == 16) return launch_w<1, 16>(ma, mp, a, node_tiles, st);
+        if (W == 32) return launch_w<1, 32>(ma, mp, a, node_tiles, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace qsk
+
+// ===========================================================================
+// The tensor-core form inside the batched simulation
+// ===========================================================================
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+namespace qsk {
+namespace {
+
+__device__ __forceinline__ void store_elem(void *base, long long idx, float v, int fmt) {
+    if (fmt == 0) {
+        reinterpret_cast<__nv_bfloat16 *>(base)[idx] = __float2bfloat16_rn(v);
+    } else {
+        reinterpret_cast<__nv_fp8_storage_t *>(base)[idx] = __nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+    }
+}
+
+// value of layer `ly` of the pattern matrix at TI cell q (natural index, x fastest)
+__device__ __forceinline__ float layer_value(const float *__restrict__ ti, int nvar, long long q, const TcLayer &ly) {
+    const float t = ti[q * nvar + ly.var];
+    if (ly.kind == 0) return isnan(t) ? 0.f : t * t;
+    if (ly.kind == 1) return isnan(t) ? 0.f : t;
+    return t == ly.code ? 1.f : 0.f;
+}
+
+// P[p][j * L + l] = layer l at TI cell p + o_j (0 outside the TI); one warp
+// per row, FP8 rows scaled by their largest magnitude (pos_scale)
+__global__ void k_tc_pattern(TcPatternArgs A) {
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int nd = A.nd;
+    for (long long p = warp; p < A.rows; p += nwarps) {
+        int pc[QSK_MAXD] = {0, 0, 0, 0};
+        long long r = p;
+        for (int d = 0; d < nd; ++d) {
+            pc[d] = int(r % A.src[d]);
+            r /= A.src[d];
+        }
+        const bool live = p < A.N;
+        float scale = 1.f;
+        if (A.fmt == 1) {
+            float mx = 0.f;
+            if (live)
+                for (long long k = lane; k < (long long)A.T * A.L; k += 32) {
+                    const int j = int(k / A.L), l = int(k % A.L);
+                    long long q = 0, st = 1;
+                    bool in = true;
+                    for (int d = 0; d < nd; ++d) {
+                        const int c = pc[d] + A.tpl[j * nd + d];
+                        in &= c >= 0 && c < A.src[d];
+                        q += (long long)c * st;
+                        st *= A.src[d];
+                    }
+                    if (in) mx = fmaxf(mx, fabsf(layer_value(A.ti, A.nvar, q, A.layer[l])));
+                }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            scale = mx > 0.f ? mx / 448.f : 1.f;
+            if (lane == 0) A.pos_scale[p] = scale;
+        }
+        const float inv = 1.f / scale;
+        for (long long k = lane; k < A.Kp; k += 32) {
+            float v = 0.f;
+            if (live && k < (long long)A.T * A.L) {
+                const int j = int(k / A.L), l = int(k % A.L);
+                long long q = 0, st = 1;
+                bool in = true;
+                for (int d = 0; d < nd; ++d) {
+                    const int c = pc[d] + A.tpl[j * nd + d];
+                    in &= c >= 0 && c < A.src[d];
+                    q += (long long)c * st;
+                    st *= A.src[d];
+                }
+                if (in) v = layer_value(A.ti, A.nvar, q, A.layer[l]) * inv;
+            }
+            store_elem(A.P, p * A.Kp + k, v, A.fmt);
+        }
+    }
+}
+
+// largest template index among a node's neighbours; -1 for nodes without a
+// neighbour other than the centre (marginal draw: the plain path)
+__global__ void k_tc_tmax(long long nodes, int n, const int *__restrict__ nb_count, const int *__restrict__ nb_tpl,
+                          int *__restrict__ tmax) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const int c = nb_count[i];
+    int m = -1;
+    if (c >= 2)
+        for (int j = 0; j < c; ++j) m = max(m, nb_tpl[i * n + j]);
+    tmax[i] = m;
+}
+
+// one warp per tensor slot: the node's row of A (coefficients of its terms at
+// their template columns), its validity box and tie seed
+__global__ void k_tc_nodes(TcNodeArgs A) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= A.nslots) return;
+    const int i = A.nodes[warp];
+    const unsigned cell = A.path[A.begin + i];
+    const int cnt = A.nb_count[i];
+    const int nd = A.nd;
+    int mn[QSK_MAXD] = {0, 0, 0, 0}, mx[QSK_MAXD] = {0, 0, 0, 0};
+    float amax = 0.f;
+    for (int j = lane; j < cnt; j += 32) {
+        const int t = A.nb_tpl[(long long)i * A.n + j];
+        const unsigned nc = A.nb_cell[(long long)i * A.n + j];
+        for (int d = 0; d < nd; ++d) {
+            const int o = A.tpl[t * nd + d];
+            mn[d] = min(mn[d], o);
+            mx[d] = max(mx[d], o);
+        }
+        for (int v = 0; v < A.nvar; ++v) {
+            const float val = nc == cell ? A.init[(long long)nc * A.nvar + v] : A.state[(long long)nc * A.nvar + v];
+            const float w = A.wtab[t * A.nvar + v];
+            if (isnan(val) || w == 0.f) continue;
+            if (A.types[v] == 0) amax = fmaxf(amax, fmaxf(fabsf(w), fabsf(2.f * __fmul_rn(w, val))));
+            else amax = fmaxf(amax, fabsf(w));
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < QSK_MAXD; ++d)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+            mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    const float scale = (A.fmt == 1 && amax > 0.f) ? amax / 448.f : 1.f;
+    const float inv = 1.f / scale;
+    for (int j = lane; j < cnt; j += 32) {
+        const int t = A.nb_tpl[(long long)i * A.n + j];
+        const unsigned nc = A.nb_cell[(long long)i * A.n + j];
+        for (int v = 0; v < A.nvar; ++v) {
+            const float val = nc == cell ? A.init[(long long)nc * A.nvar + v] : A.state[(long long)nc * A.nvar + v];
+            const float w = A.wtab[t * A.nvar + v];
+            if (isnan(val) || w == 0.f) continue;
+            const long long col = (long long)t * A.L + A.var_layer0[v];
+            if (A.types[v] == 0) {
+                store_elem(A.A, (long long)warp * A.Kp + col, -w * inv, A.fmt);
+                store_elem(A.A, (long long)warp * A.Kp + col + 1, 2.f * __fmul_rn(w, val) * inv, A.fmt);
+            } else {
+                const int nc_v = A.var_ncat[v];
+                for (int c = 0; c < nc_v; ++c)
+                    if (A.var_catv[v * QSK_CMAX + c] == val) store_elem(A.A, (long long)warp * A.Kp + col + c, w * inv, A.fmt);
+            }
+        }
+    }
+    if (lane == 0) {
+        A.node_scale[warp] = scale;
+        for (int d = 0; d < 3; ++d) {
+            const bool has = d < nd;
+            A.node_box[warp * 6 + 2 * d] = has ? -mn[d] : 0;
+            A.node_box[warp * 6 + 2 * d + 1] = has ? A.src[d] - mx[d] : 1;
+        }
+        A.node_seed[warp] = __float_as_uint(A.seeds[i]) ^ (unsigned(i) * 0x85EBCA6Bu);
+    }
+}
+
+// exact score of one candidate at scan index m, in the plain map's term order
+// (FP32, bit-identical to k_map_records) and in FP64; `scale` is the term
+// scale sum w (v^2 + t^2) (continuous) / sum w (categorical)
+__device__ __forceinline__ void exact_score(const Term *__restrict__ tm, int nt, const float *__restrict__ layers,
+                                            long long m, float &s32, double &s64, double &scale) {
+    float acc = 0.f;
+    double a64 = 0.0, sc = 0.0;
+    for (int t = 0; t < nt; ++t) {
+        const Term T = tm[t];
+        const float x = __ldg(layers + T.base + m);
+        if (T.op == OP_SQLIN) {
+            acc = __fmaf_rn(T.a, __fmul_rn(x, x), acc);
+            acc = __fmaf_rn(T.b, x, acc);
+            a64 += (double)T.a * ((double)x * (double)x) + (double)T.b * (double)x;
+            sc += -(double)T.a * ((double)x * (double)x) + ((double)T.b * (double)T.b) / (-4.0 * (double)T.a);
+        } else if (T.op == OP_EQ) {
+            acc = (x == T.b) ? __fadd_rn(acc, T.a) : acc;
+            a64 += (x == T.b) ? (double)T.a : 0.0;
+            sc += (double)T.a;
+        } else if (T.op == OP_LIN) {
+            acc = __fmaf_rn(T.a, x, acc);
+            a64 += (double)T.a * (double)x;
+            sc += fabs((double)T.a * (double)x);
+        }
+    }
+    s32 = acc;
+    s64 = a64;
+    scale = sc;
+}
+
+constexpr int SEL_WARPS = 4;
+constexpr int SEL_CAND = 768;    // candidates per slot staged in shared memory
+
+// one warp per tensor slot: the S best candidates by approximate key, their
+// exact scores, the node's k best by exact score (ties by the key's hash),
+// the draw and the write-back
+__global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
+    __shared__ unsigned long long skey[SEL_WARPS][SEL_CAND];
+    __shared__ unsigned spos[SEL_WARPS][SEL_CAND];
+    __shared__ Term sterm[SEL_WARPS][96];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * SEL_WARPS + w;
+    if (b >= A.nslots) return;
+    const Slot s = A.slots[b];
+    const Geom &g = A.g;
+    const int nt = s.nterms;
+    const Term *tm = A.terms + (long long)b * A.maxterms;
+    const bool small = nt <= 96;
+    if (small)
+        for (int t = lane; t < nt; t += 32) sterm[w][t] = tm[t];
+    const int nc = A.ncand;
+    for (int c = lane; c < nc; c += 32) {
+        skey[w][c] = A.cand_key[(long long)b * nc + c];
+        spos[w][c] = A.cand_pos[(long long)b * nc + c];
+    }
+    __syncwarp();
+    const Term *tt = small ? sterm[w] : tm;
+    // the S largest keys (S rounds of warp argmax); lane r keeps round r and r+32
+    unsigned long long mykey[2] = {0ull, 0ull};
+    unsigned mypos[2] = {0u, 0u};
+    int nsel = 0;
+    for (int r = 0; r < A.S; ++r) {
+        unsigned long long bk = 0ull;
+        int bi = -1;
+        for (int c = lane; c < nc; c += 32) {
+            const unsigned long long k = skey[w][c];
+            if (k > bk) {
+                bk = k;
+                bi = c;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long ok = __shfl_xor_sync(0xffffffffu, bk, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ok > bk || (ok == bk && oi > bi)) {
+                bk = ok;
+                bi = oi;
+            }
+        }
+        if (bk == 0ull) break;
+        if (lane == (r & 31)) {
+            mykey[r >> 5] = bk;
+            mypos[r >> 5] = spos[w][bi];
+        }
+        __syncwarp();
+        if (lane == 0) skey[w][bi] = 0ull;
+        __syncwarp();
+        ++nsel;
+    }
+    // exact scores of the shortlist
+    float e32[2] = {-INFINITY, -INFINITY};
+    double e64[2] = {-INFINITY, -INFINITY}, esc[2] = {0.0, 0.0};
+    unsigned hsh[2] = {0u, 0u};
+    bool live[2] = {false, false};
+    float errmax = 0.f;
+    double errsum = 0.0;
+    int errn = 0;
+    for (int h = 0; h < 2; ++h) {
+        const int r = h * 32 + lane;
+        if (r >= nsel) continue;
+        const unsigned p = mypos[h];
+        // natural cell -> scan index of the reference's flipped space (cvtPositionToIndex)
+        long long m = 0;
+        unsigned rem = p;
+        for (int d = 0; d < g.nd; ++d) {
+            const int pd = int(rem % (unsigned)g.src[d]);
+            rem /= (unsigned)g.src[d];
+            m += (long long)(g.fft[d] - 1 - pd - s.mn[d]) * g.sstride[d];
+        }
+        exact_score(tt, nt, A.layers, m, e32[h], e64[h], esc[h]);
+        const float approx = tc::unordered((unsigned)(mykey[h] >> 32));
+        const double err = fabs((double)approx - e64[h]) / (esc[h] > 0.0 ? esc[h] : 1.0);
+        errmax = fmaxf(errmax, (float)err);
+        errsum += err;
+        ++errn;
+        hsh[h] = (unsigned)(mykey[h] & 0xFFFFFFFFull);
+        live[h] = true;
+    }
+    // the node's K best by exact score (FP64 or FP32; equal scores ordered by
+    // the candidate's tie hash), extracted in descending order; the draw takes
+    // rank sel (the quantile rank of sample(), quantileSamplingModule.hpp:113)
+    const int K = s.K;
+    unsigned chosen = 0xFFFFFFFFu;
+    float chosen32 = -INFINITY;
+    double chosen_sc = 0.0;
+    const bool f64 = A.fp64 != 0;
+    for (int k = 0; k < K && k < nsel; ++k) {
+        int bh = -1;
+        for (int h = 0; h < 2; ++h) {
+            if (!live[h]) continue;
+            if (bh < 0) {
+                bh = h;
+                continue;
+            }
+            const bool better = f64 ? (e64[h] > e64[bh] || (e64[h] == e64[bh] && hsh[h] > hsh[bh]))
+                                    : (e32[h] > e32[bh] || (e32[h] == e32[bh] && hsh[h] > hsh[bh]));
+            if (better) bh = h;
+        }
+        double bv = bh >= 0 ? (f64 ? e64[bh] : (double)e32[bh]) : -INFINITY;
+        unsigned bhs = bh >= 0 ? hsh[bh] : 0u;
+        int bl = bh >= 0 ? lane : -1;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const unsigned oh = __shfl_xor_sync(0xffffffffu, bhs, o);
+            const int ol = __shfl_xor_sync(0xffffffffu, bl, o);
+            if (ol >= 0 && (bl < 0 || ov > bv || (ov == bv && (oh > bhs || (oh == bhs && ol > bl))))) {
+                bv = ov;
+                bhs = oh;
+                bl = ol;
+            }
+        }
+        if (bl < 0) break;
+        const int wh = __shfl_sync(0xffffffffu, bh, bl);
+        const unsigned wp = __shfl_sync(0xffffffffu, wh == 0 ? mypos[0] : mypos[1], bl);
+        const float w32 = __shfl_sync(0xffffffffu, wh == 0 ? e32[0] : e32[1], bl);
+        const double wsc = __shfl_sync(0xffffffffu, wh == 0 ? esc[0] : esc[1], bl);
+        if (lane == bl) live[wh] = false;
+        // rank sel, or the last one found when fewer than sel + 1 exist
+        chosen = wp;
+        chosen32 = w32;
+        chosen_sc = wsc;
+        if (k == s.sel) break;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        errmax = fmaxf(errmax, __shfl_xor_sync(0xffffffffu, errmax, o));
+        errsum += __shfl_xor_sync(0xffffffffu, errsum, o);
+        errn += __shfl_xor_sync(0xffffffffu, errn, o);
+    }
+    if (lane == 0) {
+        if (A.err_max) atomicMax(A.err_max, __float_as_uint(errmax));
+        if (A.err_sum) atomicAdd(A.err_sum, errsum);
+        if (A.err_n) atomicAdd(A.err_n, (unsigned long long)errn);
+        if (chosen == 0xFFFFFFFFu) {
+            if (A.status) atomicExch(A.status, DEV_BAD_INDEX);
+            return;
+        }
+        if (A.node_cell) A.node_cell[s.node] = chosen;
+        if (A.drawn_score) A.drawn_score[s.node] = chosen32;
+        if (A.drawn_scale) A.drawn_scale[s.node] = (float)chosen_sc;
+        if (A.state)
+            for (int v = 0; v < A.nvar; ++v) {
+                float *dst = A.state + (long long)s.cell * A.nvar + v;
+                if (isnan(*dst)) *dst = A.ti[(long long)chosen * A.nvar + v];
+            }
+        if (A.id_image) A.id_image[s.cell] = chosen * A.nti + A.ti_id;
+    }
+}
+
+// regret audit: the plain path's exact k best of audited node a (values
+// descending) against the candidate the tensor path drew for it
+__global__ void k_tc_audit(int n, const int *__restrict__ nodes, int K, const float *__restrict__ plain_val,
+                           const float *__restrict__ drawn_score, const float *__restrict__ drawn_scale, float tol,
+                           unsigned long long *__restrict__ counts) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const int node = nodes[a];
+    const float kth = plain_val[(long long)a * K + K - 1];
+    const float d = drawn_score[node];
+    const float t = tol * drawn_scale[node];
+    unsigned long long c0 = 1, c1 = 0, c2 = 0;
+    if (d < kth - t) c1 = 1;          // outside the exact k-best set
+    else if (d < kth) c2 = 1;         // below the k-th by at most the near-tie tolerance
+    atomicAdd(counts + 0, c0);
+    atomicAdd(counts + 1, c1);
+    atomicAdd(counts + 2, c2);
+}
+
+}  // namespace
+
+cudaError_t launch_tc_pattern(const TcPatternArgs &a, cudaStream_t st) {
+    long long warps = a.rows;
+    long long blocks = (warps * 32 + 255) / 256;
+    if (blocks > 148LL * 64) blocks = 148LL * 64;
+    k_tc_pattern<<<(unsigned)blocks, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_tmax(long long nodes, int n, const int *nb_count, const int *nb_tpl, int *tmax, cudaStream_t st) {
+    if (nodes <= 0) return cudaSuccess;
+    k_tc_tmax<<<(unsigned)((nodes + 255) / 256), 256, 0, st>>>(nodes, n, nb_count, nb_tpl, tmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st) {
+    const long long blocks = ((long long)a.nslots * 32 + 255) / 256;
+    k_tc_nodes<<<(unsigned)blocks, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st) {
+    if (a.ncand > SEL_CAND || a.S > 64) return cudaErrorInvalidValue;
+    k_tc_select<<<(unsigned)((a.nslots + SEL_WARPS - 1) / SEL_WARPS), 32 * SEL_WARPS, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_audit(int n, const int *nodes, int K, const float *plain_val, const float *drawn_score,
+                            const float *drawn_scale, float tol, unsigned long long *counts, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_tc_audit<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, nodes, K, plain_val, drawn_score, drawn_scale, tol, counts);
+    return cudaGetLastError();
+}
+
+}  // namespace qsk

@@ -236,6 +236,32 @@ int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, 
                               const qsk_term *terms, unsigned k, float seed, float *out_score, unsigned *out_index,
                               int *out_min);
 
+/* Top-W inner products on the tensor cores (tcgen05).  No G2S counterpart:
+ * it is the building block of this library's tensor-core map (the cross term
+ * of a batch of nodes over a template prefix, which replaces the per-node
+ * FFT correlation of CPUThreadDevice::candidateForPattern, G2S
+ * src/CPUThreadDevice.cpp:349-490) and of its learned proposal (node
+ * embeddings against pre-embedded TI patterns).
+ *   fmt       0: BF16 (queries/rows hold uint16 bit patterns), 1: FP8 E4M3
+ *             (uint8 bit patterns)
+ *   queries   B x K row-major, rows N x K row-major (N: positions of a TI
+ *             of X x Y x (N / (X*Y)) cells, x fastest)
+ *   score(q, p) = (queries[q] . rows[p]) * q_scale[q] * p_scale[p] + q_bias[q]
+ *             accumulated in FP32 (scales and bias may be NULL: 1 and 0)
+ *   q_box     6 ints per query: p = (x, y, z) is a candidate iff
+ *             q_box[0] <= x < q_box[1], q_box[2] <= y < q_box[3],
+ *             q_box[4] <= z < q_box[5]
+ * The positions are cut into `ranges` contiguous ranges; for every query and
+ * range the W (8, 16 or 32) largest keys are written, in no particular order,
+ * to out_key / out_pos [B][ranges][W]: key = (ordered score << 32) | tie hash
+ * of (q_seed[q], p), where the ordered score is the float's bits made
+ * monotone (negative: all bits inverted; otherwise the sign bit set); key 0
+ * marks an unused entry.  The union over the ranges holds the overall top W.
+ */
+int qsk_tc_topk(int device, int fmt, int B, long long N, int K, const void *queries, const void *rows,
+                const float *q_scale, const float *q_bias, const float *p_scale, const unsigned *q_seed,
+                const int *q_box, int X, int Y, int W, int ranges, unsigned long long *out_key, unsigned *out_pos);
+
 /* Reference scan index -> TI cell (CPUThreadDevice::cvtIndexToPosition,
  * G2S src/CPUThreadDevice.cpp:257-268). */
 unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index);
@@ -314,6 +340,15 @@ int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info);
 /* Profiling mode: record CUDA events around every kernel of the next runs so
  * that qsk_sim_info reports per-kernel device time (adds event overhead). */
 int qsk_sim_set_profiling(qsk_sim *s, int on);
+/* Bounded wait of the dependency-level pass (no G2S counterpart: G2S' path
+ * threads wait for their neighbours with unbounded 250 us sleeps,
+ * include/simulation.hpp:459-474).  A node waits for each dependency's level
+ * for at most spin_limit polls (0: 2^22, about a second); past it the run
+ * returns QSK_ERR_DEVICE ("a dependency level did not appear within the wait
+ * limit") instead of hanging.  hold_node >= 0 is a failure-path test: that
+ * path node's level is never published, so its dependants' waits run out
+ * (-1: normal operation). */
+int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node);
 /* Path (cell order), per-path-index seeds and number of informed cells. */
 int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
 int qsk_sim_destroy(qsk_sim *s);
