@@ -62,7 +62,19 @@ class QskSimInfo(ctypes.Structure):
                 ("template_size", ctypes.c_int), ("ms_setup_neighbours", ctypes.c_float),
                 ("ms_levels", ctypes.c_float), ("ms_batches", ctypes.c_float), ("ms_total", ctypes.c_float),
                 ("launches", ctypes.c_longlong), ("map_launches", ctypes.c_longlong), ("ms_map", ctypes.c_float),
-                ("ms_prep", ctypes.c_float), ("ms_replay", ctypes.c_float), ("map_positions", ctypes.c_longlong)]
+                ("ms_prep", ctypes.c_float), ("ms_replay", ctypes.c_float), ("map_positions", ctypes.c_longlong),
+                ("tensor_mode", ctypes.c_int), ("tensor_prefix", ctypes.c_int), ("tensor_width", ctypes.c_int),
+                ("tensor_shortlist", ctypes.c_int), ("tensor_nodes", ctypes.c_longlong),
+                ("plain_nodes", ctypes.c_longlong), ("audited", ctypes.c_longlong), ("regret", ctypes.c_longlong),
+                ("regret_near", ctypes.c_longlong), ("map_err_max", ctypes.c_float), ("map_err_mean", ctypes.c_float),
+                ("tensor_flops", ctypes.c_double), ("ms_tensor_gemm", ctypes.c_float),
+                ("ms_tensor_select", ctypes.c_float), ("ms_tensor_pattern", ctypes.c_float),
+                ("tensor_launches", ctypes.c_longlong)]
+
+
+class QskTensorOpts(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("prefix", ctypes.c_int), ("width", ctypes.c_int),
+                ("shortlist", ctypes.c_int), ("audit", ctypes.c_float)]
 
 
 # name -> (restype, argtypes): every entry point of include/g2s_b200.h
@@ -101,12 +113,14 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_void_p)]),
     "qsk_sim_run": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_sim_run_teacher": (ctypes.c_int, [ctypes.c_void_p, _f32p, _u32p]),
+    "qsk_sim_run_teacher_nodes": (ctypes.c_int, [ctypes.c_void_p, _f32p, _i32p, ctypes.c_int]),
     "qsk_sim_read": (ctypes.c_int, [ctypes.c_void_p, _f32p, _u32p, _u32p]),
     "qsk_sim_get_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskSimInfo)]),
     "qsk_sim_get_path": (ctypes.c_int, [ctypes.c_void_p, _u32p, _f32p, _u32p]),
     "qsk_sim_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_sim_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "qsk_sim_set_level_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_longlong]),
+    "qsk_sim_set_tensor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskTensorOpts)]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
     "qsk_set_map_mode": (ctypes.c_int, [ctypes.c_int]),
@@ -385,6 +399,15 @@ class Simulation:
         _check(lib().qsk_sim_set_profiling(self.handle, int(on)), "qsk_sim_set_profiling")
         return self
 
+    def set_tensor(self, mode: str = "bf16", prefix: int = 0, width: int = 0, shortlist: int = 0,
+                   audit: float = 0.0):
+        """Tensor-core form of the map: mode "plain" (the exact reference path),
+        "bf16" or "fp8"; zero fields take the automatic choice."""
+        m = {"plain": 0, "bf16": 1, "fp8": 2}[mode]
+        o = QskTensorOpts(m, int(prefix), int(width), int(shortlist), float(audit))
+        _check(lib().qsk_sim_set_tensor(self.handle, ctypes.byref(o)), "qsk_sim_set_tensor")
+        return self
+
     def set_level_wait(self, spin_limit: int = 0, hold_node: int = -1):
         """Bound of the dependency-level waits (polls; 0 = default) and, for
         failure-path tests, a path node whose level is never published."""
@@ -395,6 +418,14 @@ class Simulation:
         c = np.ascontiguousarray(completed, dtype=np.float32)
         ix = None if index is None else np.ascontiguousarray(index, dtype=np.uint32).ravel()
         _check(lib().qsk_sim_run_teacher(self.handle, _p(c, _f32p), _p(ix, _u32p)), "qsk_sim_run_teacher")
+        return self
+
+    def run_teacher_nodes(self, completed: np.ndarray, path_nodes):
+        """Teacher-forced draw of a sample of path nodes (no write-back)."""
+        c = np.ascontiguousarray(completed, dtype=np.float32)
+        nodes = np.ascontiguousarray(path_nodes, dtype=np.int32)
+        _check(lib().qsk_sim_run_teacher_nodes(self.handle, _p(c, _f32p), _p(nodes, _i32p), int(nodes.size)),
+               "qsk_sim_run_teacher_nodes")
         return self
 
     def info(self) -> dict:

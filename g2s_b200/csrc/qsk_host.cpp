@@ -130,6 +130,12 @@ struct qsk_ti {
     DBuf<unsigned> planes;
     DBuf<int> ncat;
     DBuf<float> catv;
+    // category codes of every categorical variable (grid-built; at most
+    // QSK_CMAX each, cat_ok false beyond): the indicator layers of the
+    // tensor-core pattern matrix
+    bool cat_ok = true;
+    std::vector<int> cat_n;           // nvar
+    std::vector<float> cat_v;         // nvar x QSK_CMAX
 };
 
 namespace {
@@ -356,6 +362,22 @@ static int ti_create_grid_impl(int device, int ndim, const unsigned *dims, int n
         if ((e = cudaMemcpy(t->complete_prefix.p, prefix.data(), sizeof(int) * cells, cudaMemcpyHostToDevice)) !=
             cudaSuccess)
             return bail(e);
+    }
+    // categories of every categorical variable (tensor-core indicator layers)
+    t->cat_n.assign(nvar, 0);
+    t->cat_v.assign(size_t(nvar) * QSK_CMAX, 0.f);
+    for (int v = 0; v < nvar; ++v) {
+        if (types[v] != 1) continue;
+        for (long long i = 0; i < t->cells && t->cat_ok; ++i) {
+            float x = data[size_t(i) * nvar + v];
+            if (std::isnan(x)) continue;
+            bool seen = false;
+            for (int q = 0; q < t->cat_n[v]; ++q) seen |= (t->cat_v[size_t(v) * QSK_CMAX + q] == x);
+            if (!seen) {
+                if (t->cat_n[v] == QSK_CMAX) t->cat_ok = false;
+                else t->cat_v[size_t(v) * QSK_CMAX + t->cat_n[v]++] = x;
+            }
+        }
     }
     // categories (distinct non-NaN codes) of categorical variables, for the bit planes
     bool all_cat = !missing;
@@ -686,6 +708,31 @@ struct qsk_sim {
     qsk_sim_info info;
     bool neighbours_ready = false;
     bool profiling = false;
+    // tensor-core form (qsk_sim_set_tensor)
+    qsk_tensor_opts topt{};             // mode 0: off
+    int tc_T = 0, tc_L = 0, tc_W = 0, tc_S = 0, tc_fmt = 0;
+    int tc_T_auto = 0;                  // automatic prefix, chosen at the first tensor run
+    long long tc_Kp = 0, tc_rows = 0;
+    bool tc_ready = false;              // pattern matrix built for (tc_T, tc_fmt)
+    std::vector<int> var_layer0;
+    DBuf<unsigned char> d_tc_P;         // tc_rows x tc_Kp
+    DBuf<float> d_tc_pscale;
+    DBuf<unsigned char> d_tc_A;         // slots x tc_Kp
+    DBuf<float> d_tc_nscale, d_tc_bias;
+    DBuf<int> d_tc_box, d_tc_tmax, d_tc_kb, d_var_layer0, d_var_ncat;
+    DBuf<unsigned> d_tc_seed, d_tc_pos, d_tc_thr;
+    DBuf<float> d_var_catv, d_drawn_score, d_drawn_scale;
+    DBuf<unsigned long long> d_tc_key, d_tc_counts;
+    DBuf<Slot> d_tc_slots;
+    DBuf<Term> d_tc_terms;
+    DBuf<int> d_audit_nodes;
+    DBuf<float> d_audit_val;
+    DBuf<unsigned> d_audit_pos, d_err_max;
+    DBuf<double> d_err_sum;
+    DBuf<unsigned long long> d_err_n;
+    int max_tc_slots = 0;
+    std::vector<cudaEvent_t> tc_ev;     // profiling: 3 events per tensor step
+    size_t tc_ev_used = 0;
     unsigned level_spin_limit = 0;      // 0: the kernel's default
     long long level_hold = -1;          // failure-path test: a node whose level is never published
     std::vector<cudaEvent_t> prof_ev;   // 4 events per batch in profiling mode
@@ -876,15 +923,41 @@ cudaEvent_t prof_event(qsk_sim *s) {
     return s->prof_ev[s->prof_used++];
 }
 
-int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
-    const Geom &g = s->ti->g;
-    s->prof_used = 0;
-    // batches: (first entry in the level node list, slots), levels in order
-    std::vector<std::pair<int, int>> batches;
+// One launch group of the batched engine: `B` nodes from `nodes + off`.
+//   PLAIN   the exact path (prep, map, k-best replay, write-back)
+//   TENSOR  the tensor-core form (node rows, GEMM shortlist, re-score, draw)
+//   AUDIT   the exact path without write-back, k best to the audit buffers
+//   HASH    the exact map, then the k best by (score, tie hash) over its
+//           records (the tensor-core form's draw rule, for the nodes it
+//           leaves to the map); marginal draws still replay
+enum StepKind { STEP_PLAIN = 0, STEP_TENSOR = 1, STEP_AUDIT = 2, STEP_HASH = 3 };
+struct Step {
+    int kind;
+    const int *nodes;   // device node list
+    int off, B;
+    int kb_off;         // TENSOR: this step's tile K-blocks in d_tc_kb
+};
+
+int tc_step(qsk_sim *s, const Step &st, bool teacher);
+
+// plain steps, one per slot budget of every level (levels in order)
+std::vector<Step> plain_steps(qsk_sim *s, const std::vector<int> &start) {
+    std::vector<Step> steps;
     for (size_t l = 0; l + 1 < start.size(); ++l)
         for (int off = start[l]; off < start[l + 1]; off += s->max_slots)
-            batches.emplace_back(off, std::min(s->max_slots, start[l + 1] - off));
-    auto prep_args = [&](int off, int B) {
+            steps.push_back({STEP_PLAIN, s->d_level_nodes.p, off, std::min(s->max_slots, start[l + 1] - off), 0});
+    return steps;
+}
+
+int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
+    const Geom &g = s->ti->g;
+    s->prof_used = 0;
+    s->tc_ev_used = 0;
+    // plain / audit steps (the generator-state pipeline runs over these only)
+    std::vector<size_t> pl;
+    for (size_t j = 0; j < steps.size(); ++j)
+        if (steps[j].kind != STEP_TENSOR) pl.push_back(j);
+    auto prep_args = [&](const int *nodes, int off, int B) {
         SimPrepArgs pa;
         pa.g = g;
         pa.dg = s->dg;
@@ -901,7 +974,7 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
         pa.n = s->n;
         pa.state = s->d_state.p;
         pa.init = s->d_init.p;
-        pa.nodes = s->d_level_nodes.p + off;
+        pa.nodes = nodes + off;
         pa.nslots = B;
         pa.k = s->k;
         pa.K = s->K;
@@ -932,7 +1005,8 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     auto launch_rng = [&](size_t j) -> int {
         const int p = int(j & 1);
         CK(cudaStreamWaitEvent(s->st_rng, s->ev_used[p], 0));
-        SimPrepArgs pa = prep_args(batches[j].first, batches[j].second);
+        const Step &sj = steps[pl[j]];
+        SimPrepArgs pa = prep_args(sj.nodes, sj.off, sj.B);
         if (bits) {
             pa.slots = s->d_sslots.p + size_t(p) * s->max_slots;
             pa.sterms = s->d_sterms.p + p * st_words;
@@ -943,15 +1017,22 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     };
     CK(cudaEventRecord(s->ev_used[0], s->st));   // after everything queued so far on st
     CK(cudaEventRecord(s->ev_used[1], s->st));
-    int rc = batches.empty() ? QSK_OK : launch_rng(0);
+    int rc = pl.empty() ? QSK_OK : launch_rng(0);
     if (rc) return rc;
-    for (size_t j = 0; j < batches.size(); ++j) {
-        const int B = batches[j].second, p = int(j & 1);
-        if (j + 1 < batches.size() && (rc = launch_rng(j + 1)) != QSK_OK) return rc;
+    size_t j = 0;   // plain / audit step counter
+    for (const Step &step : steps) {
+        if (step.kind == STEP_TENSOR) {
+            if ((rc = tc_step(s, step, teacher)) != QSK_OK) return rc;
+            continue;
+        }
+        const int B = step.B, p = int(j & 1);
+        const bool audit = step.kind == STEP_AUDIT;
+        if (j + 1 < pl.size() && (rc = launch_rng(j + 1)) != QSK_OK) return rc;
+        ++j;
         {
             Slot *slots = bits ? s->d_sslots.p + size_t(p) * s->max_slots : s->d_slots.p;
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            if (!bits) CK(launch_prep_sim(prep_args(batches[j].first, B), s->st));
+            if (!bits) CK(launch_prep_sim(prep_args(step.nodes, step.off, B), s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
             if (bits) {
                 // the slots and static terms of this batch come from k_mt_prep
@@ -1011,13 +1092,24 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
             ra.complete_prefix = s->ti->missing ? s->ti->complete_prefix.p : nullptr;
             ra.nti = 1;
             ra.ti_id = 0;
-            ra.state = teacher ? nullptr : s->d_state.p;
-            ra.id_image = teacher ? nullptr : s->d_id.p;
-            ra.node_cell = s->d_node_cell.p;
+            ra.state = (teacher || audit) ? nullptr : s->d_state.p;
+            ra.id_image = (teacher || audit) ? nullptr : s->d_id.p;
+            ra.node_cell = audit ? nullptr : s->d_node_cell.p;
+            if (audit) {
+                ra.out_val = s->d_audit_val.p + (size_t)step.off * s->K;
+                ra.out_pos = s->d_audit_pos.p + (size_t)step.off * s->K;
+            }
             ra.full = s->full ? 1 : 0;
             ra.mt_state = s->d_mt_state.p + p * mt_words;
             ra.mt_pre = s->d_mt_pre.p + size_t(p) * s->max_slots;
             CK(cudaStreamWaitEvent(s->st, s->ev_ready[p], 0));
+            if (step.kind == STEP_HASH) {
+                ra.drawn_score = s->d_drawn_score.p;
+                ra.drawn_scale = s->d_drawn_scale.p;
+                CK(launch_hash_select(ra, s->st));
+                ra.only_flagged = 1;
+                s->info.launches += 1;
+            }
             CK(launch_replay(ra, s->st));
             CK(cudaEventRecord(s->ev_used[p], s->st));
             if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
@@ -1026,9 +1118,428 @@ int sim_batches(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     return QSK_OK;
 }
 
+// ---------------------------------------------------------------------------
+// tensor-core form
+// ---------------------------------------------------------------------------
+cudaEvent_t tc_event(qsk_sim *s) {
+    if (s->tc_ev_used == s->tc_ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->tc_ev.push_back(e);
+    }
+    return s->tc_ev[s->tc_ev_used++];
+}
+
+long long rup(long long x, long long m) { return (x + m - 1) / m * m; }
+
+// pattern matrix of the template prefix (built once per simulation and mode)
+int tc_configure(qsk_sim *s, int T_auto) {
+    const Geom &g = s->ti->g;
+    const int fmt = s->topt.mode == 2 ? 1 : 0;
+    const int elem = fmt == 0 ? 2 : 1;
+    // layers: t^2, t per continuous variable; one indicator per category
+    std::vector<TcLayer> layers;
+    s->var_layer0.assign(s->nvar, 0);
+    for (int v = 0; v < s->nvar; ++v) {
+        s->var_layer0[v] = int(layers.size());
+        if (s->ti->types[v] == 0) {
+            layers.push_back({v, 0, 0.f});
+            layers.push_back({v, 1, 0.f});
+        } else {
+            for (int c = 0; c + 1 < s->ti->cat_n[v]; ++c)
+                layers.push_back({v, 2, s->ti->cat_v[size_t(v) * QSK_CMAX + c]});
+        }
+    }
+    if (layers.empty() || layers.size() > QSK_TC_MAXL)
+        return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: %zu pattern layers (1..%d)", layers.size(), QSK_TC_MAXL);
+    const int L = int(layers.size());
+    const long long rows = rup(g.N, 256);
+    int T = s->topt.prefix > 0 ? s->topt.prefix : T_auto;
+    T = std::max(1, std::min(T, s->ntpl));
+    // cap the pattern matrix at 16 GiB
+    while (T > 64 && (double)rows * rup((long long)T * L, 128 / elem) * elem > 16.0 * (1ull << 30)) T /= 2;
+    const long long Kp = rup((long long)T * L, 128 / elem);
+    const int W = s->topt.width > 0 ? s->topt.width : (fmt == 1 ? 32 : 8);
+    int S = s->topt.shortlist > 0 ? s->topt.shortlist : (fmt == 1 ? 64 : 4 * s->K);
+    if (!tc_supported_width(W)) return fail(QSK_ERR_ARG, "tensor-core width %d (8, 16 or 32)", W);
+    if (S > 64) return fail(QSK_ERR_ARG, "tensor-core shortlist %d (at most 64)", S);
+    if (S < s->K) S = s->K;
+    const bool same = s->tc_ready && s->tc_T == T && s->tc_fmt == fmt && s->tc_L == L;
+    s->tc_T = T;
+    s->tc_L = L;
+    s->tc_W = W;
+    s->tc_S = S;
+    s->tc_fmt = fmt;
+    s->tc_Kp = Kp;
+    s->tc_rows = rows;
+    if (same) return QSK_OK;
+    s->tc_ready = false;
+    CK(s->d_tc_P.alloc(size_t(rows * Kp * elem)));
+    CK(s->d_tc_pscale.alloc(size_t(rows / 256)));
+    DBuf<float> rowmax;
+    if (fmt == 1) CK(rowmax.alloc(size_t(rows)));
+    TcPatternArgs pa{};
+    pa.ti = s->ti->grid.p;
+    pa.nvar = s->nvar;
+    pa.nd = g.nd;
+    for (int d = 0; d < QSK_MAXD; ++d) pa.src[d] = d < g.nd ? g.src[d] : 1;
+    pa.N = s->ti->cells;
+    pa.rows = rows;
+    pa.tpl = s->d_tpl.p;
+    pa.T = T;
+    pa.L = L;
+    for (int l = 0; l < L; ++l) pa.layer[l] = layers[size_t(l)];
+    pa.Kp = Kp;
+    pa.fmt = fmt;
+    pa.P = s->d_tc_P.p;
+    pa.pos_scale = s->d_tc_pscale.p;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s->st));
+    CK(launch_tc_pattern(pa, rowmax.p, s->st));
+    CK(cudaEventRecord(e1, s->st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->info.ms_tensor_pattern = ms;
+    std::vector<int> ncat(s->nvar, 0);
+    for (int v = 0; v < s->nvar; ++v) ncat[v] = s->ti->types[v] == 1 ? s->ti->cat_n[v] : 0;
+    CK(s->d_var_layer0.upload(s->var_layer0.data(), s->var_layer0.size(), s->st));
+    CK(s->d_var_ncat.upload(ncat.data(), ncat.size(), s->st));
+    CK(s->d_var_catv.upload(s->ti->cat_v.data(), s->ti->cat_v.size(), s->st));
+    s->tc_ready = true;
+    return QSK_OK;
+}
+
+// Tensor steps of a run: every level's nodes whose neighbours all lie in the
+// template prefix (sorted by their largest template index, so that a tile of
+// 128 nodes needs few K blocks) take the tensor-core form, the rest the plain
+// path.  Rewrites the level node list in that order.
+// largest template index of every path node (-1: no neighbour but the centre)
+int tc_tmax(qsk_sim *s, std::vector<int> &tmax) {
+    const long long nodes = s->nodes;
+    CK(s->d_tc_tmax.ensure(size_t(std::max<long long>(nodes, 1))));
+    CK(launch_tc_tmax(nodes, s->n, s->d_nb_count.p, s->d_nb_tpl.p, s->d_tc_tmax.p, s->st));
+    tmax.resize((size_t)nodes);
+    CK(cudaMemcpyAsync(tmax.data(), s->d_tc_tmax.p, sizeof(int) * nodes, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return QSK_OK;
+}
+
+// Automatic template prefix: the smallest multiple of 256 offsets that
+// covers 97 % of the nodes with neighbours (the rest take the exact map with
+// the same hash tie rule).
+// The prefix sets the K of the GEMM for the nodes near it; the sorted nodes
+// of a level keep most 128-node tiles far below it.
+int tc_auto_prefix(const std::vector<int> &tmax) {
+    std::vector<int> v;
+    v.reserve(tmax.size());
+    for (int t : tmax)
+        if (t >= 0) v.push_back(t);
+    if (v.empty()) return 256;
+    const size_t q = std::min(v.size() - 1, size_t(double(v.size()) * 0.97));
+    std::nth_element(v.begin(), v.begin() + long(q), v.end());
+    return int((v[q] + 1 + 255) / 256 * 256);
+}
+
+int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &tmax, std::vector<Step> &steps,
+            std::vector<int> &audit_nodes) {
+    const long long nodes = s->nodes;
+    std::vector<int> order((size_t)nodes);
+    CK(cudaMemcpyAsync(order.data(), s->d_level_nodes.p, sizeof(int) * nodes, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    const int kbe = s->tc_fmt == 0 ? 64 : 128;
+    const int T = s->tc_T, L = s->tc_L;
+    std::vector<int> kb;   // K blocks of every 128-node tile of every tensor step
+    steps.clear();
+    audit_nodes.clear();
+    long long ntc = 0, npl = 0;
+    double flops = 0.0;
+    const long long ntiles_pos = s->tc_rows / 256;
+    const unsigned athr = s->topt.audit >= 1.f ? 0xFFFFFFFFu : unsigned(double(s->topt.audit) * 4294967296.0);
+    std::vector<int> el, pl;
+    for (size_t l = 0; l + 1 < start.size(); ++l) {
+        el.clear();
+        pl.clear();
+        for (int q = start[l]; q < start[l + 1]; ++q) {
+            const int i = order[size_t(q)];
+            (tmax[size_t(i)] >= 0 && tmax[size_t(i)] < T ? el : pl).push_back(i);
+        }
+        std::stable_sort(el.begin(), el.end(), [&](int a, int b) { return tmax[size_t(a)] < tmax[size_t(b)]; });
+        int q = start[l];
+        for (int i : el) order[size_t(q++)] = i;
+        for (int i : pl) order[size_t(q++)] = i;
+        for (int off = 0; off < int(el.size()); off += s->max_tc_slots) {
+            const int B = std::min(s->max_tc_slots, int(el.size()) - off);
+            Step st{STEP_TENSOR, s->d_level_nodes.p, start[l] + off, B, int(kb.size())};
+            for (int t0 = 0; t0 < B; t0 += 128) {
+                const int last = el[size_t(off + std::min(B, t0 + 128) - 1)];
+                const int k = int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
+                kb.push_back(k);
+                flops += 2.0 * 128 * 256 * double(ntiles_pos) * double(k) * kbe;
+            }
+            steps.push_back(st);
+        }
+        for (int off = 0; off < int(pl.size()); off += s->max_slots)
+            steps.push_back({STEP_HASH, s->d_level_nodes.p, start[l] + int(el.size()) + off,
+                             std::min(s->max_slots, int(pl.size()) - off), 0});
+        ntc += (long long)el.size();
+        npl += (long long)pl.size();
+        if (athr) {
+            for (int i : el)
+                if (tie_hash(0xA5D17u, unsigned(i)) < athr || s->topt.audit >= 1.f) audit_nodes.push_back(i);
+            // the exact map's nodes with neighbours (marginal draws have no k best)
+            for (int i : pl)
+                if (tmax[size_t(i)] >= 0 && (tie_hash(0xA5D17u, unsigned(i)) < athr || s->topt.audit >= 1.f))
+                    audit_nodes.push_back(i);
+        }
+    }
+    CK(cudaMemcpyAsync(s->d_level_nodes.p, order.data(), sizeof(int) * nodes, cudaMemcpyHostToDevice, s->st));
+    if (kb.empty()) kb.push_back(0);   // no tensor step: a valid (unused) upload
+    CK(s->d_tc_kb.upload(kb.data(), kb.size(), s->st));
+    CK(cudaStreamSynchronize(s->st));   // host vectors go out of scope
+    s->info.tensor_nodes = ntc;
+    s->info.plain_nodes = npl;
+    s->info.tensor_flops = flops;
+    return QSK_OK;
+}
+
+int tc_step(qsk_sim *s, const Step &step, bool teacher) {
+    const Geom &g = s->ti->g;
+    const int B = step.B;
+    const int elem = s->tc_fmt == 0 ? 2 : 1;
+    const long long Bp = rup(B, 128);
+    if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
+    // exact terms and slot geometry (the plain path's prep)
+    SimPrepArgs pa;
+    pa.g = g;
+    pa.dg = s->dg;
+    pa.nvar = s->nvar;
+    pa.types = s->d_types.p;
+    pa.tpl = s->d_tpl.p;
+    pa.wtab = s->d_wtab.p;
+    pa.path = s->d_path.p;
+    pa.begin = s->begin;
+    pa.seeds = s->d_seeds.p;
+    pa.nb_count = s->d_nb_count.p;
+    pa.nb_tpl = s->d_nb_tpl.p;
+    pa.nb_cell = s->d_nb_cell.p;
+    pa.n = s->n;
+    pa.state = s->d_state.p;
+    pa.init = s->d_init.p;
+    pa.nodes = step.nodes + step.off;
+    pa.nslots = B;
+    pa.k = s->k;
+    pa.K = s->K;
+    pa.nti = 1;
+    pa.slots = s->d_tc_slots.p;
+    pa.terms = s->d_tc_terms.p;
+    pa.maxterms = s->maxterms;
+    pa.status = s->d_status.p;
+    pa.missing = 0;
+    pa.mask_layer = s->nvar;
+    pa.no_verbatim = 0;
+    pa.id_image = s->d_id.p;
+    pa.node_nv = nullptr;
+    pa.node_k = nullptr;
+    pa.full = 0;
+    pa.nb_mask = nullptr;
+    CK(launch_prep_sim(pa, s->st));
+    // node rows of A
+    CK(cudaMemsetAsync(s->d_tc_A.p, 0, size_t(Bp * s->tc_Kp * elem), s->st));
+    TcNodeArgs na{};
+    na.nd = g.nd;
+    na.nvar = s->nvar;
+    for (int d = 0; d < QSK_MAXD; ++d) na.src[d] = d < g.nd ? g.src[d] : 1;
+    na.nodes = step.nodes + step.off;
+    na.nslots = B;
+    na.path = s->d_path.p;
+    na.begin = s->begin;
+    na.nb_count = s->d_nb_count.p;
+    na.nb_tpl = s->d_nb_tpl.p;
+    na.nb_cell = s->d_nb_cell.p;
+    na.n = s->n;
+    na.tpl = s->d_tpl.p;
+    na.wtab = s->d_wtab.p;
+    na.state = s->d_state.p;
+    na.init = s->d_init.p;
+    na.seeds = s->d_seeds.p;
+    na.types = s->d_types.p;
+    na.var_layer0 = s->d_var_layer0.p;
+    na.var_ncat = s->d_var_ncat.p;
+    na.var_catv = s->d_var_catv.p;
+    na.L = s->tc_L;
+    na.Kp = s->tc_Kp;
+    na.fmt = s->tc_fmt;
+    na.A = s->d_tc_A.p;
+    na.node_scale = s->d_tc_nscale.p;
+    na.node_bias = s->d_tc_bias.p;
+    na.node_box = s->d_tc_box.p;
+    na.node_seed = s->d_tc_seed.p;
+    CK(launch_tc_nodes(na, s->st));
+    if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
+    // GEMM shortlist: enough position ranges to fill the GPU, at most
+    // SEL_CAND / W candidates per node
+    const int node_tiles = int(Bp / 128);
+    const long long ntiles = s->tc_rows / 256;
+    int ranges = int(std::max<long long>(1, (148LL * 2 + node_tiles - 1) / node_tiles));
+    ranges = int(std::min<long long>({(long long)ranges, ntiles, 768LL / s->tc_W}));
+    TcArgs a{};
+    a.n_nodes = B;
+    a.n_pos = s->ti->cells;
+    a.n_tiles = ntiles;
+    a.ranges = ranges;
+    a.tiles_per_range = int((ntiles + ranges - 1) / ranges);
+    a.ranges = int((ntiles + a.tiles_per_range - 1) / a.tiles_per_range);
+    a.kblocks = int(s->tc_Kp * elem / 128);
+    a.tile_kblocks = s->d_tc_kb.p + step.kb_off;
+    a.node_scale = s->tc_fmt == 1 ? s->d_tc_nscale.p : nullptr;
+    a.node_bias = s->d_tc_bias.p;
+    a.pos_scale = s->tc_fmt == 1 ? s->d_tc_pscale.p : nullptr;
+    a.node_seed = s->d_tc_seed.p;
+    a.node_box = s->d_tc_box.p;
+    a.X = g.src[0];
+    a.Y = g.nd > 1 ? g.src[1] : 1;
+    // a shared bound across ranges keeps the overall top W in the union of the
+    // ranges' heaps: enough when the shortlist takes at most W of them
+    a.node_thr = s->tc_S <= s->tc_W ? s->d_tc_thr.p : nullptr;
+    a.out_key = s->d_tc_key.p;
+    a.out_pos = s->d_tc_pos.p;
+    a.status = s->d_status.p;
+    CK(cudaMemsetAsync(s->d_tc_thr.p, 0, sizeof(unsigned) * size_t(B), s->st));
+    CK(launch_tc_shortlist(s->tc_fmt, s->tc_W, s->d_tc_A.p, Bp, s->d_tc_P.p, s->tc_rows, s->tc_Kp, a, s->st));
+    if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
+    TcSelectArgs sa{};
+    sa.g = g;
+    sa.slots = s->d_tc_slots.p;
+    sa.terms = s->d_tc_terms.p;
+    sa.maxterms = s->maxterms;
+    sa.nslots = B;
+    sa.layers = s->ti->layers.p;
+    sa.cand_key = s->d_tc_key.p;
+    sa.cand_pos = s->d_tc_pos.p;
+    sa.ncand = a.ranges * s->tc_W;
+    sa.S = s->tc_S;
+    sa.fp64 = s->tc_fmt == 1 ? 1 : 0;
+    sa.ti = s->ti->grid.p;
+    sa.nvar = s->nvar;
+    sa.nti = 1;
+    sa.ti_id = 0;
+    sa.state = teacher ? nullptr : s->d_state.p;
+    sa.id_image = teacher ? nullptr : s->d_id.p;
+    sa.node_cell = s->d_node_cell.p;
+    sa.drawn_score = s->d_drawn_score.p;
+    sa.drawn_scale = s->d_drawn_scale.p;
+    sa.err_max = s->d_err_max.p;
+    sa.err_sum = s->d_err_sum.p;
+    sa.err_n = s->d_err_n.p;
+    sa.status = s->d_status.p;
+    CK(launch_tc_select(sa, s->st));
+    if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
+    s->info.launches += 4;
+    s->info.tensor_launches += 4;
+    return QSK_OK;
+}
+
+// buffers of the tensor steps (sized for max_tc_slots) and the statistics
+int tc_buffers(qsk_sim *s, size_t n_audit) {
+    const int elem = s->tc_fmt == 0 ? 2 : 1;
+    const size_t slots = size_t(s->max_tc_slots), bp = size_t(rup(s->max_tc_slots, 128));
+    CK(s->d_tc_A.ensure(bp * size_t(s->tc_Kp) * elem));
+    CK(s->d_tc_nscale.ensure(bp));
+    CK(s->d_tc_bias.ensure(bp));
+    CK(s->d_tc_box.ensure(bp * 6));
+    CK(s->d_tc_seed.ensure(bp));
+    CK(s->d_tc_thr.ensure(bp));
+    CK(s->d_tc_key.ensure(slots * 768));
+    CK(s->d_tc_pos.ensure(slots * 768));
+    CK(s->d_tc_slots.ensure(slots));
+    CK(s->d_tc_terms.ensure(slots * size_t(s->maxterms)));
+    CK(s->d_drawn_score.ensure(size_t(std::max<long long>(s->nodes, 1))));
+    CK(s->d_drawn_scale.ensure(size_t(std::max<long long>(s->nodes, 1))));
+    CK(s->d_err_max.ensure(1));
+    CK(s->d_err_sum.ensure(1));
+    CK(s->d_err_n.ensure(1));
+    CK(s->d_tc_counts.ensure(3));
+    CK(cudaMemsetAsync(s->d_err_max.p, 0, sizeof(unsigned), s->st));
+    CK(cudaMemsetAsync(s->d_err_sum.p, 0, sizeof(double), s->st));
+    CK(cudaMemsetAsync(s->d_err_n.p, 0, sizeof(unsigned long long), s->st));
+    CK(cudaMemsetAsync(s->d_tc_counts.p, 0, 3 * sizeof(unsigned long long), s->st));
+    if (n_audit) {
+        CK(s->d_audit_nodes.ensure(n_audit));
+        CK(s->d_audit_val.ensure(n_audit * size_t(s->K)));
+        CK(s->d_audit_pos.ensure(n_audit * size_t(s->K)));
+    }
+    return QSK_OK;
+}
+
+int sim_records(qsk_sim *s, long long slots);
+
+// tensor-core run: plan, steps, audit, statistics.  `start`: level bounds of
+// the level node list (one level under teacher forcing)
+int tc_run(qsk_sim *s, const std::vector<int> &start, bool teacher) {
+    std::vector<int> tmax;
+    int rc = tc_tmax(s, tmax);
+    if (rc) return rc;
+    if (s->tc_T_auto == 0) s->tc_T_auto = tc_auto_prefix(tmax);
+    if ((rc = tc_configure(s, s->tc_T_auto)) != QSK_OK) return rc;
+    std::vector<Step> steps;
+    std::vector<int> audit;
+    if ((rc = tc_plan(s, start, tmax, steps, audit)) != QSK_OK) return rc;
+    if ((rc = tc_buffers(s, audit.size())) != QSK_OK) return rc;
+    int mb = 1;
+    for (const Step &st : steps)
+        if (st.kind == STEP_PLAIN || st.kind == STEP_HASH) mb = std::max(mb, st.B);
+    if (!audit.empty()) mb = std::max(mb, std::min<int>(int(audit.size()), s->max_slots));
+    if ((rc = sim_records(s, mb)) != QSK_OK) return rc;
+    if ((rc = sim_batches(s, steps, teacher)) != QSK_OK) return rc;
+    // audit: the plain path, teacher-forced on the final grid (every node's
+    // neighbours hold the values they had at its turn), k best per node
+    if (!audit.empty()) {
+        CK(cudaMemcpyAsync(s->d_audit_nodes.p, audit.data(), sizeof(int) * audit.size(), cudaMemcpyHostToDevice, s->st));
+        std::vector<Step> as;
+        for (int off = 0; off < int(audit.size()); off += s->max_slots)
+            as.push_back({STEP_AUDIT, s->d_audit_nodes.p, off, std::min(s->max_slots, int(audit.size()) - off), 0});
+        const bool prof = s->profiling;
+        s->profiling = false;
+        const size_t used = s->prof_used, tused = s->tc_ev_used;
+        rc = sim_batches(s, as, true);
+        s->prof_used = used;
+        s->tc_ev_used = tused;
+        s->profiling = prof;
+        if (rc) return rc;
+        CK(launch_tc_audit(int(audit.size()), s->d_audit_nodes.p, s->K, s->d_audit_val.p, s->d_drawn_score.p,
+                           s->d_drawn_scale.p, 1e-5f, s->d_tc_counts.p, s->st));
+    }
+    unsigned long long counts[3] = {0, 0, 0}, en = 0;
+    unsigned emax = 0;
+    double esum = 0.0;
+    CK(cudaMemcpyAsync(counts, s->d_tc_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&emax, s->d_err_max.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&esum, s->d_err_sum.p, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&en, s->d_err_n.p, sizeof(en), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->info.tensor_mode = s->topt.mode;
+    s->info.tensor_prefix = s->tc_T;
+    s->info.tensor_width = s->tc_W;
+    s->info.tensor_shortlist = s->tc_S;
+    s->info.audited = (long long)counts[0];
+    s->info.regret = (long long)counts[1];
+    s->info.regret_near = (long long)counts[2];
+    float fm;
+    std::memcpy(&fm, &emax, sizeof(float));
+    s->info.map_err_max = fm;
+    s->info.map_err_mean = en ? float(esum / double(en)) : 0.f;
+    return QSK_OK;
+}
+
 void collect_profile(qsk_sim *s) {
-    if (!s->profiling || s->prof_used == 0) return;
-    cudaEventSynchronize(s->prof_ev[s->prof_used - 1]);
+    if (!s->profiling || (s->prof_used == 0 && s->tc_ev_used == 0)) return;
+    if (s->prof_used) cudaEventSynchronize(s->prof_ev[s->prof_used - 1]);
+    if (s->tc_ev_used) cudaEventSynchronize(s->tc_ev[s->tc_ev_used - 1]);
     float prep = 0, map = 0, rep = 0;
     for (size_t i = 0; i + 3 < s->prof_used; i += 4) {
         float a = 0, b = 0, c = 0;
@@ -1042,6 +1553,17 @@ void collect_profile(qsk_sim *s) {
     s->info.ms_prep = prep;
     s->info.ms_map = map;
     s->info.ms_replay = rep;
+    float gemm = 0, sel = 0;
+    for (size_t i = 0; i + 3 < s->tc_ev_used; i += 4) {
+        float a = 0, b = 0, c = 0;
+        cudaEventElapsedTime(&a, s->tc_ev[i], s->tc_ev[i + 1]);
+        cudaEventElapsedTime(&b, s->tc_ev[i + 1], s->tc_ev[i + 2]);
+        cudaEventElapsedTime(&c, s->tc_ev[i + 2], s->tc_ev[i + 3]);
+        sel += a + c;
+        gemm += b;
+    }
+    s->info.ms_tensor_gemm = gemm;
+    s->info.ms_tensor_select = sel;
 }
 
 // records for the largest batch a run launches (its largest level, cut at
@@ -1273,6 +1795,7 @@ int qsk_sim_run(qsk_sim *s) {
     s->info.launches = 0;
     s->info.map_launches = 0;
     s->info.map_positions = 0;
+    s->info.tensor_launches = 0;
     CK(cudaEventRecord(ev[0], s->st));
     s->neighbours_ready = false;
     int rc = sim_neighbours(s);
@@ -1313,10 +1836,14 @@ int qsk_sim_run(qsk_sim *s) {
                     s->nodes);
     int mb = 0;
     for (int l = 0; l < nl; ++l) mb = std::max(mb, start[l + 1] - start[l]);
-    rc = sim_records(s, mb);
-    if (rc) return rc;
     CK(cudaEventRecord(ev[2], s->st));
-    rc = sim_batches(s, start, false);
+    if (s->topt.mode != 0) {
+        rc = tc_run(s, start, false);
+    } else {
+        rc = sim_records(s, mb);
+        if (rc) return rc;
+        rc = sim_batches(s, plain_steps(s, start), false);
+    }
     if (rc) return rc;
     CK(cudaEventRecord(ev[3], s->st));
     CK(cudaEventSynchronize(ev[3]));
@@ -1348,14 +1875,65 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
     std::iota(ident.begin(), ident.end(), 0);
     CK(cudaMemcpyAsync(s->d_level_nodes.p, ident.data(), sizeof(int) * s->nodes, cudaMemcpyHostToDevice, s->st));
     std::vector<int> start = {0, int(s->nodes)};
-    rc = sim_records(s, s->nodes);
-    if (rc) return rc;
-    rc = sim_batches(s, start, true);
+    if (s->topt.mode != 0) {
+        rc = tc_run(s, start, true);
+    } else {
+        rc = sim_records(s, s->nodes);
+        if (rc) return rc;
+        rc = sim_batches(s, plain_steps(s, start), true);
+    }
     if (rc) return rc;
     s->info.nodes = s->nodes;
     s->info.levels = 1;
     s->info.max_batch = int(s->nodes);
     CK(cudaStreamSynchronize(s->st));
+    return sim_check_status(s);
+}
+
+int qsk_sim_run_teacher_nodes(qsk_sim *s, const float *di_completed, const int *path_nodes, int count) {
+    if (!s || !di_completed || (!path_nodes && count > 0) || count < 0) return fail(QSK_ERR_ARG, "null argument");
+    if (s->no_verbatim) return fail(QSK_ERR_UNSUPPORTED, "-nV teacher forcing on a node sample");
+    for (int q = 0; q < count; ++q)
+        if (path_nodes[q] < 0 || path_nodes[q] >= s->nodes)
+            return fail(QSK_ERR_ARG, "path node %d of %lld", path_nodes[q], s->nodes);
+    DeviceGuard dgd(s->device);
+    cudaEvent_t ev[2];
+    for (auto &x : ev) CK(cudaEventCreate(&x));
+    CK(cudaMemcpyAsync(s->d_state.p, di_completed, sizeof(float) * s->init.size(), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->d_id.p, 0, sizeof(unsigned) * s->cells * (s->full ? s->nvar : 1), s->st));
+    CK(cudaMemsetAsync(s->d_status.p, 0, sizeof(int), s->st));
+    int rc = QSK_OK;
+    if (!s->neighbours_ready) {
+        rc = sim_neighbours(s);
+        if (rc) return rc;
+    }
+    s->info.launches = 0;
+    s->info.map_launches = 0;
+    s->info.map_positions = 0;
+    s->info.tensor_launches = 0;
+    CK(cudaEventRecord(ev[0], s->st));
+    if (count > 0)
+        CK(cudaMemcpyAsync(s->d_level_nodes.p, path_nodes, sizeof(int) * count, cudaMemcpyHostToDevice, s->st));
+    std::vector<int> start = {0, count};
+    if (s->topt.mode != 0) {
+        rc = tc_run(s, start, true);
+    } else {
+        rc = sim_records(s, count);
+        if (rc) return rc;
+        rc = sim_batches(s, plain_steps(s, start), true);
+    }
+    if (rc) return rc;
+    CK(cudaEventRecord(ev[1], s->st));
+    CK(cudaEventSynchronize(ev[1]));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    for (auto &x : ev) cudaEventDestroy(x);
+    s->info.nodes = count;
+    s->info.levels = 1;
+    s->info.max_batch = count;
+    s->info.ms_batches = ms;
+    s->info.ms_total = ms;
+    collect_profile(s);
     return sim_check_status(s);
 }
 
@@ -1393,6 +1971,30 @@ int qsk_sim_set_profiling(qsk_sim *s, int on) {
     return QSK_OK;
 }
 
+int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
+    if (!s || !o) return fail(QSK_ERR_ARG, "null argument");
+    if (o->mode < 0 || o->mode > 2) return fail(QSK_ERR_ARG, "tensor mode %d (0 plain, 1 BF16, 2 FP8)", o->mode);
+    if (!(o->audit >= 0.f && o->audit <= 1.f)) return fail(QSK_ERR_ARG, "audit fraction %g", double(o->audit));
+    if (o->width != 0 && !tc_supported_width(o->width)) return fail(QSK_ERR_ARG, "width %d (8, 16 or 32)", o->width);
+    if (o->shortlist < 0 || o->shortlist > 64) return fail(QSK_ERR_ARG, "shortlist %d (at most 64)", o->shortlist);
+    if (o->prefix < 0) return fail(QSK_ERR_ARG, "prefix %d", o->prefix);
+    if (o->mode != 0) {
+        if (s->ti->missing) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: training image with missing values");
+        if (s->no_verbatim || s->full || s->local)
+            return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: -nV, -fs and local controls run on the plain path");
+        if (!s->ti->cat_ok) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: more than %d categories", QSK_CMAX);
+        if (s->ti->g.nd > 3) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: %d dimensions (at most 3)", s->ti->g.nd);
+        if (s->ti->cells > (1LL << 31)) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: TI of %lld cells", s->ti->cells);
+    }
+    s->topt = *o;
+    s->max_tc_slots = 4096;
+    if (o->mode == 0) {
+        s->info.tensor_mode = 0;
+        s->info.tensor_nodes = s->info.plain_nodes = s->info.audited = s->info.regret = s->info.regret_near = 0;
+    }
+    return QSK_OK;
+}
+
 int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node) {
     if (!s) return fail(QSK_ERR_ARG, "null sim");
     if (hold_node < -1 || hold_node >= s->nodes) return fail(QSK_ERR_ARG, "hold node %lld of %lld", hold_node, s->nodes);
@@ -1406,6 +2008,7 @@ int qsk_sim_destroy(qsk_sim *s) {
     {
         DeviceGuard dgd(s->device);
         for (auto e : s->prof_ev) cudaEventDestroy(e);
+        for (auto e : s->tc_ev) cudaEventDestroy(e);
         for (int p = 0; p < 2; ++p) {
             if (s->ev_ready[p]) cudaEventDestroy(s->ev_ready[p]);
             if (s->ev_used[p]) cudaEventDestroy(s->ev_used[p]);

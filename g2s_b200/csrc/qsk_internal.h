@@ -208,6 +208,12 @@ struct ReplayArgs {
     // skipped blocks stand for; null: each slot is seeded in the replay
     const unsigned *mt_state;
     const int *mt_pre;
+    // replay only the slots flagged SLOT_SKIP / SLOT_EMIT_MASKED (the hash
+    // select takes the others)
+    int only_flagged = 0;
+    // hash select: per path node, the drawn candidate's score (regret audit)
+    float *drawn_score = nullptr;
+    float *drawn_scale = nullptr;
 };
 
 
@@ -258,6 +264,9 @@ cudaError_t launch_build_planes(const float *layers, const Geom &g, int nvar, co
 int map_bits_segs_per_cta(const Geom &g, int nslots);
 cudaError_t launch_map_bits(const BitArgs &a, int nslots, int K, int maxterms_in_batch, cudaStream_t st);
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st);
+// k best by (score, tie hash) over the records; slots with SLOT_SKIP or
+// SLOT_EMIT_MASKED are left to launch_replay with only_flagged
+cudaError_t launch_hash_select(const ReplayArgs &a, cudaStream_t st);
 // exclusion masks: slot b's positions around scan index center[b] (radius[b] >= 1)
 cudaError_t launch_radius_mask(const int *center, const float *radius, int nslots, const Geom &g, unsigned *mask,
                                long long xwords, cudaStream_t st);
@@ -267,8 +276,8 @@ cudaError_t launch_mt_prep(const SimPrepArgs &a, unsigned *state, int *pre, cuda
 // tensor-core shortlist (qsk_tc.cu): D = A * P^T on tcgen05 for 128-row tiles
 // of A (nodes / queries) against 256-row tiles of P (TI positions), K in
 // 128-byte blocks (64 BF16 or 128 FP8 E4M3 values); per A row and position
-// range the W largest scores (acc * node_scale * pos_scale + node_bias) whose
-// position lies in the row's validity box are kept.
+// range the W largest scores (acc * node_scale * tile_scale + node_bias)
+// whose position lies in the row's validity box are kept.
 // ---------------------------------------------------------------------------
 struct TcArgs {
     int n_nodes;               // live rows of A
@@ -281,10 +290,12 @@ struct TcArgs {
     int k_per_block;           // elements per K block (set by the launcher)
     const float *node_scale;   // per A row (null: 1)
     const float *node_bias;    // per A row (null: 0)
-    const float *pos_scale;    // per P row (null: 1)
+    const float *pos_scale;    // per tile of 256 P rows (null: 1)
     const unsigned *node_seed; // per A row tie-break seed (null: 0)
     const int *node_box;       // per A row: x0, x1, y0, y1, z0, z1 (p valid iff x0 <= x < x1, ...)
     int X, Y;                  // P row p is TI cell (x, y, z), x fastest
+    unsigned *node_thr;        // per A row, zeroed before the launch: the best heap minimum of any range
+                               // (ordered score), a lower bound of the row's W-th best (null: none)
     unsigned long long *out_key;   // [row][range][W]: (ordered score << 32) | tie hash; 0 = empty
     unsigned *out_pos;             // [row][range][W]
     int *status;
@@ -299,7 +310,8 @@ cudaError_t launch_tc_shortlist(int kind, int W, const void *a_mat, long long a_
 // column j * L + l = layer l at cell p + o_j for the first T template
 // offsets (0 outside the TI), in BF16 or FP8 E4M3 (rows scaled to their
 // largest magnitude).  Layers: a continuous variable gives t^2 and t, a
-// categorical one an indicator per category code.
+// categorical one with C categories an indicator of each of its first C-1
+// codes (a match of the last code is 1 minus the others: a node constant).
 #define QSK_TC_MAXL 64
 struct TcLayer {
     int var;
@@ -318,7 +330,7 @@ struct TcPatternArgs {
     long long Kp;
     int fmt;                   // 0 BF16, 1 FP8 E4M3
     void *P;
-    float *pos_scale;          // FP8: per row
+    float *pos_scale;          // FP8: per tile of 256 rows
 };
 struct TcNodeArgs {
     int nd, nvar;
@@ -343,6 +355,7 @@ struct TcNodeArgs {
     int fmt;
     void *A;                   // slot rows x Kp (zeroed by the caller)
     float *node_scale;
+    float *node_bias;          // sum of the weights of neighbours in a variable's last category
     int *node_box;
     unsigned *node_seed;
 };
@@ -371,7 +384,8 @@ struct TcSelectArgs {
     unsigned long long *err_n;
     int *status;
 };
-cudaError_t launch_tc_pattern(const TcPatternArgs &a, cudaStream_t st);
+// FP8: rowmax is scratch of `rows` floats
+cudaError_t launch_tc_pattern(const TcPatternArgs &a, float *rowmax, cudaStream_t st);
 cudaError_t launch_tc_tmax(long long nodes, int n, const int *nb_count, const int *nb_tpl, int *tmax, cudaStream_t st);
 cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st);
 cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st);

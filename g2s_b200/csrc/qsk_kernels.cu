@@ -1684,6 +1684,9 @@ __global__ void __launch_bounds__(W == 1 ? 32 * RP_WARPS : 32 * W) k_replay(Repl
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = W == 1 ? blockIdx.x * RP_WARPS + wib : blockIdx.x;
     if (b >= A.nslots) return;
+    // only_flagged: the slots the hash select leaves (marginal draws, fewer
+    // valid positions than k); every warp of a team leaves together
+    if (A.only_flagged && !(A.slots[b].flags & (SLOT_SKIP | SLOT_EMIT_MASKED))) return;
     WarpShared &w = wsh[W == 1 ? wib : 0];
     if constexpr (W > 1) {
         if (wib > 0) {
@@ -1908,6 +1911,145 @@ __global__ void __launch_bounds__(W == 1 ? 32 * RP_WARPS : 32 * W) k_replay(Repl
             if (A.id_image) A.id_image[s.cell] = chosen_cell * A.nti + A.ti_id;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// k best with hash tie-breaks over the map's records (the draw rule of the
+// tensor-core form, for the nodes it leaves to the plain map).  Every position
+// scoring at least the k-th best is a record (the filter keeps ties), so the
+// k largest (score, tie hash) over the records are the k largest over the map.
+// One CTA per slot; slots with SLOT_SKIP or SLOT_EMIT_MASKED are left to the
+// replay (only_flagged).
+// ---------------------------------------------------------------------------
+namespace {
+template <int W>
+__device__ __forceinline__ void hs_insert(unsigned long long (&k)[W], unsigned (&p)[W], unsigned long long key,
+                                          unsigned pos) {
+    k[0] = key;
+    p[0] = pos;
+#pragma unroll
+    for (int i = 0; i + 1 < W; ++i) {
+        const bool sw = k[i] > k[i + 1];
+        const unsigned long long a = k[i], c = k[i + 1];
+        const unsigned pa = p[i], pc = p[i + 1];
+        k[i] = sw ? c : a;
+        k[i + 1] = sw ? a : c;
+        p[i] = sw ? pc : pa;
+        p[i + 1] = sw ? pa : pc;
+    }
+}
+__device__ __forceinline__ unsigned hs_ordered(float f) {
+    if (f != f) return 0u;
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+}  // namespace
+
+constexpr int HS_THREADS = 128;
+__global__ void __launch_bounds__(HS_THREADS) k_hash_select(ReplayArgs A) {
+    __shared__ unsigned long long sk[HS_THREADS * QSK_KMAX];
+    __shared__ unsigned sp[HS_THREADS * QSK_KMAX];
+    const int b = blockIdx.x;
+    if (b >= A.nslots) return;
+    const Slot s = A.slots[b];
+    if (s.flags & (SLOT_SKIP | SLOT_EMIT_MASKED)) return;
+    const Geom &g = A.g;
+    const int K = s.K;
+    const unsigned seed = __float_as_uint(s.seed) ^ (unsigned(s.node) * 0x85EBCA6Bu);
+    unsigned long long rk[QSK_KMAX];
+    unsigned rp[QSK_KMAX];
+#pragma unroll
+    for (int i = 0; i < QSK_KMAX; ++i) {
+        rk[i] = 0ull;
+        rp[i] = 0u;
+    }
+    // the thread's K best in rk[QSK_KMAX-K .. QSK_KMAX-1] (ascending array of
+    // QSK_KMAX; its minimum rk[0] bounds what may enter)
+    const long long base = (long long)b * g.nseg;
+    for (int sg = threadIdx.x; sg < g.nseg; sg += HS_THREADS) {
+        const int cnt = A.rec_cnt[base + sg];
+        if (cnt == 0) continue;
+        if (hs_ordered(A.rec_max[base + sg]) < (unsigned)(rk[QSK_KMAX - K] >> 32)) continue;
+        const float *rv = A.rec_val + (base + sg) * QSK_SEG;
+        const int *ri = A.rec_idx + (base + sg) * QSK_SEG;
+        for (int i = 0; i < cnt; ++i) {
+            const unsigned idx = (unsigned)ri[i];
+            const unsigned long long key = ((unsigned long long)hs_ordered(rv[i]) << 32) | tie_hash(seed, idx);
+            if (key > rk[QSK_KMAX - K]) {
+                // keep the array's top K: entries below QSK_KMAX-K stay at 0
+                hs_insert<QSK_KMAX>(rk, rp, key, idx);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < QSK_KMAX; ++i) {
+        sk[i * HS_THREADS + threadIdx.x] = rk[i];
+        sp[i * HS_THREADS + threadIdx.x] = rp[i];
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    // K rounds of warp argmax over the block's entries, descending
+    unsigned chosen = 0xFFFFFFFFu;
+    float cval[QSK_KMAX];
+    unsigned cpos[QSK_KMAX];
+    int got = 0;
+    for (int r = 0; r < K; ++r) {
+        unsigned long long bk = 0ull;
+        int bi = -1;
+        for (int e = lane; e < HS_THREADS * QSK_KMAX; e += 32) {
+            const unsigned long long k2 = sk[e];
+            if (k2 > bk) {
+                bk = k2;
+                bi = e;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long ok = __shfl_xor_sync(0xffffffffu, bk, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ok > bk || (ok == bk && oi > bi)) {
+                bk = ok;
+                bi = oi;
+            }
+        }
+        if (bk == 0ull) break;
+        const unsigned ord = (unsigned)(bk >> 32);
+        cval[r] = __uint_as_float((ord & 0x80000000u) ? (ord & 0x7FFFFFFFu) : ~ord);
+        cpos[r] = sp[bi];
+        __syncwarp();
+        if (lane == 0) sk[bi] = 0ull;
+        __syncwarp();
+        ++got;
+    }
+    if (lane != 0 || got == 0) return;
+    const int sel = s.sel < got ? s.sel : got - 1;
+    if (A.out_val)
+        for (int j = 0; j < K; ++j) {
+            A.out_val[(long long)b * K + j] = j < got ? cval[j] : -CUDART_INF_F;
+            A.out_pos[(long long)b * K + j] = j < got ? cpos[j] : 0u;
+        }
+    // cvtIndexToPosition (CPUThreadDevice.cpp:257-268), unsigned arithmetic
+    const unsigned index = cpos[sel];
+    unsigned position = 0;
+    unsigned div = (unsigned)g.N;
+    for (int d = g.nd - 1; d >= 0; --d) {
+        unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
+        div /= f;
+        position = position * sr + ((f - (index / div) % f - (unsigned)s.mn[d] - 1u) + sr) % sr;
+    }
+    chosen = position;
+    if (A.drawn_score) {
+        A.drawn_score[s.node] = cval[sel];
+        A.drawn_scale[s.node] = 0.f;   // the audit's k best come from the same FP32 map: no tolerance
+    }
+    if (A.node_cell) A.node_cell[s.node] = chosen;
+    if (A.state)
+        for (int v = 0; v < A.nvar; ++v) {
+            float *dst = A.state + (long long)s.cell * A.nvar + v;
+            if (isnan(*dst)) *dst = A.ti[(long long)chosen * A.nvar + v];
+        }
+    if (A.id_image) A.id_image[s.cell] = chosen * A.nti + A.ti_id;
 }
 
 // ---------------------------------------------------------------------------
@@ -2728,6 +2870,12 @@ static void launch_replay_team(const ReplayArgs &a, size_t smem, cudaStream_t st
     else if (a.K <= 4) k_replay<4, T><<<blocks, 32 * T, smem, st>>>(a);
     else if (a.K <= 8) k_replay<8, T><<<blocks, 32 * T, smem, st>>>(a);
     else k_replay<16, T><<<blocks, 32 * T, smem, st>>>(a);
+}
+
+cudaError_t launch_hash_select(const ReplayArgs &a, cudaStream_t st) {
+    if (a.nslots <= 0) return cudaSuccess;
+    k_hash_select<<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {

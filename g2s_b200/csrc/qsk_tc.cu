@@ -47,7 +47,11 @@ constexpr int BKB = 128;                 // bytes of K per block: one 128-byte s
 constexpr int A_BYTES = BM * BKB;        // 16 KB
 constexpr int B_BYTES = BN * BKB;        // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int THREADS = 192;             // producer, MMA, 4 epilogue warps
+// epilogue groups: each group is four warps, one per TMEM lane quarter, and
+// takes every G-th 32-column chunk of a tile with its own top-W; more groups
+// hide more of the insertion latency (the W = 32 registers allow two)
+__host__ __device__ constexpr int epi_groups(int W) { return W <= 16 ? 4 : 2; }
+__host__ __device__ constexpr int threads_for(int W) { return 64 + 128 * epi_groups(W); }
 constexpr long long WAIT_CYCLES = 4000000000LL;   // about two seconds at 1.9 GHz
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -159,18 +163,40 @@ __device__ __forceinline__ float unordered(unsigned o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
 
+// insert key (larger than k[0]) into the ascending register array k of W
+// keys, dropping the minimum: the new key replaces k[0] and bubbles up by
+// compare-and-swap steps (no branch, no memory)
+template <int W>
+__device__ __forceinline__ void sorted_insert(unsigned long long (&k)[W], unsigned (&p)[W], unsigned long long key,
+                                              unsigned pos) {
+    k[0] = key;
+    p[0] = pos;
+#pragma unroll
+    for (int i = 0; i + 1 < W; ++i) {
+        const bool sw = k[i] > k[i + 1];
+        const unsigned long long a = k[i], b = k[i + 1];
+        const unsigned pa = p[i], pb = p[i + 1];
+        k[i] = sw ? b : a;
+        k[i + 1] = sw ? a : b;
+        p[i] = sw ? pb : pa;
+        p[i + 1] = sw ? pa : pb;
+    }
+}
+
 template <int KIND, int W, int STAGES>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(threads_for(W), 1)
     k_tc_shortlist(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_p, TcArgs a) {
     extern __shared__ uint8_t smem_raw[];
-    // 1024-byte aligned stage ring (the swizzle atom), then heap and barriers
+    // 1024-byte aligned stage ring (the swizzle atom), then heaps and barriers
     const unsigned raw = smem_u32(smem_raw);
     uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
     uint8_t *sA = smem;                                   // STAGES x A_BYTES
     uint8_t *sB = smem + STAGES * A_BYTES;                // STAGES x B_BYTES
-    unsigned long long *hk = reinterpret_cast<unsigned long long *>(smem + STAGES * STAGE_BYTES);  // W x BM keys
-    unsigned *hp = reinterpret_cast<unsigned *>(hk + W * BM);                                       // W x BM positions
-    uint64_t *bar = reinterpret_cast<uint64_t *>(hp + W * BM);
+    constexpr int G = epi_groups(W), EPI_WARPS = 4 * G, THREADS = threads_for(W);
+    // the other epilogue groups' W best per node, for the final merge: [group-1][entry][row]
+    unsigned long long *hk = reinterpret_cast<unsigned long long *>(smem + STAGES * STAGE_BYTES);
+    unsigned *hp = reinterpret_cast<unsigned *>(hk + (G - 1) * W * BM);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(hp + (G - 1) * W * BM);
     uint64_t *full = bar, *empty = bar + STAGES, *tfull = bar + 2 * STAGES, *tempty = tfull + 2, *done = tempty + 2;
     __shared__ unsigned tmem_base_s;
     __shared__ volatile int abort_s;
@@ -189,7 +215,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&tfull[b], 1);
-            mbar_init(&tempty[b], 4);
+            mbar_init(&tempty[b], EPI_WARPS);
         }
         mbar_init(done, 1);
         abort_s = 0;
@@ -199,11 +225,6 @@ __global__ void __launch_bounds__(THREADS, 1)
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_base_s))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    // heap keys start at 0: below every real key (ordered() of a real score is > 0)
-    for (int i = threadIdx.x; i < W * BM; i += THREADS) {
-        hk[i] = 0ull;
-        hp[i] = 0xFFFFFFFFu;
     }
     tc_fence_before();
     __syncthreads();
@@ -290,8 +311,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             mbar_wait(done, 0, nullptr);
         }
     } else {
-        // ---------------- epilogue: one thread per node ----------------
-        const int q = warp & 3;
+        // ---------------- epilogue: one thread per node and half ----------------
+        // warps 2..9: lane quarter q = warp % 4 (the TMEM lanes this warp may
+        // read), half h: the even or odd 32-column chunks of every tile
+        const int e = warp - 2;
+        const int q = warp & 3, h = e >> 2;   // lane quarter, group
         const int row = q * 32 + lane;
         const int node = tile_m * BM + row;
         const bool live = node < a.n_nodes;
@@ -305,8 +329,15 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int d = 0; d < 6; ++d) box[d] = a.node_box[node * 6 + d];
         }
-        unsigned long long *myk = hk + row;
-        unsigned *myp = hp + row;
+        // this half's W best keys in registers, ascending (rk[0] the minimum);
+        // keys start at 0, below every real key (ordered() of a score is > 0)
+        unsigned long long rk[W];
+        unsigned rp[W];
+#pragma unroll
+        for (int f = 0; f < W; ++f) {
+            rk[f] = 0ull;
+            rp[f] = 0xFFFFFFFFu;
+        }
         unsigned long long root = 0ull;
         float thr = -INFINITY;
         int i = 0;
@@ -323,64 +354,121 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const long long pos0 = t * BN;
+            const int pos0 = (int)(t * BN);
+            const float s = nscale * (a.pos_scale ? __ldg(a.pos_scale + t) : 1.f);
+            if (live && a.node_thr) {
+                const unsigned g = *(volatile unsigned *)(a.node_thr + node);
+                if (g) thr = fmaxf(thr, unordered(g));
+            }
+            // TI coordinates of the tile's first position
+            const int x0 = pos0 % a.X, y0 = (pos0 / a.X) % a.Y, z0 = pos0 / (a.X * a.Y);
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
+            for (int c = h; c < BN / 32; c += G) {
                 float v[32];
                 tmem_ld32(tmem + ((unsigned)(q * 32) << 16) + (unsigned)(b * BN + c * 32), v);
-                if (!live) continue;
-                const long long pc = pos0 + c * 32;
+                // candidates of this lane (0 for a dead row, a chunk whose best
+                // score is below the threshold, or no valid position); every
+                // lane reaches the warp-wide round count below
+                unsigned cand = 0u;
+                const int pc = pos0 + c * 32;
+                // a chunk's best score is exactly fmaf(max v, s, bias): fmaf is
+                // monotone in v for s > 0
+                float m01 = fmaxf(v[0], v[1]);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const long long p = pc + j;
-                    if (p >= a.n_pos) break;
-                    const float ps = a.pos_scale ? __ldg(a.pos_scale + p) : 1.f;
-                    const float sc = fmaf(v[j], nscale * ps, nbias);
-                    if (sc >= thr) {
-                        const unsigned long long key =
-                            ((unsigned long long)ordered(sc) << 32) | tie_hash(nseed, (unsigned)p);
-                        if (key > root) {
-                            // validity: the node's template lies inside the TI at p
-                            const int x = (int)(p % a.X);
-                            const long long yz = p / a.X;
-                            const int y = (int)(yz % a.Y), z = (int)(yz / a.Y);
-                            if (x >= box[0] && x < box[1] && y >= box[2] && y < box[3] && z >= box[4] && z < box[5]) {
-                                // replace the root, sift down (min-heap, entry e of this node at e*BM)
-                                int e = 0;
-                                for (;;) {
-                                    int l = 2 * e + 1;
-                                    if (l >= W) break;
-                                    unsigned long long kl = myk[l * BM];
-                                    if (l + 1 < W) {
-                                        const unsigned long long kr = myk[(l + 1) * BM];
-                                        if (kr < kl) {
-                                            kl = kr;
-                                            ++l;
-                                        }
-                                    }
-                                    if (kl >= key) break;
-                                    myk[e * BM] = kl;
-                                    myp[e * BM] = myp[l * BM];
-                                    e = l;
-                                }
-                                myk[e * BM] = key;
-                                myp[e * BM] = (unsigned)p;
-                                root = myk[0];
-                                thr = root ? unordered((unsigned)(root >> 32)) : -INFINITY;
-                            }
+                for (int j = 2; j < 32; ++j) m01 = fmaxf(m01, v[j]);
+                if (live && fmaf(m01, s, nbias) >= thr) {
+                    // validity of the chunk's 32 positions for this node (its
+                    // template inside the TI): the box cut row by row
+                    unsigned vmask = 0u;
+                    int x = x0 + c * 32, y = y0, z = z0;
+                    while (x >= a.X) {
+                        x -= a.X;
+                        if (++y == a.Y) {
+                            y = 0;
+                            ++z;
                         }
                     }
+                    const int end = (int)min((long long)pc + 32, a.n_pos);
+                    int qp = pc;
+                    while (qp < end) {
+                        const int row0 = qp - x;
+                        const int seg_end = min(end, row0 + a.X);
+                        if (y >= box[2] && y < box[3] && z >= box[4] && z < box[5]) {
+                            const int lo = max(qp, row0 + box[0]) - pc, hi = min(seg_end, row0 + box[1]) - pc;
+                            if (lo < hi) vmask |= (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+                        }
+                        qp = seg_end;
+                        x = 0;
+                        if (++y == a.Y) {
+                            y = 0;
+                            ++z;
+                        }
+                    }
+                    // at least the threshold; a tie with the heap's own minimum
+                    // qualifies only with a larger tie hash
+                    const float thr_loc = root ? unordered((unsigned)(root >> 32)) : -INFINITY;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const float sc = fmaf(v[j], s, nbias);
+                        bool cj = sc >= thr && ((vmask >> j) & 1u);
+                        if (cj && root != 0ull && sc == thr_loc) cj = tie_hash(nseed, (unsigned)(pc + j)) > (unsigned)root;
+                        cand |= cj ? (1u << j) : 0u;
+                    }
                 }
+                // insert them in rounds: every lane its next candidate
+                const int rounds = __reduce_max_sync(0xffffffffu, __popc(cand));
+                for (int r = 0; r < rounds; ++r) {
+                    if (!cand) continue;
+                    const int j = __ffs(cand) - 1;
+                    cand &= cand - 1u;
+                    // v[j] by a 5-level select tree
+                    float t16[16], t8[8], t4[4], t2[2];
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) t16[u] = (j & 1) ? v[2 * u + 1] : v[2 * u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) t8[u] = (j & 2) ? t16[2 * u + 1] : t16[2 * u];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) t4[u] = (j & 4) ? t8[2 * u + 1] : t8[2 * u];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) t2[u] = (j & 8) ? t4[2 * u + 1] : t4[2 * u];
+                    const float sc = fmaf((j & 16) ? t2[1] : t2[0], s, nbias);
+                    const int p = pc + j;
+                    const unsigned long long key = ((unsigned long long)ordered(sc) << 32) | tie_hash(nseed, (unsigned)p);
+                    if (key <= root) continue;
+                    sorted_insert<W>(rk, rp, key, (unsigned)p);
+                    root = rk[0];
+                    thr = root ? fmaxf(thr, unordered((unsigned)(root >> 32))) : thr;
+                }
+            }
+            // publish this heap's minimum: a lower bound of the node's W-th best
+            // over all positions, which every range may filter against
+            if (live && root && a.node_thr) {
+                atomicMax(a.node_thr + node, (unsigned)(root >> 32));
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        if (live) {
+        // the other groups hand their W best to group 0, which merges and
+        // writes the node's W best of this range
+        if (h > 0) {
+#pragma unroll
+            for (int f = 0; f < W; ++f) {
+                hk[((h - 1) * W + f) * BM + row] = rk[f];
+                hp[((h - 1) * W + f) * BM + row] = rp[f];
+            }
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(EPI_WARPS * 32) : "memory");
+        if (h == 0 && live) {
+            for (int f = 0; f < (G - 1) * W; ++f) {
+                const unsigned long long key = hk[f * BM + row];
+                if (key > rk[0]) sorted_insert<W>(rk, rp, key, hp[f * BM + row]);
+            }
             const size_t o = ((size_t)node * a.ranges + range) * W;
-            for (int e = 0; e < W; ++e) {
-                a.out_key[o + e] = myk[e * BM];
-                a.out_pos[o + e] = myp[e * BM];
+#pragma unroll
+            for (int f = 0; f < W; ++f) {
+                a.out_key[o + f] = rk[f];
+                a.out_pos[o + f] = rp[f];
             }
         }
     }
@@ -430,15 +518,27 @@ cudaError_t make_map(CUtensorMap *m, const void *base, int elem, long long k_ele
 template <int KIND, int W>
 cudaError_t launch_w(const CUtensorMap &ma, const CUtensorMap &mp, const TcArgs &a, int node_tiles,
                      cudaStream_t st) {
-    constexpr int HEAP = W * tc::BM * 12;
-    constexpr int STAGES = (W <= 16) ? 4 : 3;
+    constexpr int HEAP = (tc::epi_groups(W) - 1) * W * tc::BM * 12;
+    constexpr int STAGES = 3;
     constexpr int SMEM = 1024 + STAGES * tc::STAGE_BYTES + HEAP + (2 * STAGES + 5) * 8;
     static_assert(SMEM <= 232448, "shared memory");
     auto kern = tc::k_tc_shortlist<KIND, W, STAGES>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    // the shared-memory limit, once per device for this instantiation
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= 64 || !done[dev]) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) done[dev] = true;
+        }
+    }
     dim3 grid((unsigned)node_tiles, (unsigned)a.ranges);
-    kern<<<grid, tc::THREADS, SMEM, st>>>(ma, mp, a);
+    kern<<<grid, tc::threads_for(W), SMEM, st>>>(ma, mp, a);
     return cudaGetLastError();
 }
 
@@ -489,6 +589,16 @@ __device__ __forceinline__ void store_elem(void *base, long long idx, float v, i
     }
 }
 
+// FP8 E4M3 scale of a row whose largest magnitude is mx: the power of two
+// that brings mx to at most 448 (the format's largest finite value), so that
+// scaling and unscaling are exact
+__device__ __forceinline__ float pow2_scale(float mx) {
+    if (!(mx > 0.f)) return 1.f;
+    int e;
+    frexpf(mx / 448.f, &e);   // mx / 448 = f * 2^e, f in [0.5, 1)
+    return ldexpf(1.f, e);
+}
+
 // value of layer `ly` of the pattern matrix at TI cell q (natural index, x fastest)
 __device__ __forceinline__ float layer_value(const float *__restrict__ ti, int nvar, long long q, const TcLayer &ly) {
     const float t = ti[q * nvar + ly.var];
@@ -498,8 +608,10 @@ __device__ __forceinline__ float layer_value(const float *__restrict__ ti, int n
 }
 
 // P[p][j * L + l] = layer l at TI cell p + o_j (0 outside the TI); one warp
-// per row, FP8 rows scaled by their largest magnitude (pos_scale)
-__global__ void k_tc_pattern(TcPatternArgs A) {
+// per row.  FP8: pass 0 writes every row's largest magnitude to rowmax,
+// k_tc_tile_scale turns each tile of 256 rows into one power-of-two scale
+// (pos_scale[tile]), pass 1 writes the rows divided by their tile's scale.
+__global__ void k_tc_pattern(TcPatternArgs A, int pass, float *__restrict__ rowmax) {
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -513,7 +625,7 @@ __global__ void k_tc_pattern(TcPatternArgs A) {
         }
         const bool live = p < A.N;
         float scale = 1.f;
-        if (A.fmt == 1) {
+        if (A.fmt == 1 && pass == 0) {
             float mx = 0.f;
             if (live)
                 for (long long k = lane; k < (long long)A.T * A.L; k += 32) {
@@ -530,9 +642,10 @@ __global__ void k_tc_pattern(TcPatternArgs A) {
                 }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            scale = mx > 0.f ? mx / 448.f : 1.f;
-            if (lane == 0) A.pos_scale[p] = scale;
+            if (lane == 0) rowmax[p] = mx;
+            continue;
         }
+        if (A.fmt == 1) scale = A.pos_scale[p >> 8];
         const float inv = 1.f / scale;
         for (long long k = lane; k < A.Kp; k += 32) {
             float v = 0.f;
@@ -551,6 +664,14 @@ __global__ void k_tc_pattern(TcPatternArgs A) {
             store_elem(A.P, p * A.Kp + k, v, A.fmt);
         }
     }
+}
+
+__global__ void k_tc_tile_scale(long long tiles, const float *__restrict__ rowmax, float *__restrict__ scale) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= tiles) return;
+    float mx = 0.f;
+    for (int r = 0; r < 256; ++r) mx = fmaxf(mx, rowmax[t * 256 + r]);
+    scale[t] = pow2_scale(mx);
 }
 
 // largest template index among a node's neighbours; -1 for nodes without a
@@ -601,8 +722,9 @@ __global__ void k_tc_nodes(TcNodeArgs A) {
             mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
         }
     for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    const float scale = (A.fmt == 1 && amax > 0.f) ? amax / 448.f : 1.f;
+    const float scale = A.fmt == 1 ? pow2_scale(amax) : 1.f;
     const float inv = 1.f / scale;
+    float bias = 0.f;
     for (int j = lane; j < cnt; j += 32) {
         const int t = A.nb_tpl[(long long)i * A.n + j];
         const unsigned nc = A.nb_cell[(long long)i * A.n + j];
@@ -615,14 +737,26 @@ __global__ void k_tc_nodes(TcNodeArgs A) {
                 store_elem(A.A, (long long)warp * A.Kp + col, -w * inv, A.fmt);
                 store_elem(A.A, (long long)warp * A.Kp + col + 1, 2.f * __fmul_rn(w, val) * inv, A.fmt);
             } else {
-                const int nc_v = A.var_ncat[v];
-                for (int c = 0; c < nc_v; ++c)
-                    if (A.var_catv[v * QSK_CMAX + c] == val) store_elem(A.A, (long long)warp * A.Kp + col + c, w * inv, A.fmt);
+                // C categories, C-1 indicator layers: the last category's
+                // match is 1 minus the others' (its weight goes to the bias)
+                const int C = A.var_ncat[v];
+                int ci = -1;
+                for (int c = 0; c < C; ++c)
+                    if (A.var_catv[v * QSK_CMAX + c] == val) ci = c;
+                if (ci < 0) continue;   // no category of the TI: matches nowhere
+                if (ci < C - 1) {
+                    store_elem(A.A, (long long)warp * A.Kp + col + ci, w * inv, A.fmt);
+                } else {
+                    for (int c = 0; c < C - 1; ++c) store_elem(A.A, (long long)warp * A.Kp + col + c, -w * inv, A.fmt);
+                    bias += w;
+                }
             }
         }
     }
+    for (int o = 16; o > 0; o >>= 1) bias += __shfl_xor_sync(0xffffffffu, bias, o);
     if (lane == 0) {
         A.node_scale[warp] = scale;
+        A.node_bias[warp] = bias;
         for (int d = 0; d < 3; ++d) {
             const bool has = d < nd;
             A.node_box[warp * 6 + 2 * d] = has ? -mn[d] : 0;
@@ -630,6 +764,36 @@ __global__ void k_tc_nodes(TcNodeArgs A) {
         }
         A.node_seed[warp] = __float_as_uint(A.seeds[i]) ^ (unsigned(i) * 0x85EBCA6Bu);
     }
+}
+
+// exact score of one candidate from its staged layer values xs[t] (term t's
+// gathered value), in the plain map's term order (FP32, bit-identical to
+// k_map_records) and in FP64; `scale` is the term scale
+__device__ __forceinline__ void exact_score_staged(const Term *__restrict__ tm, int nt, const float *xs, float &s32,
+                                                   double &s64, double &scale) {
+    float acc = 0.f;
+    double a64 = 0.0, sc = 0.0;
+    for (int t = 0; t < nt; ++t) {
+        const Term T = tm[t];
+        const float x = xs[t];
+        if (T.op == OP_SQLIN) {
+            acc = __fmaf_rn(T.a, __fmul_rn(x, x), acc);
+            acc = __fmaf_rn(T.b, x, acc);
+            a64 += (double)T.a * ((double)x * (double)x) + (double)T.b * (double)x;
+            sc += -(double)T.a * ((double)x * (double)x) + ((double)T.b * (double)T.b) / (-4.0 * (double)T.a);
+        } else if (T.op == OP_EQ) {
+            acc = (x == T.b) ? __fadd_rn(acc, T.a) : acc;
+            a64 += (x == T.b) ? (double)T.a : 0.0;
+            sc += (double)T.a;
+        } else if (T.op == OP_LIN) {
+            acc = __fmaf_rn(T.a, x, acc);
+            a64 += (double)T.a * (double)x;
+            sc += fabs((double)T.a * (double)x);
+        }
+    }
+    s32 = acc;
+    s64 = a64;
+    scale = sc;
 }
 
 // exact score of one candidate at scan index m, in the plain map's term order
@@ -722,7 +886,9 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         __syncwarp();
         ++nsel;
     }
-    // exact scores of the shortlist
+    // exact scores of the shortlist: the scan index of every candidate, then
+    // all (candidate, term) layer values gathered by the whole warp at once
+    // into shared memory, then each candidate's term chain from there
     float e32[2] = {-INFINITY, -INFINITY};
     double e64[2] = {-INFINITY, -INFINITY}, esc[2] = {0.0, 0.0};
     unsigned hsh[2] = {0u, 0u};
@@ -730,19 +896,46 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     float errmax = 0.f;
     double errsum = 0.0;
     int errn = 0;
+    int *msc = reinterpret_cast<int *>(&spos[w][0]);   // candidate list no longer needed
     for (int h = 0; h < 2; ++h) {
         const int r = h * 32 + lane;
         if (r >= nsel) continue;
-        const unsigned p = mypos[h];
         // natural cell -> scan index of the reference's flipped space (cvtPositionToIndex)
         long long m = 0;
-        unsigned rem = p;
+        unsigned rem = mypos[h];
         for (int d = 0; d < g.nd; ++d) {
             const int pd = int(rem % (unsigned)g.src[d]);
             rem /= (unsigned)g.src[d];
             m += (long long)(g.fft[d] - 1 - pd - s.mn[d]) * g.sstride[d];
         }
-        exact_score(tt, nt, A.layers, m, e32[h], e64[h], esc[h]);
+        msc[r] = (int)m;
+    }
+    __syncwarp();
+    float *xs = reinterpret_cast<float *>(&skey[w][0]);   // 2 * SEL_CAND floats
+    const int per = (small && nt > 0) ? max(1, min(nsel, (2 * SEL_CAND) / nt)) : 0;
+    if (per > 0) {
+        for (int r0 = 0; r0 < nsel; r0 += per) {
+            const int r1 = min(nsel, r0 + per);
+            for (int r = r0; r < r1; ++r) {
+                const long long m = msc[r];
+                for (int t = lane; t < nt; t += 32) xs[(r - r0) * nt + t] = __ldg(A.layers + tt[t].base + m);
+            }
+            __syncwarp();
+            for (int h = 0; h < 2; ++h) {
+                const int r = h * 32 + lane;
+                if (r >= r0 && r < r1) exact_score_staged(tt, nt, xs + (r - r0) * nt, e32[h], e64[h], esc[h]);
+            }
+            __syncwarp();
+        }
+    } else {
+        for (int h = 0; h < 2; ++h) {
+            const int r = h * 32 + lane;
+            if (r < nsel) exact_score(tt, nt, A.layers, (long long)msc[r], e32[h], e64[h], esc[h]);
+        }
+    }
+    for (int h = 0; h < 2; ++h) {
+        const int r = h * 32 + lane;
+        if (r >= nsel) continue;
         const float approx = tc::unordered((unsigned)(mykey[h] >> 32));
         const double err = fabs((double)approx - e64[h]) / (esc[h] > 0.0 ? esc[h] : 1.0);
         errmax = fmaxf(errmax, (float)err);
@@ -844,11 +1037,16 @@ __global__ void k_tc_audit(int n, const int *__restrict__ nodes, int K, const fl
 
 }  // namespace
 
-cudaError_t launch_tc_pattern(const TcPatternArgs &a, cudaStream_t st) {
+cudaError_t launch_tc_pattern(const TcPatternArgs &a, float *rowmax, cudaStream_t st) {
     long long warps = a.rows;
     long long blocks = (warps * 32 + 255) / 256;
     if (blocks > 148LL * 64) blocks = 148LL * 64;
-    k_tc_pattern<<<(unsigned)blocks, 256, 0, st>>>(a);
+    if (a.fmt == 1) {
+        k_tc_pattern<<<(unsigned)blocks, 256, 0, st>>>(a, 0, rowmax);
+        const long long tiles = a.rows / 256;
+        k_tc_tile_scale<<<(unsigned)((tiles + 255) / 256), 256, 0, st>>>(tiles, rowmax, a.pos_scale);
+    }
+    k_tc_pattern<<<(unsigned)blocks, 256, 0, st>>>(a, 1, rowmax);
     return cudaGetLastError();
 }
 

@@ -54,7 +54,7 @@ int qsk_tc_topk(int device, int fmt, int B, long long N, int K, const void *quer
                              cudaMemcpyHostToDevice, st));
     if (q_scale) QSK_CK(dqs.upload(q_scale, size_t(B), st));
     if (q_bias) QSK_CK(dqb.upload(q_bias, size_t(B), st));
-    if (p_scale) QSK_CK(dps.upload(p_scale, size_t(N), st));
+    if (p_scale) QSK_CK(dps.upload(p_scale, size_t((N + 255) / 256), st));
     if (q_seed) QSK_CK(dseed.upload(q_seed, size_t(B), st));
     QSK_CK(dbox.upload(q_box, size_t(B) * 6, st));
     const size_t nout = size_t(B) * size_t(ranges) * size_t(W);
@@ -77,6 +77,7 @@ int qsk_tc_topk(int device, int fmt, int B, long long N, int K, const void *quer
     a.node_box = dbox.p;
     a.X = X;
     a.Y = Y;
+    a.node_thr = nullptr;   // per-range top W, as documented (no shared bound across ranges)
     a.out_key = dkey.p;
     a.out_pos = dpos.p;
     a.status = dstat.p;

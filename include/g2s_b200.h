@@ -246,8 +246,9 @@ int qsk_pattern_kbest_noalloc(const qsk_ti *ti, void *stream, int n_neighbours, 
  *             (uint8 bit patterns)
  *   queries   B x K row-major, rows N x K row-major (N: positions of a TI
  *             of X x Y x (N / (X*Y)) cells, x fastest)
- *   score(q, p) = (queries[q] . rows[p]) * q_scale[q] * p_scale[p] + q_bias[q]
- *             accumulated in FP32 (scales and bias may be NULL: 1 and 0)
+ *   score(q, p) = (queries[q] . rows[p]) * q_scale[q] * p_scale[p / 256] + q_bias[q]
+ *             accumulated in FP32; p_scale holds one scale per tile of 256
+ *             rows (scales and bias may be NULL: 1 and 0)
  *   q_box     6 ints per query: p = (x, y, z) is a candidate iff
  *             q_box[0] <= x < q_box[1], q_box[2] <= y < q_box[3],
  *             q_box[4] <= z < q_box[5]
@@ -320,6 +321,23 @@ typedef struct {
     float ms_prep;                /* ... inside the per-batch prep kernel (profiling mode only) */
     float ms_replay;              /* ... inside the k-best replay kernel (profiling mode only) */
     long long map_positions;      /* scan positions evaluated by the map kernel (nodes x N) */
+    /* tensor-core form (qsk_sim_set_tensor); zero when it is off */
+    int tensor_mode;              /* 0 plain, 1 BF16, 2 FP8 E4M3 */
+    int tensor_prefix;            /* template offsets in the pattern matrix */
+    int tensor_width;             /* heap entries per node and position range */
+    int tensor_shortlist;         /* candidates re-scored exactly per node */
+    long long tensor_nodes;       /* nodes drawn by the tensor-core form */
+    long long plain_nodes;        /* nodes left to the exact map (neighbours beyond the prefix, marginal draws) */
+    long long audited;            /* nodes re-run on the plain path for the regret audit */
+    long long regret;             /* audited nodes whose draw lies outside the exact k best */
+    long long regret_near;        /* audited nodes below the exact k-th score by at most 1e-5 of the term scale */
+    float map_err_max;            /* largest |tensor-core score - FP64 score| / term scale, re-scored candidates */
+    float map_err_mean;
+    double tensor_flops;          /* MMA flops issued (2 x 128 x 256 x K per tile) */
+    float ms_tensor_gemm;         /* device time of the tensor-core kernel (profiling mode only) */
+    float ms_tensor_select;       /* ... of node rows, re-score and draw (profiling mode only) */
+    float ms_tensor_pattern;      /* device time of building the pattern matrix (once per simulation) */
+    long long tensor_launches;
 } qsk_sim_info;
 
 typedef struct qsk_sim qsk_sim;
@@ -333,6 +351,15 @@ int qsk_sim_run(qsk_sim *s);
  * grid (host array), as the sequential run would at that node's turn.
  * id_completed (the run's index image) is needed with -nV, else may be NULL. */
 int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *id_completed);
+/* Teacher-forced evaluation of a sample of path nodes (indices into the
+ * path, 0 .. nodes-1, any order): each is drawn against the completed grid as
+ * the sequential run would at its turn, nothing is written back; the
+ * neighbour search over the whole path runs once per simulation object and
+ * is not part of the run's device time (qsk_sim_info.ms_total).  For
+ * simulations too large to time in full (G2S times its own runs whole,
+ * src/qs.cpp:2229-2235).  node_cell of qsk_sim_read holds the sample's
+ * choices at their path indices. */
+int qsk_sim_run_teacher_nodes(qsk_sim *s, const float *di_completed, const int *path_nodes, int count);
 /* Copy results to the host: the grid, the index image (TI cell * nTI + TI,
  * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL). */
 int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out);
@@ -352,6 +379,39 @@ int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node)
 /* Path (cell order), per-path-index seeds and number of informed cells. */
 int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
 int qsk_sim_destroy(qsk_sim *s);
+
+/* Tensor-core form of the map (no G2S counterpart; it replaces, for the nodes
+ * it can take, the per-node FFT correlation and k-best of
+ * CPUThreadDevice::candidateForPattern + fKst::findKBiggest, G2S
+ * src/CPUThreadDevice.cpp:349-490, include/fKb.hpp:907-954, and of the CUDA
+ * device's cuFFT + cublasIsamin, src/NvidiaGPUAcceleratorDevice.cu:462-727).
+ * Nodes of one dependency level share the TI, so their cross terms over the
+ * first `prefix` template offsets are one GEMM: (nodes x K) . (K x TI cells)
+ * on tcgen05 in BF16 or FP8 E4M3 (per-row scales), FP32 accumulation in TMEM.
+ * Per node the `width` best approximate scores of every position range are
+ * kept, the best `shortlist` of them re-scored exactly (the plain map's FP32
+ * term order; FP64 for FP8), the node's k best taken by exact score (equal
+ * scores in the order of a per-node hash, not the reference's reservoir) and
+ * the quantile rank drawn.  Nodes with a neighbour beyond the prefix take the
+ * exact map in the same level with the same draw rule (k best by score, ties
+ * by the hash, over the map's records); nodes without neighbours the
+ * reference's marginal draw.  A fraction `audit` of the nodes with
+ * neighbours is re-run on the plain path after the simulation,
+ * teacher-forced on the final grid: `regret` counts those whose drawn
+ * candidate scores below the exact k-th (qsk_sim_info).
+ * Complete TIs only, without -nV, -fs or local controls.  Zero fields take
+ * the automatic choice: prefix = the smallest multiple of 256 offsets that
+ * covers 97 % of the path's nodes (chosen at the first tensor run from the
+ * nodes' neighbour lists), capped by a 16 GiB pattern matrix; width 8 (FP8:
+ * 32), shortlist 4 x extendK (FP8: 64). */
+typedef struct {
+    int mode;          /* 0 plain (the exact reference path), 1 BF16, 2 FP8 E4M3 */
+    int prefix;        /* template offsets in the pattern matrix */
+    int width;         /* 8, 16 or 32 */
+    int shortlist;     /* <= 64 */
+    float audit;       /* fraction of tensor-path nodes audited, 0..1 */
+} qsk_tensor_opts;
+int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *opts);
 
 /* Host-only planning helpers (no GPU needed), identical to what
  * qsk_sim_create computes.

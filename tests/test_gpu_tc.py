@@ -48,7 +48,7 @@ def to_bits(x, fmt):
 
 def reference(q, r, box, X, Y, W, ranges, qs, qb, ps, seed, n_tiles):
     B, N = q.shape[0], r.shape[0]
-    s = (q.astype(np.float64) @ r.astype(np.float64).T) * qs[:, None] * ps[None, :] + qb[:, None]
+    s = (q.astype(np.float64) @ r.astype(np.float64).T) * qs[:, None] * ps[np.arange(N) // 256][None, :] + qb[:, None]
     s32 = s.astype(np.float32)
     p = np.arange(N)
     x, y, z = p % X, (p // X) % Y, p // (X * Y)
@@ -81,7 +81,7 @@ def test_tc_topk_exact_integer_data(g2s, gpu, fmt, K, W, ranges):
     r[::7] = r[3]                                  # repeated rows: exact score ties
     qs = (2.0 ** rng.integers(-2, 3, B)).astype(np.float32)
     qb = rng.integers(-50, 50, B).astype(np.float32)
-    ps = (2.0 ** rng.integers(-1, 2, N)).astype(np.float32) if fmt == 1 else np.ones(N, np.float32)
+    ps = (2.0 ** rng.integers(-1, 2, -(-N // 256))).astype(np.float32) if fmt == 1 else np.ones(-(-N // 256), np.float32)
     seed = rng.integers(0, 2 ** 32, B, dtype=np.uint64).astype(np.uint32)
     box = np.zeros((B, 6), np.int32)
     box[:, 0] = rng.integers(0, 10, B)
