@@ -1,28 +1,47 @@
-"""QuickSampling throughput on B200 — QS nodes/s.
-
-Workload (the benchmark configuration that fits one GPU): binary sinuous-
-channel training image 250x250 (20 channels, ~25-30 % facies 1, seed 1),
-unconditional categorical simulation of a 500x500 grid, n=80 neighbours,
-k=1.5, seed 100 (+ rank): 250,000 path nodes per step.  One step is one
-complete simulation on the GPU (neighbour search, dependency levels, every
-node's mismatch map, k-best and draw).  Synthetic seeded data only.
+"""QuickSampling throughput on B200 — QS nodes/s, tensor-core form against the
+plain FP32 path, at the k-best regret the audit measures.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload config1|config0|config3] [--path bf16|fp8|plain|fp32]
+
+Workloads (seeded synthetic inputs; no public dataset is involved):
+  config1 (default)  binary sinuous-channel TI 250x250 (20 channels, seed 1),
+                     unconditional categorical simulation 500x500, n=80,
+                     k=1.5, seed 100 (+ rank): 250,000 path nodes per step,
+                     one step = one whole simulation (levels of independent
+                     nodes, every node's map, k best and draw).  Default
+                     path: BF16 tensor-core form.
+  config0            continuous GRF TI 200x200 (exponential covariance, range
+                     12 px), simulation 200x200, n=50, k=1.2.  BF16.
+  config3            continuous 3-D GRF TI 180x150x120 (ranges 20,20,5
+                     voxels), simulation 200x200x100 (4 M nodes), n=60,
+                     k=1.2.  A step is the teacher-forced draw of a fixed
+                     sample of 16,000 path nodes (every 250th) against a
+                     completed 200x200x100 GRF grid (seed 2): the whole
+                     simulation is too long to repeat K times on the plain
+                     path.  Default path: FP8 E4M3.
+Paths: bf16 / fp8 (tensor-core form, 1 % of the nodes audited on the plain
+path), plain (the exact reference path: bit-sliced counts for categorical
+unit-weight patterns, FP32 gather otherwise), fp32 (the exact path with the
+FP32 gather map forced).  The headline path is timed over K steps; the
+plain and fp32 paths of the same workload over two steps each, for the
+ratio.
 
 Multi-GPU: replicas only — each rank simulates its own realisation (seed +
 rank); no data-path collective exists in this algorithm.  ``value`` is the
 total nodes of all ranks divided by the slowest rank's device time.
 
 The reference arm (``--impl reference``) runs the G2S reference CPU
-QuickSampling (built from the G2S sources, FFTW replaced by the project's
-FFT shim) on the host cores with all threads, on a bounded sample of the same
-workload (a smaller grid with the same TI, n and k; per-node cost of the
-reference is dominated by its FFTs over the TI and does not depend on the
-grid size).
+QuickSampling (built from the G2S sources; FFTW replaced by the project's
+FFT shim unless the host has a libfftw3f) on the host cores with all
+threads, on the same TI, n and k: the full grid for configs 0 and 1, a
+small grid for config 3 (the reference's cost per node is its FFTs over the
+TI, independent of the grid).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes.util
 import json
 import os
 import statistics
@@ -38,24 +57,29 @@ sys.path.insert(0, ROOT)
 
 METRIC = "QS nodes/s on 1 B200: tensor-core/learned vs plain FP32 at ≤1% k-best regret"
 UNIT = "nodes/s"
-TI_SHAPE = (250, 250)
-DI_SHAPE = (500, 500)
-N_NB, K_CAND, SEED = 80, 1.5, 100
-WORKLOAD = "config1-categorical-channels-250x250-to-500x500-n80-k1.5"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-# DRAM bytes (read + write) per launch, averaged over every launch of one
-# step of the default workload, from one ncu capture of this script
-# (dram__bytes_read.sum + dram__bytes_write.sum; cold-cache, launches serialised)
-TRAFFIC_PER_LAUNCH = {("config1", "k_replay"): 14.54e6, ("config1", "k_map_bits"): 12.07e6}
+# DRAM bytes (read + write) per launch of the dominant kernel, from the ncu
+# captures summarised under profiles/ (per workload and kernel)
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
+
+WORKLOADS = {
+    "config1": dict(ti=("channels", (250, 250)), di=(500, 500), types=[1], n=80, k=1.5, path="bf16",
+                    name="config1-categorical-channels-250x250-to-500x500-n80-k1.5"),
+    "config0": dict(ti=("grf", (200, 200), (12, 12)), di=(200, 200), types=[0], n=50, k=1.2, path="bf16",
+                    name="config0-continuous-grf-200x200-to-200x200-n50-k1.2"),
+    "config3": dict(ti=("grf", (120, 150, 180), (5, 20, 20)), di=(100, 200, 200), types=[0], n=60, k=1.2, path="fp8",
+                    sample=250, name="config3-continuous-grf3d-180x150x120-to-200x200x100-n60-k1.2-sample16000"),
+}
+SEED = 100
 
 
 def peaks():
     try:
         with open(MEASURED_PEAKS) as f:
             p = json.load(f)
-        return float(p["hbm_gbs"]), "measured"
+        return p, "measured"
     except Exception:
-        return 6650.0, "fallback"
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
 class ClockSampler:
@@ -138,56 +162,99 @@ def dist_env():
     return ws, rank, local
 
 
+def make_inputs(w):
+    from g2s_b200 import synthetic as syn
+    kind = w["ti"][0]
+    if kind == "channels":
+        ti = syn.channels2d(w["ti"][1], n_channels=20, seed=1)
+    else:
+        ti = syn.grf(w["ti"][1], w["ti"][2], seed=1)
+    di = np.full(w["di"], np.nan, np.float32)
+    done = None
+    if w.get("sample"):
+        done = syn.grf(w["di"], w["ti"][2], seed=2)
+    return ti, di, done
+
+
+def fft_in_use() -> str:
+    lib = ctypes.util.find_library("fftw3f")
+    return f"FFTW3f API shim (project FFT; no libfftw3f on this host)" if not lib else \
+        f"FFTW3f API shim (project FFT; this host also has {lib}, not linked)"
+
+
+def reference_measure(args, w, steps: int):
+    """G2S reference CPU QS on the host cores: (nodes/s per step, description)."""
+    from oracle import ref
+    cores = os.cpu_count() or 1
+    ti, di, _ = make_inputs(w)
+    if w.get("sample"):
+        di = np.full((5, 10, 10), np.nan, np.float32)   # per-node cost: FFTs over the TI, not the grid
+        what = "5x10x10 grid (500 nodes) on the same TI, n and k"
+    else:
+        what = f"the full {'x'.join(str(d) for d in w['di'])} grid ({di.size} nodes)"
+    qsargs = ["-k", str(w["k"]), "-n", str(w["n"]), "-s", str(SEED), "-j", str(cores)]
+    vals = []
+    for s in range(max(1, steps)):
+        _, _, ms, _ = ref.run_qs(ti, di, w["types"], qsargs, job_id=9100 + s)
+        vals.append(di.size / (ms / 1000.0))
+    return vals, cores, f"G2S qs, {what}, -j {cores}, its reported compute time; {fft_in_use()}"
+
+
 def reference_arm(args):
-    """G2S reference CPU QS on the host cores: bounded sample of the workload."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     from oracle import ref
-    from g2s_b200 import synthetic as syn
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libg2sref.so not built (needs the G2S sources)"}))
         return 0
-    cores = os.cpu_count() or 1
-    ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
-    side = int(args.ref_side)
-    di = np.full((side, side), np.nan, np.float32)
-    qsargs = ["-k", str(K_CAND), "-n", str(N_NB), "-s", str(SEED), "-j", str(cores)]
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        ref.run_qs(ti, np.full((32, 32), np.nan, np.float32), [1], qsargs, job_id=9000)
-    vals = []
-    for s in range(args.steps):
-        sim, idx, ms, _ = ref.run_qs(ti, di, [1], qsargs, job_id=9100 + s)
-        vals.append(side * side / (ms / 1000.0))
+    w = WORKLOADS[args.workload]
+    vals, cores, sample = reference_measure(args, w, args.steps)
     v = float(np.mean(vals))
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": float(side * side / v * 1000.0), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"{side}x{side} grid ({side * side} of the 250000 nodes), same TI/n/k",
-                   "threads": cores},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"G2S qs (FFTW-API shim), {side}x{side} grid, -j {cores}, reported compute time"},
+        "warmup": args.warmup, "ms_per_step": float(1000.0 * np.prod(w["di"]) / v) if not w.get("sample") else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w["name"], "threads": cores},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
     return 0
 
 
-def cpu_baseline_leg(side: int):
-    """Reference CPU QS timed on the host cores (rank 0, N=1 only)."""
-    from oracle import ref
-    from g2s_b200 import synthetic as syn
-    if not ref.available():
-        return None
-    cores = os.cpu_count() or 1
-    ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
-    di = np.full((side, side), np.nan, np.float32)
-    sim, idx, ms, _ = ref.run_qs(ti, di, [1], ["-k", str(K_CAND), "-n", str(N_NB), "-s", str(SEED), "-j", str(cores)],
-                                 job_id=9500)
-    v = side * side / (ms / 1000.0)
-    return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"G2S qs (FFTW-API shim) on {side}x{side} grid ({side * side} nodes), same TI/n/k, -j {cores}"}
+def run_step(sim, w, done, sample):
+    """One step on the device; returns the engine's info (device time in ms_total)."""
+    if w.get("sample"):
+        sim.run_teacher_nodes(done, sample)
+    else:
+        sim.run()
+    return sim.info()
+
+
+def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flush, clk=None):
+    """Timed steps of one path; returns (total device ms, per-step infos, profiled info, sim info)."""
+    sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
+    if path in ("bf16", "fp8"):
+        sim.set_tensor(path, audit=0.01)
+    g2s.set_map_mode(1 if path == "fp32" else 0)
+    import torch
+    for _ in range(max(warmup, 0)):
+        run_step(sim, w, done, sample)
+    torch.cuda.synchronize()
+    infos = []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        infos.append(run_step(sim, w, done, sample))
+    torch.cuda.synchronize()
+    total = float(sum(i["ms_total"] for i in infos))
+    sim.set_profiling(True)
+    pinf = run_step(sim, w, done, sample)
+    sim.set_profiling(False)
+    g2s.set_map_mode(0)
+    sim.close()
+    return total, infos, pinf
 
 
 def main():
@@ -196,22 +263,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
-    ap.add_argument("--ref-side", type=int, default=120)
+    ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
+    ap.add_argument("--path", default="", choices=["", "bf16", "fp8", "plain", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--workload", default="config1", choices=["config1", "config0"],
-                    help="config1 (default, the benchmark line) or config0 (continuous GRF 200x200, n=50, k=1.2)")
-    ap.add_argument("--di-side", type=int, default=0,
-                    help="simulate an SxS grid instead of the workload's (small cases for profiling)")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain / fp32 comparison arms")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
 
     import torch
     import g2s_b200 as g2s
-    from g2s_b200 import synthetic as syn
 
-    global TI_SHAPE, DI_SHAPE, N_NB, K_CAND, WORKLOAD
+    w = WORKLOADS[args.workload]
+    path = args.path or w["path"]
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = None
@@ -220,115 +285,152 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = local
-
-    types = [1]
-    if args.workload == "config0":
-        TI_SHAPE, DI_SHAPE, N_NB, K_CAND = (200, 200), (200, 200), 50, 1.2
-        WORKLOAD = "config0-continuous-grf-200x200-to-200x200-n50-k1.2"
-        ti = syn.grf(TI_SHAPE, (12, 12), seed=1)
-        types = [0]
-    else:
-        ti = syn.channels2d(TI_SHAPE, n_channels=20, seed=1)
-    if args.di_side > 0:
-        DI_SHAPE = (args.di_side, args.di_side)
-        WORKLOAD += f"-grid{args.di_side}x{args.di_side}"
-    di = np.full(DI_SHAPE, np.nan, np.float32)
+    ti, di, done = make_inputs(w)
+    sample = None
+    if w.get("sample"):
+        sample = np.arange(0, int(np.prod(w["di"])), w["sample"], dtype=np.int32)
     seed = replica_seed(SEED, rank)
-    sim = g2s.Simulation(ti, di, types, n=N_NB, k=K_CAND, seed=seed, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")  # > 126 MB L2
+    own_peaks = g2s.measure_peaks(dev)
 
-    for _ in range(max(args.warmup, 0)):
-        sim.run()
-    torch.cuda.synchronize()
-
-    # timed region: device time of each full simulation (CUDA events inside
-    # the engine, first to last kernel on its stream); L2 flushed between steps
-    step_ms = []
-    launches = 0
+    # headline path: K timed steps (CUDA events inside the engine, first to
+    # last kernel of each step on its stream), L2 flushed between steps
     with ClockSampler(dev) as clk:
         if dist:
             dist.barrier()
-        torch.cuda.synchronize()
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            sim.run()
-            inf = sim.info()
-            step_ms.append(inf["ms_total"])
-            launches += int(inf["launches"])
-        torch.cuda.synchronize()
+        total_ms, infos, pinf = time_path(g2s, w, ti, di, done, sample, seed, dev, path, args.steps, args.warmup,
+                                          flush)
         if dist:
             dist.barrier()
     clocks = clk.summary()
-    total_ms = float(sum(step_ms))
-    nodes = int(sim.info()["nodes"])
+    nodes = int(infos[-1]["nodes"])
     total_ms = slowest(total_ms, dist, f"cuda:{dev}")
     value = whole_job_rate(nodes, args.steps, ws, total_ms)
+    launches = int(sum(i["launches"] for i in infos))
 
-    # roofline of the dominant kernel: one extra profiled step records events
-    # around every launch.  Algorithmic bytes per node of the reference
-    # path: the fused map reads 4*N*L bytes of correlation layers, the k-best
-    # scan 4*N bytes of scores.
-    sim.set_profiling(True)
-    sim.run()
-    pinf = sim.info()
-    sim.set_profiling(False)
-    map_kernel = "k_map_bits" if types == [1] else "k_map_records"
-    N = TI_SHAPE[0] * TI_SHAPE[1]
-    L = 2  # continuous: TI^2 and TI; binary categorical: 2 class indicators
-    launches_l = max(pinf["map_launches"], 1)
-    nodes_per_launch = pinf["map_positions"] / launches_l / N
-    peak, peak_kind = peaks()
+    # the plain paths on the same workload (two steps each): the ratio's denominator
+    compare = {}
+    if not args.no_compare:
+        for p in ("plain", "fp32"):
+            if p == path or (p == "fp32" and w["types"] != [1]):
+                continue   # continuous patterns: the plain path is the FP32 gather map already
+            t, inf2, _ = time_path(g2s, w, ti, di, done, sample, seed, dev, p, 2, 1, flush)
+            t = slowest(t, dist, f"cuda:{dev}")
+            compare[p] = {"value": whole_job_rate(nodes, 2, ws, t), "ms_per_step": t / 2,
+                          "kernel": ("k_map_bits" if (p == "plain" and w["types"] == [1]) else "k_map_records") +
+                                    " + k_replay (exact reservoir k-best)"}
+
+    # roofline of the dominant kernel of the profiled step
+    pk, pk_kind = peaks()
+    tensor = path in ("bf16", "fp8")
     kernels = {}
-    for name, ms, bpn in ((map_kernel, pinf["ms_map"], 4 * N * L), ("k_replay", pinf["ms_replay"], 4 * N)):
-        avg_ms = ms / launches_l
-        ach = bpn * nodes_per_launch / (avg_ms / 1000.0) / 1e9
-        kernels[name] = {"ms_per_step": ms, "launches": launches_l, "avg_launch_ms": avg_ms,
-                         "algorithmic_bytes_per_node": bpn, "achieved": ach, "frac": ach / peak,
-                         "share_of_step": ms / max(pinf["ms_total"], 1e-9),
-                         "traffic": TRAFFIC_PER_LAUNCH.get((args.workload, name)) if args.di_side == 0 else None}
-    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
-    roofline = {"bound": "hbm", "achieved": kernels[dom]["achieved"], "peak": peak, "unit": "GB/s",
-                "frac": kernels[dom]["frac"], "traffic": kernels[dom]["traffic"], "kernel": dom,
-                "peak_kind": f"{peak_kind} hbm_gbs", "nodes_per_launch": nodes_per_launch,
-                "algorithmic_bytes": f"{map_kernel}: 4*N*L per node, k_replay: 4*N per node (N={N}, L={L})",
-                "kernels": kernels}
-    out_info = sim.info()
-    sim.close()
+    if tensor:
+        gemm_ms = max(pinf["ms_tensor_gemm"], 1e-9)
+        tc_peak = pk.get("bf16_tflops", 1590.0) if path == "bf16" else own_peaks["fp8_tflops"]
+        tc_peak_kind = (f"{pk_kind} bf16_tflops (cuBLAS, burst)" if path == "bf16" else
+                        "fp8 E4M3 dense, this library's tcgen05 microbenchmark (qsk_measure_peaks)")
+        ach = pinf["tensor_flops"] / (gemm_ms / 1000.0) / 1e12
+        kernels["k_tc_shortlist"] = {"ms_per_step": pinf["ms_tensor_gemm"], "bound": "tensor",
+                                     "achieved_tflops": ach, "peak_tflops": tc_peak, "frac": ach / tc_peak,
+                                     "issued_flops_per_step": pinf["tensor_flops"]}
+        kernels["k_prep_sim+k_tc_nodes+k_tc_select"] = {"ms_per_step": pinf["ms_tensor_select"]}
+        kernels["pattern_matrix_build_once"] = {"ms": pinf["ms_tensor_pattern"]}
+    kernels["exact_map (" + ("k_map_bits" if w["types"] == [1] else "k_map_records") + ")"] = {
+        "ms_per_step": pinf["ms_map"], "map_launches": pinf["map_launches"]}
+    kernels["k_replay / k_hash_select"] = {"ms_per_step": pinf["ms_replay"]}
+    traffic = None
+    try:
+        traffic = json.load(open(TRAFFIC_FILE)).get(args.workload, {}).get("k_tc_shortlist" if tensor else "map")
+    except Exception:
+        pass
+    if tensor:
+        k = kernels["k_tc_shortlist"]
+        launches_gemm = max(1, int(pinf["tensor_launches"]) // 4)
+        roofline = {"bound": "tensor", "achieved": k["achieved_tflops"], "peak": k["peak_tflops"], "unit": "TFLOP/s",
+                    "frac": k["frac"], "traffic": traffic, "kernel": "k_tc_shortlist", "peak_kind": tc_peak_kind,
+                    "launches_per_step": launches_gemm,
+                    "algorithmic_work": "issued MMA flops 2 x 128 x 256 x K per (node tile, position tile); "
+                                        "K = template offsets up to the tile's widest node x pattern layers",
+                    "kernels": kernels}
+    else:
+        fp32 = own_peaks["fp32_tflops"]
+        N = int(np.prod(w["ti"][1]))
+        L = 2
+        useful = 2.0 * w["n"] * N * L * nodes / (pinf["ms_map"] / 1000.0) / 1e12
+        roofline = {"bound": "fp32" if w["types"] != [1] else "alu", "achieved": useful, "peak": fp32,
+                    "unit": "TFLOP/s (FP32-equivalent 2*n*N*L per node)", "frac": useful / fp32, "traffic": traffic,
+                    "kernel": "exact map", "peak_kind": "FP32 FMA, this library's microbenchmark (qsk_measure_peaks)",
+                    "kernels": kernels}
 
-    # e2e: the public one-call API with host buffers (H2D of TI+grid, D2H of
-    # grid+index image inside the timed region), wall clock around the call
+    # e2e: the public one-call API with host buffers (H2D of the inputs, D2H
+    # of the results inside the timed region), wall clock around the call
     e2e_vals = []
+    h2d = d2h = 0
     for _ in range(0 if args.no_e2e else max(1, min(args.steps, 3))):
-        d = np.full(DI_SHAPE, np.nan, np.float32)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        g2s.qs(ti, d, types, k=K_CAND, n=N_NB, s=seed, device=dev)
+        if w.get("sample"):
+            sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
+            if path in ("bf16", "fp8"):
+                sim.set_tensor(path, audit=0.01)
+            sim.run_teacher_nodes(done, sample)
+            _, _, cells = sim.read()
+            sim.close()
+            h2d, d2h = ti.nbytes + done.nbytes + di.nbytes + sample.nbytes, int(done.nbytes + di.size * 4 + cells.nbytes)
+        else:
+            d = np.full(w["di"], np.nan, np.float32)
+            g2s.qs(ti, d, w["types"], k=w["k"], n=w["n"], s=seed, device=dev,
+                   tensor=path if path in ("bf16", "fp8") else None)
+            h2d, d2h = ti.nbytes + di.nbytes, int(di.nbytes + di.size * 4)
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_vals)) if e2e_vals else float("nan")
     e2e_s = slowest(e2e_s, dist, f"cuda:{dev}")
-    e2e = {"value": nodes * ws / e2e_s if e2e_vals else None, "unit": UNIT,
-           "h2d_bytes_per_step": int(ti.nbytes + di.nbytes),
-           "d2h_bytes_per_step": int(di.nbytes + di.size * 4)}
+    e2e = {"value": nodes * ws / e2e_s if e2e_vals else None, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h)}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline and args.workload == "config1":
-        cpu = cpu_baseline_leg(args.ref_side)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            vals, cores, samp = reference_measure(args, w, 1)
+            cpu = {"value": float(np.mean(vals)), "unit": UNIT, "cores": cores, "kind": "reference", "sample": samp}
 
     if rank == 0:
+        last = infos[-1]
+        plain_v = compare.get("plain", {}).get("value")
+        fp32_v = compare.get("fp32", {}).get("value")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u8" if types == [1] else "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD,
-                       "path": ("bit-sliced categorical match counts (equal to the FP32 map)" if types == [1] else
-                                "FP32 direct-sum map") + " + exact reservoir k-best replay (CUDA cores)",
-                       "nodes_per_step": nodes, "levels": out_info["levels"], "max_batch": out_info["max_batch"],
+            "dtype": {"bf16": "bf16", "fp8": "fp8-e4m3", "plain": "u8" if w["types"] == [1] else "f32",
+                      "fp32": "f32"}[path],
+            "data": "synthetic",
+            "config": {"workload": w["name"], "path": path,
+                       "tensor": {"prefix": last["tensor_prefix"], "width": last["tensor_width"],
+                                  "shortlist": last["tensor_shortlist"], "tensor_nodes": last["tensor_nodes"],
+                                  "exact_map_nodes": last["plain_nodes"], "audit_fraction": 0.01} if tensor else None,
+                       "nodes_per_step": nodes, "levels": last["levels"], "max_batch": last["max_batch"],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
+            "vs_plain": {"plain": compare.get("plain"), "fp32_gather": compare.get("fp32"),
+                         "speedup_vs_plain": value / plain_v if plain_v else None,
+                         "speedup_vs_fp32_gather": value / fp32_v if fp32_v else None},
+            "regret": {"audited": int(sum(i["audited"] for i in infos)), "regret": int(sum(i["regret"] for i in infos)),
+                       "near_tie": int(sum(i["regret_near"] for i in infos)),
+                       "rate": (sum(i["regret"] for i in infos) / max(1, sum(i["audited"] for i in infos))),
+                       "definition": "audited nodes whose drawn candidate scores below the exact k-th best "
+                                     "(plain FP32 path, teacher-forced on the final grid); near_tie: below it by at "
+                                     "most 1e-5 of the term scale"} if tensor else
+                      {"regret": 0, "definition": "exact reference path: regret 0 by construction"},
+            "map_error_vs_fp64": {"max": max(i["map_err_max"] for i in infos),
+                                  "mean": float(np.mean([i["map_err_mean"] for i in infos])),
+                                  "unit": "|score - FP64 score| / term scale over the re-scored shortlists"}
+            if tensor else None,
             "roofline": roofline,
+            "own_peaks": own_peaks,
             "breakdown_ms": {"neighbours": pinf["ms_setup_neighbours"], "levels": pinf["ms_levels"],
-                             "prep": pinf["ms_prep"], "map": pinf["ms_map"], "replay": pinf["ms_replay"],
+                             "prep": pinf["ms_prep"], "exact_map": pinf["ms_map"], "replay": pinf["ms_replay"],
+                             "tensor_gemm": pinf["ms_tensor_gemm"], "tensor_select": pinf["ms_tensor_select"],
                              "total": pinf["ms_total"]},
             "cpu_baseline": cpu,
             "e2e": e2e,

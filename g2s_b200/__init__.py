@@ -69,7 +69,7 @@ class QskSimInfo(ctypes.Structure):
                 ("regret_near", ctypes.c_longlong), ("map_err_max", ctypes.c_float), ("map_err_mean", ctypes.c_float),
                 ("tensor_flops", ctypes.c_double), ("ms_tensor_gemm", ctypes.c_float),
                 ("ms_tensor_select", ctypes.c_float), ("ms_tensor_pattern", ctypes.c_float),
-                ("tensor_launches", ctypes.c_longlong)]
+                ("tensor_launches", ctypes.c_longlong), ("path_nodes", ctypes.c_longlong)]
 
 
 class QskTensorOpts(ctypes.Structure):
@@ -107,6 +107,7 @@ SIGNATURES = {
     "qsk_tc_topk": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.c_int,
                                    ctypes.c_void_p, ctypes.c_void_p, _f32p, _f32p, _f32p, _u32p, _i32p, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _u32p]),
+    "qsk_measure_peaks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_position_to_index": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,
@@ -447,7 +448,7 @@ class Simulation:
         cells = int(np.prod(self._ddims))
         out = np.empty_like(self._di)
         idx = np.zeros(cells * (self.nvar if self.full else 1), np.uint32)
-        nodes = self.info()["nodes"]
+        nodes = self.info()["path_nodes"]
         nc = np.zeros(max(nodes, 1), np.uint32)
         _check(lib().qsk_sim_read(self.handle, _p(out, _f32p), _p(idx, _u32p), _p(nc, _u32p)), "qsk_sim_read")
         shape = self._di.shape if self.full else self._di.shape[:len(self._ddims)]
@@ -463,6 +464,13 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+def measure_peaks(device: int = 0) -> dict:
+    """The library's own peak microbenchmarks (qsk_measure_peaks)."""
+    out = (ctypes.c_double * 4)()
+    _check(lib().qsk_measure_peaks(device, out), "qsk_measure_peaks")
+    return {"fp32_tflops": out[0], "int32_lop3_tops": out[1], "bf16_tflops": out[2], "fp8_tflops": out[3]}
 
 
 def tc_topk(queries: np.ndarray, rows: np.ndarray, fmt: int, X: int, Y: int, box: np.ndarray, W: int = 8,
@@ -491,11 +499,14 @@ def tc_topk(queries: np.ndarray, rows: np.ndarray, fmt: int, X: int, Y: int, box
 
 def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
        ki=None, nV: bool = False, ni: Optional[np.ndarray] = None, kvi: Optional[np.ndarray] = None,
-       kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0):
+       kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0, tensor: Optional[str] = None,
+       audit: float = 0.01):
     """QuickSampling on one GPU; arguments named after the G2S flags
     (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii -fs).  ``n`` is one count or one
     per variable; ``ki`` one kernel or a list of kernels (selected per cell by
-    ``kii``).  Returns (simulation, index) as G2S does."""
+    ``kii``).  ``tensor`` selects the tensor-core form of the map ("bf16" or
+    "fp8", with the regret audit fraction ``audit``); None is the exact
+    reference path.  Returns (simulation, index) as G2S does."""
     n_list = None
     if np.ndim(n) > 0:
         n_list = [int(x) for x in np.ravel(n)]
@@ -506,6 +517,8 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     sim = Simulation(ti, di, dt, n=n if n is not None else 0, k=k, seed=s, kernel=kernel, device=device,
                      no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii, full=fs)
     try:
+        if tensor:
+            sim.set_tensor(tensor, audit=audit)
         sim.run()
         out, idx, _ = sim.read()
     finally:

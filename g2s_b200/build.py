@@ -20,7 +20,7 @@ LIB = os.path.join(PKG, "libg2s_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["qsk_kernels.cu", "qsk_tc.cu", "qsk_host.cpp", "qsk_tensor.cpp", "qsk_bgrid.cpp"]
+SOURCES = ["qsk_kernels.cu", "qsk_tc.cu", "qsk_peaks.cu", "qsk_host.cpp", "qsk_tensor.cpp", "qsk_bgrid.cpp"]
 
 
 def _run(cmd):

@@ -1156,13 +1156,13 @@ int tc_configure(qsk_sim *s, int T_auto) {
     const long long rows = rup(g.N, 256);
     int T = s->topt.prefix > 0 ? s->topt.prefix : T_auto;
     T = std::max(1, std::min(T, s->ntpl));
-    // cap the pattern matrix at 16 GiB
-    while (T > 64 && (double)rows * rup((long long)T * L, 128 / elem) * elem > 16.0 * (1ull << 30)) T /= 2;
+    // cap the pattern matrix at 48 GiB (a quarter of the B200's HBM)
+    while (T > 64 && (double)rows * rup((long long)T * L, 128 / elem) * elem > 48.0 * (1ull << 30)) T = T / 2 / 64 * 64;
     const long long Kp = rup((long long)T * L, 128 / elem);
     const int W = s->topt.width > 0 ? s->topt.width : (fmt == 1 ? 32 : 8);
-    int S = s->topt.shortlist > 0 ? s->topt.shortlist : (fmt == 1 ? 64 : 4 * s->K);
+    int S = s->topt.shortlist > 0 ? s->topt.shortlist : (fmt == 1 ? 128 : 4 * s->K);
     if (!tc_supported_width(W)) return fail(QSK_ERR_ARG, "tensor-core width %d (8, 16 or 32)", W);
-    if (S > 64) return fail(QSK_ERR_ARG, "tensor-core shortlist %d (at most 64)", S);
+    if (S > 128) return fail(QSK_ERR_ARG, "tensor-core shortlist %d (at most 128)", S);
     if (S < s->K) S = s->K;
     const bool same = s->tc_ready && s->tc_T == T && s->tc_fmt == fmt && s->tc_L == L;
     s->tc_T = T;
@@ -1954,6 +1954,7 @@ int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cel
 int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info) {
     if (!s || !info) return fail(QSK_ERR_ARG, "null argument");
     *info = s->info;
+    info->path_nodes = s->nodes;
     return QSK_OK;
 }
 
@@ -1976,7 +1977,7 @@ int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
     if (o->mode < 0 || o->mode > 2) return fail(QSK_ERR_ARG, "tensor mode %d (0 plain, 1 BF16, 2 FP8)", o->mode);
     if (!(o->audit >= 0.f && o->audit <= 1.f)) return fail(QSK_ERR_ARG, "audit fraction %g", double(o->audit));
     if (o->width != 0 && !tc_supported_width(o->width)) return fail(QSK_ERR_ARG, "width %d (8, 16 or 32)", o->width);
-    if (o->shortlist < 0 || o->shortlist > 64) return fail(QSK_ERR_ARG, "shortlist %d (at most 64)", o->shortlist);
+    if (o->shortlist < 0 || o->shortlist > 128) return fail(QSK_ERR_ARG, "shortlist %d (at most 128)", o->shortlist);
     if (o->prefix < 0) return fail(QSK_ERR_ARG, "prefix %d", o->prefix);
     if (o->mode != 0) {
         if (s->ti->missing) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: training image with missing values");

@@ -369,7 +369,7 @@ struct TcSelectArgs {
     const unsigned long long *cand_key;  // [slot][ncand]
     const unsigned *cand_pos;
     int ncand;                           // ranges x W
-    int S;                               // candidates scored exactly (<= 64)
+    int S;                               // candidates scored exactly (<= 128)
     int fp64;                            // rank by the FP64 exact score
     const float *ti;
     int nvar;

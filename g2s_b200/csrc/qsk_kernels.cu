@@ -1945,44 +1945,45 @@ __device__ __forceinline__ unsigned hs_ordered(float f) {
 }
 }  // namespace
 
-constexpr int HS_THREADS = 128;
+constexpr int HS_THREADS = 256;
+template <int KM>
 __global__ void __launch_bounds__(HS_THREADS) k_hash_select(ReplayArgs A) {
-    __shared__ unsigned long long sk[HS_THREADS * QSK_KMAX];
-    __shared__ unsigned sp[HS_THREADS * QSK_KMAX];
+    __shared__ unsigned long long sk[HS_THREADS * KM];
+    __shared__ unsigned sp[HS_THREADS * KM];
     const int b = blockIdx.x;
     if (b >= A.nslots) return;
     const Slot s = A.slots[b];
     if (s.flags & (SLOT_SKIP | SLOT_EMIT_MASKED)) return;
     const Geom &g = A.g;
-    const int K = s.K;
+    const int K = s.K < KM ? s.K : KM;
     const unsigned seed = __float_as_uint(s.seed) ^ (unsigned(s.node) * 0x85EBCA6Bu);
-    unsigned long long rk[QSK_KMAX];
-    unsigned rp[QSK_KMAX];
+    unsigned long long rk[KM];
+    unsigned rp[KM];
 #pragma unroll
-    for (int i = 0; i < QSK_KMAX; ++i) {
+    for (int i = 0; i < KM; ++i) {
         rk[i] = 0ull;
         rp[i] = 0u;
     }
-    // the thread's K best in rk[QSK_KMAX-K .. QSK_KMAX-1] (ascending array of
-    // QSK_KMAX; its minimum rk[0] bounds what may enter)
+    // the thread's K best in rk[KM-K .. KM-1] (ascending array of
+    // KM; its minimum rk[0] bounds what may enter)
     const long long base = (long long)b * g.nseg;
     for (int sg = threadIdx.x; sg < g.nseg; sg += HS_THREADS) {
         const int cnt = A.rec_cnt[base + sg];
         if (cnt == 0) continue;
-        if (hs_ordered(A.rec_max[base + sg]) < (unsigned)(rk[QSK_KMAX - K] >> 32)) continue;
+        if (hs_ordered(A.rec_max[base + sg]) < (unsigned)(rk[KM - K] >> 32)) continue;
         const float *rv = A.rec_val + (base + sg) * QSK_SEG;
         const int *ri = A.rec_idx + (base + sg) * QSK_SEG;
         for (int i = 0; i < cnt; ++i) {
             const unsigned idx = (unsigned)ri[i];
             const unsigned long long key = ((unsigned long long)hs_ordered(rv[i]) << 32) | tie_hash(seed, idx);
-            if (key > rk[QSK_KMAX - K]) {
-                // keep the array's top K: entries below QSK_KMAX-K stay at 0
-                hs_insert<QSK_KMAX>(rk, rp, key, idx);
+            if (key > rk[KM - K]) {
+                // keep the array's top K: entries below KM-K stay at 0
+                hs_insert<KM>(rk, rp, key, idx);
             }
         }
     }
 #pragma unroll
-    for (int i = 0; i < QSK_KMAX; ++i) {
+    for (int i = 0; i < KM; ++i) {
         sk[i * HS_THREADS + threadIdx.x] = rk[i];
         sp[i * HS_THREADS + threadIdx.x] = rp[i];
     }
@@ -1991,13 +1992,13 @@ __global__ void __launch_bounds__(HS_THREADS) k_hash_select(ReplayArgs A) {
     const int lane = threadIdx.x;
     // K rounds of warp argmax over the block's entries, descending
     unsigned chosen = 0xFFFFFFFFu;
-    float cval[QSK_KMAX];
-    unsigned cpos[QSK_KMAX];
+    float cval[KM];
+    unsigned cpos[KM];
     int got = 0;
     for (int r = 0; r < K; ++r) {
         unsigned long long bk = 0ull;
         int bi = -1;
-        for (int e = lane; e < HS_THREADS * QSK_KMAX; e += 32) {
+        for (int e = lane; e < HS_THREADS * KM; e += 32) {
             const unsigned long long k2 = sk[e];
             if (k2 > bk) {
                 bk = k2;
@@ -2874,7 +2875,10 @@ static void launch_replay_team(const ReplayArgs &a, size_t smem, cudaStream_t st
 
 cudaError_t launch_hash_select(const ReplayArgs &a, cudaStream_t st) {
     if (a.nslots <= 0) return cudaSuccess;
-    k_hash_select<<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
+    if (a.K <= 2) k_hash_select<2><<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
+    else if (a.K <= 4) k_hash_select<4><<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
+    else if (a.K <= 8) k_hash_select<8><<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
+    else k_hash_select<16><<<(unsigned)a.nslots, HS_THREADS, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -828,6 +828,7 @@ __device__ __forceinline__ void exact_score(const Term *__restrict__ tm, int nt,
 
 constexpr int SEL_WARPS = 4;
 constexpr int SEL_CAND = 768;    // candidates per slot staged in shared memory
+constexpr int SEL_CPL = 4;       // shortlist entries per lane: at most 128 re-scored
 
 // one warp per tensor slot: the S best candidates by approximate key, their
 // exact scores, the node's k best by exact score (ties by the key's hash),
@@ -854,8 +855,13 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     __syncwarp();
     const Term *tt = small ? sterm[w] : tm;
     // the S largest keys (S rounds of warp argmax); lane r keeps round r and r+32
-    unsigned long long mykey[2] = {0ull, 0ull};
-    unsigned mypos[2] = {0u, 0u};
+    unsigned long long mykey[SEL_CPL];
+    unsigned mypos[SEL_CPL];
+#pragma unroll
+    for (int h = 0; h < SEL_CPL; ++h) {
+        mykey[h] = 0ull;
+        mypos[h] = 0u;
+    }
     int nsel = 0;
     for (int r = 0; r < A.S; ++r) {
         unsigned long long bk = 0ull;
@@ -878,8 +884,12 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         }
         if (bk == 0ull) break;
         if (lane == (r & 31)) {
-            mykey[r >> 5] = bk;
-            mypos[r >> 5] = spos[w][bi];
+#pragma unroll
+            for (int h = 0; h < SEL_CPL; ++h)
+                if (h == (r >> 5)) {
+                    mykey[h] = bk;
+                    mypos[h] = spos[w][bi];
+                }
         }
         __syncwarp();
         if (lane == 0) skey[w][bi] = 0ull;
@@ -889,15 +899,23 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     // exact scores of the shortlist: the scan index of every candidate, then
     // all (candidate, term) layer values gathered by the whole warp at once
     // into shared memory, then each candidate's term chain from there
-    float e32[2] = {-INFINITY, -INFINITY};
-    double e64[2] = {-INFINITY, -INFINITY}, esc[2] = {0.0, 0.0};
-    unsigned hsh[2] = {0u, 0u};
-    bool live[2] = {false, false};
+    float e32[SEL_CPL];
+    double e64[SEL_CPL], esc[SEL_CPL];
+    unsigned hsh[SEL_CPL];
+    bool live[SEL_CPL];
+#pragma unroll
+    for (int h = 0; h < SEL_CPL; ++h) {
+        e32[h] = -INFINITY;
+        e64[h] = -INFINITY;
+        esc[h] = 0.0;
+        hsh[h] = 0u;
+        live[h] = false;
+    }
     float errmax = 0.f;
     double errsum = 0.0;
     int errn = 0;
     int *msc = reinterpret_cast<int *>(&spos[w][0]);   // candidate list no longer needed
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < SEL_CPL; ++h) {
         const int r = h * 32 + lane;
         if (r >= nsel) continue;
         // natural cell -> scan index of the reference's flipped space (cvtPositionToIndex)
@@ -921,19 +939,19 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
                 for (int t = lane; t < nt; t += 32) xs[(r - r0) * nt + t] = __ldg(A.layers + tt[t].base + m);
             }
             __syncwarp();
-            for (int h = 0; h < 2; ++h) {
+            for (int h = 0; h < SEL_CPL; ++h) {
                 const int r = h * 32 + lane;
                 if (r >= r0 && r < r1) exact_score_staged(tt, nt, xs + (r - r0) * nt, e32[h], e64[h], esc[h]);
             }
             __syncwarp();
         }
     } else {
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < SEL_CPL; ++h) {
             const int r = h * 32 + lane;
             if (r < nsel) exact_score(tt, nt, A.layers, (long long)msc[r], e32[h], e64[h], esc[h]);
         }
     }
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < SEL_CPL; ++h) {
         const int r = h * 32 + lane;
         if (r >= nsel) continue;
         const float approx = tc::unordered((unsigned)(mykey[h] >> 32));
@@ -954,7 +972,7 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     const bool f64 = A.fp64 != 0;
     for (int k = 0; k < K && k < nsel; ++k) {
         int bh = -1;
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < SEL_CPL; ++h) {
             if (!live[h]) continue;
             if (bh < 0) {
                 bh = h;
@@ -980,10 +998,20 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         }
         if (bl < 0) break;
         const int wh = __shfl_sync(0xffffffffu, bh, bl);
-        const unsigned wp = __shfl_sync(0xffffffffu, wh == 0 ? mypos[0] : mypos[1], bl);
-        const float w32 = __shfl_sync(0xffffffffu, wh == 0 ? e32[0] : e32[1], bl);
-        const double wsc = __shfl_sync(0xffffffffu, wh == 0 ? esc[0] : esc[1], bl);
-        if (lane == bl) live[wh] = false;
+        unsigned wp0 = 0u;
+        float w320 = 0.f;
+        double wsc0 = 0.0;
+#pragma unroll
+        for (int h = 0; h < SEL_CPL; ++h)
+            if (h == wh) {
+                wp0 = mypos[h];
+                w320 = e32[h];
+                wsc0 = esc[h];
+                if (lane == bl) live[h] = false;
+            }
+        const unsigned wp = __shfl_sync(0xffffffffu, wp0, bl);
+        const float w32 = __shfl_sync(0xffffffffu, w320, bl);
+        const double wsc = __shfl_sync(0xffffffffu, wsc0, bl);
         // rank sel, or the last one found when fewer than sel + 1 exist
         chosen = wp;
         chosen32 = w32;
@@ -1063,7 +1091,7 @@ cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st) {
 }
 
 cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st) {
-    if (a.ncand > SEL_CAND || a.S > 64) return cudaErrorInvalidValue;
+    if (a.ncand > SEL_CAND || a.S > 32 * SEL_CPL) return cudaErrorInvalidValue;
     k_tc_select<<<(unsigned)((a.nslots + SEL_WARPS - 1) / SEL_WARPS), 32 * SEL_WARPS, 0, st>>>(a);
     return cudaGetLastError();
 }

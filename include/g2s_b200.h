@@ -263,6 +263,12 @@ int qsk_tc_topk(int device, int fmt, int B, long long N, int K, const void *quer
                 const float *q_scale, const float *q_bias, const float *p_scale, const unsigned *q_seed,
                 const int *q_box, int X, int Y, int W, int ranges, unsigned long long *out_key, unsigned *out_pos);
 
+/* Peak rates of this GPU measured by the library's own microbenchmarks (no
+ * G2S counterpart): out[0] FP32 FMA TFLOP/s, out[1] 32-bit LOP3 Tops/s,
+ * out[2] tcgen05 BF16 dense TFLOP/s, out[3] tcgen05 FP8 E4M3 dense TFLOP/s.
+ * The roofline denominators of kernels with no driver-measured peak. */
+int qsk_measure_peaks(int device, double *out);
+
 /* Reference scan index -> TI cell (CPUThreadDevice::cvtIndexToPosition,
  * G2S src/CPUThreadDevice.cpp:257-268). */
 unsigned qsk_index_to_position(const qsk_ti *ti, const int *min_offset, unsigned index);
@@ -338,6 +344,7 @@ typedef struct {
     float ms_tensor_select;       /* ... of node rows, re-score and draw (profiling mode only) */
     float ms_tensor_pattern;      /* device time of building the pattern matrix (once per simulation) */
     long long tensor_launches;
+    long long path_nodes;         /* path nodes of the simulation (nodes: those of the last run) */
 } qsk_sim_info;
 
 typedef struct qsk_sim qsk_sim;
@@ -361,7 +368,8 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
  * choices at their path indices. */
 int qsk_sim_run_teacher_nodes(qsk_sim *s, const float *di_completed, const int *path_nodes, int count);
 /* Copy results to the host: the grid, the index image (TI cell * nTI + TI,
- * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL). */
+ * src/qs.cpp:2277), and the chosen TI cell per path node (any may be NULL;
+ * node_cell_out holds qsk_sim_info.path_nodes entries). */
 int qsk_sim_read(qsk_sim *s, float *di_out, unsigned *id_out, unsigned *node_cell_out);
 int qsk_sim_get_info(const qsk_sim *s, qsk_sim_info *info);
 /* Profiling mode: record CUDA events around every kernel of the next runs so
@@ -402,13 +410,13 @@ int qsk_sim_destroy(qsk_sim *s);
  * Complete TIs only, without -nV, -fs or local controls.  Zero fields take
  * the automatic choice: prefix = the smallest multiple of 256 offsets that
  * covers 97 % of the path's nodes (chosen at the first tensor run from the
- * nodes' neighbour lists), capped by a 16 GiB pattern matrix; width 8 (FP8:
- * 32), shortlist 4 x extendK (FP8: 64). */
+ * nodes' neighbour lists), capped by a 48 GiB pattern matrix; width 8 (FP8:
+ * 32), shortlist 4 x extendK (FP8: 128). */
 typedef struct {
     int mode;          /* 0 plain (the exact reference path), 1 BF16, 2 FP8 E4M3 */
     int prefix;        /* template offsets in the pattern matrix */
     int width;         /* 8, 16 or 32 */
-    int shortlist;     /* <= 64 */
+    int shortlist;     /* <= 128 */
     float audit;       /* fraction of tensor-path nodes audited, 0..1 */
 } qsk_tensor_opts;
 int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *opts);

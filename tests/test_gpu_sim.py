@@ -77,6 +77,22 @@ def test_config0_teacher_forced_vs_reference(g2s, gpu):
     assert mismatch.sum() <= fx["near_tie"].sum() < 400
 
 
+def test_teacher_forced_node_sample_equals_full_teacher_run(g2s, gpu):
+    """qsk_sim_run_teacher_nodes on a seeded sample of path nodes draws
+    exactly what the full teacher-forced run draws at those path indices."""
+    g = golden("config0")
+    sim = g2s.Simulation(g["ti"], g["di"], [0], n=50, k=1.2, seed=100)
+    sim.run_teacher(g["sim"])
+    _, _, full = sim.read()
+    sample = np.sort(np.random.default_rng(5).choice(40000, 3000, replace=False)).astype(np.int32)
+    sim.run_teacher_nodes(g["sim"], sample)
+    info = sim.info()
+    _, _, part = sim.read()
+    sim.close()
+    assert info["nodes"] == 3000 and info["path_nodes"] == 40000 and part.size == 40000
+    assert np.array_equal(part[sample], full[sample])
+
+
 def test_config0_full_simulation_properties(g2s, gpu):
     g = golden("config0")
     (sim, idx, cells), info = run_gpu(g2s, g)
