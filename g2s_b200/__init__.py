@@ -69,7 +69,13 @@ class QskSimInfo(ctypes.Structure):
                 ("regret_near", ctypes.c_longlong), ("map_err_max", ctypes.c_float), ("map_err_mean", ctypes.c_float),
                 ("tensor_flops", ctypes.c_double), ("ms_tensor_gemm", ctypes.c_float),
                 ("ms_tensor_select", ctypes.c_float), ("ms_tensor_pattern", ctypes.c_float),
-                ("tensor_launches", ctypes.c_longlong), ("path_nodes", ctypes.c_longlong)]
+                ("tensor_launches", ctypes.c_longlong), ("path_nodes", ctypes.c_longlong),
+                ("learned_fallback", ctypes.c_longlong)]
+
+
+class QskLearnedOpts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int), ("shortlist", ctypes.c_int), ("conf_rank", ctypes.c_int),
+                ("audit", ctypes.c_float), ("conf_z", ctypes.c_float), ("conf_r2", ctypes.c_float)]
 
 
 class QskTensorOpts(ctypes.Structure):
@@ -108,6 +114,22 @@ SIGNATURES = {
                                    ctypes.c_void_p, ctypes.c_void_p, _f32p, _f32p, _f32p, _u32p, _i32p, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong), _u32p]),
     "qsk_measure_peaks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "qsk_encoder_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_void_p)]),
+    "qsk_encoder_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_encoder_param_count": (ctypes.c_longlong, [ctypes.c_void_p]),
+    "qsk_encoder_input_dim": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_encoder_get_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    "qsk_encoder_set_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
+    "qsk_encoder_loss_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, ctypes.c_float, _f32p, _f32p]),
+    "qsk_encoder_embed": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, _f32p, _f32p]),
+    "qsk_encoder_add_pairs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, _f32p, _i32p, ctypes.c_int,
+                                             ctypes.POINTER(ctypes.c_longlong)]),
+    "qsk_encoder_add_pairs_host": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, _f32p, _f32p]),
+    "qsk_encoder_pairs": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "qsk_encoder_clear_pairs": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_encoder_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_uint, _f32p]),
+    "qsk_sim_set_learned": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(QskLearnedOpts)]),
     "qsk_index_to_position": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_position_to_index": (ctypes.c_uint, [ctypes.c_void_p, _i32p, ctypes.c_uint]),
     "qsk_sim_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p,
@@ -409,6 +431,16 @@ class Simulation:
         _check(lib().qsk_sim_set_tensor(self.handle, ctypes.byref(o)), "qsk_sim_set_tensor")
         return self
 
+    def set_learned(self, encoder: Optional["Encoder"], width: int = 0, shortlist: int = 0, conf_rank: int = 0,
+                    audit: float = 0.0, conf_z: float = 2.0, conf_r2: float = 0.2):
+        """The learned proposal as the map (qsk_sim_set_learned); None: off.
+        conf_z > 0: the statistical confidence check, else the rank check."""
+        o = QskLearnedOpts(int(width), int(shortlist), int(conf_rank), float(audit), float(conf_z), float(conf_r2))
+        _check(lib().qsk_sim_set_learned(self.handle, encoder.handle if encoder else None, ctypes.byref(o)),
+               "qsk_sim_set_learned")
+        self._encoder = encoder
+        return self
+
     def set_level_wait(self, spin_limit: int = 0, hold_node: int = -1):
         """Bound of the dependency-level waits (polls; 0 = default) and, for
         failure-path tests, a path node whose level is never published."""
@@ -457,6 +489,88 @@ class Simulation:
     def close(self):
         if getattr(self, "handle", None):
             lib().qsk_sim_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Encoder:
+    """The learned proposal's neighbourhood encoder (qsk_encoder_*)."""
+
+    def __init__(self, nvar: int, seed: int = 0, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(lib().qsk_encoder_create(device, int(nvar), int(seed) & 0xffffffff, ctypes.byref(h)),
+               "qsk_encoder_create")
+        self.handle = h
+        self.nvar = nvar
+        self.input_dim = lib().qsk_encoder_input_dim(h)
+        self.param_count = lib().qsk_encoder_param_count(h)
+
+    def weights(self) -> np.ndarray:
+        w = np.zeros(self.param_count, np.float32)
+        _check(lib().qsk_encoder_get_weights(self.handle, _p(w, _f32p)), "qsk_encoder_get_weights")
+        return w
+
+    def set_weights(self, w: np.ndarray):
+        a = np.ascontiguousarray(w, dtype=np.float32)
+        assert a.size == self.param_count
+        _check(lib().qsk_encoder_set_weights(self.handle, _p(a, _f32p)), "qsk_encoder_set_weights")
+
+    def loss_grad(self, xq: np.ndarray, xp: np.ndarray, tau: float = 0.05, grad: bool = True):
+        q = np.ascontiguousarray(xq, dtype=np.float32)
+        p = np.ascontiguousarray(xp, dtype=np.float32)
+        B = q.shape[0]
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(self.param_count, np.float32) if grad else None
+        _check(lib().qsk_encoder_loss_grad(self.handle, B, _p(q, _f32p), _p(p, _f32p), float(tau), _p(loss, _f32p),
+                                           _p(g, _f32p)), "qsk_encoder_loss_grad")
+        return float(loss[0]), g
+
+    def embed(self, x: np.ndarray, head: str = "query") -> np.ndarray:
+        """Embeddings by the query head ("query") or the TI-pattern head ("pattern")."""
+        a = np.ascontiguousarray(x, dtype=np.float32)
+        out = np.zeros((a.shape[0], 64), np.float32)
+        _check(lib().qsk_encoder_embed(self.handle, {"query": 0, "pattern": 1}[head], a.shape[0], _p(a, _f32p),
+                                       _p(out, _f32p)), "qsk_encoder_embed")
+        return out
+
+    def add_pairs(self, sim: "Simulation", completed: np.ndarray, path_nodes) -> int:
+        c = np.ascontiguousarray(completed, dtype=np.float32)
+        nodes = np.ascontiguousarray(path_nodes, dtype=np.int32)
+        added = ctypes.c_longlong(0)
+        _check(lib().qsk_encoder_add_pairs(self.handle, sim.handle, _p(c, _f32p), _p(nodes, _i32p), int(nodes.size),
+                                           ctypes.byref(added)), "qsk_encoder_add_pairs")
+        return added.value
+
+    def add_pairs_host(self, xq: np.ndarray, xp: np.ndarray) -> int:
+        q = np.ascontiguousarray(xq, dtype=np.float32)
+        p = np.ascontiguousarray(xp, dtype=np.float32)
+        assert q.shape == p.shape and q.shape[1] == self.input_dim
+        _check(lib().qsk_encoder_add_pairs_host(self.handle, q.shape[0], _p(q, _f32p), _p(p, _f32p)),
+               "qsk_encoder_add_pairs_host")
+        return q.shape[0]
+
+    def pairs(self) -> int:
+        n = ctypes.c_longlong(0)
+        _check(lib().qsk_encoder_pairs(self.handle, ctypes.byref(n)), "qsk_encoder_pairs")
+        return n.value
+
+    def clear_pairs(self):
+        _check(lib().qsk_encoder_clear_pairs(self.handle), "qsk_encoder_clear_pairs")
+
+    def train(self, epochs: int = 1, batch: int = 1024, lr: float = 1e-3, tau: float = 0.05, seed: int = 0) -> float:
+        loss = np.zeros(1, np.float32)
+        _check(lib().qsk_encoder_train(self.handle, int(epochs), int(batch), float(lr), float(tau),
+                                       int(seed) & 0xffffffff, _p(loss, _f32p)), "qsk_encoder_train")
+        return float(loss[0])
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().qsk_encoder_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -20,7 +20,8 @@ LIB = os.path.join(PKG, "libg2s_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 HOSTCXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["qsk_kernels.cu", "qsk_tc.cu", "qsk_peaks.cu", "qsk_host.cpp", "qsk_tensor.cpp", "qsk_bgrid.cpp"]
+SOURCES = ["qsk_kernels.cu", "qsk_tc.cu", "qsk_peaks.cu", "qsk_learn.cu", "qsk_host.cpp", "qsk_tensor.cpp",
+           "qsk_encoder.cpp", "qsk_bgrid.cpp"]
 
 
 def _run(cmd):
@@ -38,6 +39,7 @@ def _stale(target, deps):
 def build_lib(force: bool = False) -> str:
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "qsk_internal.h"),
                                                        os.path.join(CSRC, "qsk_host_util.h"),
+                                                       os.path.join(CSRC, "qsk_encoder.h"),
                                                        os.path.join(ROOT, "include", "g2s_b200.h")]
     if not force and not _stale(LIB, deps):
         return LIB

@@ -1,0 +1,38 @@
+// The learned proposal's encoder object, shared by the encoder host code
+// (qsk_encoder.cpp) and the simulation engine (qsk_host.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "qsk_host_util.h"
+#include "qsk_internal.h"
+
+namespace qsk {
+constexpr int ENC_H = 256;   // hidden width
+constexpr int ENC_E = 64;    // embedding width
+constexpr int ENC_NP = 10;   // parameter blocks: trunk (3 layers), query head, TI-pattern head
+}  // namespace qsk
+
+struct qsk_encoder {
+    int device = 0;
+    int nvar = 1, F = 5, D0 = 320;
+    long long off[qsk::ENC_NP + 1] = {};
+    long long nparam = 0;
+    cudaStream_t st = nullptr;
+    qsk::DBuf<float> w, g, m, v;   // parameters, gradients, Adam moments
+    int t = 0;                     // Adam steps taken
+    // activations of the last forward pass (rows <= cap)
+    long long cap = 0;
+    qsk::DBuf<float> h1p, h1, h2p, h2, h3p, h3, z, y, nrm, d1, d2, dz;
+    qsk::DBuf<float> xb;           // input rows of a batch / an embedding chunk
+    qsk::DBuf<float> S, dS, loss;  // batch similarities and their gradient
+    // training pairs (device): query and positive feature rows
+    long long npairs = 0, pair_cap = 0;
+    qsk::DBuf<float> xq, xp;
+};
+
+namespace qsk {
+// rows x D0 inputs -> embeddings in e->y (rows x 64), rows [0, nq) by the
+// query head and the rest by the TI-pattern head, on stream st
+int enc_forward(qsk_encoder *e, long long rows, long long nq, const float *x, cudaStream_t st);
+}  // namespace qsk

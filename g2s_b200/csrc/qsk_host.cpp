@@ -23,6 +23,7 @@
 #include "../../include/g2s_b200.h"
 #include "qsk_internal.h"
 #include "qsk_host_util.h"
+#include "qsk_encoder.h"
 
 using namespace qsk;
 
@@ -731,6 +732,13 @@ struct qsk_sim {
     DBuf<double> d_err_sum;
     DBuf<unsigned long long> d_err_n;
     int max_tc_slots = 0;
+    // learned proposal (qsk_sim_set_learned): tensor mode 3
+    qsk_encoder *enc = nullptr;
+    qsk_learned_opts lopt{};
+    int enc_built = -1;                 // encoder Adam step count the TI embeddings were built at
+    DBuf<float> d_feat;                 // encoder input rows of a step / a chunk of TI cells
+    DBuf<int> d_fb;                     // per slot: confidence check failed
+    DBuf<int> d_fb_nodes;
     std::vector<cudaEvent_t> tc_ev;     // profiling: 3 events per tensor step
     size_t tc_ev_used = 0;
     unsigned level_spin_limit = 0;      // 0: the kernel's default
@@ -1133,7 +1141,64 @@ cudaEvent_t tc_event(qsk_sim *s) {
 long long rup(long long x, long long m) { return (x + m - 1) / m * m; }
 
 // pattern matrix of the template prefix (built once per simulation and mode)
+// learned proposal: the pattern matrix is the TI cells' embeddings (BF16,
+// 64 columns), built once per encoder state
+int tc_configure_learned(qsk_sim *s) {
+    const Geom &g = s->ti->g;
+    qsk_encoder *e = s->enc;
+    const long long rows = rup(g.N, 256);
+    s->tc_T = 0;
+    s->tc_L = 1;
+    s->tc_W = s->lopt.width > 0 ? s->lopt.width : 32;
+    s->tc_S = s->lopt.shortlist > 0 ? s->lopt.shortlist : 256;
+    if (s->tc_S < s->K) s->tc_S = s->K;
+    s->tc_fmt = 0;
+    s->tc_Kp = ENC_E;
+    s->tc_rows = rows;
+    if (s->tc_ready && s->enc_built == e->t) return QSK_OK;
+    s->tc_ready = false;
+    CK(s->d_tc_P.alloc(size_t(rows) * ENC_E * 2));
+    CK(cudaMemsetAsync(s->d_tc_P.p, 0, size_t(rows) * ENC_E * 2, s->st));
+    const long long chunk = 131072;
+    CK(s->d_feat.ensure(size_t(chunk) * size_t(e->D0)));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s->st));
+    for (long long c0 = 0; c0 < s->ti->cells; c0 += chunk) {
+        const long long n = std::min(chunk, s->ti->cells - c0);
+        FeatArgs fa;
+        fa.rows = n;
+        fa.cell0 = c0;
+        fa.cells = s->ti->cells;
+        fa.ti = s->ti->grid.p;
+        for (int d = 0; d < 3; ++d) fa.src[d] = d < g.nd ? g.src[d] : 1;
+        fa.ntpl = s->ntpl;
+        fa.tpl = s->d_tpl.p;
+        fa.nd = g.nd;
+        fa.nvar = s->nvar;
+        fa.inv_radius = 0.125f;
+        fa.entries = QSK_ENC_ENTRIES;
+        fa.out = s->d_feat.p;
+        CK(launch_feat_cells(fa, s->st));
+        int rc = enc_forward(e, n, 0, s->d_feat.p, s->st);   // TI-pattern head
+        if (rc) return rc;
+        CK(launch_to_bf16(n * ENC_E, e->y.p, reinterpret_cast<uint16_t *>(s->d_tc_P.p) + size_t(c0) * ENC_E, s->st));
+    }
+    CK(cudaEventRecord(e1, s->st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->info.ms_tensor_pattern = ms;
+    s->enc_built = e->t;
+    s->tc_ready = true;
+    return QSK_OK;
+}
+
 int tc_configure(qsk_sim *s, int T_auto) {
+    if (s->topt.mode == 3) return tc_configure_learned(s);
     const Geom &g = s->ti->g;
     const int fmt = s->topt.mode == 2 ? 1 : 0;
     const int elem = fmt == 0 ? 2 : 1;
@@ -1264,9 +1329,10 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
     for (size_t l = 0; l + 1 < start.size(); ++l) {
         el.clear();
         pl.clear();
+        const bool learned = s->topt.mode == 3;
         for (int q = start[l]; q < start[l + 1]; ++q) {
             const int i = order[size_t(q)];
-            (tmax[size_t(i)] >= 0 && tmax[size_t(i)] < T ? el : pl).push_back(i);
+            (tmax[size_t(i)] >= 0 && (learned || tmax[size_t(i)] < T) ? el : pl).push_back(i);
         }
         std::stable_sort(el.begin(), el.end(), [&](int a, int b) { return tmax[size_t(a)] < tmax[size_t(b)]; });
         int q = start[l];
@@ -1277,7 +1343,7 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
             Step st{STEP_TENSOR, s->d_level_nodes.p, start[l] + off, B, int(kb.size())};
             for (int t0 = 0; t0 < B; t0 += 128) {
                 const int last = el[size_t(off + std::min(B, t0 + 128) - 1)];
-                const int k = int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
+                const int k = learned ? 1 : int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
                 kb.push_back(k);
                 flops += 2.0 * 128 * 256 * double(ntiles_pos) * double(k) * kbe;
             }
@@ -1304,6 +1370,88 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
     s->info.tensor_nodes = ntc;
     s->info.plain_nodes = npl;
     s->info.tensor_flops = flops;
+    return QSK_OK;
+}
+
+// the exact map over the whole TI (FP32 gather) with the tensor-core form's
+// draw rule, for a device list of path nodes (the learned proposal's
+// fallback); records must hold max_slots slots
+int exact_nodes(qsk_sim *s, const int *nodes, int count, bool teacher) {
+    const Geom &g = s->ti->g;
+    for (int off = 0; off < count; off += s->max_slots) {
+        const int B = std::min(s->max_slots, count - off);
+        SimPrepArgs pa;
+        pa.g = g;
+        pa.dg = s->dg;
+        pa.nvar = s->nvar;
+        pa.types = s->d_types.p;
+        pa.tpl = s->d_tpl.p;
+        pa.wtab = s->d_wtab.p;
+        pa.path = s->d_path.p;
+        pa.begin = s->begin;
+        pa.seeds = s->d_seeds.p;
+        pa.nb_count = s->d_nb_count.p;
+        pa.nb_tpl = s->d_nb_tpl.p;
+        pa.nb_cell = s->d_nb_cell.p;
+        pa.n = s->n;
+        pa.state = s->d_state.p;
+        pa.init = s->d_init.p;
+        pa.nodes = nodes + off;
+        pa.nslots = B;
+        pa.k = s->k;
+        pa.K = s->K;
+        pa.nti = 1;
+        pa.slots = s->d_slots.p;
+        pa.terms = s->d_terms.p;
+        pa.maxterms = s->maxterms;
+        pa.status = s->d_status.p;
+        pa.missing = 0;
+        pa.mask_layer = s->nvar;
+        pa.no_verbatim = 0;
+        pa.id_image = s->d_id.p;
+        pa.node_nv = nullptr;
+        pa.node_k = nullptr;
+        pa.full = 0;
+        pa.nb_mask = nullptr;
+        CK(launch_prep_sim(pa, s->st));
+        MapArgs ma;
+        ma.g = g;
+        ma.layers = s->ti->layers.p;
+        ma.slots = s->d_slots.p;
+        ma.terms = s->d_terms.p;
+        ma.maxterms = s->maxterms;
+        ma.segs_per_cta = map_segs_per_cta(g, B);
+        ma.rec_val = s->d_rec_val.p;
+        ma.rec_idx = s->d_rec_idx.p;
+        ma.rec_cnt = s->d_rec_cnt.p;
+        ma.rec_max = s->d_rec_max.p;
+        CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+        ReplayArgs ra;
+        std::memset(&ra, 0, sizeof(ra));
+        ra.g = g;
+        ra.slots = s->d_slots.p;
+        ra.nslots = B;
+        ra.K = s->K;
+        ra.rec_val = s->d_rec_val.p;
+        ra.rec_idx = s->d_rec_idx.p;
+        ra.rec_cnt = s->d_rec_cnt.p;
+        ra.rec_max = s->d_rec_max.p;
+        ra.nvar = s->nvar;
+        ra.ti = s->ti->grid.p;
+        ra.ti_cells = s->ti->cells;
+        ra.nti = 1;
+        ra.state = teacher ? nullptr : s->d_state.p;
+        ra.id_image = teacher ? nullptr : s->d_id.p;
+        ra.node_cell = s->d_node_cell.p;
+        ra.drawn_score = s->d_drawn_score.p;
+        ra.drawn_scale = s->d_drawn_scale.p;
+        CK(launch_hash_select(ra, s->st));
+        ra.only_flagged = 1;
+        CK(launch_replay(ra, s->st));
+        s->info.launches += 4;
+        s->info.map_launches += 1;
+        s->info.map_positions += (long long)B * g.N;
+    }
     return QSK_OK;
 }
 
@@ -1348,8 +1496,34 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     pa.full = 0;
     pa.nb_mask = nullptr;
     CK(launch_prep_sim(pa, s->st));
-    // node rows of A
-    CK(cudaMemsetAsync(s->d_tc_A.p, 0, size_t(Bp * s->tc_Kp * elem), s->st));
+    const bool learned = s->topt.mode == 3;
+    if (learned) {
+        // node rows of A: the encoder's embeddings of the nodes' neighbourhoods
+        qsk_encoder *e = s->enc;
+        FeatArgs fa;
+        fa.rows = B;
+        fa.nodes = step.nodes + step.off;
+        fa.path = s->d_path.p;
+        fa.begin = s->begin;
+        fa.nb_count = s->d_nb_count.p;
+        fa.nb_tpl = s->d_nb_tpl.p;
+        fa.nb_cell = s->d_nb_cell.p;
+        fa.n = s->n;
+        fa.state = s->d_state.p;
+        fa.tpl = s->d_tpl.p;
+        fa.nd = g.nd;
+        fa.nvar = s->nvar;
+        fa.inv_radius = 0.125f;
+        fa.ntpl = s->ntpl;
+        fa.entries = QSK_ENC_ENTRIES;
+        fa.out = s->d_feat.p;
+        CK(launch_feat_nodes(fa, s->st));
+        int rc = enc_forward(e, B, B, s->d_feat.p, s->st);   // query head
+        if (rc) return rc;
+        CK(launch_to_bf16((long long)B * ENC_E, e->y.p, reinterpret_cast<uint16_t *>(s->d_tc_A.p), s->st));
+    } else {
+        CK(cudaMemsetAsync(s->d_tc_A.p, 0, size_t(Bp * s->tc_Kp * elem), s->st));
+    }
     TcNodeArgs na{};
     na.nd = g.nd;
     na.nvar = s->nvar;
@@ -1374,7 +1548,7 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     na.L = s->tc_L;
     na.Kp = s->tc_Kp;
     na.fmt = s->tc_fmt;
-    na.A = s->d_tc_A.p;
+    na.A = learned ? nullptr : s->d_tc_A.p;
     na.node_scale = s->d_tc_nscale.p;
     na.node_bias = s->d_tc_bias.p;
     na.node_box = s->d_tc_box.p;
@@ -1437,10 +1611,35 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     sa.err_sum = s->d_err_sum.p;
     sa.err_n = s->d_err_n.p;
     sa.status = s->d_status.p;
+    if (learned) {
+        sa.fallback = s->d_fb.p;
+        sa.conf_rank = s->lopt.conf_rank > 0 ? s->lopt.conf_rank : 1;
+        sa.conf_z = s->lopt.conf_z;
+        sa.conf_r2 = s->lopt.conf_r2 > 0.f ? s->lopt.conf_r2 : 0.2f;
+        sa.range_w = s->tc_W;
+    }
     CK(launch_tc_select(sa, s->st));
     if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
     s->info.launches += 4;
     s->info.tensor_launches += 4;
+    if (learned) {
+        // nodes whose confidence check failed: the exact map, in the same level
+        std::vector<int> fb((size_t)B), nd((size_t)B);
+        CK(cudaMemcpyAsync(fb.data(), s->d_fb.p, sizeof(int) * B, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaMemcpyAsync(nd.data(), step.nodes + step.off, sizeof(int) * B, cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        std::vector<int> list;
+        for (int q = 0; q < B; ++q)
+            if (fb[size_t(q)]) list.push_back(nd[size_t(q)]);
+        s->info.learned_fallback += (long long)list.size();
+        if (!list.empty()) {
+            CK(s->d_fb_nodes.ensure(list.size()));
+            CK(cudaMemcpyAsync(s->d_fb_nodes.p, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+            int rc = exact_nodes(s, s->d_fb_nodes.p, int(list.size()), teacher);
+            if (rc) return rc;
+            CK(cudaStreamSynchronize(s->st));   // the host list goes out of scope
+        }
+    }
     return QSK_OK;
 }
 
@@ -1464,6 +1663,10 @@ int tc_buffers(qsk_sim *s, size_t n_audit) {
     CK(s->d_err_sum.ensure(1));
     CK(s->d_err_n.ensure(1));
     CK(s->d_tc_counts.ensure(3));
+    if (s->topt.mode == 3) {
+        CK(s->d_feat.ensure(bp * size_t(s->enc->D0)));
+        CK(s->d_fb.ensure(bp));
+    }
     CK(cudaMemsetAsync(s->d_err_max.p, 0, sizeof(unsigned), s->st));
     CK(cudaMemsetAsync(s->d_err_sum.p, 0, sizeof(double), s->st));
     CK(cudaMemsetAsync(s->d_err_n.p, 0, sizeof(unsigned long long), s->st));
@@ -1494,6 +1697,8 @@ int tc_run(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     for (const Step &st : steps)
         if (st.kind == STEP_PLAIN || st.kind == STEP_HASH) mb = std::max(mb, st.B);
     if (!audit.empty()) mb = std::max(mb, std::min<int>(int(audit.size()), s->max_slots));
+    if (s->topt.mode == 3) mb = s->max_slots;   // fallback batches of up to max_slots
+    s->info.learned_fallback = 0;
     if ((rc = sim_records(s, mb)) != QSK_OK) return rc;
     if ((rc = sim_batches(s, steps, teacher)) != QSK_OK) return rc;
     // audit: the plain path, teacher-forced on the final grid (every node's
@@ -1993,6 +2198,121 @@ int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
         s->info.tensor_mode = 0;
         s->info.tensor_nodes = s->info.plain_nodes = s->info.audited = s->info.regret = s->info.regret_near = 0;
     }
+    return QSK_OK;
+}
+
+int qsk_sim_set_learned(qsk_sim *s, qsk_encoder *e, const qsk_learned_opts *o) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    if (!e) {
+        s->enc = nullptr;
+        s->topt = qsk_tensor_opts{};
+        s->tc_ready = false;
+        return QSK_OK;
+    }
+    qsk_learned_opts d{};
+    if (!o) o = &d;
+    if (o->width != 0 && !tc_supported_width(o->width)) return fail(QSK_ERR_ARG, "width %d (8, 16 or 32)", o->width);
+    if (o->shortlist < 0 || o->shortlist > 256) return fail(QSK_ERR_ARG, "shortlist %d (at most 256)", o->shortlist);
+    if (!(o->audit >= 0.f && o->audit <= 1.f) || o->conf_rank < 0) return fail(QSK_ERR_ARG, "audit / confidence rank");
+    if (e->nvar != s->nvar) return fail(QSK_ERR_ARG, "encoder for %d variables, simulation of %d", e->nvar, s->nvar);
+    if (e->device != s->device) return fail(QSK_ERR_ARG, "encoder on device %d, simulation on %d", e->device, s->device);
+    if (s->ti->missing || s->no_verbatim || s->full || s->local)
+        return fail(QSK_ERR_UNSUPPORTED, "learned proposal: complete TIs without -nV, -fs or local controls");
+    if (s->ti->g.nd > 3 || s->ti->cells > (1LL << 31))
+        return fail(QSK_ERR_UNSUPPORTED, "learned proposal: at most 3 dimensions and 2^31 cells");
+    s->enc = e;
+    s->lopt = *o;
+    s->topt = qsk_tensor_opts{};
+    s->topt.mode = 3;
+    s->topt.audit = o->audit;
+    s->max_tc_slots = 4096;
+    s->tc_ready = false;
+    s->enc_built = -1;
+    return QSK_OK;
+}
+
+int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed, const int *path_nodes, int count,
+                          long long *added) {
+    if (!e || !s || !di_completed || (!path_nodes && count > 0) || count < 0) return fail(QSK_ERR_ARG, "null argument");
+    if (e->nvar != s->nvar || e->device != s->device) return fail(QSK_ERR_ARG, "encoder and simulation differ");
+    DeviceGuard dgd(s->device);
+    // the exact path draws the nodes (teacher-forced), nodes without
+    // neighbours left out (their draw is the marginal one)
+    const qsk_tensor_opts keep = s->topt;
+    s->topt = qsk_tensor_opts{};
+    int rc = QSK_OK;
+    if (!s->neighbours_ready && (rc = sim_neighbours(s)) != QSK_OK) return rc;
+    std::vector<int> tmax;
+    if ((rc = tc_tmax(s, tmax)) != QSK_OK) return rc;
+    std::vector<int> nodes;
+    for (int q = 0; q < count; ++q) {
+        const int i = path_nodes[q];
+        if (i < 0 || i >= s->nodes) {
+            s->topt = keep;
+            return fail(QSK_ERR_ARG, "path node %d of %lld", i, s->nodes);
+        }
+        if (tmax[size_t(i)] >= 0) nodes.push_back(i);
+    }
+    rc = qsk_sim_run_teacher_nodes(s, di_completed, nodes.data(), int(nodes.size()));
+    s->topt = keep;
+    if (rc) return rc;
+    std::vector<unsigned> cell_all(size_t(s->nodes));
+    CK(cudaMemcpyAsync(cell_all.data(), s->d_node_cell.p, sizeof(unsigned) * size_t(s->nodes), cudaMemcpyDeviceToHost,
+                       s->st));
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<unsigned> cells(nodes.size());
+    for (size_t q = 0; q < nodes.size(); ++q) cells[q] = cell_all[size_t(nodes[q])];
+    const long long n = (long long)nodes.size();
+    const size_t rowf = size_t(e->D0);
+    if (e->npairs + n > e->pair_cap) {
+        const long long cap = std::max<long long>(e->npairs + n, 2 * e->pair_cap);
+        DBuf<float> q2, p2;
+        CK(q2.alloc(size_t(cap) * rowf));
+        CK(p2.alloc(size_t(cap) * rowf));
+        if (e->npairs) {
+            CK(cudaMemcpyAsync(q2.p, e->xq.p, sizeof(float) * size_t(e->npairs) * rowf, cudaMemcpyDeviceToDevice, s->st));
+            CK(cudaMemcpyAsync(p2.p, e->xp.p, sizeof(float) * size_t(e->npairs) * rowf, cudaMemcpyDeviceToDevice, s->st));
+            CK(cudaStreamSynchronize(s->st));
+        }
+        std::swap(e->xq.p, q2.p);
+        std::swap(e->xq.n, q2.n);
+        std::swap(e->xp.p, p2.p);
+        std::swap(e->xp.n, p2.n);
+        e->pair_cap = cap;
+    }
+    DBuf<unsigned> dcells;
+    CK(dcells.upload(cells.data(), cells.size(), s->st));
+    const Geom &g = s->ti->g;
+    FeatArgs fa;
+    fa.rows = n;
+    fa.nodes = s->d_level_nodes.p;   // the sample, in order (run_teacher_nodes)
+    fa.path = s->d_path.p;
+    fa.begin = s->begin;
+    fa.nb_count = s->d_nb_count.p;
+    fa.nb_tpl = s->d_nb_tpl.p;
+    fa.nb_cell = s->d_nb_cell.p;
+    fa.n = s->n;
+    fa.state = s->d_state.p;
+    fa.tpl = s->d_tpl.p;
+    fa.nd = g.nd;
+    fa.nvar = s->nvar;
+    fa.inv_radius = 0.125f;
+    fa.ntpl = s->ntpl;
+    fa.entries = QSK_ENC_ENTRIES;
+    fa.out = e->xq.p + size_t(e->npairs) * rowf;
+    CK(launch_feat_nodes(fa, s->st));
+    FeatArgs fc = fa;
+    fc.cell_list = dcells.p;
+    fc.cells = s->ti->cells;
+    fc.ti = s->ti->grid.p;
+    for (int d = 0; d < 3; ++d) fc.src[d] = d < g.nd ? g.src[d] : 1;
+    fc.ntpl = s->ntpl;
+    fc.entries = QSK_ENC_ENTRIES;
+    fc.out = e->xp.p + size_t(e->npairs) * rowf;
+    CK(launch_feat_cells(fc, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    e->npairs += n;
+    if (added) *added = n;
     return QSK_OK;
 }
 

@@ -369,7 +369,7 @@ struct TcSelectArgs {
     const unsigned long long *cand_key;  // [slot][ncand]
     const unsigned *cand_pos;
     int ncand;                           // ranges x W
-    int S;                               // candidates scored exactly (<= 128)
+    int S;                               // candidates scored exactly (<= 256)
     int fp64;                            // rank by the FP64 exact score
     const float *ti;
     int nvar;
@@ -383,6 +383,17 @@ struct TcSelectArgs {
     double *err_sum;
     unsigned long long *err_n;
     int *status;
+    // learned proposal: per slot 1 when the confidence check fails (the exact
+    // best of the shortlist ranks at conf_rank or later by the proposal's
+    // score); null: no check
+    int *fallback = nullptr;
+    int conf_rank = 0;
+    // > 0: the statistical check (the k-th best exact score must clear the
+    // regression bound a L_out + b + conf_z sd of the positions left out;
+    // range_w: heap entries per position range)
+    float conf_z = 0.f;
+    float conf_r2 = 0.2f;      // smallest R^2 of the fit
+    int range_w = 0;
 };
 // FP8: rowmax is scratch of `rows` floats
 cudaError_t launch_tc_pattern(const TcPatternArgs &a, float *rowmax, cudaStream_t st);
@@ -391,6 +402,49 @@ cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st);
 cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st);
 cudaError_t launch_tc_audit(int n, const int *nodes, int K, const float *plain_val, const float *drawn_score,
                             const float *drawn_scale, float tol, unsigned long long *counts, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// learned proposal (qsk_learn.cu): encoder inputs, FP32 GEMM and training ops
+// ---------------------------------------------------------------------------
+#define QSK_ENC_ENTRIES 64   // neighbourhood entries of an encoder input
+struct FeatArgs {
+    long long rows;
+    // nodes (k_feat_nodes): path indices and their neighbour lists
+    const int *nodes = nullptr;
+    const unsigned *path = nullptr;
+    unsigned begin = 0;
+    const int *nb_count = nullptr;
+    const int *nb_tpl = nullptr;
+    const unsigned *nb_cell = nullptr;
+    int n = 0;
+    const float *state = nullptr;     // grid values (cells x nvar)
+    // TI cells (k_feat_cells): cell0 + r, or cell_list[r] when given
+    long long cell0 = 0;
+    const unsigned *cell_list = nullptr;
+    long long cells = 0;
+    const float *ti = nullptr;
+    int src[3] = {1, 1, 1};
+    int ntpl = 0;
+    // both
+    const int *tpl = nullptr;         // template offsets (ntpl x nd)
+    int nd = 0, nvar = 0;
+    float inv_radius = 1.f;           // offsets are scaled by this
+    int entries = QSK_ENC_ENTRIES;    // template offsets 1..entries represented (at most 64)
+    float *out = nullptr;             // rows x (64 x (nvar + 4))
+};
+cudaError_t launch_sgemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb, int tb, float *C,
+                         int ldc, float alpha, float beta, const float *bias, cudaStream_t st);
+cudaError_t launch_gelu(long long n, const float *pre, float *out, cudaStream_t st);
+cudaError_t launch_gelu_back(long long n, const float *pre, float *d, cudaStream_t st);
+cudaError_t launch_colsum(int rows, int cols, const float *d, float *out, int accumulate, cudaStream_t st);
+cudaError_t launch_rownorm(int rows, int cols, const float *x, float *y, float *nrm, cudaStream_t st);
+cudaError_t launch_rownorm_back(int rows, int cols, const float *y, const float *nrm, float *d, cudaStream_t st);
+cudaError_t launch_infonce(int B, float tau, const float *S, float *dS, float *loss, cudaStream_t st);
+cudaError_t launch_adam(long long n, float *w, const float *g, float *m, float *v, float lr, int t, cudaStream_t st);
+cudaError_t launch_feat_nodes(const FeatArgs &a, cudaStream_t st);
+cudaError_t launch_feat_cells(const FeatArgs &a, cudaStream_t st);
+cudaError_t launch_to_bf16(long long n, const float *x, uint16_t *y, cudaStream_t st);
+cudaError_t launch_gather_rows(int n, int cols, const int *idx, const float *src, float *dst, cudaStream_t st);
 
 // 32-bit mix of a node seed and a position: the tie-break part of a
 // shortlist key (equal scores are ordered by it, uniformly at random over

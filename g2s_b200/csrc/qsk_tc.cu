@@ -725,7 +725,7 @@ __global__ void k_tc_nodes(TcNodeArgs A) {
     const float scale = A.fmt == 1 ? pow2_scale(amax) : 1.f;
     const float inv = 1.f / scale;
     float bias = 0.f;
-    for (int j = lane; j < cnt; j += 32) {
+    for (int j = lane; j < cnt && A.A; j += 32) {
         const int t = A.nb_tpl[(long long)i * A.n + j];
         const unsigned nc = A.nb_cell[(long long)i * A.n + j];
         for (int v = 0; v < A.nvar; ++v) {
@@ -828,7 +828,7 @@ __device__ __forceinline__ void exact_score(const Term *__restrict__ tm, int nt,
 
 constexpr int SEL_WARPS = 4;
 constexpr int SEL_CAND = 768;    // candidates per slot staged in shared memory
-constexpr int SEL_CPL = 4;       // shortlist entries per lane: at most 128 re-scored
+constexpr int SEL_CPL = 8;       // shortlist entries per lane: at most 256 re-scored
 
 // one warp per tensor slot: the S best candidates by approximate key, their
 // exact scores, the node's k best by exact score (ties by the key's hash),
@@ -848,11 +848,25 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     if (small)
         for (int t = lane; t < nt; t += 32) sterm[w][t] = tm[t];
     const int nc = A.ncand;
+    // largest key a position outside the final shortlist can have by the
+    // proposal (learned mode): the best of the ranges' heap minima (a full
+    // heap's minimum bounds what that range left out)
+    unsigned long long lout = 0ull;
     for (int c = lane; c < nc; c += 32) {
-        skey[w][c] = A.cand_key[(long long)b * nc + c];
+        const unsigned long long k = A.cand_key[(long long)b * nc + c];
+        skey[w][c] = k;
         spos[w][c] = A.cand_pos[(long long)b * nc + c];
     }
     __syncwarp();
+    if (A.fallback && A.conf_z > 0.f && A.range_w > 0) {
+        for (int r = lane; r * A.range_w < nc; r += 32) {
+            unsigned long long mn = ~0ull;
+            for (int f = 0; f < A.range_w; ++f) mn = min(mn, skey[w][r * A.range_w + f]);
+            lout = max(lout, mn);   // 0 when the range's heap was not full: it left nothing out
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lout = max(lout, __shfl_xor_sync(0xffffffffu, lout, o));
+    }
     const Term *tt = small ? sterm[w] : tm;
     // the S largest keys (S rounds of warp argmax); lane r keeps round r and r+32
     unsigned long long mykey[SEL_CPL];
@@ -895,6 +909,13 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         if (lane == 0) skey[w][bi] = 0ull;
         __syncwarp();
         ++nsel;
+    }
+    if (A.fallback && A.conf_z > 0.f) {
+        unsigned long long nk = 0ull;
+        for (int c = lane; c < nc; c += 32) nk = max(nk, skey[w][c]);   // best key not taken
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nk = max(nk, __shfl_xor_sync(0xffffffffu, nk, o));
+        lout = max(lout, nk);
     }
     // exact scores of the shortlist: the scan index of every candidate, then
     // all (candidate, term) layer values gathered by the whole warp at once
@@ -970,6 +991,7 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     float chosen32 = -INFINITY;
     double chosen_sc = 0.0;
     const bool f64 = A.fp64 != 0;
+    double kth_score = -INFINITY;   // the K-th best exact score (ranking precision)
     for (int k = 0; k < K && k < nsel; ++k) {
         int bh = -1;
         for (int h = 0; h < SEL_CPL; ++h) {
@@ -1013,10 +1035,12 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         const float w32 = __shfl_sync(0xffffffffu, w320, bl);
         const double wsc = __shfl_sync(0xffffffffu, wsc0, bl);
         // rank sel, or the last one found when fewer than sel + 1 exist
-        chosen = wp;
-        chosen32 = w32;
-        chosen_sc = wsc;
-        if (k == s.sel) break;
+        if (k <= s.sel) {
+            chosen = wp;
+            chosen32 = w32;
+            chosen_sc = wsc;
+        }
+        kth_score = bv;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -1024,10 +1048,101 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
         errsum += __shfl_xor_sync(0xffffffffu, errsum, o);
         errn += __shfl_xor_sync(0xffffffffu, errn, o);
     }
+    // confidence (learned proposal): the exact best of the shortlist must rank
+    // among its first conf_rank by the proposal's own score; otherwise the
+    // node goes to the exact map (no write-back here)
+    bool confident = true;
+    if (A.fallback) {
+        int br = 0x7FFFFFFF;
+        double bv2 = -INFINITY;
+        unsigned bh2 = 0u;
+        for (int h = 0; h < SEL_CPL; ++h) {
+            const int r = h * 32 + lane;
+            if (r >= nsel) continue;
+            const double v2 = f64 ? e64[h] : (double)e32[h];
+            if (v2 > bv2 || (v2 == bv2 && hsh[h] > bh2)) {
+                bv2 = v2;
+                bh2 = hsh[h];
+                br = r;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv2, o);
+            const unsigned oh = __shfl_xor_sync(0xffffffffu, bh2, o);
+            const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (ov > bv2 || (ov == bv2 && (oh > bh2 || (oh == bh2 && orr < br)))) {
+                bv2 = ov;
+                bh2 = oh;
+                br = orr;
+            }
+        }
+        confident = nsel > 0 && br < A.conf_rank;
+        if (A.conf_z > 0.f) {
+            // exact score against proposal score over the shortlist: s = a L + b
+            // with residual sd; a position left out has L <= L_out, so its
+            // score is below a L_out + b + z sd with high probability; the
+            // node is confident when its k-th best exact score clears that
+            double n = 0, sl = 0, ss = 0, sll = 0, sls = 0;
+            for (int h = 0; h < SEL_CPL; ++h) {
+                const int r = h * 32 + lane;
+                if (r >= nsel) continue;
+                const double L = (double)tc::unordered((unsigned)(mykey[h] >> 32));
+                const double v2 = f64 ? e64[h] : (double)e32[h];
+                n += 1;
+                sl += L;
+                ss += v2;
+                sll += L * L;
+                sls += L * v2;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                n += __shfl_xor_sync(0xffffffffu, n, o);
+                sl += __shfl_xor_sync(0xffffffffu, sl, o);
+                ss += __shfl_xor_sync(0xffffffffu, ss, o);
+                sll += __shfl_xor_sync(0xffffffffu, sll, o);
+                sls += __shfl_xor_sync(0xffffffffu, sls, o);
+            }
+            const double den = n * sll - sl * sl;
+            const double aa = den > 0 ? (n * sls - sl * ss) / den : 0.0;
+            const double bb = n > 0 ? (ss - aa * sl) / n : 0.0;
+            double r2 = 0;
+            for (int h = 0; h < SEL_CPL; ++h) {
+                const int r = h * 32 + lane;
+                if (r >= nsel) continue;
+                const double L = (double)tc::unordered((unsigned)(mykey[h] >> 32));
+                const double v2 = f64 ? e64[h] : (double)e32[h];
+                const double d = v2 - aa * L - bb;
+                r2 += d * d;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+            const double sd = n > 1 ? sqrt(r2 / n) : 0.0;
+            // variance of the exact scores: the fit must explain at least
+            // the fraction conf_r2 of it for its extrapolation to be trusted
+            const double var = n > 1 ? 1.0 : 0.0;
+            double tv = 0;
+            for (int h = 0; h < SEL_CPL; ++h) {
+                const int r = h * 32 + lane;
+                if (r >= nsel) continue;
+                const double v2 = (f64 ? e64[h] : (double)e32[h]) - (n > 0 ? ss / n : 0.0);
+                tv += v2 * v2;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) tv += __shfl_xor_sync(0xffffffffu, tv, o);
+            const bool fits = var > 0 && tv > 0 && aa > 0 && r2 <= (1.0 - (double)A.conf_r2) * tv;
+            const double Lout = lout ? (double)tc::unordered((unsigned)(lout >> 32)) : -INFINITY;
+            const double bound = lout ? aa * Lout + bb + (double)A.conf_z * sd : -INFINITY;
+            // the k-th best exact score of the shortlist (the K-th extraction)
+            confident = nsel >= K && fits && kth_score >= bound;
+        }
+    }
     if (lane == 0) {
         if (A.err_max) atomicMax(A.err_max, __float_as_uint(errmax));
         if (A.err_sum) atomicAdd(A.err_sum, errsum);
         if (A.err_n) atomicAdd(A.err_n, (unsigned long long)errn);
+        if (A.fallback) A.fallback[b] = confident ? 0 : 1;
+        if (!confident) return;
         if (chosen == 0xFFFFFFFFu) {
             if (A.status) atomicExch(A.status, DEV_BAD_INDEX);
             return;

@@ -345,6 +345,7 @@ typedef struct {
     float ms_tensor_pattern;      /* device time of building the pattern matrix (once per simulation) */
     long long tensor_launches;
     long long path_nodes;         /* path nodes of the simulation (nodes: those of the last run) */
+    long long learned_fallback;   /* learned proposal: nodes whose confidence check sent them to the exact map */
 } qsk_sim_info;
 
 typedef struct qsk_sim qsk_sim;
@@ -420,6 +421,80 @@ typedef struct {
     float audit;       /* fraction of tensor-path nodes audited, 0..1 */
 } qsk_tensor_opts;
 int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *opts);
+
+/* ------------------------------------------------------------------------
+ * Learned proposal (no G2S counterpart).  A small MLP encoder embeds the
+ * canonical neighbourhood of a node and of every TI cell: 64 entries, entry
+ * e for template offset e + 1, of [variable values, mask, dx, dy, dz]
+ * (offsets divided by 8); a node's entry holds the value of its neighbour at
+ * that offset (mask 1) or nothing (mask 0: no neighbour there), a TI cell's
+ * the TI value there (mask 0 outside the TI), into 64 dimensions: a shared trunk
+ * 64 x (nvar + 4) -> 256 -> 256 -> 256 (GELU), then a query head (nodes) or
+ * a TI-pattern head (TI cells) -> 64, unnormalised, so that the inner
+ * product can take the form of the QS score (2 v . t - |t|^2 for a
+ * continuous variable is the inner product of [2v, -1] and [t, |t|^2]).
+ * The tensor-core top-W
+ * kernel proposes, per node, the TI cells of largest inner product; the
+ * exact map (the plain path's FP32 terms) scores that shortlist; a node
+ * that fails the confidence check (qsk_learned_opts) goes to the exact map
+ * over the whole TI (the reference method,
+ * CPUThreadDevice::candidateForPattern + fKst::findKBiggest,
+ * src/CPUThreadDevice.cpp:349-490, include/fKb.hpp:907-954).
+ * ---------------------------------------------------------------------- */
+typedef struct qsk_encoder qsk_encoder;
+/* Encoder for TIs of nvar variables, weights uniform in +-1/sqrt(fan-in)
+ * from mt19937(seed), biases 0. */
+int qsk_encoder_create(int device, int nvar, unsigned seed, qsk_encoder **out);
+int qsk_encoder_destroy(qsk_encoder *e);
+long long qsk_encoder_param_count(const qsk_encoder *e);
+int qsk_encoder_input_dim(const qsk_encoder *e);
+/* All parameters, flattened: W1 (256 x D0), b1, W2 (256 x 256), b2, W3, b3,
+ * W4q (64 x 256), b4q (query head), W4p, b4p (TI-pattern head); weights
+ * row-major (out x in).  set resets Adam. */
+int qsk_encoder_get_weights(const qsk_encoder *e, float *out);
+int qsk_encoder_set_weights(qsk_encoder *e, const float *w);
+/* Symmetric InfoNCE loss of B (query, positive) input pairs (host, B x D0
+ * each; logits q . p / tau, in-batch negatives) and, if grad is not NULL,
+ * its gradient with respect to every parameter; no update. */
+int qsk_encoder_loss_grad(qsk_encoder *e, int B, const float *xq, const float *xp, float tau, float *loss,
+                          float *grad);
+/* Embeddings (rows x 64) of input rows (rows x D0), host arrays; head 0 the
+ * query head, 1 the TI-pattern head. */
+int qsk_encoder_embed(qsk_encoder *e, int head, long long rows, const float *x, float *out);
+/* Training pairs: the listed path nodes of simulation s are drawn by the
+ * exact path, teacher-forced on the completed grid; each (node
+ * neighbourhood, drawn TI cell's neighbourhood) pair is kept on the device.
+ * Nodes without neighbours are skipped.  *added: pairs appended. */
+int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed, const int *path_nodes, int count,
+                          long long *added);
+/* Training pairs from host arrays (n x D0 each): queries and their positives. */
+int qsk_encoder_add_pairs_host(qsk_encoder *e, long long n, const float *xq, const float *xp);
+int qsk_encoder_pairs(const qsk_encoder *e, long long *count);
+int qsk_encoder_clear_pairs(qsk_encoder *e);
+/* Adam (lr, betas 0.9 / 0.999) on the stored pairs, shuffled every epoch by
+ * mt19937(seed), minibatches of `batch`; *last_loss: the last batch's loss. */
+int qsk_encoder_train(qsk_encoder *e, int epochs, int batch, float lr, float tau, unsigned seed, float *last_loss);
+
+/* The learned proposal as the simulation's map: every node with neighbours
+ * is embedded, its `width` best TI cells per position range proposed on the
+ * tensor cores (BF16 inner products with the pre-embedded TI, built once per
+ * simulation and encoder state), the best `shortlist` (<= 256) scored
+ * exactly and drawn as in the tensor-core form; nodes failing the confidence
+ * check (exact best ranked at conf_rank or later by the proposal) and nodes
+ * without neighbours take the exact map.  The encoder must outlive its use
+ * by s.  `audit` as in qsk_tensor_opts.  e = NULL turns it off. */
+typedef struct {
+    int width;         /* 8, 16 or 32 (0: 32) */
+    int shortlist;     /* <= 256 (0: 256) */
+    int conf_rank;     /* rank check (used when conf_z <= 0): the exact best of the shortlist must be among
+                          the proposal's first conf_rank candidates (0: 1) */
+    float audit;
+    float conf_z;      /* statistical check (> 0): exact score against proposal score is fitted over the
+                          shortlist (s = a L + b, residual sd); the node's k-th best exact score must clear
+                          a L_out + b + conf_z sd, L_out the largest proposal score of a position left out */
+    float conf_r2;     /* ... and the fit must explain this fraction of the exact scores' variance (0: 0.2) */
+} qsk_learned_opts;
+int qsk_sim_set_learned(qsk_sim *s, qsk_encoder *e, const qsk_learned_opts *opts);
 
 /* Host-only planning helpers (no GPU needed), identical to what
  * qsk_sim_create computes.
