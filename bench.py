@@ -2,7 +2,8 @@
 plain FP32 path, at the k-best regret the audit measures.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload config1|config0|config3] [--path bf16|fp8|plain|fp32]
+                    [--workload config1|config0|config3|config4]
+                    [--path bf16|fp8|learned|plain|fp32]
 
 Workloads (seeded synthetic inputs; no public dataset is involved):
   config1 (default)  binary sinuous-channel TI 250x250 (20 channels, seed 1),
@@ -20,8 +21,20 @@ Workloads (seeded synthetic inputs; no public dataset is involved):
                      completed 200x200x100 GRF grid (seed 2): the whole
                      simulation is too long to repeat K times on the plain
                      path.  Default path: FP8 E4M3.
+  config4            bivariate 3-D TI 256^3 (continuous GRF, ranges 24,24,8
+                     voxels, plus a sinusoid-tube indicator, ~20 % facies 1),
+                     simulation 256^3, n=64, k=1.5; a step is the
+                     teacher-forced draw of every 4096th path node (4,096
+                     nodes) against a completed grid of other seeds.
+                     Default path: the learned proposal, its encoder trained
+                     first (untimed) on 2 M pairs drawn by the exact path on
+                     96^3 TIs of other seeds.  The line also reports the
+                     proposal with every node accepted (no confidence check,
+                     no fallback): its rate and its regret.
 Paths: bf16 / fp8 (tensor-core form, 1 % of the nodes audited on the plain
-path), plain (the exact reference path: bit-sliced counts for categorical
+path), learned (top-256 inner-product shortlist of the encoder's
+embeddings, exact re-scoring, confidence check with the plain path as
+fallback, 1 % audited), plain (the exact reference path: bit-sliced counts for categorical
 unit-weight patterns, FP32 gather otherwise), fp32 (the exact path with the
 FP32 gather map forced).  The headline path is timed over K steps; the
 plain and fp32 paths of the same workload over two steps each, for the
@@ -69,6 +82,10 @@ WORKLOADS = {
                     name="config0-continuous-grf-200x200-to-200x200-n50-k1.2"),
     "config3": dict(ti=("grf", (120, 150, 180), (5, 20, 20)), di=(100, 200, 200), types=[0], n=60, k=1.2, path="fp8",
                     sample=250, name="config3-continuous-grf3d-180x150x120-to-200x200x100-n60-k1.2-sample16000"),
+    "config4": dict(ti=("bivariate3d", (256, 256, 256), (8, 24, 24)), di=(256, 256, 256), types=[0, 1], n=64, k=1.5,
+                    path="learned", sample=4096, ref_grid=(2, 4, 4),
+                    train=dict(pairs=2_000_000, size=96, per_ti=300_000, epochs=20, batch=1024),
+                    name="config4-learned-bivariate3d-256^3-to-256^3-n64-k1.5-sample4096"),
 }
 SEED = 100
 
@@ -162,18 +179,75 @@ def dist_env():
     return ws, rank, local
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg: str):
+    """Progress on stderr (the result line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
+def bivariate3d(shape, ranges, seed):
+    """Continuous GRF and the 3-D sinusoid-tube indicator (about 20 % facies
+    1), variables interleaved."""
+    from g2s_b200 import synthetic as syn
+    return np.stack([syn.grf(shape, ranges, seed=seed), syn.tubes3d(shape, seed=seed)], axis=-1)
+
+
 def make_inputs(w):
     from g2s_b200 import synthetic as syn
     kind = w["ti"][0]
+    nv = len(w["types"])
     if kind == "channels":
         ti = syn.channels2d(w["ti"][1], n_channels=20, seed=1)
+    elif kind == "bivariate3d":
+        ti = bivariate3d(w["ti"][1], w["ti"][2], 1)
     else:
         ti = syn.grf(w["ti"][1], w["ti"][2], seed=1)
-    di = np.full(w["di"], np.nan, np.float32)
+    di = np.full(tuple(w["di"]) + ((nv,) if nv > 1 else ()), np.nan, np.float32)
     done = None
     if w.get("sample"):
-        done = syn.grf(w["di"], w["ti"][2], seed=2)
+        done = bivariate3d(w["di"], w["ti"][2], 2) if kind == "bivariate3d" else syn.grf(w["di"], w["ti"][2], seed=2)
     return ti, di, done
+
+
+def train_encoder(g2s, w, dev):
+    """The learned proposal's encoder, trained on (neighbourhood, drawn TI
+    cell) pairs that the exact path draws, teacher-forced, on TIs and
+    completed grids of other seeds (1000 + i, 2000 + i) of the workload's
+    generator; returns the encoder and a description."""
+    t = w["train"]
+    m = t["size"]
+    enc = g2s.Encoder(nvar=len(w["types"]), seed=11, device=dev)
+    t0 = time.perf_counter()
+    # a fixed number of training TIs, each giving up to per_ti pairs (path
+    # nodes without neighbours give none)
+    per = min(t["per_ti"], m ** 3)
+    n_ti = -(-t["pairs"] // per)
+    for i in range(n_ti):
+        tis = bivariate3d((m, m, m), w["ti"][2], 1000 + i)
+        done = bivariate3d((m, m, m), w["ti"][2], 2000 + i)
+        sim = g2s.Simulation(tis, np.full(done.shape, np.nan, np.float32), w["types"], n=w["n"], k=w["k"],
+                             seed=5 + i, device=dev)
+        take = min(per, t["pairs"] - per * i)
+        nodes = np.arange(0, m ** 3, max(1, m ** 3 // take), dtype=np.int32)[:take]
+        enc.add_pairs(sim, done, nodes)
+        sim.close()
+        log(f"training pairs: {enc.pairs()}")
+    i = n_ti
+    t1 = time.perf_counter()
+    loss = enc.train(epochs=t["epochs"] // 2, batch=t["batch"], lr=1e-3, tau=1.0, seed=1)
+    loss = enc.train(epochs=t["epochs"] - t["epochs"] // 2, batch=t["batch"], lr=3e-4, tau=1.0, seed=2)
+    t2 = time.perf_counter()
+    return enc, {"pairs": enc.pairs(), "training_tis": i, "training_ti": f"{m}^3 bivariate, seeds 1000..{999 + i}",
+                 "epochs": t["epochs"], "batch": t["batch"], "loss": loss, "pair_s": t1 - t0, "train_s": t2 - t1}
+
+
+def set_path(sim, path, enc=None, audit=0.01):
+    if path in ("bf16", "fp8"):
+        sim.set_tensor(path, audit=audit)
+    elif path == "learned":
+        sim.set_learned(enc, shortlist=256, audit=audit)
 
 
 def fft_in_use() -> str:
@@ -187,16 +261,20 @@ def reference_measure(args, w, steps: int):
     from oracle import ref
     cores = os.cpu_count() or 1
     ti, di, _ = make_inputs(w)
+    nv = len(w["types"])
     if w.get("sample"):
-        di = np.full((5, 10, 10), np.nan, np.float32)   # per-node cost: FFTs over the TI, not the grid
-        what = "5x10x10 grid (500 nodes) on the same TI, n and k"
+        # per-node cost: FFTs over the TI, not the grid
+        g = w.get("ref_grid", (5, 10, 10))
+        di = np.full(tuple(g) + ((nv,) if nv > 1 else ()), np.nan, np.float32)
+        what = f"{'x'.join(str(d) for d in g)} grid ({int(np.prod(g))} nodes) on the same TI, n and k"
     else:
-        what = f"the full {'x'.join(str(d) for d in w['di'])} grid ({di.size} nodes)"
+        what = f"the full {'x'.join(str(d) for d in w['di'])} grid ({int(np.prod(w['di']))} nodes)"
+    nodes = int(di.size // nv)
     qsargs = ["-k", str(w["k"]), "-n", str(w["n"]), "-s", str(SEED), "-j", str(cores)]
     vals = []
     for s in range(max(1, steps)):
         _, _, ms, _ = ref.run_qs(ti, di, w["types"], qsargs, job_id=9100 + s)
-        vals.append(di.size / (ms / 1000.0))
+        vals.append(nodes / (ms / 1000.0))
     return vals, cores, f"G2S qs, {what}, -j {cores}, its reported compute time; {fft_in_use()}"
 
 
@@ -232,11 +310,10 @@ def run_step(sim, w, done, sample):
     return sim.info()
 
 
-def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flush, clk=None):
-    """Timed steps of one path; returns (total device ms, per-step infos, profiled info, sim info)."""
+def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flush, enc=None):
+    """Timed steps of one path; returns (total device ms, per-step infos, profiled info)."""
     sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
-    if path in ("bf16", "fp8"):
-        sim.set_tensor(path, audit=0.01)
+    set_path(sim, path, enc)
     g2s.set_map_mode(1 if path == "fp32" else 0)
     import torch
     for _ in range(max(warmup, 0)):
@@ -264,7 +341,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--workload", default="config1", choices=sorted(WORKLOADS))
-    ap.add_argument("--path", default="", choices=["", "bf16", "fp8", "plain", "fp32"])
+    ap.add_argument("--path", default="", choices=["", "bf16", "fp8", "learned", "plain", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / fp32 comparison arms")
@@ -285,6 +362,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = local
+    log(f"inputs of {w['name']}")
     ti, di, done = make_inputs(w)
     sample = None
     if w.get("sample"):
@@ -292,6 +370,10 @@ def main():
     seed = replica_seed(SEED, rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")  # > 126 MB L2
     own_peaks = g2s.measure_peaks(dev)
+    log("peaks measured")
+    enc, enc_info = (train_encoder(g2s, w, dev) if path == "learned" else (None, None))
+    if enc_info:
+        log(f"encoder trained: {enc_info}")
 
     # headline path: K timed steps (CUDA events inside the engine, first to
     # last kernel of each step on its stream), L2 flushed between steps
@@ -299,10 +381,11 @@ def main():
         if dist:
             dist.barrier()
         total_ms, infos, pinf = time_path(g2s, w, ti, di, done, sample, seed, dev, path, args.steps, args.warmup,
-                                          flush)
+                                          flush, enc)
         if dist:
             dist.barrier()
     clocks = clk.summary()
+    log(f"headline path {path}: {total_ms:.1f} ms over {args.steps} steps")
     nodes = int(infos[-1]["nodes"])
     total_ms = slowest(total_ms, dist, f"cuda:{dev}")
     value = whole_job_rate(nodes, args.steps, ws, total_ms)
@@ -315,19 +398,41 @@ def main():
             if p == path or (p == "fp32" and w["types"] != [1]):
                 continue   # continuous patterns: the plain path is the FP32 gather map already
             t, inf2, _ = time_path(g2s, w, ti, di, done, sample, seed, dev, p, 2, 1, flush)
+            log(f"comparison path {p}: {t:.1f} ms over 2 steps")
             t = slowest(t, dist, f"cuda:{dev}")
             compare[p] = {"value": whole_job_rate(nodes, 2, ws, t), "ms_per_step": t / 2,
                           "kernel": ("k_map_bits" if (p == "plain" and w["types"] == [1]) else "k_map_records") +
                                     " + k_replay (exact reservoir k-best)"}
 
+    # learned proposal, diagnostic: every proposal accepted (no confidence
+    # check, no fallback): its rate and its regret over all nodes
+    accept_all = None
+    if path == "learned":
+        sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
+        sim.set_learned(enc, shortlist=256, conf_z=0.0, conf_rank=256, audit=1.0)
+        run_step(sim, w, done, sample)
+        a = sim.info()
+        sim.set_learned(enc, shortlist=256, conf_z=0.0, conf_rank=256, audit=0.0)
+        run_step(sim, w, done, sample)
+        sim.set_profiling(True)
+        b = run_step(sim, w, done, sample)
+        sim.set_profiling(False)
+        sim.close()
+        accept_all = {"value": a["nodes"] / (b["ms_total"] / 1000.0), "unit": UNIT, "ms_per_step": b["ms_total"],
+                      "ms_gemm": b["ms_tensor_gemm"], "ms_select": b["ms_tensor_select"],
+                      "regret": a["regret"], "audited": a["audited"],
+                      "rate": a["regret"] / max(1, a["audited"])}
+
+    if accept_all:
+        log(f"accept-all diagnostic: {accept_all}")
     # roofline of the dominant kernel of the profiled step
     pk, pk_kind = peaks()
-    tensor = path in ("bf16", "fp8")
+    tensor = path in ("bf16", "fp8", "learned")
     kernels = {}
     if tensor:
         gemm_ms = max(pinf["ms_tensor_gemm"], 1e-9)
-        tc_peak = pk.get("bf16_tflops", 1590.0) if path == "bf16" else own_peaks["fp8_tflops"]
-        tc_peak_kind = (f"{pk_kind} bf16_tflops (cuBLAS, burst)" if path == "bf16" else
+        tc_peak = pk.get("bf16_tflops", 1590.0) if path != "fp8" else own_peaks["fp8_tflops"]
+        tc_peak_kind = (f"{pk_kind} bf16_tflops (cuBLAS, burst)" if path != "fp8" else
                         "fp8 E4M3 dense, this library's tcgen05 microbenchmark (qsk_measure_peaks)")
         ach = pinf["tensor_flops"] / (gemm_ms / 1000.0) / 1e12
         kernels["k_tc_shortlist"] = {"ms_per_step": pinf["ms_tensor_gemm"], "bound": "tensor",
@@ -338,12 +443,16 @@ def main():
     kernels["exact_map (" + ("k_map_bits" if w["types"] == [1] else "k_map_records") + ")"] = {
         "ms_per_step": pinf["ms_map"], "map_launches": pinf["map_launches"]}
     kernels["k_replay / k_hash_select"] = {"ms_per_step": pinf["ms_replay"]}
+    # the dominant kernel of the step by device time: the shortlist GEMM, or
+    # the exact map (plain path; a tensor path's exact-map and fallback nodes)
+    gemm_dominant = tensor and pinf["ms_tensor_gemm"] >= pinf["ms_map"]
+    map_nodes = nodes if not tensor else int(pinf["plain_nodes"] + pinf["learned_fallback"])
     traffic = None
     try:
-        traffic = json.load(open(TRAFFIC_FILE)).get(args.workload, {}).get("k_tc_shortlist" if tensor else "map")
+        traffic = json.load(open(TRAFFIC_FILE)).get(args.workload, {}).get("k_tc_shortlist" if gemm_dominant else "map")
     except Exception:
         pass
-    if tensor:
+    if gemm_dominant:
         k = kernels["k_tc_shortlist"]
         launches_gemm = max(1, int(pinf["tensor_launches"]) // 4)
         roofline = {"bound": "tensor", "achieved": k["achieved_tflops"], "peak": k["peak_tflops"], "unit": "TFLOP/s",
@@ -355,12 +464,12 @@ def main():
     else:
         fp32 = own_peaks["fp32_tflops"]
         N = int(np.prod(w["ti"][1]))
-        L = 2
-        useful = 2.0 * w["n"] * N * L * nodes / (pinf["ms_map"] / 1000.0) / 1e12
+        L = 2 * len(w["types"])
+        useful = 2.0 * w["n"] * N * L * map_nodes / (max(pinf["ms_map"], 1e-9) / 1000.0) / 1e12
         roofline = {"bound": "fp32" if w["types"] != [1] else "alu", "achieved": useful, "peak": fp32,
-                    "unit": "TFLOP/s (FP32-equivalent 2*n*N*L per node)", "frac": useful / fp32, "traffic": traffic,
-                    "kernel": "exact map", "peak_kind": "FP32 FMA, this library's microbenchmark (qsk_measure_peaks)",
-                    "kernels": kernels}
+                    "unit": "TFLOP/s (FP32-equivalent 2*n*N*L per node, L = 2 per variable)", "frac": useful / fp32,
+                    "traffic": traffic, "kernel": "exact map", "map_nodes_per_step": map_nodes,
+                    "peak_kind": "FP32 FMA, this library's microbenchmark (qsk_measure_peaks)", "kernels": kernels}
 
     # e2e: the public one-call API with host buffers (H2D of the inputs, D2H
     # of the results inside the timed region), wall clock around the call
@@ -371,19 +480,19 @@ def main():
         t0 = time.perf_counter()
         if w.get("sample"):
             sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
-            if path in ("bf16", "fp8"):
-                sim.set_tensor(path, audit=0.01)
+            set_path(sim, path, enc)
             sim.run_teacher_nodes(done, sample)
             _, _, cells = sim.read()
             sim.close()
             h2d, d2h = ti.nbytes + done.nbytes + di.nbytes + sample.nbytes, int(done.nbytes + di.size * 4 + cells.nbytes)
         else:
-            d = np.full(w["di"], np.nan, np.float32)
+            d = np.full(di.shape, np.nan, np.float32)
             g2s.qs(ti, d, w["types"], k=w["k"], n=w["n"], s=seed, device=dev,
                    tensor=path if path in ("bf16", "fp8") else None)
             h2d, d2h = ti.nbytes + di.nbytes, int(di.nbytes + di.size * 4)
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
+        log(f"e2e call: {e2e_vals[-1]:.2f} s")
     e2e_s = float(np.mean(e2e_vals)) if e2e_vals else float("nan")
     e2e_s = slowest(e2e_s, dist, f"cuda:{dev}")
     e2e = {"value": nodes * ws / e2e_s if e2e_vals else None, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -393,7 +502,9 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         from oracle import ref
         if ref.available():
+            log("cpu baseline (reference) ...")
             vals, cores, samp = reference_measure(args, w, 1)
+            log(f"cpu baseline: {vals}")
             cpu = {"value": float(np.mean(vals)), "unit": UNIT, "cores": cores, "kind": "reference", "sample": samp}
 
     if rank == 0:
@@ -403,13 +514,17 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"bf16": "bf16", "fp8": "fp8-e4m3", "plain": "u8" if w["types"] == [1] else "f32",
+            "dtype": {"bf16": "bf16", "fp8": "fp8-e4m3", "learned": "bf16", "plain": "u8" if w["types"] == [1] else "f32",
                       "fp32": "f32"}[path],
             "data": "synthetic",
             "config": {"workload": w["name"], "path": path,
                        "tensor": {"prefix": last["tensor_prefix"], "width": last["tensor_width"],
                                   "shortlist": last["tensor_shortlist"], "tensor_nodes": last["tensor_nodes"],
                                   "exact_map_nodes": last["plain_nodes"], "audit_fraction": 0.01} if tensor else None,
+                       "learned": {"encoder": enc_info, "shortlist": 256, "confidence": "fit R^2 >= 0.2, z = 2",
+                                   "confident_nodes": int(last["tensor_nodes"] - last["learned_fallback"]),
+                                   "fallback_nodes": int(last["learned_fallback"]),
+                                   "accept_all_diagnostic": accept_all} if path == "learned" else None,
                        "nodes_per_step": nodes, "levels": last["levels"], "max_batch": last["max_batch"],
                        "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{ws}"},
             "vs_plain": {"plain": compare.get("plain"), "fp32_gather": compare.get("fp32"),
@@ -425,7 +540,7 @@ def main():
             "map_error_vs_fp64": {"max": max(i["map_err_max"] for i in infos),
                                   "mean": float(np.mean([i["map_err_mean"] for i in infos])),
                                   "unit": "|score - FP64 score| / term scale over the re-scored shortlists"}
-            if tensor else None,
+            if path in ("bf16", "fp8") else None,
             "roofline": roofline,
             "own_peaks": own_peaks,
             "breakdown_ms": {"neighbours": pinf["ms_setup_neighbours"], "levels": pinf["ms_levels"],

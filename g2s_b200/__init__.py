@@ -118,6 +118,8 @@ SIGNATURES = {
     "qsk_encoder_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_encoder_param_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "qsk_encoder_input_dim": (ctypes.c_int, [ctypes.c_void_p]),
+    "qsk_encoder_set_scales": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]),
+    "qsk_encoder_get_pairs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, _f32p, _f32p]),
     "qsk_encoder_get_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
     "qsk_encoder_set_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
     "qsk_encoder_loss_grad": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _f32p, _f32p, ctypes.c_float, _f32p, _f32p]),
@@ -510,6 +512,11 @@ class Encoder:
         self.input_dim = lib().qsk_encoder_input_dim(h)
         self.param_count = lib().qsk_encoder_param_count(h)
 
+    def set_scales(self, nscales: int = 4, cov_min: float = 0.9):
+        """Stencil scales of the inputs (qsk_encoder_set_scales)."""
+        _check(lib().qsk_encoder_set_scales(self.handle, int(nscales), float(cov_min)), "qsk_encoder_set_scales")
+        return self
+
     def weights(self) -> np.ndarray:
         w = np.zeros(self.param_count, np.float32)
         _check(lib().qsk_encoder_get_weights(self.handle, _p(w, _f32p)), "qsk_encoder_get_weights")
@@ -558,6 +565,15 @@ class Encoder:
         n = ctypes.c_longlong(0)
         _check(lib().qsk_encoder_pairs(self.handle, ctypes.byref(n)), "qsk_encoder_pairs")
         return n.value
+
+    def get_pairs(self, first: int = 0, n: Optional[int] = None):
+        """Stored (query, positive) input rows [first, first + n) as two arrays."""
+        n = self.pairs() - first if n is None else n
+        q = np.zeros((n, self.input_dim), np.float32)
+        p = np.zeros((n, self.input_dim), np.float32)
+        _check(lib().qsk_encoder_get_pairs(self.handle, int(first), int(n), _p(q, _f32p), _p(p, _f32p)),
+               "qsk_encoder_get_pairs")
+        return q, p
 
     def clear_pairs(self):
         _check(lib().qsk_encoder_clear_pairs(self.handle), "qsk_encoder_clear_pairs")

@@ -201,6 +201,15 @@ int qsk_encoder_destroy(qsk_encoder *e) {
 long long qsk_encoder_param_count(const qsk_encoder *e) { return e ? e->nparam : -1; }
 int qsk_encoder_input_dim(const qsk_encoder *e) { return e ? e->D0 : -1; }
 
+int qsk_encoder_set_scales(qsk_encoder *e, int nscales, float cov_min) {
+    if (!e) return set_error(QSK_ERR_ARG, "null argument");
+    if (nscales < 1 || nscales > 16 || !(cov_min >= 0.f && cov_min <= 1.f))
+        return set_error(QSK_ERR_ARG, "scales %d, coverage %g", nscales, double(cov_min));
+    e->nscales = nscales;
+    e->cov_min = cov_min;
+    return QSK_OK;
+}
+
 int qsk_encoder_get_weights(const qsk_encoder *e, float *out) {
     if (!e || !out) return set_error(QSK_ERR_ARG, "null argument");
     DeviceGuard dg(e->device);
@@ -286,6 +295,19 @@ int qsk_encoder_add_pairs_host(qsk_encoder *e, long long n, const float *xq, con
 int qsk_encoder_pairs(const qsk_encoder *e, long long *count) {
     if (!e || !count) return set_error(QSK_ERR_ARG, "null argument");
     *count = e->npairs;
+    return QSK_OK;
+}
+
+int qsk_encoder_get_pairs(const qsk_encoder *e, long long first, long long n, float *xq, float *xp) {
+    if (!e || (n > 0 && (!xq || !xp))) return set_error(QSK_ERR_ARG, "null argument");
+    if (first < 0 || n < 0 || first + n > e->npairs)
+        return set_error(QSK_ERR_ARG, "pairs [%lld, %lld) of %lld", first, first + n, e->npairs);
+    if (n == 0) return QSK_OK;
+    DeviceGuard dg(e->device);
+    const size_t row = size_t(e->D0), at = size_t(first) * row, cnt = size_t(n) * row;
+    QSK_CK(cudaMemcpyAsync(xq, e->xq.p + at, sizeof(float) * cnt, cudaMemcpyDeviceToHost, e->st));
+    QSK_CK(cudaMemcpyAsync(xp, e->xp.p + at, sizeof(float) * cnt, cudaMemcpyDeviceToHost, e->st));
+    QSK_CK(cudaStreamSynchronize(e->st));
     return QSK_OK;
 }
 

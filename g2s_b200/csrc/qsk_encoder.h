@@ -16,6 +16,10 @@ constexpr int ENC_NP = 10;   // parameter blocks: trunk (3 layers), query head, 
 struct qsk_encoder {
     int device = 0;
     int nvar = 1, F = 5, D0 = 320;
+    // stencil scales of the inputs: the TI is embedded at scales 1..nscales;
+    // a node takes the smallest holding cov_min of its neighbours
+    int nscales = 4;
+    float cov_min = 0.9f;
     long long off[qsk::ENC_NP + 1] = {};
     long long nparam = 0;
     cudaStream_t st = nullptr;

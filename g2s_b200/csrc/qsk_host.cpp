@@ -736,6 +736,10 @@ struct qsk_sim {
     qsk_encoder *enc = nullptr;
     qsk_learned_opts lopt{};
     int enc_built = -1;                 // encoder Adam step count the TI embeddings were built at
+    int enc_ns = 0;                     // ... and its number of stencil scales (P holds one matrix per scale)
+    DBuf<int> d_ent_cube;               // stencil entry of every offset of the stencil's box (-1: none)
+    int cube_lo[3] = {0, 0, 0}, cube_dim[3] = {1, 1, 1};
+    DBuf<int> d_lscale;                 // stencil scale per position of the level order
     DBuf<float> d_feat;                 // encoder input rows of a step / a chunk of TI cells
     DBuf<int> d_fb;                     // per slot: confidence check failed
     DBuf<int> d_fb_nodes;
@@ -944,6 +948,7 @@ struct Step {
     const int *nodes;   // device node list
     int off, B;
     int kb_off;         // TENSOR: this step's tile K-blocks in d_tc_kb
+    int scale = 1;      // TENSOR, learned proposal: the nodes' stencil scale
 };
 
 int tc_step(qsk_sim *s, const Step &st, bool teacher);
@@ -1140,9 +1145,76 @@ cudaEvent_t tc_event(qsk_sim *s) {
 
 long long rup(long long x, long long m) { return (x + m - 1) / m * m; }
 
+// the encoder stencil's lookup: entry e (template offset e + 1, e < 64) at
+// its offset in the bounding box of those offsets, -1 elsewhere
+int stencil_cube(qsk_sim *s) {
+    const int nd = s->ti->g.nd;
+    const int E = std::min(QSK_ENC_ENTRIES, s->ntpl - 1);
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int t = 1; t <= E; ++t)
+        for (int d = 0; d < nd; ++d) {
+            lo[d] = std::min(lo[d], s->tpl[size_t(t * nd + d)]);
+            hi[d] = std::max(hi[d], s->tpl[size_t(t * nd + d)]);
+        }
+    size_t n = 1;
+    for (int d = 0; d < 3; ++d) {
+        s->cube_lo[d] = d < nd ? lo[d] : 0;
+        s->cube_dim[d] = d < nd ? hi[d] - lo[d] + 1 : 1;
+        n *= size_t(s->cube_dim[d]);
+    }
+    std::vector<int> cube(n, -1);
+    for (int t = 1; t <= E; ++t) {
+        size_t idx = 0, st = 1;
+        for (int d = 0; d < nd; ++d) {
+            idx += size_t(s->tpl[size_t(t * nd + d)] - s->cube_lo[d]) * st;
+            st *= size_t(s->cube_dim[d]);
+        }
+        cube[idx] = t - 1;
+    }
+    CK(s->d_ent_cube.upload(cube.data(), cube.size(), s->st));
+    CK(cudaStreamSynchronize(s->st));   // the host vector goes out of scope
+    return QSK_OK;
+}
+
+void feat_stencil(const qsk_sim *s, const qsk_encoder *e, FeatArgs &fa) {
+    fa.cube = s->d_ent_cube.p;
+    for (int d = 0; d < 3; ++d) {
+        fa.cube_lo[d] = s->cube_lo[d];
+        fa.cube_dim[d] = s->cube_dim[d];
+    }
+    fa.nscales = e->nscales;
+    fa.cov_min = e->cov_min;
+}
+
+// the stencil scale (encoder e's) of each of `rows` nodes (device list) into scale_out
+int node_scales(qsk_sim *s, const qsk_encoder *e, const int *nodes, long long rows, int *scale_out) {
+    if (!s->d_ent_cube.p) {
+        int rc = stencil_cube(s);
+        if (rc) return rc;
+    }
+    FeatArgs fa;
+    fa.rows = rows;
+    fa.nodes = nodes;
+    fa.path = s->d_path.p;
+    fa.begin = s->begin;
+    fa.nb_count = s->d_nb_count.p;
+    fa.nb_tpl = s->d_nb_tpl.p;
+    fa.nb_cell = s->d_nb_cell.p;
+    fa.n = s->n;
+    fa.tpl = s->d_tpl.p;
+    fa.nd = s->ti->g.nd;
+    fa.nvar = s->nvar;
+    fa.ntpl = s->ntpl;
+    fa.entries = QSK_ENC_ENTRIES;
+    feat_stencil(s, e, fa);
+    fa.scale_out = scale_out;
+    CK(launch_node_scale(fa, s->st));
+    return QSK_OK;
+}
+
 // pattern matrix of the template prefix (built once per simulation and mode)
-// learned proposal: the pattern matrix is the TI cells' embeddings (BF16,
-// 64 columns), built once per encoder state
+// learned proposal: the pattern matrices are the TI cells' embeddings (BF16,
+// 64 columns), one per stencil scale, built once per encoder state
 int tc_configure_learned(qsk_sim *s) {
     const Geom &g = s->ti->g;
     qsk_encoder *e = s->enc;
@@ -1155,35 +1227,42 @@ int tc_configure_learned(qsk_sim *s) {
     s->tc_fmt = 0;
     s->tc_Kp = ENC_E;
     s->tc_rows = rows;
-    if (s->tc_ready && s->enc_built == e->t) return QSK_OK;
+    if (s->tc_ready && s->enc_built == e->t && s->enc_ns == e->nscales) return QSK_OK;
     s->tc_ready = false;
-    CK(s->d_tc_P.alloc(size_t(rows) * ENC_E * 2));
-    CK(cudaMemsetAsync(s->d_tc_P.p, 0, size_t(rows) * ENC_E * 2, s->st));
+    int rc = stencil_cube(s);
+    if (rc) return rc;
+    const size_t per_scale = size_t(rows) * ENC_E * 2;
+    CK(s->d_tc_P.alloc(per_scale * size_t(e->nscales)));
+    CK(cudaMemsetAsync(s->d_tc_P.p, 0, per_scale * size_t(e->nscales), s->st));
     const long long chunk = 131072;
     CK(s->d_feat.ensure(size_t(chunk) * size_t(e->D0)));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, s->st));
-    for (long long c0 = 0; c0 < s->ti->cells; c0 += chunk) {
-        const long long n = std::min(chunk, s->ti->cells - c0);
-        FeatArgs fa;
-        fa.rows = n;
-        fa.cell0 = c0;
-        fa.cells = s->ti->cells;
-        fa.ti = s->ti->grid.p;
-        for (int d = 0; d < 3; ++d) fa.src[d] = d < g.nd ? g.src[d] : 1;
-        fa.ntpl = s->ntpl;
-        fa.tpl = s->d_tpl.p;
-        fa.nd = g.nd;
-        fa.nvar = s->nvar;
-        fa.inv_radius = 0.125f;
-        fa.entries = QSK_ENC_ENTRIES;
-        fa.out = s->d_feat.p;
-        CK(launch_feat_cells(fa, s->st));
-        int rc = enc_forward(e, n, 0, s->d_feat.p, s->st);   // TI-pattern head
-        if (rc) return rc;
-        CK(launch_to_bf16(n * ENC_E, e->y.p, reinterpret_cast<uint16_t *>(s->d_tc_P.p) + size_t(c0) * ENC_E, s->st));
+    for (int sc = 1; sc <= e->nscales; ++sc) {
+        uint16_t *P = reinterpret_cast<uint16_t *>(s->d_tc_P.p + per_scale * size_t(sc - 1));
+        for (long long c0 = 0; c0 < s->ti->cells; c0 += chunk) {
+            const long long n = std::min(chunk, s->ti->cells - c0);
+            FeatArgs fa;
+            fa.rows = n;
+            fa.cell0 = c0;
+            fa.cells = s->ti->cells;
+            fa.ti = s->ti->grid.p;
+            for (int d = 0; d < 3; ++d) fa.src[d] = d < g.nd ? g.src[d] : 1;
+            fa.ntpl = s->ntpl;
+            fa.tpl = s->d_tpl.p;
+            fa.nd = g.nd;
+            fa.nvar = s->nvar;
+            fa.inv_radius = 0.125f;
+            fa.entries = QSK_ENC_ENTRIES;
+            fa.scale = sc;
+            fa.out = s->d_feat.p;
+            CK(launch_feat_cells(fa, s->st));
+            rc = enc_forward(e, n, 0, s->d_feat.p, s->st);   // TI-pattern head
+            if (rc) return rc;
+            CK(launch_to_bf16(n * ENC_E, e->y.p, P + size_t(c0) * ENC_E, s->st));
+        }
     }
     CK(cudaEventRecord(e1, s->st));
     CK(cudaEventSynchronize(e1));
@@ -1193,6 +1272,7 @@ int tc_configure_learned(qsk_sim *s) {
     cudaEventDestroy(e1);
     s->info.ms_tensor_pattern = ms;
     s->enc_built = e->t;
+    s->enc_ns = e->nscales;
     s->tc_ready = true;
     return QSK_OK;
 }
@@ -1325,29 +1405,66 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
     double flops = 0.0;
     const long long ntiles_pos = s->tc_rows / 256;
     const unsigned athr = s->topt.audit >= 1.f ? 0xFFFFFFFFu : unsigned(double(s->topt.audit) * 4294967296.0);
-    std::vector<int> el, pl;
+    const bool learned = s->topt.mode == 3;
+    // learned proposal: every node's stencil scale (per position of the level order)
+    std::vector<int> lscale;
+    if (learned && !start.empty() && start.back() > 0) {
+        const long long tot = start.back();
+        CK(s->d_lscale.ensure(size_t(tot)));
+        int rc = node_scales(s, s->enc, s->d_level_nodes.p, tot, s->d_lscale.p);
+        if (rc) return rc;
+        lscale.resize(size_t(tot));
+        CK(cudaMemcpyAsync(lscale.data(), s->d_lscale.p, sizeof(int) * size_t(tot), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    std::vector<int> el, pl, esc, idx;
     for (size_t l = 0; l + 1 < start.size(); ++l) {
         el.clear();
         pl.clear();
-        const bool learned = s->topt.mode == 3;
+        esc.clear();
         for (int q = start[l]; q < start[l + 1]; ++q) {
             const int i = order[size_t(q)];
-            (tmax[size_t(i)] >= 0 && (learned || tmax[size_t(i)] < T) ? el : pl).push_back(i);
+            const bool tc = tmax[size_t(i)] >= 0 && (learned || tmax[size_t(i)] < T);
+            (tc ? el : pl).push_back(i);
+            if (tc && learned) esc.push_back(lscale[size_t(q)]);
         }
-        std::stable_sort(el.begin(), el.end(), [&](int a, int b) { return tmax[size_t(a)] < tmax[size_t(b)]; });
+        if (learned) {
+            // one stencil scale per step: the level's nodes grouped by scale
+            idx.resize(el.size());
+            for (size_t j = 0; j < idx.size(); ++j) idx[j] = int(j);
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return esc[size_t(a)] < esc[size_t(b)]; });
+            std::vector<int> e2(el.size()), s2(el.size());
+            for (size_t j = 0; j < idx.size(); ++j) {
+                e2[j] = el[size_t(idx[j])];
+                s2[j] = esc[size_t(idx[j])];
+            }
+            el.swap(e2);
+            esc.swap(s2);
+        } else {
+            std::stable_sort(el.begin(), el.end(), [&](int a, int b) { return tmax[size_t(a)] < tmax[size_t(b)]; });
+        }
         int q = start[l];
         for (int i : el) order[size_t(q++)] = i;
         for (int i : pl) order[size_t(q++)] = i;
-        for (int off = 0; off < int(el.size()); off += s->max_tc_slots) {
-            const int B = std::min(s->max_tc_slots, int(el.size()) - off);
-            Step st{STEP_TENSOR, s->d_level_nodes.p, start[l] + off, B, int(kb.size())};
-            for (int t0 = 0; t0 < B; t0 += 128) {
-                const int last = el[size_t(off + std::min(B, t0 + 128) - 1)];
-                const int k = learned ? 1 : int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
-                kb.push_back(k);
-                flops += 2.0 * 128 * 256 * double(ntiles_pos) * double(k) * kbe;
+        for (int g0 = 0; g0 < int(el.size());) {
+            int g1 = int(el.size());
+            if (learned) {
+                g1 = g0 + 1;
+                while (g1 < int(el.size()) && esc[size_t(g1)] == esc[size_t(g0)]) ++g1;
             }
-            steps.push_back(st);
+            for (int off = g0; off < g1; off += s->max_tc_slots) {
+                const int B = std::min(s->max_tc_slots, g1 - off);
+                Step st{STEP_TENSOR, s->d_level_nodes.p, start[l] + off, B, int(kb.size())};
+                st.scale = learned ? esc[size_t(off)] : 1;
+                for (int t0 = 0; t0 < B; t0 += 128) {
+                    const int last = el[size_t(off + std::min(B, t0 + 128) - 1)];
+                    const int k = learned ? 1 : int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
+                    kb.push_back(k);
+                    flops += 2.0 * 128 * 256 * double(ntiles_pos) * double(k) * kbe;
+                }
+                steps.push_back(st);
+            }
+            g0 = g1;
         }
         for (int off = 0; off < int(pl.size()); off += s->max_slots)
             steps.push_back({STEP_HASH, s->d_level_nodes.p, start[l] + int(el.size()) + off,
@@ -1413,7 +1530,9 @@ int exact_nodes(qsk_sim *s, const int *nodes, int count, bool teacher) {
         pa.node_k = nullptr;
         pa.full = 0;
         pa.nb_mask = nullptr;
+        if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         CK(launch_prep_sim(pa, s->st));
+        if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         MapArgs ma;
         ma.g = g;
         ma.layers = s->ti->layers.p;
@@ -1426,6 +1545,7 @@ int exact_nodes(qsk_sim *s, const int *nodes, int count, bool teacher) {
         ma.rec_cnt = s->d_rec_cnt.p;
         ma.rec_max = s->d_rec_max.p;
         CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+        if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         ReplayArgs ra;
         std::memset(&ra, 0, sizeof(ra));
         ra.g = g;
@@ -1448,6 +1568,7 @@ int exact_nodes(qsk_sim *s, const int *nodes, int count, bool teacher) {
         CK(launch_hash_select(ra, s->st));
         ra.only_flagged = 1;
         CK(launch_replay(ra, s->st));
+        if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
         s->info.launches += 4;
         s->info.map_launches += 1;
         s->info.map_positions += (long long)B * g.N;
@@ -1516,6 +1637,8 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
         fa.inv_radius = 0.125f;
         fa.ntpl = s->ntpl;
         fa.entries = QSK_ENC_ENTRIES;
+        feat_stencil(s, e, fa);
+        fa.scale = step.scale;
         fa.out = s->d_feat.p;
         CK(launch_feat_nodes(fa, s->st));
         int rc = enc_forward(e, B, B, s->d_feat.p, s->st);   // query head
@@ -1584,7 +1707,9 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     a.out_pos = s->d_tc_pos.p;
     a.status = s->d_status.p;
     CK(cudaMemsetAsync(s->d_tc_thr.p, 0, sizeof(unsigned) * size_t(B), s->st));
-    CK(launch_tc_shortlist(s->tc_fmt, s->tc_W, s->d_tc_A.p, Bp, s->d_tc_P.p, s->tc_rows, s->tc_Kp, a, s->st));
+    // learned proposal: the pattern matrix of the step's stencil scale
+    const unsigned char *P = s->d_tc_P.p + (learned ? size_t(step.scale - 1) * size_t(s->tc_rows) * ENC_E * 2 : 0);
+    CK(launch_tc_shortlist(s->tc_fmt, s->tc_W, s->d_tc_A.p, Bp, P, s->tc_rows, s->tc_Kp, a, s->st));
     if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
     TcSelectArgs sa{};
     sa.g = g;
@@ -2220,14 +2345,19 @@ int qsk_sim_set_learned(qsk_sim *s, qsk_encoder *e, const qsk_learned_opts *o) {
         return fail(QSK_ERR_UNSUPPORTED, "learned proposal: complete TIs without -nV, -fs or local controls");
     if (s->ti->g.nd > 3 || s->ti->cells > (1LL << 31))
         return fail(QSK_ERR_UNSUPPORTED, "learned proposal: at most 3 dimensions and 2^31 cells");
+    // the pre-embedded TI stays while the same encoder is set again (it is
+    // rebuilt when the encoder has trained or changed its scales since)
+    const bool same = s->enc == e && s->topt.mode == 3;
     s->enc = e;
     s->lopt = *o;
     s->topt = qsk_tensor_opts{};
     s->topt.mode = 3;
     s->topt.audit = o->audit;
     s->max_tc_slots = 4096;
-    s->tc_ready = false;
-    s->enc_built = -1;
+    if (!same) {
+        s->tc_ready = false;
+        s->enc_built = -1;
+    }
     return QSK_OK;
 }
 
@@ -2282,6 +2412,10 @@ int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed,
     }
     DBuf<unsigned> dcells;
     CK(dcells.upload(cells.data(), cells.size(), s->st));
+    // both sides of a pair at the node's stencil scale
+    DBuf<int> dscale;
+    CK(dscale.ensure(size_t(std::max<long long>(n, 1))));
+    if ((rc = node_scales(s, e, s->d_level_nodes.p, n, dscale.p)) != QSK_OK) return rc;
     const Geom &g = s->ti->g;
     FeatArgs fa;
     fa.rows = n;
@@ -2299,6 +2433,8 @@ int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed,
     fa.inv_radius = 0.125f;
     fa.ntpl = s->ntpl;
     fa.entries = QSK_ENC_ENTRIES;
+    feat_stencil(s, e, fa);
+    fa.row_scale = dscale.p;
     fa.out = e->xq.p + size_t(e->npairs) * rowf;
     CK(launch_feat_nodes(fa, s->st));
     FeatArgs fc = fa;

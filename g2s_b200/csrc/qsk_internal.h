@@ -431,7 +431,20 @@ struct FeatArgs {
     float inv_radius = 1.f;           // offsets are scaled by this
     int entries = QSK_ENC_ENTRIES;    // template offsets 1..entries represented (at most 64)
     float *out = nullptr;             // rows x (64 x (nvar + 4))
+    // multi-scale stencil: at scale s, entry e sits at s x (template offset
+    // e + 1); a neighbour at offset o falls in the entry whose offset is
+    // round(o / s) (half away from zero), the values falling in one entry
+    // averaged
+    int scale = 1;                    // the rows' scale when row_scale is null
+    const int *row_scale = nullptr;   // per row scale (1..nscales)
+    const int *cube = nullptr;        // entry of every offset of the stencil's box (-1: none)
+    int cube_lo[3] = {0, 0, 0};
+    int cube_dim[3] = {1, 1, 1};
+    int nscales = 1;
+    float cov_min = 0.9f;             // k_node_scale: smallest scale covering this fraction of the neighbours
+    int *scale_out = nullptr;         // k_node_scale: the chosen scale per row
 };
+cudaError_t launch_node_scale(const FeatArgs &a, cudaStream_t st);
 cudaError_t launch_sgemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb, int tb, float *C,
                          int ldc, float alpha, float beta, const float *bias, cudaStream_t st);
 cudaError_t launch_gelu(long long n, const float *pre, float *out, cudaStream_t st);

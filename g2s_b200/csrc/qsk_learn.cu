@@ -1,16 +1,21 @@
 // Learned proposal: a small MLP encoder of neighbourhoods, its training
 // (forward, backward and Adam, FP32 on the CUDA cores) and the features it
-// reads.  The encoder embeds a node's informed neighbourhood and the
-// canonical neighbourhood of every TI cell into one 64-d space; the
-// tensor-core top-W kernel (qsk_tc.cu) then proposes, per node, the TI cells
-// whose embeddings have the largest inner product with the node's, and the
-// exact map scores that shortlist.
+// reads.  The encoder embeds a node's informed neighbourhood (query head)
+// and the neighbourhood of every TI cell (pattern head) into one 64-d space;
+// the tensor-core top-W kernel (qsk_tc.cu) then proposes, per node, the TI
+// cells whose embeddings have the largest inner product with the node's, and
+// the exact map scores that shortlist.
 //
 // Encoder: E = 64 entries x F features (F = nvar values, mask, dx, dy, dz),
 // D0 = 64 F -> 256 -> 256 -> 256 (GELU, tanh form of Hendrycks & Gimpel
-// 2016) -> 64, rows normalised to unit length.  Training pairs (query
-// neighbourhood, TI cell the exact path drew for it) use the symmetric
-// InfoNCE loss over the in-batch negatives (logits = q . p / tau).
+// 2016, shared) -> 64 (one linear head per side, not normalised).  Training
+// pairs (query neighbourhood, TI cell the exact path drew for it) use the
+// symmetric InfoNCE loss over the in-batch negatives (logits = q . p / tau).
+//
+// Entries form a stencil: the template's first 64 offsets, dilated by a
+// scale s in 1..nscales.  A node takes the smallest scale whose stencil
+// holds most of its informed neighbours (sparse neighbourhoods early on the
+// path take a coarse stencil); the TI is embedded once per scale.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -177,50 +182,94 @@ __global__ void k_adam(long long n, float *__restrict__ w, const float *__restri
     w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
 }
 
-// encoder input of nodes: entry e is template offset e + 1 (the canonical
-// neighbourhood of the TI cells' input, so that both align by offset);
-// [values, 1, dx, dy, dz] where that offset holds one of the node's
-// neighbours, [0, 0, dx, dy, dz] elsewhere (the centre and neighbours
-// beyond offset 64 are not represented; the exact map still uses them)
+// entry of the stencil a neighbour at template offset tp falls in at scale s
+// (-1: outside it; the centre is no entry)
+__device__ __forceinline__ int stencil_entry(const FeatArgs &A, const int *tp, int s) {
+    int idx = 0, st = 1;
+    for (int d = 0; d < A.nd; ++d) {
+        const int o = tp[d];
+        const int a = o < 0 ? -o : o;
+        int q = (2 * a + s) / (2 * s);
+        if (o < 0) q = -q;
+        const int c = q - A.cube_lo[d];
+        if (c < 0 || c >= A.cube_dim[d]) return -1;
+        idx += c * st;
+        st *= A.cube_dim[d];
+    }
+    return A.cube[idx];
+}
+
+// encoder input of nodes: entry e of the row's stencil holds
+// [mean of the values of the neighbours falling in it, 1, dx, dy, dz], or
+// [0, 0, dx, dy, dz] when none does (the centre and neighbours beyond the
+// stencil are not represented; the exact map still uses them); dx, dy, dz
+// is the entry's offset (scale included) times inv_radius
 __global__ void k_feat_nodes(FeatArgs A) {
     const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
-    if (r >= A.rows) return;
+    if (r >= A.rows) return;   // r is the same for the whole warp
     const int i = A.nodes[r];
     const unsigned cell = A.path[A.begin + i];
     const int cnt = A.nb_count[i];
     const int F = A.nvar + 4;
     const int E = min(A.entries, QSK_ENC_ENTRIES);
+    const int s = A.row_scale ? A.row_scale[r] : A.scale;
     float *out = A.out + (long long)r * QSK_ENC_ENTRIES * F;
     for (int e = lane; e < QSK_ENC_ENTRIES; e += 32) {
         float *o = out + e * F;
         for (int v = 0; v <= A.nvar; ++v) o[v] = 0.f;
         const int t = e + 1;
         for (int d = 0; d < 3; ++d)
-            o[A.nvar + 1 + d] = (d < A.nd && t < A.ntpl && e < E) ? float(A.tpl[t * A.nd + d]) * A.inv_radius : 0.f;
+            o[A.nvar + 1 + d] =
+                (d < A.nd && t < A.ntpl && e < E) ? float(s * A.tpl[t * A.nd + d]) * A.inv_radius : 0.f;
     }
-    __syncwarp();
-    for (int j = lane; j < cnt; j += 32) {
-        const int t = A.nb_tpl[(long long)i * A.n + j];
-        const unsigned nc = A.nb_cell[(long long)i * A.n + j];
-        if (t < 1 || t > E || nc == cell) continue;
-        float *o = out + (t - 1) * F;
-        for (int v = 0; v < A.nvar; ++v) {
-            const float x = A.state[(long long)nc * A.nvar + v];
-            o[v] = isnan(x) ? 0.f : x;
+    // neighbours in their order; the lane owning an entry (e mod 32) adds
+    // them up, so every entry's sum has a fixed order
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+        const int j = j0 + lane;
+        int ent = -1;
+        unsigned nc = 0;
+        if (j < cnt) {
+            const int t = A.nb_tpl[(long long)i * A.n + j];
+            nc = A.nb_cell[(long long)i * A.n + j];
+            if (t >= 1 && t < A.ntpl && nc != cell) {
+                ent = stencil_entry(A, A.tpl + t * A.nd, s);
+                if (ent >= E) ent = -1;
+            }
         }
-        o[A.nvar] = 1.f;
+        const int m = min(32, cnt - j0);
+        for (int jj = 0; jj < m; ++jj) {
+            const int e = __shfl_sync(0xffffffffu, ent, jj);
+            const unsigned c = __shfl_sync(0xffffffffu, nc, jj);
+            if (e >= 0 && (e & 31) == lane) {
+                float *o = out + e * F;
+                for (int v = 0; v < A.nvar; ++v) {
+                    const float x = A.state[(long long)c * A.nvar + v];
+                    o[v] += isnan(x) ? 0.f : x;
+                }
+                o[A.nvar] += 1.f;
+            }
+        }
+    }
+    for (int e = lane; e < QSK_ENC_ENTRIES; e += 32) {
+        float *o = out + e * F;
+        const float c = o[A.nvar];
+        if (c > 1.f)
+            for (int v = 0; v < A.nvar; ++v) o[v] = o[v] / c;
+        o[A.nvar] = c > 0.f ? 1.f : 0.f;
     }
 }
 
-// encoder input of TI cells: template offsets 1..entries around the cell (the
-// neighbours a node with a complete neighbourhood has, centre excluded)
+// encoder input of TI cells: the stencil's entries around the cell at the
+// row's scale (the neighbours a node with a complete neighbourhood has,
+// centre excluded)
 __global__ void k_feat_cells(FeatArgs A) {
     const long long r = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     const int lane = threadIdx.x & 31;
     if (r >= A.rows) return;
     const long long p = A.cell_list ? (long long)A.cell_list[r] : A.cell0 + r;
     const int F = A.nvar + 4;
+    const int s = A.row_scale ? A.row_scale[r] : A.scale;
     int pc[3] = {0, 0, 0};
     long long rem = p;
     for (int d = 0; d < A.nd; ++d) {
@@ -234,7 +283,7 @@ __global__ void k_feat_cells(FeatArgs A) {
         long long q = 0, st = 1;
         bool in = p < A.cells && t < A.ntpl && e < A.entries;
         for (int d = 0; d < A.nd; ++d) {
-            const int off = t < A.ntpl ? A.tpl[t * A.nd + d] : 0;
+            const int off = t < A.ntpl ? s * A.tpl[t * A.nd + d] : 0;
             const int c = pc[d] + off;
             in &= c >= 0 && c < A.src[d];
             q += (long long)c * st;
@@ -246,8 +295,47 @@ __global__ void k_feat_cells(FeatArgs A) {
         }
         o[A.nvar] = in ? 1.f : 0.f;
         for (int d = 0; d < 3; ++d)
-            o[A.nvar + 1 + d] = (d < A.nd && t < A.ntpl && e < A.entries) ? float(A.tpl[t * A.nd + d]) * A.inv_radius : 0.f;
+            o[A.nvar + 1 + d] =
+                (d < A.nd && t < A.ntpl && e < A.entries) ? float(s * A.tpl[t * A.nd + d]) * A.inv_radius : 0.f;
     }
+}
+
+// the scale of each node's stencil: the smallest scale whose entries hold at
+// least cov_min of its neighbours, else the one holding the most
+__global__ void k_node_scale(FeatArgs A) {
+    const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (r >= A.rows) return;   // r is the same for the whole warp
+    const int i = A.nodes[r];
+    const unsigned cell = A.path[A.begin + i];
+    const int cnt = A.nb_count[i];
+    const int E = min(A.entries, QSK_ENC_ENTRIES);
+    int best = 1, bestc = -1;
+    for (int s = 1; s <= A.nscales; ++s) {
+        int c = 0;
+        for (int j0 = 0; j0 < cnt; j0 += 32) {
+            const int j = j0 + lane;
+            bool in = false;
+            if (j < cnt) {
+                const int t = A.nb_tpl[(long long)i * A.n + j];
+                const unsigned nc = A.nb_cell[(long long)i * A.n + j];
+                if (t >= 1 && t < A.ntpl && nc != cell) {
+                    const int e = stencil_entry(A, A.tpl + t * A.nd, s);
+                    in = e >= 0 && e < E;
+                }
+            }
+            c += __popc(__ballot_sync(0xffffffffu, in));
+        }
+        if (float(c) >= A.cov_min * float(cnt)) {
+            best = s;
+            break;
+        }
+        if (c > bestc) {
+            best = s;
+            bestc = c;
+        }
+    }
+    if (lane == 0) A.scale_out[r] = best;
 }
 
 __global__ void k_to_bf16(long long n, const float *__restrict__ x, uint16_t *__restrict__ y) {
@@ -319,6 +407,12 @@ cudaError_t launch_feat_nodes(const FeatArgs &a, cudaStream_t st) {
 cudaError_t launch_feat_cells(const FeatArgs &a, cudaStream_t st) {
     if (a.rows <= 0) return cudaSuccess;
     k_feat_cells<<<blocks_for(a.rows * 32, 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_node_scale(const FeatArgs &a, cudaStream_t st) {
+    if (a.rows <= 0) return cudaSuccess;
+    if (!a.cube || !a.scale_out || a.nscales < 1) return cudaErrorInvalidValue;
+    k_node_scale<<<blocks_for(a.rows * 32, 256), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 cudaError_t launch_gather_rows(int n, int cols, const int *idx, const float *src, float *dst, cudaStream_t st) {

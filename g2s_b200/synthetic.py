@@ -104,12 +104,19 @@ def tubes3d(shape=(256, 256, 256), seed: int = 1, target: float = 0.20) -> np.nd
     zz = np.arange(nz, dtype=np.float64)[:, None, None]
 
     def render(scale):
+        # each tube is rendered only over the (z, y) window its centre line
+        # and radius can reach (outside it d2 >= r^2 everywhere)
         img = np.zeros(shape, dtype=bool)
         for i in range(n):
+            r = rad[i] * scale
             cy = ay[i] * np.sin(2 * np.pi * x / lam[i] + phi[i]) + y0[i]
             cz = az[i] * np.cos(2 * np.pi * x / lam[i] + phi[i]) + z0[i]
-            d2 = (yy[None, :, :] - cy[None, None, :]) ** 2 + (zz - cz[None, None, :]) ** 2
-            img |= d2 < (rad[i] * scale) ** 2
+            ya, yb = max(0, int(np.floor(cy.min() - r))), min(ny, int(np.ceil(cy.max() + r)) + 1)
+            za, zb = max(0, int(np.floor(cz.min() - r))), min(nz, int(np.ceil(cz.max() + r)) + 1)
+            if ya >= yb or za >= zb:
+                continue
+            d2 = (yy[None, ya:yb, :] - cy[None, None, :]) ** 2 + (zz[za:zb] - cz[None, None, :]) ** 2
+            img[za:zb, ya:yb, :] |= d2 < r ** 2
         return img
 
     lo, hi, mid = 0.05, 6.0, 1.0

@@ -448,6 +448,13 @@ int qsk_encoder_create(int device, int nvar, unsigned seed, qsk_encoder **out);
 int qsk_encoder_destroy(qsk_encoder *e);
 long long qsk_encoder_param_count(const qsk_encoder *e);
 int qsk_encoder_input_dim(const qsk_encoder *e);
+/* Stencil scales of the inputs (default 4 and 0.9): an input's 64 entries
+ * are the template's first 64 offsets dilated by a scale in 1..nscales; a
+ * node takes the smallest scale whose stencil holds cov_min of its informed
+ * neighbours (values falling in one entry averaged), and the TI is embedded
+ * once per scale.  Applies to pairs added and pattern matrices built
+ * afterwards. */
+int qsk_encoder_set_scales(qsk_encoder *e, int nscales, float cov_min);
 /* All parameters, flattened: W1 (256 x D0), b1, W2 (256 x 256), b2, W3, b3,
  * W4q (64 x 256), b4q (query head), W4p, b4p (TI-pattern head); weights
  * row-major (out x in).  set resets Adam. */
@@ -470,6 +477,8 @@ int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed,
 /* Training pairs from host arrays (n x D0 each): queries and their positives. */
 int qsk_encoder_add_pairs_host(qsk_encoder *e, long long n, const float *xq, const float *xp);
 int qsk_encoder_pairs(const qsk_encoder *e, long long *count);
+/* Stored pairs [first, first + n) to host arrays (n x D0 each). */
+int qsk_encoder_get_pairs(const qsk_encoder *e, long long first, long long n, float *xq, float *xp);
 int qsk_encoder_clear_pairs(qsk_encoder *e);
 /* Adam (lr, betas 0.9 / 0.999) on the stored pairs, shuffled every epoch by
  * mt19937(seed), minibatches of `batch`; *last_loss: the last batch's loss. */

@@ -105,3 +105,27 @@ def test_learned_simulation_regret_and_what_training_gains(g2s, gpu):
     assert conf > 0.2 * info["tensor_nodes"] and conf > 10 * max(conf0, 1)
     enc.close()
     raw.close()
+
+
+def test_query_and_pattern_features_align(g2s, gpu):
+    """The TI is the completed grid itself, so every node has a TI cell of
+    mismatch 0 (its own) and the exact path (k = 1) draws a cell of mismatch
+    0.  At stencil scale 1 the node's entries must then equal that cell's
+    entries wherever the node has a neighbour: the node and TI-cell feature
+    kernels read the same offsets, values and layout."""
+    done = bivariate_ti((48, 48), 3)
+    di = np.full(done.shape, np.nan, np.float32)
+    enc = g2s.Encoder(nvar=2, seed=1).set_scales(1)
+    sim = g2s.Simulation(done.copy(), di, [0, 1], n=16, k=1.0, seed=4)
+    added = enc.add_pairs(sim, done, np.arange(48 * 48, dtype=np.int32))
+    sim.close()
+    q, p = enc.get_pairs()
+    assert len(q) == added > 0.99 * 48 * 48
+    q = q.reshape(len(q), 64, 6)
+    p = p.reshape(len(p), 64, 6)
+    mask = q[:, :, 2] > 0
+    assert mask.sum() > 10 * len(q)
+    assert np.all(p[:, :, 2][mask] == 1.0)
+    assert np.array_equal(q[:, :, :2][mask], p[:, :, :2][mask])
+    assert np.array_equal(q[:, :, 3:], p[:, :, 3:])   # entry offsets
+    enc.close()
