@@ -2,7 +2,7 @@
 plain FP32 path, at the k-best regret the audit measures.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload config1|config0|config3|config4]
+                    [--workload config1|config0|config2|config3|config4]
                     [--path bf16|fp8|learned|plain|fp32]
 
 Workloads (seeded synthetic inputs; no public dataset is involved):
@@ -21,6 +21,15 @@ Workloads (seeded synthetic inputs; no public dataset is involved):
                      completed 200x200x100 GRF grid (seed 2): the whole
                      simulation is too long to repeat K times on the plain
                      path.  Default path: FP8 E4M3.
+  config2            64 jobs in one call (qsk_jobs_run: each job on its own
+                     streams, 16 host threads feeding them) over 3 TIs
+                     (continuous GRF 512^2, range 20 px; binary channels
+                     500^2; GRF 512^2 plus its indicator at the 0.7
+                     quantile), grids log-uniform from 128^2 to 1024^2
+                     (16.2 M nodes), n from {20, 40, 60, 100}, k=1.2; the
+                     tensor-core form autotuned per (TI, n) shape (untimed,
+                     reported) against the plain path.  A step is all 64
+                     whole simulations.
   config4            bivariate 3-D TI 256^3 (continuous GRF, ranges 24,24,8
                      voxels, plus a sinusoid-tube indicator, ~20 % facies 1),
                      simulation 256^3, n=64, k=1.5; a step is the
@@ -82,6 +91,8 @@ WORKLOADS = {
                     name="config0-continuous-grf-200x200-to-200x200-n50-k1.2"),
     "config3": dict(ti=("grf", (120, 150, 180), (5, 20, 20)), di=(100, 200, 200), types=[0], n=60, k=1.2, path="fp8",
                     sample=250, name="config3-continuous-grf3d-180x150x120-to-200x200x100-n60-k1.2-sample16000"),
+    "config2": dict(jobs=64, path="bf16", k=1.2, ns=(20, 40, 60, 100), sides=(128, 1024), ref_grid=(24, 24),
+                    name="config2-batched-64-jobs-3-TIs-grids-128^2-1024^2-n20-100-k1.2"),
     "config4": dict(ti=("bivariate3d", (256, 256, 256), (8, 24, 24)), di=(256, 256, 256), types=[0, 1], n=64, k=1.5,
                     path="learned", sample=4096, ref_grid=(2, 4, 4),
                     train=dict(pairs=2_000_000, size=96, per_ti=300_000, epochs=20, batch=1024),
@@ -287,11 +298,15 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libg2sref.so not built (needs the G2S sources)"}))
         return 0
     w = WORKLOADS[args.workload]
-    vals, cores, sample = reference_measure(args, w, args.steps)
-    v = float(np.mean(vals))
+    if w.get("jobs"):
+        v, cores, sample = jobs_reference(w, config2_jobs(w))
+    else:
+        vals, cores, sample = reference_measure(args, w, args.steps)
+        v = float(np.mean(vals))
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": float(1000.0 * np.prod(w["di"]) / v) if not w.get("sample") else None,
+        "warmup": args.warmup,
+        "ms_per_step": float(1000.0 * np.prod(w["di"]) / v) if not (w.get("sample") or w.get("jobs")) else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": w["name"], "threads": cores},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
@@ -334,6 +349,163 @@ def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flus
     return total, infos, pinf
 
 
+def config2_jobs(w):
+    """The 64 jobs: TI j mod 3 (continuous GRF 512^2, range 20 px; binary
+    channels 500^2, 40 channels, ~25-30 % facies 1; the GRF 512^2 of another
+    seed with its indicator at the 0.7 quantile), n = ns[j mod 4], grid side
+    128 * 8^r with r = ((37 j) mod 64) / 63 (log-uniform from 128 to 1024),
+    seed 100 + j."""
+    from g2s_b200 import synthetic as syn
+    tis = [("grf512", syn.grf((512, 512), (20, 20), seed=21), [0]),
+           ("channels500", syn.channels2d((500, 500), n_channels=40, seed=22), [1]),
+           ("bivariate512", syn.bivariate(syn.grf((512, 512), (20, 20), seed=23)), [0, 1])]
+    jobs = []
+    J = w["jobs"]
+    lo, hi = w["sides"]
+    for j in range(J):
+        r = ((37 * j) % J) / max(1, J - 1)
+        side = int(round(lo * (hi / lo) ** r))
+        name, ti, types = tis[j % 3]
+        jobs.append(dict(ti_name=name, ti=ti, types=types, n=w["ns"][j % 4], k=w["k"], seed=SEED + j,
+                         shape=(side, side) + ((2,) if len(types) > 1 else ())))
+    return jobs
+
+
+def jobs_reference(w, jobs):
+    """G2S reference CPU QS on the first job of each TI type, on a small grid
+    (its TI, n, k): (harmonic mean of the rates, cores, description)."""
+    from oracle import ref
+    cores = os.cpu_count() or 1
+    rates, done = [], set()
+    g = w["ref_grid"]
+    for j in jobs:
+        if j["ti_name"] in done:
+            continue
+        done.add(j["ti_name"])
+        di = np.full(tuple(g) + j["shape"][2:], np.nan, np.float32)
+        qsargs = ["-k", str(j["k"]), "-n", str(j["n"]), "-s", str(j["seed"]), "-j", str(cores)]
+        _, _, rms, _ = ref.run_qs(j["ti"], di, j["types"], qsargs, job_id=9200 + len(done))
+        rates.append(int(np.prod(g)) / (rms / 1000.0))
+    v = float(len(rates) / sum(1.0 / r for r in rates))
+    return v, cores, (f"G2S qs, the first job of each TI type on a {g[0]}x{g[1]} grid (its TI, n, k), -j {cores}, "
+                      f"harmonic mean of the rates; {fft_in_use()}")
+
+
+def jobs_main(args, w, g2s, dev):
+    """Config 2: all jobs in one qsk_jobs_run call per step (each job on its
+    own streams, host threads feeding them), the tensor-core form with
+    settings autotuned per (TI, n) shape, against the plain path."""
+    import torch
+    from g2s_b200 import autotune as at
+    path = args.path or w["path"]
+    jobs = config2_jobs(w)
+    nodes = int(sum(int(np.prod(j["shape"][:2])) for j in jobs))
+    log(f"{len(jobs)} jobs, {nodes} nodes")
+    tuned, t0 = {}, time.perf_counter()
+    if path in ("bf16", "fp8"):
+        cache = os.path.join(tempfile.gettempdir(), f"g2s_b200_tune_{os.getpid()}.json")
+        for j in jobs:
+            key = (j["ti_name"], j["n"])
+            if key not in tuned:
+                tuned[key] = at.tune(j["ti"], j["types"], j["n"], j["k"], mode=path, device=dev, cache=cache)
+                log(f"tuned {key}: {tuned[key]}")
+    tune_s = time.perf_counter() - t0
+
+    def make(p, audit=0.01):
+        sims = []
+        for j in jobs:
+            sim = g2s.Simulation(j["ti"], np.full(j["shape"], np.nan, np.float32), j["types"], n=j["n"], k=j["k"],
+                                 seed=j["seed"], device=dev)
+            if p in ("bf16", "fp8"):
+                at.apply(sim, tuned[(j["ti_name"], j["n"])], mode=p, audit=audit)
+            sims.append(sim)
+        return sims
+
+    def timed(sims):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        g2s.run_jobs(sims, threads=16)
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    with ClockSampler(dev) as clk:
+        sims = make(path)
+        for _ in range(max(args.warmup, 0)):
+            timed(sims)
+        ms = [timed(sims) for _ in range(args.steps)]
+        infos = [s.info() for s in sims]
+        for s in sims:
+            s.close()
+    clocks = clk.summary()
+    total_ms = float(sum(ms))
+    value = nodes * args.steps / (total_ms / 1000.0)
+    log(f"{path}: {ms} ms per step")
+    compare = {}
+    if not args.no_compare and path != "plain":
+        sims = make("plain")
+        pm = timed(sims)
+        compare["plain"] = {"value": nodes / (pm / 1000.0), "ms_per_step": pm,
+                            "kernel": "k_map_bits / k_map_records + k_replay (exact reservoir k-best)"}
+        for s in sims:
+            s.close()
+        log(f"plain: {pm:.0f} ms")
+    e2e_vals = []
+    for _ in range(0 if args.no_e2e else 1):
+        t1 = time.perf_counter()
+        sims = make(path)
+        g2s.run_jobs(sims, threads=16)
+        for s in sims:
+            s.read()
+            s.close()
+        e2e_vals.append(time.perf_counter() - t1)
+        log(f"e2e: {e2e_vals[-1]:.2f} s")
+    h2d = int(sum(j["ti"].nbytes + int(np.prod(j["shape"])) * 4 for j in jobs))
+    d2h = int(sum(int(np.prod(j["shape"])) * 4 + int(np.prod(j["shape"][:2])) * 8 for j in jobs))
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            v, cores, samp = jobs_reference(w, jobs)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": samp}
+            log(f"cpu baseline: {cpu}")
+    plain_v = compare.get("plain", {}).get("value")
+    tensor = path in ("bf16", "fp8")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"bf16": "bf16", "fp8": "fp8-e4m3", "plain": "mixed (u8 bit-sliced / f32)"}[path],
+        "data": "synthetic",
+        "config": {"workload": w["name"], "path": path, "jobs": len(jobs), "nodes_per_step": nodes,
+                   "one_call": "qsk_jobs_run over all jobs (16 host threads, each job on its own streams)",
+                   "tuned": {f"{a}|n={b}": {k2: v[k2] for k2 in ("width", "prefix", "batch", "ms", "runs", "ok")}
+                             for (a, b), v in tuned.items()},
+                   "tuning_s": tune_s, "l2": "inputs and working set larger than L2 (16 M nodes per step)",
+                   "parallelism": "jobs x64 on one GPU"},
+        "vs_plain": {"plain": compare.get("plain"), "speedup_vs_plain": value / plain_v if plain_v else None},
+        "regret": {"audited": int(sum(i["audited"] for i in infos)), "regret": int(sum(i["regret"] for i in infos)),
+                   "near_tie": int(sum(i["regret_near"] for i in infos)),
+                   "rate": sum(i["regret"] for i in infos) / max(1, sum(i["audited"] for i in infos)),
+                   "definition": "audited nodes (1 % per job) whose drawn candidate scores below the exact k-th best"}
+        if tensor else {"regret": 0, "definition": "exact reference path: regret 0 by construction"},
+        "map_error_vs_fp64": {"max": max(i["map_err_max"] for i in infos),
+                              "mean": float(np.mean([i["map_err_mean"] for i in infos]))} if tensor else None,
+        "roofline": None,
+        "roofline_note": "jobs of different shapes overlap on separate streams; the kernel rooflines are the "
+                         "single-job workloads' (config1, config3)",
+        "breakdown_ms_summed_over_jobs": {"total": float(sum(i["ms_total"] for i in infos)),
+                                          "tensor_pattern_build_once": float(sum(i["ms_tensor_pattern"] for i in infos))},
+        "cpu_baseline": cpu,
+        "e2e": {"value": nodes / float(np.mean(e2e_vals)) if e2e_vals else None, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(sum(i["launches"] for i in infos)) * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,6 +528,11 @@ def main():
     path = args.path or w["path"]
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    if w.get("jobs"):
+        if ws > 1:
+            print(json.dumps({"unavailable": "the batched-jobs workload runs on one GPU"}))
+            return 0
+        return jobs_main(args, w, g2s, local)
     dist = None
     if ws > 1:
         import torch.distributed as dist

@@ -70,7 +70,8 @@ class QskSimInfo(ctypes.Structure):
                 ("tensor_flops", ctypes.c_double), ("ms_tensor_gemm", ctypes.c_float),
                 ("ms_tensor_select", ctypes.c_float), ("ms_tensor_pattern", ctypes.c_float),
                 ("tensor_launches", ctypes.c_longlong), ("path_nodes", ctypes.c_longlong),
-                ("learned_fallback", ctypes.c_longlong)]
+                ("learned_fallback", ctypes.c_longlong), ("graph_nodes", ctypes.c_longlong),
+                ("ms_graph_build", ctypes.c_float)]
 
 
 class QskLearnedOpts(ctypes.Structure):
@@ -80,7 +81,7 @@ class QskLearnedOpts(ctypes.Structure):
 
 class QskTensorOpts(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("prefix", ctypes.c_int), ("width", ctypes.c_int),
-                ("shortlist", ctypes.c_int), ("audit", ctypes.c_float)]
+                ("shortlist", ctypes.c_int), ("audit", ctypes.c_float), ("batch", ctypes.c_int)]
 
 
 # name -> (restype, argtypes): every entry point of include/g2s_b200.h
@@ -145,6 +146,8 @@ SIGNATURES = {
     "qsk_sim_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_sim_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "qsk_sim_set_level_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_longlong]),
+    "qsk_sim_set_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "qsk_jobs_run": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, _i32p]),
     "qsk_sim_set_tensor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskTensorOpts)]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
@@ -425,11 +428,11 @@ class Simulation:
         return self
 
     def set_tensor(self, mode: str = "bf16", prefix: int = 0, width: int = 0, shortlist: int = 0,
-                   audit: float = 0.0):
+                   audit: float = 0.0, batch: int = 0):
         """Tensor-core form of the map: mode "plain" (the exact reference path),
         "bf16" or "fp8"; zero fields take the automatic choice."""
         m = {"plain": 0, "bf16": 1, "fp8": 2}[mode]
-        o = QskTensorOpts(m, int(prefix), int(width), int(shortlist), float(audit))
+        o = QskTensorOpts(m, int(prefix), int(width), int(shortlist), float(audit), int(batch))
         _check(lib().qsk_sim_set_tensor(self.handle, ctypes.byref(o)), "qsk_sim_set_tensor")
         return self
 
@@ -447,6 +450,11 @@ class Simulation:
         """Bound of the dependency-level waits (polls; 0 = default) and, for
         failure-path tests, a path node whose level is never published."""
         _check(lib().qsk_sim_set_level_wait(self.handle, int(spin_limit), int(hold_node)), "qsk_sim_set_level_wait")
+        return self
+
+    def set_graph(self, on: bool = True):
+        """Graph mode of the plain path (qsk_sim_set_graph)."""
+        _check(lib().qsk_sim_set_graph(self.handle, int(bool(on))), "qsk_sim_set_graph")
         return self
 
     def run_teacher(self, completed: np.ndarray, index: Optional[np.ndarray] = None):
@@ -594,6 +602,18 @@ class Encoder:
             self.close()
         except Exception:
             pass
+
+
+def run_jobs(sims: Sequence["Simulation"], threads: int = 0) -> np.ndarray:
+    """Run several distinct simulations in one call (qsk_jobs_run); returns
+    each job's status (all 0 on success; the first error raises)."""
+    n = len(sims)
+    if len({id(s) for s in sims}) != n:
+        raise ValueError("run_jobs: every simulation must be distinct")
+    arr = (ctypes.c_void_p * max(n, 1))(*[s.handle for s in sims])
+    status = np.zeros(max(n, 1), np.int32)
+    _check(lib().qsk_jobs_run(arr, n, int(threads), _p(status, _i32p)), "qsk_jobs_run")
+    return status[:n]
 
 
 def measure_peaks(device: int = 0) -> dict:

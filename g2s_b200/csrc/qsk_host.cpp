@@ -5,6 +5,7 @@
 // 1604-1641) with the same libstdc++ algorithms, so paths and seeds are
 // identical for a given -s.  Everything per node runs on the GPU.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -709,6 +710,7 @@ struct qsk_sim {
     qsk_sim_info info;
     bool neighbours_ready = false;
     bool profiling = false;
+    bool use_graph = false;             // plain path: the batch chain as one CUDA graph
     // tensor-core form (qsk_sim_set_tensor)
     qsk_tensor_opts topt{};             // mode 0: off
     int tc_T = 0, tc_L = 0, tc_W = 0, tc_S = 0, tc_fmt = 0;
@@ -1232,7 +1234,7 @@ int tc_configure_learned(qsk_sim *s) {
     int rc = stencil_cube(s);
     if (rc) return rc;
     const size_t per_scale = size_t(rows) * ENC_E * 2;
-    CK(s->d_tc_P.alloc(per_scale * size_t(e->nscales)));
+    CK(s->d_tc_P.ensure(per_scale * size_t(e->nscales)));
     CK(cudaMemsetAsync(s->d_tc_P.p, 0, per_scale * size_t(e->nscales), s->st));
     const long long chunk = 131072;
     CK(s->d_feat.ensure(size_t(chunk) * size_t(e->D0)));
@@ -1319,8 +1321,10 @@ int tc_configure(qsk_sim *s, int T_auto) {
     s->tc_rows = rows;
     if (same) return QSK_OK;
     s->tc_ready = false;
-    CK(s->d_tc_P.alloc(size_t(rows * Kp * elem)));
-    CK(s->d_tc_pscale.alloc(size_t(rows / 256)));
+    // every element is written by the pattern kernel: a large enough buffer
+    // (a job runner's scratch included) is reused as it is
+    CK(s->d_tc_P.ensure(size_t(rows * Kp * elem)));
+    CK(s->d_tc_pscale.ensure(size_t(rows / 256)));
     DBuf<float> rowmax;
     if (fmt == 1) CK(rowmax.alloc(size_t(rows)));
     TcPatternArgs pa{};
@@ -1866,6 +1870,32 @@ int tc_run(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     return QSK_OK;
 }
 
+// the batch chain of a plain run captured into one CUDA graph (both
+// streams: the generator pipeline joins through its events), instantiated
+// and launched on s->st; the graph is released once the run has finished
+int sim_batches_graph(qsk_sim *s, const std::vector<Step> &steps, cudaGraphExec_t *exec_out) {
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    int rc = sim_batches(s, steps, false);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->st, &graph);
+    if (rc != QSK_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(QSK_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    size_t nn = 0;
+    cudaError_t e2 = cudaGraphGetNodes(graph, nullptr, &nn);
+    if (e2 == cudaSuccess) e2 = cudaGraphInstantiate(exec_out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) return fail(QSK_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e2));
+    s->info.graph_nodes = (long long)nn;
+    s->info.ms_graph_build =
+        float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    CK(cudaGraphLaunch(*exec_out, s->st));
+    return QSK_OK;
+}
+
 void collect_profile(qsk_sim *s) {
     if (!s->profiling || (s->prof_used == 0 && s->tc_ev_used == 0)) return;
     if (s->prof_used) cudaEventSynchronize(s->prof_ev[s->prof_used - 1]);
@@ -2126,6 +2156,8 @@ int qsk_sim_run(qsk_sim *s) {
     s->info.map_launches = 0;
     s->info.map_positions = 0;
     s->info.tensor_launches = 0;
+    s->info.graph_nodes = 0;
+    s->info.ms_graph_build = 0.f;
     CK(cudaEventRecord(ev[0], s->st));
     s->neighbours_ready = false;
     int rc = sim_neighbours(s);
@@ -2167,16 +2199,21 @@ int qsk_sim_run(qsk_sim *s) {
     int mb = 0;
     for (int l = 0; l < nl; ++l) mb = std::max(mb, start[l + 1] - start[l]);
     CK(cudaEventRecord(ev[2], s->st));
+    cudaGraphExec_t gexec = nullptr;
     if (s->topt.mode != 0) {
         rc = tc_run(s, start, false);
     } else {
         rc = sim_records(s, mb);
         if (rc) return rc;
-        rc = sim_batches(s, plain_steps(s, start), false);
+        if (s->use_graph && !s->profiling)
+            rc = sim_batches_graph(s, plain_steps(s, start), &gexec);
+        else
+            rc = sim_batches(s, plain_steps(s, start), false);
     }
     if (rc) return rc;
     CK(cudaEventRecord(ev[3], s->st));
     CK(cudaEventSynchronize(ev[3]));
+    if (gexec) cudaGraphExecDestroy(gexec);
     s->info.levels = nl;
     s->info.max_batch = mb;
     cudaEventElapsedTime(&s->info.ms_setup_neighbours, ev[0], ev[1]);
@@ -2309,6 +2346,8 @@ int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
     if (o->width != 0 && !tc_supported_width(o->width)) return fail(QSK_ERR_ARG, "width %d (8, 16 or 32)", o->width);
     if (o->shortlist < 0 || o->shortlist > 128) return fail(QSK_ERR_ARG, "shortlist %d (at most 128)", o->shortlist);
     if (o->prefix < 0) return fail(QSK_ERR_ARG, "prefix %d", o->prefix);
+    if (o->batch < 0 || o->batch > 16384 || o->batch % 128)
+        return fail(QSK_ERR_ARG, "batch %d (a multiple of 128 up to 16384)", o->batch);
     if (o->mode != 0) {
         if (s->ti->missing) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: training image with missing values");
         if (s->no_verbatim || s->full || s->local)
@@ -2318,7 +2357,7 @@ int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
         if (s->ti->cells > (1LL << 31)) return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: TI of %lld cells", s->ti->cells);
     }
     s->topt = *o;
-    s->max_tc_slots = 4096;
+    s->max_tc_slots = o->batch > 0 ? o->batch : 4096;
     if (o->mode == 0) {
         s->info.tensor_mode = 0;
         s->info.tensor_nodes = s->info.plain_nodes = s->info.audited = s->info.regret = s->info.regret_near = 0;
@@ -2450,6 +2489,92 @@ int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed,
     e->npairs += n;
     if (added) *added = n;
     return QSK_OK;
+}
+
+int qsk_sim_set_graph(qsk_sim *s, int on) {
+    if (!s) return fail(QSK_ERR_ARG, "null sim");
+    s->use_graph = on != 0;
+    return QSK_OK;
+}
+
+int qsk_jobs_run(qsk_sim *const *sims, int count, int threads, int *status) {
+    if (count < 0 || (count > 0 && !sims)) return fail(QSK_ERR_ARG, "jobs: %d simulations", count);
+    for (int i = 0; i < count; ++i) {
+        if (!sims[i]) return fail(QSK_ERR_ARG, "job %d: null simulation", i);
+        for (int j = 0; j < i; ++j)
+            if (sims[j] == sims[i]) return fail(QSK_ERR_ARG, "jobs %d and %d are the same simulation", j, i);
+    }
+    if (count == 0) return QSK_OK;
+    const int T = std::max(1, std::min(threads > 0 ? threads : 16, count));
+    // largest jobs first (a long job started last would end the call late)
+    std::vector<int> order((size_t)count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sims[a]->nodes > sims[b]->nodes; });
+    std::atomic<int> next{0};
+    std::vector<int> rc((size_t)count, QSK_OK);
+    std::vector<std::string> msg((size_t)count);
+    // each thread lends its own batch scratch (map records, pattern matrix)
+    // to the job it runs, so that the memory held is that of the jobs in
+    // flight and buffers are not freed and reallocated between jobs; a
+    // simulation's own buffers are left as they were
+    struct Scratch {
+        DBuf<float> rv, rm;
+        DBuf<int> ri, rc;
+        DBuf<unsigned char> P;
+        DBuf<float> pscale;
+    };
+    auto swap_scratch = [](qsk_sim *s, Scratch &x) {
+        auto sw = [](auto &a, auto &b) {
+            std::swap(a.p, b.p);
+            std::swap(a.n, b.n);
+        };
+        sw(s->d_rec_val, x.rv);
+        sw(s->d_rec_idx, x.ri);
+        sw(s->d_rec_cnt, x.rc);
+        sw(s->d_rec_max, x.rm);
+        sw(s->d_tc_P, x.P);
+        sw(s->d_tc_pscale, x.pscale);
+        s->tc_ready = false;   // the pattern matrix now in s (if any) is not its own
+    };
+    auto worker = [&]() {
+        std::vector<std::pair<int, Scratch *>> mine;   // per device
+        for (int q = next.fetch_add(1); q < count; q = next.fetch_add(1)) {
+            const int i = order[size_t(q)];
+            qsk_sim *s = sims[i];
+            Scratch *x = nullptr;
+            for (auto &m : mine)
+                if (m.first == s->device) x = m.second;
+            if (!x) {
+                x = new Scratch();
+                mine.emplace_back(s->device, x);
+            }
+            {
+                DeviceGuard dg(s->device);
+                swap_scratch(s, *x);
+                rc[size_t(i)] = qsk_sim_run(s);
+                cudaStreamSynchronize(s->st);   // nothing of the run still reads the scratch
+                swap_scratch(s, *x);
+            }
+            if (rc[size_t(i)] != QSK_OK) msg[size_t(i)] = g_err;
+        }
+        for (auto &m : mine) {
+            DeviceGuard dg(m.first);
+            delete m.second;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < T; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto &th : pool) th.join();
+    int first = QSK_OK;
+    for (int i = 0; i < count; ++i) {
+        if (status) status[i] = rc[size_t(i)];
+        if (first == QSK_OK && rc[size_t(i)] != QSK_OK) {
+            first = rc[size_t(i)];
+            g_err = "job " + std::to_string(i) + ": " + msg[size_t(i)];
+        }
+    }
+    return first;
 }
 
 int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node) {

@@ -20,6 +20,8 @@
 // k_level_count / k_level_scatter (dependency levels of the path DAG, nodes
 // grouped by level).
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <math_constants.h>
 #include <cstdint>
 
@@ -2890,7 +2892,7 @@ cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
     // take teams of four, 8 CTAs per SM, so that they still run in one wave
     // up to 1184 slots.  A warp per slot with a state of its own (8 warps per
     // SM) measured slower at every batch size of the simulations.
-    static int wave8[64][5] = {};
+    static std::atomic<int> wave8[64][5];   // per device and K class; 0 until measured (jobs may run in threads)
     const size_t smem = sizeof(WarpShared);
     if (a.nslots <= 0) return cudaSuccess;
     int dev = 0;
@@ -2898,7 +2900,8 @@ cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     const int kc = a.K <= 1 ? 0 : a.K <= 2 ? 1 : a.K <= 4 ? 2 : a.K <= 8 ? 3 : 4;
-    if (wave8[dev][kc] == 0) {
+    int wave = wave8[dev][kc].load(std::memory_order_relaxed);
+    if (wave == 0) {
         int sms = 0, per_sm = 0;
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
         const void *fn = kc == 0   ? (const void *)k_replay<1, TEAM_MAX>
@@ -2908,9 +2911,10 @@ cudaError_t launch_replay(const ReplayArgs &a, cudaStream_t st) {
                                    : (const void *)k_replay<16, TEAM_MAX>;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * TEAM_MAX, smem)) != cudaSuccess)
             return e;
-        wave8[dev][kc] = sms * (per_sm > 0 ? per_sm : 1);
+        wave = sms * (per_sm > 0 ? per_sm : 1);
+        wave8[dev][kc].store(wave, std::memory_order_relaxed);
     }
-    if (a.nslots <= wave8[dev][kc]) launch_replay_team<TEAM_MAX>(a, smem, st);
+    if (a.nslots <= wave) launch_replay_team<TEAM_MAX>(a, smem, st);
     else launch_replay_team<TEAM_MAX / 2>(a, smem, st);
     return cudaGetLastError();
 }

@@ -346,6 +346,8 @@ typedef struct {
     long long tensor_launches;
     long long path_nodes;         /* path nodes of the simulation (nodes: those of the last run) */
     long long learned_fallback;   /* learned proposal: nodes whose confidence check sent them to the exact map */
+    long long graph_nodes;        /* graph mode: nodes of the captured batch chain of the last run (0: direct launches) */
+    float ms_graph_build;         /* graph mode: host time of capture and instantiation of the last run */
 } qsk_sim_info;
 
 typedef struct qsk_sim qsk_sim;
@@ -385,6 +387,20 @@ int qsk_sim_set_profiling(qsk_sim *s, int on);
  * path node's level is never published, so its dependants' waits run out
  * (-1: normal operation). */
 int qsk_sim_set_level_wait(qsk_sim *s, unsigned spin_limit, long long hold_node);
+/* Graph mode (plain path): qsk_sim_run captures its whole chain of batches
+ * (prep, map, draw of every level, and the generator pipeline on the second
+ * stream) into one CUDA graph, instantiates it and launches it, instead of
+ * launching each kernel on the streams.  Results are identical.  Ignored by
+ * the tensor-core and learned forms and in profiling mode. */
+int qsk_sim_set_graph(qsk_sim *s, int on);
+/* Several simulations in one call (the reference's concurrency over
+ * realisations: one qs run per realisation, src/qs.cpp): each simulation's
+ * qsk_sim_run on its own streams, `threads` host threads (0: up to 16)
+ * taking the jobs in order, so that the levels of different jobs (TIs,
+ * grids, n) share the GPU.  Every simulation must be distinct.  status
+ * (optional, count entries) receives each job's return code; the call
+ * returns the first job error (its message prefixed with the job index). */
+int qsk_jobs_run(qsk_sim *const *sims, int count, int threads, int *status);
 /* Path (cell order), per-path-index seeds and number of informed cells. */
 int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
 int qsk_sim_destroy(qsk_sim *s);
@@ -419,16 +435,20 @@ typedef struct {
     int width;         /* 8, 16 or 32 */
     int shortlist;     /* <= 128 */
     float audit;       /* fraction of tensor-path nodes audited, 0..1 */
+    int batch;         /* nodes per tensor step (GEMM launch): a multiple of 128 up to 16384; 0: 4096 */
 } qsk_tensor_opts;
 int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *opts);
 
 /* ------------------------------------------------------------------------
- * Learned proposal (no G2S counterpart).  A small MLP encoder embeds the
- * canonical neighbourhood of a node and of every TI cell: 64 entries, entry
- * e for template offset e + 1, of [variable values, mask, dx, dy, dz]
- * (offsets divided by 8); a node's entry holds the value of its neighbour at
- * that offset (mask 1) or nothing (mask 0: no neighbour there), a TI cell's
- * the TI value there (mask 0 outside the TI), into 64 dimensions: a shared trunk
+ * Learned proposal (no G2S counterpart).  A small MLP encoder embeds a
+ * node's informed neighbourhood and the neighbourhood of every TI cell as 64
+ * entries of [variable values, mask, dx, dy, dz] (offsets divided by 8).
+ * The entries form a stencil: the template's first 64 offsets dilated by a
+ * scale s in 1..nscales (qsk_encoder_set_scales); a node takes the smallest
+ * scale whose stencil holds most of its neighbours, each entry holding the
+ * mean of the neighbour values falling in it (mask 1) or nothing (mask 0); a
+ * TI cell's entry holds the TI value at s x the offset (mask 0 outside the
+ * TI), and the TI is embedded once per scale.  Shared trunk
  * 64 x (nvar + 4) -> 256 -> 256 -> 256 (GELU), then a query head (nodes) or
  * a TI-pattern head (TI cells) -> 64, unnormalised, so that the inner
  * product can take the form of the QS score (2 v . t - |t|^2 for a

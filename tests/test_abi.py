@@ -75,3 +75,13 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(g2s_b200, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(RuntimeError):
         g2s_b200.lib()
+
+
+def test_jobs_run_checks_arguments_without_a_gpu(g2s):
+    L = g2s.lib()
+    assert L.qsk_jobs_run(None, 0, 0, None) == 0
+    assert L.qsk_jobs_run(None, 1, 0, None) != 0
+    assert L.qsk_jobs_run(None, -1, 0, None) != 0
+    arr = (__import__("ctypes").c_void_p * 2)(None, None)
+    assert L.qsk_jobs_run(arr, 2, 2, None) != 0
+    assert b"null simulation" in L.qsk_last_error()
