@@ -261,6 +261,12 @@ def set_path(sim, path, enc=None, audit=0.01):
         sim.set_learned(enc, shortlist=256, audit=audit)
 
 
+def fft_kind() -> str:
+    """The FFT under the reference build: always the project FFT behind the
+    FFTW3f API ("shim"); a host libfftw3f, if any, is not linked."""
+    return "shim"
+
+
 def fft_in_use() -> str:
     lib = ctypes.util.find_library("fftw3f")
     return f"FFTW3f API shim (project FFT; no libfftw3f on this host)" if not lib else \
@@ -309,7 +315,8 @@ def reference_arm(args):
         "ms_per_step": float(1000.0 * np.prod(w["di"]) / v) if not (w.get("sample") or w.get("jobs")) else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": w["name"], "threads": cores},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "fft": fft_kind(),
+                         "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -468,7 +475,7 @@ def jobs_main(args, w, g2s, dev):
         from oracle import ref
         if ref.available():
             v, cores, samp = jobs_reference(w, jobs)
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": samp}
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "fft": fft_kind(), "sample": samp}
             log(f"cpu baseline: {cpu}")
     plain_v = compare.get("plain", {}).get("value")
     tensor = path in ("bf16", "fp8")
@@ -517,6 +524,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / fp32 comparison arms")
+    ap.add_argument("--grid", type=int, default=0,
+                    help="profiling only: simulation grid side (2-D whole-simulation workloads); not a bench line")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -525,6 +534,10 @@ def main():
     import g2s_b200 as g2s
 
     w = WORKLOADS[args.workload]
+    if args.grid:
+        if w.get("sample") or w.get("jobs") or len(w["di"]) != 2:
+            raise SystemExit("--grid applies to the 2-D whole-simulation workloads")
+        w = dict(w, di=(args.grid, args.grid), name=w["name"] + f"-profiling-grid{args.grid}")
     path = args.path or w["path"]
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -682,7 +695,8 @@ def main():
             log("cpu baseline (reference) ...")
             vals, cores, samp = reference_measure(args, w, 1)
             log(f"cpu baseline: {vals}")
-            cpu = {"value": float(np.mean(vals)), "unit": UNIT, "cores": cores, "kind": "reference", "sample": samp}
+            cpu = {"value": float(np.mean(vals)), "unit": UNIT, "cores": cores, "kind": "reference", "fft": fft_kind(),
+                   "sample": samp}
 
     if rank == 0:
         last = infos[-1]

@@ -120,6 +120,9 @@ SIGNATURES = {
     "qsk_encoder_param_count": (ctypes.c_longlong, [ctypes.c_void_p]),
     "qsk_encoder_input_dim": (ctypes.c_int, [ctypes.c_void_p]),
     "qsk_encoder_set_scales": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]),
+    "qsk_encoder_set_tensor_cores": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "qsk_gemm_bf16": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
+                                     _f32p]),
     "qsk_encoder_get_pairs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_longlong, _f32p, _f32p]),
     "qsk_encoder_get_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
     "qsk_encoder_set_weights": (ctypes.c_int, [ctypes.c_void_p, _f32p]),
@@ -520,6 +523,12 @@ class Encoder:
         self.input_dim = lib().qsk_encoder_input_dim(h)
         self.param_count = lib().qsk_encoder_param_count(h)
 
+    def set_tensor_cores(self, on: bool = True):
+        """Encoder products on the tensor cores (BF16, default) or in FP32
+        on the CUDA cores (qsk_encoder_set_tensor_cores)."""
+        _check(lib().qsk_encoder_set_tensor_cores(self.handle, int(bool(on))), "qsk_encoder_set_tensor_cores")
+        return self
+
     def set_scales(self, nscales: int = 4, cov_min: float = 0.9):
         """Stencil scales of the inputs (qsk_encoder_set_scales)."""
         _check(lib().qsk_encoder_set_scales(self.handle, int(nscales), float(cov_min)), "qsk_encoder_set_scales")
@@ -602,6 +611,20 @@ class Encoder:
             self.close()
         except Exception:
             pass
+
+
+def gemm_bf16(a: np.ndarray, b: np.ndarray, bias: Optional[np.ndarray] = None, device: int = 0) -> np.ndarray:
+    """C = bf16(a) @ bf16(b).T (+ bias) on the tensor cores (qsk_gemm_bf16)."""
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    b = np.ascontiguousarray(b, dtype=np.float32)
+    M, K = a.shape
+    N, K2 = b.shape
+    assert K == K2
+    bi = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
+    c = np.zeros((M, N), np.float32)
+    _check(lib().qsk_gemm_bf16(device, M, N, K, _p(a, _f32p), _p(b, _f32p), _p(bi, _f32p), _p(c, _f32p)),
+           "qsk_gemm_bf16")
+    return c
 
 
 def run_jobs(sims: Sequence["Simulation"], threads: int = 0) -> np.ndarray:

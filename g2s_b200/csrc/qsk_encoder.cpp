@@ -16,6 +16,13 @@
 
 using namespace qsk;
 
+// return a failing status code of a call
+#define QSK_RC(expr)                \
+    do {                            \
+        const int rc_ = (expr);     \
+        if (rc_ != QSK_OK) return rc_; \
+    } while (0)
+
 namespace qsk {
 
 // parameter layout: W1 [H x D0], b1 [H], W2 [H x H], b2, W3 [H x H], b3
@@ -52,6 +59,48 @@ int enc_scratch(qsk_encoder *e, long long rows) {
     return QSK_OK;
 }
 
+// C = op(A) op(B) (+ bias[n]), op(A) M x K and op(B) K x N as in
+// launch_sgemm (ta: A stored K x M; tb: B stored N x K): on the tensor cores
+// (op(A) and op(B)^T packed to zero-padded BF16, FP32 accumulation) or in
+// FP32 on the CUDA cores
+int enc_gemm(qsk_encoder *e, int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb, int tb,
+             float *C, int ldc, const float *bias, cudaStream_t st) {
+    if (!e->tensor) {
+        QSK_CK(launch_sgemm(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, 1.f, 0.f, bias, st));
+        return QSK_OK;
+    }
+    if (M <= 0 || N <= 0) return QSK_OK;
+    const int kpad = (K + 63) / 64 * 64;
+    const long long ar = (M + 127LL) / 128 * 128;
+    const int bn = tc_gemm_bn(N);
+    const long long br = (N + bn - 1LL) / bn * bn;
+    QSK_CK(e->pa.ensure(size_t(ar) * kpad));
+    QSK_CK(e->pb.ensure(size_t(br) * kpad));
+    QSK_CK(launch_pack_bf16(M, K, A, lda, ta, ar, kpad, e->pa.p, st));
+    QSK_CK(launch_pack_bf16(N, K, B, ldb, tb ? 0 : 1, br, kpad, e->pb.p, st));
+    TcGemmArgs g;
+    g.M = M;
+    g.N = N;
+    g.kpad = kpad;
+    g.C = C;
+    g.ldc = ldc;
+    g.bias = bias;
+    g.status = e->status.p;
+    QSK_CK(launch_tc_gemm(e->pa.p, ar, e->pb.p, br, g, st));
+    return QSK_OK;
+}
+
+int enc_check(qsk_encoder *e, cudaStream_t st) {
+    int v = 0;
+    QSK_CK(cudaMemcpyAsync(&v, e->status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QSK_CK(cudaStreamSynchronize(st));
+    if (v != 0) {
+        QSK_CK(cudaMemsetAsync(e->status.p, 0, sizeof(int), st));
+        return set_error(QSK_ERR_DEVICE, "encoder: a tensor-core product's pipeline wait ran out (status %d)", v);
+    }
+    return QSK_OK;
+}
+
 // rows x D0 inputs x -> embeddings e->y (rows x E) by the trunk and a head:
 // rows [0, nq) the query head, rows [nq, rows) the TI-pattern head;
 // activations kept for the backward pass
@@ -61,17 +110,17 @@ int enc_forward(qsk_encoder *e, long long rows, long long nq, const float *x, cu
     const float *w = e->w.p;
     const long long *o = e->off;
     const int R = int(rows), Q = int(nq);
-    QSK_CK(launch_sgemm(R, ENC_H, e->D0, x, e->D0, 0, w + o[0], e->D0, 1, e->h1p.p, ENC_H, 1.f, 0.f, w + o[1], st));
+    QSK_RC(enc_gemm(e, R, ENC_H, e->D0, x, e->D0, 0, w + o[0], e->D0, 1, e->h1p.p, ENC_H, w + o[1], st));
     QSK_CK(launch_gelu((long long)R * ENC_H, e->h1p.p, e->h1.p, st));
-    QSK_CK(launch_sgemm(R, ENC_H, ENC_H, e->h1.p, ENC_H, 0, w + o[2], ENC_H, 1, e->h2p.p, ENC_H, 1.f, 0.f, w + o[3], st));
+    QSK_RC(enc_gemm(e, R, ENC_H, ENC_H, e->h1.p, ENC_H, 0, w + o[2], ENC_H, 1, e->h2p.p, ENC_H, w + o[3], st));
     QSK_CK(launch_gelu((long long)R * ENC_H, e->h2p.p, e->h2.p, st));
-    QSK_CK(launch_sgemm(R, ENC_H, ENC_H, e->h2.p, ENC_H, 0, w + o[4], ENC_H, 1, e->h3p.p, ENC_H, 1.f, 0.f, w + o[5], st));
+    QSK_RC(enc_gemm(e, R, ENC_H, ENC_H, e->h2.p, ENC_H, 0, w + o[4], ENC_H, 1, e->h3p.p, ENC_H, w + o[5], st));
     QSK_CK(launch_gelu((long long)R * ENC_H, e->h3p.p, e->h3.p, st));
     if (Q > 0)
-        QSK_CK(launch_sgemm(Q, ENC_E, ENC_H, e->h3.p, ENC_H, 0, w + o[6], ENC_H, 1, e->y.p, ENC_E, 1.f, 0.f, w + o[7], st));
+        QSK_RC(enc_gemm(e, Q, ENC_E, ENC_H, e->h3.p, ENC_H, 0, w + o[6], ENC_H, 1, e->y.p, ENC_E, w + o[7], st));
     if (R > Q)
-        QSK_CK(launch_sgemm(R - Q, ENC_E, ENC_H, e->h3.p + size_t(Q) * ENC_H, ENC_H, 0, w + o[8], ENC_H, 1,
-                            e->y.p + size_t(Q) * ENC_E, ENC_E, 1.f, 0.f, w + o[9], st));
+        QSK_RC(enc_gemm(e, R - Q, ENC_E, ENC_H, e->h3.p + size_t(Q) * ENC_H, ENC_H, 0, w + o[8], ENC_H, 1,
+                        e->y.p + size_t(Q) * ENC_E, ENC_E, w + o[9], st));
     return QSK_OK;
 }
 
@@ -87,31 +136,31 @@ int enc_backward(qsk_encoder *e, long long rows, long long nq, const float *x) {
     // heads: dW4 = dz^T h3, db4 = colsum dz, dh3 = dz W4 (per head's rows)
     QSK_CK(cudaMemsetAsync(g + o[6], 0, sizeof(float) * size_t(o[10] - o[6]), st));
     if (Q > 0) {
-        QSK_CK(launch_sgemm(ENC_E, ENC_H, Q, e->dz.p, ENC_E, 1, e->h3.p, ENC_H, 0, g + o[6], ENC_H, 1.f, 0.f, nullptr, st));
+        QSK_RC(enc_gemm(e, ENC_E, ENC_H, Q, e->dz.p, ENC_E, 1, e->h3.p, ENC_H, 0, g + o[6], ENC_H, nullptr, st));
         QSK_CK(launch_colsum(Q, ENC_E, e->dz.p, g + o[7], 0, st));
-        QSK_CK(launch_sgemm(Q, ENC_H, ENC_E, e->dz.p, ENC_E, 0, w + o[6], ENC_H, 0, e->d1.p, ENC_H, 1.f, 0.f, nullptr, st));
+        QSK_RC(enc_gemm(e, Q, ENC_H, ENC_E, e->dz.p, ENC_E, 0, w + o[6], ENC_H, 0, e->d1.p, ENC_H, nullptr, st));
     }
     if (R > Q) {
         const float *dzp = e->dz.p + size_t(Q) * ENC_E;
-        QSK_CK(launch_sgemm(ENC_E, ENC_H, R - Q, dzp, ENC_E, 1, e->h3.p + size_t(Q) * ENC_H, ENC_H, 0, g + o[8], ENC_H,
-                            1.f, 0.f, nullptr, st));
+        QSK_RC(enc_gemm(e, ENC_E, ENC_H, R - Q, dzp, ENC_E, 1, e->h3.p + size_t(Q) * ENC_H, ENC_H, 0, g + o[8], ENC_H,
+                        nullptr, st));
         QSK_CK(launch_colsum(R - Q, ENC_E, dzp, g + o[9], 0, st));
-        QSK_CK(launch_sgemm(R - Q, ENC_H, ENC_E, dzp, ENC_E, 0, w + o[8], ENC_H, 0, e->d1.p + size_t(Q) * ENC_H, ENC_H,
-                            1.f, 0.f, nullptr, st));
+        QSK_RC(enc_gemm(e, R - Q, ENC_H, ENC_E, dzp, ENC_E, 0, w + o[8], ENC_H, 0, e->d1.p + size_t(Q) * ENC_H, ENC_H,
+                        nullptr, st));
     }
     QSK_CK(launch_gelu_back((long long)R * ENC_H, e->h3p.p, e->d1.p, st));
     // layer 3
-    QSK_CK(launch_sgemm(ENC_H, ENC_H, R, e->d1.p, ENC_H, 1, e->h2.p, ENC_H, 0, g + o[4], ENC_H, 1.f, 0.f, nullptr, st));
+    QSK_RC(enc_gemm(e, ENC_H, ENC_H, R, e->d1.p, ENC_H, 1, e->h2.p, ENC_H, 0, g + o[4], ENC_H, nullptr, st));
     QSK_CK(launch_colsum(R, ENC_H, e->d1.p, g + o[5], 0, st));
-    QSK_CK(launch_sgemm(R, ENC_H, ENC_H, e->d1.p, ENC_H, 0, w + o[4], ENC_H, 0, e->d2.p, ENC_H, 1.f, 0.f, nullptr, st));
+    QSK_RC(enc_gemm(e, R, ENC_H, ENC_H, e->d1.p, ENC_H, 0, w + o[4], ENC_H, 0, e->d2.p, ENC_H, nullptr, st));
     QSK_CK(launch_gelu_back((long long)R * ENC_H, e->h2p.p, e->d2.p, st));
     // layer 2
-    QSK_CK(launch_sgemm(ENC_H, ENC_H, R, e->d2.p, ENC_H, 1, e->h1.p, ENC_H, 0, g + o[2], ENC_H, 1.f, 0.f, nullptr, st));
+    QSK_RC(enc_gemm(e, ENC_H, ENC_H, R, e->d2.p, ENC_H, 1, e->h1.p, ENC_H, 0, g + o[2], ENC_H, nullptr, st));
     QSK_CK(launch_colsum(R, ENC_H, e->d2.p, g + o[3], 0, st));
-    QSK_CK(launch_sgemm(R, ENC_H, ENC_H, e->d2.p, ENC_H, 0, w + o[2], ENC_H, 0, e->d1.p, ENC_H, 1.f, 0.f, nullptr, st));
+    QSK_RC(enc_gemm(e, R, ENC_H, ENC_H, e->d2.p, ENC_H, 0, w + o[2], ENC_H, 0, e->d1.p, ENC_H, nullptr, st));
     QSK_CK(launch_gelu_back((long long)R * ENC_H, e->h1p.p, e->d1.p, st));
     // layer 1 (the input needs no gradient)
-    QSK_CK(launch_sgemm(ENC_H, e->D0, R, e->d1.p, ENC_H, 1, x, e->D0, 0, g + o[0], e->D0, 1.f, 0.f, nullptr, st));
+    QSK_RC(enc_gemm(e, ENC_H, e->D0, R, e->d1.p, ENC_H, 1, x, e->D0, 0, g + o[0], e->D0, nullptr, st));
     QSK_CK(launch_colsum(R, ENC_H, e->d1.p, g + o[1], 0, st));
     return QSK_OK;
 }
@@ -126,6 +175,10 @@ int enc_loss_grad(qsk_encoder *e, int B, float tau) {
     QSK_CK(e->loss.ensure(1));
     const float *Q = e->y.p, *P = e->y.p + (size_t)B * ENC_E;
     cudaStream_t st = e->st;
+    // the logits and their gradient stay FP32 in either mode: the column
+    // sums of dS nearly cancel (every softmax row and column sums to one), so
+    // the heads' bias gradients are small differences that BF16 operands
+    // would swamp; these B x B x 64 products are a small part of a step
     // S = Q P^T
     QSK_CK(launch_sgemm(B, B, ENC_E, Q, ENC_E, 0, P, ENC_E, 1, e->S.p, B, 1.f, 0.f, nullptr, st));
     QSK_CK(cudaMemsetAsync(e->dS.p, 0, sizeof(float) * size_t(B) * B, st));
@@ -166,7 +219,8 @@ int qsk_encoder_create(int device, int nvar, unsigned seed, qsk_encoder **out) {
         for (long long i = e->off[2 * l]; i < e->off[2 * l + 1]; ++i) w[size_t(i)] = u(rng);
     }
     int rc = QSK_OK;
-    if (e->w.upload(w.data(), w.size(), e->st) != cudaSuccess || e->g.alloc(w.size()) != cudaSuccess ||
+    if (e->status.alloc(1) != cudaSuccess || cudaMemsetAsync(e->status.p, 0, sizeof(int), e->st) != cudaSuccess ||
+        e->w.upload(w.data(), w.size(), e->st) != cudaSuccess || e->g.alloc(w.size()) != cudaSuccess ||
         e->m.alloc(w.size()) != cudaSuccess || e->v.alloc(w.size()) != cudaSuccess ||
         cudaMemsetAsync(e->m.p, 0, sizeof(float) * w.size(), e->st) != cudaSuccess ||
         cudaMemsetAsync(e->v.p, 0, sizeof(float) * w.size(), e->st) != cudaSuccess ||
@@ -200,6 +254,53 @@ int qsk_encoder_destroy(qsk_encoder *e) {
 
 long long qsk_encoder_param_count(const qsk_encoder *e) { return e ? e->nparam : -1; }
 int qsk_encoder_input_dim(const qsk_encoder *e) { return e ? e->D0 : -1; }
+
+int qsk_gemm_bf16(int device, int M, int N, int K, const float *A, const float *B, const float *bias, float *C) {
+    if (M < 1 || N < 1 || K < 1 || !A || !B || !C) return set_error(QSK_ERR_ARG, "gemm: arguments");
+    DeviceGuard dg(device);
+    cudaStream_t st = nullptr;
+    QSK_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{st};
+    const int kpad = (K + 63) / 64 * 64, bn = tc_gemm_bn(N);
+    const long long ar = (M + 127LL) / 128 * 128, br = (N + bn - 1LL) / bn * bn;
+    DBuf<float> a, b, bi, c;
+    DBuf<unsigned short> pa, pb;
+    DBuf<int> status;
+    QSK_CK(a.upload(A, size_t(M) * K, st));
+    QSK_CK(b.upload(B, size_t(N) * K, st));
+    if (bias) QSK_CK(bi.upload(bias, size_t(N), st));
+    QSK_CK(c.alloc(size_t(M) * N));
+    QSK_CK(pa.alloc(size_t(ar) * kpad));
+    QSK_CK(pb.alloc(size_t(br) * kpad));
+    QSK_CK(status.alloc(1));
+    QSK_CK(cudaMemsetAsync(status.p, 0, sizeof(int), st));
+    QSK_CK(launch_pack_bf16(M, K, a.p, K, 0, ar, kpad, pa.p, st));
+    QSK_CK(launch_pack_bf16(N, K, b.p, K, 0, br, kpad, pb.p, st));
+    TcGemmArgs g;
+    g.M = M;
+    g.N = N;
+    g.kpad = kpad;
+    g.C = c.p;
+    g.ldc = N;
+    g.bias = bias ? bi.p : nullptr;
+    g.status = status.p;
+    QSK_CK(launch_tc_gemm(pa.p, ar, pb.p, br, g, st));
+    int v = 0;
+    QSK_CK(cudaMemcpyAsync(C, c.p, sizeof(float) * size_t(M) * N, cudaMemcpyDeviceToHost, st));
+    QSK_CK(cudaMemcpyAsync(&v, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QSK_CK(cudaStreamSynchronize(st));
+    if (v != 0) return set_error(QSK_ERR_DEVICE, "gemm: a pipeline wait ran out (status %d)", v);
+    return QSK_OK;
+}
+
+int qsk_encoder_set_tensor_cores(qsk_encoder *e, int on) {
+    if (!e) return set_error(QSK_ERR_ARG, "null argument");
+    e->tensor = on != 0;
+    return QSK_OK;
+}
 
 int qsk_encoder_set_scales(qsk_encoder *e, int nscales, float cov_min) {
     if (!e) return set_error(QSK_ERR_ARG, "null argument");
@@ -240,8 +341,7 @@ int qsk_encoder_loss_grad(qsk_encoder *e, int B, const float *xq, const float *x
     if (rc) return rc;
     QSK_CK(cudaMemcpyAsync(loss, e->loss.p, sizeof(float), cudaMemcpyDeviceToHost, e->st));
     if (grad) QSK_CK(cudaMemcpyAsync(grad, e->g.p, sizeof(float) * size_t(e->nparam), cudaMemcpyDeviceToHost, e->st));
-    QSK_CK(cudaStreamSynchronize(e->st));
-    return QSK_OK;
+    return enc_check(e, e->st);
 }
 
 int qsk_encoder_embed(qsk_encoder *e, int head, long long rows, const float *x, float *out) {
@@ -259,8 +359,7 @@ int qsk_encoder_embed(qsk_encoder *e, int head, long long rows, const float *x, 
         QSK_CK(cudaMemcpyAsync(out + size_t(r0) * ENC_E, e->y.p, sizeof(float) * size_t(n) * ENC_E, cudaMemcpyDeviceToHost,
                                e->st));
     }
-    QSK_CK(cudaStreamSynchronize(e->st));
-    return QSK_OK;
+    return enc_check(e, e->st);
 }
 
 int qsk_encoder_add_pairs_host(qsk_encoder *e, long long n, const float *xq, const float *xp) {
@@ -341,7 +440,7 @@ int qsk_encoder_train(qsk_encoder *e, int epochs, int batch, float lr, float tau
             QSK_CK(launch_adam(e->nparam, e->w.p, e->g.p, e->m.p, e->v.p, lr, ++e->t, e->st));
         }
         QSK_CK(cudaMemcpyAsync(&l, e->loss.p, sizeof(float), cudaMemcpyDeviceToHost, e->st));
-        QSK_CK(cudaStreamSynchronize(e->st));
+        if (int rc = enc_check(e, e->st)) return rc;
     }
     if (last_loss) *last_loss = l;
     return QSK_OK;

@@ -20,6 +20,11 @@ struct qsk_encoder {
     // a node takes the smallest holding cov_min of its neighbours
     int nscales = 4;
     float cov_min = 0.9f;
+    // matrix products on the tensor cores (BF16 operands, FP32 accumulation)
+    // or, when false, on the CUDA cores in FP32
+    bool tensor = true;
+    qsk::DBuf<unsigned short> pa, pb;   // packed BF16 operands of one product
+    qsk::DBuf<int> status;              // DEV_TC_WAIT from the tensor-core kernel
     long long off[qsk::ENC_NP + 1] = {};
     long long nparam = 0;
     cudaStream_t st = nullptr;
@@ -39,4 +44,7 @@ namespace qsk {
 // rows x D0 inputs -> embeddings in e->y (rows x 64), rows [0, nq) by the
 // query head and the rest by the TI-pattern head, on stream st
 int enc_forward(qsk_encoder *e, long long rows, long long nq, const float *x, cudaStream_t st);
+// QSK_OK unless a tensor-core product of the encoder ran out of a wait
+// (synchronises st); clears the flag
+int enc_check(qsk_encoder *e, cudaStream_t st);
 }  // namespace qsk

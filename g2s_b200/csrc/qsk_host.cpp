@@ -1273,6 +1273,7 @@ int tc_configure_learned(qsk_sim *s) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     s->info.ms_tensor_pattern = ms;
+    if ((rc = enc_check(e, s->st)) != QSK_OK) return rc;
     s->enc_built = e->t;
     s->enc_ns = e->nscales;
     s->tc_ready = true;
@@ -1756,7 +1757,7 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
         std::vector<int> fb((size_t)B), nd((size_t)B);
         CK(cudaMemcpyAsync(fb.data(), s->d_fb.p, sizeof(int) * B, cudaMemcpyDeviceToHost, s->st));
         CK(cudaMemcpyAsync(nd.data(), step.nodes + step.off, sizeof(int) * B, cudaMemcpyDeviceToHost, s->st));
-        CK(cudaStreamSynchronize(s->st));
+        if (int rc = enc_check(s->enc, s->st)) return rc;
         std::vector<int> list;
         for (int q = 0; q < B; ++q)
             if (fb[size_t(q)]) list.push_back(nd[size_t(q)]);

@@ -303,6 +303,19 @@ struct TcArgs {
 int tc_supported_width(int w);
 // kind 0: BF16 (kind::f16), 1: FP8 E4M3 (kind::f8f6f4); a_rows % 128 == 0,
 // p_rows % 256 == 0, k_elems * element size % 128 == 0
+// C[M x N] = A * B^T (+ bias) on the tensor cores: A (a_rows x kpad) and B
+// (b_rows x kpad) BF16 K-major, a_rows a multiple of 128, b_rows of the N
+// tile (tc_gemm_bn(N)), kpad of 64, padding zero; C FP32 row-major (ldc)
+struct TcGemmArgs {
+    int M = 0, N = 0, kpad = 0;
+    float *C = nullptr;
+    long long ldc = 0;
+    const float *bias = nullptr;
+    int *status = nullptr;   // DEV_TC_WAIT when a wait ran out
+};
+int tc_gemm_bn(int N);
+cudaError_t launch_tc_gemm(const void *a_bf16, long long a_rows, const void *b_bf16, long long b_rows,
+                           const TcGemmArgs &g, cudaStream_t st);
 cudaError_t launch_tc_shortlist(int kind, int W, const void *a_mat, long long a_rows, const void *p_mat,
                                 long long p_rows, long long k_elems, const TcArgs &args, cudaStream_t st);
 // Tensor-core form inside the simulation.  Pattern matrix P: one row per TI
@@ -455,6 +468,10 @@ cudaError_t launch_rownorm_back(int rows, int cols, const float *y, const float 
 cudaError_t launch_infonce(int B, float tau, const float *S, float *dS, float *loss, cudaStream_t st);
 cudaError_t launch_adam(long long n, float *w, const float *g, float *m, float *v, float lr, int t, cudaStream_t st);
 cudaError_t launch_feat_nodes(const FeatArgs &a, cudaStream_t st);
+// rows_pad x kpad BF16 copy of a rows x cols FP32 matrix (tr: of its
+// transpose, src then cols x rows), zero-padded; both pads multiples of 32
+cudaError_t launch_pack_bf16(int rows, int cols, const float *src, long long ld, int tr, long long rows_pad, int kpad,
+                             void *dst, cudaStream_t st);
 cudaError_t launch_feat_cells(const FeatArgs &a, cudaStream_t st);
 cudaError_t launch_to_bf16(long long n, const float *x, uint16_t *y, cudaStream_t st);
 cudaError_t launch_gather_rows(int n, int cols, const int *idx, const float *src, float *dst, cudaStream_t st);

@@ -16,6 +16,7 @@
 // scale s in 1..nscales.  A node takes the smallest scale whose stencil
 // holds most of its informed neighbours (sparse neighbourhoods early on the
 // path take a coarse stencil); the TI is embedded once per scale.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -358,6 +359,28 @@ __global__ void k_gather_rows(int n, int cols, const int *__restrict__ idx, cons
     for (int c = threadIdx.x; c < cols; c += blockDim.x) d[c] = s[c];
 }
 
+// BF16 operand of the tensor-core GEMM: dst (rows_pad x kpad) element
+// (r, c) = src[r * ld + c] (tr 0) or src[c * ld + r] (tr 1) for r < rows and
+// c < cols, zero elsewhere; 32 x 32 tiles through shared memory, so that
+// reads and writes are coalesced either way
+__global__ void k_pack_bf16(int rows, int cols, const float *__restrict__ src, long long ld, int tr, int kpad,
+                            __nv_bfloat16 *__restrict__ dst) {
+    __shared__ float t[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int i = ty; i < 32; i += 8) {
+        if (!tr) {
+            const int r = r0 + i, c = c0 + tx;
+            t[i][tx] = (r < rows && c < cols) ? src[(long long)r * ld + c] : 0.f;
+        } else {
+            const int c = c0 + i, r = r0 + tx;
+            t[tx][i] = (r < rows && c < cols) ? src[(long long)c * ld + r] : 0.f;
+        }
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) dst[(long long)(r0 + i) * kpad + c0 + tx] = __float2bfloat16_rn(t[i][tx]);
+}
+
 unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -397,6 +420,14 @@ cudaError_t launch_adam(long long n, float *w, const float *g, float *m, float *
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - powf(b1, (float)t), c2 = 1.f - powf(b2, (float)t);
     k_adam<<<blocks_for(n, 256), 256, 0, st>>>(n, w, g, m, v, lr, b1, b2, 1e-8f, c1, c2);
+    return cudaGetLastError();
+}
+cudaError_t launch_pack_bf16(int rows, int cols, const float *src, long long ld, int tr, long long rows_pad, int kpad,
+                             void *dst, cudaStream_t st) {
+    if (rows_pad <= 0 || kpad <= 0) return cudaSuccess;
+    if (rows_pad % 32 || kpad % 32 || rows > rows_pad || cols > kpad) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)(kpad / 32), (unsigned)(rows_pad / 32));
+    k_pack_bf16<<<grid, dim3(32, 8), 0, st>>>(rows, cols, src, ld, tr, kpad, reinterpret_cast<__nv_bfloat16 *>(dst));
     return cudaGetLastError();
 }
 cudaError_t launch_feat_nodes(const FeatArgs &a, cudaStream_t st) {

@@ -480,6 +480,141 @@ __global__ void __launch_bounds__(threads_for(W), 1)
     }
 }
 
+// General BF16 GEMM on the tensor cores (the learned proposal's encoder):
+// C[M x N] = A[M x K] * B[N x K]^T (+ bias[n]), A and B BF16 K-major with
+// rows padded to the tile and K to 64 elements (zeros), C FP32 row-major.
+// One 128 x BNG output tile per CTA: warp 0 streams the K blocks of A and B
+// through a 4-stage ring with TMA, warp 1 allocates BNG TMEM columns and
+// issues the MMAs (kind::f16, BF16 in, FP32 accumulate), warps 2-5 read the
+// accumulator (one row per thread) and store the rows inside M x N.  Waits
+// are bounded as in k_tc_shortlist.
+template <int BNG>
+__global__ void __launch_bounds__(192, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b, TcGemmArgs g) {
+    constexpr int STAGES = 4;
+    constexpr int AB = BM * BKB, BB = BNG * BKB;
+    extern __shared__ uint8_t smem_raw[];
+    const unsigned raw = smem_u32(smem_raw);
+    uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+    uint8_t *sA = smem, *sB = smem + STAGES * AB;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + STAGES * (AB + BB));
+    uint64_t *full = bar, *empty = bar + STAGES, *tfull = bar + 2 * STAGES, *done = tfull + 1;
+    __shared__ unsigned tmem_base_s;
+    __shared__ volatile int abort_s;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile_m = blockIdx.x, tile_n = blockIdx.y;
+    const int nkb = g.kpad / (BKB / 2);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < STAGES; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(tfull, 1);
+        mbar_init(done, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                     "r"(BNG)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_base_s;
+    if (warp == 0) {
+        if (lane == 0) {
+            int s = 0;
+            unsigned ph = 0, issued_ph[STAGES];
+            bool pending[STAGES];
+            for (int i = 0; i < STAGES; ++i) pending[i] = false;
+            bool ok = true;
+            for (int kb = 0; kb < nkb; ++kb) {
+                if (!mbar_wait(&empty[s], ph ^ 1u, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[s], AB + BB);
+                tma_load_2d(sA + s * AB, &map_a, &full[s], kb * (BKB / 2), tile_m * BM);
+                tma_load_2d(sB + s * BB, &map_b, &full[s], kb * (BKB / 2), tile_n * BNG);
+                pending[s] = true;
+                issued_ph[s] = ph;
+                if (++s == STAGES) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            if (!ok) {
+                atomicExch(g.status, DEV_TC_WAIT);
+                abort_s = 1;
+            }
+            for (int i = 0; i < STAGES; ++i)
+                if (pending[i]) mbar_wait(&full[i], issued_ph[i], nullptr);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr unsigned idesc = make_idesc(1u, BM, BNG);
+            int s = 0;
+            unsigned ph = 0;
+            bool ok = true;
+            for (int kb = 0; kb < nkb; ++kb) {
+                if (!mbar_wait(&full[s], ph, &abort_s)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t ad = sw128_desc(smem_u32(sA + s * AB));
+                const uint64_t bd = sw128_desc(smem_u32(sB + s * BB));
+#pragma unroll
+                for (int k = 0; k < 4; ++k) mma<0>(tmem, ad + (uint64_t)(2 * k), bd + (uint64_t)(2 * k), idesc, (kb | k) != 0);
+                mma_commit(&empty[s]);
+                if (++s == STAGES) {
+                    s = 0;
+                    ph ^= 1u;
+                }
+            }
+            if (ok) {
+                mma_commit(tfull);
+            } else {
+                atomicExch(g.status, DEV_TC_WAIT);
+                abort_s = 1;
+            }
+            mma_commit(done);
+            mbar_wait(done, 0, nullptr);
+        }
+    } else {
+        const int q = warp & 3;   // the TMEM lane quarter this warp may read
+        // the TMEM loads below are warp-collective: every lane takes the same branch
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(tfull, 0, &abort_s));
+        if (ok) {
+            tc_fence_after();
+            const int row = tile_m * BM + q * 32 + lane;
+            float v[32];
+#pragma unroll 1
+            for (int c = 0; c < BNG / 32; ++c) {
+                tmem_ld32(tmem + ((unsigned)(q * 32) << 16) + (unsigned)(c * 32), v);
+                if (row < g.M) {
+                    float *crow = g.C + (long long)row * g.ldc;
+                    const int col0 = tile_n * BNG + c * 32;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (col0 + i < g.N) crow[col0 + i] = v[i] + (g.bias ? g.bias[col0 + i] : 0.f);
+                }
+            }
+        } else if (lane == 0) {
+            atomicExch(g.status, DEV_TC_WAIT);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BNG) : "memory");
+    }
+}
+
 }  // namespace tc
 
 // ---------------------------------------------------------------------------
@@ -568,6 +703,50 @@ cudaError_t launch_tc_shortlist(int kind, int W, const void *a_mat, long long a_
         if (W == 32) return launch_w<1, 32>(ma, mp, a, node_tiles, st);
     }
     return cudaErrorInvalidValue;
+}
+
+namespace {
+template <int BNG>
+cudaError_t launch_gemm_bn(const CUtensorMap &ma, const CUtensorMap &mb, const TcGemmArgs &g, cudaStream_t st) {
+    // alignment slack, the 4-stage ring, 10 mbarriers
+    constexpr int SMEM = 1024 + 4 * (tc::BM + BNG) * tc::BKB + 10 * 8;
+    static_assert(SMEM <= 232448, "shared memory");
+    auto kern = tc::k_tc_gemm<BNG>;
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 0 || dev >= 64 || !done[dev]) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+            if (e != cudaSuccess) return e;
+            if (dev >= 0 && dev < 64) done[dev] = true;
+        }
+    }
+    dim3 grid((unsigned)((g.M + tc::BM - 1) / tc::BM), (unsigned)((g.N + BNG - 1) / BNG));
+    kern<<<grid, 192, SMEM, st>>>(ma, mb, g);
+    return cudaGetLastError();
+}
+}  // namespace
+
+int tc_gemm_bn(int N) { return N <= 64 ? 64 : N <= 128 ? 128 : 256; }
+
+cudaError_t launch_tc_gemm(const void *a_bf16, long long a_rows, const void *b_bf16, long long b_rows,
+                           const TcGemmArgs &g, cudaStream_t st) {
+    if (g.M <= 0 || g.N <= 0) return cudaSuccess;
+    const int BNG = tc_gemm_bn(g.N);
+    // operands are padded: rows to the tile, K to whole 64-element blocks
+    if (g.kpad <= 0 || g.kpad % 64 || a_rows % tc::BM || b_rows % BNG || a_rows < g.M || b_rows < g.N)
+        return cudaErrorInvalidValue;
+    CUtensorMap ma, mb;
+    cudaError_t e;
+    if ((e = make_map(&ma, a_bf16, 2, g.kpad, a_rows, tc::BM)) != cudaSuccess) return e;
+    if ((e = make_map(&mb, b_bf16, 2, g.kpad, b_rows, BNG)) != cudaSuccess) return e;
+    if (BNG == 64) return launch_gemm_bn<64>(ma, mb, g, st);
+    if (BNG == 128) return launch_gemm_bn<128>(ma, mb, g, st);
+    return launch_gemm_bn<256>(ma, mb, g, st);
 }
 
 }  // namespace qsk

@@ -475,6 +475,16 @@ int qsk_encoder_input_dim(const qsk_encoder *e);
  * once per scale.  Applies to pairs added and pattern matrices built
  * afterwards. */
 int qsk_encoder_set_scales(qsk_encoder *e, int nscales, float cov_min);
+/* Matrix products of the encoder's layers (forward and backward): on = 1
+ * (default) on the tensor cores (tcgen05, operands rounded to BF16, FP32
+ * accumulation), on = 0 on the CUDA cores in FP32.  The InfoNCE logits and
+ * their gradient (B x B x 64 products), parameters, Adam state and
+ * activations are FP32 either way. */
+int qsk_encoder_set_tensor_cores(qsk_encoder *e, int on);
+/* The encoder's tensor-core product on its own (host arrays, row-major):
+ * C[M x N] = bf16(A)[M x K] * bf16(B)[N x K]^T (+ bias[N] when not NULL),
+ * FP32 accumulation; operands rounded to nearest-even BF16. */
+int qsk_gemm_bf16(int device, int M, int N, int K, const float *A, const float *B, const float *bias, float *C);
 /* All parameters, flattened: W1 (256 x D0), b1, W2 (256 x 256), b2, W3, b3,
  * W4q (64 x 256), b4q (query head), W4p, b4p (TI-pattern head); weights
  * row-major (out x in).  set resets Adam. */

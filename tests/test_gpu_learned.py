@@ -12,7 +12,9 @@ pytestmark = pytest.mark.gpu
 
 
 def test_encoder_gradient_matches_oracle(g2s, gpu):
-    enc = g2s.Encoder(nvar=2, seed=7)
+    """FP32 products on the CUDA cores: the gradient of every parameter
+    block within 1e-3 (relative norm) of the float64 oracle."""
+    enc = g2s.Encoder(nvar=2, seed=7).set_tensor_cores(False)
     assert enc.input_dim == 64 * 6
     w = enc.weights()
     rng = np.random.default_rng(1)
@@ -32,12 +34,39 @@ def test_encoder_gradient_matches_oracle(g2s, gpu):
 
 
 def test_encoder_embedding_matches_oracle_forward(g2s, gpu):
-    enc = g2s.Encoder(nvar=1, seed=3)
+    enc = g2s.Encoder(nvar=1, seed=3).set_tensor_cores(False)
     x = np.random.default_rng(4).standard_normal((300, enc.input_dim)).astype(np.float32)
     for head in ("query", "pattern"):
         y = enc.embed(x, head)
         ref, _ = eo.forward(enc.weights().astype(np.float64), x, enc.input_dim, head)
         assert np.abs(y - ref).max() < 1e-4 * max(1.0, np.abs(ref).max())
+    enc.close()
+
+
+def test_encoder_tensor_cores_match_oracle_at_bf16_precision(g2s, gpu):
+    """The default mode: every product on the tensor cores (operands rounded
+    to BF16, FP32 accumulation).  Embeddings within 2 % of the largest
+    float64 oracle value, the loss within 1 % and every parameter block's
+    gradient within 5 % (relative norm): the rounding of BF16 operands,
+    not a layout error (which is O(1))."""
+    enc = g2s.Encoder(nvar=2, seed=7)
+    w = enc.weights().astype(np.float64)
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((300, enc.input_dim)).astype(np.float32)
+    for head in ("query", "pattern"):
+        ref, _ = eo.forward(w, x, enc.input_dim, head)
+        assert np.abs(enc.embed(x, head) - ref).max() < 2e-2 * np.abs(ref).max()
+    B = 64
+    xq = rng.standard_normal((B, enc.input_dim)).astype(np.float32)
+    xp = (xq + 0.5 * rng.standard_normal(xq.shape)).astype(np.float32)
+    loss, g = enc.loss_grad(xq, xp, tau=0.5)
+    loss_ref, g_ref = eo.loss_grad(w, xq, xp, tau=0.5)
+    assert abs(loss - loss_ref) <= 1e-2 * abs(loss_ref)
+    off, n = eo.layout(enc.input_dim)
+    for b in range(eo.NBLOCKS):
+        a, r = g[off[b]:off[b + 1]].astype(np.float64), g_ref[off[b]:off[b + 1]]
+        rel = np.linalg.norm(a - r) / max(np.linalg.norm(r), 1e-12)
+        assert rel < 5e-2, (b, rel)
     enc.close()
 
 

@@ -102,3 +102,29 @@ def test_tc_topk_exact_integer_data(g2s, gpu, fmt, K, W, ranges):
         got_all = sorted({(int(k), int(p)) for k, p in zip(keys[b].ravel(), pos[b].ravel()) if k != 0},
                          key=lambda t: -t[0])[:W]
         assert got_all == allg
+
+
+def bf16_round(x):
+    """Round float32 to the nearest-even BF16 value (as float64)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (5, 7, 3), (130, 70, 100), (300, 257, 384), (1024, 64, 2048),
+                                   (17, 384, 256), (256, 256, 64), (129, 128, 65)])
+def test_gemm_bf16_matches_float64_of_rounded_operands(g2s, gpu, M, N, K):
+    """The encoder's tcgen05 product: every output of bf16(A) bf16(B)^T +
+    bias within the FP32-accumulation bound of the float64 product (edges of
+    the 128-row, 64/128/256-column tiles and of the 64-element K blocks)."""
+    rng = np.random.default_rng(M * 7919 + N * 31 + K)
+    a = rng.standard_normal((M, K)).astype(np.float32)
+    b = rng.standard_normal((N, K)).astype(np.float32)
+    bias = rng.standard_normal(N).astype(np.float32)
+    c = g2s.gemm_bf16(a, b, bias)
+    ar, br = bf16_round(a), bf16_round(b)
+    ref = ar @ br.T + bias.astype(np.float64)
+    scale = np.abs(ar) @ np.abs(br).T + np.abs(bias)
+    assert np.all(np.abs(c - ref) <= 2e-4 * scale + 1e-6)
+    c0 = g2s.gemm_bf16(a, b)
+    assert np.all(np.abs(c0 - (ar @ br.T)) <= 2e-4 * (np.abs(ar) @ np.abs(br).T) + 1e-6)
