@@ -254,8 +254,11 @@ def train_encoder(g2s, w, dev):
                  "epochs": t["epochs"], "batch": t["batch"], "loss": loss, "pair_s": t1 - t0, "train_s": t2 - t1}
 
 
-def set_path(sim, path, enc=None, audit=0.01):
-    if path in ("bf16", "fp8"):
+def set_path(sim, path, enc=None, audit=0.01, tuned=None):
+    if path in ("bf16", "fp8") and tuned:
+        from g2s_b200 import autotune as at
+        at.apply(sim, tuned, mode=path, audit=audit)
+    elif path in ("bf16", "fp8"):
         sim.set_tensor(path, audit=audit)
     elif path == "learned":
         sim.set_learned(enc, shortlist=256, audit=audit)
@@ -332,10 +335,10 @@ def run_step(sim, w, done, sample):
     return sim.info()
 
 
-def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flush, enc=None):
+def time_path(g2s, w, ti, di, done, sample, seed, dev, path, steps, warmup, flush, enc=None, tuned=None):
     """Timed steps of one path; returns (total device ms, per-step infos, profiled info)."""
     sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
-    set_path(sim, path, enc)
+    set_path(sim, path, enc, tuned=tuned)
     g2s.set_map_mode(1 if path == "fp32" else 0)
     import torch
     for _ in range(max(warmup, 0)):
@@ -524,6 +527,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / fp32 comparison arms")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="whole-simulation tensor workloads: the automatic settings instead of the autotuner's")
     ap.add_argument("--grid", type=int, default=0,
                     help="profiling only: simulation grid side (2-D whole-simulation workloads); not a bench line")
     args = ap.parse_args()
@@ -564,6 +569,16 @@ def main():
     enc, enc_info = (train_encoder(g2s, w, dev) if path == "learned" else (None, None))
     if enc_info:
         log(f"encoder trained: {enc_info}")
+    # whole simulations on the tensor-core form: width, prefix tile and batch
+    # from the autotuner (tuned on a smaller grid of the same shape, untimed)
+    tuned, tune_s = None, 0.0
+    if path in ("bf16", "fp8") and not w.get("sample") and not args.no_tune:
+        from g2s_b200 import autotune as at
+        t0 = time.perf_counter()
+        tuned = at.tune(ti, w["types"], w["n"], w["k"], mode=path, device=dev,
+                        cache=os.path.join(tempfile.gettempdir(), f"g2s_b200_tune_{os.getpid()}.json"))
+        tune_s = time.perf_counter() - t0
+        log(f"tuned: {tuned}")
 
     # headline path: K timed steps (CUDA events inside the engine, first to
     # last kernel of each step on its stream), L2 flushed between steps
@@ -571,7 +586,7 @@ def main():
         if dist:
             dist.barrier()
         total_ms, infos, pinf = time_path(g2s, w, ti, di, done, sample, seed, dev, path, args.steps, args.warmup,
-                                          flush, enc)
+                                          flush, enc, tuned)
         if dist:
             dist.barrier()
     clocks = clk.summary()
@@ -670,15 +685,18 @@ def main():
         t0 = time.perf_counter()
         if w.get("sample"):
             sim = g2s.Simulation(ti, di, w["types"], n=w["n"], k=w["k"], seed=seed, device=dev)
-            set_path(sim, path, enc)
+            set_path(sim, path, enc, tuned=tuned)
             sim.run_teacher_nodes(done, sample)
             _, _, cells = sim.read()
             sim.close()
             h2d, d2h = ti.nbytes + done.nbytes + di.nbytes + sample.nbytes, int(done.nbytes + di.size * 4 + cells.nbytes)
         else:
             d = np.full(di.shape, np.nan, np.float32)
-            g2s.qs(ti, d, w["types"], k=w["k"], n=w["n"], s=seed, device=dev,
-                   tensor=path if path in ("bf16", "fp8") else None)
+            tensor = None
+            if path in ("bf16", "fp8"):
+                tensor = dict(mode=path, prefix=tuned["prefix"], width=tuned["width"],
+                              batch=tuned["batch"]) if tuned else path
+            g2s.qs(ti, d, w["types"], k=w["k"], n=w["n"], s=seed, device=dev, tensor=tensor)
             h2d, d2h = ti.nbytes + di.nbytes, int(di.nbytes + di.size * 4)
         torch.cuda.synchronize()
         e2e_vals.append(time.perf_counter() - t0)
@@ -711,7 +729,10 @@ def main():
             "config": {"workload": w["name"], "path": path,
                        "tensor": {"prefix": last["tensor_prefix"], "width": last["tensor_width"],
                                   "shortlist": last["tensor_shortlist"], "tensor_nodes": last["tensor_nodes"],
-                                  "exact_map_nodes": last["plain_nodes"], "audit_fraction": 0.01} if tensor else None,
+                                  "exact_map_nodes": last["plain_nodes"], "audit_fraction": 0.01,
+                                  "autotuned": {k2: tuned[k2] for k2 in ("width", "prefix", "batch", "ms", "runs",
+                                                                         "grid", "ok")} if tuned else None,
+                                  "tuning_s": tune_s} if tensor else None,
                        "learned": {"encoder": enc_info, "shortlist": 256, "confidence": "fit R^2 >= 0.2, z = 2",
                                    "confident_nodes": int(last["tensor_nodes"] - last["learned_fallback"]),
                                    "fallback_nodes": int(last["learned_fallback"]),

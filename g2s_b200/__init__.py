@@ -672,14 +672,15 @@ def tc_topk(queries: np.ndarray, rows: np.ndarray, fmt: int, X: int, Y: int, box
 
 def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
        ki=None, nV: bool = False, ni: Optional[np.ndarray] = None, kvi: Optional[np.ndarray] = None,
-       kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0, tensor: Optional[str] = None,
+       kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0, tensor=None,
        audit: float = 0.01):
     """QuickSampling on one GPU; arguments named after the G2S flags
     (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii -fs).  ``n`` is one count or one
     per variable; ``ki`` one kernel or a list of kernels (selected per cell by
     ``kii``).  ``tensor`` selects the tensor-core form of the map ("bf16" or
-    "fp8", with the regret audit fraction ``audit``); None is the exact
-    reference path.  Returns (simulation, index) as G2S does."""
+    "fp8", or a dict {"mode", "prefix", "width", "shortlist", "batch"} such as
+    the autotuner's choice), with the regret audit fraction ``audit``; None is
+    the exact reference path.  Returns (simulation, index) as G2S does."""
     n_list = None
     if np.ndim(n) > 0:
         n_list = [int(x) for x in np.ravel(n)]
@@ -690,7 +691,10 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     sim = Simulation(ti, di, dt, n=n if n is not None else 0, k=k, seed=s, kernel=kernel, device=device,
                      no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii, full=fs)
     try:
-        if tensor:
+        if isinstance(tensor, dict):
+            sim.set_tensor(tensor["mode"], prefix=int(tensor.get("prefix", 0)), width=int(tensor.get("width", 0)),
+                           shortlist=int(tensor.get("shortlist", 0)), batch=int(tensor.get("batch", 0)), audit=audit)
+        elif tensor:
             sim.set_tensor(tensor, audit=audit)
         sim.run()
         out, idx, _ = sim.read()

@@ -10,9 +10,9 @@ GPU.  Tuning runs the simulation of that shape on a tuning grid (by default
 (after an untimed run that builds each prefix's pattern matrix) and keeps
 the fastest by device time whose regret audit (every node re-run on the
 plain path) stays within ``max_regret``; only a candidate that would
-replace the best (and the automatic choice) is audited.  The search is a coordinate descent from the
-automatic choice: width, then prefix, then batch, each over its candidates
-with the others held.
+replace the best (and the automatic choice) is audited.  The search is a
+coordinate descent from the automatic choice: width, then prefix, then
+batch, each over its candidates with the others held.
 
 The reference has no counterpart: G2S's throughput knobs are the thread
 counts of `-j` (src/qs.cpp), chosen by the user.
@@ -27,7 +27,7 @@ import numpy as np
 
 WIDTHS = (8, 16, 32)
 BATCHES = (2048, 4096, 8192)
-PREFIX_SCALES = (0.5, 1.0, 2.0)   # times the automatic prefix, rounded to 64 offsets
+PREFIX_SCALES = (0.125, 0.25, 0.5, 1.0, 2.0)   # times the automatic prefix, rounded to 64 offsets
 
 
 def default_cache() -> str:

@@ -661,6 +661,11 @@ struct qsk_sim {
     // generator states are prepared on st_rng while st runs the map
     cudaStream_t st_rng = nullptr;
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
+    // tensor-core form: a level's exact-map steps run on st2 beside its
+    // tensor steps on st (ev_level: the level's start on st; ev_side: the
+    // end of st2's work, which the next level waits for)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_level = nullptr, ev_side = nullptr;
     qsk_ti *ti = nullptr;
     int nd = 0, nvar = 0, n = 0, K = 1;
     float k = 1.f;
@@ -951,6 +956,7 @@ struct Step {
     int off, B;
     int kb_off;         // TENSOR: this step's tile K-blocks in d_tc_kb
     int scale = 1;      // TENSOR, learned proposal: the nodes' stencil scale
+    int level = -1;     // tensor-core form: the dependency level (-1: one stream for all steps)
 };
 
 int tc_step(qsk_sim *s, const Step &st, bool teacher);
@@ -1035,10 +1041,29 @@ int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
     int rc = pl.empty() ? QSK_OK : launch_rng(0);
     if (rc) return rc;
     size_t j = 0;   // plain / audit step counter
+    // tensor-core form: the exact-map steps of a level (its nodes beyond the
+    // prefix) run on st2 while its tensor steps run on st; the nodes of a
+    // level are independent (they read earlier levels only and write their
+    // own cells) and the two kinds of step share no scratch.  A level
+    // starts when both streams have finished the one before.
+    int cur_level = -1, side_level = -1;
+    bool side_pending = false;
     for (const Step &step : steps) {
+        if (step.level >= 0 && step.level != cur_level) {
+            if (side_pending) CK(cudaStreamWaitEvent(s->st, s->ev_side, 0));
+            side_pending = false;
+            CK(cudaEventRecord(s->ev_level, s->st));
+            cur_level = step.level;
+        }
         if (step.kind == STEP_TENSOR) {
             if ((rc = tc_step(s, step, teacher)) != QSK_OK) return rc;
             continue;
+        }
+        const bool side = step.kind == STEP_HASH && step.level >= 0;
+        cudaStream_t ws = side ? s->st2 : s->st;
+        if (side && side_level != step.level) {
+            CK(cudaStreamWaitEvent(s->st2, s->ev_level, 0));
+            side_level = step.level;
         }
         const int B = step.B, p = int(j & 1);
         const bool audit = step.kind == STEP_AUDIT;
@@ -1046,12 +1071,12 @@ int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
         ++j;
         {
             Slot *slots = bits ? s->d_sslots.p + size_t(p) * s->max_slots : s->d_slots.p;
-            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
-            if (!bits) CK(launch_prep_sim(prep_args(step.nodes, step.off, B), s->st));
-            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), ws));
+            if (!bits) CK(launch_prep_sim(prep_args(step.nodes, step.off, B), ws));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), ws));
             if (bits) {
                 // the slots and static terms of this batch come from k_mt_prep
-                CK(cudaStreamWaitEvent(s->st, s->ev_ready[p], 0));
+                CK(cudaStreamWaitEvent(ws, s->ev_ready[p], 0));
                 BitArgs ba;
                 ba.g = g;
                 ba.planes = s->ti->planes.p;
@@ -1072,7 +1097,7 @@ int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
                 ba.rec_idx = s->d_rec_idx.p;
                 ba.rec_cnt = s->d_rec_cnt.p;
                 ba.rec_max = s->d_rec_max.p;
-                CK(launch_map_bits(ba, B, s->K, s->maxterms, s->st));
+                CK(launch_map_bits(ba, B, s->K, s->maxterms, ws));
             } else {
                 MapArgs ma;
                 ma.g = g;
@@ -1085,9 +1110,9 @@ int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
                 ma.rec_idx = s->d_rec_idx.p;
                 ma.rec_cnt = s->d_rec_cnt.p;
                 ma.rec_max = s->d_rec_max.p;
-                CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+                CK(launch_map_records(ma, B, s->K, s->maxterms, ws));
             }
-            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), ws));
             s->info.launches += bits ? 3 : 4;
             s->info.map_launches += 1;
             s->info.map_positions += (long long)B * g.N;
@@ -1117,19 +1142,24 @@ int sim_batches(qsk_sim *s, const std::vector<Step> &steps, bool teacher) {
             ra.full = s->full ? 1 : 0;
             ra.mt_state = s->d_mt_state.p + p * mt_words;
             ra.mt_pre = s->d_mt_pre.p + size_t(p) * s->max_slots;
-            CK(cudaStreamWaitEvent(s->st, s->ev_ready[p], 0));
+            CK(cudaStreamWaitEvent(ws, s->ev_ready[p], 0));
             if (step.kind == STEP_HASH) {
                 ra.drawn_score = s->d_drawn_score.p;
                 ra.drawn_scale = s->d_drawn_scale.p;
-                CK(launch_hash_select(ra, s->st));
+                CK(launch_hash_select(ra, ws));
                 ra.only_flagged = 1;
                 s->info.launches += 1;
             }
-            CK(launch_replay(ra, s->st));
-            CK(cudaEventRecord(s->ev_used[p], s->st));
-            if (s->profiling) CK(cudaEventRecord(prof_event(s), s->st));
+            CK(launch_replay(ra, ws));
+            CK(cudaEventRecord(s->ev_used[p], ws));
+            if (s->profiling) CK(cudaEventRecord(prof_event(s), ws));
+            if (side) {
+                CK(cudaEventRecord(s->ev_side, s->st2));
+                side_pending = true;
+            }
         }
     }
+    if (side_pending) CK(cudaStreamWaitEvent(s->st, s->ev_side, 0));
     return QSK_OK;
 }
 
@@ -1461,6 +1491,7 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
                 const int B = std::min(s->max_tc_slots, g1 - off);
                 Step st{STEP_TENSOR, s->d_level_nodes.p, start[l] + off, B, int(kb.size())};
                 st.scale = learned ? esc[size_t(off)] : 1;
+                st.level = int(l);
                 for (int t0 = 0; t0 < B; t0 += 128) {
                     const int last = el[size_t(off + std::min(B, t0 + 128) - 1)];
                     const int k = learned ? 1 : int((((long long)tmax[size_t(last)] + 1) * L + kbe - 1) / kbe);
@@ -1471,9 +1502,14 @@ int tc_plan(qsk_sim *s, const std::vector<int> &start, const std::vector<int> &t
             }
             g0 = g1;
         }
-        for (int off = 0; off < int(pl.size()); off += s->max_slots)
-            steps.push_back({STEP_HASH, s->d_level_nodes.p, start[l] + int(el.size()) + off,
-                             std::min(s->max_slots, int(pl.size()) - off), 0});
+        for (int off = 0; off < int(pl.size()); off += s->max_slots) {
+            Step st{STEP_HASH, s->d_level_nodes.p, start[l] + int(el.size()) + off,
+                    std::min(s->max_slots, int(pl.size()) - off), 0};
+            // the learned proposal's fallback uses the exact map's buffers
+            // inside its tensor steps: its levels stay on one stream
+            st.level = learned ? -1 : int(l);
+            steps.push_back(st);
+        }
         ntc += (long long)el.size();
         npl += (long long)pl.size();
         if (athr) {
@@ -2005,6 +2041,9 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         return bail(fail(QSK_ERR_UNSUPPORTED, "-fs with missing training-image values is not implemented"));
     cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st_rng, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_level, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_side, cudaEventDisableTiming);
     for (int p = 0; p < 2 && e == cudaSuccess; ++p) {
         e = cudaEventCreateWithFlags(&s->ev_ready[p], cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_used[p], cudaEventDisableTiming);
@@ -2596,6 +2635,9 @@ int qsk_sim_destroy(qsk_sim *s) {
             if (s->ev_ready[p]) cudaEventDestroy(s->ev_ready[p]);
             if (s->ev_used[p]) cudaEventDestroy(s->ev_used[p]);
         }
+        if (s->ev_level) cudaEventDestroy(s->ev_level);
+        if (s->ev_side) cudaEventDestroy(s->ev_side);
+        if (s->st2) cudaStreamDestroy(s->st2);
         if (s->st_rng) cudaStreamDestroy(s->st_rng);
         if (s->st) cudaStreamDestroy(s->st);
         s->st = nullptr;

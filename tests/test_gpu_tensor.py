@@ -93,6 +93,29 @@ def test_tensor_deterministic_and_options(g2s, gpu):
         run(g2s, g["ti"], g["di"], [0], 20, 1.2, 100, "bf16", width=12)
 
 
+@pytest.mark.parametrize("kind", ["channels", "grf"])
+def test_exact_map_nodes_beside_tensor_nodes_in_every_level(g2s, gpu, kind):
+    """A short prefix gives every level tensor-path nodes and exact-map nodes
+    (neighbours beyond the prefix), which run side by side on two streams.
+    Two runs give the same grid bit for bit, and the audit of every node
+    (plain path, teacher-forced) finds the draws within the exact k best."""
+    if kind == "channels":
+        ti, types, n = syn.channels2d((120, 120), n_channels=8, seed=3), [1], 40
+    else:
+        ti, types, n = syn.grf((120, 120), (8, 8), seed=3), [0], 30
+    di = np.full((160, 160), np.nan, np.float32)
+    (a, ia, _), inf_a = run(g2s, ti, di, types, n, 1.5, 7, "bf16", audit=1.0, prefix=256)
+    (b, ib, _), inf_b = run(g2s, ti, di, types, n, 1.5, 7, "bf16", audit=1.0, prefix=256)
+    print(kind, {k: inf_a[k] for k in ("tensor_nodes", "plain_nodes", "levels", "audited", "regret", "regret_near")})
+    assert inf_a["plain_nodes"] > 0.05 * inf_a["tensor_nodes"] and inf_a["tensor_nodes"] > 0
+    assert np.array_equal(a, b, equal_nan=True) and np.array_equal(ia, ib)
+    assert inf_a["audited"] > 0.9 * 160 * 160
+    if kind == "channels":
+        assert inf_a["regret"] == 0   # 0/1 indicators: exact in BF16
+    else:
+        assert inf_a["regret"] <= 0.01 * inf_a["audited"]
+
+
 def test_tensor_config1_full_size(g2s, gpu):
     """Config 1 (channels 250x250 -> 500x500, n=80, k=1.5) on the BF16 form:
     exact counts, so no regret; values from the TI, facies proportion kept."""
