@@ -770,6 +770,137 @@ NodeResult run_node_full(const Problem &P, const Path &path, const float *state,
     return r;
 }
 
+/* Several training images (-ti with more than one grid), one node, as G2S
+ * runs it with one accelerator device per TI (src/qs.cpp:1560-1598):
+ *  - no informed neighbour and no centre value: the marginal draw over the
+ *    TIs' cells laid end to end (simulation.hpp:586-610);
+ *  - otherwise every TI (or only the cell's TI of the -ii image,
+ *    simulation.hpp:560, samplingModule.hpp:70-73; QS leaves nodes without
+ *    neighbours to the marginal draw) reports its K best with the same seed
+ *    (quantileSamplingModule.hpp:455-575), scored as the CUDA device reports
+ *    them: the map plus the constant delta = sum over continuous variables
+ *    and informed neighbours of -1 * (w * v * v) in the reference's float
+ *    order (quantileSamplingModule.hpp:412-457, DataImage.hpp:660-676);
+ *  - the TIs x K candidates are sorted by score with std::sort (the same
+ *    call and comparator as quantileSamplingModule.hpp:101-104), the rank
+ *    drawn with the TI count (:113) names the TI (rank / K) and the
+ *    candidate.
+ * Complete TIs only. */
+struct MultiResult {
+    unsigned ti;
+    unsigned cell;
+    int marginal;
+    int near_tie;   /* FP64: an adjacent gap among the merged top-(K+1) within tol of the term scale */
+};
+
+MultiResult run_node_multi(const std::vector<Grid> &tis, const std::vector<const float *> &tivals, const Grid &di,
+                           const int *types, const KernelTpl &KT, int n, float k, const Path &path, const float *state,
+                           unsigned idx_path, const float *ii, bool own_cell_unknown, bool want_fp64, double tol) {
+    MultiResult r{0u, 0u, 0, 0};
+    const unsigned cell = path.order[path.begin + idx_path];
+    const unsigned order = path.posterior[cell];
+    const float seed = path.seeds[idx_path];
+    const int nvar = di.nvar;
+    auto value = [&](unsigned c, int v) -> float {
+        if (own_cell_unknown && c == cell) return NAN;
+        return state[size_t(c) * nvar + v];
+    };
+    std::vector<int> tix(size_t(std::max(n, 1)));
+    std::vector<unsigned> ncell(size_t(std::max(n, 1)));
+    const int cnt = neighbours(di, KT.tpl, path.posterior.data(), cell, order, n, tix.data(), ncell.data());
+    bool withDataInCenter = false;
+    for (int v = 0; v < nvar; ++v) withDataInCenter |= !std::isnan(value(cell, v));
+    if (cnt <= 1 && !withDataInCenter) {
+        r.marginal = 1;
+        unsigned cumulated = 0;
+        for (const Grid &t : tis) cumulated += unsigned(t.cells()) * unsigned(nvar);
+        const unsigned position = unsigned(int(std::floor(double(seed * float(cumulated / unsigned(nvar))))));
+        cumulated = 0;
+        for (size_t t = 0; t < tis.size(); ++t) {
+            const unsigned size = unsigned(tis[t].cells()) * unsigned(nvar);
+            if (position * unsigned(nvar) < cumulated + size) {
+                r.ti = unsigned(t);
+                r.cell = position - cumulated / unsigned(nvar);
+                break;
+            }
+            cumulated += size;
+        }
+        return r;
+    }
+    std::vector<int> offs(size_t(cnt) * di.nd);
+    std::vector<float> vals(size_t(cnt) * nvar);
+    for (int j = 0; j < cnt; ++j) {
+        for (int d = 0; d < di.nd; ++d) offs[j * di.nd + d] = KT.tpl[tix[j]][d];
+        for (int v = 0; v < nvar; ++v) vals[j * nvar + v] = value(ncell[j], v);
+    }
+    float delta = 0.f;
+    for (int i = 0; i < nvar; ++i) {
+        if (types[i] != 0) continue;
+        for (int j = 0; j < cnt; ++j) {
+            const float v = vals[j * nvar + i];
+            if (std::isnan(v)) continue;
+            const float w = kweight(KT.kg, KT.kernel, offs.data() + j * di.nd, i);
+            delta += -1.f * (w * v * v);
+        }
+    }
+    const int req = ii ? int(ii[cell]) : -1;
+    const unsigned nti = unsigned(tis.size());
+    const unsigned short K = (unsigned short)int(std::ceil(k));
+    std::vector<float> errors(size_t(nti) * K, -INFINITY);
+    std::vector<unsigned> enc(size_t(nti) * K, 0u);
+    std::vector<Node> nodes(nti);
+    std::vector<Scan> scans(nti);
+    for (unsigned t = 0; t < nti; ++t) {
+        if (req >= 0 && int(t) != req) continue;
+        nodes[t] = build_node(tis[t], types, KT.kg, KT.kernel, cnt, offs.data(), vals.data());
+        scans[t] = make_scan(tis[t], nodes[t]);
+        std::vector<float> map(scans[t].N);
+        map_fp32(tis[t], tivals[t], nodes[t], scans[t], map.data());
+        std::vector<float> ev(K);
+        std::vector<unsigned> ep(K);
+        kbiggest(map.data(), unsigned(scans[t].N), K, seed, ev.data(), ep.data());
+        for (int j = 0; j < K; ++j) {
+            errors[size_t(t) * K + j] = ev[j] + delta;
+            enc[size_t(t) * K + j] = ep[j];
+        }
+    }
+    std::vector<unsigned> lp(errors.size());
+    std::iota(lp.begin(), lp.end(), 0u);
+    const float *e = errors.data();
+    std::sort(lp.begin(), lp.end(), [e](unsigned a, unsigned b) { return e[a] > e[b]; });
+    const unsigned sel = selected_index(seed, k, nti);
+    const unsigned t = lp[sel] / K;
+    r.ti = t;
+    r.cell = index_to_position(scans[t], tis[t], nodes[t], enc[lp[sel]]);
+    if (want_fp64) {
+        /* the FP64 scores of every updated TI's top K+1, merged */
+        std::vector<std::pair<double, double>> top;   /* (score, term scale) */
+        for (unsigned u = 0; u < nti; ++u) {
+            if (req >= 0 && int(u) != req) continue;
+            std::vector<double> m64(scans[u].N), s64(scans[u].N);
+            map_fp64(tis[u], tivals[u], nodes[u], scans[u], m64.data(), s64.data());
+            std::vector<long> ord(scans[u].N);
+            std::iota(ord.begin(), ord.end(), 0L);
+            const size_t m = std::min<size_t>(size_t(K) + 1, ord.size());
+            std::partial_sort(ord.begin(), ord.begin() + m, ord.end(), [&](long a, long b) { return m64[a] > m64[b]; });
+            for (size_t j = 0; j < m; ++j) top.push_back({m64[ord[j]], s64[ord[j]]});
+        }
+        std::sort(top.begin(), top.end(), [](const std::pair<double, double> &a, const std::pair<double, double> &b) {
+            return a.first > b.first;
+        });
+        const size_t m = std::min<size_t>(size_t(K) + 1, top.size());
+        double scale = 0.0;
+        for (size_t j = 0; j < m; ++j) scale = std::max(scale, top[j].second);
+        double gmin = INFINITY;
+        for (size_t j = 0; j + 1 < m; ++j) {
+            const double g = top[j].first - top[j + 1].first;
+            gmin = std::min(gmin, scale > 0 ? g / scale : g);
+        }
+        r.near_tie = gmin <= tol;
+    }
+    return r;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1041,6 +1172,81 @@ long orc_pattern_map(int nd, const unsigned *ti_dims, int nvar, const int *types
     return sc.N;
 }
 
+
+/* Vector QS simulation with several training images: nti TIs of the same
+ * nvar (dims per TI, x first, in ti_dims[t*nd..]), the default uniform
+ * kernel of size min over TIs of (dims/2 + 1) per dimension
+ * (src/qs.cpp:1010-1042) or the given kernel, one neighbour count; ii
+ * (optional, per DI cell) the -ii image.  mode 0: di simulated in place,
+ * out_id the index image, TI cell * nti + TI (simulation.hpp:658); mode 1:
+ * every path node teacher-forced against the completed grid di, the path
+ * built from di_init, with the FP64 near-tie flag (tol of the term scale).
+ * Per path node: chosen TI and TI cell, near-tie and marginal flags.
+ * Returns the path nodes, -1 for a TI with missing values. */
+long orc_simulate_multi(int mode, int nd, int nti, const unsigned *ti_dims, int nvar, const int *types,
+                        const float *const *ti, const unsigned *di_dims, float *di, const float *di_init,
+                        const unsigned *kdims, const float *kernel, int n, float k, unsigned seed, const float *ii,
+                        double tol, unsigned *out_id, unsigned *out_ti, unsigned *out_cell, int *out_near_tie,
+                        int *out_marginal) {
+    std::vector<Grid> tis((size_t)nti);
+    std::vector<const float *> tivals((size_t)nti);
+    for (int t = 0; t < nti; ++t) {
+        tis[t].nd = nd;
+        tis[t].nvar = nvar;
+        for (int d = 0; d < nd; ++d) tis[t].dims[d] = ti_dims[t * nd + d];
+        tivals[t] = ti[t];
+        for (size_t c = 0; c < tis[t].cells() * size_t(nvar); ++c)
+            if (std::isnan(ti[t][c])) return -1;
+    }
+    Grid dg;
+    dg.nd = nd;
+    dg.nvar = nvar;
+    for (int d = 0; d < nd; ++d) dg.dims[d] = di_dims[d];
+    KernelTpl KT;
+    KT.kg.nd = nd;
+    KT.kg.nvar = nvar;
+    if (kernel) {
+        KT.kernel = kernel;
+        for (int d = 0; d < nd; ++d) KT.kg.dims[d] = kdims[d];
+    } else {
+        for (int d = 0; d < nd; ++d) {
+            unsigned m = ti_dims[d];
+            for (int t = 0; t < nti; ++t) m = std::min(m, ti_dims[t * nd + d] / 2 + 1);
+            KT.kg.dims[d] = m;
+        }
+    }
+    KT.tpl = make_template(nd, KT.kg.dims, KT.kernel, nvar);
+    std::vector<float> state(di, di + dg.cells() * nvar);
+    Path path = make_path(dg, di_init ? di_init : state.data(), seed);
+    const long nodes = long(dg.cells()) - long(path.begin);
+    auto record = [&](long i, const MultiResult &r) {
+        if (out_ti) out_ti[i] = r.ti;
+        if (out_cell) out_cell[i] = r.cell;
+        if (out_near_tie) out_near_tie[i] = r.near_tie;
+        if (out_marginal) out_marginal[i] = r.marginal;
+    };
+    if (mode == 1) {
+        /* teacher forcing: every node against the completed grid di, its own
+         * cell not yet simulated */
+#pragma omp parallel for schedule(dynamic, 16)
+        for (long i = 0; i < nodes; ++i)
+            record(i, run_node_multi(tis, tivals, dg, types, KT, n, k, path, state.data(), unsigned(i), ii, true,
+                                     true, tol));
+        return nodes;
+    }
+    for (long i = 0; i < nodes; ++i) {
+        const unsigned cell = path.order[path.begin + i];
+        MultiResult r = run_node_multi(tis, tivals, dg, types, KT, n, k, path, state.data(), unsigned(i), ii, false,
+                                       false, tol);
+        for (int v = 0; v < nvar; ++v)
+            if (std::isnan(state[size_t(cell) * nvar + v]))
+                state[size_t(cell) * nvar + v] = tivals[r.ti][size_t(r.cell) * nvar + v];
+        if (out_id) out_id[cell] = r.cell * unsigned(nti) + r.ti;
+        record(i, r);
+    }
+    std::copy(state.begin(), state.end(), di);
+    return nodes;
+}
 }  /* extern "C" */
 
 /* ------------------------------------------------------------------ */

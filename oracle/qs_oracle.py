@@ -49,6 +49,11 @@ def lib():
         L.orc_simulate.restype = ctypes.c_long
         L.orc_simulate_ex.argtypes = L.orc_simulate.argtypes + [ctypes.c_void_p]
         L.orc_simulate_ex.restype = ctypes.c_long
+        L.orc_simulate_multi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _u32p, ctypes.c_int, _i32p,
+                                         ctypes.POINTER(ctypes.c_void_p), _u32p, _f32p, _f32p, _u32p, _f32p,
+                                         ctypes.c_int, ctypes.c_float, ctypes.c_uint, _f32p, ctypes.c_double, _u32p,
+                                         _u32p, _u32p, _i32p, _i32p]
+        L.orc_simulate_multi.restype = ctypes.c_long
         L.orc_pattern_map.argtypes = [ctypes.c_int, _u32p, ctypes.c_int, _i32p, _f32p, ctypes.c_int, _i32p, _f32p,
                                       _f32p, _f64p, _f64p, _i32p, _i32p]
         L.orc_pattern_map.restype = ctypes.c_long
@@ -148,6 +153,47 @@ def _controls(cells, n_per_var=None, ni=None, kvi=None, kernels=None, kii=None, 
         c.kii = arr(kii, np.float32)
     keep.append(c)
     return c, keep
+
+
+def simulate_multi(tis, di, types, n, k, seed, ii=None, kernel=None, kdims=None, mode=0, di_init=None, tol=1e-5):
+    """Vector simulation with several training images, as G2S runs it with
+    one accelerator device per TI: per node every TI's k best (or only the
+    -ii image's TI), scored as the CUDA device reports them, merged with
+    std::sort and drawn with the TI count.  mode 0: sequential simulation of
+    ``di``; mode 1: every path node teacher-forced against the completed grid
+    ``di`` (path from ``di_init``) with its FP64 near-tie flag.  Returns
+    dict(sim, id, ti, cell, near_tie, marginal, begin); id = TI cell *
+    len(tis) + TI; the per-node arrays are in path order."""
+    nvar = len(types)
+    dims = [grid_dims(t, nvar) for t in tis]
+    nd = len(dims[0])
+    assert all(len(d) == nd for d in dims)
+    tdims = np.concatenate(dims).astype(np.uint32)
+    arrs = [np.ascontiguousarray(t, dtype=np.float32) for t in tis]
+    ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    ddims = grid_dims(di, nvar)
+    d = np.ascontiguousarray(di, dtype=np.float32).copy()
+    init = d if di_init is None else np.ascontiguousarray(di_init, dtype=np.float32)
+    cells = int(np.prod(ddims))
+    nodes = cells - int(np.sum(~np.isnan(init.reshape(cells, nvar)).any(axis=1)))
+    ty = np.asarray(types, dtype=np.int32)
+    oid = np.zeros(cells, np.uint32)
+    oti = np.zeros(max(nodes, 1), np.uint32)
+    ocell = np.zeros(max(nodes, 1), np.uint32)
+    ont = np.zeros(max(nodes, 1), np.int32)
+    omg = np.zeros(max(nodes, 1), np.int32)
+    iiw = None if ii is None else np.ascontiguousarray(ii, dtype=np.float32).ravel()
+    kd = None if kdims is None else np.asarray(kdims, dtype=np.uint32)
+    kern = None if kernel is None else np.ascontiguousarray(kernel, dtype=np.float32)
+    rc = lib().orc_simulate_multi(int(mode), nd, len(arrs), _p(tdims, _u32p), nvar, _p(ty, _i32p), ptrs,
+                                  _p(ddims, _u32p), _p(d, _f32p), None if di_init is None else _p(init, _f32p),
+                                  _p(kd, _u32p), _p(kern, _f32p), int(n), float(k), int(seed), _p(iiw, _f32p),
+                                  float(tol), _p(oid, _u32p), _p(oti, _u32p), _p(ocell, _u32p), _p(ont, _i32p),
+                                  _p(omg, _i32p))
+    if rc < 0:
+        raise ValueError("orc_simulate_multi: training images with missing values are not supported")
+    return {"sim": d, "id": oid, "ti": oti[:nodes], "cell": ocell[:nodes], "near_tie": ont[:nodes].astype(bool),
+            "marginal": omg[:nodes].astype(bool), "begin": cells - nodes}
 
 
 def simulate(ti, di, types, n, k, seed, mode=0, kernel=None, kdims=None, want_fp64=False, tol=1e-5,

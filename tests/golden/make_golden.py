@@ -7,6 +7,7 @@ reference's own reported compute time).  Needs oracle/_ref/libg2sref.so,
 which is built only where the G2S sources are present:
 
     make -C oracle && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py multi     # several training images
 """
 import os
 import sys
@@ -160,6 +161,48 @@ def main(names=None):
 
 
 
+# several training images in one run (-ti with more than one grid; -ii the TI
+# index image): name -> (TI builders, di shape, types, k, n, seed, ii builder)
+# TI shapes whose spectrum length ny*(nx/2+1) is a multiple of 8 (exact in the
+# reference build)
+MULTI = {
+    "multi_ti": ([lambda: syn.grf((48, 48), (6, 6), seed=11), lambda: syn.grf((40, 40), (6, 6), seed=12)],
+                 (32, 32), [0], 1.2, 12, 7, None),
+    "multi_ti_ii": ([lambda: syn.grf((48, 48), (6, 6), seed=11), lambda: syn.grf((40, 40), (6, 6), seed=12)],
+                    (32, 32), [0], 1.2, 12, 7, lambda: np.repeat((np.arange(32) >= 16)[None, :], 32, 0)),
+    # equal sizes: the reference CPU device's unnormalised scores (N x S)
+    # share one N, so its merge orders candidates as the true scores do
+    "multi_ti_eq": ([lambda: syn.grf((48, 48), (6, 6), seed=11), lambda: syn.grf((48, 48), (6, 6), seed=13)],
+                    (32, 32), [0], 1.5, 12, 8, None),
+    "multi_ti3": ([lambda: syn.grf((40, 40), (5, 5), seed=13), lambda: syn.grf((48, 48), (5, 5), seed=14),
+                   lambda: syn.grf((32, 32), (5, 5), seed=15)], (30, 30), [0], 2.5, 10, 9, None),
+}
+
+
+def make_multi(names=None):
+    """The reference `qs` with several `-ti` grids (and `-ii`): its cross-TI
+    merge of the per-TI k best (quantileSamplingModule.hpp:90-126) and
+    index image `index * nTI + TI` (simulation.hpp:658)."""
+    for name, (mks, dshape, types, k, n, seed, mkii) in MULTI.items():
+        if names and name not in names:
+            continue
+        tis = [mk() for mk in mks]
+        di = np.full(dshape, np.nan, np.float32)
+        images = {"-ti": [(t, types) for t in tis[1:]]}
+        ii = None
+        if mkii is not None:
+            ii = mkii().astype(np.float32)
+            images["-ii"] = [(ii, [0])]
+        sim, idx, ms, _ = ref.run_qs(tis[0], di, types, ["-k", str(k), "-n", str(n), "-s", str(seed), "-j", "1"],
+                                     images=images)
+        extra = {f"ti{i}": t for i, t in enumerate(tis)}
+        if ii is not None:
+            extra["ii"] = ii
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), di=di, types=np.array(types), k=k, n=n, seed=seed,
+                            nti=len(tis), sim=sim, idx=idx, ref_ms=ms, **extra)
+        print(name, [t.shape for t in tis], dshape, "from TI", np.bincount((idx.ravel() % len(tis)).astype(int)))
+
+
 def oracle_teacher_config0():
     """Teacher-forced oracle evaluation of every config-0 path node against the
     reference's completed grid: chosen TI cell and FP64 near-tie flag."""
@@ -183,5 +226,7 @@ if __name__ == "__main__":
         make_full(args[1:])
     elif args == ["bgrid"]:
         make_bgrid()
+    elif args[:1] == ["multi"]:
+        make_multi(args[1:])
     else:
         main(args)

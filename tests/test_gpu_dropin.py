@@ -144,3 +144,50 @@ def test_auto_qs_w_cuda_calibration_agrees_with_oracle(oracle):
     z = np.abs(m1 - m2) / np.sqrt(od[ok].astype(np.float64) ** 4 / on[ok] + rd[ok] ** 4 / rn[ok])
     assert ok.sum() >= 10
     assert np.all(z < 5.0), (z.max(), m1, m2)
+
+
+@pytest.mark.parametrize("name,job", [("multi_ti", 31040), ("multi_ti_ii", 31041), ("multi_ti3", 31042),
+                                      ("multi_ti_eq", 31043)])
+def test_qs_w_cuda_several_training_images_equal_oracle(oracle, name, job):
+    """Several training images (`-ti a b [c]`, and `-ii`, the TI each cell
+    samples from): the unmodified G2S `qs -W_CUDA` gives every TI its own
+    device of this library (src/qs.cpp:1560-1598), asks each for its k best
+    with the same seed and merges them itself (quantileSamplingModule.hpp:
+    90-126; the index image is index * nTI + TI, simulation.hpp:658).  The
+    simulation and index image equal the oracle's several-TI simulation bit
+    for bit (the oracle is pinned to the reference in
+    test_oracle_multi_ti.py)."""
+    from oracle import ref
+    g = golden(name)
+    types = [int(t) for t in g["types"]]
+    nti = int(g["nti"])
+    tis = [f"dropin_ti{i}_{job}" for i in range(nti)]
+    for i, nm in enumerate(tis):
+        ref.write_image(nm, g[f"ti{i}"], types)
+    ref.write_image(f"dropin_di_{job}", g["di"], types)
+    outputs = [str(job), f"id_{job}", f"im_1_{job}", f"im_2_{job}"]
+    _cleanup(outputs)
+    log = f"/tmp/G2S/logs/dropin_{job}.log"
+    cmd = [QS, "-ti", tis[0], "-di", f"dropin_di_{job}", "-k", str(float(g["k"])), "-n", str(int(g["n"])),
+           "-s", str(int(g["seed"])), "-j", "1", "-W_CUDA", "0", "-id", str(job), "-r", log]
+    for nm in tis[1:]:
+        cmd += ["-ti", nm]
+    extra = []
+    if "ii" in g:
+        ref.write_image(f"dropin_ii_{job}", g["ii"], [0])
+        cmd += ["-ii", f"dropin_ii_{job}"]
+        extra.append(f"dropin_ii_{job}")
+    r = subprocess.run(cmd, cwd=DROPIN_DIR, capture_output=True, text=True, timeout=600)
+    text = open(log).read() if os.path.exists(log) else ""
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:], text[-2000:])
+    assert "Could not load g2s_cuda.so" not in text
+    sim = ref.read_image(str(job))
+    idx = ref.read_image("id_" + str(job))
+    _cleanup(outputs + tis + [f"dropin_di_{job}"] + extra)
+    if idx.dtype != np.uint32:
+        idx = idx.view(np.uint32)
+    o = oracle.simulate_multi([g[f"ti{i}"] for i in range(nti)], g["di"], types, int(g["n"]), float(g["k"]),
+                              int(g["seed"]), ii=g.get("ii"))
+    assert np.array_equal(sim, o["sim"])
+    assert np.array_equal(idx.ravel(), o["id"])
+    assert len(np.unique(idx.ravel() % nti)) > 1   # candidates come from more than one TI
