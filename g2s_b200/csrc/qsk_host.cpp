@@ -739,6 +739,7 @@ struct qsk_sim {
     DBuf<double> d_err_sum;
     DBuf<unsigned long long> d_err_n;
     int max_tc_slots = 0;
+    int sm_count = 0;                   // SMs of the device (grid sizing of the shortlist kernel)
     // learned proposal (qsk_sim_set_learned): tensor mode 3
     qsk_encoder *enc = nullptr;
     qsk_learned_opts lopt{};
@@ -1720,10 +1721,22 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     CK(launch_tc_nodes(na, s->st));
     if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
     // GEMM shortlist: enough position ranges to fill the GPU, at most
-    // SEL_CAND / W candidates per node
+    // SEL_CAND / W candidates per node.  With a shortlist of at most W the
+    // shared bound makes the ranges' union hold the exact overall top W for
+    // any number of ranges: one wave of CTAs (one per SM), each scanning
+    // more position tiles, saves a second wave's set-up (TMEM allocation,
+    // pipeline fill) on the short levels.  A longer shortlist keeps two
+    // waves' worth of ranges, whose heaps it is drawn from.
+    if (s->sm_count <= 0) {
+        int sms = 0;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device));
+        s->sm_count = std::max(1, sms);
+    }
     const int node_tiles = int(Bp / 128);
     const long long ntiles = s->tc_rows / 256;
-    int ranges = int(std::max<long long>(1, (148LL * 2 + node_tiles - 1) / node_tiles));
+    const long long sms = s->sm_count;
+    int ranges = int(s->tc_S <= s->tc_W ? std::max<long long>(1, sms / node_tiles)
+                                        : std::max<long long>(1, (2 * sms + node_tiles - 1) / node_tiles));
     ranges = int(std::min<long long>({(long long)ranges, ntiles, 768LL / s->tc_W}));
     TcArgs a{};
     a.n_nodes = B;
