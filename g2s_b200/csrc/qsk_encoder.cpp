@@ -49,9 +49,7 @@ int enc_scratch(qsk_encoder *e, long long rows) {
     QSK_CK(e->h2.alloc(r * ENC_H));
     QSK_CK(e->h3p.alloc(r * ENC_H));
     QSK_CK(e->h3.alloc(r * ENC_H));
-    QSK_CK(e->z.alloc(r * ENC_E));
     QSK_CK(e->y.alloc(r * ENC_E));
-    QSK_CK(e->nrm.alloc(r));
     QSK_CK(e->d1.alloc(r * ENC_H));
     QSK_CK(e->d2.alloc(r * ENC_H));
     QSK_CK(e->dz.alloc(r * ENC_E));

@@ -32,7 +32,7 @@ struct qsk_encoder {
     int t = 0;                     // Adam steps taken
     // activations of the last forward pass (rows <= cap)
     long long cap = 0;
-    qsk::DBuf<float> h1p, h1, h2p, h2, h3p, h3, z, y, nrm, d1, d2, dz;
+    qsk::DBuf<float> h1p, h1, h2p, h2, h3p, h3, y, d1, d2, dz;
     qsk::DBuf<float> xb;           // input rows of a batch / an embedding chunk
     qsk::DBuf<float> S, dS, loss;  // batch similarities and their gradient
     // training pairs (device): query and positive feature rows

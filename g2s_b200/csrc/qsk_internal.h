@@ -463,8 +463,6 @@ cudaError_t launch_sgemm(int M, int N, int K, const float *A, int lda, int ta, c
 cudaError_t launch_gelu(long long n, const float *pre, float *out, cudaStream_t st);
 cudaError_t launch_gelu_back(long long n, const float *pre, float *d, cudaStream_t st);
 cudaError_t launch_colsum(int rows, int cols, const float *d, float *out, int accumulate, cudaStream_t st);
-cudaError_t launch_rownorm(int rows, int cols, const float *x, float *y, float *nrm, cudaStream_t st);
-cudaError_t launch_rownorm_back(int rows, int cols, const float *y, const float *nrm, float *d, cudaStream_t st);
 cudaError_t launch_infonce(int B, float tau, const float *S, float *dS, float *loss, cudaStream_t st);
 cudaError_t launch_adam(long long n, float *w, const float *g, float *m, float *v, float lr, int t, cudaStream_t st);
 cudaError_t launch_feat_nodes(const FeatArgs &a, cudaStream_t st);

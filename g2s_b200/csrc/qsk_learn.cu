@@ -115,34 +115,6 @@ __global__ void k_colsum(int rows, int cols, const float *__restrict__ d, float 
     out[c] = accumulate ? out[c] + s : s;
 }
 
-// rows normalised to unit length (norm kept for the backward pass)
-__global__ void k_rownorm(int rows, int cols, const float *__restrict__ x, float *__restrict__ y, float *__restrict__ nrm) {
-    const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
-    float s = 0.f;
-    for (int c = lane; c < cols; c += 32) s += x[(long long)r * cols + c] * x[(long long)r * cols + c];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const float n = sqrtf(s) + 1e-12f;
-    if (lane == 0 && nrm) nrm[r] = n;
-    for (int c = lane; c < cols; c += 32) y[(long long)r * cols + c] = x[(long long)r * cols + c] / n;
-}
-// d x = (d y - y (y . d y)) / |x|
-__global__ void k_rownorm_back(int rows, int cols, const float *__restrict__ y, const float *__restrict__ nrm,
-                               float *__restrict__ d) {
-    const int r = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-    const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
-    float s = 0.f;
-    for (int c = lane; c < cols; c += 32) s += y[(long long)r * cols + c] * d[(long long)r * cols + c];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const float n = nrm[r];
-    for (int c = lane; c < cols; c += 32) {
-        const long long i = (long long)r * cols + c;
-        d[i] = (d[i] - y[i] * s) / n;
-    }
-}
-
 // symmetric InfoNCE on logits L = S / tau (B x B, positives on the diagonal):
 // loss = (mean_i CE(row i) + mean_j CE(column j)) / 2; writes dS (the
 // gradient with respect to S) and adds the loss to *loss
@@ -402,14 +374,6 @@ cudaError_t launch_gelu_back(long long n, const float *pre, float *d, cudaStream
 }
 cudaError_t launch_colsum(int rows, int cols, const float *d, float *out, int accumulate, cudaStream_t st) {
     k_colsum<<<blocks_for(cols, 128), 128, 0, st>>>(rows, cols, d, out, accumulate);
-    return cudaGetLastError();
-}
-cudaError_t launch_rownorm(int rows, int cols, const float *x, float *y, float *nrm, cudaStream_t st) {
-    k_rownorm<<<blocks_for((long long)rows * 32, 256), 256, 0, st>>>(rows, cols, x, y, nrm);
-    return cudaGetLastError();
-}
-cudaError_t launch_rownorm_back(int rows, int cols, const float *y, const float *nrm, float *d, cudaStream_t st) {
-    k_rownorm_back<<<blocks_for((long long)rows * 32, 256), 256, 0, st>>>(rows, cols, y, nrm, d);
     return cudaGetLastError();
 }
 cudaError_t launch_infonce(int B, float tau, const float *S, float *dS, float *loss, cudaStream_t st) {
