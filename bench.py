@@ -529,6 +529,9 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain / fp32 comparison arms")
     ap.add_argument("--no-tune", action="store_true",
                     help="whole-simulation tensor workloads: the automatic settings instead of the autotuner's")
+    ap.add_argument("--tune-cache", default="",
+                    help="autotuner cache file (default: a new one per run); a run given the file of an earlier run "
+                         "reuses its choice (profiling)")
     ap.add_argument("--grid", type=int, default=0,
                     help="profiling only: simulation grid side (2-D whole-simulation workloads); not a bench line")
     args = ap.parse_args()
@@ -576,7 +579,7 @@ def main():
         from g2s_b200 import autotune as at
         t0 = time.perf_counter()
         tuned = at.tune(ti, w["types"], w["n"], w["k"], mode=path, device=dev,
-                        cache=os.path.join(tempfile.gettempdir(), f"g2s_b200_tune_{os.getpid()}.json"))
+                        cache=args.tune_cache or os.path.join(tempfile.gettempdir(), f"g2s_b200_tune_{os.getpid()}.json"))
         tune_s = time.perf_counter() - t0
         log(f"tuned: {tuned}")
 
