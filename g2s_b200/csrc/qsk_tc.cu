@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(threads_for(W), 1)
         }
         unsigned long long root = 0ull;
         float thr = -INFINITY;
+        unsigned g_seen = 0u;   // largest value of the shared bound this thread has read or published
         int i = 0;
         for (long long t = t_begin; t < t_end; ++t, ++i) {
             const int b = i & 1;
@@ -358,6 +359,7 @@ __global__ void __launch_bounds__(threads_for(W), 1)
             const float s = nscale * (a.pos_scale ? __ldg(a.pos_scale + t) : 1.f);
             if (live && a.node_thr) {
                 const unsigned g = *(volatile unsigned *)(a.node_thr + node);
+                g_seen = g > g_seen ? g : g_seen;
                 if (g) thr = fmaxf(thr, unordered(g));
             }
             // TI coordinates of the tile's first position
@@ -441,9 +443,13 @@ __global__ void __launch_bounds__(threads_for(W), 1)
                 }
             }
             // publish this heap's minimum: a lower bound of the node's W-th best
-            // over all positions, which every range may filter against
-            if (live && root && a.node_thr) {
+            // over all positions, which every range may filter against.  The
+            // bound only grows, so a minimum at or below the value last read
+            // changes nothing: skipping it spares the bound's few cache lines,
+            // which every CTA of the launch reads and updates, most updates
+            if (live && root && a.node_thr && (unsigned)(root >> 32) > g_seen) {
                 atomicMax(a.node_thr + node, (unsigned)(root >> 32));
+                g_seen = (unsigned)(root >> 32);
             }
             tc_fence_before();
             __syncwarp();
