@@ -40,7 +40,9 @@ class QskParams(ctypes.Structure):
                 ("n", ctypes.c_int), ("k", ctypes.c_float), ("seed", ctypes.c_uint), ("no_verbatim", ctypes.c_int),
                 ("n_counts", ctypes.c_int), ("n_per_variable", _i32p), ("n_image_vars", ctypes.c_int),
                 ("n_image", _f32p), ("k_image", _f32p), ("n_kernels", ctypes.c_int), ("kernels_dims", _u32p),
-                ("kernels", ctypes.POINTER(_f32p)), ("kernel_index_image", _f32p), ("full_simulation", ctypes.c_int)]
+                ("kernels", ctypes.POINTER(_f32p)), ("kernel_index_image", _f32p), ("full_simulation", ctypes.c_int),
+                ("n_extra_tis", ctypes.c_int), ("extra_ti_dims", _u32p), ("extra_tis", ctypes.POINTER(_f32p)),
+                ("ti_index_image", _f32p)]
 
 
 class QskPatternOpts(ctypes.Structure):
@@ -369,12 +371,15 @@ class Simulation:
                  kernel: Optional[np.ndarray] = None, device: int = 0, no_verbatim: bool = False,
                  n_per_var: Optional[Sequence[int]] = None, ni: Optional[np.ndarray] = None,
                  kvi: Optional[np.ndarray] = None, kernels: Optional[Sequence[np.ndarray]] = None,
-                 kii: Optional[np.ndarray] = None, full: bool = False):
+                 kii: Optional[np.ndarray] = None, full: bool = False,
+                 extra_tis: Optional[Sequence[np.ndarray]] = None, ii: Optional[np.ndarray] = None):
         """Local controls as in G2S: ``n_per_var`` (-n n1 n2 ...), ``ni``
         (-ni image, grid shape [+ counts]), ``kvi`` (-kvi image), ``kernels``
         (the -ki list) with ``kii`` (-kii image of kernel indices); ``full``
         is -fs (one path node per cell value; the index image then has one
-        entry per value)."""
+        entry per value).  ``extra_tis``: further training images (-ti a b
+        ...; the index image holds TI cell * nTI + TI) with ``ii`` (-ii, the
+        TI each grid cell samples from)."""
         self.nvar = len(types)
         self._ti = np.ascontiguousarray(ti, dtype=np.float32)
         self._di = np.ascontiguousarray(di, dtype=np.float32)
@@ -416,6 +421,18 @@ class Simulation:
             self.params.kernels = ptrs
         if kii is not None:
             self.params.kernel_index_image = _p(keep(kii, np.float32), _f32p)
+        self.nti = 1
+        if extra_tis:
+            arrs = [keep(t, np.float32) for t in extra_tis]
+            dims = keep(np.concatenate([_grid_dims(np.asarray(t), self.nvar) for t in extra_tis]), np.uint32)
+            ptrs = (_f32p * len(arrs))(*[_p(a, _f32p) for a in arrs])
+            self._keep.append(ptrs)
+            self.params.n_extra_tis = len(arrs)
+            self.params.extra_ti_dims = _p(dims, _u32p)
+            self.params.extra_tis = ptrs
+            self.nti = 1 + len(arrs)
+        if ii is not None:
+            self.params.ti_index_image = _p(keep(ii, np.float32), _f32p)
         h = ctypes.c_void_p()
         _check(lib().qsk_sim_create(device, ctypes.byref(self.params), _p(self._di, _f32p), ctypes.byref(h)),
                "qsk_sim_create")

@@ -739,7 +739,17 @@ struct qsk_sim {
     DBuf<double> d_err_sum;
     DBuf<unsigned long long> d_err_n;
     int max_tc_slots = 0;
-    int sm_count = 0;                   // SMs of the device (grid sizing of the shortlist kernel)
+    int sm_count = 0;
+    // several training images: the TIs after ti, the -ii image, and every
+    // TI's K best per slot of a batch ([ti][slot][K], TI cells)
+    std::vector<qsk_ti *> xti;
+    DBuf<float> d_ii, d_mval;
+    DBuf<unsigned> d_mcell;
+    std::vector<qsk_ti *> all_tis() const {
+        std::vector<qsk_ti *> v{ti};
+        v.insert(v.end(), xti.begin(), xti.end());
+        return v;
+    }                   // SMs of the device (grid sizing of the shortlist kernel)
     // learned proposal (qsk_sim_set_learned): tensor mode 3
     qsk_encoder *enc = nullptr;
     qsk_learned_opts lopt{};
@@ -1920,6 +1930,115 @@ int tc_run(qsk_sim *s, const std::vector<int> &start, bool teacher) {
     return QSK_OK;
 }
 
+// several training images (the plain path): per batch and TI the exact map
+// and the reservoir k best with the same seed (quantileSamplingModule.hpp:
+// 455-575), each TI's K best kept as TI cells, then one merge and draw over
+// the TIs (k_multi_draw); levels in order on s->st
+int sim_batches_multi(qsk_sim *s, const std::vector<Step> &steps) {
+    const std::vector<qsk_ti *> tis = s->all_tis();
+    const int nti = int(tis.size());
+    const size_t stride = size_t(s->max_slots) * size_t(s->K);
+    CK(s->d_mval.ensure(stride * nti));
+    CK(s->d_mcell.ensure(stride * nti));
+    for (const Step &step : steps) {
+        const int B = step.B;
+        for (int t = 0; t < nti; ++t) {
+            const qsk_ti *T = tis[size_t(t)];
+            SimPrepArgs pa;
+            std::memset(&pa, 0, sizeof(pa));
+            pa.g = T->g;
+            pa.dg = s->dg;
+            pa.nvar = s->nvar;
+            pa.types = s->d_types.p;
+            pa.tpl = s->d_tpl.p;
+            pa.wtab = s->d_wtab.p;
+            pa.path = s->d_path.p;
+            pa.begin = s->begin;
+            pa.seeds = s->d_seeds.p;
+            pa.nb_count = s->d_nb_count.p;
+            pa.nb_tpl = s->d_nb_tpl.p;
+            pa.nb_cell = s->d_nb_cell.p;
+            pa.n = s->n;
+            pa.state = s->d_state.p;
+            pa.init = s->d_init.p;
+            pa.nodes = step.nodes + step.off;
+            pa.nslots = B;
+            pa.k = s->k;
+            pa.K = s->K;
+            pa.nti = unsigned(nti);
+            pa.slots = s->d_slots.p;
+            pa.terms = s->d_terms.p;
+            pa.maxterms = s->maxterms;
+            pa.status = s->d_status.p;
+            pa.mask_layer = s->nvar;
+            pa.id_image = s->d_id.p;
+            pa.sterms = nullptr;
+            CK(launch_prep_sim(pa, s->st));
+            MapArgs ma;
+            std::memset(&ma, 0, sizeof(ma));
+            ma.g = T->g;
+            ma.layers = T->layers.p;
+            ma.slots = s->d_slots.p;
+            ma.terms = s->d_terms.p;
+            ma.maxterms = s->maxterms;
+            ma.segs_per_cta = map_segs_per_cta(T->g, B);
+            ma.rec_val = s->d_rec_val.p;
+            ma.rec_idx = s->d_rec_idx.p;
+            ma.rec_cnt = s->d_rec_cnt.p;
+            ma.rec_max = s->d_rec_max.p;
+            CK(launch_map_records(ma, B, s->K, s->maxterms, s->st));
+            ReplayArgs ra;
+            std::memset(&ra, 0, sizeof(ra));
+            ra.g = T->g;
+            ra.slots = s->d_slots.p;
+            ra.nslots = B;
+            ra.K = s->K;
+            ra.rec_val = s->d_rec_val.p;
+            ra.rec_idx = s->d_rec_idx.p;
+            ra.rec_cnt = s->d_rec_cnt.p;
+            ra.rec_max = s->d_rec_max.p;
+            ra.out_val = s->d_mval.p + stride * size_t(t);
+            ra.out_pos = s->d_mcell.p + stride * size_t(t);
+            ra.out_cells = 1;
+            ra.nvar = s->nvar;
+            ra.ti = T->grid.p;
+            ra.ti_cells = T->cells;
+            ra.nti = unsigned(nti);
+            ra.ti_id = unsigned(t);
+            CK(launch_replay(ra, s->st));
+            s->info.launches += 3;
+            s->info.map_launches += 1;
+            s->info.map_positions += (long long)B * T->g.N;
+        }
+        MultiDrawArgs md;
+        md.slots = s->d_slots.p;
+        md.nslots = B;
+        md.K = s->K;
+        md.nti = nti;
+        md.nvar = s->nvar;
+        md.vals = s->d_mval.p;
+        md.cells = s->d_mcell.p;
+        md.ti_stride = (long long)stride;
+        for (int t = 0; t < nti; ++t) {
+            md.ti[t] = tis[size_t(t)]->grid.p;
+            md.ti_cells[t] = tis[size_t(t)]->cells;
+        }
+        md.types = s->d_types.p;
+        md.nb_count = s->d_nb_count.p;
+        md.nb_tpl = s->d_nb_tpl.p;
+        md.nb_cell = s->d_nb_cell.p;
+        md.n = s->n;
+        md.wtab = s->d_wtab.p;
+        md.ii = s->d_ii.p;
+        md.state = s->d_state.p;
+        md.id_image = s->d_id.p;
+        md.node_cell = s->d_node_cell.p;
+        CK(launch_multi_draw(md, s->st));
+        s->info.launches += 1;
+    }
+    return QSK_OK;
+}
+
 // the batch chain of a plain run captured into one CUDA graph (both
 // streams: the generator pipeline joins through its events), instantiated
 // and launched on s->st; the graph is released once the run has finished
@@ -1981,7 +2100,9 @@ void collect_profile(qsk_sim *s) {
 // fewer slots than the budget allows never maps the whole budget
 int sim_records(qsk_sim *s, long long slots) {
     const int n = int(std::max<long long>(1, std::min<long long>(slots, s->max_slots)));
-    cudaError_t e = ensure_records(s->ti->g, n, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max);
+    cudaError_t e = cudaSuccess;
+    for (qsk_ti *x : s->all_tis())
+        if (e == cudaSuccess) e = ensure_records(x->g, n, s->d_rec_val, s->d_rec_idx, s->d_rec_cnt, s->d_rec_max);
     if (e != cudaSuccess)
         return fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "records: %s", cudaGetErrorString(e));
     return QSK_OK;
@@ -2050,6 +2171,25 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         delete s;
         return rc;
     }
+    if (p->n_extra_tis > 0) {
+        if (!p->extra_ti_dims || !p->extra_tis) return bail(fail(QSK_ERR_ARG, "null extra training images"));
+        if (p->n_extra_tis + 1 > QSK_MAX_TIS)
+            return bail(fail(QSK_ERR_UNSUPPORTED, "%d training images (at most %d)", p->n_extra_tis + 1, QSK_MAX_TIS));
+        if ((p->n_extra_tis + 1) * K > 16)
+            return bail(fail(QSK_ERR_UNSUPPORTED, "%d candidates to merge (TIs x ceil(k), at most 16)",
+                             (p->n_extra_tis + 1) * K));
+        if (counts_given || p->k_image || p->kernel_index_image || p->n_kernels > 1 || s->full || s->no_verbatim)
+            return bail(fail(QSK_ERR_UNSUPPORTED, "several training images: no local controls, -fs or -nV"));
+        for (int t = 0; t < p->n_extra_tis; ++t) {
+            qsk_ti *x = nullptr;
+            rc = qsk_ti_create_grid(device, p->ndim, p->extra_ti_dims + size_t(t) * p->ndim, p->nvar, p->types,
+                                    p->extra_tis[t], &x);
+            if (rc) return bail(rc);
+            s->xti.push_back(x);
+        }
+        for (qsk_ti *x : s->all_tis())
+            if (x->missing) return bail(fail(QSK_ERR_UNSUPPORTED, "several training images: missing values"));
+    }
     if (s->full && s->ti->missing)
         return bail(fail(QSK_ERR_UNSUPPORTED, "-fs with missing training-image values is not implemented"));
     cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
@@ -2072,6 +2212,16 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     }
     if (s->cells >= (1LL << 32) - 1) return bail(fail(QSK_ERR_UNSUPPORTED, "grid too large"));
     s->init.assign(di_init, di_init + size_t(s->cells) * s->nvar);
+    if (p->ti_index_image) {
+        // -ii: the TI of each cell, int(value) (samplingModule.hpp:70-73); a
+        // negative value leaves the cell to every TI
+        const int nti = int(s->xti.size()) + 1;
+        for (long long c = 0; c < s->cells; ++c)
+            if (int(p->ti_index_image[c]) >= nti)
+                return bail(fail(QSK_ERR_ARG, "-ii: cell %lld names TI %d of %d", c, int(p->ti_index_image[c]), nti));
+        if ((e = s->d_ii.upload(p->ti_index_image, size_t(s->cells), s->st)) != cudaSuccess)
+            return bail(fail(QSK_ERR_CUDA, "-ii upload: %s", cudaGetErrorString(e)));
+    }
     // kernels: the -ki list, the given one, or uniform of size min(TI/2+1)
     // (src/qs.cpp:1000-1042); one sorted template per kernel
     std::vector<unsigned> kd(p->ndim);
@@ -2081,7 +2231,10 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
         for (int d = 0; d < p->ndim; ++d) kd[d] = p->kernel_dims[d];
         add_template(s, kd.data(), p->kernel);
     } else {
-        for (int d = 0; d < p->ndim; ++d) kd[d] = std::min(p->ti_dims[d] / 2 + 1, p->ti_dims[d]);
+        for (int d = 0; d < p->ndim; ++d) {
+            kd[d] = std::min(p->ti_dims[d] / 2 + 1, p->ti_dims[d]);
+            for (int t = 0; t < p->n_extra_tis; ++t) kd[d] = std::min(kd[d], p->extra_ti_dims[t * p->ndim + d] / 2 + 1);
+        }
         add_template(s, kd.data(), nullptr);
     }
     if (s->full) build_path_full(s);
@@ -2136,7 +2289,7 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
     }
     s->maxterms = std::max(1, s->n * s->nvar * (s->ti->missing ? 2 : 1));
     // bit-sliced map: every variable categorical with bit planes, unit weights
-    s->use_bits = s->ti->planes_ok && s->maxterms <= 255;
+    s->use_bits = s->ti->planes_ok && s->maxterms <= 255 && s->xti.empty();
     for (float wv : s->wtab) s->use_bits &= (wv == 1.f);
     // uploads
     if ((e = s->d_tpl.upload(s->tpl.data(), s->tpl.size(), s->st)) != cudaSuccess ||
@@ -2168,9 +2321,11 @@ int qsk_sim_create(int device, const qsk_qs_params *p, const float *di_init, qsk
                       (e = s->d_node_k.upload(s->node_k.data(), s->node_k.size(), s->st)) != cudaSuccess)))
         return bail(fail(e == cudaErrorMemoryAllocation ? QSK_ERR_NOMEM : QSK_ERR_CUDA, "upload: %s",
                          cudaGetErrorString(e)));
-    // batch scratch: slots up to a record budget of ~2 GiB
-    const Geom &g = s->ti->g;
-    size_t per_slot = size_t(g.nseg) * QSK_SEG * 8 + size_t(g.nseg) * 8 + sizeof(Term) * s->maxterms +
+    // batch scratch: slots up to a record budget of ~2 GiB (records sized
+    // for the largest training image)
+    int nseg_max = 0;
+    for (qsk_ti *x : s->all_tis()) nseg_max = std::max(nseg_max, x->g.nseg);
+    size_t per_slot = size_t(nseg_max) * QSK_SEG * 8 + size_t(nseg_max) * 8 + sizeof(Term) * s->maxterms +
                       (s->use_bits ? 2 * (sizeof(StaticTerm) * s->maxterms + sizeof(Slot)) : 0);
     size_t budget = size_t(2) << 30;
     long long ms = (long long)(budget / per_slot);
@@ -2258,7 +2413,9 @@ int qsk_sim_run(qsk_sim *s) {
     } else {
         rc = sim_records(s, mb);
         if (rc) return rc;
-        if (s->use_graph && !s->profiling)
+        if (!s->xti.empty())
+            rc = sim_batches_multi(s, plain_steps(s, start));
+        else if (s->use_graph && !s->profiling)
             rc = sim_batches_graph(s, plain_steps(s, start), &gexec);
         else
             rc = sim_batches(s, plain_steps(s, start), false);
@@ -2280,6 +2437,7 @@ int qsk_sim_run(qsk_sim *s) {
 
 int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *id_completed) {
     if (!s || !di_completed) return fail(QSK_ERR_ARG, "null argument");
+    if (!s->xti.empty()) return fail(QSK_ERR_UNSUPPORTED, "teacher forcing with several training images");
     if (s->no_verbatim && !id_completed) return fail(QSK_ERR_ARG, "-nV teacher forcing needs the index image");
     DeviceGuard dgd(s->device);
     CK(cudaMemcpyAsync(s->d_state.p, di_completed, sizeof(float) * s->init.size(), cudaMemcpyHostToDevice, s->st));
@@ -2311,6 +2469,7 @@ int qsk_sim_run_teacher(qsk_sim *s, const float *di_completed, const unsigned *i
 }
 
 int qsk_sim_run_teacher_nodes(qsk_sim *s, const float *di_completed, const int *path_nodes, int count) {
+    if (s && !s->xti.empty()) return fail(QSK_ERR_UNSUPPORTED, "teacher forcing with several training images");
     if (!s || !di_completed || (!path_nodes && count > 0) || count < 0) return fail(QSK_ERR_ARG, "null argument");
     if (s->no_verbatim) return fail(QSK_ERR_UNSUPPORTED, "-nV teacher forcing on a node sample");
     for (int q = 0; q < count; ++q)
@@ -2394,6 +2553,8 @@ int qsk_sim_set_profiling(qsk_sim *s, int on) {
 
 int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
     if (!s || !o) return fail(QSK_ERR_ARG, "null argument");
+    if (o->mode != 0 && !s->xti.empty())
+        return fail(QSK_ERR_UNSUPPORTED, "tensor-core form: one training image (several run on the plain path)");
     if (o->mode < 0 || o->mode > 2) return fail(QSK_ERR_ARG, "tensor mode %d (0 plain, 1 BF16, 2 FP8)", o->mode);
     if (!(o->audit >= 0.f && o->audit <= 1.f)) return fail(QSK_ERR_ARG, "audit fraction %g", double(o->audit));
     if (o->width != 0 && !tc_supported_width(o->width)) return fail(QSK_ERR_ARG, "width %d (8, 16 or 32)", o->width);
@@ -2420,6 +2581,7 @@ int qsk_sim_set_tensor(qsk_sim *s, const qsk_tensor_opts *o) {
 
 int qsk_sim_set_learned(qsk_sim *s, qsk_encoder *e, const qsk_learned_opts *o) {
     if (!s) return fail(QSK_ERR_ARG, "null sim");
+    if (e && !s->xti.empty()) return fail(QSK_ERR_UNSUPPORTED, "learned proposal: one training image");
     if (!e) {
         s->enc = nullptr;
         s->topt = qsk_tensor_opts{};
@@ -2655,6 +2817,8 @@ int qsk_sim_destroy(qsk_sim *s) {
         if (s->st) cudaStreamDestroy(s->st);
         s->st = nullptr;
         if (s->ti) qsk_ti_destroy(s->ti);
+        for (qsk_ti *x : s->xti) qsk_ti_destroy(x);
+        s->xti.clear();
         s->ti = nullptr;
         delete s;
     }

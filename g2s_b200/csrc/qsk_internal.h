@@ -214,7 +214,43 @@ struct ReplayArgs {
     // hash select: per path node, the drawn candidate's score (regret audit)
     float *drawn_score = nullptr;
     float *drawn_scale = nullptr;
+    // pattern outputs: out_pos holds TI cells (cvtIndexToPosition of the
+    // slot's geometry) instead of scan indices
+    int out_cells = 0;
 };
+
+// several training images (batched engine): per slot, every TI's K best
+// (vals / cells, [ti][slot][K], TI cells) merged and drawn as G2S does with
+// one CUDA device per TI (quantileSamplingModule.hpp:90-126): scores plus the
+// constant delta, stable sort of the TIs x K candidates, the slot's rank
+// (drawn with the TI count) naming TI and cell; slots flagged SLOT_SKIP draw
+// from the TIs' cells laid end to end (simulation.hpp:586-610); write-back of
+// the value and the index image (cell * nti + TI)
+#define QSK_MAX_TIS 8
+struct MultiDrawArgs {
+    const Slot *slots = nullptr;
+    int nslots = 0;
+    int K = 0;
+    int nti = 0;
+    int nvar = 0;
+    const float *vals = nullptr;
+    const unsigned *cells = nullptr;
+    long long ti_stride = 0;              // entries between two TIs' blocks of vals / cells
+    const float *ti[QSK_MAX_TIS] = {};    // TI grids (cells x nvar)
+    long long ti_cells[QSK_MAX_TIS] = {};
+    const int *types = nullptr;
+    // delta: the node's neighbours and weights
+    const int *nb_count = nullptr;
+    const int *nb_tpl = nullptr;
+    const unsigned *nb_cell = nullptr;
+    int n = 0;
+    const float *wtab = nullptr;          // ntpl x nvar
+    const float *ii = nullptr;            // -ii: the TI each grid cell samples from (null: all)
+    float *state = nullptr;
+    unsigned *id_image = nullptr;
+    unsigned *node_cell = nullptr;
+};
+cudaError_t launch_multi_draw(const MultiDrawArgs &a, cudaStream_t st);
 
 
 // record the calling thread's error message (qsk_last_error) and return code

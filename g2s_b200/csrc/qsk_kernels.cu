@@ -1872,8 +1872,19 @@ __global__ void __launch_bounds__(W == 1 ? 32 * RP_WARPS : 32 * W) k_replay(Repl
 #pragma unroll
             for (int j = 0; j < KM; ++j)
                 if (j < K) {
+                    unsigned out = fp[j];
+                    if (A.out_cells) {
+                        // cvtIndexToPosition (CPUThreadDevice.cpp:257-268)
+                        unsigned position = 0, div = (unsigned)g.N;
+                        for (int d = g.nd - 1; d >= 0; --d) {
+                            unsigned f = (unsigned)g.fft[d], sr = (unsigned)g.src[d];
+                            div /= f;
+                            position = position * sr + ((f - (out / div) % f - (unsigned)s.mn[d] - 1u) + sr) % sr;
+                        }
+                        out = position;
+                    }
                     A.out_val[(long long)b * K + j] = fv[j];
-                    A.out_pos[(long long)b * K + j] = fp[j];
+                    A.out_pos[(long long)b * K + j] = out;
                 }
         }
         if (A.state || A.node_cell) {
@@ -2857,6 +2868,91 @@ cudaError_t launch_radius_mask(const int *center, const float *radius, int nslot
                                long long xwords, cudaStream_t st) {
     if (nslots <= 0) return cudaSuccess;
     k_radius_mask<<<(unsigned)nslots, 256, 0, st>>>(center, radius, g, mask, xwords);
+    return cudaGetLastError();
+}
+
+// Several training images: one thread per slot merges every TI's K best
+// and draws (see MultiDrawArgs).  The merge is the reference's std::sort of
+// the TIs x K candidates by score (quantileSamplingModule.hpp:101-104),
+// which for at most 16 candidates is libstdc++'s insertion sort: stable.
+__global__ void k_multi_draw(MultiDrawArgs A) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= A.nslots) return;
+    const Slot s = A.slots[b];
+    const int nvar = A.nvar;
+    unsigned ti = 0, tcell = 0;
+    if (s.flags & SLOT_SKIP) {
+        // marginal: the TIs' cells end to end (simulation.hpp:586-610)
+        unsigned cumulated = 0;
+        for (int t = 0; t < A.nti; ++t) cumulated += (unsigned)A.ti_cells[t] * (unsigned)nvar;
+        const unsigned position =
+            (unsigned)(int)floorf(__fmul_rn(s.seed, __uint2float_rn(cumulated / (unsigned)nvar)));
+        cumulated = 0;
+        for (int t = 0; t < A.nti; ++t) {
+            const unsigned size = (unsigned)A.ti_cells[t] * (unsigned)nvar;
+            if (position * (unsigned)nvar < cumulated + size) {
+                ti = (unsigned)t;
+                tcell = position - cumulated / (unsigned)nvar;
+                break;
+            }
+            cumulated += size;
+        }
+    } else {
+        // delta = sum over continuous variables, then neighbours, of
+        // -1 * (w * v * v) in the reference's float order
+        // (quantileSamplingModule.hpp:412-457)
+        float delta = 0.f;
+        const int cnt = A.nb_count[s.node];
+        for (int i = 0; i < nvar; ++i) {
+            if (A.types[i] != 0) continue;
+            for (int j = 0; j < cnt; ++j) {
+                const unsigned c = A.nb_cell[(long long)s.node * A.n + j];
+                const float v = A.state[(long long)c * nvar + i];
+                if (isnan(v)) continue;
+                const float w = A.wtab[(long long)A.nb_tpl[(long long)s.node * A.n + j] * nvar + i];
+                delta = __fadd_rn(delta, __fmul_rn(-1.f, __fmul_rn(__fmul_rn(w, v), v)));
+            }
+        }
+        const int req = A.ii ? (int)A.ii[s.cell] : -1;
+        float v[16];
+        int o[16];
+        const int m = A.nti * A.K;
+        for (int q = 0; q < m; ++q) {
+            const int t = q / A.K;
+            v[q] = (req < 0 || t == req) ? __fadd_rn(A.vals[t * A.ti_stride + (long long)b * A.K + q % A.K], delta)
+                                         : -CUDART_INF_F;
+            o[q] = q;
+        }
+        for (int q = 1; q < m; ++q) {
+            const float x = v[q];
+            const int y = o[q];
+            int j = q;
+            while (j > 0 && x > v[j - 1]) {
+                v[j] = v[j - 1];
+                o[j] = o[j - 1];
+                --j;
+            }
+            v[j] = x;
+            o[j] = y;
+        }
+        const int q = o[s.sel < m ? s.sel : m - 1];
+        ti = (unsigned)(q / A.K);
+        tcell = A.cells[ti * A.ti_stride + (long long)b * A.K + q % A.K];
+    }
+    if (A.node_cell) A.node_cell[s.node] = tcell;
+    if (A.state) {
+        for (int v2 = 0; v2 < nvar; ++v2) {
+            float *dst = A.state + (long long)s.cell * nvar + v2;
+            if (isnan(*dst)) *dst = A.ti[ti][(long long)tcell * nvar + v2];
+        }
+    }
+    if (A.id_image) A.id_image[s.cell] = tcell * (unsigned)A.nti + ti;
+}
+
+cudaError_t launch_multi_draw(const MultiDrawArgs &a, cudaStream_t st) {
+    if (a.nslots <= 0) return cudaSuccess;
+    if (a.nti < 1 || a.nti > QSK_MAX_TIS || a.nti * a.K > 16) return cudaErrorInvalidValue;
+    k_multi_draw<<<(unsigned)((a.nslots + 127) / 128), 128, 0, st>>>(a);
     return cudaGetLastError();
 }
 

@@ -310,6 +310,16 @@ typedef struct {
     const float *kernel_index_image; /* -kii: kernel index per cell (required when n_kernels > 1) */
     int full_simulation;          /* -fs: one path node per (cell, variable) value (simulationFull,
                                      include/simulation.hpp:712-1066); index image per value */
+    /* Several training images (-ti with more than one grid, src/qs.cpp;
+     * merged as quantileSamplingModule.hpp:90-126 does with one CUDA device
+     * per TI): the grids after `ti`, each of ndim dims and nvar variables;
+     * complete TIs, one neighbour count, no -nV, -fs or local controls, the
+     * plain map, at most 8 TIs and 16 candidates (TIs x ceil(k)).  The index
+     * image holds TI cell * nTI + TI (simulation.hpp:658). */
+    int n_extra_tis;
+    const unsigned *extra_ti_dims; /* n_extra_tis * ndim, x first */
+    const float *const *extra_tis;
+    const float *ti_index_image;   /* -ii: the TI each grid cell samples from (its value, as an int); NULL: all */
 } qsk_qs_params;
 
 typedef struct {
