@@ -8,7 +8,7 @@
 // arguments follow G2S' own reader (include/utils.hpp:115-138: a flag
 // followed by its values) and the flags of src/qs.cpp:356-357,552-760.
 //
-//   qs_b200 -ti TI -di DI -k 1.5 -n 80 -s 100 [-ki K1 [K2 ...]] [-kii KII]
+//   qs_b200 -ti TI [TI2 ...] -di DI -k 1.5 -n 80 -s 100 [-ki K1 [K2 ...]] [-kii KII] [-ii II]
 //           [-ni NI] [-kvi KVI] [-fs] [-nV] [-id JOB] [-r REPORT] [-W_CUDA 0]
 //
 // Flags of the reference that this path does not implement (several
@@ -102,24 +102,34 @@ int main(int argc, char **argv) {
         return 1;
     };
     if (arg.count("-h") || arg.count("--help")) {
-        std::printf("qs_b200 -ti TI -di DI -k K -n N [N2 ...] -s SEED [-ki K1 ...] [-kii KII] [-ni NI] [-kvi KVI]\n"
-                    "        [-fs] [-nV] [-id JOB] [-r REPORT] [-W_CUDA DEVICE]\n");
+        std::printf("qs_b200 -ti TI [TI2 ...] -di DI -k K -n N [N2 ...] -s SEED [-ki K1 ...] [-kii KII] [-ni NI]\n"
+                    "        [-kvi KVI] [-ii II] [-fs] [-nV] [-id JOB] [-r REPORT] [-W_CUDA DEVICE]\n");
         return 0;
     }
-    static const std::set<std::string> known = {"-ti", "-di", "-dt", "-k", "-n", "-s", "-ki", "-kii", "-ni",
-                                                "-kvi", "-fs", "-nV", "-id", "-r", "-j", "-W_CUDA", "-W_GPU"};
+    static const std::set<std::string> known = {"-ti", "-di", "-dt", "-k", "-n", "-s", "-ki", "-kii", "-ni", "-kvi",
+                                                "-ii", "-fs", "-nV", "-id", "-r", "-j", "-W_CUDA", "-W_GPU"};
     for (auto &kv : arg)
         if (!known.count(kv.first)) {
             std::string m = "flag " + kv.first + " is not implemented on the B200 path";
             return fail(m.c_str());
         }
-    if (arg.count("-ti") != 1) return fail("exactly one training image (-ti) is supported");
+    if (arg.count("-ti") < 1) return fail("-ti is required");
     if (!arg.count("-di")) return fail("-di is required");
     if (!arg.count("-n") && !arg.count("-ni")) return fail("number of neighbours (-n or -ni) is required");
 
-    Grid ti, di;
-    if (!load(arg.find("-ti")->second, ti, rep) || !load(arg.find("-di")->second, di, rep)) return fail("input grids");
-    if (ti.ndim != di.ndim || ti.nvar != di.nvar) return fail("training image and grid differ in dimensions or variables");
+    // training images in the order given (-ti a b ... ; src/qs.cpp reads them so)
+    std::vector<Grid> tis;
+    for (auto it = arg.equal_range("-ti").first; it != arg.equal_range("-ti").second; ++it) {
+        Grid g;
+        if (!load(it->second, g, rep)) return fail("training image grid");
+        tis.push_back(std::move(g));
+    }
+    Grid di;
+    if (!load(arg.find("-di")->second, di, rep)) return fail("input grid");
+    const Grid &ti = tis[0];
+    for (const Grid &t : tis)
+        if (t.ndim != di.ndim || t.nvar != di.nvar)
+            return fail("training images and grid differ in dimensions or variables");
 
     std::vector<int> nlist;
     for (auto it = arg.equal_range("-n").first; it != arg.equal_range("-n").second; ++it)
@@ -148,6 +158,23 @@ int main(int argc, char **argv) {
     p.seed = seed;
     p.no_verbatim = arg.count("-nV") ? 1 : 0;
     p.full_simulation = arg.count("-fs") ? 1 : 0;
+    std::vector<unsigned> xdims;
+    std::vector<const float *> xptr;
+    for (size_t t = 1; t < tis.size(); ++t) {
+        for (int d = 0; d < tis[t].ndim; ++d) xdims.push_back(tis[t].dims[d]);
+        xptr.push_back(tis[t].data.data());
+    }
+    if (!xptr.empty()) {
+        p.n_extra_tis = int(xptr.size());
+        p.extra_ti_dims = xdims.data();
+        p.extra_tis = xptr.data();
+    }
+    Grid ii;
+    if (arg.count("-ii")) {
+        if (!load(arg.find("-ii")->second, ii, rep)) return fail("-ii grid");
+        if (ii.cells() != di.cells()) return fail("-ii grid size differs from -di");
+        p.ti_index_image = ii.data.data();
+    }
 
     // kernels: one weight per cell and variable (a one-variable kernel is
     // shared by all variables, as G2S reads it with i % nbVariable)

@@ -33,7 +33,7 @@ def grf(shape, ranges, seed: int) -> np.ndarray:
     spec = np.sqrt(np.maximum(spec, 0.0))
     rng = np.random.default_rng(seed)
     noise = rng.standard_normal(big)
-    field = np.fft.irfftn(np.fft.rfftn(noise) * spec, s=big)
+    field = np.fft.irfftn(np.fft.rfftn(noise) * spec, s=big, axes=tuple(range(len(big))))
     field = field[tuple(slice(0, s) for s in shape)]
     field = (field - field.mean()) / field.std()
     return field.astype(np.float32)

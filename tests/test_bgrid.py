@@ -61,10 +61,24 @@ def _cli():
 
 
 def test_cli_rejects_unimplemented_flags(tmp_path):
-    r = subprocess.run([_cli(), "-ti", "a", "b", "-di", "c", "-n", "5", "-k", "1.2"], capture_output=True, text=True)
-    assert r.returncode == 1 and "one training image" in r.stderr
     r = subprocess.run([_cli(), "-ti", "a", "-di", "c", "-n", "5", "-k", "1.2", "-csim"], capture_output=True, text=True)
     assert r.returncode == 1 and "-csim" in r.stderr
+
+
+def test_cli_checks_several_training_images(g2s, tmp_path):
+    """-ti a b: every training image must match the grid in dimensions and
+    variables, and an -ii grid must have the simulation grid's cells."""
+    env = dict(os.environ, G2S_DATA_DIR=str(tmp_path))
+    g2s.write_bgrid(str(tmp_path / "a.bgrid"), np.zeros((8, 8), np.float32), [0])
+    g2s.write_bgrid(str(tmp_path / "b.bgrid"), np.zeros((8, 8, 2), np.float32), [0, 0])
+    g2s.write_bgrid(str(tmp_path / "c.bgrid"), np.full((6, 6), np.nan, np.float32), [0])
+    g2s.write_bgrid(str(tmp_path / "ii.bgrid"), np.zeros((5, 5), np.float32), [0])
+    r = subprocess.run([_cli(), "-ti", "a", "b", "-di", "c", "-n", "5", "-k", "1.2"], capture_output=True, text=True,
+                       env=env)
+    assert r.returncode == 1 and "differ in dimensions or variables" in r.stderr
+    r = subprocess.run([_cli(), "-ti", "a", "a", "-di", "c", "-n", "5", "-k", "1.2", "-ii", "ii"], capture_output=True,
+                       text=True, env=env)
+    assert r.returncode == 1 and "-ii grid size" in r.stderr
 
 
 def test_cli_reports_missing_grid(tmp_path):

@@ -84,3 +84,31 @@ def test_auto_qs_cli_equals_calibrate(g2s, gpu, oracle, tmp_path):
                           else np.asarray(n).reshape(on.shape), on)
     assert np.array_equal(np.asarray(m).reshape(om.shape), om, equal_nan=True)
     assert np.array_equal(np.asarray(d).reshape(od.shape), od, equal_nan=True)
+
+
+@pytest.mark.parametrize("name", ["multi_ti_ii", "multi_ti3"])
+def test_cli_several_tis_equal_oracle(g2s, gpu, oracle, tmp_path, name):
+    """-ti a b [c] (and -ii) on the batched engine: the simulation and the
+    index image (TI cell * nTI + TI) equal the oracle's several-TI run."""
+    g = golden(name)
+    nti = int(g["nti"])
+    types = [int(t) for t in g["types"]]
+    tis = [g[f"ti{i}"] for i in range(nti)]
+    for i, t in enumerate(tis):
+        g2s.write_bgrid(str(tmp_path / f"ti{i}.bgrid"), t, types)
+    g2s.write_bgrid(str(tmp_path / "di.bgrid"), g["di"], types)
+    args = [EXE, "-ti"] + [f"ti{i}" for i in range(nti)] + ["-di", "di", "-k", str(float(g["k"])), "-n",
+                                                              str(int(g["n"])), "-s", str(int(g["seed"])),
+                                                              "-id", "job", "-W_CUDA", "0"]
+    ii = g["ii"] if "ii" in g else None
+    if ii is not None:
+        g2s.write_bgrid(str(tmp_path / "ii.bgrid"), ii, [0])
+        args += ["-ii", "ii"]
+    r = subprocess.run(args, capture_output=True, text=True, env=dict(os.environ, G2S_DATA_DIR=str(tmp_path)),
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    sim, _ = g2s.read_bgrid(str(tmp_path / "job.bgrid"))
+    idx, _ = g2s.read_bgrid(str(tmp_path / "id_job.bgrid"))
+    o = oracle.simulate_multi(tis, g["di"], types, int(g["n"]), float(g["k"]), int(g["seed"]), ii=ii)
+    assert np.array_equal(sim, o["sim"])
+    assert np.array_equal(idx.ravel(), o["id"])
