@@ -153,6 +153,11 @@ SIGNATURES = {
     "qsk_sim_set_level_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint, ctypes.c_longlong]),
     "qsk_sim_set_graph": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "qsk_jobs_run": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, _i32p]),
+    "qsk_blocks_set_limit": (ctypes.c_int, [ctypes.c_ulonglong]),
+    "qsk_blocks_release": (ctypes.c_int, []),
+    "qsk_blocks_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
+                                       ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
     "qsk_sim_set_tensor": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(QskTensorOpts)]),
     "qsk_simulate": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(QskParams), _f32p, _u32p]),
     "qsk_qs_template": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _u32p, _f32p, _i32p, _f32p, ctypes.c_int]),
@@ -654,6 +659,25 @@ def run_jobs(sims: Sequence["Simulation"], threads: int = 0) -> np.ndarray:
     status = np.zeros(max(n, 1), np.int32)
     _check(lib().qsk_jobs_run(arr, n, int(threads), _p(status, _i32p)), "qsk_jobs_run")
     return status[:n]
+
+
+def blocks_info(device: int = 0) -> dict:
+    """Device blocks kept from ended simulations (qsk_blocks_info): bytes and
+    blocks kept on ``device``, allocations served from them (hits) or not."""
+    by, nb, h, m = ctypes.c_ulonglong(), ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    _check(lib().qsk_blocks_info(int(device), ctypes.byref(by), ctypes.byref(nb), ctypes.byref(h), ctypes.byref(m)),
+           "qsk_blocks_info")
+    return {"bytes": by.value, "blocks": nb.value, "hits": h.value, "misses": m.value}
+
+
+def blocks_release() -> None:
+    """Free every kept device block (qsk_blocks_release)."""
+    _check(lib().qsk_blocks_release(), "qsk_blocks_release")
+
+
+def blocks_set_limit(nbytes: int) -> None:
+    """Bytes kept per device from ended simulations (0: keep none)."""
+    _check(lib().qsk_blocks_set_limit(int(nbytes)), "qsk_blocks_set_limit")
 
 
 def measure_peaks(device: int = 0) -> dict:

@@ -374,10 +374,8 @@ int qsk_encoder_add_pairs_host(qsk_encoder *e, long long n, const float *xq, con
             QSK_CK(cudaMemcpyAsync(p2.p, e->xp.p, sizeof(float) * size_t(e->npairs) * rowf, cudaMemcpyDeviceToDevice, e->st));
             QSK_CK(cudaStreamSynchronize(e->st));
         }
-        std::swap(e->xq.p, q2.p);
-        std::swap(e->xq.n, q2.n);
-        std::swap(e->xp.p, p2.p);
-        std::swap(e->xp.n, p2.n);
+        e->xq.swap(q2);
+        e->xp.swap(p2);
         e->pair_cap = cap;
     }
     QSK_CK(cudaMemcpyAsync(e->xq.p + size_t(e->npairs) * rowf, xq, sizeof(float) * size_t(n) * rowf,

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <chrono>
@@ -54,7 +55,91 @@ int set_error(int code, const char *fmt, ...) {
     g_err = buf;
     return code;
 }
+
+// Kept device blocks (DBuf::alloc / DBuf::release): per device, by size.
+namespace {
+struct KeptBlocks {
+    std::mutex mu;
+    std::map<int, std::multimap<size_t, void *>> free;   // device -> cap -> block
+    std::map<int, size_t> bytes;
+    unsigned long long limit = 8ull << 30;               // per device
+    long long hits = 0, misses = 0;
+};
+KeptBlocks &kept() {
+    static KeptBlocks *k = new KeptBlocks();   // never destroyed: no CUDA call at process exit
+    return *k;
+}
+}  // namespace
+
+thread_local bool g_keep_blocks = false;
+
+void *block_take(size_t bytes, size_t *cap) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    KeptBlocks &k = kept();
+    std::lock_guard<std::mutex> lock(k.mu);
+    auto f = k.free.find(dev);
+    if (f == k.free.end() || f->second.empty()) {
+        ++k.misses;
+        return nullptr;
+    }
+    auto it = f->second.lower_bound(bytes);
+    if (it == f->second.end() || it->first > 2 * bytes + (2u << 20)) {
+        ++k.misses;
+        return nullptr;
+    }
+    void *p = it->second;
+    *cap = it->first;
+    k.bytes[dev] -= it->first;
+    f->second.erase(it);
+    ++k.hits;
+    return p;
+}
+
+bool block_keep(void *p, size_t cap) {
+    int dev = -1;
+    if (!p || cap == 0 || cudaGetDevice(&dev) != cudaSuccess) return false;
+    KeptBlocks &k = kept();
+    std::lock_guard<std::mutex> lock(k.mu);
+    if (k.bytes[dev] + cap > k.limit) return false;
+    k.free[dev].emplace(cap, p);
+    k.bytes[dev] += cap;
+    return true;
+}
 }  // namespace qsk
+
+int qsk_blocks_set_limit(unsigned long long bytes) {
+    KeptBlocks &k = kept();
+    std::lock_guard<std::mutex> lock(k.mu);
+    k.limit = bytes;
+    return QSK_OK;
+}
+
+int qsk_blocks_release(void) {
+    KeptBlocks &k = kept();
+    std::lock_guard<std::mutex> lock(k.mu);
+    int rc = QSK_OK;
+    for (auto &f : k.free) {
+        DeviceGuard dg(f.first);
+        for (auto &b : f.second)
+            if (cudaFree(b.second) != cudaSuccess && rc == QSK_OK)
+                rc = fail(QSK_ERR_CUDA, "cudaFree of a kept block on device %d", f.first);
+        f.second.clear();
+        k.bytes[f.first] = 0;
+    }
+    return rc;
+}
+
+int qsk_blocks_info(int device, unsigned long long *bytes, long long *blocks, long long *hits, long long *misses) {
+    KeptBlocks &k = kept();
+    std::lock_guard<std::mutex> lock(k.mu);
+    auto f = k.free.find(device);
+    if (bytes) *bytes = k.bytes.count(device) ? k.bytes[device] : 0;
+    if (blocks) *blocks = f == k.free.end() ? 0 : (long long)f->second.size();
+    if (hits) *hits = k.hits;
+    if (misses) *misses = k.misses;
+    return QSK_OK;
+}
 
 namespace {
 
@@ -2658,10 +2743,8 @@ int qsk_encoder_add_pairs(qsk_encoder *e, qsk_sim *s, const float *di_completed,
             CK(cudaMemcpyAsync(p2.p, e->xp.p, sizeof(float) * size_t(e->npairs) * rowf, cudaMemcpyDeviceToDevice, s->st));
             CK(cudaStreamSynchronize(s->st));
         }
-        std::swap(e->xq.p, q2.p);
-        std::swap(e->xq.n, q2.n);
-        std::swap(e->xp.p, p2.p);
-        std::swap(e->xp.n, p2.n);
+        e->xq.swap(q2);
+        e->xp.swap(p2);
         e->pair_cap = cap;
     }
     DBuf<unsigned> dcells;
@@ -2739,10 +2822,7 @@ int qsk_jobs_run(qsk_sim *const *sims, int count, int threads, int *status) {
         DBuf<float> pscale;
     };
     auto swap_scratch = [](qsk_sim *s, Scratch &x) {
-        auto sw = [](auto &a, auto &b) {
-            std::swap(a.p, b.p);
-            std::swap(a.n, b.n);
-        };
+        auto sw = [](auto &a, auto &b) { a.swap(b); };
         sw(s->d_rec_val, x.rv);
         sw(s->d_rec_idx, x.ri);
         sw(s->d_rec_cnt, x.rc);
@@ -2804,6 +2884,10 @@ int qsk_sim_destroy(qsk_sim *s) {
     if (!s) return QSK_OK;
     {
         DeviceGuard dgd(s->device);
+        // the simulation's device buffers go to the kept blocks (reused by
+        // the next simulations of this device) once nothing on the device
+        // reads them any more: cudaFree would wait for the device as well
+        g_keep_blocks = cudaDeviceSynchronize() == cudaSuccess;
         for (auto e : s->prof_ev) cudaEventDestroy(e);
         for (auto e : s->tc_ev) cudaEventDestroy(e);
         for (int p = 0; p < 2; ++p) {
@@ -2821,6 +2905,7 @@ int qsk_sim_destroy(qsk_sim *s) {
         s->xti.clear();
         s->ti = nullptr;
         delete s;
+        g_keep_blocks = false;
     }
     return QSK_OK;
 }

@@ -226,8 +226,7 @@ int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, floa
  * (from several threads, or on several streams) race on it and give wrong
  * results; serialise them.
  * The first call on a device looks the scratch address up with
- * cudaGetSymbolAddress (with that device current, the return code checked);
- * make that first call before any stream capture begins.
+ * cudaGetSymbolAddress (with that device current, the return code checked).
  * `stream` is a cudaStream_t of ti's device (NULL: the legacy default
  * stream); the call returns after its work on that stream has finished. */
 #define QSK_NOALLOC_SCRATCH_BYTES (16u << 20)
@@ -413,7 +412,18 @@ int qsk_sim_set_graph(qsk_sim *s, int on);
 int qsk_jobs_run(qsk_sim *const *sims, int count, int threads, int *status);
 /* Path (cell order), per-path-index seeds and number of informed cells. */
 int qsk_sim_get_path(const qsk_sim *s, unsigned *order, float *seeds, unsigned *begin);
+/* Ends a simulation: waits for the device (as cudaFree does) and keeps the
+ * simulation's device buffers as blocks for the next simulations created on
+ * that device, up to a limit per device (default 8 GiB); buffers beyond it
+ * are freed.  No G2S counterpart: each G2S run allocates and frees its own. */
 int qsk_sim_destroy(qsk_sim *s);
+/* Kept blocks: the limit per device (0: keep none), freeing every kept block
+ * of every device (nothing reads them), and the kept bytes and blocks of one
+ * device with the process-wide count of allocations served from them (hits)
+ * or not (misses). */
+int qsk_blocks_set_limit(unsigned long long bytes);
+int qsk_blocks_release(void);
+int qsk_blocks_info(int device, unsigned long long *bytes, long long *blocks, long long *hits, long long *misses);
 
 /* Tensor-core form of the map (no G2S counterpart; it replaces, for the nodes
  * it can take, the per-node FFT correlation and k-best of

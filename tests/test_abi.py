@@ -85,3 +85,12 @@ def test_jobs_run_checks_arguments_without_a_gpu(g2s):
     arr = (__import__("ctypes").c_void_p * 2)(None, None)
     assert L.qsk_jobs_run(arr, 2, 2, None) != 0
     assert b"null simulation" in L.qsk_last_error()
+
+
+def test_kept_blocks_without_a_gpu(g2s):
+    """Nothing kept before any simulation ends; limit and release need no GPU."""
+    g2s.blocks_set_limit(1 << 30)
+    g2s.blocks_release()
+    info = g2s.blocks_info(0)
+    assert info["bytes"] == 0 and info["blocks"] == 0
+    g2s.blocks_set_limit(8 << 30)
