@@ -226,7 +226,10 @@ int qsk_calibrate(int device, const qsk_calib_params *p, float *mean_error, floa
  * (from several threads, or on several streams) race on it and give wrong
  * results; serialise them.
  * The first call on a device looks the scratch address up with
- * cudaGetSymbolAddress (with that device current, the return code checked).
+ * cudaGetSymbolAddress (with that device current, the return code checked)
+ * and keeps it for the life of the process: do not call it again after a
+ * cudaDeviceReset of that device (the module, and the scratch, reload at
+ * another address).
  * `stream` is a cudaStream_t of ti's device (NULL: the legacy default
  * stream); the call returns after its work on that stream has finished. */
 #define QSK_NOALLOC_SCRATCH_BYTES (16u << 20)
@@ -420,7 +423,9 @@ int qsk_sim_destroy(qsk_sim *s);
 /* Kept blocks: the limit per device (0: keep none), freeing every kept block
  * of every device (nothing reads them), and the kept bytes and blocks of one
  * device with the process-wide count of allocations served from them (hits)
- * or not (misses). */
+ * or not (misses).  Kept blocks belong to the device's primary context: call
+ * qsk_blocks_release before a cudaDeviceReset (or any reset of that context),
+ * after which they would no longer be valid device memory. */
 int qsk_blocks_set_limit(unsigned long long bytes);
 int qsk_blocks_release(void);
 int qsk_blocks_info(int device, unsigned long long *bytes, long long *blocks, long long *hits, long long *misses);
