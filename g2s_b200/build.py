@@ -40,6 +40,7 @@ def build_lib(force: bool = False) -> str:
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "qsk_internal.h"),
                                                        os.path.join(CSRC, "qsk_host_util.h"),
                                                        os.path.join(CSRC, "qsk_encoder.h"),
+                                                       os.path.join(CSRC, "qsk_pdl.cuh"),
                                                        os.path.join(ROOT, "include", "g2s_b200.h")]
     if not force and not _stale(LIB, deps):
         return LIB

@@ -1781,8 +1781,6 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
         int rc = enc_forward(e, B, B, s->d_feat.p, s->st);   // query head
         if (rc) return rc;
         CK(launch_to_bf16((long long)B * ENC_E, e->y.p, reinterpret_cast<uint16_t *>(s->d_tc_A.p), s->st));
-    } else {
-        CK(cudaMemsetAsync(s->d_tc_A.p, 0, size_t(Bp * s->tc_Kp * elem), s->st));
     }
     TcNodeArgs na{};
     na.nd = g.nd;
@@ -1808,7 +1806,9 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     na.L = s->tc_L;
     na.Kp = s->tc_Kp;
     na.fmt = s->tc_fmt;
-    na.A = learned ? nullptr : s->d_tc_A.p;
+    na.A = learned ? nullptr : s->d_tc_A.p;   // rows zeroed by the kernel
+    na.rows = Bp;
+    na.node_thr = s->d_tc_thr.p;
     na.node_scale = s->d_tc_nscale.p;
     na.node_bias = s->d_tc_bias.p;
     na.node_box = s->d_tc_box.p;
@@ -1855,7 +1855,6 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     a.out_key = s->d_tc_key.p;
     a.out_pos = s->d_tc_pos.p;
     a.status = s->d_status.p;
-    CK(cudaMemsetAsync(s->d_tc_thr.p, 0, sizeof(unsigned) * size_t(B), s->st));
     // learned proposal: the pattern matrix of the step's stencil scale
     const unsigned char *P = s->d_tc_P.p + (learned ? size_t(step.scale - 1) * size_t(s->tc_rows) * ENC_E * 2 : 0);
     CK(launch_tc_shortlist(s->tc_fmt, s->tc_W, s->d_tc_A.p, Bp, P, s->tc_rows, s->tc_Kp, a, s->st));

@@ -402,7 +402,9 @@ struct TcNodeArgs {
     int L;
     long long Kp;
     int fmt;
-    void *A;                   // slot rows x Kp (zeroed by the caller)
+    void *A;                   // rows x Kp, zeroed here (rows >= nslots: the padding rows too)
+    long long rows;
+    unsigned *node_thr;        // the shortlist's per-node bound, zeroed here (may be null)
     float *node_scale;
     float *node_bias;          // sum of the weights of neighbours in a variable's last category
     int *node_box;

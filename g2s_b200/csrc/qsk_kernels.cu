@@ -26,6 +26,7 @@
 #include <cstdint>
 
 #include "qsk_internal.h"
+#include "qsk_pdl.cuh"
 
 namespace qsk {
 
@@ -503,6 +504,7 @@ __device__ int verbatim_excl(const Geom &g, const int *tpl1, unsigned id_src, co
 }
 
 __global__ void k_prep_sim(SimPrepArgs A) {
+    griddep_launch();   // a programmatic successor (k_tc_nodes) may begin launching
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= A.nslots) return;

@@ -37,6 +37,7 @@
 #include <mutex>
 
 #include "qsk_internal.h"
+#include "qsk_pdl.cuh"
 
 namespace qsk {
 namespace tc {
@@ -230,6 +231,11 @@ __global__ void __launch_bounds__(threads_for(W), 1)
     __syncthreads();
     tc_fence_after();
     const unsigned tmem = tmem_base_s;
+    // launched programmatically after the kernel that writes A and the
+    // per-node bounds: the set-up above overlaps its end, nothing below
+    // reads or writes global memory before it has completed
+    griddep_wait();
+    griddep_launch();
 
     if (warp == 0) {
         // ---------------- TMA producer ----------------
@@ -679,8 +685,7 @@ cudaError_t launch_w(const CUtensorMap &ma, const CUtensorMap &mp, const TcArgs 
         }
     }
     dim3 grid((unsigned)node_tiles, (unsigned)a.ranges);
-    kern<<<grid, tc::threads_for(W), SMEM, st>>>(ma, mp, a);
-    return cudaGetLastError();
+    return launch_pdl(kern, grid, dim3(tc::threads_for(W)), SMEM, st, ma, mp, a);
 }
 
 }  // namespace
@@ -875,9 +880,21 @@ __global__ void k_tc_tmax(long long nodes, int n, const int *__restrict__ nb_cou
 // one warp per tensor slot: the node's row of A (coefficients of its terms at
 // their template columns), its validity box and tie seed
 __global__ void k_tc_nodes(TcNodeArgs A) {
+    griddep_wait();   // launched programmatically after k_prep_sim
+    griddep_launch();
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
+    if (A.A) {
+        // the warp's row of A starts as zeros (the entries below are sparse);
+        // a row is Kp * elem bytes, a multiple of 128
+        if (warp >= A.rows) return;
+        const long long rb = A.Kp * (A.fmt == 1 ? 1 : 2);
+        uint4 *row = reinterpret_cast<uint4 *>(static_cast<unsigned char *>(A.A) + (long long)warp * rb);
+        for (long long q = lane; q < rb / 16; q += 32) row[q] = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+    }
     if (warp >= A.nslots) return;
+    if (A.node_thr && lane == 0) A.node_thr[warp] = 0u;
     const int i = A.nodes[warp];
     const unsigned cell = A.path[A.begin + i];
     const int cnt = A.nb_count[i];
@@ -1022,6 +1039,7 @@ __global__ void __launch_bounds__(32 * SEL_WARPS) k_tc_select(TcSelectArgs A) {
     __shared__ unsigned long long skey[SEL_WARPS][SEL_CAND];
     __shared__ unsigned spos[SEL_WARPS][SEL_CAND];
     __shared__ Term sterm[SEL_WARPS][96];
+    griddep_wait();   // launched programmatically after the shortlist
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * SEL_WARPS + w;
     if (b >= A.nslots) return;
@@ -1385,15 +1403,16 @@ cudaError_t launch_tc_tmax(long long nodes, int n, const int *nb_count, const in
 }
 
 cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st) {
-    const long long blocks = ((long long)a.nslots * 32 + 255) / 256;
-    k_tc_nodes<<<(unsigned)blocks, 256, 0, st>>>(a);
-    return cudaGetLastError();
+    if (a.A && (a.rows < a.nslots || (a.Kp * (a.fmt == 1 ? 1 : 2)) % 16 != 0)) return cudaErrorInvalidValue;
+    const long long warps = a.A ? a.rows : a.nslots;
+    const long long blocks = (warps * 32 + 255) / 256;
+    return launch_pdl(k_tc_nodes, dim3((unsigned)blocks), dim3(256), 0, st, a);
 }
 
 cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st) {
     if (a.ncand > SEL_CAND || a.S > 32 * SEL_CPL) return cudaErrorInvalidValue;
-    k_tc_select<<<(unsigned)((a.nslots + SEL_WARPS - 1) / SEL_WARPS), 32 * SEL_WARPS, 0, st>>>(a);
-    return cudaGetLastError();
+    return launch_pdl(k_tc_select, dim3((unsigned)((a.nslots + SEL_WARPS - 1) / SEL_WARPS)), dim3(32 * SEL_WARPS), 0,
+                      st, a);
 }
 
 cudaError_t launch_tc_audit(int n, const int *nodes, int K, const float *plain_val, const float *drawn_score,
