@@ -662,7 +662,8 @@ def main():
         pass
     if gemm_dominant:
         k = kernels["k_tc_shortlist"]
-        launches_gemm = max(1, int(pinf["tensor_launches"]) // 4)
+        # per tensor step: terms + node rows (one launch; two when learned), shortlist, select
+        launches_gemm = max(1, int(pinf["tensor_launches"]) // (4 if path == "learned" else 3))
         roofline = {"bound": "tensor", "achieved": k["achieved_tflops"], "peak": k["peak_tflops"], "unit": "TFLOP/s",
                     "frac": k["frac"], "traffic": traffic, "kernel": "k_tc_shortlist", "peak_kind": tc_peak_kind,
                     "launches_per_step": launches_gemm,

@@ -41,6 +41,7 @@ def build_lib(force: bool = False) -> str:
                                                        os.path.join(CSRC, "qsk_host_util.h"),
                                                        os.path.join(CSRC, "qsk_encoder.h"),
                                                        os.path.join(CSRC, "qsk_pdl.cuh"),
+                                                       os.path.join(CSRC, "qsk_tc_nodes.cuh"),
                                                        os.path.join(ROOT, "include", "g2s_b200.h")]
     if not force and not _stale(LIB, deps):
         return LIB

@@ -1753,9 +1753,9 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     pa.node_k = nullptr;
     pa.full = 0;
     pa.nb_mask = nullptr;
-    CK(launch_prep_sim(pa, s->st));
     const bool learned = s->topt.mode == 3;
     if (learned) {
+        CK(launch_prep_sim(pa, s->st));
         // node rows of A: the encoder's embeddings of the nodes' neighbourhoods
         qsk_encoder *e = s->enc;
         FeatArgs fa;
@@ -1813,7 +1813,10 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     na.node_bias = s->d_tc_bias.p;
     na.node_box = s->d_tc_box.p;
     na.node_seed = s->d_tc_seed.p;
-    CK(launch_tc_nodes(na, s->st));
+    // the exact terms and the node rows in one launch (learned: the rows of
+    // A come from the encoder, after the terms)
+    if (learned) CK(launch_tc_nodes(na, s->st));
+    else CK(launch_prep_tc_nodes(pa, na, s->st));
     if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
     // GEMM shortlist: enough position ranges to fill the GPU, at most
     // SEL_CAND / W candidates per node.  With a shortlist of at most W the
@@ -1893,8 +1896,8 @@ int tc_step(qsk_sim *s, const Step &step, bool teacher) {
     }
     CK(launch_tc_select(sa, s->st));
     if (s->profiling) CK(cudaEventRecord(tc_event(s), s->st));
-    s->info.launches += 4;
-    s->info.tensor_launches += 4;
+    s->info.launches += learned ? 4 : 3;
+    s->info.tensor_launches += learned ? 4 : 3;
     if (learned) {
         // nodes whose confidence check failed: the exact map, in the same level
         std::vector<int> fb((size_t)B), nd((size_t)B);

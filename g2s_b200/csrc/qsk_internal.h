@@ -450,6 +450,9 @@ struct TcSelectArgs {
 cudaError_t launch_tc_pattern(const TcPatternArgs &a, float *rowmax, cudaStream_t st);
 cudaError_t launch_tc_tmax(long long nodes, int n, const int *nb_count, const int *nb_tpl, int *tmax, cudaStream_t st);
 cudaError_t launch_tc_nodes(const TcNodeArgs &a, cudaStream_t st);
+// k_prep_sim and k_tc_nodes of one tensor-core step in one launch (rows of A
+// written, not learned)
+cudaError_t launch_prep_tc_nodes(const SimPrepArgs &p, const TcNodeArgs &a, cudaStream_t st);
 cudaError_t launch_tc_select(const TcSelectArgs &a, cudaStream_t st);
 cudaError_t launch_tc_audit(int n, const int *nodes, int K, const float *plain_val, const float *drawn_score,
                             const float *drawn_scale, float tol, unsigned long long *counts, cudaStream_t st);

@@ -27,6 +27,7 @@
 
 #include "qsk_internal.h"
 #include "qsk_pdl.cuh"
+#include "qsk_tc_nodes.cuh"
 
 namespace qsk {
 
@@ -503,10 +504,8 @@ __device__ int verbatim_excl(const Geom &g, const int *tpl1, unsigned id_src, co
     return index < (unsigned)g.N ? int(index) : -1;
 }
 
-__global__ void k_prep_sim(SimPrepArgs A) {
-    griddep_launch();   // a programmatic successor (k_tc_nodes) may begin launching
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+// slot `warp` of a batch (one warp)
+__device__ __forceinline__ void prep_sim_warp(const SimPrepArgs &A, const int warp, const int lane) {
     if (warp >= A.nslots) return;
     const int i = A.nodes[warp];
     const unsigned pv = A.path[A.begin + i];
@@ -627,6 +626,22 @@ __global__ void k_prep_sim(SimPrepArgs A) {
     s.vcell = 0;
     s.vtpl = -1;
     if (lane == 0) A.slots[warp] = s;
+}
+
+__global__ void k_prep_sim(SimPrepArgs A) {
+    griddep_launch();   // a programmatic successor (k_tc_nodes) may begin launching
+    prep_sim_warp(A, int((blockIdx.x * blockDim.x + threadIdx.x) >> 5), int(threadIdx.x & 31));
+}
+
+// A tensor-core level's exact terms (k_prep_sim) and node rows (k_tc_nodes)
+// in one grid: blocks [0, prep_blocks) prepare the slots, the others write
+// the rows.  Neither part reads what the other writes (both read only the
+// neighbours, values and seeds of earlier levels), so they need no order.
+__global__ void k_prep_tc_nodes(SimPrepArgs P, TcNodeArgs T, unsigned prep_blocks) {
+    griddep_launch();   // the shortlist (a programmatic successor) may begin launching
+    const int lane = int(threadIdx.x & 31);
+    if (blockIdx.x < prep_blocks) prep_sim_warp(P, int((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane);
+    else tc_nodes_warp(T, int(((blockIdx.x - prep_blocks) * blockDim.x + threadIdx.x) >> 5), lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -2787,6 +2802,15 @@ cudaError_t launch_levels(const LevelArgs &a, cudaStream_t st) {
     k_scan_sums<<<1, 32, 0, st>>>((int)ntiles, a.tile_sum);
     k_scan_add<<<(unsigned)((nodes + 1 + 255) / 256), 256, 0, st>>>(nodes, a.start, a.cursor, a.tile_sum);
     k_level_scatter<<<nb, 256, 0, st>>>(nodes, a.level, a.cursor, a.level_nodes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prep_tc_nodes(const SimPrepArgs &p, const TcNodeArgs &a, cudaStream_t st) {
+    if (!a.A || a.nslots != p.nslots || a.rows < a.nslots || (a.Kp * (a.fmt == 1 ? 1 : 2)) % 16 != 0)
+        return cudaErrorInvalidValue;
+    const long long prep_blocks = ((long long)p.nslots * 32 + 255) / 256;
+    const long long node_blocks = (a.rows * 32 + 255) / 256;
+    k_prep_tc_nodes<<<(unsigned)(prep_blocks + node_blocks), 256, 0, st>>>(p, a, (unsigned)prep_blocks);
     return cudaGetLastError();
 }
 
