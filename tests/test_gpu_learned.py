@@ -1,7 +1,7 @@
 """Learned proposal: the encoder's FP32 forward and backward kernels against
 the float64 CPU oracle (oracle/encoder_oracle.py), training on pairs the
-exact path draws, and the learned map inside the simulation judged by the
-plain path (regret audit), with and without training."""
+exact path draws, and the learned map inside the simulation audited on the
+plain path (regret), with and without training."""
 import numpy as np
 import pytest
 

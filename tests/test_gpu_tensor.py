@@ -1,8 +1,8 @@
 """Tensor-core form of the map inside the batched simulation (tcgen05, BF16
-and FP8 E4M3, shortlist re-scored exactly) judged by the plain path.
+and FP8 E4M3, shortlist re-scored exactly) audited by the plain path.
 
 The plain path is pinned bit for bit to the oracle (test_gpu_sim.py); here
-it is the judge: every tensor-path node is re-run on it, teacher-forced on
+it is the audit: every tensor-path node is re-run on it, teacher-forced on
 the final grid (audit fraction 1), and `regret` counts the nodes whose drawn
 candidate scores below the exact k-th best (the metric's k-best regret).
 Categorical patterns with unit weights are exact in both formats (0/1
