@@ -8,6 +8,7 @@ which is built only where the G2S sources are present:
 
     make -C oracle && python tests/golden/make_golden.py
     python tests/golden/make_golden.py multi     # several training images
+    python tests/golden/make_golden.py kernel    # one -ki weight kernel
 """
 import os
 import sys
@@ -28,6 +29,8 @@ CASES = {
     "bivar2d_small": (lambda: syn.bivariate(syn.grf((64, 64), (8, 8), seed=2), 0.7), (32, 32, 2), [0, 1], 1.2, 16, 7),
     "grf3d_small": (lambda: syn.grf((16, 20, 24), (5, 6, 6), seed=4), (8, 12, 12), [0], 1.2, 12, 11),
     "grf2d_k3": (lambda: syn.grf((48, 48), (6, 6), seed=5), (30, 30), [0], 3.0, 12, 3),
+    # three facies (codes 0, 1, 2: a GRF cut at its terciles), categorical
+    "cat3_small": (lambda: facies3(syn.grf((64, 64), (7, 7), seed=9)), (36, 36), [1], 1.5, 16, 21),
     # configuration 0: 200x200 GRF (range 12), unconditional 200x200, n=50, k=1.2, seed 100
     "config0": (lambda: syn.grf((200, 200), (12, 12), seed=1), (200, 200), [0], 1.2, 50, 100),
 }
@@ -110,6 +113,34 @@ def make_bgrid():
     print("bgrid fixtures", a.shape)
 
 
+# one weight kernel (-ki): name -> (ti builder, di shape, types, k, n, seed, kernel builder).  Real-valued
+# weights make categorical match scores rarely tie, so most nodes are decided
+KERNEL = {
+    "cat3_ki": (lambda: facies3(syn.grf((64, 64), (7, 7), seed=9)), (36, 36), [1], 1.5, 16, 21,
+                lambda: gauss_kernel(15, 3.0)),
+}
+
+
+def gauss_kernel(size, sigma):
+    r = np.arange(size) - size // 2
+    yy, xx = np.meshgrid(r, r, indexing="ij")
+    return np.exp(-(yy * yy + xx * xx) / (2.0 * sigma * sigma)).astype(np.float32)
+
+
+def make_kernel(names=None):
+    for name, (mk, dshape, types, k, n, seed, kmk) in KERNEL.items():
+        if names and name not in names:
+            continue
+        ti = mk()
+        di = np.full(dshape, np.nan, np.float32)
+        kern = kmk()
+        args = ["-k", str(k), "-n", str(n), "-s", str(seed), "-j", "1"]
+        sim, idx, ms, _ = ref.run_qs(ti, di, types, args, images={"-ki": [(kern, [0])]}, job_id=3300 + len(name))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k, n=n,
+                            seed=seed, sim=sim, idx=idx, ref_ms=ms, kernel=kern)
+        print(name, ti.shape, dshape, "kernel", kern.shape)
+
+
 def make_local(names=None):
     for name, (mk, dshape, types, k, n, seed, what) in LOCAL.items():
         if names and name not in names:
@@ -132,6 +163,12 @@ def make_local(names=None):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), ti=ti, di=di, types=np.array(types), k=k,
                             n=np.array(-1 if n is None else n), seed=seed, sim=sim, idx=idx, ref_ms=ms, **arrs)
         print(name, ti.shape, dshape, sorted(arrs))
+
+
+def facies3(field):
+    """Three categories: a continuous field cut at its terciles (codes 0, 1, 2)."""
+    lo, hi = np.quantile(field, [1.0 / 3.0, 2.0 / 3.0])
+    return np.where(field < lo, 0.0, np.where(field < hi, 1.0, 2.0)).astype(np.float32)
 
 
 def holes(field, seed):
@@ -228,5 +265,7 @@ if __name__ == "__main__":
         make_bgrid()
     elif args[:1] == ["multi"]:
         make_multi(args[1:])
+    elif args[:1] == ["kernel"]:
+        make_kernel(args[1:])
     else:
         main(args)

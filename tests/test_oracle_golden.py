@@ -17,7 +17,8 @@ def test_oracle_sequential_equals_reference(oracle, name):
     assert np.array_equal(out["id"], g["idx"].ravel())
 
 
-@pytest.mark.parametrize("name", ["grf2d_small", "cat2d_small", "bivar2d_small", "grf3d_small", "grf2d_k3"])
+@pytest.mark.parametrize("name", ["grf2d_small", "cat2d_small", "bivar2d_small", "grf3d_small", "grf2d_k3",
+                                  "cat3_small"])
 def test_oracle_teacher_forced_outside_near_ties(oracle, name):
     g = golden(name)
     types = [int(t) for t in g["types"]]
@@ -27,6 +28,23 @@ def test_oracle_teacher_forced_outside_near_ties(oracle, name):
     ref_cells = g["idx"].ravel()[order[begin:]]
     mismatch = tf["cell"] != ref_cells
     assert not np.any(mismatch & ~tf["near_tie"]), "draw differs from the reference outside near-ties"
+
+
+def test_oracle_three_facies_weighted_kernel_outside_near_ties(oracle):
+    """Three categories (codes 0, 1, 2) with a Gaussian -ki weight kernel:
+    real-valued weights leave fewer match-score ties than unit weights, so
+    a large share of the nodes is decided, and every decided node draws the
+    reference's TI cell."""
+    g = golden("cat3_ki")
+    kern = g["kernel"]
+    tf = oracle.simulate(g["ti"], g["sim"], [1], int(g["n"]), float(g["k"]), int(g["seed"]), mode=1,
+                         want_fp64=True, di_init=g["di"], kernel=kern, kdims=kern.shape[::-1])
+    order, seeds, post, begin = oracle.path(g["di"], 1, int(g["seed"]))
+    ref_cells = g["idx"].ravel()[order[begin:]]
+    decided = ~tf["near_tie"]
+    assert decided.sum() > 0.3 * len(ref_cells)
+    assert np.array_equal(tf["cell"][decided], ref_cells[decided])
+    assert set(np.unique(g["sim"])) == {0.0, 1.0, 2.0}
 
 
 def test_oracle_config0_prefix_teacher_forced(oracle):
