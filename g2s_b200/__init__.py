@@ -711,17 +711,25 @@ def tc_topk(queries: np.ndarray, rows: np.ndarray, fmt: int, X: int, Y: int, box
     return keys, pos
 
 
-def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
+def qs(ti, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
        ki=None, nV: bool = False, ni: Optional[np.ndarray] = None, kvi: Optional[np.ndarray] = None,
        kii: Optional[np.ndarray] = None, fs: bool = False, device: int = 0, tensor=None,
-       audit: float = 0.01):
+       audit: float = 0.01, ii: Optional[np.ndarray] = None):
     """QuickSampling on one GPU; arguments named after the G2S flags
-    (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii -fs).  ``n`` is one count or one
-    per variable; ``ki`` one kernel or a list of kernels (selected per cell by
-    ``kii``).  ``tensor`` selects the tensor-core form of the map ("bf16" or
-    "fp8", or a dict {"mode", "prefix", "width", "shortlist", "batch"} such as
-    the autotuner's choice), with the regret audit fraction ``audit``; None is
-    the exact reference path.  Returns (simulation, index) as G2S does."""
+    (-ti -di -dt -k -n -s -ki -nV -ni -kvi -kii -fs -ii).  ``ti`` is one
+    training image or a list of them (-ti a b ...; the index image then holds
+    TI cell * number of TIs + TI, and ``ii`` may name each cell's TI).  ``n``
+    is one count or one per variable; ``ki`` one kernel or a list of kernels
+    (selected per cell by ``kii``).  ``tensor`` selects the tensor-core form of
+    the map ("bf16" or "fp8", or a dict {"mode", "prefix", "width",
+    "shortlist", "batch"} such as the autotuner's choice), with the regret
+    audit fraction ``audit``; None is the exact reference path.  Returns
+    (simulation, index) as G2S does."""
+    extra = None
+    if isinstance(ti, (list, tuple)):
+        if not ti:
+            raise ValueError("qs: no training image")
+        ti, extra = ti[0], list(ti[1:]) or None
     n_list = None
     if np.ndim(n) > 0:
         n_list = [int(x) for x in np.ravel(n)]
@@ -730,7 +738,8 @@ def qs(ti: np.ndarray, di: np.ndarray, dt: Sequence[int], k: float, n, s: int,
     if isinstance(ki, (list, tuple)):
         kernel, kernels = None, list(ki)
     sim = Simulation(ti, di, dt, n=n if n is not None else 0, k=k, seed=s, kernel=kernel, device=device,
-                     no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii, full=fs)
+                     no_verbatim=nV, n_per_var=n_list, ni=ni, kvi=kvi, kernels=kernels, kii=kii, full=fs,
+                     extra_tis=extra, ii=ii)
     try:
         if isinstance(tensor, dict):
             sim.set_tensor(tensor["mode"], prefix=int(tensor.get("prefix", 0)), width=int(tensor.get("width", 0)),

@@ -94,3 +94,10 @@ def test_kept_blocks_without_a_gpu(g2s):
     info = g2s.blocks_info(0)
     assert info["bytes"] == 0 and info["blocks"] == 0
     g2s.blocks_set_limit(8 << 30)
+
+
+def test_qs_needs_a_training_image(g2s):
+    """qs() takes one training image or a list (-ti a b ...); an empty list is
+    refused before any device work."""
+    with pytest.raises(ValueError):
+        g2s.qs([], np.full((8, 8), np.nan, np.float32), [0], k=1.2, n=4, s=1)
