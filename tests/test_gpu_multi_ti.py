@@ -41,3 +41,13 @@ def test_batched_several_tis_rejections(g2s, gpu):
     with pytest.raises(RuntimeError):   # -ii naming a third TI
         g2s.Simulation(tis[0], g["di"], [0], n=12, k=1.2, seed=7, extra_tis=tis[1:],
                        ii=np.full(g["di"].shape, 2.0, np.float32))
+
+
+def test_one_call_qs_with_several_tis_equals_oracle(g2s, gpu, oracle):
+    """The one-call API with a list of training images and -ii."""
+    g = golden("multi_ti_ii")
+    tis = [g["ti0"], g["ti1"]]
+    out, idx = g2s.qs(tis, g["di"], [0], k=float(g["k"]), n=int(g["n"]), s=int(g["seed"]), ii=g["ii"])
+    o = oracle.simulate_multi(tis, g["di"], [0], int(g["n"]), float(g["k"]), int(g["seed"]), ii=g["ii"])
+    assert np.array_equal(out, o["sim"])
+    assert np.array_equal(idx.ravel(), o["id"])
