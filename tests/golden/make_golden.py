@@ -29,6 +29,9 @@ CASES = {
     "bivar2d_small": (lambda: syn.bivariate(syn.grf((64, 64), (8, 8), seed=2), 0.7), (32, 32, 2), [0, 1], 1.2, 16, 7),
     "grf3d_small": (lambda: syn.grf((16, 20, 24), (5, 6, 6), seed=4), (8, 12, 12), [0], 1.2, 12, 11),
     "grf1d_small": (lambda: syn.grf((400,), (8,), seed=17), (150,), [0], 1.2, 10, 33),
+    # 3-D bivariate (continuous + indicator), the kind of data of configuration 4
+    "bivar3d_small": (lambda: syn.bivariate(syn.grf((16, 20, 24), (4, 6, 6), seed=23)), (8, 10, 12, 2), [0, 1],
+                      1.5, 14, 41),
     "grf2d_k3": (lambda: syn.grf((48, 48), (6, 6), seed=5), (30, 30), [0], 3.0, 12, 3),
     # three facies (codes 0, 1, 2: a GRF cut at its terciles), categorical
     "cat3_small": (lambda: facies3(syn.grf((64, 64), (7, 7), seed=9)), (36, 36), [1], 1.5, 16, 21),

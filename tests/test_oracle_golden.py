@@ -18,7 +18,7 @@ def test_oracle_sequential_equals_reference(oracle, name):
 
 
 @pytest.mark.parametrize("name", ["grf2d_small", "cat2d_small", "bivar2d_small", "grf3d_small", "grf2d_k3",
-                                  "cat3_small", "grf1d_small"])
+                                  "cat3_small", "grf1d_small", "bivar3d_small"])
 def test_oracle_teacher_forced_outside_near_ties(oracle, name):
     g = golden(name)
     types = [int(t) for t in g["types"]]
